@@ -1,0 +1,143 @@
+/*
+ * lsmoke_gpu.h -- C ABI of the B200 reaction step for laminarSMOKE.
+ *
+ * The laminarSMOKE unsteady solvers advance chemistry by operator splitting:
+ * every CFD cell is a constant-pressure batch reactor integrated over the
+ * cell's time step by the OpenSMOKE++ Gear/BDF multivalue solver.  In the
+ * reference this is a serial per-cell loop compiled into the solver
+ * (solvers/laminarSMOKE/unsteady/chemistry_DI.H:76-331).  This library
+ * replaces that loop with one batched call.  Plain C types only; no CUDA or
+ * torch types cross this boundary.
+ *
+ * Conventions
+ *   - Return value 0 = success, negative = library error (lsg_strerror).
+ *   - Per-cell ODE outcomes are written to status_out with the reference's
+ *     OdeStatus values (math/native-ode-solvers/OdeSolverUtilities.h:83-97):
+ *     2 = integrated, 0 = skipped (T <= tmin_chem), -1 max steps, -2 too
+ *     strict tolerances, -4 error-test failures, -5 convergence failures,
+ *     -6 step too small, -9 illegal initial constraints.  A failed cell keeps
+ *     its last accepted state (the reference would hand back stale data).
+ *   - Nothing exits, prints or blocks indefinitely.  One context per host
+ *     thread per GPU.  Host-pointer calls are synchronous.
+ */
+#ifndef LSMOKE_GPU_H
+#define LSMOKE_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LSG_ABI_VERSION 1
+
+/* library error codes */
+#define LSG_OK 0
+#define LSG_ERR_ARG -1         /* invalid argument */
+#define LSG_ERR_MECH -2        /* mechanism blob could not be read */
+#define LSG_ERR_CUDA -3        /* CUDA runtime error */
+#define LSG_ERR_NOMEM -4       /* device allocation failed */
+#define LSG_ERR_UNSUPPORTED -5 /* option or mechanism size not supported */
+#define LSG_ERR_DEVICE -6      /* a kernel reported an internal error flag */
+#define LSG_ERR_IO -7          /* file could not be read */
+
+/* precision / algorithm forms */
+#define LSG_PRECISION_FP64 0   /* plain: the reference method in FP64 */
+#define LSG_PRECISION_MIXED 1  /* FP64 rates/residual/error control, FP32 factorisation + FP64 refinement */
+
+/* counters per cell (lsg_reaction_step_device counters_out layout) */
+#define LSG_NCOUNTERS 8        /* steps, rhs, jacobians, factorisations, solves, error-test fails, convergence fails, jacobian rhs */
+
+typedef struct lsg_mech lsg_mech; /* device-resident mechanism tables */
+typedef struct lsg_ctx lsg_ctx;   /* per-thread, per-GPU context (stream + buffers) */
+
+/* Solver options.  Defaults (lsg_options_default) are the values the
+ * reference tutorials use (run/tutorials/ToroFlames/F3/.../solverOptions:60-64)
+ * and the bounds chemistry_DI.H:82-83 sets. */
+typedef struct lsg_options {
+  double rtol;          /* OdeHomogeneous relTolerance (1e-7) */
+  double atol;          /* OdeHomogeneous absTolerance (1e-12) */
+  double tmin_chem;     /* minTemperature4Chemistry: cells with T <= tmin_chem are skipped (0) */
+  double y_min_T;       /* lower bound on T during integration (200 K) */
+  double y_max_T;       /* upper bound on T during integration (6000 K) */
+  int max_steps;        /* maximum BDF steps per cell (500000) */
+  int full_pivoting;    /* must be 0: partial pivoting (fullPivoting false) */
+  int energy;           /* energy equation on (1) / off (0) */
+  int precision;        /* LSG_PRECISION_FP64 or LSG_PRECISION_MIXED */
+  /* Order-selection state of the reference's solver object: the Gear method
+   * lowers alfa2[4], alfa2[5] and its maximum order on every Newton
+   * convergence failure and never restores them between cells
+   * (MethodGear.hpp:361-385).  Defaults (0.8, 0.8, 5) are a fresh solver. */
+  double alfa2_4;
+  double alfa2_5;
+  int maximum_order;
+  int reserved[7];
+} lsg_options;
+
+void lsg_options_default(lsg_options* opt);
+
+/* ---- mechanism --------------------------------------------------------
+ * The blob is produced offline from CHEMKIN files by
+ * `python -m laminarsmoke_b200.mech compile KIN.CKI THERMO.CKT -o mech.lsmech`
+ * (it replaces openSMOKEppCHEMKINPreProcessor + kinetics.xml, which the
+ * reference loads at solvers/laminarSMOKE/readOptions.H:62-78). */
+int lsg_mech_load_blob(const void* blob, size_t nbytes, int device, lsg_mech** out);
+int lsg_mech_load_file(const char* path, int device, lsg_mech** out);
+int lsg_mech_info(const lsg_mech* mech, int* nspecies, int* nreactions);
+int lsg_mech_destroy(lsg_mech* mech);
+
+/* ---- context ---------------------------------------------------------- */
+int lsg_ctx_create(const lsg_mech* mech, const lsg_options* opt, int device, lsg_ctx** out);
+int lsg_ctx_set_options(lsg_ctx* ctx, const lsg_options* opt);
+int lsg_ctx_destroy(lsg_ctx* ctx);
+
+/* ---- reaction step, host arrays ----------------------------------------
+ * Replaces the OpenSMOKE branch of chemistry_DI.H:92-327 (and the
+ * SetReactor / SetInitialConditions / Solve / Solution / QR calls it makes,
+ * MultiValueSolver.hpp:367-617, BatchReactorHomogeneousConstantPressure.H:60,141).
+ *   Y_species  nspecies host pointers, each an array of ncells mass fractions
+ *              (OpenFOAM PtrList<volScalarField> layout); updated in place
+ *   T          [ncells] temperatures [K]; updated in place when energy is on
+ *   p          thermodynamic pressure [Pa]
+ *   t0         absolute start time (the initial step size depends on it)
+ *   dt         [ncells] per-cell time steps (local time stepping) or NULL
+ *   dt_scalar  time step used when dt is NULL
+ *   Q_out      [ncells] heat release rate [W/m3] or NULL
+ *   status_out [ncells] OdeStatus or NULL
+ *   nsteps_out [ncells] accepted BDF steps or NULL */
+int lsg_reaction_step(lsg_ctx* ctx, int ncells, int nspecies, double* const* Y_species, double* T, double p,
+                      double t0, const double* dt, double dt_scalar, double* Q_out, int* status_out,
+                      int* nsteps_out);
+
+/* ---- reaction step, device arrays (state resident in HBM) ---------------
+ * Y_dev is species-major: Y_dev[i * ld + cell], ld >= ncells.  All pointers are
+ * device pointers; stream is the cudaStream_t the work is enqueued on, used as
+ * given (NULL = the legacy default stream; lsg_ctx_stream returns the
+ * context's own stream).  Asynchronous: returns after enqueueing.
+ * counters_out (optional) receives LSG_NCOUNTERS int64 per cell. */
+int lsg_reaction_step_device(lsg_ctx* ctx, int ncells, int nspecies, double* Y_dev, long ld, double* T_dev,
+                             double p, double t0, const double* dt_dev, double dt_scalar, double* Q_dev,
+                             int* status_dev, int* nsteps_dev, long long* counters_dev, void* stream);
+
+/* The context's own stream (a cudaStream_t), for callers without one. */
+void* lsg_ctx_stream(lsg_ctx* ctx);
+
+/* Waits for the device, then reads and clears the error flags kernels raised
+ * (0 = none).  Returns LSG_ERR_DEVICE when a flag was set. */
+int lsg_ctx_check(lsg_ctx* ctx, int* device_flags);
+
+/* ---- right-hand side -----------------------------------------------------
+ * f(y) of the constant-pressure reactor for ncells states
+ * (BatchReactorHomogeneousConstantPressure::Equations, :175-223).
+ * y_dev/dy_dev are species-major [(nspecies+1) * ld], row nspecies = T. */
+int lsg_rhs_device(lsg_ctx* ctx, int ncells, const double* y_dev, double* dy_dev, long ld, double p,
+                   double* qr_dev, void* stream);
+
+const char* lsg_strerror(int code);
+int lsg_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LSMOKE_GPU_H */

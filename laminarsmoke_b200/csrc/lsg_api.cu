@@ -1,0 +1,357 @@
+// C ABI implementation (include/lsmoke_gpu.h): mechanism upload, contexts,
+// buffers, dispatch to the kernel translation units.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/lsmoke_gpu.h"
+#include "lsg_kernels.h"
+#include "lsg_mech_host.h"
+
+using namespace lsg;
+
+struct lsg_mech {
+  HostMech host;
+  int device = 0;
+  unsigned char* d_buf = nullptr;
+};
+
+struct lsg_ctx {
+  const lsg_mech* mech = nullptr;
+  lsg_options opt{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int* d_err = nullptr;
+  long cap = 0;
+  double* dY = nullptr;
+  double* dT = nullptr;
+  double* ddt = nullptr;
+  double* dQ = nullptr;
+  int* dstatus = nullptr;
+  int* dnsteps = nullptr;
+};
+
+namespace {
+
+std::mutex g_mutex;
+bool g_gear_uploaded[64] = {};
+
+GearConsts make_gear_consts() {
+  // MethodGear::MemoryAllocationMethod (MethodGear.hpp:125-193)
+  GearConsts g{};
+  auto fact = [](unsigned n) { unsigned r = 1; for (unsigned k = 2; k <= n; ++k) r *= k; return r; };
+  for (int j = 0; j <= 5; ++j) g.Ep[j] = (double)fact(j);
+  for (int i = 0; i <= 5; ++i)
+    for (int j = 0; j < 5; ++j) g.r[i][j] = 0.;
+  g.r[0][0] = 1.;
+  g.r[1][0] = 1.;
+  for (int j = 2; j <= 5; ++j) {
+    g.r[0][j - 1] = (double)fact(j);
+    for (int i = 2; i <= j; ++i) g.r[i - 1][j - 1] = double(j) * g.r[i - 1][j - 2] + g.r[i - 2][j - 2];
+    g.r[j][j - 1] = 1.;
+  }
+  double sum = 1.;
+  for (int j = 2; j <= 5; ++j) {
+    sum += 1. / double(j);
+    for (int i = 1; i <= j + 1; ++i) g.r[i - 1][j - 1] /= (fact(j) * sum);
+  }
+  return g;
+}
+
+int ensure_gear(int device) {
+  std::lock_guard<std::mutex> lk(g_mutex);
+  if (device < 0 || device >= 64) return LSG_ERR_ARG;
+  if (g_gear_uploaded[device]) return LSG_OK;
+  const GearConsts g = make_gear_consts();
+  if (upload_gear_plain(g) != cudaSuccess) return LSG_ERR_CUDA;
+  g_gear_uploaded[device] = true;
+  return LSG_OK;
+}
+
+StepOptions to_step_options(const lsg_options& o) {
+  StepOptions s{};
+  s.rtol = o.rtol;
+  s.atol = o.atol;
+  s.tmin_chem = o.tmin_chem;
+  s.y_min_T = o.y_min_T;
+  s.y_max_T = o.y_max_T;
+  s.max_steps = o.max_steps;
+  s.energy = o.energy;
+  s.alfa2_4 = o.alfa2_4;
+  s.alfa2_5 = o.alfa2_5;
+  s.maximum_order = o.maximum_order;
+  return s;
+}
+
+int validate_options(const lsg_options* o) {
+  if (!o) return LSG_ERR_ARG;
+  if (!(o->rtol >= 1.e-32) || !(o->atol >= 1.e-32)) return LSG_ERR_ARG;  // MultiValueSolver.hpp:183-199
+  if (o->max_steps <= 0) return LSG_ERR_ARG;
+  if (!(o->y_min_T < o->y_max_T)) return LSG_ERR_ARG;
+  if (o->full_pivoting != 0) return LSG_ERR_UNSUPPORTED;
+  if (o->precision != LSG_PRECISION_FP64 && o->precision != LSG_PRECISION_MIXED) return LSG_ERR_ARG;
+  if (o->maximum_order < 1 || o->maximum_order > 5) return LSG_ERR_ARG;
+  return LSG_OK;
+}
+
+void free_buffers(lsg_ctx* c) {
+  cudaFree(c->dY); cudaFree(c->dT); cudaFree(c->ddt); cudaFree(c->dQ); cudaFree(c->dstatus); cudaFree(c->dnsteps);
+  c->dY = c->dT = c->ddt = c->dQ = nullptr;
+  c->dstatus = c->dnsteps = nullptr;
+  c->cap = 0;
+}
+
+int ensure_capacity(lsg_ctx* c, long n) {
+  if (n <= c->cap) return LSG_OK;
+  free_buffers(c);
+  const int nc = c->mech->host.layout.nc;
+  long cap = n;
+  if (cudaMalloc(&c->dY, sizeof(double) * (size_t)nc * cap) != cudaSuccess ||
+      cudaMalloc(&c->dT, sizeof(double) * cap) != cudaSuccess ||
+      cudaMalloc(&c->ddt, sizeof(double) * cap) != cudaSuccess ||
+      cudaMalloc(&c->dQ, sizeof(double) * cap) != cudaSuccess ||
+      cudaMalloc(&c->dstatus, sizeof(int) * cap) != cudaSuccess ||
+      cudaMalloc(&c->dnsteps, sizeof(int) * cap) != cudaSuccess) {
+    free_buffers(c);
+    cudaGetLastError();
+    return LSG_ERR_NOMEM;
+  }
+  c->cap = cap;
+  return LSG_OK;
+}
+
+int launch_step(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
+  const MechLayout& L = c->mech->host.layout;
+  if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
+  if (c->opt.precision != LSG_PRECISION_FP64) return LSG_ERR_UNSUPPORTED;
+  const StepOptions so = to_step_options(c->opt);
+  if (plain_smem_bytes(L) > 227 * 1024) return LSG_ERR_UNSUPPORTED;
+  if (launch_plain(L, c->mech->d_buf, so, a, c->d_err, s) != cudaSuccess) return LSG_ERR_CUDA;
+  return LSG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void lsg_options_default(lsg_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->rtol = 1.e-7;
+  o->atol = 1.e-12;
+  o->tmin_chem = 0.;
+  o->y_min_T = 200.;
+  o->y_max_T = 6000.;
+  o->max_steps = 500000;
+  o->full_pivoting = 0;
+  o->energy = 1;
+  o->precision = LSG_PRECISION_FP64;
+  o->alfa2_4 = 0.8;
+  o->alfa2_5 = 0.8;
+  o->maximum_order = 5;
+}
+
+int lsg_abi_version(void) { return LSG_ABI_VERSION; }
+
+const char* lsg_strerror(int code) {
+  switch (code) {
+    case LSG_OK: return "success";
+    case LSG_ERR_ARG: return "invalid argument";
+    case LSG_ERR_MECH: return "mechanism blob could not be read";
+    case LSG_ERR_CUDA: return "CUDA runtime error";
+    case LSG_ERR_NOMEM: return "device allocation failed";
+    case LSG_ERR_UNSUPPORTED: return "option or mechanism size not supported";
+    case LSG_ERR_DEVICE: return "a kernel reported an internal error";
+    case LSG_ERR_IO: return "file could not be read";
+    default: return "unknown error";
+  }
+}
+
+int lsg_mech_load_blob(const void* blob, size_t nbytes, int device, lsg_mech** out) {
+  if (!blob || !out) return LSG_ERR_ARG;
+  *out = nullptr;
+  lsg_mech* m = new (std::nothrow) lsg_mech();
+  if (!m) return LSG_ERR_NOMEM;
+  std::string err;
+  if (!build_mechanism(blob, nbytes, m->host, err)) { delete m; return LSG_ERR_MECH; }
+  m->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) { delete m; cudaGetLastError(); return LSG_ERR_CUDA; }
+  if (cudaMalloc(&m->d_buf, m->host.buffer.size()) != cudaSuccess) { delete m; cudaGetLastError(); return LSG_ERR_NOMEM; }
+  if (cudaMemcpy(m->d_buf, m->host.buffer.data(), m->host.buffer.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(m->d_buf);
+    delete m;
+    return LSG_ERR_CUDA;
+  }
+  *out = m;
+  return LSG_OK;
+}
+
+int lsg_mech_load_file(const char* path, int device, lsg_mech** out) {
+  if (!path || !out) return LSG_ERR_ARG;
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return LSG_ERR_IO;
+  std::vector<char> data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+  return lsg_mech_load_blob(data.data(), data.size(), device, out);
+}
+
+int lsg_mech_info(const lsg_mech* m, int* nspecies, int* nreactions) {
+  if (!m) return LSG_ERR_ARG;
+  if (nspecies) *nspecies = m->host.layout.nc;
+  if (nreactions) *nreactions = m->host.layout.nr;
+  return LSG_OK;
+}
+
+int lsg_mech_destroy(lsg_mech* m) {
+  if (!m) return LSG_OK;
+  cudaSetDevice(m->device);
+  cudaFree(m->d_buf);
+  delete m;
+  return LSG_OK;
+}
+
+int lsg_ctx_create(const lsg_mech* mech, const lsg_options* opt, int device, lsg_ctx** out) {
+  if (!mech || !out) return LSG_ERR_ARG;
+  *out = nullptr;
+  lsg_options o;
+  lsg_options_default(&o);
+  if (opt) o = *opt;
+  const int v = validate_options(&o);
+  if (v != LSG_OK) return v;
+  if (device != mech->device) return LSG_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_CUDA; }
+  const int g = ensure_gear(device);
+  if (g != LSG_OK) return g;
+  lsg_ctx* c = new (std::nothrow) lsg_ctx();
+  if (!c) return LSG_ERR_NOMEM;
+  c->mech = mech;
+  c->opt = o;
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess || cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess) {
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    cudaGetLastError();
+    return LSG_ERR_CUDA;
+  }
+  *out = c;
+  return LSG_OK;
+}
+
+int lsg_ctx_set_options(lsg_ctx* c, const lsg_options* opt) {
+  if (!c) return LSG_ERR_ARG;
+  const int v = validate_options(opt);
+  if (v != LSG_OK) return v;
+  c->opt = *opt;
+  return LSG_OK;
+}
+
+int lsg_ctx_destroy(lsg_ctx* c) {
+  if (!c) return LSG_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  free_buffers(c);
+  cudaFree(c->d_err);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return LSG_OK;
+}
+
+void* lsg_ctx_stream(lsg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int lsg_ctx_check(lsg_ctx* c, int* flags) {
+  if (!c) return LSG_ERR_ARG;
+  int h = 0;
+  // device-wide: kernels may have been enqueued on caller streams
+  if (cudaDeviceSynchronize() != cudaSuccess) return LSG_ERR_CUDA;
+  if (cudaMemcpy(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return LSG_ERR_CUDA;
+  if (cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess) return LSG_ERR_CUDA;
+  if (flags) *flags = h;
+  return h ? LSG_ERR_DEVICE : LSG_OK;
+}
+
+int lsg_reaction_step_device(lsg_ctx* c, int ncells, int nspecies, double* Y, long ld, double* T, double p,
+                             double t0, const double* dt, double dt_scalar, double* Q, int* status, int* nsteps,
+                             long long* counters, void* stream) {
+  if (!c || ncells < 0 || !Y || !T || ld < ncells) return LSG_ERR_ARG;
+  if (nspecies != c->mech->host.layout.nc) return LSG_ERR_ARG;
+  if (!(p > 0.)) return LSG_ERR_ARG;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  StepArgs a{};
+  a.ncells = ncells;
+  a.ld = ld;
+  a.Y = Y;
+  a.T = T;
+  a.dt = dt;
+  a.dt_scalar = dt_scalar;
+  a.t0 = t0;
+  a.p = p;
+  a.Q = Q;
+  a.status = status;
+  a.nsteps = nsteps;
+  a.counters = counters;
+  return launch_step(c, a, (cudaStream_t)stream);
+}
+
+int lsg_reaction_step(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, double* T, double p, double t0,
+                      const double* dt, double dt_scalar, double* Q, int* status, int* nsteps) {
+  if (!c || ncells < 0 || !Ys || !T) return LSG_ERR_ARG;
+  if (nspecies != c->mech->host.layout.nc) return LSG_ERR_ARG;
+  for (int i = 0; i < nspecies; ++i) if (!Ys[i]) return LSG_ERR_ARG;
+  if (!(p > 0.)) return LSG_ERR_ARG;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  int r = ensure_capacity(c, ncells);
+  if (r != LSG_OK) return r;
+  cudaStream_t s = c->stream;
+  const size_t nb = sizeof(double) * (size_t)ncells;
+  for (int i = 0; i < nspecies; ++i)
+    if (cudaMemcpyAsync(c->dY + (size_t)i * c->cap, Ys[i], nb, cudaMemcpyHostToDevice, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (cudaMemcpyAsync(c->dT, T, nb, cudaMemcpyHostToDevice, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (dt && cudaMemcpyAsync(c->ddt, dt, nb, cudaMemcpyHostToDevice, s) != cudaSuccess) return LSG_ERR_CUDA;
+  StepArgs a{};
+  a.ncells = ncells;
+  a.ld = c->cap;
+  a.Y = c->dY;
+  a.T = c->dT;
+  a.dt = dt ? c->ddt : nullptr;
+  a.dt_scalar = dt_scalar;
+  a.t0 = t0;
+  a.p = p;
+  a.Q = Q ? c->dQ : nullptr;
+  a.status = status ? c->dstatus : nullptr;
+  a.nsteps = nsteps ? c->dnsteps : nullptr;
+  r = launch_step(c, a, s);
+  if (r != LSG_OK) return r;
+  for (int i = 0; i < nspecies; ++i)
+    if (cudaMemcpyAsync(Ys[i], c->dY + (size_t)i * c->cap, nb, cudaMemcpyDeviceToHost, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (cudaMemcpyAsync(T, c->dT, nb, cudaMemcpyDeviceToHost, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (Q && cudaMemcpyAsync(Q, c->dQ, nb, cudaMemcpyDeviceToHost, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (status && cudaMemcpyAsync(status, c->dstatus, sizeof(int) * ncells, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return LSG_ERR_CUDA;
+  if (nsteps && cudaMemcpyAsync(nsteps, c->dnsteps, sizeof(int) * ncells, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return LSG_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return LSG_ERR_CUDA;
+  int flags = 0;
+  return lsg_ctx_check(c, &flags);
+}
+
+int lsg_rhs_device(lsg_ctx* c, int ncells, const double* y, double* dy, long ld, double p, double* qr, void* stream) {
+  if (!c || ncells < 0 || !y || !dy || ld < ncells || !(p > 0.)) return LSG_ERR_ARG;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  const MechLayout& L = c->mech->host.layout;
+  if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
+  if (launch_rhs_warp(L, c->mech->d_buf, ncells, y, dy, ld, p, c->opt.energy, qr, c->d_err,
+                      (cudaStream_t)stream) != cudaSuccess)
+    return LSG_ERR_CUDA;
+  return LSG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,76 @@
+// Common device helpers: constants, warp reductions in a fixed order, the
+// bulk (TMA engine) staging of the mechanism table into shared memory.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lsg_mech.h"
+
+namespace lsg {
+
+// math/OpenSMOKEFunctions.hpp:60-87 and math/OpenSMOKEStdInclude.h:53-55
+constexpr double kMachEpsDouble = 2.220446049250313e-16;
+constexpr double kMachEpsFloat = 1.1920928955078125e-07;   // (double)1.192092896e-07F
+constexpr double kTinyFloat = 1.1754943508222875e-38;      // (double)1.175494351e-38F
+constexpr double kRgas = 8314.4621;                        // J/kmol/K, math/PhysicalConstants.h:24
+constexpr unsigned kFull = 0xffffffffu;
+
+// Error flags written to the per-call device error word.
+enum : int {
+  kErrNone = 0,
+  kErrStageTimeout = 1,     // bulk copy of the mechanism did not complete in time
+  kErrBadSize = 2,
+  kErrQueueTimeout = 4,
+};
+
+// Sum of v over lanes 0..n-1, added strictly in lane order (the reference's
+// sequential loops).  Every lane receives the result.
+__device__ __forceinline__ double seq_sum(double v, int n) {
+  double s = 0.;
+  for (int i = 0; i < n; ++i) s += __shfl_sync(kFull, v, i);
+  return s;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Stage `bytes` (multiple of 16, both addresses 16-byte aligned) from global
+// to shared memory with one-dimensional bulk copies issued by thread 0 and
+// completed on an mbarrier.  Waits are bounded; on timeout the block's
+// error flag is raised and false is returned (the caller must then not use
+// the shared copy).  Must be called by all threads of the block.
+__device__ inline bool stage_bulk(void* smem_dst, const void* gsrc, uint32_t bytes, uint64_t* mbar, int* err) {
+  const uint32_t bar = smem_u32(mbar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    const uint32_t dst = smem_u32(smem_dst);
+    const uint32_t chunk = 32768;   // several copies, each a multiple of 16 bytes
+    for (uint32_t off = 0; off < bytes; off += chunk) {
+      const uint32_t n = (bytes - off) < chunk ? (bytes - off) : chunk;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst + off),
+          "l"((const char*)gsrc + off), "r"(n), "r"(bar)
+          : "memory");
+    }
+  }
+  uint32_t done = 0;
+  for (long it = 0; it < (1L << 22); ++it) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar)
+        : "memory");
+    if (done) break;
+  }
+  const int ok = __syncthreads_and(done ? 1 : 0);
+  if (!ok && threadIdx.x == 0) atomicOr(err, kErrStageTimeout);
+  return ok != 0;
+}
+
+}  // namespace lsg

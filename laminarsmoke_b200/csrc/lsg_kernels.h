@@ -1,0 +1,52 @@
+// Kernel launch interface between the host runtime (lsg_api.cu) and the
+// kernel translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "lsg_mech.h"
+
+namespace lsg {
+
+struct StepOptions {
+  double rtol, atol, tmin_chem, y_min_T, y_max_T;
+  int max_steps, energy;
+  double alfa2_4, alfa2_5;
+  int maximum_order;
+};
+
+enum { CNT_STEPS, CNT_RHS, CNT_JAC, CNT_FACT, CNT_SOLVE, CNT_ERRFAIL, CNT_CONVFAIL, CNT_JAC_RHS, NCNT };
+
+// Gear method constants (MethodGear::MemoryAllocationMethod, MethodGear.hpp:125-193),
+// computed once on the host and uploaded to each kernel unit's constant bank.
+struct GearConsts {
+  double r[6][5];
+  double Ep[6];
+};
+
+constexpr int kPlainWarpsPerBlock = 4;
+
+// Arguments of one reaction-step launch (device pointers).
+struct StepArgs {
+  long ncells;
+  long ld;            // leading dimension of the species-major Y: Y[species * ld + cell]
+  double* Y;
+  double* T;
+  const double* dt;   // per-cell dt or nullptr
+  double dt_scalar;
+  double t0;
+  double p;
+  double* Q;          // optional
+  int* status;        // optional
+  int* nsteps;        // optional
+  long long* counters;  // optional [ncells][NCNT]
+};
+
+size_t plain_smem_bytes(const MechLayout& L);
+cudaError_t upload_gear_plain(const GearConsts& gc);
+cudaError_t launch_plain(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                         const StepArgs& a, int* err, cudaStream_t stream);
+cudaError_t launch_rhs_warp(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y,
+                            double* dy, long ld, double p, int energy, double* qr, int* err, cudaStream_t stream);
+
+}  // namespace lsg

@@ -1,0 +1,46 @@
+// Device-side mechanism layout shared by the host runtime and the kernels.
+//
+// The packed blob (named arrays) is flattened on the host into ONE buffer:
+// a double region followed by an int region.  Every array starts on a
+// 16-byte boundary so the whole table (or any array of it) can be moved by a
+// bulk copy.  Offsets are in elements of the region they live in.
+#pragma once
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define LSG_HD __host__ __device__
+#else
+#define LSG_HD
+#endif
+
+namespace lsg {
+
+struct MechLayout {
+  int nc, nr;                 // species, reactions
+  int n_tb, n_fo, n_rev_th, n_rev_ex;
+  int nnz_reac, nnz_prod, nnz_fr, nnz_tb, nnz_fo;
+  int n_double, n_int;        // region sizes (elements, padded)
+  uint32_t bytes;             // total bytes of the flattened buffer
+  // ---- double region offsets
+  int mw, cp_ht, cp_lt, dh_ht, dh_lt, ds_ht, ds_lt, t_mid;   // species
+  int lnA, beta, eor, dnu;                                   // reactions
+  int rev_lnA, rev_beta, rev_eor;                            // explicit reverse (by slot)
+  int fo_lnA, fo_beta, fo_eor, fo_a, fo_b, fo_c, fo_d, fo_e; // fall-off (by slot)
+  int reac_nu, prod_nu, fr_coef, tb_eff, fo_eff;             // CSR values
+  // ---- int region offsets
+  int a_sign, rev_kind, rev_slot, tb_slot, fo_slot;          // per reaction
+  int reac_ptr, reac_sp, prod_ptr, prod_sp;                  // per reaction CSR
+  int fr_ptr, fr_rxn;                                        // per species CSR
+  int tb_ptr, tb_sp;                                         // third body CSR (by slot)
+  int fo_type, fo_single, fo_ptr, fo_sp;                     // fall-off (by slot)
+};
+
+// Views into a flattened table (global or shared memory).
+struct MechView {
+  const double* d;
+  const int* i;
+  LSG_HD const double* D(int off) const { return d + off; }
+  LSG_HD const int* I(int off) const { return i + off; }
+};
+
+}  // namespace lsg

@@ -1,0 +1,201 @@
+// Host side: packed blob (named arrays) -> flattened device table (lsg_mech.h).
+#include "lsg_mech_host.h"
+
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace lsg {
+
+namespace {
+struct Blob {
+  std::map<std::string, std::vector<double>> f;
+  std::map<std::string, std::vector<int>> i;
+  const std::vector<double>& F(const char* k) const {
+    auto it = f.find(k);
+    if (it == f.end()) throw std::runtime_error(std::string("mechanism blob: missing array ") + k);
+    return it->second;
+  }
+  const std::vector<int>& I(const char* k) const {
+    auto it = i.find(k);
+    if (it == i.end()) throw std::runtime_error(std::string("mechanism blob: missing array ") + k);
+    return it->second;
+  }
+};
+
+bool parse(const unsigned char* p, size_t n, Blob& b, std::string& err) {
+  if (n < 16 || std::memcmp(p, "LSMECH01", 8) != 0) { err = "bad magic"; return false; }
+  uint32_t na;
+  std::memcpy(&na, p + 8, 4);
+  size_t pos = 16;
+  for (uint32_t a = 0; a < na; ++a) {
+    if (pos + 48 > n) { err = "truncated header"; return false; }
+    char name[33];
+    std::memcpy(name, p + pos, 32);
+    name[32] = 0;
+    uint32_t code;
+    uint64_t count;
+    std::memcpy(&code, p + pos + 32, 4);
+    std::memcpy(&count, p + pos + 40, 8);
+    pos += 48;
+    if (code > 1) { err = "bad dtype"; return false; }
+    const size_t nb = (code == 0 ? 8 : 4) * count;
+    if (pos + nb > n) { err = "truncated payload"; return false; }
+    if (code == 0) {
+      std::vector<double> v(count);
+      if (nb) std::memcpy(v.data(), p + pos, nb);
+      b.f[name] = std::move(v);
+    } else {
+      std::vector<int> v(count);
+      if (nb) std::memcpy(v.data(), p + pos, nb);
+      b.i[name] = std::move(v);
+    }
+    pos += nb + ((8 - nb % 8) % 8);
+  }
+  return true;
+}
+
+struct Builder {
+  std::vector<double> d;
+  std::vector<int> iv;
+  int addd(const std::vector<double>& v) {
+    while (d.size() % 2) d.push_back(0.);  // 16-byte alignment
+    const int off = (int)d.size();
+    d.insert(d.end(), v.begin(), v.end());
+    return off;
+  }
+  int addi(const std::vector<int>& v) {
+    while (iv.size() % 4) iv.push_back(0);
+    const int off = (int)iv.size();
+    iv.insert(iv.end(), v.begin(), v.end());
+    return off;
+  }
+};
+}  // namespace
+
+bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string& err) {
+  Blob b;
+  if (!parse((const unsigned char*)blob, nbytes, b, err)) return false;
+  try {
+    const auto& dims = b.I("dims");
+    const int nc = dims.at(0), nr = dims.at(1);
+    if (nc <= 0 || nr < 0) { err = "bad dimensions"; return false; }
+    MechLayout L{};
+    L.nc = nc;
+    L.nr = nr;
+    Builder B;
+    L.mw = B.addd(b.F("mw"));
+    L.cp_ht = B.addd(b.F("cp_ht"));
+    L.cp_lt = B.addd(b.F("cp_lt"));
+    L.dh_ht = B.addd(b.F("dh_ht"));
+    L.dh_lt = B.addd(b.F("dh_lt"));
+    L.ds_ht = B.addd(b.F("ds_ht"));
+    L.ds_lt = B.addd(b.F("ds_lt"));
+    L.t_mid = B.addd(b.F("t_mid"));
+    L.lnA = B.addd(b.F("lnA"));
+    L.beta = B.addd(b.F("beta"));
+    L.eor = B.addd(b.F("e_over_r"));
+    L.dnu = B.addd(b.F("delta_nu"));
+    L.rev_lnA = B.addd(b.F("lnA_rev"));
+    L.rev_beta = B.addd(b.F("beta_rev"));
+    L.rev_eor = B.addd(b.F("e_over_r_rev"));
+    L.fo_lnA = B.addd(b.F("fo_lnA"));
+    L.fo_beta = B.addd(b.F("fo_beta"));
+    L.fo_eor = B.addd(b.F("fo_e_over_r"));
+    L.fo_a = B.addd(b.F("fo_a"));
+    L.fo_b = B.addd(b.F("fo_b"));
+    L.fo_c = B.addd(b.F("fo_c"));
+    L.fo_d = B.addd(b.F("fo_d"));
+    L.fo_e = B.addd(b.F("fo_e"));
+    L.reac_nu = B.addd(b.F("reac_nu"));
+    L.prod_nu = B.addd(b.F("prod_nu"));
+    L.fr_coef = B.addd(b.F("fr_coef"));
+    L.tb_eff = B.addd(b.F("tb_eff_m1"));
+    L.fo_eff = B.addd(b.F("fo_eff_m1"));
+
+    const auto& isrev = b.I("is_reversible");
+    const auto& rth = b.I("rev_thermo");
+    const auto& rex = b.I("rev_explicit");
+    std::vector<int> rev_kind(nr, 0), rev_slot(nr, -1), tb_slot(nr, -1), fo_slot(nr, -1);
+    for (size_t k = 0; k < rth.size(); ++k) { rev_kind.at(rth[k]) = 1; rev_slot.at(rth[k]) = (int)k; }
+    for (size_t k = 0; k < rex.size(); ++k) { rev_kind.at(rex[k]) = 2; rev_slot.at(rex[k]) = (int)k; }
+    for (int j = 0; j < nr; ++j)
+      if (isrev.at(j) && rev_kind[j] == 0) { err = "reversible reaction without reverse data"; return false; }
+    const auto& tbr = b.I("tb_rxn");
+    const auto& fr = b.I("fo_rxn");
+    for (size_t k = 0; k < tbr.size(); ++k) tb_slot.at(tbr[k]) = (int)k;
+    for (size_t k = 0; k < fr.size(); ++k) fo_slot.at(fr[k]) = (int)k;
+
+    L.a_sign = B.addi(b.I("a_sign"));
+    L.rev_kind = B.addi(rev_kind);
+    L.rev_slot = B.addi(rev_slot);
+    L.tb_slot = B.addi(tb_slot);
+    L.fo_slot = B.addi(fo_slot);
+    L.reac_ptr = B.addi(b.I("reac_ptr"));
+    L.reac_sp = B.addi(b.I("reac_species"));
+    L.prod_ptr = B.addi(b.I("prod_ptr"));
+    L.prod_sp = B.addi(b.I("prod_species"));
+    L.fr_ptr = B.addi(b.I("fr_ptr"));
+    L.fr_rxn = B.addi(b.I("fr_rxn"));
+    L.tb_ptr = B.addi(b.I("tb_ptr"));
+    L.tb_sp = B.addi(b.I("tb_species"));
+    L.fo_type = B.addi(b.I("fo_type"));
+    L.fo_single = B.addi(b.I("fo_single"));
+    L.fo_ptr = B.addi(b.I("fo_ptr"));
+    L.fo_sp = B.addi(b.I("fo_species"));
+
+    L.n_tb = (int)tbr.size();
+    L.n_fo = (int)fr.size();
+    L.n_rev_th = (int)rth.size();
+    L.n_rev_ex = (int)rex.size();
+    L.nnz_reac = (int)b.I("reac_species").size();
+    L.nnz_prod = (int)b.I("prod_species").size();
+    L.nnz_fr = (int)b.I("fr_rxn").size();
+    L.nnz_tb = (int)b.I("tb_species").size();
+    L.nnz_fo = (int)b.I("fo_species").size();
+
+    // consistency checks (index ranges) so a corrupt blob fails here, not on the device
+    auto in_range = [&](const std::vector<int>& v, int lo, int hi) {
+      for (int x : v) if (x < lo || x >= hi) return false;
+      return true;
+    };
+    if (!in_range(b.I("reac_species"), 0, nc) || !in_range(b.I("prod_species"), 0, nc) ||
+        !in_range(b.I("fr_rxn"), 0, nr) || !in_range(b.I("tb_species"), 0, nc) ||
+        !in_range(b.I("fo_species"), 0, nc) || !in_range(tbr, 0, nr) || !in_range(fr, 0, nr)) {
+      err = "index out of range in mechanism blob";
+      return false;
+    }
+    if ((int)b.I("reac_ptr").size() != nr + 1 || (int)b.I("prod_ptr").size() != nr + 1 ||
+        (int)b.I("fr_ptr").size() != nc + 1 || (int)b.F("mw").size() != nc ||
+        (int)b.F("cp_ht").size() != 5 * nc || (int)b.F("dh_ht").size() != 6 * nc ||
+        (int)b.F("lnA").size() != nr) {
+      err = "inconsistent array sizes in mechanism blob";
+      return false;
+    }
+    while (B.d.size() % 2) B.d.push_back(0.);
+    while (B.iv.size() % 4) B.iv.push_back(0);
+    L.n_double = (int)B.d.size();
+    L.n_int = (int)B.iv.size();
+    L.bytes = (uint32_t)(B.d.size() * sizeof(double) + B.iv.size() * sizeof(int));
+    out.layout = L;
+    out.buffer.resize(L.bytes);
+    std::memcpy(out.buffer.data(), B.d.data(), B.d.size() * sizeof(double));
+    std::memcpy(out.buffer.data() + B.d.size() * sizeof(double), B.iv.data(), B.iv.size() * sizeof(int));
+    out.species.clear();
+    const auto& nm = b.I("species_names");
+    std::string cur;
+    for (int ch : nm) {
+      if (ch == 0) { out.species.push_back(cur); cur.clear(); }
+      else cur.push_back((char)ch);
+    }
+    out.mw = b.F("mw");
+  } catch (const std::exception& e) {
+    err = e.what();
+    return false;
+  }
+  return true;
+}
+
+}  // namespace lsg

@@ -1,0 +1,211 @@
+"""Python binding of the C ABI (include/lsmoke_gpu.h) over ctypes.
+
+This is the harness the tests and the benchmark drive the library through; it
+adds no computation of its own.  The shared library must have been built
+(``python -m laminarsmoke_b200.csrc.build`` or ``__graft_entry__.build()``);
+importing this module without it raises, there is no fallback path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblsmoke_gpu.so")
+
+LSG_PRECISION_FP64 = 0
+LSG_PRECISION_MIXED = 1
+NCOUNTERS = 8
+COUNTER_NAMES = ("steps", "rhs", "jacobians", "factorizations", "solves",
+                 "error_failures", "convergence_failures", "jacobian_rhs")
+
+
+class LsgError(RuntimeError):
+    pass
+
+
+class Options(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("tmin_chem", C.c_double),
+                ("y_min_T", C.c_double), ("y_max_T", C.c_double),
+                ("max_steps", C.c_int), ("full_pivoting", C.c_int), ("energy", C.c_int),
+                ("precision", C.c_int),
+                ("alfa2_4", C.c_double), ("alfa2_5", C.c_double), ("maximum_order", C.c_int),
+                ("reserved", C.c_int * 7)]
+
+
+EXPORTS = (
+    "lsg_options_default", "lsg_mech_load_blob", "lsg_mech_load_file", "lsg_mech_info",
+    "lsg_mech_destroy", "lsg_ctx_create", "lsg_ctx_set_options", "lsg_ctx_destroy",
+    "lsg_reaction_step", "lsg_reaction_step_device", "lsg_ctx_check", "lsg_rhs_device",
+    "lsg_strerror", "lsg_abi_version", "lsg_ctx_stream",
+)
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise LsgError(f"{LIB_PATH} is not built; run __graft_entry__.build()")
+    L = C.CDLL(LIB_PATH)
+    vp, i, d, l = C.c_void_p, C.c_int, C.c_double, C.c_long
+    L.lsg_options_default.argtypes = [C.POINTER(Options)]
+    L.lsg_options_default.restype = None
+    L.lsg_mech_load_blob.argtypes = [vp, C.c_size_t, i, C.POINTER(vp)]
+    L.lsg_mech_load_file.argtypes = [C.c_char_p, i, C.POINTER(vp)]
+    L.lsg_mech_info.argtypes = [vp, C.POINTER(i), C.POINTER(i)]
+    L.lsg_mech_destroy.argtypes = [vp]
+    L.lsg_ctx_create.argtypes = [vp, C.POINTER(Options), i, C.POINTER(vp)]
+    L.lsg_ctx_set_options.argtypes = [vp, C.POINTER(Options)]
+    L.lsg_ctx_destroy.argtypes = [vp]
+    L.lsg_reaction_step.argtypes = [vp, i, i, C.POINTER(vp), vp, d, d, vp, d, vp, vp, vp]
+    L.lsg_reaction_step_device.argtypes = [vp, i, i, vp, l, vp, d, d, vp, d, vp, vp, vp, vp, vp]
+    L.lsg_ctx_check.argtypes = [vp, C.POINTER(i)]
+    L.lsg_rhs_device.argtypes = [vp, i, vp, vp, l, d, vp, vp]
+    L.lsg_strerror.argtypes = [i]
+    L.lsg_strerror.restype = C.c_char_p
+    L.lsg_abi_version.restype = i
+    L.lsg_ctx_stream.argtypes = [vp]
+    L.lsg_ctx_stream.restype = vp
+    _lib = L
+    return L
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise LsgError(f"{what}: {lib().lsg_strerror(rc).decode()} ({rc})")
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    lib().lsg_options_default(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+class Mechanism:
+    """Device-resident mechanism tables (lsg_mech)."""
+
+    def __init__(self, blob: bytes, device: int = 0):
+        self.device = device
+        self.h = C.c_void_p()
+        buf = (C.c_ubyte * len(blob)).from_buffer_copy(blob)
+        _check(lib().lsg_mech_load_blob(C.cast(buf, C.c_void_p), len(blob), device, C.byref(self.h)),
+               "lsg_mech_load_blob")
+        ns, nr = C.c_int(), C.c_int()
+        _check(lib().lsg_mech_info(self.h, C.byref(ns), C.byref(nr)), "lsg_mech_info")
+        self.n_species, self.n_reactions = ns.value, nr.value
+
+    def close(self):
+        if self.h:
+            lib().lsg_mech_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _require_layout(*tensors):
+    for t in tensors:
+        if t is None:
+            continue
+        if not t.is_cuda or not t.is_contiguous():
+            raise TypeError("device arrays must be contiguous CUDA tensors (species-major [rows, ld])")
+
+
+def _stream_handle(stream):
+    """The caller's stream for device calls: torch's current stream unless one is given."""
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream
+
+
+class ReactionStep:
+    """A context (lsg_ctx): options + stream + staging buffers."""
+
+    def __init__(self, mech: Mechanism, options: Optional[Options] = None, **kw):
+        self.mech = mech
+        self.options = options if options is not None else default_options(**kw)
+        self.h = C.c_void_p()
+        _check(lib().lsg_ctx_create(mech.h, C.byref(self.options), mech.device, C.byref(self.h)),
+               "lsg_ctx_create")
+
+    def set_options(self, **kw):
+        for k, v in kw.items():
+            setattr(self.options, k, v)
+        _check(lib().lsg_ctx_set_options(self.h, C.byref(self.options)), "lsg_ctx_set_options")
+
+    def close(self):
+        if self.h:
+            lib().lsg_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- host arrays (the OpenFOAM-facing call) ----
+    def step(self, Y_species: np.ndarray, T: np.ndarray, dt, p: float = 101325.0, t0: float = 0.0,
+             want_q: bool = True):
+        """Y_species: [NC, ncells] float64 (updated in place), T: [ncells] (in place)."""
+        Y = Y_species
+        if Y.dtype != np.float64 or not Y.flags.c_contiguous or T.dtype != np.float64:
+            raise TypeError("Y_species and T must be C-contiguous float64")
+        nc, n = Y.shape
+        ptrs = (C.c_void_p * nc)(*[Y[i].ctypes.data for i in range(nc)])
+        dt_arr = None
+        dt_s = 0.0
+        if np.ndim(dt) == 0:
+            dt_s = float(dt)
+        else:
+            dt_arr = np.ascontiguousarray(dt, dtype=np.float64)
+        Q = np.zeros(n) if want_q else None
+        st = np.zeros(n, dtype=np.int32)
+        ns = np.zeros(n, dtype=np.int32)
+        _check(lib().lsg_reaction_step(self.h, n, nc, ptrs, T.ctypes.data, p, t0,
+                                       None if dt_arr is None else dt_arr.ctypes.data, dt_s,
+                                       None if Q is None else Q.ctypes.data, st.ctypes.data, ns.ctypes.data),
+               "lsg_reaction_step")
+        return Q, st, ns
+
+    # ---- device arrays (torch tensors) ----
+    def step_device(self, Y, T, dt=1e-5, p: float = 101325.0, t0: float = 0.0, Q=None, status=None,
+                    nsteps=None, counters=None, stream=None):
+        """Y: cuda float64 [NC, ld] species-major, T: [ncells]; in place."""
+        _require_layout(Y, T, Q, status, nsteps, counters, dt if hasattr(dt, "data_ptr") else None)
+        nc, ld = Y.shape
+        n = T.shape[0]
+        dtp, dts = (None, float(dt)) if not hasattr(dt, "data_ptr") else (dt.data_ptr(), 0.0)
+        _check(lib().lsg_reaction_step_device(
+            self.h, n, nc, Y.data_ptr(), ld, T.data_ptr(), p, t0, dtp, dts,
+            None if Q is None else Q.data_ptr(), None if status is None else status.data_ptr(),
+            None if nsteps is None else nsteps.data_ptr(), None if counters is None else counters.data_ptr(),
+            _stream_handle(stream)), "lsg_reaction_step_device")
+
+    def rhs_device(self, y, dy, p: float = 101325.0, qr=None, stream=None):
+        _require_layout(y, dy, qr)
+        n1, ld = y.shape
+        n = ld if qr is None else qr.shape[0]
+        _check(lib().lsg_rhs_device(self.h, n, y.data_ptr(), dy.data_ptr(), ld, p,
+                                    None if qr is None else qr.data_ptr(),
+                                    _stream_handle(stream)), "lsg_rhs_device")
+
+    def check(self):
+        f = C.c_int()
+        rc = lib().lsg_ctx_check(self.h, C.byref(f))
+        if rc != 0:
+            raise LsgError(f"device error flags 0x{f.value:x}: {lib().lsg_strerror(rc).decode()}")

@@ -1,0 +1,1000 @@
+// CPU oracle for the laminarSMOKE reaction step -- TEST INFRASTRUCTURE ONLY.
+//
+// This file restates, in plain FP64 C++, the reference's constant-pressure
+// batch-reactor chemistry step.  It is used by the tests (as the parity
+// checker), by __graft_entry__.smoke() and by bench.py's CPU baseline leg,
+// and by nothing else: the product path (the CUDA library) never calls it.
+//
+// Parity status: UNPINNED.  The reference ships no tests, fixtures or golden
+// vectors for this path, and its code cannot be compiled here (it needs
+// Eigen 3.3.7, Boost 1.69, RapidXML and OpenFOAM, none of which is present).
+// The restatement follows the reference line by line instead; each function
+// below names the file:line it follows (paths relative to
+// solvers/openSMOKEpp4laminarSMOKE unless they start with solvers/).
+//
+// Build: oracle/Makefile (g++ -O2 -ffp-contract=off -fopenmp).
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cfloat>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include <map>
+#include <stdexcept>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+
+// math/OpenSMOKEFunctions.hpp:60-87, math/OpenSMOKEStdInclude.h:53-55
+static const double MACH_EPS_DOUBLE = 2.220446049250313e-16;      // MachEps()
+static const double MACH_EPS_FLOAT = (double)1.192092896e-07F;      // MachEpsFloat()
+static const double TINY_FLOAT = (double)1.175494351e-38F;         // OPENSMOKE_TINY_FLOAT
+static const double R_J_KMOL = 8314.4621;                            // math/PhysicalConstants.h:24
+
+// ---------------------------------------------------------------------------
+// Packed mechanism (the blob written by laminarsmoke_b200/mech/blob.py)
+// ---------------------------------------------------------------------------
+struct Mech {
+  int nc = 0, nr = 0;
+  std::map<std::string, std::vector<double>> f;
+  std::map<std::string, std::vector<int>> i;
+  const std::vector<double>& F(const char* k) const {
+    auto it = f.find(k);
+    if (it == f.end()) throw std::runtime_error(std::string("missing array ") + k);
+    return it->second;
+  }
+  const std::vector<int>& I(const char* k) const {
+    auto it = i.find(k);
+    if (it == i.end()) throw std::runtime_error(std::string("missing array ") + k);
+    return it->second;
+  }
+};
+
+static Mech* load_blob(const unsigned char* p, size_t n) {
+  if (n < 16 || std::memcmp(p, "LSMECH01", 8) != 0) return nullptr;
+  uint32_t na; std::memcpy(&na, p + 8, 4);
+  size_t pos = 16;
+  Mech* m = new Mech();
+  for (uint32_t a = 0; a < na; ++a) {
+    if (pos + 48 > n) { delete m; return nullptr; }
+    char name[33]; std::memcpy(name, p + pos, 32); name[32] = 0;
+    uint32_t code; uint64_t count;
+    std::memcpy(&code, p + pos + 32, 4); std::memcpy(&count, p + pos + 40, 8);
+    pos += 48;
+    size_t item = code == 0 ? 8 : 4, nb = item * count;
+    if (pos + nb > n) { delete m; return nullptr; }
+    if (code == 0) { std::vector<double> v(count); std::memcpy(v.data(), p + pos, nb); m->f[name] = v; }
+    else { std::vector<int> v(count); std::memcpy(v.data(), p + pos, nb); m->i[name] = v; }
+    pos += nb + ((8 - nb % 8) % 8);
+  }
+  m->nc = m->I("dims")[0];
+  m->nr = m->I("dims")[1];
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// Reactor right-hand side with the reference's per-temperature caching.
+//   solvers/laminarSMOKE/unsteady/BatchReactorHomogeneousConstantPressure.H:175-223
+//   maps/ThermodynamicsMap_CHEMKIN.hpp:158-164, 429-520
+//   maps/KineticsMap_CHEMKIN.hpp:271-297, 1181-1398, 1496-1550, 1683-1768, 1956-1964
+//   maps/StoichiometricMap.hpp:512-598, 656-729, 916-1001
+// ---------------------------------------------------------------------------
+struct Reactor {
+  const Mech& m;
+  int NC, NR;
+  double P0 = 101325.;
+  bool energy = true;
+  double QR = 0.;
+  // thermo map
+  std::vector<double> cp, h, s;
+  // kinetics map caches
+  double T_ = 0., T_old_ = 0.;
+  bool arr_recalc = true, hs_recalc = true;
+  std::vector<double> kArr, uKeq, kRev, kInf, logFcent, rdh, rds, kMod, fwd, rev, net, corr;
+  std::vector<double> x, c, R;
+  long long n_calls = 0;
+
+  explicit Reactor(const Mech& mech) : m(mech), NC(mech.nc), NR(mech.nr) {
+    cp.resize(NC); h.resize(NC); s.resize(NC);
+    kArr.resize(NR); kMod.resize(NR); fwd.resize(NR); rev.resize(NR); net.resize(NR);
+    rdh.resize(NR); rds.resize(NR);
+    uKeq.resize(m.I("rev_thermo").size());
+    kRev.resize(m.I("rev_explicit").size());
+    kInf.resize(m.I("fo_rxn").size()); logFcent.resize(kInf.size()); corr.resize(kInf.size());
+    x.resize(NC); c.resize(NC); R.resize(NC);
+  }
+
+  // ThermodynamicsMap_CHEMKIN::cp_over_R (:436-454)
+  void cp_over_R(double T) {
+    const auto& HT = m.F("cp_ht"); const auto& LT = m.F("cp_lt"); const auto& TM = m.F("t_mid");
+    const double T2 = T * T, T3 = T2 * T, T4 = T3 * T;
+    int j = 0;
+    for (int k = 0; k < NC; ++k) {
+      cp[k] = (T > TM[k]) ? HT[j] + T * HT[j + 1] + T2 * HT[j + 2] + T3 * HT[j + 3] + T4 * HT[j + 4]
+                          : LT[j] + T * LT[j + 1] + T2 * LT[j + 2] + T3 * LT[j + 3] + T4 * LT[j + 4];
+      j += 5;
+    }
+  }
+  // ThermodynamicsMap_CHEMKIN::h_over_RT (:456-475)
+  void h_over_RT(double T) {
+    const auto& HT = m.F("dh_ht"); const auto& LT = m.F("dh_lt"); const auto& TM = m.F("t_mid");
+    const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, uT = 1. / T;
+    int j = 0;
+    for (int k = 0; k < NC; ++k) {
+      h[k] = (T > TM[k]) ? HT[j] + T * HT[j + 1] + T2 * HT[j + 2] + T3 * HT[j + 3] + T4 * HT[j + 4] + uT * HT[j + 5]
+                         : LT[j] + T * LT[j + 1] + T2 * LT[j + 2] + T3 * LT[j + 3] + T4 * LT[j + 4] + uT * LT[j + 5];
+      j += 6;
+    }
+  }
+  // ThermodynamicsMap_CHEMKIN::s_over_R (:477-496)
+  void s_over_R(double T) {
+    const auto& HT = m.F("ds_ht"); const auto& LT = m.F("ds_lt"); const auto& TM = m.F("t_mid");
+    const double logT = std::log(T), T2 = T * T, T3 = T2 * T, T4 = T3 * T;
+    int j = 0;
+    for (int k = 0; k < NC; ++k) {
+      s[k] = (T > TM[k]) ? HT[j] * logT + T * HT[j + 1] + T2 * HT[j + 2] + T3 * HT[j + 3] + T4 * HT[j + 4] + HT[j + 5]
+                         : LT[j] * logT + T * LT[j + 1] + T2 * LT[j + 2] + T3 * LT[j + 3] + T4 * LT[j + 4] + LT[j + 5];
+      j += 6;
+    }
+  }
+
+  // StoichiometricMap::ReactionEnthalpyAndEntropy (:916-1001): per reaction the
+  // species contributions are added in species order, reactant side first.
+  void reaction_h_s() {
+    const auto& rp = m.I("reac_ptr"); const auto& rs = m.I("reac_species"); const auto& rn = m.F("reac_nu");
+    const auto& pp = m.I("prod_ptr"); const auto& ps = m.I("prod_species"); const auto& pn = m.F("prod_nu");
+    for (int j = 0; j < NR; ++j) {
+      double dh = 0., ds = 0.;
+      int a = rp[j], b = pp[j];
+      while (a < rp[j + 1] || b < pp[j + 1]) {
+        int sa = a < rp[j + 1] ? rs[a] : 1 << 30;
+        int sb = b < pp[j + 1] ? ps[b] : 1 << 30;
+        if (sa <= sb) {  // reactant contribution of species sa
+          const double nu = rn[a];
+          dh -= contrib(nu, h[sa]); ds -= contrib(nu, s[sa]); ++a;
+        } else {
+          const double nu = pn[b];
+          dh += contrib(nu, h[sb]); ds += contrib(nu, s[sb]); ++b;
+        }
+      }
+      rdh[j] = dh; rds[j] = ds;
+    }
+  }
+  static double contrib(double nu, double v) {
+    if (nu == 1.) return v;
+    if (nu == 2.) return v + v;
+    if (nu == 3.) return v + v + v;
+    if (nu == 0.5) return 0.5 * v;
+    return nu * v;
+  }
+
+  // KineticsMap_CHEMKIN::SetTemperature (:271-287)
+  void kin_set_T(double T) {
+    T_old_ = T_; T_ = T;
+    if (std::fabs(T_ - T_old_) / T_ > 0.) { arr_recalc = true; hs_recalc = true; }
+  }
+
+  // KineticsMap_CHEMKIN::KineticConstants (:1181-1386)
+  void kinetic_constants() {
+    const double T = T_, uT = 1. / T, logT = std::log(T);
+    const double Patm_over_RT = 101325. / R_J_KMOL / T;
+    const double log_Patm_over_RT = std::log(Patm_over_RT);
+    if (hs_recalc) { s_over_R(T); reaction_h_s(); hs_recalc = false; }
+    if (arr_recalc) {
+      const auto& lnA = m.F("lnA"); const auto& beta = m.F("beta"); const auto& eor = m.F("e_over_r");
+      const auto& sgn = m.I("a_sign");
+      for (int j = 0; j < NR; ++j) kArr[j] = std::exp(lnA[j] + beta[j] * logT - eor[j] * uT);
+      for (int j = 0; j < NR; ++j) if (sgn[j] < 0) kArr[j] *= -1.;
+      const auto& rth = m.I("rev_thermo"); const auto& dnu = m.F("delta_nu");
+      for (size_t k = 0; k < rth.size(); ++k) {
+        const int j = rth[k];
+        uKeq[k] = std::exp(-rds[j] + rdh[j] - log_Patm_over_RT * dnu[j]);
+      }
+      const auto& lr = m.F("lnA_rev"); const auto& br = m.F("beta_rev"); const auto& er = m.F("e_over_r_rev");
+      for (size_t k = 0; k < kRev.size(); ++k) kRev[k] = std::exp(lr[k] + br[k] * logT - er[k] * uT);
+      const auto& fl = m.F("fo_lnA"); const auto& fb = m.F("fo_beta"); const auto& fe = m.F("fo_e_over_r");
+      const auto& ft = m.I("fo_type");
+      const auto& a = m.F("fo_a"); const auto& b = m.F("fo_b"); const auto& cc = m.F("fo_c"); const auto& d = m.F("fo_d");
+      for (size_t k = 0; k < kInf.size(); ++k) kInf[k] = std::exp(fl[k] + fb[k] * logT - fe[k] * uT);
+      for (size_t k = 0; k < kInf.size(); ++k) {
+        if (ft[k] == 1) {
+          double v = (d[k] != 0.) ? (1. - a[k]) * std::exp(-T / b[k]) + a[k] * std::exp(-T / cc[k]) + std::exp(-d[k] / T)
+                                  : (1. - a[k]) * std::exp(-T / b[k]) + a[k] * std::exp(-T / cc[k]);
+          logFcent[k] = (v < 1.e-300) ? -300. : std::log10(v);
+        } else if (ft[k] == 2) {
+          logFcent[k] = a[k] * std::exp(-b[k] / T) + std::exp(-T / cc[k]);
+        }
+      }
+      arr_recalc = false;
+    }
+    kMod = kArr;
+  }
+
+  // KineticsMap_CHEMKIN::ReactionRates (:1683-1768) and FallOffReactions (:1496-1550)
+  void reaction_rates() {
+    double cTot = 0.;
+    for (int i = 0; i < NC; ++i) cTot += c[i];
+    kinetic_constants();
+    const auto& tbr = m.I("tb_rxn"); const auto& tbp = m.I("tb_ptr");
+    const auto& tbs = m.I("tb_species"); const auto& tbe = m.F("tb_eff_m1");
+    for (size_t sidx = 0; sidx < tbr.size(); ++sidx) {
+      double M = cTot;
+      for (int q = tbp[sidx]; q < tbp[sidx + 1]; ++q) M += c[tbs[q]] * tbe[q];
+      kMod[tbr[sidx]] *= M;
+    }
+    const auto& fr = m.I("fo_rxn"); const auto& fty = m.I("fo_type"); const auto& fsg = m.I("fo_single");
+    const auto& fp = m.I("fo_ptr"); const auto& fs = m.I("fo_species"); const auto& fe = m.F("fo_eff_m1");
+    const auto& fd = m.F("fo_d"); const auto& fee = m.F("fo_e");
+    for (size_t k = 0; k < fr.size(); ++k) {
+      double M;
+      if (fsg[k] < 0) {
+        M = cTot;
+        for (int q = fp[k]; q < fp[k + 1]; ++q) M += c[fs[q]] * fe[q];
+      } else {
+        M = c[fsg[k]] + 1.e-16;
+      }
+      const int j = fr[k];
+      const double Pr = kArr[j] * M / kInf[k];
+      double wF = 1.;
+      if (fty[k] == 1) {
+        if (Pr > 1.e-32) {
+          const double nTroe = 0.75 - 1.27 * logFcent[k];
+          const double cTroe = -0.4 - 0.67 * logFcent[k];
+          const double sTroe = std::log10(Pr) + cTroe;
+          const double q = sTroe / (nTroe - 0.14 * sTroe);
+          wF = std::pow(10., logFcent[k] / (1. + q * q));
+        } else {
+          const double q = 1. / 0.14;
+          wF = std::pow(10., logFcent[k] / (1. + q * q));
+        }
+      } else if (fty[k] == 2) {
+        const double l = std::log10(Pr);
+        const double xSRI = 1. / (1. + l * l);
+        wF = std::pow(logFcent[k], xSRI) * fd[k];
+        if (fee[k] != 0.) wF *= std::pow(T_, fee[k]);
+      }
+      corr[k] = kInf[k] * (Pr / (1. + Pr)) * wF / kArr[j];
+    }
+    for (size_t k = 0; k < fr.size(); ++k) kMod[fr[k]] *= corr[k];
+
+    // StoichiometricMap::ProductOfConcentrations (:512-598): factors in species order
+    const auto& rp = m.I("reac_ptr"); const auto& rs = m.I("reac_species"); const auto& rn = m.F("reac_nu");
+    const auto& pp = m.I("prod_ptr"); const auto& ps = m.I("prod_species"); const auto& pn = m.F("prod_nu");
+    const auto& isrev = m.I("is_reversible");
+    for (int j = 0; j < NR; ++j) {
+      double pr = 1.;
+      for (int q = rp[j]; q < rp[j + 1]; ++q) pr *= conc_factor(rn[q], c[rs[q]]);
+      fwd[j] = pr;
+      double pv = 1.;
+      if (isrev[j]) for (int q = pp[j]; q < pp[j + 1]; ++q) pv *= conc_factor(pn[q], c[ps[q]]);
+      rev[j] = pv;
+    }
+    const auto& rth = m.I("rev_thermo");
+    for (size_t k = 0; k < rth.size(); ++k) rev[rth[k]] *= uKeq[k];
+    const auto& rex = m.I("rev_explicit");
+    for (size_t k = 0; k < rex.size(); ++k) rev[rex[k]] *= kRev[k] / kArr[rex[k]];
+    for (int j = 0; j < NR; ++j) net[j] = fwd[j];
+    for (int j = 0; j < NR; ++j) if (isrev[j]) net[j] -= rev[j];
+    for (int j = 0; j < NR; ++j) net[j] *= kMod[j];
+  }
+  static double conc_factor(double nu, double c1) {
+    if (nu == 1.) return c1;
+    if (nu == 2.) return c1 * c1;
+    if (nu == 3.) return c1 * c1 * c1;
+    if (nu == 0.5) return std::sqrt(c1);
+    return std::pow(c1, nu);
+  }
+
+  // StoichiometricMap::FormationRatesFromReactionRates (:656-729)
+  void formation_rates() {
+    const auto& fp = m.I("fr_ptr"); const auto& fr = m.I("fr_rxn"); const auto& fc = m.F("fr_coef");
+    for (int i = 0; i < NC; ++i) {
+      double rate = 0.;
+      for (int q = fp[i]; q < fp[i + 1]; ++q) rate += contrib(fc[q] < 0 ? -fc[q] : fc[q], net[fr[q]]) * (fc[q] < 0 ? -1. : 1.);
+      R[i] = rate;
+    }
+  }
+
+  // BatchReactorHomogeneousConstantPressure::Equations (:175-223)
+  void equations(const double* y, double* dy) {
+    ++n_calls;
+    const auto& MW = m.F("mw");
+    const double T = y[NC];
+    // ThermodynamicsMap_CHEMKIN::MoleFractions_From_MassFractions (:429-434)
+    double u = 0.;
+    for (int i = 0; i < NC; ++i) u += y[i] / MW[i];
+    const double MWmix = 1. / u;
+    for (int i = 0; i < NC; ++i) x[i] = MWmix * y[i];
+    for (int i = 0; i < NC; ++i) x[i] = x[i] / MW[i];
+    const double cTot = P0 / R_J_KMOL / T;
+    for (int i = 0; i < NC; ++i) c[i] = cTot * x[i];
+    const double rho = cTot * MWmix;
+    h_over_RT(T);   // species h/RT at T: used by the reaction enthalpies and by QR
+    kin_set_T(T);
+    reaction_rates();
+    formation_rates();
+    for (int i = 0; i < NC; ++i) dy[i] = MW[i] * R[i] / rho;
+    dy[NC] = 0.;
+    if (energy) {
+      cp_over_R(T);
+      double cpm = 0.;
+      for (int i = 0; i < NC; ++i) cpm += cp[i] * x[i];
+      cpm *= R_J_KMOL;
+      const double CpMixMass = cpm / MWmix;
+      double d = 0.;
+      for (int i = 0; i < NC; ++i) d += R[i] * h[i];
+      QR = -d * R_J_KMOL * T;
+      dy[NC] = QR / (rho * CpMixMass);
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Options and per-cell results
+// ---------------------------------------------------------------------------
+struct Options {
+  double rtol, atol, tmin_chem;
+  double y_min_T, y_max_T;
+  int max_steps;
+  int full_pivoting;
+  int energy;
+  double alfa2_4, alfa2_5;   // order-selection state carried by the reference's solver object
+  int maximum_order;
+};
+
+enum { COUNT_STEPS, COUNT_RHS, COUNT_JAC, COUNT_FACT, COUNT_SOLVE, COUNT_ERRFAIL, COUNT_CONVFAIL, COUNT_JAC_RHS, NCOUNT };
+
+// ---------------------------------------------------------------------------
+// OdeSMOKE::MultiValueSolver< MethodGear< KernelDense<...> > >
+//   math/native-ode-solvers/MultiValueSolver.hpp:40-1328
+//   math/native-ode-solvers/MethodGear.hpp:40-568
+//   math/native-ode-solvers/KernelDense.hpp:44-245
+// ---------------------------------------------------------------------------
+class Gear {
+ public:
+  enum { H_DEC, H_CONST, H_INC };
+  enum { O_DEC, O_CONST, O_INC };
+  enum { JAC_CHANGE, JAC_MODIFIED, JAC_OK };
+  enum { M_TO_FACT, M_FACT };
+  enum { CONV_FAIL, CONV_OK };
+  static const int MAX_ORDER = 5, MIN_ORDER = 1;
+  static const unsigned MAX_ITERATIONS_JACOBIAN = 50, MAX_CONVERGENCE_FAILURE = 50, MAX_ERROR_FAILURE = 50;
+
+  Reactor& sys;
+  unsigned ne;
+  // method constants (MethodGear.hpp:125-193)
+  double r_[MAX_ORDER + 1][MAX_ORDER];
+  double Ep_[MAX_ORDER + 1];
+  double alfa2_[MAX_ORDER + 1];
+  double deltaAlfa1_ = .05, deltaAlfa3_ = .25;
+  // state
+  std::vector<std::vector<double>> z_, v_;
+  std::vector<double> b_, y_, va_, deltab_, f_, vb_, aux_, y0_, oneOverEps_, minv_, maxv_;
+  std::vector<double> J_, G_;   // column major n x n
+  std::vector<int> piv_;
+  double abs_tol_, rel_tol_;
+  bool min_c_ = true, max_c_ = true;
+  bool full_piv_ = false;
+  unsigned maximum_order_ = MAX_ORDER;
+  unsigned max_number_steps_ = 500000;
+  double max_step_size_ = 1.7976931348623154e+308;
+  double min_step_size_ = 0.;
+  bool direction_plus_ = true;
+  // MultiValueSolver scalars
+  double t_, t0_, tOut_, tInMeshPoint_, tStabilize_;
+  double hPreviousStep_, hNordsieck_, hScaleMax_, first_step_size_;
+  bool fixedOrderMin_;
+  unsigned iterOfConstStepsForLargeFactorizationTime_, iterConstSteps_, iterMinimumOrder_;
+  double cpuTimeEquationSystem_ = 0., cpuTimeToFactorize_ = 0.;
+  // MethodGear scalars
+  unsigned p_, iterOrder_, orderInNextStep_, maxConvergenceIterations_, maxIterationsJacobian_;
+  int odeHStatus_, odeOrderStatus_, status_, factorizationStatus_, jacobianStatus_, convergenceStatus_;
+  double h_, hNextStep_, hScale_;
+  unsigned numberOfSteps_, iterConvergence_, iterConvergenceRate_, iterConvergenceFailure_, iterErrorFailure_;
+  unsigned numberOfConvergenceFailuresForOrderMax_;
+  unsigned stepOfLastJacobian_ = 0, stepOfLastFactorization_ = 0;
+  long long cnt_[NCOUNT];
+
+  explicit Gear(Reactor& s, unsigned n) : sys(s), ne(n) {
+    // MethodGear::MemoryAllocationMethod (:125-193)
+    for (int i = 0; i <= MAX_ORDER; ++i) alfa2_[i] = .8;
+    for (int j = 0; j <= MAX_ORDER; ++j) Ep_[j] = (double)factorial(j);
+    for (int i = 0; i <= MAX_ORDER; ++i) for (int j = 0; j < MAX_ORDER; ++j) r_[i][j] = 0.;
+    r_[0][0] = 1.; r_[1][0] = 1.;
+    for (int j = 2; j <= MAX_ORDER; ++j) {
+      r_[0][j - 1] = (double)factorial(j);
+      for (int i = 2; i <= j; ++i) r_[i - 1][j - 1] = double(j) * r_[i - 1][j - 2] + r_[i - 2][j - 2];
+      r_[j][j - 1] = 1.;
+    }
+    double sum = 1.;
+    for (int j = 2; j <= MAX_ORDER; ++j) {
+      sum += 1. / double(j);
+      for (int i = 1; i <= j + 1; ++i) r_[i - 1][j - 1] /= (factorial(j) * sum);
+    }
+    z_.assign(MAX_ORDER + 3, std::vector<double>(n, 0.));
+    v_.assign(MAX_ORDER + 3, std::vector<double>(n, 0.));
+    b_.assign(n, 0.); y_.assign(n, 0.); va_.assign(n, 0.); deltab_.assign(n, 0.); f_.assign(n, 0.);
+    vb_.assign(n, 0.); aux_.assign(n, 0.); y0_.assign(n, 0.); oneOverEps_.assign(n, 0.);
+    minv_.assign(n, 0.); maxv_.assign(n, 0.);
+    J_.assign((size_t)n * n, 0.); G_.assign((size_t)n * n, 0.); piv_.assign(n, 0);
+  }
+  static unsigned factorial(unsigned n) { return n == 0 ? 1 : n * factorial(n - 1); }
+
+  void equations(const std::vector<double>& y, std::vector<double>& dy) { sys.equations(y.data(), dy.data()); ++cnt_[COUNT_RHS]; }
+
+  static double error_control(const std::vector<double>& w, const std::vector<double>& e) {
+    // math/OpenSMOKEUtilities.hpp:689-701
+    double sum = 0.;
+    for (size_t i = 0; i < w.size(); ++i) { const double c = w[i] * e[i]; sum += c * c; }
+    return std::sqrt(sum / double(w.size()));
+  }
+
+  // MultiValueSolver::SetInitialConditions (:367-407) with MethodGear::ResetMethod (:79-123)
+  // and MultiValueSolver::Reset (:107-134)
+  void set_initial_conditions(double t0, const double* y0) {
+    tOut_ = t_ = t0_ = tInMeshPoint_ = tStabilize_ = t0;
+    full_piv_ = false;
+    p_ = 1; iterOrder_ = 0; orderInNextStep_ = 1; maxConvergenceIterations_ = 4;
+    maxIterationsJacobian_ = 20 + 5 * (ne - 3);
+    if (maxIterationsJacobian_ > MAX_ITERATIONS_JACOBIAN && ne < 80) maxIterationsJacobian_ = MAX_ITERATIONS_JACOBIAN;
+    odeHStatus_ = H_CONST; odeOrderStatus_ = O_CONST; status_ = 1;
+    factorizationStatus_ = M_TO_FACT; jacobianStatus_ = JAC_CHANGE; convergenceStatus_ = CONV_OK;
+    h_ = 0.; min_step_size_ = 0.; hNextStep_ = 0.; hScale_ = 0.;
+    numberOfSteps_ = 0; numberOfConvergenceFailuresForOrderMax_ = 0;
+    iterConvergence_ = 0; iterConvergenceRate_ = 0; iterConvergenceFailure_ = 0; iterErrorFailure_ = 0;
+    for (unsigned i = 0; i < ne; ++i) y0_[i] = y0[i];
+    hPreviousStep_ = 0.; hNordsieck_ = 0.; hScaleMax_ = 1000.;
+    fixedOrderMin_ = false;
+    iterOfConstStepsForLargeFactorizationTime_ = 0; iterConstSteps_ = 0; iterMinimumOrder_ = 0;
+    for (int k = 0; k < NCOUNT; ++k) cnt_[k] = 0;
+    equations(y0_, f_);
+  }
+
+  void check_constraints(std::vector<double>& y) {   // MethodGear::CheckConstraints (:518-536)
+    if (min_c_) for (unsigned i = 0; i < ne; ++i) if (y[i] < minv_[i]) y[i] = minv_[i];
+    if (max_c_) for (unsigned i = 0; i < ne; ++i) if (y[i] > maxv_[i]) y[i] = maxv_[i];
+  }
+  unsigned check_illegal(const std::vector<double>& y) {  // MethodGear::CheckIllegalConstraints (:538-568)
+    unsigned n = 0;
+    if (min_c_) for (unsigned i = 0; i < ne; ++i) if (y[i] < minv_[i]) ++n;
+    if (max_c_) for (unsigned i = 0; i < ne; ++i) if (y[i] > maxv_[i]) ++n;
+    return n;
+  }
+
+  void one_over_epsilon(const std::vector<double>& w) {   // MultiValueSolver.hpp:619-645
+    for (unsigned i = 0; i < ne; ++i) oneOverEps_[i] = abs_tol_ + rel_tol_ * std::fabs(w[i]);
+    for (unsigned i = 0; i < ne; ++i) oneOverEps_[i] = 1. / oneOverEps_[i];
+  }
+
+  double initial_step() {   // MultiValueSolver.hpp:648-685
+    double lo, hi;
+    if (t0_ != 0.) { lo = 100. * MACH_EPS_DOUBLE * std::fabs(t0_); hi = std::fabs(t0_); }
+    else { lo = MACH_EPS_DOUBLE; hi = 1.e-4; }
+    one_over_epsilon(y0_);
+    double h0 = 0.5 / (error_control(f_, oneOverEps_) + MACH_EPS_FLOAT);
+    if (h0 < lo) h0 = lo;
+    if (h0 > hi) h0 = hi;
+    h0 *= std::fabs(tOut_ - t0_) / (tOut_ - t0_);
+    return h0;
+  }
+
+  void interpolation() {   // MultiValueSolver.hpp:687-706
+    const double hp = (tOut_ - t_) / hNordsieck_;
+    double hr = 1.;
+    y_ = z_[0];
+    if (hp == 0.) return;
+    for (unsigned i = 1; i <= p_; ++i) {
+      hr *= hp;
+      for (unsigned k = 0; k < ne; ++k) va_[k] = z_[i][k] * hr;
+      for (unsigned k = 0; k < ne; ++k) y_[k] += va_[k];
+    }
+    check_constraints(y_);
+  }
+
+  // KernelDense::NumericalJacobian (:111-193), constrained branch taken when max constraints are on
+  void numerical_jacobian(std::vector<double>& y, const std::vector<double>& f, double h, const std::vector<double>& e) {
+    const double ZERO_DER = std::sqrt(TINY_FLOAT);
+    const double ETA2 = std::sqrt(MACH_EPS_DOUBLE);
+    const double BETA = 1.e+3 * MACH_EPS_DOUBLE;
+    double hf = BETA * std::fabs(h) * error_control(f, e) * double(ne);
+    if (hf < 1.e-10) hf = 1.;
+    for (unsigned j = 0; j < ne; ++j) {
+      const double yh = y[j];
+      double hJ;
+      if (!max_c_) {
+        hJ = ETA2 * std::fabs(std::max(yh, 1. / e[j]));
+        const double hJf = hf / e[j];
+        hJ = std::max(hJ, hJf);
+        hJ = std::max(hJ, ZERO_DER);
+        hJ = std::min(hJ, 0.001 + 0.001 * std::fabs(yh));
+      } else {
+        const double a = std::fabs(yh), b = std::fabs(1. / e[j]);
+        hJ = ETA2 * (a > b ? a : b);
+        const double hJf = hf / e[j];
+        hJ = std::max(hJ, hJf);
+        hJ = std::max(hJ, ZERO_DER);
+        if (yh + hJ > maxv_[j]) hJ = -hJ;
+      }
+      y[j] += hJ;
+      sys.equations(y.data(), aux_.data());
+      ++cnt_[COUNT_JAC_RHS];
+      y[j] = yh;
+      for (unsigned i = 0; i < ne; ++i) aux_[i] -= f[i];
+      const double hInv = 1. / hJ;
+      for (unsigned i = 0; i < ne; ++i) J_[(size_t)j * ne + i] = hInv * aux_[i];
+    }
+  }
+
+  // KernelDense::BuildAndFactorizeMatrixG (:195-220): G = I - hr0 J, partial-pivot LU
+  // (Eigen::PartialPivLU picks the row of largest magnitude in the column).
+  void build_and_factorize(double hr0) {
+    for (size_t q = 0; q < G_.size(); ++q) G_[q] = J_[q];
+    for (size_t q = 0; q < G_.size(); ++q) G_[q] *= -hr0;
+    for (unsigned i = 0; i < ne; ++i) G_[(size_t)i * ne + i] += 1.;
+    const unsigned n = ne;
+    for (unsigned k = 0; k < n; ++k) {
+      unsigned pr = k; double best = std::fabs(G_[(size_t)k * n + k]);
+      for (unsigned i = k + 1; i < n; ++i) { const double a = std::fabs(G_[(size_t)k * n + i]); if (a > best) { best = a; pr = i; } }
+      piv_[k] = (int)pr;
+      if (pr != k) for (unsigned j = 0; j < n; ++j) std::swap(G_[(size_t)j * n + k], G_[(size_t)j * n + pr]);
+      const double d = G_[(size_t)k * n + k];
+      if (d != 0.) for (unsigned i = k + 1; i < n; ++i) G_[(size_t)k * n + i] /= d;
+      for (unsigned j = k + 1; j < n; ++j) {
+        const double ukj = G_[(size_t)j * n + k];
+        for (unsigned i = k + 1; i < n; ++i) G_[(size_t)j * n + i] -= G_[(size_t)k * n + i] * ukj;
+      }
+    }
+    ++cnt_[COUNT_FACT];
+  }
+
+  void solve_linear_system(std::vector<double>& db) {   // KernelDense::SolveLinearSystem (:222-245)
+    const unsigned n = ne;
+    for (unsigned k = 0; k < n; ++k) if (piv_[k] != (int)k) std::swap(db[k], db[piv_[k]]);
+    for (unsigned j = 0; j < n; ++j) { const double v = db[j]; for (unsigned i = j + 1; i < n; ++i) db[i] -= G_[(size_t)j * n + i] * v; }
+    for (int j = (int)n - 1; j >= 0; --j) {
+      db[j] /= G_[(size_t)j * n + j];
+      const double v = db[j];
+      for (int i = 0; i < j; ++i) db[i] -= G_[(size_t)j * n + i] * v;
+    }
+    ++cnt_[COUNT_SOLVE];
+  }
+
+  void jacobian_times_vector(const std::vector<double>& vin, std::vector<double>& vout) {   // KernelDense.hpp:90-94
+    for (unsigned i = 0; i < ne; ++i) {
+      double s = 0.;
+      for (unsigned j = 0; j < ne; ++j) s += J_[(size_t)j * ne + i] * vin[j];
+      vout[i] = s;
+    }
+  }
+
+  // MethodGear::FindCorrection (:195-341)
+  unsigned find_correction(double t) {
+    vb_ = v_[0];
+    check_constraints(vb_);
+    equations(vb_, f_);
+    if (numberOfSteps_ >= stepOfLastJacobian_ + maxIterationsJacobian_) jacobianStatus_ = JAC_CHANGE;
+    if (jacobianStatus_ == JAC_CHANGE) {
+      stepOfLastJacobian_ = numberOfSteps_;
+      jacobianStatus_ = JAC_MODIFIED;
+      numerical_jacobian(vb_, f_, h_, oneOverEps_);
+      ++cnt_[COUNT_JAC];
+      factorizationStatus_ = M_TO_FACT;
+    }
+    const double hr0 = h_ * r_[0][p_ - 1];
+    if (factorizationStatus_ == M_FACT && iterOrder_ == 0) factorizationStatus_ = M_TO_FACT;
+    if (factorizationStatus_ == M_TO_FACT) {
+      stepOfLastFactorization_ = numberOfSteps_;
+      build_and_factorize(hr0);
+      factorizationStatus_ = M_FACT;
+    }
+    for (unsigned i = 0; i < ne; ++i) deltab_[i] = f_[i] * h_;
+    for (unsigned i = 0; i < ne; ++i) deltab_[i] -= v_[1][i];
+    solve_linear_system(deltab_);
+    b_ = deltab_;
+    double oldCC = 0.;
+    for (unsigned k = 1; k <= maxConvergenceIterations_; ++k) {
+      const double cc = r_[0][p_ - 1] * error_control(deltab_, oneOverEps_);
+      if (cc < 1.) { convergenceStatus_ = CONV_OK; return k; }
+      if (k > 1 && cc > 2. * oldCC) { convergenceStatus_ = CONV_FAIL; return k; }
+      oldCC = cc;
+      for (unsigned i = 0; i < ne; ++i) va_[i] = b_[i] * r_[0][p_ - 1];
+      for (unsigned i = 0; i < ne; ++i) va_[i] += v_[0][i];
+      if (min_c_) for (unsigned j = 0; j < ne; ++j) if (va_[j] < minv_[j]) { va_[j] = minv_[j]; b_[j] = (minv_[j] - z_[0][j]) / r_[0][p_ - 1]; }
+      if (max_c_) for (unsigned j = 0; j < ne; ++j) if (va_[j] > maxv_[j]) { va_[j] = maxv_[j]; b_[j] = (maxv_[j] - z_[0][j]) / r_[0][p_ - 1]; }
+      equations(va_, f_);
+      for (unsigned i = 0; i < ne; ++i) deltab_[i] = f_[i] * h_;
+      for (unsigned i = 0; i < ne; ++i) deltab_[i] -= v_[1][i];
+      for (unsigned i = 0; i < ne; ++i) deltab_[i] -= b_[i];
+      solve_linear_system(deltab_);
+      for (unsigned i = 0; i < ne; ++i) b_[i] += deltab_[i];
+    }
+    convergenceStatus_ = CONV_FAIL;
+    return maxConvergenceIterations_;
+  }
+
+  // MethodGear::WhatToDoInCaseOfConvergenceFailure (:343-423)
+  void convergence_failure_recovery() {
+    hScale_ = 0.25;
+    if (numberOfSteps_ < 10) hScale_ = 0.1;
+    hScale_ = std::max(hScale_, min_step_size_ / std::fabs(h_));
+    odeHStatus_ = H_DEC;
+    if (p_ > (unsigned)MIN_ORDER) { p_ -= 1; odeOrderStatus_ = O_DEC; }
+    alfa2_[4] -= 0.01;
+    alfa2_[5] -= 0.02;
+    if (alfa2_[4] < 0.) { alfa2_[4] = 0.; maximum_order_ = 3; if (p_ > 3) { p_ = 3; odeOrderStatus_ = O_DEC; } }
+    if (alfa2_[5] < 0.) { alfa2_[5] = 0.; maximum_order_ = 4; if (p_ > 4) { p_ = 4; odeOrderStatus_ = O_DEC; } }
+    if (numberOfSteps_ > 5) {
+      numberOfConvergenceFailuresForOrderMax_++;
+      if (numberOfConvergenceFailuresForOrderMax_ % 5 == 0) {
+        if (p_ != (unsigned)MIN_ORDER) { p_ = MIN_ORDER; odeOrderStatus_ = O_DEC; }
+      }
+      if (numberOfConvergenceFailuresForOrderMax_ % 10 == 0 && tStabilize_ != tInMeshPoint_) {
+        equations(z_[0], va_);
+        for (unsigned i = 0; i < ne; ++i) z_[1][i] = va_[i] * h_;
+        tStabilize_ = tInMeshPoint_;
+      }
+    }
+    if (numberOfSteps_ > stepOfLastJacobian_ + MAX_ITERATIONS_JACOBIAN / 10) jacobianStatus_ = JAC_CHANGE;
+    if (numberOfSteps_ != stepOfLastJacobian_ && iterConvergenceFailure_ == MAX_CONVERGENCE_FAILURE) jacobianStatus_ = JAC_CHANGE;
+    hNextStep_ *= hScale_;
+  }
+
+  // MethodGear::ConvergenceRate (:425-516)
+  void convergence_rate() {
+    if (iterErrorFailure_ > 0 || iterConvergenceFailure_ > 0) iterConvergenceRate_ = 0;
+    if (iterConvergence_ <= 1) return;
+    for (unsigned i = 0; i < ne; ++i) vb_[i] = v_[0][i] - z_[0][i];
+    jacobian_times_vector(vb_, va_);
+    for (unsigned i = 0; i < ne; ++i) va_[i] *= h_;
+    for (unsigned i = 0; i < ne; ++i) va_[i] += z_[1][i];
+    for (unsigned i = 0; i < ne; ++i) va_[i] = v_[1][i] - va_[i];
+    double normd = 0., normf = 0.;
+    for (unsigned i = 0; i < ne; ++i) normd += std::fabs(va_[i]);
+    for (unsigned i = 0; i < ne; ++i) normf += std::fabs(v_[1][i]);
+    if (normd > 3. * normf + .1 && iterConvergence_ > 2) {
+      if (numberOfSteps_ > stepOfLastJacobian_ + MAX_ITERATIONS_JACOBIAN / 10) jacobianStatus_ = JAC_CHANGE;
+      hScale_ = 0.5; odeHStatus_ = H_DEC; hNextStep_ = h_ * hScale_;
+      if (p_ > 1) { orderInNextStep_ = p_ - 1; odeOrderStatus_ = O_DEC; }
+      iterConvergenceRate_ = 0; iterConvergenceFailure_ = 1;
+      return;
+    }
+    if (normd > normf + 0.1) {
+      iterConvergenceRate_++;
+      if (iterConvergenceRate_ >= 5) {
+        hScale_ = 0.8; odeHStatus_ = H_DEC; hNextStep_ = h_ * hScale_;
+        iterConvergenceRate_ = 0; iterConvergenceFailure_ = 1;
+      }
+      if (numberOfSteps_ > stepOfLastJacobian_ + MAX_ITERATIONS_JACOBIAN / 10 && iterConvergence_ > 2) {
+        jacobianStatus_ = JAC_CHANGE;
+        iterConvergenceRate_ = 0; iterConvergenceFailure_ = 1;
+      }
+    }
+  }
+
+  // MultiValueSolver::MultiValueStep (:1212-1328)
+  void multi_value_step() {
+    for (unsigned i = 0; i <= p_; ++i) v_[i] = z_[i];
+    for (int i = 0; i < int(p_); ++i)
+      for (int j = int(p_ - 1); j >= i; --j)
+        for (unsigned k = 0; k < ne; ++k) v_[j][k] += v_[j + 1][k];
+    if (min_c_) for (unsigned j = 0; j < ne; ++j) if (v_[0][j] < minv_[j]) {
+      if (std::fabs(v_[0][j] - minv_[j]) * oneOverEps_[j] < double(ne)) {
+        v_[0][j] = minv_[j]; v_[1][j] = minv_[j] - z_[0][j];
+        for (unsigned i = 2; i <= p_; ++i) v_[i][j] = 0.;
+      }
+    }
+    if (max_c_) for (unsigned j = 0; j < ne; ++j) if (v_[0][j] > maxv_[j]) {
+      if (std::fabs(v_[0][j] - maxv_[j]) * oneOverEps_[j] < double(ne)) {
+        v_[0][j] = maxv_[j]; v_[1][j] = maxv_[j] - z_[0][j];
+        for (unsigned i = 2; i <= p_; ++i) v_[i][j] = 0.;
+      }
+    }
+    iterConvergence_ = find_correction(t_);
+    if (convergenceStatus_ == CONV_FAIL) return;
+    const double r0 = r_[0][p_ - 1];
+    for (unsigned i = 0; i < ne; ++i) va_[i] = b_[i] * r0;
+    if (min_c_) for (unsigned j = 0; j < ne; ++j) if (v_[0][j] + va_[j] < minv_[j]) {
+      b_[j] = minv_[j] - z_[0][j] - v_[1][j];
+      v_[0][j] = minv_[j] - va_[j];
+      if (v_[0][j] < minv_[j]) v_[0][j] = minv_[j];
+    }
+    if (max_c_) for (unsigned j = 0; j < ne; ++j) if (v_[0][j] + va_[j] > maxv_[j]) {
+      b_[j] = maxv_[j] - z_[0][j] - v_[1][j];
+      v_[0][j] = maxv_[j] - va_[j];
+      if (v_[0][j] > maxv_[j]) v_[0][j] = maxv_[j];
+    }
+    for (unsigned k = 0; k < ne; ++k) v_[0][k] += va_[k];
+    for (unsigned k = 0; k < ne; ++k) v_[1][k] += b_[k];
+    for (unsigned i = 2; i <= p_; ++i) {
+      const double ri = r_[i][p_ - 1];
+      for (unsigned k = 0; k < ne; ++k) va_[k] = b_[k] * ri;
+      for (unsigned k = 0; k < ne; ++k) v_[i][k] += va_[k];
+    }
+    for (unsigned k = 0; k < ne; ++k) va_[k] = v_[p_][k] - z_[p_][k];
+    for (unsigned k = 0; k < ne; ++k) v_[p_ + 1][k] = va_[k] / (double(p_) + 1.);
+    if (iterOrder_ >= p_) {
+      for (unsigned k = 0; k < ne; ++k) va_[k] = v_[p_ + 1][k] - z_[p_ + 1][k];
+      for (unsigned k = 0; k < ne; ++k) v_[p_ + 2][k] = va_[k] / (double(p_) + 2.);
+    }
+  }
+
+  // MultiValueSolver::NewOrderNewH (:1042-1210); the CPU-time heuristics are
+  // always false because cpuTimeToFactorize_ stays 0 (MultiValueSolver.hpp:133).
+  void new_order_new_h() {
+    double hMinus = 0., hCur = 0., hPlus = 0., alfa1 = 0., alfa3 = 0.;
+    if (p_ > (unsigned)MIN_ORDER && odeOrderStatus_ != O_INC) {
+      hMinus = Ep_[p_ - 1] * error_control(v_[p_], oneOverEps_) + MACH_EPS_FLOAT;
+      hMinus = 1. / hMinus;
+      alfa1 = alfa2_[p_ - 1] - deltaAlfa1_;
+      hMinus = alfa1 * std::pow(hMinus, 1. / double(p_));
+    }
+    {
+      hCur = Ep_[p_] * error_control(v_[p_ + 1], oneOverEps_) + MACH_EPS_FLOAT;
+      hCur = 1. / hCur;
+      hCur = alfa2_[p_] * std::pow(hCur, 1. / double(p_ + 1));
+    }
+    if (p_ < maximum_order_ && odeOrderStatus_ != O_DEC) {
+      hPlus = Ep_[p_ + 1] * error_control(v_[p_ + 2], oneOverEps_) + MACH_EPS_FLOAT;
+      hPlus = 1. / hPlus;
+      alfa3 = alfa2_[p_ + 1] - deltaAlfa3_;
+      hPlus = alfa3 * std::pow(hPlus, 1. / double(p_ + 2));
+    }
+    if (hMinus > hCur && hMinus > hPlus) {
+      hScale_ = (.75 / alfa1) * hMinus; orderInNextStep_ = p_ - 1; odeOrderStatus_ = O_DEC;
+    } else if (hCur > hMinus && hCur > hPlus) {
+      hScale_ = (.75 / alfa2_[p_]) * hCur; orderInNextStep_ = p_; odeOrderStatus_ = O_CONST;
+    } else {
+      hScale_ = (.75 / alfa3) * hPlus; orderInNextStep_ = p_ + 1; odeOrderStatus_ = O_INC;
+    }
+    if (fixedOrderMin_) {
+      iterMinimumOrder_++;
+      if (iterMinimumOrder_ < 2000) {
+        hScale_ = (.75 / alfa2_[p_]) * hCur; orderInNextStep_ = p_; odeOrderStatus_ = O_CONST;
+      } else fixedOrderMin_ = false;
+    }
+    {
+      double scl = 1.2;
+      if (hScale_ < scl) {
+        iterOfConstStepsForLargeFactorizationTime_ = 0;
+        iterConstSteps_++;
+        hScale_ = 1.; odeHStatus_ = H_CONST; orderInNextStep_ = p_; odeOrderStatus_ = O_CONST; hNextStep_ = h_;
+      } else {
+        iterConstSteps_ = 0;
+        hScale_ = std::min(hScale_, hScaleMax_);
+        odeHStatus_ = H_INC;
+        hNextStep_ = h_ * hScale_;
+        if (hNextStep_ > max_step_size_) hNextStep_ = max_step_size_;
+      }
+    }
+    if (iterConstSteps_ > 500 || (numberOfSteps_ % 1000 == 0 && numberOfSteps_ != 0 &&
+                                  (std::fabs(h_) < 1.e-7 || std::fabs(h_) < 1.e-5 * t_))) {
+      if (p_ > (unsigned)MIN_ORDER) {
+        fixedOrderMin_ = true; iterMinimumOrder_ = 0;
+        orderInNextStep_ = MIN_ORDER; odeOrderStatus_ = O_DEC;
+        hScale_ = 0.5; hNextStep_ = h_ * hScale_; odeHStatus_ = H_DEC;
+      }
+    }
+  }
+
+  // MultiValueSolver::DriverStep (:753-1040)
+  void driver_step() {
+    iterConvergenceFailure_ = 0; iterErrorFailure_ = 0; convergenceStatus_ = CONV_OK;
+    if (odeOrderStatus_ != O_CONST || odeHStatus_ != H_CONST) iterOrder_ = 0;
+    p_ = orderInNextStep_;
+    odeOrderStatus_ = O_CONST;
+    hScaleMax_ = 2.;
+    if (numberOfSteps_ < 10) hScaleMax_ = 1000.;
+    else if (numberOfSteps_ > 10 && numberOfSteps_ < 20) hScaleMax_ = 10.;
+    while (true) {
+      if (odeHStatus_ != H_CONST) {
+        hScale_ = hNextStep_ / hNordsieck_;
+        double hr = 1.;
+        for (unsigned i = 1; i <= p_; ++i) { hr *= hScale_; for (unsigned k = 0; k < ne; ++k) z_[i][k] *= hr; }
+        check_constraints(z_[0]);
+        iterOrder_ = 0;
+        odeHStatus_ = H_CONST;
+      }
+      h_ = hNextStep_;
+      hNordsieck_ = hNextStep_;
+      if (std::fabs(h_) < MACH_EPS_FLOAT * min_step_size_) { status_ = -6; return; }
+      t_ = tInMeshPoint_ + h_;
+      if (t_ == tInMeshPoint_) { status_ = -6; return; }
+      multi_value_step();
+      if (convergenceStatus_ == CONV_FAIL) {
+        iterConvergenceFailure_++;
+        ++cnt_[COUNT_CONVFAIL];
+        if (iterConvergenceFailure_ >= MAX_CONVERGENCE_FAILURE) { status_ = -5; return; }
+        if (std::fabs(h_ - min_step_size_) <= MACH_EPS_DOUBLE * std::fabs(min_step_size_)) { status_ = -6; return; }
+        convergence_failure_recovery();
+      } else {
+        double hCur = Ep_[p_] * error_control(v_[p_ + 1], oneOverEps_);
+        if (hCur > 1.) {
+          iterErrorFailure_++;
+          ++cnt_[COUNT_ERRFAIL];
+          if (iterErrorFailure_ >= MAX_ERROR_FAILURE) { status_ = -4; return; }
+          if (std::fabs(h_ - min_step_size_) <= MACH_EPS_DOUBLE * std::fabs(min_step_size_)) { status_ = -6; return; }
+          hScaleMax_ = 1.;
+          hCur = 0.8 * std::pow(1. / hCur, 1. / double(p_ + 1));
+          hScale_ = hCur;
+          if (p_ > (unsigned)MIN_ORDER) {
+            double hMinus = Ep_[p_ - 1] * error_control(v_[p_], oneOverEps_);
+            hMinus = 1. / (hMinus + MACH_EPS_FLOAT);
+            hMinus = 0.8 * std::pow(hMinus, 1. / double(p_));
+            if (hMinus > hCur) { hScale_ = hMinus; p_ -= 1; odeOrderStatus_ = O_DEC; }
+          }
+          hScale_ = std::min(hScale_, 0.5);
+          hScale_ = std::max(hScale_, min_step_size_ / std::fabs(h_));
+          hScale_ = std::max(hScale_, 1.e-3);
+          if (p_ == 1 && hScale_ < 0.1 && numberOfSteps_ > 10 && tInMeshPoint_ != tStabilize_) {
+            equations(z_[0], va_);
+            for (unsigned i = 0; i < ne; ++i) z_[1][i] = va_[i] * h_;
+            tStabilize_ = tInMeshPoint_;
+          }
+          odeHStatus_ = H_DEC;
+          hNextStep_ *= hScale_;
+        } else {
+          hNordsieck_ = h_; hPreviousStep_ = h_; hNextStep_ = h_;
+          orderInNextStep_ = p_; odeOrderStatus_ = O_CONST; odeHStatus_ = H_CONST;
+          convergence_rate();
+          if (iterErrorFailure_ > 0 || iterConvergenceFailure_ > 0) { iterErrorFailure_ = 0; iterConvergenceFailure_ = 0; }
+          else { iterOrder_++; if (iterOrder_ > p_ + 1) new_order_new_h(); }
+          for (unsigned i = 0; i <= p_ + 2; ++i) z_[i] = v_[i];
+          check_constraints(z_[0]);
+          break;
+        }
+      }
+    }
+  }
+
+  // MultiValueSolver::Solve (:423-617), first call after SetInitialConditions.
+  // Returns the status; on failure y_ holds the last accepted state (the
+  // reference would hand back stale data here, MultiValueSolver.hpp:567-574).
+  int solve(double tOut) {
+    tOut_ = tOut;
+    if (t0_ > tOut_) direction_plus_ = false;
+    if (check_illegal(y0_) != 0) { status_ = -9; y_ = y0_; return status_; }
+    first_step_size_ = initial_step();
+    z_[0] = y0_;
+    for (unsigned i = 0; i < ne; ++i) z_[1][i] = f_[i] * first_step_size_;
+    hPreviousStep_ = first_step_size_; hNordsieck_ = first_step_size_; hNextStep_ = first_step_size_;
+    status_ = 2;
+    for (unsigned k = 1; k <= max_number_steps_; ++k) {
+      one_over_epsilon(z_[0]);
+      const double tolSafe = MACH_EPS_DOUBLE * error_control(z_[0], oneOverEps_);
+      if (tolSafe > 1.) { status_ = -2; y_ = z_[0]; return status_; }
+      tInMeshPoint_ = t_;
+      driver_step();
+      if (status_ <= 0) { t_ = tInMeshPoint_; y_ = z_[0]; return status_; }
+      numberOfSteps_++;
+      ++cnt_[COUNT_STEPS];
+      if (tOut_ == t_) { y_ = z_[0]; return status_; }
+      if ((direction_plus_ && tOut_ < t_) || (!direction_plus_ && tOut_ > t_)) {
+        interpolation();
+        equations(y_, va_);   // printResults_ == true: sets the reactor's QR at tOut (:605-609)
+        return status_;
+      }
+    }
+    status_ = -1;
+    y_ = z_[0];
+    return status_;
+  }
+};
+
+}  // namespace orc
+
+// ---------------------------------------------------------------------------
+// C interface used by the tests and by bench.py's CPU baseline.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+struct orc_options {
+  double rtol, atol, tmin_chem, y_min_T, y_max_T;
+  int max_steps, full_pivoting, energy;
+  double alfa2_4, alfa2_5;
+  int maximum_order;
+  int sequential_state;   // 1: carry alfa2/maximum_order across cells like one solver object per rank
+};
+
+void* orc_mech_load(const void* blob, size_t n) {
+  try { return orc::load_blob((const unsigned char*)blob, n); } catch (...) { return nullptr; }
+}
+void orc_mech_free(void* m) { delete (orc::Mech*)m; }
+
+// One right-hand side evaluation: y = [Y_1..Y_NC, T] -> dy, and the heat release.
+int orc_rhs(void* mech, double P, const double* y, double* dy, double* qr) {
+  const orc::Mech& m = *(const orc::Mech*)mech;
+  orc::Reactor r(m);
+  r.P0 = P;
+  r.equations(y, dy);
+  if (qr) *qr = r.QR;
+  return 0;
+}
+
+// Finite-difference Jacobian exactly as the solver builds it (for tests).
+int orc_fd_jacobian(void* mech, double P, const double* y, double h, double rtol, double atol,
+                    double y_max_T, double* J_colmajor) {
+  const orc::Mech& m = *(const orc::Mech*)mech;
+  orc::Reactor r(m);
+  r.P0 = P;
+  const unsigned n = m.nc + 1;
+  orc::Gear g(r, n);
+  for (unsigned i = 0; i < n; ++i) { g.minv_[i] = 0.; g.maxv_[i] = 1.; }
+  g.minv_[n - 1] = 200.; g.maxv_[n - 1] = y_max_T;
+  g.abs_tol_ = atol; g.rel_tol_ = rtol;
+  std::vector<double> yy(y, y + n), f(n);
+  r.equations(yy.data(), f.data());
+  g.one_over_epsilon(yy);
+  g.numerical_jacobian(yy, f, h, g.oneOverEps_);
+  std::memcpy(J_colmajor, g.J_.data(), sizeof(double) * n * n);
+  return 0;
+}
+
+// Batched reaction step, cell-major state Y[ncells][NC] (in/out), T[ncells] (in/out).
+// solvers/laminarSMOKE/unsteady/chemistry_DI.H:76-331 (OpenSMOKE native branch)
+// and solvers/laminarSMOKE/utilities.H:153-200 (normalizeMassFractions).
+int orc_reaction_step(void* mech, const orc_options* o, int ncells, double* Y, double* T, double p,
+                      double t0, const double* dt, double dt_scalar, double* Q, int* status,
+                      long long* counters, int nthreads) {
+  const orc::Mech& m = *(const orc::Mech*)mech;
+  const int NC = m.nc;
+  const unsigned NEQ = NC + 1;
+  int nerr = 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  const bool seq = o->sequential_state != 0;
+#pragma omp parallel if (!seq) reduction(+ : nerr)
+  {
+    orc::Reactor reactor(m);
+    orc::Gear g(reactor, NEQ);
+    g.alfa2_[4] = o->alfa2_4; g.alfa2_[5] = o->alfa2_5; g.maximum_order_ = o->maximum_order;
+    std::vector<double> y0(NEQ), yf(NEQ);
+#pragma omp for schedule(dynamic, 1)
+    for (int cell = 0; cell < ncells; ++cell) {
+      if (!seq) { g.alfa2_[4] = o->alfa2_4; g.alfa2_[5] = o->alfa2_5; g.maximum_order_ = o->maximum_order; }
+      double* Yc = Y + (size_t)cell * NC;
+      int st = 0;
+      if (T[cell] > o->tmin_chem) {
+        for (int i = 0; i < NC; ++i) y0[i] = Yc[i];
+        y0[NC] = T[cell];
+        double sum = 0.;
+        for (int i = 0; i < NC; ++i) { if (y0[i] < 0.) y0[i] = 0.; sum += y0[i]; }
+        for (int i = 0; i < NC; ++i) y0[i] /= sum;
+        reactor.P0 = p;
+        reactor.energy = o->energy != 0;
+        if (!reactor.energy) reactor.QR = 0.;
+        g.set_initial_conditions(t0, y0.data());
+        g.full_piv_ = o->full_pivoting != 0;
+        g.abs_tol_ = o->atol; g.rel_tol_ = o->rtol;
+        for (unsigned i = 0; i < NEQ; ++i) { g.minv_[i] = 0.; g.maxv_[i] = 1.; }
+        g.minv_[NC] = o->y_min_T; g.maxv_[NC] = o->y_max_T;
+        g.max_number_steps_ = (unsigned)o->max_steps;
+        const double dtc = dt ? dt[cell] : dt_scalar;
+        st = g.solve(t0 + dtc);
+        yf = g.y_;
+        if (Q) Q[cell] = reactor.QR;
+        if (counters) for (int k = 0; k < orc::NCOUNT; ++k) counters[(size_t)cell * orc::NCOUNT + k] = g.cnt_[k];
+        if (st < 0) nerr++;
+      } else {
+        for (int i = 0; i < NC; ++i) yf[i] = Yc[i];
+        yf[NC] = T[cell];
+        st = 0;
+        if (counters) for (int k = 0; k < orc::NCOUNT; ++k) counters[(size_t)cell * orc::NCOUNT + k] = 0;
+      }
+      double s = 0.;
+      for (int i = 0; i < NC; ++i) s += yf[i];
+      for (int i = 0; i < NC; ++i) yf[i] /= s;
+      for (int i = 0; i < NC; ++i) Yc[i] = yf[i];
+      if (o->energy) T[cell] = yf[NC];
+      if (status) status[cell] = st;
+    }
+  }
+  return nerr;
+}
+
+int orc_num_counters() { return orc::NCOUNT; }
+
+}  // extern "C"

@@ -1,0 +1,109 @@
+"""ctypes binding of liblsmoke_oracle.so -- test infrastructure only.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, as the checker; the product path never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liblsmoke_oracle.so")
+NCOUNT = 8
+COUNTER_NAMES = ("steps", "rhs", "jacobians", "factorizations", "solves",
+                 "error_failures", "convergence_failures", "jacobian_rhs")
+
+
+class OrcOptions(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("tmin_chem", C.c_double),
+                ("y_min_T", C.c_double), ("y_max_T", C.c_double),
+                ("max_steps", C.c_int), ("full_pivoting", C.c_int), ("energy", C.c_int),
+                ("alfa2_4", C.c_double), ("alfa2_5", C.c_double),
+                ("maximum_order", C.c_int), ("sequential_state", C.c_int)]
+
+
+def build() -> str:
+    subprocess.check_call(["make", "-s", "-C", HERE])
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.orc_mech_load.restype = C.c_void_p
+        L.orc_mech_load.argtypes = [C.c_void_p, C.c_size_t]
+        L.orc_mech_free.argtypes = [C.c_void_p]
+        L.orc_rhs.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_fd_jacobian.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_double,
+                                      C.c_double, C.c_double, C.c_void_p]
+        L.orc_reaction_step.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_double, C.c_double, C.c_void_p, C.c_double, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_reaction_step.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+class OracleMechanism:
+    def __init__(self, blob: bytes):
+        self._buf = (C.c_ubyte * len(blob)).from_buffer_copy(blob)
+        self.h = lib().orc_mech_load(C.cast(self._buf, C.c_void_p), len(blob))
+        if not self.h:
+            raise ValueError("oracle: bad mechanism blob")
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().orc_mech_free(self.h)
+        except Exception:
+            pass
+
+    def rhs(self, y: np.ndarray, p: float = 101325.0):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        dy = np.zeros_like(y)
+        q = np.zeros(1)
+        lib().orc_rhs(self.h, p, _ptr(y), _ptr(dy), _ptr(q))
+        return dy, float(q[0])
+
+    def fd_jacobian(self, y, h, rtol=1e-7, atol=1e-12, p=101325.0, y_max_T=6000.0):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        n = y.size
+        J = np.zeros(n * n)
+        lib().orc_fd_jacobian(self.h, p, _ptr(y), h, rtol, atol, y_max_T, _ptr(J))
+        return J.reshape(n, n).T.copy()  # stored column-major
+
+    def reaction_step(self, Y, T, dt, p=101325.0, t0=0.0, rtol=1e-7, atol=1e-12, tmin_chem=0.0,
+                      max_steps=500000, energy=True, alfa2_4=0.8, alfa2_5=0.8, maximum_order=5,
+                      sequential_state=False, nthreads=0, y_min_T=200.0, y_max_T=6000.0):
+        """Cell-major Y[ncells, NC], T[ncells]; returns (Y, T, Q, status, counters)."""
+        Y = np.array(Y, dtype=np.float64, order="C", copy=True)
+        T = np.array(T, dtype=np.float64, copy=True)
+        n = T.size
+        dt_arr = None
+        dt_s = 0.0
+        if np.ndim(dt) == 0:
+            dt_s = float(dt)
+        else:
+            dt_arr = np.ascontiguousarray(dt, dtype=np.float64)
+        Q = np.zeros(n)
+        st = np.zeros(n, dtype=np.int32)
+        cnt = np.zeros((n, NCOUNT), dtype=np.int64)
+        o = OrcOptions(rtol, atol, tmin_chem, y_min_T, y_max_T, max_steps, 0, int(energy),
+                       alfa2_4, alfa2_5, maximum_order, int(sequential_state))
+        lib().orc_reaction_step(self.h, C.byref(o), n, _ptr(Y), _ptr(T), p, t0, _ptr(dt_arr), dt_s,
+                                _ptr(Q), _ptr(st), _ptr(cnt), nthreads)
+        return Y, T, Q, st, cnt

@@ -1,0 +1,45 @@
+"""The C-ABI library loads and exports every entry point include/lsmoke_gpu.h declares (no GPU needed)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HDR = os.path.join(ROOT, "include", "lsmoke_gpu.h")
+
+
+def declared_symbols():
+    txt = open(HDR).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(lsg_[a-z_0-9]+)\s*\(", txt)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ("lsg_reaction_step", "lsg_reaction_step_device", "lsg_mech_load_blob", "lsg_ctx_create"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    from laminarsmoke_b200 import lsg
+    if not os.path.exists(lsg.LIB_PATH):
+        from laminarsmoke_b200.csrc import build
+        build.build()
+    L = C.CDLL(lsg.LIB_PATH)
+    missing = [s for s in declared_symbols() if not hasattr(L, s)]
+    assert not missing, missing
+    assert set(lsg.EXPORTS) <= set(declared_symbols())
+
+
+def test_options_defaults_and_errors_without_gpu():
+    from laminarsmoke_b200 import lsg
+    o = lsg.default_options()
+    assert (o.rtol, o.atol, o.y_min_T, o.y_max_T, o.max_steps, o.maximum_order) == (1e-7, 1e-12, 200.0, 6000.0, 500000, 5)
+    assert (o.alfa2_4, o.alfa2_5, o.energy, o.precision) == (0.8, 0.8, 1, 0)
+    L = lsg.lib()
+    assert L.lsg_abi_version() == 1
+    h = C.c_void_p()
+    bad = (C.c_ubyte * 16)(*b"NOTAMECHANISM000")
+    assert L.lsg_mech_load_blob(C.cast(bad, C.c_void_p), 16, 0, C.byref(h)) == -2
+    assert L.lsg_strerror(-2) == b"mechanism blob could not be read"

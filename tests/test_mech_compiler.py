@@ -1,0 +1,144 @@
+"""CHEMKIN compiler: hand-computed known answers for the reference's preprocessing rules."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from laminarsmoke_b200.mech import blob, chemkin, synthetic
+
+REF = "/root/reference/run/kinetic-mechanisms/POLIMI_H2CO_1412/"
+have_ref = os.path.exists(REF)
+
+R_J_KMOL = 8314.4621
+J_FROM_CAL = 8.3144621 / (8.3144621 / 4.18443)
+
+
+def test_h2co_dimensions(h2co):
+    data, species, A = h2co
+    assert species == ["H2", "O2", "H2O", "H2O2", "O", "H", "OH", "HO2", "CO", "CO2", "HCO", "HE", "AR", "N2"]
+    assert list(A["dims"]) == [14, 33]
+    assert len(A["rev_thermo"]) == 29 and len(A["rev_explicit"]) == 0
+    assert len(A["tb_rxn"]) == 5 and list(A["fo_rxn"]) == [2, 12, 16]
+    assert list(A["fo_type"]) == [1, 1, 0]   # Troe, Troe, Lindemann
+
+
+def test_molecular_weights_float_rounded_elements(h2co):
+    _, species, A = h2co
+    H, O, C, N = 1.008000016212463, 15.998999595642090, 12.010999679565430, 14.0069999694824
+    mw = dict(zip(species, A["mw"]))
+    assert mw["H2"] == 0.0 + H * 2.0
+    assert mw["O2"] == 0.0 + O * 2.0
+    assert mw["N2"] == 0.0 + N * 2.0
+    assert mw["AR"] == 39.948001861572270
+    assert mw["CO2"] == (0.0 + C * 1.0) + O * 2.0
+
+
+def test_unit_conversion_bimolecular(h2co):
+    _, _, A = h2co
+    # H+O2=OH+O  .9600E+15 -.200 16625.0 (cal/mol, cm3/mol/s)
+    a = 0.96e15 * (math.pow(1.e3, 1. - 2.) / math.pow(1., 1. - 2.))
+    assert A["lnA"][0] == math.log(a)
+    assert A["beta"][0] == -0.2
+    assert A["e_over_r"][0] == (16625.0 * (1.e3 * J_FROM_CAL)) / R_J_KMOL
+    # J_FROM_CAL is computed as R_J_mol / R_cal_mol (it rounds to 4.18443 in double)
+
+
+def test_low_swap_and_falloff_units(h2co):
+    _, _, A = h2co
+    # H+O2(+M)=HO2(+M) main line .5580E+13 .400 .0 ; LOW/ .8400E+18 -.800 .0/
+    k0 = 0.84e18 * (math.pow(1.e3, -2.) / math.pow(1., -2.))
+    kinf = 0.558e13 * (math.pow(1.e3, 1. - 2.) / math.pow(1., 1. - 2.))
+    assert A["lnA"][2] == math.log(k0)     # "direct" constant is k0
+    assert A["beta"][2] == -0.8
+    assert A["fo_lnA"][0] == math.log(kinf)
+    assert A["fo_beta"][0] == 0.4
+    assert (A["fo_a"][0], A["fo_b"][0], A["fo_c"][0], A["fo_d"][0]) == (0.5, 1.0e-30, 1.0e30, 0.0)
+    # TROE with 4 parameters
+    assert (A["fo_a"][1], A["fo_b"][1], A["fo_c"][1], A["fo_d"][1]) == (0.7346, 94.0, 1756.0, 5182.0)
+
+
+def test_third_body_units_and_efficiencies(h2co):
+    _, species, A = h2co
+    # H2+M=H+H+M .1115E+15 .000 96081.0 ; sum of reactant orders = 1 + 1 (M)
+    j = 7
+    assert A["lnA"][j] == math.log(0.1115e15 * math.pow(1.e3, 1. - 2.))
+    k = list(A["tb_rxn"]).index(j)
+    sl = slice(A["tb_ptr"][k], A["tb_ptr"][k + 1])
+    eff = dict(zip([species[s] for s in A["tb_species"][sl]], A["tb_eff_m1"][sl]))
+    assert eff == {"H2": 2.5 - 1., "H2O": 12.0 - 1., "AR": 0.5 - 1., "CO": 1.9 - 1., "CO2": 3.8 - 1.}
+    # products H+H merged into one entry with nu = 2
+    ps = slice(A["prod_ptr"][j], A["prod_ptr"][j + 1])
+    assert [species[s] for s in A["prod_species"][ps]] == ["H"]
+    assert list(A["prod_nu"][ps]) == [2.0]
+    assert A["delta_nu"][j] == 1.0
+
+
+def test_irreversible_and_duplicates(h2co):
+    _, _, A = h2co
+    # 4 irreversible reactions ('=>'); the DUPLICATE pair stays two reactions
+    assert int((A["is_reversible"] == 0).sum()) == 4
+    assert A["lnA"][18] != A["lnA"][19]
+
+
+def test_formation_list_order_matches_buckets(h2co):
+    _, species, A = h2co
+    # species H: reactant entries first (bucket order, reactions ascending), then products
+    i = species.index("H")
+    sl = slice(A["fr_ptr"][i], A["fr_ptr"][i + 1])
+    coef = A["fr_coef"][sl]
+    neg = np.where(coef < 0)[0]
+    pos = np.where(coef > 0)[0]
+    assert neg.max() < pos.min()
+    assert 2.0 in coef  # H produced with nu = 2 by H2+M=H+H+M
+
+
+def test_nasa_tables(h2co):
+    _, species, A = h2co
+    k = species.index("H2O")
+    raw = A["nasa_raw"].reshape(-1, 18)[k]
+    assert A["dh_ht"][6 * k + 2] == (1. / 3.) * raw[2]
+    assert A["ds_lt"][6 * k + 3] == (1. / 3.) * raw[10]
+    assert A["t_mid"][k] == raw[16]
+
+
+def test_blob_roundtrip(h2co):
+    data, species, A = h2co
+    A2, sp2 = blob.unpack(blob.pack(A, species))
+    assert sp2 == species
+    for k in A:
+        np.testing.assert_array_equal(A[k], A2[k])
+
+
+@pytest.mark.skipif(not have_ref, reason="reference CHEMKIN files not present")
+def test_packaged_blob_matches_fresh_compile(h2co):
+    m = chemkin.compile_files(REF + "POLIMI_H2CO_1412.CKI", REF + "POLIMI_TOT_NOX_1412.CKT")
+    assert blob.pack(m.arrays, m.species) == h2co[0]
+
+
+def test_tmid_correction_is_off_by_default():
+    s = synthetic.generate(20, 30, seed=7)
+    a = chemkin.compile_mechanism(s.kinetics, s.thermo)
+    b = chemkin.compile_mechanism(s.kinetics, s.thermo, tmid_correct=True)
+    assert not np.array_equal(a.arrays["cp_lt"], b.arrays["cp_lt"])
+
+
+def test_parser_rejects_unknown_species():
+    kin = "ELEMENTS\nH\nEND\nSPECIES\nH H2\nEND\nREACTIONS\nH+X=H2 1.0 0.0 0.0\nEND\n"
+    s = synthetic.generate(12, 10, seed=1)
+    with pytest.raises(chemkin.ChemkinError):
+        chemkin.compile_mechanism(kin, s.thermo)
+
+
+@pytest.mark.parametrize("ns,nr", [(120, 800)])
+def test_synthetic_mechanism_is_element_balanced(ns, nr):
+    s = synthetic.generate(ns, nr, seed=1201)
+    m = chemkin.compile_mechanism(s.kinetics, s.thermo)
+    assert m.n_species == ns and m.n_reactions == nr
+    comp = np.array([s.compositions[n] for n in m.species], dtype=float)
+    A = m.arrays
+    for j in range(nr):
+        lhs = sum(A["reac_nu"][q] * comp[A["reac_species"][q]] for q in range(A["reac_ptr"][j], A["reac_ptr"][j + 1]))
+        rhs = sum(A["prod_nu"][q] * comp[A["prod_species"][q]] for q in range(A["prod_ptr"][j], A["prod_ptr"][j + 1]))
+        np.testing.assert_array_equal(lhs, rhs)
+    assert len(A["tb_rxn"]) == round(0.15 * nr) and len(A["fo_rxn"]) == round(0.10 * nr)

@@ -45,6 +45,11 @@ extern "C" {
 #define LSG_PRECISION_FP64 0   /* plain: the reference method in FP64 */
 #define LSG_PRECISION_MIXED 1  /* FP64 rates/residual/error control, FP32 factorisation + FP64 refinement */
 
+/* work decomposition (lsg_options.tile) */
+#define LSG_TILE_AUTO 0        /* FP64 -> warp per cell; MIXED -> lane per cell */
+#define LSG_TILE_WARP 1        /* one warp per cell, the reference's operation order (FP64 only) */
+#define LSG_TILE_LANE 2        /* one thread per cell, persistent grid + device work queue */
+
 /* counters per cell (lsg_reaction_step_device counters_out layout) */
 #define LSG_NCOUNTERS 8        /* steps, rhs, jacobians, factorisations, solves, error-test fails, convergence fails, jacobian rhs */
 
@@ -71,7 +76,8 @@ typedef struct lsg_options {
   double alfa2_4;
   double alfa2_5;
   int maximum_order;
-  int reserved[7];
+  int tile;             /* LSG_TILE_* */
+  int reserved[6];
 } lsg_options;
 
 void lsg_options_default(lsg_options* opt);

@@ -18,6 +18,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
 
 UNITS = [
     ("lsg_plain.cu", ["-fmad=false"]),
+    ("lsg_batched.cu", []),
     ("lsg_api.cu", []),
     ("lsg_mech_host.cpp", []),
 ]

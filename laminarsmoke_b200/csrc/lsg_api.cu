@@ -35,6 +35,11 @@ struct lsg_ctx {
   double* dQ = nullptr;
   int* dstatus = nullptr;
   int* dnsteps = nullptr;
+  // lane-per-cell (batched) resources
+  double* slots = nullptr;
+  long nslots = 0;
+  int* queue = nullptr;
+  int sm_count = 0;
 };
 
 namespace {
@@ -70,6 +75,7 @@ int ensure_gear(int device) {
   if (g_gear_uploaded[device]) return LSG_OK;
   const GearConsts g = make_gear_consts();
   if (upload_gear_plain(g) != cudaSuccess) return LSG_ERR_CUDA;
+  if (upload_gear_batched(g) != cudaSuccess) return LSG_ERR_CUDA;
   g_gear_uploaded[device] = true;
   return LSG_OK;
 }
@@ -97,6 +103,8 @@ int validate_options(const lsg_options* o) {
   if (o->full_pivoting != 0) return LSG_ERR_UNSUPPORTED;
   if (o->precision != LSG_PRECISION_FP64 && o->precision != LSG_PRECISION_MIXED) return LSG_ERR_ARG;
   if (o->maximum_order < 1 || o->maximum_order > 5) return LSG_ERR_ARG;
+  if (o->tile < LSG_TILE_AUTO || o->tile > LSG_TILE_LANE) return LSG_ERR_ARG;
+  if (o->tile == LSG_TILE_WARP && o->precision != LSG_PRECISION_FP64) return LSG_ERR_UNSUPPORTED;
   return LSG_OK;
 }
 
@@ -126,13 +134,49 @@ int ensure_capacity(lsg_ctx* c, long n) {
   return LSG_OK;
 }
 
+int resolve_tile(const lsg_options& o) {
+  if (o.tile != LSG_TILE_AUTO) return o.tile;
+  return o.precision == LSG_PRECISION_FP64 ? LSG_TILE_WARP : LSG_TILE_LANE;
+}
+
+int ensure_batched(lsg_ctx* c, bool lu64) {
+  const MechLayout& L = c->mech->host.layout;
+  if (!c->sm_count) {
+    if (cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess)
+      return LSG_ERR_CUDA;
+  }
+  int bps = 0;
+  if (batched_occupancy(L, lu64, &bps) != cudaSuccess || bps <= 0) return LSG_ERR_UNSUPPORTED;
+  const long want = (long)c->sm_count * bps * batched_threads_per_block();
+  const size_t per = batched_slot_doubles(L, lu64);
+  if (c->slots && c->nslots == want) return LSG_OK;
+  cudaFree(c->slots);
+  c->slots = nullptr;
+  c->nslots = 0;
+  if (cudaMalloc(&c->slots, sizeof(double) * per * (size_t)want) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+  if (!c->queue && cudaMalloc(&c->queue, sizeof(int)) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+  c->nslots = want;
+  return LSG_OK;
+}
+
 int launch_step(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
   const MechLayout& L = c->mech->host.layout;
-  if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
-  if (c->opt.precision != LSG_PRECISION_FP64) return LSG_ERR_UNSUPPORTED;
   const StepOptions so = to_step_options(c->opt);
-  if (plain_smem_bytes(L) > 227 * 1024) return LSG_ERR_UNSUPPORTED;
-  if (launch_plain(L, c->mech->d_buf, so, a, c->d_err, s) != cudaSuccess) return LSG_ERR_CUDA;
+  const int tile = resolve_tile(c->opt);
+  if (tile == LSG_TILE_WARP) {
+    if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
+    if (plain_smem_bytes(L) > 227 * 1024) return LSG_ERR_UNSUPPORTED;
+    if (launch_plain(L, c->mech->d_buf, so, a, c->d_err, s) != cudaSuccess) return LSG_ERR_CUDA;
+    return LSG_OK;
+  }
+  const bool lu64 = c->opt.precision == LSG_PRECISION_FP64;
+  if (batched_smem_bytes(L, lu64) > 227 * 1024) return LSG_ERR_UNSUPPORTED;
+  const int r = ensure_batched(c, lu64);
+  if (r != LSG_OK) return r;
+  if (cudaMemsetAsync(c->queue, 0, sizeof(int), s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (launch_batched(L, c->mech->d_buf, so, a, c->slots, c->nslots, nullptr, c->queue, lu64, c->d_err, s) !=
+      cudaSuccess)
+    return LSG_ERR_CUDA;
   return LSG_OK;
 }
 
@@ -256,6 +300,8 @@ int lsg_ctx_destroy(lsg_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   free_buffers(c);
+  cudaFree(c->slots);
+  cudaFree(c->queue);
   cudaFree(c->d_err);
   cudaStreamDestroy(c->stream);
   delete c;

@@ -46,6 +46,14 @@ size_t plain_smem_bytes(const MechLayout& L);
 cudaError_t upload_gear_plain(const GearConsts& gc);
 cudaError_t launch_plain(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
                          const StepArgs& a, int* err, cudaStream_t stream);
+size_t batched_slot_doubles(const MechLayout& L, bool lu64);
+size_t batched_smem_bytes(const MechLayout& L, bool lu64);
+int batched_threads_per_block();
+cudaError_t upload_gear_batched(const GearConsts& gc);
+cudaError_t batched_occupancy(const MechLayout& L, bool lu64, int* blocks_per_sm);
+cudaError_t launch_batched(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                           const StepArgs& a, double* slots, long nslots, const int* order, int* queue, bool lu64,
+                           int* err, cudaStream_t stream);
 cudaError_t launch_rhs_warp(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y,
                             double* dy, long ld, double p, int energy, double* qr, int* err, cudaStream_t stream);
 

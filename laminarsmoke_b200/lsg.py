@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(HERE, "liblsmoke_gpu.so")
 
 LSG_PRECISION_FP64 = 0
 LSG_PRECISION_MIXED = 1
+LSG_TILE_AUTO, LSG_TILE_WARP, LSG_TILE_LANE = 0, 1, 2
 NCOUNTERS = 8
 COUNTER_NAMES = ("steps", "rhs", "jacobians", "factorizations", "solves",
                  "error_failures", "convergence_failures", "jacobian_rhs")
@@ -33,7 +34,7 @@ class Options(C.Structure):
                 ("max_steps", C.c_int), ("full_pivoting", C.c_int), ("energy", C.c_int),
                 ("precision", C.c_int),
                 ("alfa2_4", C.c_double), ("alfa2_5", C.c_double), ("maximum_order", C.c_int),
-                ("reserved", C.c_int * 7)]
+                ("tile", C.c_int), ("reserved", C.c_int * 6)]
 
 
 EXPORTS = (

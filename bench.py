@@ -30,6 +30,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 NCELLS = 1 << 20
+NCELLS_REF = NCELLS   # ms_per_step of the reference arm: time for the full workload at the sampled rate
 DT = 1.0e-5
 P_ATM = 101325.0
 METRIC = "chemistry cells·steps/s: mixed-prec batched vs plain FP64 on 1 B200 at ≤1e-6 rel T err"
@@ -45,7 +46,10 @@ def parse():
     ap.add_argument("--form", choices=("mixed", "plain"), default="mixed")
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cells", type=int, default=NCELLS)
-    ap.add_argument("--cpu-sample", type=int, default=2048, help="cells of the CPU baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="cells of the CPU baseline sample (0: sized for about 10 s of CPU work)")
+    ap.add_argument("--tile", choices=("lane", "persistent"), default="lane",
+                    help="batched form: round scheme (lane) or persistent lane kernel")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
@@ -125,13 +129,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def cpu_baseline(data, Y, T, sample: int, seed: int = 7):
-    """The reference's CPU step (oracle restatement) on the host cores, bounded sample."""
+def cpu_baseline(data, Y, T, sample: int = 0, seed: int = 7, target_s: float = 10.0):
+    """The reference's CPU step (oracle restatement) on the host cores, bounded sample.
+
+    sample = 0 sizes the sample from a 256-cell pilot so that it takes about
+    target_s seconds of CPU work (capped at the workload size)."""
     from oracle.oracle import OracleMechanism
-    rng = np.random.default_rng(seed)
-    pick = rng.choice(Y.shape[0], size=min(sample, Y.shape[0]), replace=False)
     om = OracleMechanism(data)
     threads = os.cpu_count() or 1
+    rng = np.random.default_rng(seed)
+    if sample <= 0:
+        pilot = rng.choice(Y.shape[0], size=min(256 * threads, Y.shape[0]), replace=False)
+        t0 = time.perf_counter()
+        om.reaction_step(Y[pilot], T[pilot], DT, nthreads=threads)
+        rate = len(pilot) / max(time.perf_counter() - t0, 1e-6)
+        sample = int(min(Y.shape[0], max(len(pilot), rate * target_s)))
+    pick = rng.choice(Y.shape[0], size=min(sample, Y.shape[0]), replace=False)
     t0 = time.perf_counter()
     om.reaction_step(Y[pick], T[pick], DT, nthreads=threads)
     el = time.perf_counter() - t0
@@ -153,20 +166,22 @@ def run_reference(args, rank: int, world: int):
     from laminarsmoke_b200 import mech
     data_holder = [mech.load("h2co")[0]]
     data, species, arrays, Y, T = workload(args.cells, 2, pool_cpu)
-    per = []
-    for _ in range(args.warmup + args.steps):
-        r = cpu_baseline(data, Y, T, args.cpu_sample, seed=7 + len(per))
+    per, samples = [], []
+    for k in range(args.warmup + args.steps):
+        target = 2.0 if k < args.warmup else 10.0
+        r = cpu_baseline(data, Y, T, args.cpu_sample, seed=7 + k, target_s=target)
         per.append(r["value"])
+        samples.append(r["sample"])
     vals = per[args.warmup:]
     v = float(np.mean(vals))
     threads = os.cpu_count() or 1
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": args.cpu_sample / v * 1e3,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(NCELLS_REF / v * 1e3),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic", "config": {"workload": "h2co_uneven_1M", "ncells": args.cells,
-                                           "mechanism": "POLIMI_H2CO_1412", "dt": DT, "sample": args.cpu_sample},
+                                           "mechanism": "POLIMI_H2CO_1412", "dt": DT},
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                            "sample": f"{args.cpu_sample} cells of the workload per step, {threads} threads"},
+                            "sample": "; ".join(samples[args.warmup:])},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
@@ -195,8 +210,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     n = Y.shape[0]
     nc = Y.shape[1]
     if args.form == "mixed":
-        ctx = lsg.ReactionStep(m, tile=lsg.LSG_TILE_LANE, precision=lsg.LSG_PRECISION_MIXED)
-        kernel_name, dtype = "batched_kernel<float>", "f64"
+        tile = lsg.LSG_TILE_LANE if args.tile == "lane" else 3
+        ctx = lsg.ReactionStep(m, tile=tile, precision=lsg.LSG_PRECISION_MIXED)
+        kernel_name = "rounds_*" if args.tile == "lane" else "batched_kernel<float>"
+        dtype = "f64+f32"
     else:
         ctx = plain
         kernel_name, dtype = "plain_warp_kernel", "f64"
@@ -228,9 +245,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    l0 = ctx.launches()
     with ClockSampler(local_rank) as clk:
         evs = [one() for _ in range(args.steps)]
         torch.cuda.synchronize()
+    launches = ctx.launches() - l0
     if world > 1:
         dist.barrier()
     ms = float(sum(a.elapsed_time(b) for a, b in evs))
@@ -311,7 +330,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "statuses": {str(k): int(v) for k, v in zip(*np.unique(st, return_counts=True))},
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": args.steps,
+            "gpu_launches": launches,
             "clocks": clk.summary(),
         }
         print(json.dumps(out), flush=True)

@@ -128,6 +128,10 @@ int lsg_reaction_step_device(lsg_ctx* ctx, int ncells, int nspecies, double* Y_d
 /* The context's own stream (a cudaStream_t), for callers without one. */
 void* lsg_ctx_stream(lsg_ctx* ctx);
 
+/* Number of kernels this context has enqueued so far (diagnostics; no
+ * counterpart in the reference). */
+long long lsg_ctx_launches(const lsg_ctx* ctx);
+
 /* Waits for the device, then reads and clears the error flags kernels raised
  * (0 = none).  Returns LSG_ERR_DEVICE when a flag was set. */
 int lsg_ctx_check(lsg_ctx* ctx, int* device_flags);

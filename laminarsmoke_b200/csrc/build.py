@@ -19,6 +19,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
 UNITS = [
     ("lsg_plain.cu", ["-fmad=false"]),
     ("lsg_batched.cu", []),
+    ("lsg_rounds.cu", []),
     ("lsg_api.cu", []),
     ("lsg_mech_host.cpp", []),
 ]

@@ -40,6 +40,14 @@ struct lsg_ctx {
   long nslots = 0;
   int* queue = nullptr;
   int sm_count = 0;
+  // round-scheme (lane-per-cell) resources
+  void* rstate = nullptr;
+  long rcap = 0;
+  int rstate_lu64 = -1;
+  RoundsPlan rplan{};
+  int rplan_lu64 = -1;
+  int* nact_host = nullptr;   // pinned
+  long long launches = 0;     // kernels enqueued by this context
 };
 
 namespace {
@@ -76,6 +84,7 @@ int ensure_gear(int device) {
   const GearConsts g = make_gear_consts();
   if (upload_gear_plain(g) != cudaSuccess) return LSG_ERR_CUDA;
   if (upload_gear_batched(g) != cudaSuccess) return LSG_ERR_CUDA;
+  if (upload_gear_rounds(g) != cudaSuccess) return LSG_ERR_CUDA;
   g_gear_uploaded[device] = true;
   return LSG_OK;
 }
@@ -103,7 +112,7 @@ int validate_options(const lsg_options* o) {
   if (o->full_pivoting != 0) return LSG_ERR_UNSUPPORTED;
   if (o->precision != LSG_PRECISION_FP64 && o->precision != LSG_PRECISION_MIXED) return LSG_ERR_ARG;
   if (o->maximum_order < 1 || o->maximum_order > 5) return LSG_ERR_ARG;
-  if (o->tile < LSG_TILE_AUTO || o->tile > LSG_TILE_LANE) return LSG_ERR_ARG;
+  if (o->tile < LSG_TILE_AUTO || o->tile > 3) return LSG_ERR_ARG;
   if (o->tile == LSG_TILE_WARP && o->precision != LSG_PRECISION_FP64) return LSG_ERR_UNSUPPORTED;
   return LSG_OK;
 }
@@ -159,14 +168,58 @@ int ensure_batched(lsg_ctx* c, bool lu64) {
   return LSG_OK;
 }
 
+int sm_count(lsg_ctx* c) {
+  if (!c->sm_count &&
+      cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess)
+    return 0;
+  return c->sm_count;
+}
+
+int ensure_rounds(lsg_ctx* c, long n, bool lu64) {
+  const MechLayout& L = c->mech->host.layout;
+  if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
+  if (!sm_count(c)) return LSG_ERR_CUDA;
+  if (c->rplan_lu64 != (int)lu64) {
+    if (rounds_prepare(L, lu64, c->sm_count, &c->rplan) != cudaSuccess) {
+      cudaGetLastError();
+      return LSG_ERR_UNSUPPORTED;
+    }
+    c->rplan_lu64 = (int)lu64;
+  }
+  if (!c->nact_host && cudaMallocHost(&c->nact_host, 2 * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    return LSG_ERR_NOMEM;
+  }
+  if (c->rstate && c->rcap >= n && c->rstate_lu64 == (int)lu64) return LSG_OK;
+  cudaFree(c->rstate);
+  c->rstate = nullptr;
+  c->rcap = 0;
+  const long cap = (n + 255) & ~255L;
+  if (cudaMalloc(&c->rstate, rounds_bytes(L, cap, lu64)) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+  c->rcap = cap;
+  c->rstate_lu64 = (int)lu64;
+  return LSG_OK;
+}
+
 int launch_step(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
   const MechLayout& L = c->mech->host.layout;
   const StepOptions so = to_step_options(c->opt);
   const int tile = resolve_tile(c->opt);
+  if (tile == LSG_TILE_LANE) {
+    const bool lu64 = c->opt.precision == LSG_PRECISION_FP64;
+    const int r = ensure_rounds(c, a.ncells, lu64);
+    if (r != LSG_OK) return r;
+    const long max_rounds = 4L * (long)c->opt.max_steps * (L.nc + 9) + 64;
+    const cudaError_t e = launch_rounds(c->rplan, L, c->mech->d_buf, so, a, c->rstate, c->rcap, c->nact_host,
+                                        max_rounds, c->d_err, s, &c->launches);
+    if (e == cudaErrorLaunchTimeout) return LSG_ERR_DEVICE;
+    return e == cudaSuccess ? LSG_OK : LSG_ERR_CUDA;
+  }
   if (tile == LSG_TILE_WARP) {
     if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
     if (plain_smem_bytes(L) > 227 * 1024) return LSG_ERR_UNSUPPORTED;
     if (launch_plain(L, c->mech->d_buf, so, a, c->d_err, s) != cudaSuccess) return LSG_ERR_CUDA;
+    c->launches += 1;
     return LSG_OK;
   }
   const bool lu64 = c->opt.precision == LSG_PRECISION_FP64;
@@ -177,6 +230,7 @@ int launch_step(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
   if (launch_batched(L, c->mech->d_buf, so, a, c->slots, c->nslots, nullptr, c->queue, lu64, c->d_err, s) !=
       cudaSuccess)
     return LSG_ERR_CUDA;
+  c->launches += 1;
   return LSG_OK;
 }
 
@@ -302,6 +356,8 @@ int lsg_ctx_destroy(lsg_ctx* c) {
   free_buffers(c);
   cudaFree(c->slots);
   cudaFree(c->queue);
+  cudaFree(c->rstate);
+  if (c->nact_host) cudaFreeHost(c->nact_host);
   cudaFree(c->d_err);
   cudaStreamDestroy(c->stream);
   delete c;
@@ -309,6 +365,8 @@ int lsg_ctx_destroy(lsg_ctx* c) {
 }
 
 void* lsg_ctx_stream(lsg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+long long lsg_ctx_launches(const lsg_ctx* c) { return c ? c->launches : -1; }
 
 int lsg_ctx_check(lsg_ctx* c, int* flags) {
   if (!c) return LSG_ERR_ARG;

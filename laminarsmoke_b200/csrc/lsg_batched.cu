@@ -499,6 +499,9 @@ batched_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem, StepO
         const int orr = __shfl_xor_sync(kFull, r, off);
         if (ov > v || (ov == v && orr < r)) { v = ov; r = orr; }
       }
+      // one pivot for the whole warp; a NaN column cannot send it outside rows k..n-1
+      r = __shfl_sync(kFull, r, 0);
+      if (r < k || r >= n) r = k;
       if (lane == 0) sPIV[k * kBT + q] = r;
       if (r != k && i < n) {
         const LUT tmp = lq[(k * n + i) * kLS];

@@ -54,6 +54,18 @@ cudaError_t batched_occupancy(const MechLayout& L, bool lu64, int* blocks_per_sm
 cudaError_t launch_batched(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
                            const StepArgs& a, double* slots, long nslots, const int* order, int* queue, bool lu64,
                            int* err, cudaStream_t stream);
+// Round scheme (lsg_rounds.cu): launch geometry chosen once per context.
+struct RoundsPlan {
+  bool lu64;
+  size_t rhs_smem, adv_smem, fac_smem;
+  unsigned g_rhs, g_adv, g_fac, g_cmp, g_init;
+};
+size_t rounds_bytes(const MechLayout& L, long ns, bool lu64);
+cudaError_t upload_gear_rounds(const GearConsts& gc);
+cudaError_t rounds_prepare(const MechLayout& L, bool lu64, int sm_count, RoundsPlan* plan);
+cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsigned char* mech_gmem,
+                          const StepOptions& o, const StepArgs& a, void* state, long ns, int* nact_host,
+                          long max_rounds, int* err, cudaStream_t stream, long long* launches);
 cudaError_t launch_rhs_warp(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y,
                             double* dy, long ld, double p, int energy, double* qr, int* err, cudaStream_t stream);
 

@@ -41,7 +41,7 @@ EXPORTS = (
     "lsg_options_default", "lsg_mech_load_blob", "lsg_mech_load_file", "lsg_mech_info",
     "lsg_mech_destroy", "lsg_ctx_create", "lsg_ctx_set_options", "lsg_ctx_destroy",
     "lsg_reaction_step", "lsg_reaction_step_device", "lsg_ctx_check", "lsg_rhs_device",
-    "lsg_strerror", "lsg_abi_version", "lsg_ctx_stream",
+    "lsg_strerror", "lsg_abi_version", "lsg_ctx_stream", "lsg_ctx_launches",
 )
 
 _lib = None
@@ -73,6 +73,8 @@ def lib():
     L.lsg_abi_version.restype = i
     L.lsg_ctx_stream.argtypes = [vp]
     L.lsg_ctx_stream.restype = vp
+    L.lsg_ctx_launches.argtypes = [vp]
+    L.lsg_ctx_launches.restype = C.c_longlong
     _lib = L
     return L
 
@@ -204,6 +206,10 @@ class ReactionStep:
         _check(lib().lsg_rhs_device(self.h, n, y.data_ptr(), dy.data_ptr(), ld, p,
                                     None if qr is None else qr.data_ptr(),
                                     _stream_handle(stream)), "lsg_rhs_device")
+
+    def launches(self) -> int:
+        """Kernels this context has enqueued so far."""
+        return int(lib().lsg_ctx_launches(self.h))
 
     def check(self):
         f = C.c_int()

@@ -40,6 +40,7 @@ extern "C" {
 #define LSG_ERR_UNSUPPORTED -5 /* option or mechanism size not supported */
 #define LSG_ERR_DEVICE -6      /* a kernel reported an internal error flag */
 #define LSG_ERR_IO -7          /* file could not be read */
+#define LSG_ERR_SCRATCH -8     /* problem does not fit the fixed scratch of lsg_reaction_step_device_noalloc */
 
 /* precision / algorithm forms */
 #define LSG_PRECISION_FP64 0   /* plain: the reference method in FP64 */
@@ -48,7 +49,8 @@ extern "C" {
 /* work decomposition (lsg_options.tile) */
 #define LSG_TILE_AUTO 0        /* FP64 -> warp per cell; MIXED -> lane per cell */
 #define LSG_TILE_WARP 1        /* one warp per cell, the reference's operation order (FP64 only) */
-#define LSG_TILE_LANE 2        /* one thread per cell, persistent grid + device work queue */
+#define LSG_TILE_LANE 2        /* one thread per cell, rounds of RHS / solver / factor kernels over the live cells */
+#define LSG_TILE_PERSISTENT 3  /* one thread per cell, one persistent kernel + device work queue */
 
 /* counters per cell (lsg_reaction_step_device counters_out layout) */
 #define LSG_NCOUNTERS 8        /* steps, rhs, jacobians, factorisations, solves, error-test fails, convergence fails, jacobian rhs */
@@ -135,6 +137,33 @@ long long lsg_ctx_launches(const lsg_ctx* ctx);
 /* Waits for the device, then reads and clears the error flags kernels raised
  * (0 = none).  Returns LSG_ERR_DEVICE when a flag was set. */
 int lsg_ctx_check(lsg_ctx* ctx, int* device_flags);
+
+/* ---- reaction step without device allocation ------------------------------
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory while they advance the chemistry -- a CFD code that
+ * gives all free device memory to its own pool allocator at start-up, or one
+ * that keeps cudaMalloc/cudaFree (which synchronise the whole device) out of
+ * its time-step loop.  It needs no context: mech (loaded beforehand) and the
+ * caller's device arrays, laid out as for lsg_reaction_step_device, are all it
+ * takes.  It runs the persistent lane-per-cell kernel (LSG_TILE_PERSISTENT)
+ * with its per-cell work space in a fixed array of LSG_NOALLOC_SCRATCH_BYTES
+ * that every GPU loading this part of the library keeps until the process
+ * exits; as many cells are in flight as that array holds, and any number of
+ * cells is processed.
+ *   - opt: NULL for the defaults; precision FP64 or MIXED, tile is ignored.
+ *   - Mechanisms with more than 31 species do not fit: LSG_ERR_SCRATCH.
+ *   - Synchronous: returns when the step has finished on `stream` (NULL = the
+ *     legacy default stream).  The first call on a device looks up the device
+ *     address of the array (once per device); make that first call before any
+ *     stream capture.
+ *   - All calls on a device share the array and it keeps the previous call's
+ *     contents: calls that overlap on the GPU (several streams or host
+ *     threads at once) race and must be serialised by the caller. */
+#define LSG_NOALLOC_SCRATCH_BYTES (16u << 20)
+int lsg_reaction_step_device_noalloc(const lsg_mech* mech, const lsg_options* opt, int ncells, int nspecies,
+                                     double* Y_dev, long ld, double* T_dev, double p, double t0, const double* dt_dev,
+                                     double dt_scalar, double* Q_dev, int* status_dev, int* nsteps_dev,
+                                     long long* counters_dev, void* stream);
 
 /* ---- right-hand side -----------------------------------------------------
  * f(y) of the constant-pressure reactor for ncells states

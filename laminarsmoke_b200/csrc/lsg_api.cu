@@ -267,6 +267,7 @@ const char* lsg_strerror(int code) {
     case LSG_ERR_UNSUPPORTED: return "option or mechanism size not supported";
     case LSG_ERR_DEVICE: return "a kernel reported an internal error";
     case LSG_ERR_IO: return "file could not be read";
+    case LSG_ERR_SCRATCH: return "problem exceeds the fixed no-allocation scratch (at most 31 species)";
     default: return "unknown error";
   }
 }
@@ -444,6 +445,52 @@ int lsg_reaction_step(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, d
   if (cudaStreamSynchronize(s) != cudaSuccess) return LSG_ERR_CUDA;
   int flags = 0;
   return lsg_ctx_check(c, &flags);
+}
+
+int lsg_reaction_step_device_noalloc(const lsg_mech* m, const lsg_options* opt, int ncells, int nspecies,
+                                     double* Y, long ld, double* T, double p, double t0, const double* dt,
+                                     double dt_scalar, double* Q, int* status, int* nsteps, long long* counters,
+                                     void* stream) {
+  if (!m || ncells < 0 || !Y || !T || ld < ncells) return LSG_ERR_ARG;
+  lsg_options o;
+  lsg_options_default(&o);
+  if (opt) o = *opt;
+  o.tile = LSG_TILE_PERSISTENT;
+  const int v = validate_options(&o);
+  if (v != LSG_OK) return v;
+  const MechLayout& L = m->host.layout;
+  if (nspecies != L.nc || !(p > 0.)) return LSG_ERR_ARG;
+  if (L.nc + 1 > 32) return LSG_ERR_SCRATCH;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(m->device) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_CUDA; }
+  const int g = ensure_gear(m->device);
+  if (g != LSG_OK) return g;
+  const bool lu64 = o.precision == LSG_PRECISION_FP64;
+  if (batched_smem_bytes(L, lu64) > 227 * 1024) return LSG_ERR_SCRATCH;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess) return LSG_ERR_CUDA;
+  const long nslots = batched_noalloc_slots(L, lu64, sms);
+  if (nslots <= 0) return LSG_ERR_SCRATCH;
+  StepArgs a{};
+  a.ncells = ncells;
+  a.ld = ld;
+  a.Y = Y;
+  a.T = T;
+  a.dt = dt;
+  a.dt_scalar = dt_scalar;
+  a.t0 = t0;
+  a.p = p;
+  a.Q = Q;
+  a.status = status;
+  a.nsteps = nsteps;
+  a.counters = counters;
+  int flags = 0;
+  if (launch_batched_noalloc(L, m->d_buf, to_step_options(o), a, lu64, m->device, nslots, &flags,
+                             (cudaStream_t)stream) != cudaSuccess) {
+    cudaGetLastError();
+    return LSG_ERR_CUDA;
+  }
+  return flags ? LSG_ERR_DEVICE : LSG_OK;
 }
 
 int lsg_rhs_device(lsg_ctx* c, int ncells, const double* y, double* dy, long ld, double p, double* qr, void* stream) {

@@ -27,6 +27,8 @@
 // The RHS computes each reaction's rate constants inside the rate loop and
 // scatters rates into formation rates (reaction order) instead of gathering
 // per species; it agrees with the reference to rounding.
+#include <mutex>
+
 #include "lsg_common.cuh"
 #include "lsg_kernels.h"
 
@@ -1141,6 +1143,73 @@ cudaError_t batched_occupancy(const MechLayout& L, bool lu64, int* blocks_per_sm
   e = cudaFuncSetAttribute(batched_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, batched_kernel<float>, kBT, smem);
+}
+
+// ---------------------------------------------------------------------------
+// No-allocation variant.  Some callers cannot allocate device memory when they
+// advance the chemistry: a solver that hands all free device memory to its own
+// pool allocator at start-up, or one that must not let cudaMalloc/cudaFree
+// (which synchronise the device) into its time-step loop.  For them the lane
+// kernel above runs with its slot scratch in this fixed array instead of a
+// context buffer; the number of slots is whatever fits, so any cell count is
+// served (cells are taken from the queue), just with fewer cells in flight.
+//
+// Layout: bytes [0, 256) hold the control words (int queue counter, int error
+// flags), zeroed by every call; the slots start at byte 256.  Every call on a
+// device shares the array and the array keeps the last call's contents, so
+// calls that overlap on the GPU (two streams, two host threads) race: callers
+// serialise them.  Every GPU that loads this part of the library holds the
+// array until the process exits.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[64] = {};
+}  // namespace
+
+// Device address of the scratch array on the current device (set up once per
+// device; host code cannot use the array's name as a device address).
+static cudaError_t noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[device] = p;
+  }
+  *out = (unsigned char*)g_noalloc_ptr[device];
+  return cudaSuccess;
+}
+
+long batched_noalloc_slots(const MechLayout& L, bool lu64, int sm_count) {
+  int bps = 0;
+  if (batched_occupancy(L, lu64, &bps) != cudaSuccess || bps <= 0) return -1;
+  const size_t per_block = batched_slot_doubles(L, lu64) * sizeof(double) * kBT;
+  const long fit = (long)((kNoAllocScratchBytes - 256) / per_block);
+  const long full = (long)sm_count * bps;
+  const long blocks = fit < full ? fit : full;
+  return blocks * kBT;   // 0 when not even one block of slots fits
+}
+
+cudaError_t launch_batched_noalloc(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                                   const StepArgs& a, bool lu64, int device, long nslots, int* host_flags,
+                                   cudaStream_t stream) {
+  if (nslots < kBT) return cudaErrorInvalidValue;
+  unsigned char* base = nullptr;
+  cudaError_t e = noalloc_scratch(device, &base);
+  if (e != cudaSuccess) return e;
+  int* queue = (int*)base;
+  int* err = queue + 1;
+  double* slots = (double*)(base + 256);
+  e = cudaMemsetAsync(base, 0, 256, stream);   // the queue counter and the error flags start at zero
+  if (e != cudaSuccess) return e;
+  e = launch_batched(L, mech_gmem, o, a, slots, nslots, nullptr, queue, lu64, err, stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyAsync(host_flags, err, sizeof(int), cudaMemcpyDeviceToHost, stream);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(stream);
 }
 
 }  // namespace lsg

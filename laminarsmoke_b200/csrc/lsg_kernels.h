@@ -54,6 +54,13 @@ cudaError_t batched_occupancy(const MechLayout& L, bool lu64, int* blocks_per_sm
 cudaError_t launch_batched(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
                            const StepArgs& a, double* slots, long nslots, const int* order, int* queue, bool lu64,
                            int* err, cudaStream_t stream);
+// Fixed device scratch of the no-allocation entry point (lsg_batched.cu).
+constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
+long batched_noalloc_slots(const MechLayout& L, bool lu64, int sm_count);
+cudaError_t launch_batched_noalloc(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                                   const StepArgs& a, bool lu64, int device, long nslots, int* host_flags,
+                                   cudaStream_t stream);
+
 // Round scheme (lsg_rounds.cu): launch geometry chosen once per context.
 struct RoundsPlan {
   bool lu64;

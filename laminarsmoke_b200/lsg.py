@@ -18,14 +18,18 @@ LIB_PATH = os.path.join(HERE, "liblsmoke_gpu.so")
 
 LSG_PRECISION_FP64 = 0
 LSG_PRECISION_MIXED = 1
-LSG_TILE_AUTO, LSG_TILE_WARP, LSG_TILE_LANE = 0, 1, 2
+LSG_TILE_AUTO, LSG_TILE_WARP, LSG_TILE_LANE, LSG_TILE_PERSISTENT = 0, 1, 2, 3
+LSG_ERR_SCRATCH = -8
+NOALLOC_SCRATCH_BYTES = 16 << 20
 NCOUNTERS = 8
 COUNTER_NAMES = ("steps", "rhs", "jacobians", "factorizations", "solves",
                  "error_failures", "convergence_failures", "jacobian_rhs")
 
 
 class LsgError(RuntimeError):
-    pass
+    def __init__(self, msg: str, code: int = 0):
+        super().__init__(msg)
+        self.code = code
 
 
 class Options(C.Structure):
@@ -42,6 +46,7 @@ EXPORTS = (
     "lsg_mech_destroy", "lsg_ctx_create", "lsg_ctx_set_options", "lsg_ctx_destroy",
     "lsg_reaction_step", "lsg_reaction_step_device", "lsg_ctx_check", "lsg_rhs_device",
     "lsg_strerror", "lsg_abi_version", "lsg_ctx_stream", "lsg_ctx_launches",
+    "lsg_reaction_step_device_noalloc",
 )
 
 _lib = None
@@ -73,6 +78,8 @@ def lib():
     L.lsg_abi_version.restype = i
     L.lsg_ctx_stream.argtypes = [vp]
     L.lsg_ctx_stream.restype = vp
+    L.lsg_reaction_step_device_noalloc.argtypes = [vp, C.POINTER(Options), i, i, vp, l, vp, d, d, vp, d, vp,
+                                                   vp, vp, vp, vp]
     L.lsg_ctx_launches.argtypes = [vp]
     L.lsg_ctx_launches.restype = C.c_longlong
     _lib = L
@@ -81,7 +88,7 @@ def lib():
 
 def _check(rc: int, what: str):
     if rc != 0:
-        raise LsgError(f"{what}: {lib().lsg_strerror(rc).decode()} ({rc})")
+        raise LsgError(f"{what}: {lib().lsg_strerror(rc).decode()} ({rc})", rc)
 
 
 def default_options(**kw) -> Options:
@@ -216,3 +223,22 @@ class ReactionStep:
         rc = lib().lsg_ctx_check(self.h, C.byref(f))
         if rc != 0:
             raise LsgError(f"device error flags 0x{f.value:x}: {lib().lsg_strerror(rc).decode()}")
+
+
+def step_device_noalloc(mech: Mechanism, Y, T, dt=1e-5, p: float = 101325.0, t0: float = 0.0,
+                        options: Optional[Options] = None, Q=None, status=None, nsteps=None, counters=None,
+                        stream=None):
+    """lsg_reaction_step_device_noalloc: the reaction step without any device
+    allocation, for callers that cannot allocate while they advance the
+    chemistry (see include/lsmoke_gpu.h).  Same array layout as
+    ReactionStep.step_device; synchronous; calls must not overlap on the GPU."""
+    _require_layout(Y, T, Q, status, nsteps, counters, dt if hasattr(dt, "data_ptr") else None)
+    nc, ld = Y.shape
+    n = T.shape[0]
+    dtp, dts = (None, float(dt)) if not hasattr(dt, "data_ptr") else (dt.data_ptr(), 0.0)
+    opt = None if options is None else C.byref(options)
+    _check(lib().lsg_reaction_step_device_noalloc(
+        mech.h, opt, n, nc, Y.data_ptr(), ld, T.data_ptr(), p, t0, dtp, dts,
+        None if Q is None else Q.data_ptr(), None if status is None else status.data_ptr(),
+        None if nsteps is None else nsteps.data_ptr(), None if counters is None else counters.data_ptr(),
+        _stream_handle(stream)), "lsg_reaction_step_device_noalloc")

@@ -1,0 +1,73 @@
+"""The reaction step that allocates no device memory (lsg_reaction_step_device_noalloc).
+
+Callers such as a CFD solver that hands all free device memory to its own pool
+allocator, or one that keeps cudaMalloc/cudaFree (which synchronise the device)
+out of its time loop, use this entry point.  It runs the persistent lane kernel
+with its work space in a fixed 16 MiB device array, so it must give the same
+cells the same answers as the context-based call of that kernel, call after
+call (the array keeps the previous call's contents), and it must refuse a
+mechanism whose work space does not fit.
+
+This file is collected last on purpose: it runs after every other test.
+"""
+import numpy as np
+import pytest
+
+from laminarsmoke_b200 import cells
+
+pytestmark = pytest.mark.gpu
+
+RTOL_T = 1e-6
+ATOL_Y = 1e-9
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64-lu", "fp32-lu"])
+def test_noalloc_matches_context_call_twice(h2co, cuda, precision):
+    import torch
+    from laminarsmoke_b200 import lsg
+    _, species, A = h2co
+    mech = lsg.Mechanism(h2co[0])
+    # more cells than the fixed array has slots, so slots are reused through the queue
+    n = 12000
+    Y, T = cells.h2co_mixing(species, A["mw"], n, seed=3)
+    Y0 = torch.tensor(np.ascontiguousarray(Y.T), device=cuda)
+    T0 = torch.tensor(T, device=cuda)
+
+    ctx = lsg.ReactionStep(mech, tile=lsg.LSG_TILE_PERSISTENT, precision=precision)
+    Yr, Tr = Y0.clone(), T0.clone()
+    str_ = torch.zeros(n, dtype=torch.int32, device=cuda)
+    nsr = torch.zeros(n, dtype=torch.int32, device=cuda)
+    Qr = torch.zeros(n, dtype=torch.float64, device=cuda)
+    ctx.step_device(Yr, Tr, 1e-5, Q=Qr, status=str_, nsteps=nsr)
+    ctx.check()
+    ctx.close()
+
+    opt = lsg.default_options(precision=precision)
+    for call in range(2):
+        Yn, Tn = Y0.clone(), T0.clone()
+        stn = torch.full((n,), 99, dtype=torch.int32, device=cuda)
+        nsn = torch.zeros(n, dtype=torch.int32, device=cuda)
+        Qn = torch.zeros(n, dtype=torch.float64, device=cuda)
+        lsg.step_device_noalloc(mech, Yn, Tn, 1e-5, options=opt, Q=Qn, status=stn, nsteps=nsn)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(stn.cpu().numpy(), str_.cpu().numpy(), err_msg=f"call {call}")
+        np.testing.assert_array_equal(nsn.cpu().numpy(), nsr.cpu().numpy(), err_msg=f"call {call}")
+        np.testing.assert_allclose(Tn.cpu().numpy(), Tr.cpu().numpy(), rtol=RTOL_T, err_msg=f"call {call}")
+        np.testing.assert_allclose(Yn.cpu().numpy(), Yr.cpu().numpy(), rtol=0, atol=ATOL_Y, err_msg=f"call {call}")
+        np.testing.assert_allclose(Qn.cpu().numpy(), Qr.cpu().numpy(), rtol=1e-9, atol=1e-6, err_msg=f"call {call}")
+    mech.close()
+
+
+def test_noalloc_rejects_mechanism_beyond_scratch(cuda):
+    import torch
+    from laminarsmoke_b200 import lsg, mech as mechs
+    data, species = mechs.load("syn120")
+    mech = lsg.Mechanism(data)
+    n = 64
+    Y = torch.full((len(species), n), 1.0 / len(species), dtype=torch.float64, device=cuda)
+    T = torch.full((n,), 1500.0, dtype=torch.float64, device=cuda)
+    with pytest.raises(lsg.LsgError) as info:
+        lsg.step_device_noalloc(mech, Y, T, 1e-5)
+    assert info.value.code == lsg.LSG_ERR_SCRATCH
+    assert "scratch" in str(info.value)
+    mech.close()

@@ -50,6 +50,8 @@ def parse():
                     help="cells of the CPU baseline sample (0: sized for about 10 s of CPU work)")
     ap.add_argument("--tile", choices=("lane", "persistent"), default="lane",
                     help="batched form: round scheme (lane) or persistent lane kernel")
+    ap.add_argument("--factors", choices=("fp32", "fp64"), default="fp32",
+                    help="batched form: precision of the LU factors")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
@@ -210,10 +212,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     n = Y.shape[0]
     nc = Y.shape[1]
     if args.form == "mixed":
-        tile = lsg.LSG_TILE_LANE if args.tile == "lane" else 3
-        ctx = lsg.ReactionStep(m, tile=tile, precision=lsg.LSG_PRECISION_MIXED)
-        kernel_name = "rounds_*" if args.tile == "lane" else "batched_kernel<float>"
-        dtype = "f64+f32"
+        tile = lsg.LSG_TILE_LANE if args.tile == "lane" else lsg.LSG_TILE_PERSISTENT
+        prec = lsg.LSG_PRECISION_MIXED if args.factors == "fp32" else lsg.LSG_PRECISION_FP64
+        ctx = lsg.ReactionStep(m, tile=tile, precision=prec)
+        kernel_name = "rounds_*" if args.tile == "lane" else "batched_kernel"
+        dtype = "f64+f32" if args.factors == "fp32" else "f64"
     else:
         ctx = plain
         kernel_name, dtype = "plain_warp_kernel", "f64"
@@ -316,7 +319,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                        "ncells_per_gpu": n, "mechanism": "POLIMI_H2CO_1412 (14 species, 33 reactions)",
                        "dt": DT, "t0": 0.0, "p": P_ATM, "rtol": 1e-7, "atol": 1e-12, "form": args.form,
                        "tile": "lane-per-cell" if args.form == "mixed" else "warp-per-cell",
-                       "lu": "fp32 + fp64 Newton residual" if args.form == "mixed" else "fp64",
+                       "lu": ("fp32 factors refined on the fp64 residual" if args.factors == "fp32" else "fp64")
+                             if args.form == "mixed" else "fp64",
                        "l2": "flushed (1 GiB write) between timed steps; inputs restored from HBM copy",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",

@@ -64,8 +64,8 @@ cudaError_t launch_batched_noalloc(const MechLayout& L, const unsigned char* mec
 // Round scheme (lsg_rounds.cu): launch geometry chosen once per context.
 struct RoundsPlan {
   bool lu64;
-  size_t rhs_smem, adv_smem, fac_smem;
-  unsigned g_rhs, g_adv, g_fac, g_cmp, g_init;
+  size_t rhs_smem, adv_smem;
+  unsigned g_rhs, g_adv, g_cmp, g_init;
 };
 size_t rounds_bytes(const MechLayout& L, long ns, bool lu64);
 cudaError_t upload_gear_rounds(const GearConsts& gc);

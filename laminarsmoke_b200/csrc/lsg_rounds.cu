@@ -1,31 +1,31 @@
-// Batched reaction step, round scheme: every cell of the batch is one
-// thread-sized state machine with its whole state in HBM (structure of arrays,
-// [field][cell], so a warp's accesses are coalesced); the step advances in
-// rounds, each a fixed sequence of throughput kernels over the list of cells
+// Batched reaction step, round scheme.  Every cell of the batch keeps its
+// whole solver state in one contiguous record in HBM, and the step advances in
+// rounds, each a fixed sequence of kernels over the list of cells that are
 // still integrating:
 //
-//   rhs       one thread per cell evaluates the RHS the cell asked for
-//             (f(y0), the predictor, a finite-difference Jacobian column, a
-//             Newton iterate, a stabilisation call or the final call at tOut);
-//             mechanism tables staged into shared memory by a bulk copy;
-//   advance   one thread per cell consumes the result and runs the cell's
-//             Gear/BDF solver until its next RHS request, a factorisation
-//             request, or the end of its integration;
-//   factor    one warp per requested factorisation: G = I - h r0 J, partial
-//             pivoting, factors in FP32 (mixed precision) or FP64;
-//   advance   cells that were just factorised continue to their next RHS
-//             request;
-//   compact   the cells that are still integrating form the next round's
-//             list (order-preserving inside each warp).
+//   rhs       one thread per cell evaluates the RHS the cell asked for (f(y0),
+//             the predictor, a finite-difference Jacobian column, a Newton
+//             iterate, a stabilisation call or the final call at tOut): the
+//             reaction loop runs convergent across the warp, with the
+//             mechanism tables staged once per block into shared memory by a
+//             bulk copy;
+//   advance   one warp per cell (lane = ODE component) consumes the result and
+//             runs the cell's Gear/BDF solver to its next RHS request or to
+//             the end of its integration: the record is loaded in one coalesced
+//             pass, every vector operation is lane-parallel, norms are warp
+//             tree reductions; a factorisation of G = I - h r0 J (partial
+//             pivoting, FP32 or FP64) is done by the warp in shared memory and
+//             turned into G^-1 (one column per lane), so every Newton solve is
+//             one matrix-vector product whose broadcasts are independent;
+//   compact   the cells still integrating form the next round's list
+//             (order-preserving inside each warp).
 //
-// Each kernel keeps many warps in flight (little per-cell on-chip state), so the
-// latency of the solver's scattered control flow is hidden by occupancy instead
-// of being paid once per thread.  The method is the one of the plain step --
-// MultiValueSolver.hpp:423-1328, MethodGear.hpp:195-516, KernelDense.hpp:111-193
-// (under solvers/openSMOKEpp4laminarSMOKE/math/native-ode-solvers) -- with the
-// RHS of BatchReactorHomogeneousConstantPressure.H:175-223.  With FP32 factors
-// every linear solve is refined against its FP64 residual (the matrix rebuilt in
-// FP64 from the stored Jacobian) until it equals the FP64 solve to rounding.
+// The method is the one of the plain step -- MultiValueSolver.hpp:423-1328,
+// MethodGear.hpp:195-516, KernelDense.hpp:111-245 (under
+// solvers/openSMOKEpp4laminarSMOKE/math/native-ode-solvers) -- with the RHS of
+// BatchReactorHomogeneousConstantPressure.H:175-223.  With FP32 factors every
+// linear solve is refined against its FP64 residual (the matrix rebuilt in FP64
+// from the stored Jacobian) until it equals the FP64 solve to rounding.
 #include "lsg_common.cuh"
 #include "lsg_kernels.h"
 
@@ -36,10 +36,10 @@ static __constant__ GearConsts c_gear_r;
 namespace {
 
 constexpr int kRT = 128;       // threads per block of the RHS kernel (one cell each)
-constexpr int kAT = 128;       // threads per block of the advance kernel
-constexpr int kFW = 4;         // warps per block of the factor kernel
+constexpr int kWA = 4;         // warps per block of the advance kernel (one cell each)
+constexpr int kAT = 128;       // threads per block of the init kernel
 constexpr int kCT = 256;       // threads per block of the compaction kernel
-constexpr int kRefineR = 2;    // refinement sweeps of a solve with FP32 factors
+constexpr int kRefineR = 1;    // refinement sweeps of a solve with FP32 factors
 
 enum Phase : int {
   PH_DONE = 0,
@@ -50,13 +50,11 @@ enum Phase : int {
   PH_STAB_CONV,  // f(z0) during convergence-failure recovery
   PH_STAB_ERR,   // f(z0) after an error-test failure
   PH_FINAL,      // f(y(tOut)) -> QR
-  PH_FACT,       // waiting for the factorisation of G
-  PH_FACTORED,   // factorised, continue after FindCorrection's factorisation
 };
 
 __device__ __forceinline__ bool rhs_phase(int ph) { return ph >= PH_INIT && ph <= PH_FINAL; }
 
-// scalar state of a cell: doubles [D_*][ns], ints [I_*][ns]
+// scalar state of a cell: doubles D_* at the record start, ints I_* after them
 enum : int {
   D_T = 0, D_T0, D_TOUT, D_TMESH, D_TSTAB, D_H, D_HNEXT, D_HNORD, D_HSCALE, D_HSCALEMAX,
   D_A24, D_A25, D_QR, D_OLDCC, D_HF, D_HJ, D_PENDHS, D_HR0, ND_
@@ -66,6 +64,34 @@ enum : int {
   I_CONVOK, I_NSTEPS, I_ITCONV, I_ITCONVRATE, I_ITCONVFAIL, I_ITERRFAIL, I_NCFOM, I_STEPLASTJ, I_ITCONST,
   I_ITMINORD, I_FIXEDMIN, I_NEWTONK, I_JCOL, I_MAXORD, I_CNT0, NI_ = I_CNT0 + NCNT
 };
+
+// Record of one cell (offsets in doubles from the record start; RS doubles per
+// record, a multiple of 32 so records start on 256-byte boundaries):
+//   [0, ND_)            scalar doubles
+//   [ND_, ND_ + NI_/2)  scalar ints
+//   oz   z[8][n]  Nordsieck array      ov   v[8][n]
+//   ob, of, of0, ova, ovb, oeps         n each
+//   ojac J[n][n] float (row major)      oinv G^-1[n][n] LUT (row major)
+struct RecLayout {
+  int oz, ov, ob, of, of0, ova, ovb, oeps, ojac, oinv, RS;
+};
+
+__host__ __device__ inline RecLayout rec_layout(int n, bool lu64) {
+  RecLayout r{};
+  int o = ND_ + NI_ / 2;
+  r.oz = o; o += 8 * n;
+  r.ov = o; o += 8 * n;
+  r.ob = o; o += n;
+  r.of = o; o += n;
+  r.of0 = o; o += n;
+  r.ova = o; o += n;
+  r.ovb = o; o += n;
+  r.oeps = o; o += n;
+  r.ojac = o; o += (n * n + 1) / 2;
+  r.oinv = o; o += lu64 ? n * n : (n * n + 1) / 2;
+  r.RS = (o + 31) & ~31;
+  return r;
+}
 
 __device__ __forceinline__ double contrib_r(double nu, double v) {
   if (nu == 1.) return v;
@@ -265,157 +291,32 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
   return QR;
 }
 
-// ---------------------------------------------------------------------------
-// Per-cell vector helpers.  Pointers address element 0 of a cell's vector;
-// element k is at [k * ns].  __restrict__ lets each loop keep all its loads in
-// flight at once (the vectors never overlap).
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double wrms_r(const double* __restrict__ x, const double* __restrict__ e, int n, long ns) {
-  double s = 0.;
-#pragma unroll 4
-  for (int k = 0; k < n; ++k) {
-    const double c = x[k * ns] * e[k * ns];
-    s += c * c;
-  }
-  return sqrt(s / double(n));
-}
 
-__device__ __forceinline__ void set_eps_r(const double* __restrict__ w, double* __restrict__ e, int n, long ns,
-                                        double atol, double rtol) {
-#pragma unroll 4
-  for (int k = 0; k < n; ++k) e[k * ns] = 1. / (atol + rtol * fabs(w[k * ns]));
-}
-
-// DriverStep rescale of z[1..p] and CheckConstraints(z0) (MultiValueSolver.hpp:780-797)
-__device__ __forceinline__ void rescale_z_r(double* __restrict__ z, int n, long ns, unsigned p, double hScale, int NC,
-                                          double yminT, double ymaxT) {
-  double hr = 1.;
-  for (unsigned i = 1; i <= p; ++i) {
-    hr *= hScale;
-    double* zi = z + (long)i * n * ns;
-#pragma unroll 4
-    for (int k = 0; k < n; ++k) zi[k * ns] *= hr;
-  }
-#pragma unroll 4
-  for (int k = 0; k < n; ++k) {
-    double z0 = z[k * ns];
-    const double lo = lo_b(k, NC, yminT), hi = hi_b(k, NC, ymaxT);
-    if (z0 < lo) z0 = lo;
-    if (z0 > hi) z0 = hi;
-    z[k * ns] = z0;
-  }
-}
-
-// MultiValueStep prediction v = D z with min/max handling (MultiValueSolver.hpp:1214-1262) and
-// FindCorrection's vb = CheckConstraints(v0) (MethodGear.hpp:198-202)
-__device__ __forceinline__ void predict_r(const double* __restrict__ z, double* __restrict__ v,
-                                        double* __restrict__ vb, const double* __restrict__ e, int n, long ns,
-                                        unsigned p, int NC, double yminT, double ymaxT) {
-  for (int k = 0; k < n; ++k) {
-    double w[8];
+// Warp tree sum (every lane receives the total).
+__device__ __forceinline__ double wsum(double v) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) w[i] = (i <= (int)p) ? z[((long)i * n + k) * ns] : 0.;
-#pragma unroll
-    for (int i = 0; i < 7; ++i)
-#pragma unroll
-      for (int j = 6; j >= 0; --j)
-        if (i < (int)p && j >= i && j <= (int)p - 1) w[j] += w[j + 1];
-    const double lo = lo_b(k, NC, yminT), hi = hi_b(k, NC, ymaxT);
-    const double ek = e[k * ns];
-    const double z0 = z[k * ns];
-    if (w[0] < lo && fabs(w[0] - lo) * ek < double(n)) {
-      w[1] = lo - z0;
-      w[0] = lo;
-#pragma unroll
-      for (int i = 2; i < 8; ++i) w[i] = 0.;
-    }
-    if (w[0] > hi && fabs(w[0] - hi) * ek < double(n)) {
-      w[1] = hi - z0;
-      w[0] = hi;
-#pragma unroll
-      for (int i = 2; i < 8; ++i) w[i] = 0.;
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-      if (i <= (int)p) v[((long)i * n + k) * ns] = w[i];
-    double b = w[0];
-    if (b < lo) b = lo;
-    if (b > hi) b = hi;
-    vb[k * ns] = b;
-  }
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+  return v;
 }
 
-
-// Forward and back substitution with factors of P G = L U (row-permuted right
-// hand side already in x); column-oriented as KernelDense::SolveLinearSystem.
-// x: this thread's vector in shared memory, element k at x[k * kAT].
-template <typename LUT>
-__device__ __forceinline__ void lu_fwd_bwd(double* __restrict__ x, const LUT* __restrict__ lu, int n, long ns) {
-  for (int j = 0; j < n; ++j) {
-    const double xj = x[j * kAT];
-#pragma unroll 4
-    for (int i = j + 1; i < n; ++i) x[i * kAT] -= (double)lu[(long)(i * n + j) * ns] * xj;
-  }
-  for (int j = n - 1; j >= 0; --j) {
-    const double xj = x[j * kAT] / (double)lu[(long)(j * n + j) * ns];
-    x[j * kAT] = xj;
-#pragma unroll 4
-    for (int i = 0; i < j; ++i) x[i * kAT] -= (double)lu[(long)(i * n + j) * ns] * xj;
-  }
+// a[i] for a runtime index 0 <= i < 8 without local-memory indexing
+__device__ __forceinline__ double get8(const double (&a)[8], unsigned i) {
+  double r = a[0];
+#pragma unroll
+  for (unsigned k = 1; k < 8; ++k)
+    if (i == k) r = a[k];
+  return r;
+}
+__device__ __forceinline__ void set8(double (&a)[8], unsigned i, double x) {
+#pragma unroll
+  for (unsigned k = 0; k < 8; ++k)
+    if (i == k) a[k] = x;
 }
 
-// x <- G^-1 r for the cell's last factorisation (r in global memory, natural
-// order; perm maps factor rows to rows of G).  FP32 factors: kRefineR sweeps of
-// iterative refinement on the FP64 residual r - (I - hr0 J) x.  d: second
-// shared-memory vector, tmp: global scratch vector.
-template <typename LUT>
-__device__ __forceinline__ void lin_solve_r(double* __restrict__ x, double* __restrict__ d,
-                                            const double* __restrict__ r, const LUT* __restrict__ lu,
-                                            const int* __restrict__ perm, const float* __restrict__ jac,
-                                            double* __restrict__ tmp, double hr0, int n, long ns) {
-#pragma unroll 4
-  for (int k = 0; k < n; ++k) x[k * kAT] = r[(long)perm[k * ns] * ns];
-  lu_fwd_bwd<LUT>(x, lu, n, ns);
-  if (sizeof(LUT) == sizeof(float)) {
-    for (int it = 0; it < kRefineR; ++it) {
-      for (int i = 0; i < n; ++i) {
-        double s = 0.;
-#pragma unroll 4
-        for (int j = 0; j < n; ++j) s += (double)jac[(long)(i * n + j) * ns] * x[j * kAT];
-        tmp[i * ns] = r[i * ns] - (x[i * kAT] - hr0 * s);
-      }
-#pragma unroll 4
-      for (int k = 0; k < n; ++k) d[k * kAT] = tmp[(long)perm[k * ns] * ns];
-      lu_fwd_bwd<LUT>(d, lu, n, ns);
-#pragma unroll 4
-      for (int k = 0; k < n; ++k) x[k * kAT] += d[k * kAT];
-    }
-  }
-}
-
-__device__ __forceinline__ void copy_r(const double* __restrict__ s, double* __restrict__ d, int n, long ns) {
-#pragma unroll 4
-  for (int k = 0; k < n; ++k) d[k * ns] = s[k * ns];
-}
-
-// Buffers of the round scheme (all [field][ns], ns = capacity).
+// Buffers of the round scheme.
 struct RoundBufs {
-  long ns;
-  double* sd;       // [ND_] scalar state
-  int* si;          // [NI_] scalar state
-  double* z;        // [8n] Nordsieck array
-  double* v;        // [8n] predicted / corrected array
-  double* b;
-  double* f;
-  double* f0;
-  double* va;
-  double* vb;
-  double* eps;
-  double* r;        // right-hand side of the current linear solve
-  double* tmp;      // refinement residual
-  float* jac;       // [n*n] finite-difference Jacobian
-  void* lu;         // [n*n] factors (float or double)
-  int* perm;        // [n] row permutation of the factors
+  double* rec;      // [capacity][RS] cell records
+  RecLayout L;
   int* act0;        // active lists (round parity 0 / 1)
   int* act1;
   int* nact;        // [2] list lengths
@@ -428,7 +329,6 @@ struct RoundBufs {
 // (MultiValueSolver.hpp:367-420); cells at or below tmin_chem finish here.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kAT) rounds_init_kernel(int NC, StepOptions o, StepArgs a, RoundBufs B) {
-  const long ns = B.ns;
   const int n = NC + 1;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     B.nact[0] = (int)a.ncells;
@@ -437,8 +337,8 @@ __global__ void __launch_bounds__(kAT) rounds_init_kernel(int NC, StepOptions o,
   for (long cell = (long)blockIdx.x * blockDim.x + threadIdx.x; cell < a.ncells;
        cell += (long)gridDim.x * blockDim.x) {
     B.act0[cell] = (int)cell;
-    int* si = B.si + cell;
-    double* sd = B.sd + cell;
+    double* R = B.rec + cell * B.L.RS;
+    int* RI = (int*)(R + ND_);
     const double Tc = a.T[cell];
     if (!(Tc > o.tmin_chem)) {
       double s = 0.;
@@ -447,34 +347,33 @@ __global__ void __launch_bounds__(kAT) rounds_init_kernel(int NC, StepOptions o,
       if (a.status) a.status[cell] = 0;
       if (a.nsteps) a.nsteps[cell] = 0;
       if (a.counters)
-        for (int k = 0; k < NCNT; ++k) a.counters[(long)cell * NCNT + k] = 0;
-      si[I_PHASE * ns] = PH_DONE;
+        for (int k = 0; k < NCNT; ++k) a.counters[cell * NCNT + k] = 0;
+      RI[I_PHASE] = PH_DONE;
       continue;
     }
-    double* va = B.va + cell;
+    double* va = R + B.L.ova;
     double s = 0.;
     for (int i = 0; i < NC; ++i) {
       double yi = a.Y[(long)i * a.ld + cell];
       if (yi < 0.) yi = 0.;
-      va[i * ns] = yi;
+      va[i] = yi;
       s += yi;
     }
-    for (int i = 0; i < NC; ++i) va[i * ns] /= s;
-    va[NC * ns] = Tc;
+    for (int i = 0; i < NC; ++i) va[i] /= s;
+    va[NC] = Tc;
     const double t0 = a.t0;
-    sd[D_T * ns] = t0; sd[D_T0 * ns] = t0; sd[D_TOUT * ns] = t0; sd[D_TMESH * ns] = t0; sd[D_TSTAB * ns] = t0;
-    sd[D_H * ns] = 0.; sd[D_HNEXT * ns] = 0.; sd[D_HNORD * ns] = 0.; sd[D_HSCALE * ns] = 0.;
-    sd[D_HSCALEMAX * ns] = 1000.; sd[D_A24 * ns] = o.alfa2_4; sd[D_A25 * ns] = o.alfa2_5; sd[D_QR * ns] = 0.;
-    sd[D_OLDCC * ns] = 0.; sd[D_HF * ns] = 0.; sd[D_HJ * ns] = 0.; sd[D_PENDHS * ns] = 0.; sd[D_HR0 * ns] = 0.;
+    R[D_T] = t0; R[D_T0] = t0; R[D_TOUT] = t0; R[D_TMESH] = t0; R[D_TSTAB] = t0;
+    R[D_H] = 0.; R[D_HNEXT] = 0.; R[D_HNORD] = 0.; R[D_HSCALE] = 0.; R[D_HSCALEMAX] = 1000.;
+    R[D_A24] = o.alfa2_4; R[D_A25] = o.alfa2_5; R[D_QR] = 0.; R[D_OLDCC] = 0.; R[D_HF] = 0.; R[D_HJ] = 0.;
+    R[D_PENDHS] = 0.; R[D_HR0] = 0.;
     unsigned mij = 20u + 5u * (unsigned)(n - 3);
     if (mij > 50u && n < 80) mij = 50u;
-    si[I_PHASE * ns] = PH_INIT; si[I_STATUS * ns] = 1; si[I_P * ns] = 1; si[I_ITORDER * ns] = 0;
-    si[I_ORDNEXT * ns] = 1; si[I_MAXITJ * ns] = (int)mij; si[I_HSTAT * ns] = 1; si[I_OSTAT * ns] = 1;
-    si[I_FACTORIZED * ns] = 0; si[I_JACCHANGE * ns] = 1; si[I_CONVOK * ns] = 1; si[I_NSTEPS * ns] = 0;
-    si[I_ITCONV * ns] = 0; si[I_ITCONVRATE * ns] = 0; si[I_ITCONVFAIL * ns] = 0; si[I_ITERRFAIL * ns] = 0;
-    si[I_NCFOM * ns] = 0; si[I_STEPLASTJ * ns] = 0; si[I_ITCONST * ns] = 0; si[I_ITMINORD * ns] = 0;
-    si[I_FIXEDMIN * ns] = 0; si[I_NEWTONK * ns] = 0; si[I_JCOL * ns] = 0; si[I_MAXORD * ns] = o.maximum_order;
-    for (int k = 0; k < NCNT; ++k) si[(I_CNT0 + k) * ns] = 0;
+    RI[I_PHASE] = PH_INIT; RI[I_STATUS] = 1; RI[I_P] = 1; RI[I_ITORDER] = 0; RI[I_ORDNEXT] = 1;
+    RI[I_MAXITJ] = (int)mij; RI[I_HSTAT] = 1; RI[I_OSTAT] = 1; RI[I_FACTORIZED] = 0; RI[I_JACCHANGE] = 1;
+    RI[I_CONVOK] = 1; RI[I_NSTEPS] = 0; RI[I_ITCONV] = 0; RI[I_ITCONVRATE] = 0; RI[I_ITCONVFAIL] = 0;
+    RI[I_ITERRFAIL] = 0; RI[I_NCFOM] = 0; RI[I_STEPLASTJ] = 0; RI[I_ITCONST] = 0; RI[I_ITMINORD] = 0;
+    RI[I_FIXEDMIN] = 0; RI[I_NEWTONK] = 0; RI[I_JCOL] = 0; RI[I_MAXORD] = o.maximum_order;
+    for (int k = 0; k < NCNT; ++k) RI[I_CNT0 + k] = 0;
   }
 }
 
@@ -492,99 +391,233 @@ __global__ void __launch_bounds__(kRT) rounds_rhs_kernel(MechLayout Lp, const un
   const double* Md = (const double*)smem;
   const int* Mi = (const int*)(smem + (size_t)Lp.n_double * sizeof(double));
   double* scratch = (double*)(smem + ((Lp.bytes + 15u) & ~15u));
-  const long ns = B.ns;
+  const RecLayout RL = B.L;
   const int nact = B.nact[par];
   const int* act = par ? B.act1 : B.act0;
   for (int idx = blockIdx.x * kRT + threadIdx.x; idx < nact; idx += gridDim.x * kRT) {
     const int cell = act[idx];
-    int* si = B.si + cell;
-    const int ph = si[I_PHASE * ns];
+    double* R = B.rec + (long)cell * RL.RS;
+    int* RI = (int*)(R + ND_);
+    const int ph = RI[I_PHASE];
     if (!rhs_phase(ph)) continue;
-    const double* src = B.va + cell;
-    double* dst = B.f + cell;
+    const double* src = R + RL.ova;
+    double* dst = R + RL.of;
     int pj = -1;
     double pval = 0.;
     if (ph == PH_PRED) {
-      src = B.vb + cell;
-      dst = B.f0 + cell;
+      src = R + RL.ovb;
+      dst = R + RL.of0;
     } else if (ph == PH_JAC) {
-      src = B.vb + cell;
-      pj = si[I_JCOL * ns];
-      pval = src[(long)pj * ns] + B.sd[D_HJ * ns + cell];
+      src = R + RL.ovb;
+      pj = RI[I_JCOL];
+      pval = src[pj] + R[D_HJ];
     } else if (ph == PH_STAB_CONV || ph == PH_STAB_ERR) {
-      src = B.z + cell;
+      src = R + RL.oz;
     }
-    const double QR = rhs_cell(&sL, Md, Mi, scratch, src, ns, pj, pval, dst, P0, energy);
-    B.sd[D_QR * ns + cell] = QR;
+    R[D_QR] = rhs_cell(&sL, Md, Mi, scratch, src, 1, pj, pval, dst, P0, energy);
     const int ck = (ph == PH_JAC) ? CNT_JAC_RHS : CNT_RHS;
-    si[(I_CNT0 + ck) * ns] += 1;
+    RI[I_CNT0 + ck] += 1;
   }
 }
 
 // ---------------------------------------------------------------------------
-// advance: consume the RHS result (mode 0) or the fresh factorisation (mode 1)
-// and run the cell's solver to its next request.
+// advance: one warp per listed cell; lane k holds component k of every
+// vector.  Consumes the RHS result and runs the solver to its next request.
 // ---------------------------------------------------------------------------
-template <typename LUT>
-__global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions o, StepArgs a, RoundBufs B, int par,
-                                                              int mode) {
-  extern __shared__ double sxd[];   // this thread's two solve vectors, element k at [k * kAT]
-  const long ns = B.ns;
-  const int n = NC + 1;
-  double* const x = sxd + threadIdx.x;
-  double* const dd = sxd + n * kAT + threadIdx.x;
+template <typename LUT, int NM>
+__global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, StepOptions o, StepArgs a, RoundBufs B,
+                                                                      int par) {
+  extern __shared__ __align__(16) unsigned char wsm[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int n = NC + 1, ld = n + 1;
+  const RecLayout RL = B.L;
+  // per-warp shared memory: factors G[n][ld] and inverse X[n][ld] (LUT), Jacobian J[n][ld] (float),
+  // permutation [32]
+  LUT* Gs = (LUT*)wsm + (size_t)w * n * ld;
+  LUT* Xs = (LUT*)wsm + (size_t)kWA * n * ld + (size_t)w * n * ld;
+  float* Js = (float*)((LUT*)wsm + (size_t)2 * kWA * n * ld) + (size_t)w * n * ld;
+  int* Ps = (int*)((float*)((LUT*)wsm + (size_t)2 * kWA * n * ld) + (size_t)kWA * n * ld) + w * 32;
+  const bool al = lane < n;
+  const double lo = lane < NC ? 0. : o.y_min_T, hi = lane < NC ? 1. : o.y_max_T;
   const int nact = B.nact[par];
   const int* act = par ? B.act1 : B.act0;
-  const double yminT = o.y_min_T, ymaxT = o.y_max_T;
-  for (int idx = blockIdx.x * kAT + threadIdx.x; idx < nact; idx += gridDim.x * kAT) {
-    const int cell = act[idx];
-    int* si = B.si + cell;
-    double* sd = B.sd + cell;
-    int phase = si[I_PHASE * ns];
-    if (mode == 0 ? !rhs_phase(phase) : phase != PH_FACTORED) continue;
-    double* const pz = B.z + cell;
-    double* const pv = B.v + cell;
-    double* const pb = B.b + cell;
-    double* const pf = B.f + cell;
-    double* const pf0 = B.f0 + cell;
-    double* const pva = B.va + cell;
-    double* const pvb = B.vb + cell;
-    double* const peps = B.eps + cell;
-    double* const pr = B.r + cell;
-    double* const ptmp = B.tmp + cell;
-    float* const pjac = B.jac + cell;
-    const LUT* const plu = (const LUT*)B.lu + cell;
-    const int* const pperm = B.perm + cell;
-    // ---- the cell's scalar state ----
-    double t = sd[D_T * ns];
-    const double t0 = sd[D_T0 * ns];
-    double tOut = sd[D_TOUT * ns], tInMeshPoint = sd[D_TMESH * ns];
-    double tStabilize = sd[D_TSTAB * ns], h = sd[D_H * ns], hNextStep = sd[D_HNEXT * ns];
-    double hNordsieck = sd[D_HNORD * ns], hScale = sd[D_HSCALE * ns], hScaleMax = sd[D_HSCALEMAX * ns];
-    double alfa2_4 = sd[D_A24 * ns], alfa2_5 = sd[D_A25 * ns], oldCC = sd[D_OLDCC * ns];
-    const double QR = sd[D_QR * ns];
-    double hf = sd[D_HF * ns], hJ = sd[D_HJ * ns], pendHScale = sd[D_PENDHS * ns], hr0f = sd[D_HR0 * ns];
-    int status = si[I_STATUS * ns];
-    unsigned p = si[I_P * ns], iterOrder = si[I_ITORDER * ns], orderInNextStep = si[I_ORDNEXT * ns];
-    const unsigned maxIterationsJacobian = si[I_MAXITJ * ns];
-    int odeHStatus = si[I_HSTAT * ns], odeOrderStatus = si[I_OSTAT * ns], factorized = si[I_FACTORIZED * ns];
-    int jacobianChange = si[I_JACCHANGE * ns], convOK = si[I_CONVOK * ns];
-    unsigned numberOfSteps = si[I_NSTEPS * ns], iterConvergence = si[I_ITCONV * ns];
-    unsigned iterConvergenceRate = si[I_ITCONVRATE * ns], iterConvergenceFailure = si[I_ITCONVFAIL * ns];
-    unsigned iterErrorFailure = si[I_ITERRFAIL * ns], nConvFailOrderMax = si[I_NCFOM * ns];
-    unsigned stepOfLastJacobian = si[I_STEPLASTJ * ns], iterConstSteps = si[I_ITCONST * ns];
-    unsigned iterMinimumOrder = si[I_ITMINORD * ns];
-    bool fixedOrderMin = si[I_FIXEDMIN * ns] != 0;
-    unsigned newtonK = si[I_NEWTONK * ns];
-    int jcol = si[I_JCOL * ns];
-    unsigned maximum_order = si[I_MAXORD * ns];
+  for (int widx = blockIdx.x * kWA + w; widx < nact; widx += gridDim.x * kWA) {
+    const int cell = act[widx];
+    double* R = B.rec + (long)cell * RL.RS;
+    int* RI = (int*)(R + ND_);
+    int phase = RI[I_PHASE];
+    if (!rhs_phase(phase)) continue;   // same in all lanes
+    // ---- scalar state (every lane reads the same words) ----
+    double t = R[D_T];
+    const double t0 = R[D_T0];
+    double tOut = R[D_TOUT], tInMeshPoint = R[D_TMESH], tStabilize = R[D_TSTAB], h = R[D_H];
+    double hNextStep = R[D_HNEXT], hNordsieck = R[D_HNORD], hScale = R[D_HSCALE], hScaleMax = R[D_HSCALEMAX];
+    double alfa2_4 = R[D_A24], alfa2_5 = R[D_A25], oldCC = R[D_OLDCC];
+    const double QR = R[D_QR];
+    double hf = R[D_HF], hJ = R[D_HJ], pendHScale = R[D_PENDHS], hr0f = R[D_HR0];
+    int status = RI[I_STATUS];
+    unsigned p = RI[I_P], iterOrder = RI[I_ITORDER], orderInNextStep = RI[I_ORDNEXT];
+    const unsigned maxIterationsJacobian = RI[I_MAXITJ];
+    int odeHStatus = RI[I_HSTAT], odeOrderStatus = RI[I_OSTAT], factorized = RI[I_FACTORIZED];
+    int jacobianChange = RI[I_JACCHANGE], convOK = RI[I_CONVOK];
+    unsigned numberOfSteps = RI[I_NSTEPS], iterConvergence = RI[I_ITCONV];
+    unsigned iterConvergenceRate = RI[I_ITCONVRATE], iterConvergenceFailure = RI[I_ITCONVFAIL];
+    unsigned iterErrorFailure = RI[I_ITERRFAIL], nConvFailOrderMax = RI[I_NCFOM];
+    unsigned stepOfLastJacobian = RI[I_STEPLASTJ], iterConstSteps = RI[I_ITCONST];
+    unsigned iterMinimumOrder = RI[I_ITMINORD];
+    bool fixedOrderMin = RI[I_FIXEDMIN] != 0;
+    unsigned newtonK = RI[I_NEWTONK];
+    int jcol = RI[I_JCOL];
+    unsigned maximum_order = RI[I_MAXORD];
     int cstep = 0, csolve = 0, cjac = 0, cfact = 0, cerr = 0, cconv = 0;
+    // ---- vectors, one component per lane ----
+    double z[8], v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      z[i] = al ? R[RL.oz + i * n + lane] : 0.;
+      v[i] = al ? R[RL.ov + i * n + lane] : 0.;
+    }
+    double b = al ? R[RL.ob + lane] : 0., f = al ? R[RL.of + lane] : 0., f0 = al ? R[RL.of0 + lane] : 0.;
+    double va = al ? R[RL.ova + lane] : 0., vb = al ? R[RL.ovb + lane] : 0., eps = al ? R[RL.oeps + lane] : 0.;
+    double x = 0.;                 // latest Newton correction
+    bool dz = false, dv = false;   // z / v modified
+    bool j_in = false, inv_in = false;
+    float* const Jg = (float*)(R + RL.ojac);
+    LUT* const Ig = (LUT*)(R + RL.oinv);
 
     enum : int { H_DEC = 0, H_CONST = 1, H_INC = 2 };
     enum : int { O_DEC = 0, O_CONST = 1, O_INC = 2 };
     auto alfa2 = [&](unsigned k) { return k == 4 ? alfa2_4 : (k == 5 ? alfa2_5 : .8); };
-    auto Zp = [&](unsigned i) { return pz + (long)i * n * ns; };
-    auto Vp = [&](unsigned i) { return pv + (long)i * n * ns; };
+    auto wrms = [&](double xv) {   // OpenSMOKEUtilities.hpp:689-701 (tree-ordered sum)
+      const double c = al ? xv * eps : 0.;
+      return sqrt(wsum(c * c) / double(n));
+    };
+    auto clamp = [&](double y) {
+      if (al) {
+        if (y < lo) y = lo;
+        if (y > hi) y = hi;
+      }
+      return y;
+    };
+    auto load_j = [&]() {   // this cell's Jacobian rows into shared memory
+      if (!j_in) {
+        if (al)
+          for (int j = 0; j < n; ++j) Js[lane * ld + j] = Jg[lane * n + j];
+        __syncwarp();
+        j_in = true;
+      }
+    };
+    auto load_inv = [&]() {
+      if (!inv_in) {
+        if (al)
+          for (int j = 0; j < n; ++j) Xs[lane * ld + j] = Ig[lane * n + j];
+        __syncwarp();
+        inv_in = true;
+      }
+    };
+    // sum_j M[lane][j] * y_j (M row-major in shared memory, leading dimension ld);
+    // the broadcasts do not depend on each other
+    auto rowdot = [&](const auto* M, double y) {
+      double s0 = 0., s1 = 0.;
+      for (int j = 0; j + 1 < n; j += 2) {
+        const double y0 = __shfl_sync(kFull, y, j);
+        const double y1 = __shfl_sync(kFull, y, j + 1);
+        if (al) {
+          s0 += (double)M[lane * ld + j] * y0;
+          s1 += (double)M[lane * ld + j + 1] * y1;
+        }
+      }
+      if (n & 1) {
+        const double y0 = __shfl_sync(kFull, y, n - 1);
+        if (al) s0 += (double)M[lane * ld + n - 1] * y0;
+      }
+      return s0 + s1;
+    };
+    // x = G^-1 rhs; with FP32 factors one refinement sweep on the FP64 residual
+    // rhs - (x - hr0 J x), the matrix rebuilt in FP64 from the stored Jacobian
+    auto solve = [&](double rhs) {
+      load_inv();
+      double xv = rowdot(Xs, rhs);
+      if (sizeof(LUT) == sizeof(float)) {
+        load_j();
+        for (int it = 0; it < kRefineR; ++it) {
+          const double s = rowdot(Js, xv);
+          const double res = al ? rhs - (xv - hr0f * s) : 0.;
+          xv += rowdot(Xs, res);
+        }
+      }
+      if (!al) xv = 0.;
+      ++csolve;
+      return xv;
+    };
+    // G = I - hr0 J, partial pivoting on the largest magnitude, first occurrence
+    // (KernelDense::BuildAndFactorizeMatrixG), rows swapped whole: P G = L U;
+    // then G^-1 = U^-1 L^-1 P, lane c solving for column c.
+    auto factorize = [&]() {
+      load_j();
+      if (al)
+        for (int j = 0; j < n; ++j) {
+          double g = -hr0f * (double)Js[lane * ld + j];
+          if (j == lane) g += 1.;
+          Gs[lane * ld + j] = (LUT)g;
+        }
+      Ps[lane] = lane;
+      __syncwarp();
+      for (int k = 0; k < n; ++k) {
+        LUT vv = (lane >= k && lane < n) ? (LUT)fabs((double)Gs[lane * ld + k]) : (LUT)-1;
+        int r = lane;
+        for (int off = 16; off > 0; off >>= 1) {
+          const LUT ov = __shfl_xor_sync(kFull, vv, off);
+          const int orr = __shfl_xor_sync(kFull, r, off);
+          if (ov > vv || (ov == vv && orr < r)) { vv = ov; r = orr; }
+        }
+        r = __shfl_sync(kFull, r, 0);
+        if (r < k || r >= n) r = k;   // a NaN column cannot send the pivot outside rows k..n-1
+        if (r != k) {
+          if (al) {
+            const LUT tmp = Gs[k * ld + lane];
+            Gs[k * ld + lane] = Gs[r * ld + lane];
+            Gs[r * ld + lane] = tmp;
+          }
+          if (lane == 0) {
+            const int tp = Ps[k];
+            Ps[k] = Ps[r];
+            Ps[r] = tp;
+          }
+        }
+        __syncwarp();
+        const LUT dg = Gs[k * ld + k];
+        if (lane > k && lane < n) {
+          LUT l = Gs[lane * ld + k];
+          if (dg != (LUT)0) l /= dg;
+          Gs[lane * ld + k] = l;
+          for (int j = k + 1; j < n; ++j) Gs[lane * ld + j] -= l * Gs[k * ld + j];
+        }
+        __syncwarp();
+      }
+      if (al) {
+        const int c = lane;
+        for (int k = 0; k < n; ++k) Xs[k * ld + c] = (Ps[k] == c) ? (LUT)1 : (LUT)0;
+        for (int j = 0; j < n; ++j) {
+          const LUT xj = Xs[j * ld + c];
+          for (int i = j + 1; i < n; ++i) Xs[i * ld + c] -= Gs[i * ld + j] * xj;
+        }
+        for (int j = n - 1; j >= 0; --j) {
+          const LUT xj = Xs[j * ld + c] / Gs[j * ld + j];
+          Xs[j * ld + c] = xj;
+          for (int i = 0; i < j; ++i) Xs[i * ld + c] -= Gs[i * ld + j] * xj;
+        }
+      }
+      __syncwarp();
+      if (al)
+        for (int j = 0; j < n; ++j) Ig[lane * n + j] = Xs[lane * ld + j];
+      inv_in = true;
+      ++cfact;
+    };
+    auto fail_keep_z = [&](int st) {
+      status = st;
+      va = z[0];
+    };
 
     enum : int { L_NONE, L_START_STEP, L_DRIVER_LOOP, L_JAC_COLUMN, L_AFTER_JAC, L_AFTER_FACT, L_NEWTON_TEST,
                  L_CORR_DONE, L_FINISH };
@@ -592,27 +625,21 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
     switch (phase) {
       case PH_INIT: {
         // MultiValueSolver::Solve, first call (:445-469)
-        bool illegal = false;
-        for (int k = 0; k < n; ++k) {
-          const double yk = pva[k * ns];
-          if (yk < lo_b(k, NC, yminT) || yk > hi_b(k, NC, ymaxT)) illegal = true;
-        }
-        if (illegal) { status = -9; lab = L_FINISH; break; }
-        set_eps_r(pva, peps, n, ns, o.atol, o.rtol);
-        double lo, hi;
-        if (t0 != 0.) { lo = 100. * kMachEpsDouble * fabs(t0); hi = fabs(t0); }
-        else { lo = kMachEpsDouble; hi = 1.e-4; }
-        double h0 = 0.5 / (wrms_r(pf, peps, n, ns) + kMachEpsFloat);
-        if (h0 < lo) h0 = lo;
-        if (h0 > hi) h0 = hi;
+        const bool illegal = al && (va < lo || va > hi);
+        if (__any_sync(kFull, illegal)) { status = -9; lab = L_FINISH; break; }
+        eps = al ? 1. / (o.atol + o.rtol * fabs(va)) : 0.;
+        double lo0, hi0;
+        if (t0 != 0.) { lo0 = 100. * kMachEpsDouble * fabs(t0); hi0 = fabs(t0); }
+        else { lo0 = kMachEpsDouble; hi0 = 1.e-4; }
+        double h0 = 0.5 / (wrms(f) + kMachEpsFloat);
+        if (h0 < lo0) h0 = lo0;
+        if (h0 > hi0) h0 = hi0;
         const double dtc = a.dt ? a.dt[cell] : a.dt_scalar;
         tOut = t0 + dtc;
         h0 *= fabs(tOut - t0) / (tOut - t0);
-        double* z1 = Zp(1);
-        for (int k = 0; k < n; ++k) {
-          pz[k * ns] = pva[k * ns];
-          z1[k * ns] = pf[k * ns] * h0;
-        }
+        z[0] = va;
+        z[1] = f * h0;
+        dz = true;
         hNordsieck = h0; hNextStep = h0;
         status = 2;
         lab = L_START_STEP;
@@ -624,7 +651,7 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
         if (jacobianChange) {
           stepOfLastJacobian = numberOfSteps;
           jacobianChange = 0;
-          hf = 1.e+3 * kMachEpsDouble * fabs(h) * wrms_r(pf0, peps, n, ns) * double(n);
+          hf = 1.e+3 * kMachEpsDouble * fabs(h) * wrms(f0) * double(n);
           if (hf < 1.e-10) hf = 1.;
           jcol = 0;
           lab = L_JAC_COLUMN;
@@ -635,8 +662,7 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
       }
       case PH_JAC: {
         const double hInv = 1. / hJ;
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) pjac[(long)(i * n + jcol) * ns] = (float)(hInv * (pf[i * ns] - pf0[i * ns]));
+        if (al) Jg[lane * n + jcol] = (float)(hInv * (f - f0));
         ++jcol;
         if (jcol < n) { lab = L_JAC_COLUMN; break; }
         ++cjac;
@@ -645,21 +671,16 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
         break;
       }
       case PH_NEWTON: {
-        const double* v1 = Vp(1);
-#pragma unroll 4
-        for (int k = 0; k < n; ++k) pr[k * ns] = pf[k * ns] * h - v1[k * ns] - pb[k * ns];
-        lin_solve_r<LUT>(x, dd, pr, plu, pperm, pjac, ptmp, hr0f, n, ns);
-        ++csolve;
-#pragma unroll 4
-        for (int k = 0; k < n; ++k) pb[k * ns] += x[k * kAT];
+        x = solve(al ? f * h - v[1] - b : 0.);
+        b += x;
         ++newtonK;
         if (newtonK > 4u) { convOK = 0; iterConvergence = 4; lab = L_CORR_DONE; }
         else lab = L_NEWTON_TEST;
         break;
       }
       case PH_STAB_CONV: {
-        double* z1 = Zp(1);
-        for (int k = 0; k < n; ++k) z1[k * ns] = pf[k * ns] * h;
+        z[1] = f * h;
+        dz = true;
         tStabilize = tInMeshPoint;
         if (numberOfSteps > stepOfLastJacobian + 5u) jacobianChange = 1;
         if (numberOfSteps != stepOfLastJacobian && iterConvergenceFailure == 50u) jacobianChange = 1;
@@ -668,25 +689,15 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
         break;
       }
       case PH_STAB_ERR: {
-        double* z1 = Zp(1);
-        for (int k = 0; k < n; ++k) z1[k * ns] = pf[k * ns] * h;
+        z[1] = f * h;
+        dz = true;
         tStabilize = tInMeshPoint;
         odeHStatus = H_DEC;
         hNextStep *= hScale;
         lab = L_DRIVER_LOOP;
         break;
       }
-      case PH_FINAL:
-        lab = L_FINISH;
-        break;
-      case PH_FACTORED:
-        factorized = 1;
-        ++cfact;
-        lab = L_AFTER_FACT;
-        break;
-      default:
-        status = -10;
-        copy_r(pz, pva, n, ns);
+      default:   // PH_FINAL
         lab = L_FINISH;
         break;
     }
@@ -694,26 +705,15 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
     // labels that need no RHS; a request or a finish is reached within a few hops
     for (int hop = 0; lab != L_NONE; ++hop) {
       if (hop >= 64) {
-        status = -10;
-        copy_r(pz, pva, n, ns);
+        fail_keep_z(-10);
         lab = L_FINISH;
       }
       switch (lab) {
         case L_START_STEP: {
           // MultiValueSolver::Solve loop (:532-560) + DriverStep prologue (:753-776)
-          if (numberOfSteps >= (unsigned)o.max_steps) {
-            status = -1;
-            copy_r(pz, pva, n, ns);
-            lab = L_FINISH;
-            break;
-          }
-          set_eps_r(pz, peps, n, ns, o.atol, o.rtol);
-          if (kMachEpsDouble * wrms_r(pz, peps, n, ns) > 1.) {
-            status = -2;
-            copy_r(pz, pva, n, ns);
-            lab = L_FINISH;
-            break;
-          }
+          if (numberOfSteps >= (unsigned)o.max_steps) { fail_keep_z(-1); lab = L_FINISH; break; }
+          eps = al ? 1. / (o.atol + o.rtol * fabs(z[0])) : 0.;
+          if (kMachEpsDouble * wrms(z[0]) > 1.) { fail_keep_z(-2); lab = L_FINISH; break; }
           tInMeshPoint = t;
           iterConvergenceFailure = 0; iterErrorFailure = 0; convOK = 1;
           if (odeOrderStatus != O_CONST || odeHStatus != H_CONST) iterOrder = 0;
@@ -729,7 +729,16 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
           // DriverStep while(1) body up to FindCorrection (:778-820, :1212-1266)
           if (odeHStatus != H_CONST) {
             hScale = hNextStep / hNordsieck;
-            rescale_z_r(pz, n, ns, p, hScale, NC, yminT, ymaxT);
+            double hr = 1.;
+#pragma unroll
+            for (unsigned i = 1; i < 8; ++i) {
+              if (i <= p) {
+                hr *= hScale;
+                z[i] *= hr;
+              }
+            }
+            z[0] = clamp(z[0]);
+            dz = true;
             iterOrder = 0;
             odeHStatus = H_CONST;
           }
@@ -737,26 +746,54 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
           hNordsieck = hNextStep;
           t = tInMeshPoint + h;
           if (t == tInMeshPoint) {
-            status = -6;
-            copy_r(pz, pva, n, ns);
+            fail_keep_z(-6);
             t = tInMeshPoint;
             lab = L_FINISH;
             break;
           }
-          predict_r(pz, pv, pvb, peps, n, ns, p, NC, yminT, ymaxT);
+          {
+            // MultiValueStep prediction v = D z with min/max handling, then vb = CheckConstraints(v0)
+            double wv[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) wv[i] = (i <= (int)p) ? z[i] : 0.;
+#pragma unroll
+            for (int i = 0; i < 7; ++i)
+#pragma unroll
+              for (int j = 6; j >= 0; --j)
+                if (i < (int)p && j >= i && j <= (int)p - 1) wv[j] += wv[j + 1];
+            if (al) {
+              if (wv[0] < lo && fabs(wv[0] - lo) * eps < double(n)) {
+                wv[1] = lo - z[0];
+                wv[0] = lo;
+#pragma unroll
+                for (int i = 2; i < 8; ++i) wv[i] = 0.;
+              }
+              if (wv[0] > hi && fabs(wv[0] - hi) * eps < double(n)) {
+                wv[1] = hi - z[0];
+                wv[0] = hi;
+#pragma unroll
+                for (int i = 2; i < 8; ++i) wv[i] = 0.;
+              }
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+              if (i <= (int)p) v[i] = wv[i];
+            dv = true;
+            vb = clamp(wv[0]);
+          }
           phase = PH_PRED;
           lab = L_NONE;
           break;
         }
         case L_JAC_COLUMN: {
           // KernelDense::NumericalJacobian, constrained branch: increment of column jcol
-          const double yh = pvb[jcol * ns];
-          const double ej = peps[jcol * ns];
+          const double yh = __shfl_sync(kFull, vb, jcol);
+          const double ej = __shfl_sync(kFull, eps, jcol);
           const double aa = fabs(yh), bb = fabs(1. / ej);
           hJ = sqrt(kMachEpsDouble) * (aa > bb ? aa : bb);
           hJ = fmax(hJ, hf / ej);
           hJ = fmax(hJ, sqrt(kTinyFloat));
-          if (yh + hJ > hi_b(jcol, NC, ymaxT)) hJ = -hJ;
+          if (yh + hJ > (jcol < NC ? 1. : o.y_max_T)) hJ = -hJ;
           phase = PH_JAC;
           lab = L_NONE;
           break;
@@ -765,46 +802,31 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
           if (factorized && iterOrder == 0) factorized = 0;
           if (!factorized) {
             hr0f = h * c_gear_r.r[0][p - 1];
-            phase = PH_FACT;
-            lab = L_NONE;
-            break;
+            factorize();
+            factorized = 1;
           }
           lab = L_AFTER_FACT;
           break;
         }
         case L_AFTER_FACT: {
-          const double* v1 = Vp(1);
-#pragma unroll 4
-          for (int k = 0; k < n; ++k) pr[k * ns] = pf0[k * ns] * h - v1[k * ns];
-          lin_solve_r<LUT>(x, dd, pr, plu, pperm, pjac, ptmp, hr0f, n, ns);
-          ++csolve;
-#pragma unroll 4
-          for (int k = 0; k < n; ++k) pb[k * ns] = x[k * kAT];
+          x = solve(al ? f0 * h - v[1] : 0.);
+          b = x;
           newtonK = 1;
           lab = L_NEWTON_TEST;
           break;
         }
         case L_NEWTON_TEST: {
           const double r0 = c_gear_r.r[0][p - 1];
-          double s2 = 0.;
-#pragma unroll 4
-          for (int k = 0; k < n; ++k) {
-            const double c = x[k * kAT] * peps[k * ns];
-            s2 += c * c;
-          }
-          const double cc = r0 * sqrt(s2 / double(n));
+          const double cc = r0 * wrms(x);
           if (cc < 1.) { convOK = 1; iterConvergence = newtonK; lab = L_CORR_DONE; break; }
           if (newtonK > 1 && cc > 2. * oldCC) { convOK = 0; iterConvergence = newtonK; lab = L_CORR_DONE; break; }
           oldCC = cc;
-          const double* v0 = Vp(0);
-#pragma unroll 4
-          for (int k = 0; k < n; ++k) {
-            double va = pb[k * ns] * r0 + v0[k * ns];
-            const double lo = lo_b(k, NC, yminT), hi = hi_b(k, NC, ymaxT);
-            if (va < lo) { va = lo; pb[k * ns] = (lo - pz[k * ns]) / r0; }
-            if (va > hi) { va = hi; pb[k * ns] = (hi - pz[k * ns]) / r0; }
-            pva[k * ns] = va;
+          double vn = b * r0 + v[0];
+          if (al) {
+            if (vn < lo) { vn = lo; b = (lo - z[0]) / r0; }
+            if (vn > hi) { vn = hi; b = (hi - z[0]) / r0; }
           }
+          va = vn;
           phase = PH_NEWTON;
           lab = L_NONE;
           break;
@@ -815,8 +837,7 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
             iterConvergenceFailure++;
             ++cconv;
             if (iterConvergenceFailure >= 50u || fabs(h) <= 0.) {
-              status = iterConvergenceFailure >= 50u ? -5 : -6;
-              copy_r(pz, pva, n, ns);
+              fail_keep_z(iterConvergenceFailure >= 50u ? -5 : -6);
               t = tInMeshPoint;
               lab = L_FINISH;
               break;
@@ -850,48 +871,31 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
           // MultiValueStep tail (:1271-1327)
           {
             const double r0 = c_gear_r.r[0][p - 1];
-            double* v0 = Vp(0);
-            double* v1 = Vp(1);
-            for (int k = 0; k < n; ++k) {
-              const double lo = lo_b(k, NC, yminT), hi = hi_b(k, NC, ymaxT);
-              double b = pb[k * ns];
-              const double va = b * r0;
-              double x0 = v0[k * ns];
-              const double x1 = v1[k * ns];
-              const double z0 = pz[k * ns];
-              if (x0 + va < lo) { b = lo - z0 - x1; x0 = lo - va; if (x0 < lo) x0 = lo; }
-              if (x0 + va > hi) { b = hi - z0 - x1; x0 = hi - va; if (x0 > hi) x0 = hi; }
-              v0[k * ns] = x0 + va;
-              v1[k * ns] = x1 + b;
-              pb[k * ns] = b;
+            double bb = b;
+            const double vr = bb * r0;
+            double x0 = v[0];
+            const double x1 = v[1];
+            if (al) {
+              if (x0 + vr < lo) { bb = lo - z[0] - x1; x0 = lo - vr; if (x0 < lo) x0 = lo; }
+              if (x0 + vr > hi) { bb = hi - z[0] - x1; x0 = hi - vr; if (x0 > hi) x0 = hi; }
             }
-            for (unsigned i = 2; i <= p; ++i) {
-              const double ri = c_gear_r.r[i][p - 1];
-              double* vi = Vp(i);
-#pragma unroll 4
-              for (int k = 0; k < n; ++k) vi[k * ns] += pb[k * ns] * ri;
-            }
-            {
-              double* vp1 = Vp(p + 1);
-              const double* vpp = Vp(p);
-              const double* zpp = Zp(p);
-              for (int k = 0; k < n; ++k) vp1[k * ns] = (vpp[k * ns] - zpp[k * ns]) / (double(p) + 1.);
-            }
-            if (iterOrder >= p) {
-              double* vp2 = Vp(p + 2);
-              const double* vp1 = Vp(p + 1);
-              const double* zp1 = Zp(p + 1);
-              for (int k = 0; k < n; ++k) vp2[k * ns] = (vp1[k * ns] - zp1[k * ns]) / (double(p) + 2.);
-            }
+            v[0] = x0 + vr;
+            v[1] = x1 + bb;
+            b = bb;
+#pragma unroll
+            for (unsigned i = 2; i < 8; ++i)
+              if (i <= p) v[i] += b * c_gear_r.r[i][p - 1];
+            set8(v, p + 1, (get8(v, p) - get8(z, p)) / (double(p) + 1.));
+            if (iterOrder >= p) set8(v, p + 2, (get8(v, p + 1) - get8(z, p + 1)) / (double(p) + 2.));
+            dv = true;
           }
           // error test (:876-962)
-          double hCur = c_gear_r.Ep[p] * wrms_r(Vp(p + 1), peps, n, ns);
+          double hCur = c_gear_r.Ep[p] * wrms(get8(v, p + 1));
           if (hCur > 1.) {
             iterErrorFailure++;
             ++cerr;
             if (iterErrorFailure >= 50u || fabs(h) <= 0.) {
-              status = iterErrorFailure >= 50u ? -4 : -6;
-              copy_r(pz, pva, n, ns);
+              fail_keep_z(iterErrorFailure >= 50u ? -4 : -6);
               t = tInMeshPoint;
               lab = L_FINISH;
               break;
@@ -900,7 +904,7 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
             hCur = 0.8 * pow(1. / hCur, 1. / double(p + 1));
             hScale = hCur;
             if (p > 1u) {
-              double hMinus = c_gear_r.Ep[p - 1] * wrms_r(Vp(p), peps, n, ns);
+              double hMinus = c_gear_r.Ep[p - 1] * wrms(get8(v, p));
               hMinus = 1. / (hMinus + kMachEpsFloat);
               hMinus = 0.8 * pow(hMinus, 1. / double(p));
               if (hMinus > hCur) { hScale = hMinus; p -= 1; odeOrderStatus = O_DEC; }
@@ -925,20 +929,11 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
             // MethodGear::ConvergenceRate (:425-516) with the stored Jacobian
             if (iterErrorFailure > 0 || iterConvergenceFailure > 0) iterConvergenceRate = 0;
             if (iterConvergence > 1) {
-              const double* v0 = Vp(0);
-              const double* v1 = Vp(1);
-              const double* z1 = Zp(1);
-#pragma unroll 4
-              for (int j = 0; j < n; ++j) x[j * kAT] = v0[j * ns] - pz[j * ns];
-              double normd = 0., normf = 0.;
-              for (int i = 0; i < n; ++i) {
-                double s = 0.;
-#pragma unroll 4
-                for (int j = 0; j < n; ++j) s += (double)pjac[(long)(i * n + j) * ns] * x[j * kAT];
-                const double va = v1[i * ns] - (s * h + z1[i * ns]);
-                normd += fabs(va);
-                normf += fabs(v1[i * ns]);
-              }
+              load_j();
+              const double s = rowdot(Js, v[0] - z[0]);
+              const double vr = v[1] - (s * h + z[1]);
+              const double normd = wsum(al ? fabs(vr) : 0.);
+              const double normf = wsum(al ? fabs(v[1]) : 0.);
               if (normd > 3. * normf + .1 && iterConvergence > 2) {
                 if (numberOfSteps > stepOfLastJacobian + 5u) jacobianChange = 1;
                 hScale = 0.5; odeHStatus = H_DEC; hNextStep = h * hScale;
@@ -965,16 +960,16 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
               // NewOrderNewH (:1042-1210)
               double hMinus = 0., hC = 0., hPlus = 0., alfa1 = 0., alfa3 = 0.;
               if (p > 1u && odeOrderStatus != O_INC) {
-                hMinus = c_gear_r.Ep[p - 1] * wrms_r(Vp(p), peps, n, ns) + kMachEpsFloat;
+                hMinus = c_gear_r.Ep[p - 1] * wrms(get8(v, p)) + kMachEpsFloat;
                 hMinus = 1. / hMinus;
                 alfa1 = alfa2(p - 1) - .05;
                 hMinus = alfa1 * pow(hMinus, 1. / double(p));
               }
-              hC = c_gear_r.Ep[p] * wrms_r(Vp(p + 1), peps, n, ns) + kMachEpsFloat;
+              hC = c_gear_r.Ep[p] * wrms(get8(v, p + 1)) + kMachEpsFloat;
               hC = 1. / hC;
               hC = alfa2(p) * pow(hC, 1. / double(p + 1));
               if (p < maximum_order && odeOrderStatus != O_DEC) {
-                hPlus = c_gear_r.Ep[p + 1] * wrms_r(Vp(p + 2), peps, n, ns) + kMachEpsFloat;
+                hPlus = c_gear_r.Ep[p + 1] * wrms(get8(v, p + 2)) + kMachEpsFloat;
                 hPlus = 1. / hPlus;
                 alfa3 = alfa2(p + 1) - .25;
                 hPlus = alfa3 * pow(hPlus, 1. / double(p + 2));
@@ -1013,36 +1008,34 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
               }
             }
           }
-          for (unsigned i = 0; i <= p + 2; ++i) copy_r(Vp(i), Zp(i), n, ns);
-#pragma unroll 4
-          for (int k = 0; k < n; ++k) {
-            double z0 = pz[k * ns];
-            const double lo = lo_b(k, NC, yminT), hi = hi_b(k, NC, ymaxT);
-            if (z0 < lo) z0 = lo;
-            if (z0 > hi) z0 = hi;
-            pz[k * ns] = z0;
-          }
+#pragma unroll
+          for (unsigned i = 0; i < 8; ++i)
+            if (i <= p + 2) z[i] = v[i];
+          z[0] = clamp(z[0]);
+          dz = true;
           numberOfSteps++;
           ++cstep;
           if (tOut == t) {
-            copy_r(pz, pva, n, ns);
+            va = z[0];
             lab = L_FINISH;
             break;
           }
           if (tOut < t) {
             // Interpolation (:687-706); the RHS at tOut then sets QR (:599-611)
             const double hp = (tOut - t) / hNordsieck;
-            for (int k = 0; k < n; ++k) {
-              double yv = pz[k * ns];
-              if (hp != 0.) {
-                double hr = 1.;
-                for (unsigned i = 1; i <= p; ++i) { hr *= hp; yv += Zp(i)[k * ns] * hr; }
-                const double lo = lo_b(k, NC, yminT), hi = hi_b(k, NC, ymaxT);
-                if (yv < lo) yv = lo;
-                if (yv > hi) yv = hi;
+            double yv = z[0];
+            if (hp != 0.) {
+              double hr = 1.;
+#pragma unroll
+              for (unsigned i = 1; i < 8; ++i) {
+                if (i <= p) {
+                  hr *= hp;
+                  yv += z[i] * hr;
+                }
               }
-              pva[k * ns] = yv;
+              yv = clamp(yv);
             }
+            va = yv;
             phase = PH_FINAL;
             lab = L_NONE;
             break;
@@ -1052,13 +1045,14 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
         }
         case L_FINISH: {
           // utilities.H:153-200 and the scatter of chemistry_DI.H:221-235
-          double s = 0.;
-          for (int i = 0; i < NC; ++i) s += pva[i * ns];
-          for (int i = 0; i < NC; ++i) a.Y[(long)i * a.ld + cell] = pva[i * ns] / s;
-          if (o.energy) a.T[cell] = pva[NC * ns];
-          if (a.Q) a.Q[cell] = QR;
-          if (a.status) a.status[cell] = status;
-          if (a.nsteps) a.nsteps[cell] = (int)numberOfSteps;
+          const double s = wsum(lane < NC ? va : 0.);
+          if (lane < NC) a.Y[(long)lane * a.ld + cell] = va / s;
+          if (o.energy && lane == NC) a.T[cell] = va;
+          if (lane == 0) {
+            if (a.Q) a.Q[cell] = QR;
+            if (a.status) a.status[cell] = status;
+            if (a.nsteps) a.nsteps[cell] = (int)numberOfSteps;
+          }
           phase = PH_DONE;
           lab = L_NONE;
           break;
@@ -1068,111 +1062,41 @@ __global__ void __launch_bounds__(kAT) rounds_advance_kernel(int NC, StepOptions
           break;
       }
     }
-    // ---- store the cell's scalar state ----
-    sd[D_T * ns] = t; sd[D_TOUT * ns] = tOut; sd[D_TMESH * ns] = tInMeshPoint; sd[D_TSTAB * ns] = tStabilize;
-    sd[D_H * ns] = h; sd[D_HNEXT * ns] = hNextStep; sd[D_HNORD * ns] = hNordsieck; sd[D_HSCALE * ns] = hScale;
-    sd[D_HSCALEMAX * ns] = hScaleMax; sd[D_A24 * ns] = alfa2_4; sd[D_A25 * ns] = alfa2_5;
-    sd[D_OLDCC * ns] = oldCC; sd[D_HF * ns] = hf; sd[D_HJ * ns] = hJ; sd[D_PENDHS * ns] = pendHScale;
-    sd[D_HR0 * ns] = hr0f;
-    si[I_PHASE * ns] = phase; si[I_STATUS * ns] = status; si[I_P * ns] = (int)p; si[I_ITORDER * ns] = (int)iterOrder;
-    si[I_ORDNEXT * ns] = (int)orderInNextStep; si[I_HSTAT * ns] = odeHStatus; si[I_OSTAT * ns] = odeOrderStatus;
-    si[I_FACTORIZED * ns] = factorized; si[I_JACCHANGE * ns] = jacobianChange; si[I_CONVOK * ns] = convOK;
-    si[I_NSTEPS * ns] = (int)numberOfSteps; si[I_ITCONV * ns] = (int)iterConvergence;
-    si[I_ITCONVRATE * ns] = (int)iterConvergenceRate; si[I_ITCONVFAIL * ns] = (int)iterConvergenceFailure;
-    si[I_ITERRFAIL * ns] = (int)iterErrorFailure; si[I_NCFOM * ns] = (int)nConvFailOrderMax;
-    si[I_STEPLASTJ * ns] = (int)stepOfLastJacobian; si[I_ITCONST * ns] = (int)iterConstSteps;
-    si[I_ITMINORD * ns] = (int)iterMinimumOrder; si[I_FIXEDMIN * ns] = fixedOrderMin ? 1 : 0;
-    si[I_NEWTONK * ns] = (int)newtonK; si[I_JCOL * ns] = jcol; si[I_MAXORD * ns] = (int)maximum_order;
-    int c8[NCNT];
+    // ---- write the state back ----
+    if (al) {
+      if (dz)
 #pragma unroll
-    for (int k = 0; k < NCNT; ++k) c8[k] = si[(I_CNT0 + k) * ns];
-    c8[CNT_STEPS] += cstep; c8[CNT_JAC] += cjac; c8[CNT_FACT] += cfact; c8[CNT_SOLVE] += csolve;
-    c8[CNT_ERRFAIL] += cerr; c8[CNT_CONVFAIL] += cconv;
+        for (int i = 0; i < 8; ++i) R[RL.oz + i * n + lane] = z[i];
+      if (dv)
 #pragma unroll
-    for (int k = 0; k < NCNT; ++k) si[(I_CNT0 + k) * ns] = c8[k];
-    if (phase == PH_DONE && a.counters)
-      for (int k = 0; k < NCNT; ++k) a.counters[(long)cell * NCNT + k] = c8[k];
-  }
-}
-
-// ---------------------------------------------------------------------------
-// factor: one warp per cell that requested a factorisation.  G = I - hr0 J
-// (built in FP64, stored as LUT), partial pivoting on the largest magnitude,
-// first occurrence (KernelDense LU), rows = lanes, matrix in shared memory.
-// The factors are stored as P G = L U with perm[k] = row of G in position k.
-// ---------------------------------------------------------------------------
-template <typename LUT>
-__global__ void __launch_bounds__(kFW * 32) rounds_factor_kernel(int NC, RoundBufs B, int par) {
-  extern __shared__ __align__(16) unsigned char fsm[];
-  const long ns = B.ns;
-  const int n = NC + 1, ld = n + 1;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  LUT* G = (LUT*)fsm + (size_t)w * n * ld;
-  int* rowof = (int*)((LUT*)fsm + (size_t)kFW * n * ld) + w * 32;
-  const int nact = B.nact[par];
-  const int* act = par ? B.act1 : B.act0;
-  const int nwarps = gridDim.x * kFW;
-  for (int base = (blockIdx.x * kFW + w) * 32; base < nact; base += nwarps * 32) {
-    const int idx = base + lane;
-    const int mycell = idx < nact ? act[idx] : 0;
-    const bool want = idx < nact && B.si[I_PHASE * ns + mycell] == PH_FACT;
-    unsigned m = __ballot_sync(kFull, want);
-    while (m) {
-      const int q = __ffs(m) - 1;
-      m &= m - 1;
-      const int cell = __shfl_sync(kFull, mycell, q);
-      const double hr0 = B.sd[D_HR0 * ns + cell];
-      const float* J = B.jac + cell;
-      if (lane < n) {
-        for (int j = 0; j < n; ++j) {
-          double g = -hr0 * (double)J[(long)(lane * n + j) * ns];
-          if (j == lane) g += 1.;
-          G[lane * ld + j] = (LUT)g;
-        }
-      }
-      rowof[lane] = lane;   // rowof[k]: row of G now in position k
-      __syncwarp();
-      for (int k = 0; k < n; ++k) {
-        LUT v = (lane >= k && lane < n) ? (LUT)fabs((double)G[lane * ld + k]) : (LUT)-1;
-        int r = lane;
-        for (int off = 16; off > 0; off >>= 1) {
-          const LUT ov = __shfl_xor_sync(kFull, v, off);
-          const int orr = __shfl_xor_sync(kFull, r, off);
-          if (ov > v || (ov == v && orr < r)) { v = ov; r = orr; }
-        }
-        // one pivot for the whole warp; a NaN column cannot send it outside rows k..n-1
-        r = __shfl_sync(kFull, r, 0);
-        if (r < k || r >= n) r = k;
-        if (r != k) {
-          if (lane < n) {
-            const LUT tmp = G[k * ld + lane];
-            G[k * ld + lane] = G[r * ld + lane];
-            G[r * ld + lane] = tmp;
-          }
-          if (lane == 0) {
-            const int t = rowof[k];
-            rowof[k] = rowof[r];
-            rowof[r] = t;
-          }
-        }
-        __syncwarp();
-        const LUT d = G[k * ld + k];
-        if (lane > k && lane < n) {
-          LUT l = G[lane * ld + k];
-          if (d != (LUT)0) l /= d;
-          G[lane * ld + k] = l;
-          for (int j = k + 1; j < n; ++j) G[lane * ld + j] -= l * G[k * ld + j];
-        }
-        __syncwarp();
-      }
-      LUT* lu = (LUT*)B.lu + cell;
-      if (lane < n) {
-        for (int j = 0; j < n; ++j) lu[(long)(lane * n + j) * ns] = G[lane * ld + j];
-        B.perm[(long)lane * ns + cell] = rowof[lane];
-      }
-      if (lane == 0) B.si[I_PHASE * ns + cell] = PH_FACTORED;
-      __syncwarp();
+        for (int i = 0; i < 8; ++i) R[RL.ov + i * n + lane] = v[i];
+      R[RL.ob + lane] = b;
+      R[RL.ova + lane] = va;
+      R[RL.ovb + lane] = vb;
+      R[RL.oeps + lane] = eps;
     }
+    if (lane == 0) {
+      R[D_T] = t; R[D_TOUT] = tOut; R[D_TMESH] = tInMeshPoint; R[D_TSTAB] = tStabilize; R[D_H] = h;
+      R[D_HNEXT] = hNextStep; R[D_HNORD] = hNordsieck; R[D_HSCALE] = hScale; R[D_HSCALEMAX] = hScaleMax;
+      R[D_A24] = alfa2_4; R[D_A25] = alfa2_5; R[D_OLDCC] = oldCC; R[D_HF] = hf; R[D_HJ] = hJ;
+      R[D_PENDHS] = pendHScale; R[D_HR0] = hr0f;
+      RI[I_PHASE] = phase; RI[I_STATUS] = status; RI[I_P] = (int)p; RI[I_ITORDER] = (int)iterOrder;
+      RI[I_ORDNEXT] = (int)orderInNextStep; RI[I_HSTAT] = odeHStatus; RI[I_OSTAT] = odeOrderStatus;
+      RI[I_FACTORIZED] = factorized; RI[I_JACCHANGE] = jacobianChange; RI[I_CONVOK] = convOK;
+      RI[I_NSTEPS] = (int)numberOfSteps; RI[I_ITCONV] = (int)iterConvergence;
+      RI[I_ITCONVRATE] = (int)iterConvergenceRate; RI[I_ITCONVFAIL] = (int)iterConvergenceFailure;
+      RI[I_ITERRFAIL] = (int)iterErrorFailure; RI[I_NCFOM] = (int)nConvFailOrderMax;
+      RI[I_STEPLASTJ] = (int)stepOfLastJacobian; RI[I_ITCONST] = (int)iterConstSteps;
+      RI[I_ITMINORD] = (int)iterMinimumOrder; RI[I_FIXEDMIN] = fixedOrderMin ? 1 : 0;
+      RI[I_NEWTONK] = (int)newtonK; RI[I_JCOL] = jcol; RI[I_MAXORD] = (int)maximum_order;
+      RI[I_CNT0 + CNT_STEPS] += cstep; RI[I_CNT0 + CNT_JAC] += cjac; RI[I_CNT0 + CNT_FACT] += cfact;
+      RI[I_CNT0 + CNT_SOLVE] += csolve; RI[I_CNT0 + CNT_ERRFAIL] += cerr; RI[I_CNT0 + CNT_CONVFAIL] += cconv;
+    }
+    if (phase == PH_DONE && a.counters) {
+      __syncwarp();
+      if (lane < NCNT) a.counters[(long)cell * NCNT + lane] = RI[I_CNT0 + lane];
+    }
+    __syncwarp();
   }
 }
 
@@ -1180,7 +1104,6 @@ __global__ void __launch_bounds__(kFW * 32) rounds_factor_kernel(int NC, RoundBu
 // compact: cells still integrating form the next list (warp-aggregated append).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kCT) rounds_compact_kernel(RoundBufs B, int par) {
-  const long ns = B.ns;
   const int nact = B.nact[par];
   const int* in = par ? B.act1 : B.act0;
   int* out = par ? B.act0 : B.act1;
@@ -1191,7 +1114,7 @@ __global__ void __launch_bounds__(kCT) rounds_compact_kernel(RoundBufs B, int pa
   for (int base = gw * 32; base < nact; base += nw * 32) {
     const int idx = base + lane;
     const int cell = idx < nact ? in[idx] : 0;
-    const bool alive = idx < nact && B.si[I_PHASE * ns + cell] != PH_DONE;
+    const bool alive = idx < nact && ((const int*)(B.rec + (long)cell * B.L.RS + ND_))[I_PHASE] != PH_DONE;
     const unsigned m = __ballot_sync(kFull, alive);
     int off = 0;
     if (lane == 0 && m) off = atomicAdd(cnt, __popc(m));
@@ -1205,69 +1128,39 @@ __global__ void __launch_bounds__(kCT) rounds_compact_kernel(RoundBufs B, int pa
 // ---------------------------------------------------------------------------
 namespace {
 
-RoundBufs carve(const MechLayout& L, void* base, long ns, bool lu64) {
-  const int n = L.nc + 1;
+size_t list_bytes(long cap) { return ((sizeof(int) * (size_t)cap) + 255) & ~(size_t)255; }
+
+RoundBufs carve(const MechLayout& L, void* base, long cap, bool lu64) {
   RoundBufs B{};
-  B.ns = ns;
+  B.L = rec_layout(L.nc + 1, lu64);
   char* p = (char*)base;
-  auto take = [&](size_t bytes) {
-    char* r = p;
-    p += (bytes + 255) & ~(size_t)255;
-    return (void*)r;
-  };
-  B.sd = (double*)take(sizeof(double) * ND_ * ns);
-  B.si = (int*)take(sizeof(int) * NI_ * ns);
-  B.z = (double*)take(sizeof(double) * 8 * n * ns);
-  B.v = (double*)take(sizeof(double) * 8 * n * ns);
-  B.b = (double*)take(sizeof(double) * n * ns);
-  B.f = (double*)take(sizeof(double) * n * ns);
-  B.f0 = (double*)take(sizeof(double) * n * ns);
-  B.va = (double*)take(sizeof(double) * n * ns);
-  B.vb = (double*)take(sizeof(double) * n * ns);
-  B.eps = (double*)take(sizeof(double) * n * ns);
-  B.r = (double*)take(sizeof(double) * n * ns);
-  B.tmp = (double*)take(sizeof(double) * n * ns);
-  B.jac = (float*)take(sizeof(float) * n * n * ns);
-  B.lu = take((lu64 ? sizeof(double) : sizeof(float)) * n * n * ns);
-  B.perm = (int*)take(sizeof(int) * n * ns);
-  B.act0 = (int*)take(sizeof(int) * ns);
-  B.act1 = (int*)take(sizeof(int) * ns);
-  B.nact = (int*)take(sizeof(int) * 2);
+  B.rec = (double*)p;
+  p += sizeof(double) * (size_t)B.L.RS * cap;
+  B.act0 = (int*)p; p += list_bytes(cap);
+  B.act1 = (int*)p; p += list_bytes(cap);
+  B.nact = (int*)p;
   return B;
 }
 
-// One round's kernels for a factor type.
-template <typename LUT>
-struct RoundKernels {
-  static cudaError_t prepare(size_t as, size_t fs, int* adv_bps, int* fac_bps) {
-    cudaError_t e = cudaFuncSetAttribute(rounds_factor_kernel<LUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)fs);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(rounds_advance_kernel<LUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)as);
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(adv_bps, rounds_advance_kernel<LUT>, kAT, as);
-    if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(fac_bps, rounds_factor_kernel<LUT>, kFW * 32, fs);
-  }
-  static void launch(const RoundsPlan& P, const MechLayout& L, const unsigned char* mech, const StepOptions& o,
-                     const StepArgs& a, const RoundBufs& B, int par, int* err, cudaStream_t s) {
-    rounds_rhs_kernel<<<P.g_rhs, kRT, P.rhs_smem, s>>>(L, mech, o.energy, a.p, B, par, err);
-    rounds_advance_kernel<LUT><<<P.g_adv, kAT, P.adv_smem, s>>>(L.nc, o, a, B, par, 0);
-    rounds_factor_kernel<LUT><<<P.g_fac, kFW * 32, P.fac_smem, s>>>(L.nc, B, par);
-    rounds_advance_kernel<LUT><<<P.g_adv, kAT, P.adv_smem, s>>>(L.nc, o, a, B, par, 1);
-    rounds_compact_kernel<<<P.g_cmp, kCT, 0, s>>>(B, par);
-  }
-};
+size_t advance_smem(const MechLayout& L, bool lu64) {
+  const size_t n = L.nc + 1;
+  return (size_t)kWA * n * (n + 1) * (2 * (lu64 ? sizeof(double) : sizeof(float)) + sizeof(float)) +
+         kWA * 32 * sizeof(int);
+}
+
+template <typename LUT, int NM>
+cudaError_t prepare_advance(size_t as, int* bps) {
+  cudaError_t e = cudaFuncSetAttribute(rounds_advance_kernel<LUT, NM>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)as);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, rounds_advance_kernel<LUT, NM>, kWA * 32, as);
+}
 
 }  // namespace
 
-size_t rounds_bytes(const MechLayout& L, long ns, bool lu64) {
-  const int n = L.nc + 1;
-  auto r = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  return r(sizeof(double) * ND_ * ns) + r(sizeof(int) * NI_ * ns) + 2 * r(sizeof(double) * 8 * n * ns) +
-         10 * r(sizeof(double) * n * ns) + r(sizeof(float) * n * n * ns) +
-         r((lu64 ? sizeof(double) : sizeof(float)) * n * n * ns) + r(sizeof(int) * n * ns) +
-         2 * r(sizeof(int) * ns) + r(sizeof(int) * 2);
+size_t rounds_bytes(const MechLayout& L, long cap, bool lu64) {
+  const RecLayout R = rec_layout(L.nc + 1, lu64);
+  return sizeof(double) * (size_t)R.RS * cap + 2 * list_bytes(cap) + 256;
 }
 
 cudaError_t upload_gear_rounds(const GearConsts& gc) { return cudaMemcpyToSymbol(c_gear_r, &gc, sizeof(GearConsts)); }
@@ -1278,36 +1171,34 @@ cudaError_t rounds_prepare(const MechLayout& L, bool lu64, int sm_count, RoundsP
   *P = RoundsPlan{};
   P->lu64 = lu64;
   P->rhs_smem = ((L.bytes + 15u) & ~15u) + (size_t)4 * L.nc * kRT * sizeof(double);
-  P->adv_smem = (size_t)2 * n * kAT * sizeof(double);
-  P->fac_smem = (size_t)kFW * n * (n + 1) * (lu64 ? sizeof(double) : sizeof(float)) + kFW * 32 * sizeof(int);
+  P->adv_smem = advance_smem(L, lu64);
   cudaError_t e = cudaFuncSetAttribute(rounds_rhs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)P->rhs_smem);
   if (e != cudaSuccess) return e;
-  int rhs_bps = 0, adv_bps = 0, fac_bps = 0, cmp_bps = 0;
+  int rhs_bps = 0, adv_bps = 0, cmp_bps = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rhs_bps, rounds_rhs_kernel, kRT, P->rhs_smem);
   if (e != cudaSuccess) return e;
-  if (lu64) e = RoundKernels<double>::prepare(P->adv_smem, P->fac_smem, &adv_bps, &fac_bps);
-  else e = RoundKernels<float>::prepare(P->adv_smem, P->fac_smem, &adv_bps, &fac_bps);
+  if (lu64) e = n <= 16 ? prepare_advance<double, 16>(P->adv_smem, &adv_bps) : prepare_advance<double, 32>(P->adv_smem, &adv_bps);
+  else e = n <= 16 ? prepare_advance<float, 16>(P->adv_smem, &adv_bps) : prepare_advance<float, 32>(P->adv_smem, &adv_bps);
   if (e != cudaSuccess) return e;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cmp_bps, rounds_compact_kernel, kCT, 0);
   if (e != cudaSuccess) return e;
-  if (rhs_bps <= 0 || adv_bps <= 0 || fac_bps <= 0 || cmp_bps <= 0) return cudaErrorInvalidConfiguration;
+  if (rhs_bps <= 0 || adv_bps <= 0 || cmp_bps <= 0) return cudaErrorInvalidConfiguration;
   // persistent grids: every kernel fills the GPU once and strides over the list
   P->g_rhs = (unsigned)(sm_count * rhs_bps);
   P->g_adv = (unsigned)(sm_count * adv_bps);
-  P->g_fac = (unsigned)(sm_count * fac_bps);
   P->g_cmp = (unsigned)(sm_count * cmp_bps);
   P->g_init = (unsigned)(sm_count * 8);
   return cudaSuccess;
 }
 
 cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsigned char* mech_gmem,
-                          const StepOptions& o, const StepArgs& a, void* state, long ns, int* nact_host,
+                          const StepOptions& o, const StepArgs& a, void* state, long cap, int* nact_host,
                           long max_rounds, int* err, cudaStream_t stream, long long* launches) {
   // nact_host: two pinned ints (list length, error flags); launches: kernels enqueued (added to)
   const int n = L.nc + 1;
-  if (n > 32 || a.ncells > ns || a.ncells <= 0) return cudaErrorInvalidValue;
-  const RoundBufs B = carve(L, state, ns, P.lu64);
+  if (n > 32 || a.ncells > cap || a.ncells <= 0) return cudaErrorInvalidValue;
+  const RoundBufs B = carve(L, state, cap, P.lu64);
   rounds_init_kernel<<<P.g_init, kAT, 0, stream>>>(L.nc, o, a, B);
   *launches += 1;
   cudaError_t e = cudaGetLastError();
@@ -1316,9 +1207,17 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
   int par = 0;
   for (long round = 0; round < max_rounds; round += kBatch) {
     for (int r = 0; r < kBatch; ++r) {
-      if (P.lu64) RoundKernels<double>::launch(P, L, mech_gmem, o, a, B, par, err, stream);
-      else RoundKernels<float>::launch(P, L, mech_gmem, o, a, B, par, err, stream);
-      *launches += 5;
+      rounds_rhs_kernel<<<P.g_rhs, kRT, P.rhs_smem, stream>>>(L, mech_gmem, o.energy, a.p, B, par, err);
+      const dim3 ga(P.g_adv), ta(kWA * 32);
+      if (P.lu64) {
+        if (n <= 16) rounds_advance_kernel<double, 16><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
+        else rounds_advance_kernel<double, 32><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
+      } else {
+        if (n <= 16) rounds_advance_kernel<float, 16><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
+        else rounds_advance_kernel<float, 32><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
+      }
+      rounds_compact_kernel<<<P.g_cmp, kCT, 0, stream>>>(B, par);
+      *launches += 3;
       par ^= 1;
     }
     e = cudaGetLastError();

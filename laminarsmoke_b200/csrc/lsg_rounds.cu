@@ -292,6 +292,20 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
 }
 
 
+// Asynchronous global -> shared copies (no register staging); completed by cp_async_wait_all.
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+template <typename T>
+__device__ __forceinline__ void cp_async_el(T* sdst, const T* gsrc) {
+  if (sizeof(T) == 8) cp_async8(sdst, gsrc);
+  else cp_async4(sdst, gsrc);
+}
+
 // Warp tree sum (every lane receives the total).
 __device__ __forceinline__ double wsum(double v) {
 #pragma unroll
@@ -431,12 +445,13 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int n = NC + 1, ld = n + 1;
   const RecLayout RL = B.L;
-  // per-warp shared memory: factors G[n][ld] and inverse X[n][ld] (LUT), Jacobian J[n][ld] (float),
-  // permutation [32]
-  LUT* Gs = (LUT*)wsm + (size_t)w * n * ld;
-  LUT* Xs = (LUT*)wsm + (size_t)kWA * n * ld + (size_t)w * n * ld;
-  float* Js = (float*)((LUT*)wsm + (size_t)2 * kWA * n * ld) + (size_t)w * n * ld;
-  int* Ps = (int*)((float*)((LUT*)wsm + (size_t)2 * kWA * n * ld) + (size_t)kWA * n * ld) + w * 32;
+  // per-warp shared memory: G^-1 X[n][ld] (LUT), the Gauss-Jordan work array A[n][2n+1] (LUT), its pivot
+  // row K[2n] (LUT) and the Jacobian J[n][ld] (float)
+  const int la = 2 * n + 1;
+  LUT* Xs = (LUT*)wsm + (size_t)w * n * ld;
+  LUT* As = (LUT*)wsm + (size_t)kWA * n * ld + (size_t)w * n * la;
+  LUT* Ks = (LUT*)wsm + (size_t)kWA * n * ld + (size_t)kWA * n * la + (size_t)w * 2 * n;
+  float* Js = (float*)((LUT*)wsm + (size_t)kWA * (n * ld + n * la + 2 * n)) + (size_t)w * n * ld;
   const bool al = lane < n;
   const double lo = lane < NC ? 0. : o.y_min_T, hi = lane < NC ? 1. : o.y_max_T;
   const int nact = B.nact[par];
@@ -484,6 +499,25 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
     bool j_in = false, inv_in = false;
     float* const Jg = (float*)(R + RL.ojac);
     LUT* const Ig = (LUT*)(R + RL.oinv);
+    // Rounds that solve (predictor and Newton results) will want G^-1 and, for the refinement and the
+    // convergence-rate test, J: start copying this lane's rows into shared memory now.
+    bool pending = false;
+    if (phase == PH_PRED || phase == PH_NEWTON) {
+      if (al)
+        for (int j = 0; j < n; ++j) {
+          cp_async_el(&Xs[lane * ld + j], &Ig[lane * n + j]);
+          cp_async4(&Js[lane * ld + j], &Jg[lane * n + j]);
+        }
+      pending = true;
+    }
+    auto drain = [&]() {
+      if (pending) {
+        cp_async_wait_all();
+        __syncwarp();
+        pending = false;
+        inv_in = j_in = true;
+      }
+    };
 
     enum : int { H_DEC = 0, H_CONST = 1, H_INC = 2 };
     enum : int { O_DEC = 0, O_CONST = 1, O_INC = 2 };
@@ -500,6 +534,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
       return y;
     };
     auto load_j = [&]() {   // this cell's Jacobian rows into shared memory
+      drain();
       if (!j_in) {
         if (al)
           for (int j = 0; j < n; ++j) Js[lane * ld + j] = Jg[lane * n + j];
@@ -508,6 +543,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
       }
     };
     auto load_inv = [&]() {
+      drain();
       if (!inv_in) {
         if (al)
           for (int j = 0; j < n; ++j) Xs[lane * ld + j] = Ig[lane * n + j];
@@ -550,21 +586,24 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
       ++csolve;
       return xv;
     };
-    // G = I - hr0 J, partial pivoting on the largest magnitude, first occurrence
-    // (KernelDense::BuildAndFactorizeMatrixG), rows swapped whole: P G = L U;
-    // then G^-1 = U^-1 L^-1 P, lane c solving for column c.
+    // G^-1 for G = I - hr0 J by Gauss-Jordan elimination on [G | I] with partial
+    // pivoting on the largest magnitude, first occurrence -- the pivots of the
+    // partial-pivot LU of KernelDense::BuildAndFactorizeMatrixG.  Lane i owns
+    // row i; each step's updates are independent and loaded in chunks of 4.
     auto factorize = [&]() {
       load_j();
-      if (al)
+      const int m2 = 2 * n;
+      if (al) {
         for (int j = 0; j < n; ++j) {
           double g = -hr0f * (double)Js[lane * ld + j];
           if (j == lane) g += 1.;
-          Gs[lane * ld + j] = (LUT)g;
+          As[lane * la + j] = (LUT)g;
+          As[lane * la + n + j] = (j == lane) ? (LUT)1 : (LUT)0;
         }
-      Ps[lane] = lane;
+      }
       __syncwarp();
       for (int k = 0; k < n; ++k) {
-        LUT vv = (lane >= k && lane < n) ? (LUT)fabs((double)Gs[lane * ld + k]) : (LUT)-1;
+        LUT vv = (lane >= k && lane < n) ? (LUT)fabs((double)As[lane * la + k]) : (LUT)-1;
         int r = lane;
         for (int off = 16; off > 0; off >>= 1) {
           const LUT ov = __shfl_xor_sync(kFull, vv, off);
@@ -573,44 +612,41 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
         }
         r = __shfl_sync(kFull, r, 0);
         if (r < k || r >= n) r = k;   // a NaN column cannot send the pivot outside rows k..n-1
-        if (r != k) {
-          if (al) {
-            const LUT tmp = Gs[k * ld + lane];
-            Gs[k * ld + lane] = Gs[r * ld + lane];
-            Gs[r * ld + lane] = tmp;
-          }
-          if (lane == 0) {
-            const int tp = Ps[k];
-            Ps[k] = Ps[r];
-            Ps[r] = tp;
-          }
+        // swap rows k and r and scale the pivot row into K (lanes = columns)
+        const LUT pv = As[r * la + k];
+        const LUT ipv = (pv != (LUT)0) ? (LUT)1 / pv : (LUT)0;
+        for (int j = lane; j < m2; j += 32) {
+          const LUT ak = As[k * la + j], ar = As[r * la + j];
+          Ks[j] = ar * ipv;
+          if (r != k) As[r * la + j] = ak;
         }
         __syncwarp();
-        const LUT dg = Gs[k * ld + k];
-        if (lane > k && lane < n) {
-          LUT l = Gs[lane * ld + k];
-          if (dg != (LUT)0) l /= dg;
-          Gs[lane * ld + k] = l;
-          for (int j = k + 1; j < n; ++j) Gs[lane * ld + j] -= l * Gs[k * ld + j];
+        // eliminate column k from every other row (lane = row)
+        if (al && lane != k) {
+          const LUT fct = As[lane * la + k];
+          LUT* Ai = As + lane * la;
+          int j = k;
+          for (; j + 4 <= m2; j += 4) {
+            const LUT a0 = Ai[j], a1 = Ai[j + 1], a2 = Ai[j + 2], a3 = Ai[j + 3];
+            const LUT k0 = Ks[j], k1 = Ks[j + 1], k2 = Ks[j + 2], k3 = Ks[j + 3];
+            Ai[j] = a0 - fct * k0;
+            Ai[j + 1] = a1 - fct * k1;
+            Ai[j + 2] = a2 - fct * k2;
+            Ai[j + 3] = a3 - fct * k3;
+          }
+          for (; j < m2; ++j) Ai[j] = Ai[j] - fct * Ks[j];
         }
         __syncwarp();
+        for (int j = lane; j < m2; j += 32) As[k * la + j] = Ks[j];
+        __syncwarp();
       }
-      if (al) {
-        const int c = lane;
-        for (int k = 0; k < n; ++k) Xs[k * ld + c] = (Ps[k] == c) ? (LUT)1 : (LUT)0;
-        for (int j = 0; j < n; ++j) {
-          const LUT xj = Xs[j * ld + c];
-          for (int i = j + 1; i < n; ++i) Xs[i * ld + c] -= Gs[i * ld + j] * xj;
-        }
-        for (int j = n - 1; j >= 0; --j) {
-          const LUT xj = Xs[j * ld + c] / Gs[j * ld + j];
-          Xs[j * ld + c] = xj;
-          for (int i = 0; i < j; ++i) Xs[i * ld + c] -= Gs[i * ld + j] * xj;
-        }
-      }
-      __syncwarp();
       if (al)
-        for (int j = 0; j < n; ++j) Ig[lane * n + j] = Xs[lane * ld + j];
+        for (int j = 0; j < n; ++j) {
+          const LUT g = As[lane * la + n + j];
+          Xs[lane * ld + j] = g;
+          Ig[lane * n + j] = g;
+        }
+      __syncwarp();
       inv_in = true;
       ++cfact;
     };
@@ -1096,6 +1132,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
       __syncwarp();
       if (lane < NCNT) a.counters[(long)cell * NCNT + lane] = RI[I_CNT0 + lane];
     }
+    drain();   // no copy may still be landing in this warp's shared memory when the next cell starts
     __syncwarp();
   }
 }
@@ -1144,8 +1181,8 @@ RoundBufs carve(const MechLayout& L, void* base, long cap, bool lu64) {
 
 size_t advance_smem(const MechLayout& L, bool lu64) {
   const size_t n = L.nc + 1;
-  return (size_t)kWA * n * (n + 1) * (2 * (lu64 ? sizeof(double) : sizeof(float)) + sizeof(float)) +
-         kWA * 32 * sizeof(int);
+  const size_t lut = lu64 ? sizeof(double) : sizeof(float);
+  return (size_t)kWA * (n * (n + 1) + n * (2 * n + 1) + 2 * n) * lut + (size_t)kWA * n * (n + 1) * sizeof(float);
 }
 
 template <typename LUT, int NM>

@@ -306,10 +306,11 @@ __device__ __forceinline__ void cp_async_el(T* sdst, const T* gsrc) {
   else cp_async4(sdst, gsrc);
 }
 
-// Warp tree sum (every lane receives the total).
-__device__ __forceinline__ double wsum(double v) {
+// Tree sum over a lane group of W lanes (mask gm); every lane receives the total.
+template <int W>
+__device__ __forceinline__ double wsum_g(unsigned gm, double v) {
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+  for (int off = W / 2; off > 0; off >>= 1) v += __shfl_xor_sync(gm, v, off, W);
   return v;
 }
 
@@ -435,28 +436,34 @@ __global__ void __launch_bounds__(kRT) rounds_rhs_kernel(MechLayout Lp, const un
 }
 
 // ---------------------------------------------------------------------------
-// advance: one warp per listed cell; lane k holds component k of every
-// vector.  Consumes the RHS result and runs the solver to its next request.
+// advance: one lane group per listed cell -- a warp, or half a warp when the
+// cell has at most 16 components (two cells per warp) -- lane k of the group
+// holds component k of every vector.  Consumes the RHS result and runs the solver to its next request.
 // ---------------------------------------------------------------------------
-template <typename LUT, int NM>
+template <typename LUT, int W>
 __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, StepOptions o, StepArgs a, RoundBufs B,
                                                                       int par) {
   extern __shared__ __align__(16) unsigned char wsm[];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  constexpr int CPW = 32 / W;   // cells per warp
+  const int wl = threadIdx.x & 31;
+  const int lane = wl & (W - 1);                     // component owned by this thread
+  const int w = (threadIdx.x >> 5) * CPW + wl / W;   // lane group within the block
+  const unsigned gm = W == 32 ? kFull : (0xffffu << (wl & 16));
   const int n = NC + 1, ld = n + 1;
   const RecLayout RL = B.L;
   // per-warp shared memory: G^-1 X[n][ld] (LUT), the Gauss-Jordan work array A[n][2n+1] (LUT), its pivot
   // row K[2n] (LUT) and the Jacobian J[n][ld] (float)
   const int la = 2 * n + 1;
+  constexpr int G = kWA * CPW;   // lane groups per block
   LUT* Xs = (LUT*)wsm + (size_t)w * n * ld;
-  LUT* As = (LUT*)wsm + (size_t)kWA * n * ld + (size_t)w * n * la;
-  LUT* Ks = (LUT*)wsm + (size_t)kWA * n * ld + (size_t)kWA * n * la + (size_t)w * 2 * n;
-  float* Js = (float*)((LUT*)wsm + (size_t)kWA * (n * ld + n * la + 2 * n)) + (size_t)w * n * ld;
+  LUT* As = (LUT*)wsm + (size_t)G * n * ld + (size_t)w * n * la;
+  LUT* Ks = (LUT*)wsm + (size_t)G * n * ld + (size_t)G * n * la + (size_t)w * 2 * n;
+  float* Js = (float*)((LUT*)wsm + (size_t)G * (n * ld + n * la + 2 * n)) + (size_t)w * n * ld;
   const bool al = lane < n;
   const double lo = lane < NC ? 0. : o.y_min_T, hi = lane < NC ? 1. : o.y_max_T;
   const int nact = B.nact[par];
   const int* act = par ? B.act1 : B.act0;
-  for (int widx = blockIdx.x * kWA + w; widx < nact; widx += gridDim.x * kWA) {
+  for (int widx = blockIdx.x * G + w; widx < nact; widx += gridDim.x * G) {
     const int cell = act[widx];
     double* R = B.rec + (long)cell * RL.RS;
     int* RI = (int*)(R + ND_);
@@ -513,7 +520,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
     auto drain = [&]() {
       if (pending) {
         cp_async_wait_all();
-        __syncwarp();
+        __syncwarp(gm);
         pending = false;
         inv_in = j_in = true;
       }
@@ -524,7 +531,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
     auto alfa2 = [&](unsigned k) { return k == 4 ? alfa2_4 : (k == 5 ? alfa2_5 : .8); };
     auto wrms = [&](double xv) {   // OpenSMOKEUtilities.hpp:689-701 (tree-ordered sum)
       const double c = al ? xv * eps : 0.;
-      return sqrt(wsum(c * c) / double(n));
+      return sqrt(wsum_g<W>(gm, c * c) / double(n));
     };
     auto clamp = [&](double y) {
       if (al) {
@@ -538,7 +545,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
       if (!j_in) {
         if (al)
           for (int j = 0; j < n; ++j) Js[lane * ld + j] = Jg[lane * n + j];
-        __syncwarp();
+        __syncwarp(gm);
         j_in = true;
       }
     };
@@ -547,7 +554,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
       if (!inv_in) {
         if (al)
           for (int j = 0; j < n; ++j) Xs[lane * ld + j] = Ig[lane * n + j];
-        __syncwarp();
+        __syncwarp(gm);
         inv_in = true;
       }
     };
@@ -556,15 +563,15 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
     auto rowdot = [&](const auto* M, double y) {
       double s0 = 0., s1 = 0.;
       for (int j = 0; j + 1 < n; j += 2) {
-        const double y0 = __shfl_sync(kFull, y, j);
-        const double y1 = __shfl_sync(kFull, y, j + 1);
+        const double y0 = __shfl_sync(gm, y, j, W);
+        const double y1 = __shfl_sync(gm, y, j + 1, W);
         if (al) {
           s0 += (double)M[lane * ld + j] * y0;
           s1 += (double)M[lane * ld + j + 1] * y1;
         }
       }
       if (n & 1) {
-        const double y0 = __shfl_sync(kFull, y, n - 1);
+        const double y0 = __shfl_sync(gm, y, n - 1, W);
         if (al) s0 += (double)M[lane * ld + n - 1] * y0;
       }
       return s0 + s1;
@@ -601,26 +608,26 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
           As[lane * la + n + j] = (j == lane) ? (LUT)1 : (LUT)0;
         }
       }
-      __syncwarp();
+      __syncwarp(gm);
       for (int k = 0; k < n; ++k) {
         LUT vv = (lane >= k && lane < n) ? (LUT)fabs((double)As[lane * la + k]) : (LUT)-1;
         int r = lane;
-        for (int off = 16; off > 0; off >>= 1) {
-          const LUT ov = __shfl_xor_sync(kFull, vv, off);
-          const int orr = __shfl_xor_sync(kFull, r, off);
+        for (int off = W / 2; off > 0; off >>= 1) {
+          const LUT ov = __shfl_xor_sync(gm, vv, off, W);
+          const int orr = __shfl_xor_sync(gm, r, off, W);
           if (ov > vv || (ov == vv && orr < r)) { vv = ov; r = orr; }
         }
-        r = __shfl_sync(kFull, r, 0);
+        r = __shfl_sync(gm, r, 0, W);
         if (r < k || r >= n) r = k;   // a NaN column cannot send the pivot outside rows k..n-1
         // swap rows k and r and scale the pivot row into K (lanes = columns)
         const LUT pv = As[r * la + k];
         const LUT ipv = (pv != (LUT)0) ? (LUT)1 / pv : (LUT)0;
-        for (int j = lane; j < m2; j += 32) {
+        for (int j = lane; j < m2; j += W) {
           const LUT ak = As[k * la + j], ar = As[r * la + j];
           Ks[j] = ar * ipv;
           if (r != k) As[r * la + j] = ak;
         }
-        __syncwarp();
+        __syncwarp(gm);
         // eliminate column k from every other row (lane = row)
         if (al && lane != k) {
           const LUT fct = As[lane * la + k];
@@ -636,9 +643,9 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
           }
           for (; j < m2; ++j) Ai[j] = Ai[j] - fct * Ks[j];
         }
-        __syncwarp();
-        for (int j = lane; j < m2; j += 32) As[k * la + j] = Ks[j];
-        __syncwarp();
+        __syncwarp(gm);
+        for (int j = lane; j < m2; j += W) As[k * la + j] = Ks[j];
+        __syncwarp(gm);
       }
       if (al)
         for (int j = 0; j < n; ++j) {
@@ -646,7 +653,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
           Xs[lane * ld + j] = g;
           Ig[lane * n + j] = g;
         }
-      __syncwarp();
+      __syncwarp(gm);
       inv_in = true;
       ++cfact;
     };
@@ -662,7 +669,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
       case PH_INIT: {
         // MultiValueSolver::Solve, first call (:445-469)
         const bool illegal = al && (va < lo || va > hi);
-        if (__any_sync(kFull, illegal)) { status = -9; lab = L_FINISH; break; }
+        if (__any_sync(gm, illegal)) { status = -9; lab = L_FINISH; break; }
         eps = al ? 1. / (o.atol + o.rtol * fabs(va)) : 0.;
         double lo0, hi0;
         if (t0 != 0.) { lo0 = 100. * kMachEpsDouble * fabs(t0); hi0 = fabs(t0); }
@@ -823,8 +830,8 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
         }
         case L_JAC_COLUMN: {
           // KernelDense::NumericalJacobian, constrained branch: increment of column jcol
-          const double yh = __shfl_sync(kFull, vb, jcol);
-          const double ej = __shfl_sync(kFull, eps, jcol);
+          const double yh = __shfl_sync(gm, vb, jcol, W);
+          const double ej = __shfl_sync(gm, eps, jcol, W);
           const double aa = fabs(yh), bb = fabs(1. / ej);
           hJ = sqrt(kMachEpsDouble) * (aa > bb ? aa : bb);
           hJ = fmax(hJ, hf / ej);
@@ -968,8 +975,8 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
               load_j();
               const double s = rowdot(Js, v[0] - z[0]);
               const double vr = v[1] - (s * h + z[1]);
-              const double normd = wsum(al ? fabs(vr) : 0.);
-              const double normf = wsum(al ? fabs(v[1]) : 0.);
+              const double normd = wsum_g<W>(gm, al ? fabs(vr) : 0.);
+              const double normf = wsum_g<W>(gm, al ? fabs(v[1]) : 0.);
               if (normd > 3. * normf + .1 && iterConvergence > 2) {
                 if (numberOfSteps > stepOfLastJacobian + 5u) jacobianChange = 1;
                 hScale = 0.5; odeHStatus = H_DEC; hNextStep = h * hScale;
@@ -1081,7 +1088,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
         }
         case L_FINISH: {
           // utilities.H:153-200 and the scatter of chemistry_DI.H:221-235
-          const double s = wsum(lane < NC ? va : 0.);
+          const double s = wsum_g<W>(gm, lane < NC ? va : 0.);
           if (lane < NC) a.Y[(long)lane * a.ld + cell] = va / s;
           if (o.energy && lane == NC) a.T[cell] = va;
           if (lane == 0) {
@@ -1129,11 +1136,11 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
       RI[I_CNT0 + CNT_SOLVE] += csolve; RI[I_CNT0 + CNT_ERRFAIL] += cerr; RI[I_CNT0 + CNT_CONVFAIL] += cconv;
     }
     if (phase == PH_DONE && a.counters) {
-      __syncwarp();
+      __syncwarp(gm);
       if (lane < NCNT) a.counters[(long)cell * NCNT + lane] = RI[I_CNT0 + lane];
     }
     drain();   // no copy may still be landing in this warp's shared memory when the next cell starts
-    __syncwarp();
+    __syncwarp(gm);
   }
 }
 
@@ -1181,8 +1188,9 @@ RoundBufs carve(const MechLayout& L, void* base, long cap, bool lu64) {
 
 size_t advance_smem(const MechLayout& L, bool lu64) {
   const size_t n = L.nc + 1;
+  const size_t groups = (size_t)kWA * (n <= 16 ? 2 : 1);
   const size_t lut = lu64 ? sizeof(double) : sizeof(float);
-  return (size_t)kWA * (n * (n + 1) + n * (2 * n + 1) + 2 * n) * lut + (size_t)kWA * n * (n + 1) * sizeof(float);
+  return groups * (n * (n + 1) + n * (2 * n + 1) + 2 * n) * lut + groups * n * (n + 1) * sizeof(float);
 }
 
 template <typename LUT, int NM>

@@ -38,6 +38,48 @@ UNIT = "cells*steps/s"
 TRANSCENDENTAL_FLOPS = 20.0   # FP64-instruction equivalent charged per exp/log/pow in the work model
 
 
+# Algorithmic bytes per unit of each kernel kind (what the algorithm must move
+# through HBM, not what a kernel happens to move):
+#   plain (one launch = the whole step of every cell): read Y,T and write Y,T,
+#     status of every cell: 2 (n) 8 + 8 bytes per cell (n = species + 1);
+#   advance (per cell-round): read the cell's solver record -- scalar state
+#     (18 doubles + 32 ints), z and v (16 n doubles), b, f, f0, va, vb, eps
+#     (6 n doubles) -- and write it back without f, f0: (42 n) 8 + 2 * 272 bytes;
+#   rhs (per cell-round): read y (n doubles), write f (n doubles), QR and the
+#     phase/counter words: 2 n 8 + 16 bytes.
+# A cell-round is one RHS evaluation of one cell: the per-cell counters give
+# their number (rhs + jacobian-column rhs).
+def kernel_roofline(args, ktimes, counters, nc, ncells, hbm, peak_src):
+    n = nc + 1
+    cell_rounds = float(counters[:, 1].sum() + counters[:, 7].sum())
+    per_unit = {"plain": 2 * n * 8 + 8, "advance": 42 * n * 8 + 2 * 272, "rhs": 2 * n * 8 + 16}
+    units = {"plain": float(ncells), "advance": cell_rounds, "rhs": cell_rounds}
+    timed = {k: v for k, v in ktimes.items() if v[1] > 0}
+    if not timed:
+        return None
+    dom = max(timed, key=lambda k: timed[k][0])
+    ms, nl = timed[dom]
+    steps_launches = nl / max(args.steps, 1)          # launches of this kernel per step
+    alg = per_unit.get(dom, 0) * units.get(dom, 0.) / max(steps_launches, 1)   # bytes per launch
+    avg_s = ms / nl / 1e3
+    achieved = alg / avg_s / 1e9 if avg_s > 0 else None
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            with open(tfile) as f:
+                tr = json.load(f).get(args.form + ("" if args.form == "plain" else "_" + args.factors), {})
+            if tr.get("kernel") == dom and tr.get("bytes_per_unit"):
+                traffic = tr["bytes_per_unit"] * units[dom] / max(steps_launches, 1)
+        except (OSError, ValueError):
+            traffic = None
+    return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm if achieved else None, "traffic": traffic,
+            "kernel": dom, "launch_ms": avg_s * 1e3, "algorithmic_bytes_per_launch": alg,
+            "peak_source": peak_src,
+            "note": "latency-bound BDF solver kernel; bytes are its solver-record traffic"}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -199,7 +241,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     from laminarsmoke_b200 import mech
     data = mech.load("h2co")[0]
     m = lsg.Mechanism(data, device=local_rank)
-    plain = lsg.ReactionStep(m, tile=lsg.LSG_TILE_WARP, precision=lsg.LSG_PRECISION_FP64)
+    plain = lsg.ReactionStep(m, tile=lsg.LSG_TILE_WARP, precision=lsg.LSG_PRECISION_FP64,
+                             kernel_timing=int(args.form == "plain"))
 
     def pool_gpu(Yp, Tp, dt):
         Yd = torch.tensor(np.ascontiguousarray(Yp.T), device=dev)
@@ -214,12 +257,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if args.form == "mixed":
         tile = lsg.LSG_TILE_LANE if args.tile == "lane" else lsg.LSG_TILE_PERSISTENT
         prec = lsg.LSG_PRECISION_MIXED if args.factors == "fp32" else lsg.LSG_PRECISION_FP64
-        ctx = lsg.ReactionStep(m, tile=tile, precision=prec)
-        kernel_name = "rounds_*" if args.tile == "lane" else "batched_kernel"
+        ctx = lsg.ReactionStep(m, tile=tile, precision=prec, kernel_timing=1)
         dtype = "f64+f32" if args.factors == "fp32" else "f64"
     else:
         ctx = plain
-        kernel_name, dtype = "plain_warp_kernel", "f64"
+        dtype = "f64"
     Y0 = torch.tensor(np.ascontiguousarray(Y.T), device=dev)
     T0 = torch.tensor(T, device=dev)
     Yw = torch.empty_like(Y0)
@@ -249,10 +291,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dist.barrier()
     torch.cuda.synchronize()
     l0 = ctx.launches()
+    ctx.kernel_times(reset=True)
     with ClockSampler(local_rank) as clk:
         evs = [one() for _ in range(args.steps)]
         torch.cuda.synchronize()
     launches = ctx.launches() - l0
+    ktimes = ctx.kernel_times(reset=True)
     if world > 1:
         dist.barrier()
     ms = float(sum(a.elapsed_time(b) for a, b in evs))
@@ -299,17 +343,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         hbm = peaks.get("hbm_gbs")
         peak_src = "measured" if hbm else "fallback"
         hbm = hbm or 6650.0
-        # algorithmic bytes of one launch: read Y,T and write Y,T,status of every cell (SURVEY work unit 2n*8+8)
-        alg_bytes = n * (2 * (nc + 1) * 8 + 8)
-        achieved_gbs = alg_bytes / (ms_per_step / 1e3) / 1e9
-        traffic = None
-        tfile = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tfile):
-            try:
-                with open(tfile) as f:
-                    traffic = json.load(f).get(args.form)
-            except (OSError, ValueError):
-                traffic = None
+        roofline = kernel_roofline(args, ktimes, counters, nc, n, hbm, peak_src)
         cpu = cpu_baseline(data, Y, T, args.cpu_sample)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -323,10 +357,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                              if args.form == "mixed" else "fp64",
                        "l2": "flushed (1 GiB write) between timed steps; inputs restored from HBM copy",
                        "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved_gbs / hbm, "traffic": traffic,
-                         "kernel": kernel_name, "peak_source": peak_src,
-                         "note": "FP64-latency-bound BDF solver; HBM is not the binding resource"},
+            "roofline": roofline,
+            "kernel_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in ktimes.items() if v[1]},
             "fp64_work": {"algorithmic_tflops": flops / (ms_per_step / 1e3) / 1e12 if ms_per_step > 0 else None,
                           "flops_per_cell_step": flops / n,
                           "bdf_steps_per_cell": nsteps_total / n,

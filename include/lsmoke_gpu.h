@@ -79,7 +79,8 @@ typedef struct lsg_options {
   double alfa2_5;
   int maximum_order;
   int tile;             /* LSG_TILE_* */
-  int reserved[6];
+  int kernel_timing;    /* 1: time every kernel kind with CUDA events (lsg_ctx_kernel_times) */
+  int reserved[5];
 } lsg_options;
 
 void lsg_options_default(lsg_options* opt);
@@ -133,6 +134,15 @@ void* lsg_ctx_stream(lsg_ctx* ctx);
 /* Number of kernels this context has enqueued so far (diagnostics; no
  * counterpart in the reference). */
 long long lsg_ctx_launches(const lsg_ctx* ctx);
+
+/* Device time per kernel kind, from CUDA events recorded on the launching
+ * stream when lsg_options.kernel_timing is set (diagnostics; no counterpart in
+ * the reference).  Kinds: 0 RHS, 1 solver advance, 2 compaction, 3 round
+ * initialisation (lane-per-cell form), 4 plain warp kernel, 5 persistent lane
+ * kernel.  ms[k] total milliseconds, launches[k] timed launches; reset != 0
+ * clears the totals after reading.  Waits for the last timed kernel. */
+#define LSG_NKERNEL_KINDS 6
+int lsg_ctx_kernel_times(lsg_ctx* ctx, double* ms, long long* launches, int nkinds, int reset);
 
 /* Waits for the device, then reads and clears the error flags kernels raised
  * (0 = none).  Returns LSG_ERR_DEVICE when a flag was set. */

@@ -48,6 +48,7 @@ struct lsg_ctx {
   int rplan_lu64 = -1;
   int* nact_host = nullptr;   // pinned
   long long launches = 0;     // kernels enqueued by this context
+  KernelTimer timer;          // per-kernel device time (lsg_options.kernel_timing)
 };
 
 namespace {
@@ -168,6 +169,19 @@ int ensure_batched(lsg_ctx* c, bool lu64) {
   return LSG_OK;
 }
 
+// Creates the timing events the first time kernel timing is switched on.
+void apply_timing(lsg_ctx* c) {
+  if (c->opt.kernel_timing && !c->timer.on) {
+    bool ok = true;
+    for (cudaEvent_t& e : c->timer.ev)
+      if (!e && cudaEventCreate(&e) != cudaSuccess) ok = false;
+    c->timer.on = ok;
+    if (!ok) cudaGetLastError();
+  } else if (!c->opt.kernel_timing) {
+    c->timer.on = false;
+  }
+}
+
 int sm_count(lsg_ctx* c) {
   if (!c->sm_count &&
       cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess)
@@ -211,14 +225,20 @@ int launch_step(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
     if (r != LSG_OK) return r;
     const long max_rounds = 4L * (long)c->opt.max_steps * (L.nc + 9) + 64;
     const cudaError_t e = launch_rounds(c->rplan, L, c->mech->d_buf, so, a, c->rstate, c->rcap, c->nact_host,
-                                        max_rounds, c->d_err, s, &c->launches);
+                                        max_rounds, c->d_err, s, &c->launches, &c->timer);
     if (e == cudaErrorLaunchTimeout) return LSG_ERR_DEVICE;
     return e == cudaSuccess ? LSG_OK : LSG_ERR_CUDA;
   }
   if (tile == LSG_TILE_WARP) {
     if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
     if (plain_smem_bytes(L) > 227 * 1024) return LSG_ERR_UNSUPPORTED;
+    if (c->timer.used >= KernelTimer::kPairs) {
+      cudaStreamSynchronize(s);
+      c->timer.collect();
+    }
+    c->timer.begin(KT_PLAIN, s);
     if (launch_plain(L, c->mech->d_buf, so, a, c->d_err, s) != cudaSuccess) return LSG_ERR_CUDA;
+    c->timer.end(s);
     c->launches += 1;
     return LSG_OK;
   }
@@ -227,9 +247,15 @@ int launch_step(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
   const int r = ensure_batched(c, lu64);
   if (r != LSG_OK) return r;
   if (cudaMemsetAsync(c->queue, 0, sizeof(int), s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (c->timer.used >= KernelTimer::kPairs) {
+    cudaStreamSynchronize(s);
+    c->timer.collect();
+  }
+  c->timer.begin(KT_PERSISTENT, s);
   if (launch_batched(L, c->mech->d_buf, so, a, c->slots, c->nslots, nullptr, c->queue, lu64, c->d_err, s) !=
       cudaSuccess)
     return LSG_ERR_CUDA;
+  c->timer.end(s);
   c->launches += 1;
   return LSG_OK;
 }
@@ -330,6 +356,7 @@ int lsg_ctx_create(const lsg_mech* mech, const lsg_options* opt, int device, lsg
   if (!c) return LSG_ERR_NOMEM;
   c->mech = mech;
   c->opt = o;
+  apply_timing(c);
   c->device = device;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess || cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess) {
@@ -347,6 +374,7 @@ int lsg_ctx_set_options(lsg_ctx* c, const lsg_options* opt) {
   const int v = validate_options(opt);
   if (v != LSG_OK) return v;
   c->opt = *opt;
+  apply_timing(c);
   return LSG_OK;
 }
 
@@ -360,6 +388,8 @@ int lsg_ctx_destroy(lsg_ctx* c) {
   cudaFree(c->rstate);
   if (c->nact_host) cudaFreeHost(c->nact_host);
   cudaFree(c->d_err);
+  for (cudaEvent_t& e : c->timer.ev)
+    if (e) cudaEventDestroy(e);
   cudaStreamDestroy(c->stream);
   delete c;
   return LSG_OK;
@@ -368,6 +398,25 @@ int lsg_ctx_destroy(lsg_ctx* c) {
 void* lsg_ctx_stream(lsg_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 long long lsg_ctx_launches(const lsg_ctx* c) { return c ? c->launches : -1; }
+
+int lsg_ctx_kernel_times(lsg_ctx* c, double* ms, long long* launches, int nkinds, int reset) {
+  if (!c || nkinds < 0) return LSG_ERR_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  if (c->timer.used > 0) {
+    if (cudaEventSynchronize(c->timer.ev[2 * c->timer.used - 1]) != cudaSuccess) return LSG_ERR_CUDA;
+    c->timer.collect();
+  }
+  for (int k = 0; k < nkinds && k < KT_NKINDS; ++k) {
+    if (ms) ms[k] = c->timer.ms[k];
+    if (launches) launches[k] = c->timer.n[k];
+  }
+  if (reset)
+    for (int k = 0; k < KT_NKINDS; ++k) {
+      c->timer.ms[k] = 0.;
+      c->timer.n[k] = 0;
+    }
+  return LSG_OK;
+}
 
 int lsg_ctx_check(lsg_ctx* c, int* flags) {
   if (!c) return LSG_ERR_ARG;

@@ -61,6 +61,40 @@ cudaError_t launch_batched_noalloc(const MechLayout& L, const unsigned char* mec
                                    const StepArgs& a, bool lu64, int device, long nslots, int* host_flags,
                                    cudaStream_t stream);
 
+// Optional device timing of each kernel kind with CUDA events recorded on the
+// launching stream (lsg_options.kernel_timing).  Pairs are collected after the
+// stream has been synchronised.
+enum { KT_RHS = 0, KT_ADVANCE, KT_COMPACT, KT_INIT, KT_PLAIN, KT_PERSISTENT, KT_NKINDS };
+struct KernelTimer {
+  static constexpr int kPairs = 64;
+  bool on = false;
+  cudaEvent_t ev[2 * kPairs] = {};
+  int kind[kPairs] = {};
+  int used = 0;
+  double ms[KT_NKINDS] = {};
+  long long n[KT_NKINDS] = {};
+  void begin(int k, cudaStream_t s) {
+    if (!on || used >= kPairs) return;
+    kind[used] = k;
+    cudaEventRecord(ev[2 * used], s);
+  }
+  void end(cudaStream_t s) {
+    if (!on || used >= kPairs) return;
+    cudaEventRecord(ev[2 * used + 1], s);
+    ++used;
+  }
+  void collect() {   // the stream the events were recorded on has been synchronised
+    for (int i = 0; i < used; ++i) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]) == cudaSuccess) {
+        ms[kind[i]] += t;
+        n[kind[i]] += 1;
+      }
+    }
+    used = 0;
+  }
+};
+
 // Round scheme (lsg_rounds.cu): launch geometry chosen once per context.
 struct RoundsPlan {
   bool lu64;
@@ -72,7 +106,8 @@ cudaError_t upload_gear_rounds(const GearConsts& gc);
 cudaError_t rounds_prepare(const MechLayout& L, bool lu64, int sm_count, RoundsPlan* plan);
 cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsigned char* mech_gmem,
                           const StepOptions& o, const StepArgs& a, void* state, long ns, int* nact_host,
-                          long max_rounds, int* err, cudaStream_t stream, long long* launches);
+                          long max_rounds, int* err, cudaStream_t stream, long long* launches,
+                          KernelTimer* timer);
 cudaError_t launch_rhs_warp(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y,
                             double* dy, long ld, double p, int energy, double* qr, int* err, cudaStream_t stream);
 

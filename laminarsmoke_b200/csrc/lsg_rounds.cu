@@ -306,6 +306,77 @@ __device__ __forceinline__ void cp_async_el(T* sdst, const T* gsrc) {
   else cp_async4(sdst, gsrc);
 }
 
+// One out-of-line copy of pow for the step-size selection (keeps the solver
+// kernel's instruction footprint small).
+__device__ __noinline__ double pow_ol(double x, double y) { return pow(x, y); }
+
+// G^-1 for G = I - hr0 J by Gauss-Jordan elimination on [G | I] with partial
+// pivoting on the largest magnitude, first occurrence -- the pivots of the
+// partial-pivot LU of KernelDense::BuildAndFactorizeMatrixG.  Lane i of the
+// group owns row i; each step's updates are independent and loaded in chunks of
+// 4.  Js: J rows (shared), As/Ks: work arrays, Xs: G^-1 (shared), Ig: G^-1 in
+// the cell record.  Out of line: one copy serves every call site.
+template <typename LUT, int W>
+__device__ __noinline__ void gj_inverse(const float* Js, LUT* As, LUT* Ks, LUT* Xs, LUT* Ig, double hr0, int n,
+                                        int lane, unsigned gm) {
+  const int ld = n + 1, la = 2 * n + 1, m2 = 2 * n;
+  const bool al = lane < n;
+  if (al) {
+    for (int j = 0; j < n; ++j) {
+      double g = -hr0 * (double)Js[lane * ld + j];
+      if (j == lane) g += 1.;
+      As[lane * la + j] = (LUT)g;
+      As[lane * la + n + j] = (j == lane) ? (LUT)1 : (LUT)0;
+    }
+  }
+  __syncwarp(gm);
+  for (int k = 0; k < n; ++k) {
+    LUT vv = (lane >= k && lane < n) ? (LUT)fabs((double)As[lane * la + k]) : (LUT)-1;
+    int r = lane;
+    for (int off = W / 2; off > 0; off >>= 1) {
+      const LUT ov = __shfl_xor_sync(gm, vv, off, W);
+      const int orr = __shfl_xor_sync(gm, r, off, W);
+      if (ov > vv || (ov == vv && orr < r)) { vv = ov; r = orr; }
+    }
+    r = __shfl_sync(gm, r, 0, W);
+    if (r < k || r >= n) r = k;   // a NaN column cannot send the pivot outside rows k..n-1
+    // swap rows k and r and scale the pivot row into K (lanes = columns)
+    const LUT pv = As[r * la + k];
+    const LUT ipv = (pv != (LUT)0) ? (LUT)1 / pv : (LUT)0;
+    for (int j = lane; j < m2; j += W) {
+      const LUT ak = As[k * la + j], ar = As[r * la + j];
+      Ks[j] = ar * ipv;
+      if (r != k) As[r * la + j] = ak;
+    }
+    __syncwarp(gm);
+    // eliminate column k from every other row (lane = row)
+    if (al && lane != k) {
+      const LUT fct = As[lane * la + k];
+      LUT* Ai = As + lane * la;
+      int j = k;
+      for (; j + 4 <= m2; j += 4) {
+        const LUT a0 = Ai[j], a1 = Ai[j + 1], a2 = Ai[j + 2], a3 = Ai[j + 3];
+        const LUT k0 = Ks[j], k1 = Ks[j + 1], k2 = Ks[j + 2], k3 = Ks[j + 3];
+        Ai[j] = a0 - fct * k0;
+        Ai[j + 1] = a1 - fct * k1;
+        Ai[j + 2] = a2 - fct * k2;
+        Ai[j + 3] = a3 - fct * k3;
+      }
+      for (; j < m2; ++j) Ai[j] = Ai[j] - fct * Ks[j];
+    }
+    __syncwarp(gm);
+    for (int j = lane; j < m2; j += W) As[k * la + j] = Ks[j];
+    __syncwarp(gm);
+  }
+  if (al)
+    for (int j = 0; j < n; ++j) {
+      const LUT g = As[lane * la + n + j];
+      Xs[lane * ld + j] = g;
+      Ig[lane * n + j] = g;
+    }
+  __syncwarp(gm);
+}
+
 // Tree sum over a lane group of W lanes (mask gm); every lane receives the total.
 template <int W>
 __device__ __forceinline__ double wsum_g(unsigned gm, double v) {
@@ -593,67 +664,9 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
       ++csolve;
       return xv;
     };
-    // G^-1 for G = I - hr0 J by Gauss-Jordan elimination on [G | I] with partial
-    // pivoting on the largest magnitude, first occurrence -- the pivots of the
-    // partial-pivot LU of KernelDense::BuildAndFactorizeMatrixG.  Lane i owns
-    // row i; each step's updates are independent and loaded in chunks of 4.
     auto factorize = [&]() {
       load_j();
-      const int m2 = 2 * n;
-      if (al) {
-        for (int j = 0; j < n; ++j) {
-          double g = -hr0f * (double)Js[lane * ld + j];
-          if (j == lane) g += 1.;
-          As[lane * la + j] = (LUT)g;
-          As[lane * la + n + j] = (j == lane) ? (LUT)1 : (LUT)0;
-        }
-      }
-      __syncwarp(gm);
-      for (int k = 0; k < n; ++k) {
-        LUT vv = (lane >= k && lane < n) ? (LUT)fabs((double)As[lane * la + k]) : (LUT)-1;
-        int r = lane;
-        for (int off = W / 2; off > 0; off >>= 1) {
-          const LUT ov = __shfl_xor_sync(gm, vv, off, W);
-          const int orr = __shfl_xor_sync(gm, r, off, W);
-          if (ov > vv || (ov == vv && orr < r)) { vv = ov; r = orr; }
-        }
-        r = __shfl_sync(gm, r, 0, W);
-        if (r < k || r >= n) r = k;   // a NaN column cannot send the pivot outside rows k..n-1
-        // swap rows k and r and scale the pivot row into K (lanes = columns)
-        const LUT pv = As[r * la + k];
-        const LUT ipv = (pv != (LUT)0) ? (LUT)1 / pv : (LUT)0;
-        for (int j = lane; j < m2; j += W) {
-          const LUT ak = As[k * la + j], ar = As[r * la + j];
-          Ks[j] = ar * ipv;
-          if (r != k) As[r * la + j] = ak;
-        }
-        __syncwarp(gm);
-        // eliminate column k from every other row (lane = row)
-        if (al && lane != k) {
-          const LUT fct = As[lane * la + k];
-          LUT* Ai = As + lane * la;
-          int j = k;
-          for (; j + 4 <= m2; j += 4) {
-            const LUT a0 = Ai[j], a1 = Ai[j + 1], a2 = Ai[j + 2], a3 = Ai[j + 3];
-            const LUT k0 = Ks[j], k1 = Ks[j + 1], k2 = Ks[j + 2], k3 = Ks[j + 3];
-            Ai[j] = a0 - fct * k0;
-            Ai[j + 1] = a1 - fct * k1;
-            Ai[j + 2] = a2 - fct * k2;
-            Ai[j + 3] = a3 - fct * k3;
-          }
-          for (; j < m2; ++j) Ai[j] = Ai[j] - fct * Ks[j];
-        }
-        __syncwarp(gm);
-        for (int j = lane; j < m2; j += W) As[k * la + j] = Ks[j];
-        __syncwarp(gm);
-      }
-      if (al)
-        for (int j = 0; j < n; ++j) {
-          const LUT g = As[lane * la + n + j];
-          Xs[lane * ld + j] = g;
-          Ig[lane * n + j] = g;
-        }
-      __syncwarp(gm);
+      gj_inverse<LUT, W>(Js, As, Ks, Xs, Ig, hr0f, n, lane, gm);
       inv_in = true;
       ++cfact;
     };
@@ -944,12 +957,12 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
               break;
             }
             hScaleMax = 1.;
-            hCur = 0.8 * pow(1. / hCur, 1. / double(p + 1));
+            hCur = 0.8 * pow_ol(1. / hCur, 1. / double(p + 1));
             hScale = hCur;
             if (p > 1u) {
               double hMinus = c_gear_r.Ep[p - 1] * wrms(get8(v, p));
               hMinus = 1. / (hMinus + kMachEpsFloat);
-              hMinus = 0.8 * pow(hMinus, 1. / double(p));
+              hMinus = 0.8 * pow_ol(hMinus, 1. / double(p));
               if (hMinus > hCur) { hScale = hMinus; p -= 1; odeOrderStatus = O_DEC; }
             }
             hScale = fmin(hScale, 0.5);
@@ -1006,16 +1019,16 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
                 hMinus = c_gear_r.Ep[p - 1] * wrms(get8(v, p)) + kMachEpsFloat;
                 hMinus = 1. / hMinus;
                 alfa1 = alfa2(p - 1) - .05;
-                hMinus = alfa1 * pow(hMinus, 1. / double(p));
+                hMinus = alfa1 * pow_ol(hMinus, 1. / double(p));
               }
               hC = c_gear_r.Ep[p] * wrms(get8(v, p + 1)) + kMachEpsFloat;
               hC = 1. / hC;
-              hC = alfa2(p) * pow(hC, 1. / double(p + 1));
+              hC = alfa2(p) * pow_ol(hC, 1. / double(p + 1));
               if (p < maximum_order && odeOrderStatus != O_DEC) {
                 hPlus = c_gear_r.Ep[p + 1] * wrms(get8(v, p + 2)) + kMachEpsFloat;
                 hPlus = 1. / hPlus;
                 alfa3 = alfa2(p + 1) - .25;
-                hPlus = alfa3 * pow(hPlus, 1. / double(p + 2));
+                hPlus = alfa3 * pow_ol(hPlus, 1. / double(p + 2));
               }
               if (hMinus > hC && hMinus > hPlus) {
                 hScale = (.75 / alfa1) * hMinus; orderInNextStep = p - 1; odeOrderStatus = O_DEC;
@@ -1239,12 +1252,15 @@ cudaError_t rounds_prepare(const MechLayout& L, bool lu64, int sm_count, RoundsP
 
 cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsigned char* mech_gmem,
                           const StepOptions& o, const StepArgs& a, void* state, long cap, int* nact_host,
-                          long max_rounds, int* err, cudaStream_t stream, long long* launches) {
+                          long max_rounds, int* err, cudaStream_t stream, long long* launches,
+                          KernelTimer* kt) {
   // nact_host: two pinned ints (list length, error flags); launches: kernels enqueued (added to)
   const int n = L.nc + 1;
   if (n > 32 || a.ncells > cap || a.ncells <= 0) return cudaErrorInvalidValue;
   const RoundBufs B = carve(L, state, cap, P.lu64);
+  kt->begin(KT_INIT, stream);
   rounds_init_kernel<<<P.g_init, kAT, 0, stream>>>(L.nc, o, a, B);
+  kt->end(stream);
   *launches += 1;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -1252,8 +1268,11 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
   int par = 0;
   for (long round = 0; round < max_rounds; round += kBatch) {
     for (int r = 0; r < kBatch; ++r) {
+      kt->begin(KT_RHS, stream);
       rounds_rhs_kernel<<<P.g_rhs, kRT, P.rhs_smem, stream>>>(L, mech_gmem, o.energy, a.p, B, par, err);
+      kt->end(stream);
       const dim3 ga(P.g_adv), ta(kWA * 32);
+      kt->begin(KT_ADVANCE, stream);
       if (P.lu64) {
         if (n <= 16) rounds_advance_kernel<double, 16><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
         else rounds_advance_kernel<double, 32><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
@@ -1261,7 +1280,10 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
         if (n <= 16) rounds_advance_kernel<float, 16><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
         else rounds_advance_kernel<float, 32><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
       }
+      kt->end(stream);
+      kt->begin(KT_COMPACT, stream);
       rounds_compact_kernel<<<P.g_cmp, kCT, 0, stream>>>(B, par);
+      kt->end(stream);
       *launches += 3;
       par ^= 1;
     }
@@ -1273,6 +1295,7 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
     if (e != cudaSuccess) return e;
     e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return e;
+    kt->collect();
     if (nact_host[0] == 0) return cudaSuccess;
     if (nact_host[1] != 0) return cudaErrorLaunchTimeout;   // a kernel raised a flag: stop, the caller reports it
   }

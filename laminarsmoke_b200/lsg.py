@@ -38,7 +38,7 @@ class Options(C.Structure):
                 ("max_steps", C.c_int), ("full_pivoting", C.c_int), ("energy", C.c_int),
                 ("precision", C.c_int),
                 ("alfa2_4", C.c_double), ("alfa2_5", C.c_double), ("maximum_order", C.c_int),
-                ("tile", C.c_int), ("reserved", C.c_int * 6)]
+                ("tile", C.c_int), ("kernel_timing", C.c_int), ("reserved", C.c_int * 5)]
 
 
 EXPORTS = (
@@ -46,7 +46,7 @@ EXPORTS = (
     "lsg_mech_destroy", "lsg_ctx_create", "lsg_ctx_set_options", "lsg_ctx_destroy",
     "lsg_reaction_step", "lsg_reaction_step_device", "lsg_ctx_check", "lsg_rhs_device",
     "lsg_strerror", "lsg_abi_version", "lsg_ctx_stream", "lsg_ctx_launches",
-    "lsg_reaction_step_device_noalloc",
+    "lsg_reaction_step_device_noalloc", "lsg_ctx_kernel_times",
 )
 
 _lib = None
@@ -80,6 +80,7 @@ def lib():
     L.lsg_ctx_stream.restype = vp
     L.lsg_reaction_step_device_noalloc.argtypes = [vp, C.POINTER(Options), i, i, vp, l, vp, d, d, vp, d, vp,
                                                    vp, vp, vp, vp]
+    L.lsg_ctx_kernel_times.argtypes = [vp, vp, vp, i, i]
     L.lsg_ctx_launches.argtypes = [vp]
     L.lsg_ctx_launches.restype = C.c_longlong
     _lib = L
@@ -217,6 +218,18 @@ class ReactionStep:
     def launches(self) -> int:
         """Kernels this context has enqueued so far."""
         return int(lib().lsg_ctx_launches(self.h))
+
+    KERNEL_KINDS = ("rhs", "advance", "compact", "init", "plain", "persistent")
+
+    def kernel_times(self, reset: bool = False) -> dict:
+        """{kind: (total ms, timed launches)} from the CUDA events recorded when
+        the context was created with kernel_timing=1."""
+        nk = len(self.KERNEL_KINDS)
+        ms = (C.c_double * nk)()
+        nl = (C.c_longlong * nk)()
+        _check(lib().lsg_ctx_kernel_times(self.h, C.cast(ms, C.c_void_p), C.cast(nl, C.c_void_p), nk, int(reset)),
+               "lsg_ctx_kernel_times")
+        return {k: (ms[i], nl[i]) for i, k in enumerate(self.KERNEL_KINDS)}
 
     def check(self):
         f = C.c_int()

@@ -26,6 +26,8 @@
 // BatchReactorHomogeneousConstantPressure.H:175-223.  With FP32 factors every
 // linear solve is refined against its FP64 residual (the matrix rebuilt in FP64
 // from the stored Jacobian) until it equals the FP64 solve to rounding.
+#include <type_traits>
+
 #include "lsg_common.cuh"
 #include "lsg_kernels.h"
 
@@ -385,6 +387,34 @@ __device__ __forceinline__ double wsum_g(unsigned gm, double v) {
   return v;
 }
 
+// Weighted RMS norm over the group (OpenSMOKEUtilities.hpp:689-701, tree-ordered sum); out of line.
+template <int W>
+__device__ __noinline__ double wrms_ol(double x, double e, bool al, int n, unsigned gm) {
+  const double c = al ? x * e : 0.;
+  return sqrt(wsum_g<W>(gm, c * c) / double(n));
+}
+
+// sum_j M[lane][j] * y_j (M row-major in shared memory, leading dimension ld); the broadcasts do not
+// depend on each other.  Out of line.
+template <typename T, int W>
+__device__ __noinline__ double rowdot_ol(const T* M, double y, int n, int ld, int lane, unsigned gm) {
+  const bool al = lane < n;
+  double s0 = 0., s1 = 0.;
+  for (int j = 0; j + 1 < n; j += 2) {
+    const double y0 = __shfl_sync(gm, y, j, W);
+    const double y1 = __shfl_sync(gm, y, j + 1, W);
+    if (al) {
+      s0 += (double)M[lane * ld + j] * y0;
+      s1 += (double)M[lane * ld + j + 1] * y1;
+    }
+  }
+  if (n & 1) {
+    const double y0 = __shfl_sync(gm, y, n - 1, W);
+    if (al) s0 += (double)M[lane * ld + n - 1] * y0;
+  }
+  return s0 + s1;
+}
+
 // a[i] for a runtime index 0 <= i < 8 without local-memory indexing
 __device__ __forceinline__ double get8(const double (&a)[8], unsigned i) {
   double r = a[0];
@@ -600,10 +630,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
     enum : int { H_DEC = 0, H_CONST = 1, H_INC = 2 };
     enum : int { O_DEC = 0, O_CONST = 1, O_INC = 2 };
     auto alfa2 = [&](unsigned k) { return k == 4 ? alfa2_4 : (k == 5 ? alfa2_5 : .8); };
-    auto wrms = [&](double xv) {   // OpenSMOKEUtilities.hpp:689-701 (tree-ordered sum)
-      const double c = al ? xv * eps : 0.;
-      return sqrt(wsum_g<W>(gm, c * c) / double(n));
-    };
+    auto wrms = [&](double xv) { return wrms_ol<W>(xv, eps, al, n, gm); };
     auto clamp = [&](double y) {
       if (al) {
         if (y < lo) y = lo;
@@ -629,23 +656,9 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
         inv_in = true;
       }
     };
-    // sum_j M[lane][j] * y_j (M row-major in shared memory, leading dimension ld);
-    // the broadcasts do not depend on each other
     auto rowdot = [&](const auto* M, double y) {
-      double s0 = 0., s1 = 0.;
-      for (int j = 0; j + 1 < n; j += 2) {
-        const double y0 = __shfl_sync(gm, y, j, W);
-        const double y1 = __shfl_sync(gm, y, j + 1, W);
-        if (al) {
-          s0 += (double)M[lane * ld + j] * y0;
-          s1 += (double)M[lane * ld + j + 1] * y1;
-        }
-      }
-      if (n & 1) {
-        const double y0 = __shfl_sync(gm, y, n - 1, W);
-        if (al) s0 += (double)M[lane * ld + n - 1] * y0;
-      }
-      return s0 + s1;
+      return rowdot_ol<typename std::remove_const<typename std::remove_pointer<decltype(M)>::type>::type, W>(
+          M, y, n, ld, lane, gm);
     };
     // x = G^-1 rhs; with FP32 factors one refinement sweep on the FP64 residual
     // rhs - (x - hr0 J x), the matrix rebuilt in FP64 from the stored Jacobian

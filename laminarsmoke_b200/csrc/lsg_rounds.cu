@@ -26,8 +26,6 @@
 // BatchReactorHomogeneousConstantPressure.H:175-223.  With FP32 factors every
 // linear solve is refined against its FP64 residual (the matrix rebuilt in FP64
 // from the stored Jacobian) until it equals the FP64 solve to rounding.
-#include <type_traits>
-
 #include "lsg_common.cuh"
 #include "lsg_kernels.h"
 
@@ -118,7 +116,8 @@ __device__ __forceinline__ double hi_b(int k, int NC, double ymaxT) { return k <
 // Thread-serial RHS of the constant-pressure reactor
 // (BatchReactorHomogeneousConstantPressure.H:175-223).  y: this cell's input
 // vector (stride ns) with component pj replaced by pval when pj >= 0; f: output.
-// C,H,S,R scratch in shared memory, [species][thread].  Returns QR.
+// C (concentrations), G (h/RT - s/R) and R (formation rates) scratch in shared
+// memory, [species][thread].  Returns QR.
 // ---------------------------------------------------------------------------
 __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const double* __restrict__ Md,
                                         const int* __restrict__ Mi, double* __restrict__ scratch,
@@ -129,9 +128,8 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
   const int NC = L.nc, NR = L.nr;
   const int tid = threadIdx.x;
   double* C = scratch;
-  double* H = scratch + NC * kRT;
-  double* Sx = scratch + 2 * NC * kRT;
-  double* R = scratch + 3 * NC * kRT;
+  double* G = scratch + NC * kRT;        // h/RT - s/R of each species
+  double* R = scratch + 2 * NC * kRT;
 #define SC_(arr, i) arr[(i) * kRT + tid]
   const double* MW = M.D(L.mw);
   const double T = (pj == NC) ? pval : y[(long)NC * ns];
@@ -158,9 +156,9 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
     cTotSum += c;
     const bool hi = T > TM[i];
     const double* A = hi ? M.D(L.dh_ht) + 6 * i : M.D(L.dh_lt) + 6 * i;
-    SC_(H, i) = A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4] + uT * A[5];
+    const double hrt = A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4] + uT * A[5];
     const double* B = hi ? M.D(L.ds_ht) + 6 * i : M.D(L.ds_lt) + 6 * i;
-    SC_(Sx, i) = B[0] * logT + T * B[1] + T2 * B[2] + T3 * B[3] + T4 * B[4] + B[5];
+    SC_(G, i) = hrt - (B[0] * logT + T * B[1] + T2 * B[2] + T3 * B[3] + T4 * B[4] + B[5]);
     SC_(R, i) = 0.;
   }
   const double* lnA = M.D(L.lnA);
@@ -242,24 +240,12 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
       double rv = 1.;
       for (int q = pp[j]; q < pp[j + 1]; ++q) rv *= conc_factor_r(pnu[q], SC_(C, psp[q]));
       if (kind == 1) {
-        // 1/Keq from reaction enthalpy and entropy (StoichiometricMap.hpp:916-1001, KineticsMap_CHEMKIN.hpp:1217-1222)
-        double dh = 0., ds = 0.;
-        int qa = rp[j], qb = pp[j];
-        const int ae = rp[j + 1], be = pp[j + 1];
-        while (qa < ae || qb < be) {
-          const int sa = qa < ae ? rsp[qa] : (1 << 30);
-          const int sb = qb < be ? psp[qb] : (1 << 30);
-          if (sa <= sb) {
-            dh -= contrib_r(rnu[qa], SC_(H, sa));
-            ds -= contrib_r(rnu[qa], SC_(Sx, sa));
-            ++qa;
-          } else {
-            dh += contrib_r(pnu[qb], SC_(H, sb));
-            ds += contrib_r(pnu[qb], SC_(Sx, sb));
-            ++qb;
-          }
-        }
-        rv *= exp(-ds + dh - lP * dnu[j]);
+        // 1/Keq = exp(sum_products nu g - sum_reactants nu g - dnu ln(Patm/RT)), g = h/RT - s/R
+        // (StoichiometricMap.hpp:916-1001, KineticsMap_CHEMKIN.hpp:1217-1222, summed per side)
+        double dg = 0.;
+        for (int q = pp[j]; q < pp[j + 1]; ++q) dg += contrib_r(pnu[q], SC_(G, psp[q]));
+        for (int q = rp[j]; q < rp[j + 1]; ++q) dg -= contrib_r(rnu[q], SC_(G, rsp[q]));
+        rv *= exp(dg - lP * dnu[j]);
       } else {
         const int s = rs[j];
         rv *= exp(M.D(L.rev_lnA)[s] + M.D(L.rev_beta)[s] * logT - M.D(L.rev_eor)[s] * uT) / kArr;
@@ -275,10 +261,12 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
     const double Ri = SC_(R, i);
     f[(long)i * ns] = MW[i] * Ri / rho;
     if (energy) {
-      const double* A = (T > TM[i]) ? M.D(L.cp_ht) + 5 * i : M.D(L.cp_lt) + 5 * i;
+      const bool hi = T > TM[i];
+      const double* A = hi ? M.D(L.cp_ht) + 5 * i : M.D(L.cp_lt) + 5 * i;
       const double cpi = A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4];
       cpm += cpi * (SC_(C, i) / cTot);
-      dsum += Ri * SC_(H, i);
+      const double* Hc = hi ? M.D(L.dh_ht) + 6 * i : M.D(L.dh_lt) + 6 * i;
+      dsum += Ri * (Hc[0] + T * Hc[1] + T2 * Hc[2] + T3 * Hc[3] + T4 * Hc[4] + uT * Hc[5]);
     }
   }
   double dT = 0.;
@@ -427,6 +415,51 @@ __device__ __forceinline__ void set8(double (&a)[8], unsigned i, double x) {
 #pragma unroll
   for (unsigned k = 0; k < 8; ++k)
     if (i == k) a[k] = x;
+}
+
+// x = G^-1 rhs for one lane group (Xs = G^-1 rows in shared memory); with FP32
+// factors (refine) one sweep of iterative refinement on the FP64 residual
+// rhs - (x - hr0 J x), the matrix rebuilt in FP64 from the Jacobian rows Js.
+template <typename LUT, int W>
+__device__ __noinline__ double solve_ol(const LUT* Xs, const float* Js, double rhs, double hr0, int n, int lane,
+                                        unsigned gm, int refine) {
+  const int ld = n + 1;
+  const bool al = lane < n;
+  double xv = rowdot_ol<LUT, W>(Xs, rhs, n, ld, lane, gm);
+  for (int it = 0; it < refine; ++it) {
+    const double s = rowdot_ol<float, W>(Js, xv, n, ld, lane, gm);
+    const double res = al ? rhs - (xv - hr0 * s) : 0.;
+    xv += rowdot_ol<LUT, W>(Xs, res, n, ld, lane, gm);
+  }
+  return al ? xv : 0.;
+}
+
+// Candidate step scales of NewOrderNewH (MultiValueSolver.hpp:1042-1105) for
+// orders p-1, p, p+1 from the last three Nordsieck differences; out of line.
+struct HCand {
+  double hMinus, hC, hPlus, alfa1, alfa3;
+};
+template <int W>
+__device__ __noinline__ HCand order_candidates(double vp, double vp1, double vp2, double eps, bool al, int n,
+                                               unsigned gm, unsigned p, bool try_lower, bool try_higher,
+                                               double a2m, double a2p, double a2h) {
+  HCand c{0., 0., 0., 0., 0.};
+  if (try_lower) {
+    double hm = c_gear_r.Ep[p - 1] * wrms_ol<W>(vp, eps, al, n, gm) + kMachEpsFloat;
+    hm = 1. / hm;
+    c.alfa1 = a2m - .05;
+    c.hMinus = c.alfa1 * pow(hm, 1. / double(p));
+  }
+  double hc = c_gear_r.Ep[p] * wrms_ol<W>(vp1, eps, al, n, gm) + kMachEpsFloat;
+  hc = 1. / hc;
+  c.hC = a2p * pow(hc, 1. / double(p + 1));
+  if (try_higher) {
+    double hp = c_gear_r.Ep[p + 1] * wrms_ol<W>(vp2, eps, al, n, gm) + kMachEpsFloat;
+    hp = 1. / hp;
+    c.alfa3 = a2h - .25;
+    c.hPlus = c.alfa3 * pow(hp, 1. / double(p + 2));
+  }
+  return c;
 }
 
 // Buffers of the round scheme.
@@ -656,26 +689,14 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
         inv_in = true;
       }
     };
-    auto rowdot = [&](const auto* M, double y) {
-      return rowdot_ol<typename std::remove_const<typename std::remove_pointer<decltype(M)>::type>::type, W>(
-          M, y, n, ld, lane, gm);
-    };
     // x = G^-1 rhs; with FP32 factors one refinement sweep on the FP64 residual
     // rhs - (x - hr0 J x), the matrix rebuilt in FP64 from the stored Jacobian
     auto solve = [&](double rhs) {
       load_inv();
-      double xv = rowdot(Xs, rhs);
-      if (sizeof(LUT) == sizeof(float)) {
-        load_j();
-        for (int it = 0; it < kRefineR; ++it) {
-          const double s = rowdot(Js, xv);
-          const double res = al ? rhs - (xv - hr0f * s) : 0.;
-          xv += rowdot(Xs, res);
-        }
-      }
-      if (!al) xv = 0.;
+      const bool fp32 = sizeof(LUT) == sizeof(float);
+      if (fp32) load_j();
       ++csolve;
-      return xv;
+      return solve_ol<LUT, W>(Xs, Js, rhs, hr0f, n, lane, gm, fp32 ? kRefineR : 0);
     };
     auto factorize = [&]() {
       load_j();
@@ -999,7 +1020,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
             if (iterErrorFailure > 0 || iterConvergenceFailure > 0) iterConvergenceRate = 0;
             if (iterConvergence > 1) {
               load_j();
-              const double s = rowdot(Js, v[0] - z[0]);
+              const double s = rowdot_ol<float, W>(Js, v[0] - z[0], n, ld, lane, gm);
               const double vr = v[1] - (s * h + z[1]);
               const double normd = wsum_g<W>(gm, al ? fabs(vr) : 0.);
               const double normf = wsum_g<W>(gm, al ? fabs(v[1]) : 0.);
@@ -1027,22 +1048,11 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
             iterOrder++;
             if (iterOrder > p + 1) {
               // NewOrderNewH (:1042-1210)
-              double hMinus = 0., hC = 0., hPlus = 0., alfa1 = 0., alfa3 = 0.;
-              if (p > 1u && odeOrderStatus != O_INC) {
-                hMinus = c_gear_r.Ep[p - 1] * wrms(get8(v, p)) + kMachEpsFloat;
-                hMinus = 1. / hMinus;
-                alfa1 = alfa2(p - 1) - .05;
-                hMinus = alfa1 * pow_ol(hMinus, 1. / double(p));
-              }
-              hC = c_gear_r.Ep[p] * wrms(get8(v, p + 1)) + kMachEpsFloat;
-              hC = 1. / hC;
-              hC = alfa2(p) * pow_ol(hC, 1. / double(p + 1));
-              if (p < maximum_order && odeOrderStatus != O_DEC) {
-                hPlus = c_gear_r.Ep[p + 1] * wrms(get8(v, p + 2)) + kMachEpsFloat;
-                hPlus = 1. / hPlus;
-                alfa3 = alfa2(p + 1) - .25;
-                hPlus = alfa3 * pow_ol(hPlus, 1. / double(p + 2));
-              }
+              const HCand hc = order_candidates<W>(get8(v, p), get8(v, p + 1), get8(v, p + 2), eps, al, n, gm, p,
+                                                   p > 1u && odeOrderStatus != O_INC,
+                                                   p < maximum_order && odeOrderStatus != O_DEC,
+                                                   alfa2(p - 1), alfa2(p), alfa2(p + 1));
+              const double hMinus = hc.hMinus, hC = hc.hC, hPlus = hc.hPlus, alfa1 = hc.alfa1, alfa3 = hc.alfa3;
               if (hMinus > hC && hMinus > hPlus) {
                 hScale = (.75 / alfa1) * hMinus; orderInNextStep = p - 1; odeOrderStatus = O_DEC;
               } else if (hC > hMinus && hC > hPlus) {
@@ -1241,7 +1251,7 @@ cudaError_t rounds_prepare(const MechLayout& L, bool lu64, int sm_count, RoundsP
   if (n > 32) return cudaErrorInvalidValue;
   *P = RoundsPlan{};
   P->lu64 = lu64;
-  P->rhs_smem = ((L.bytes + 15u) & ~15u) + (size_t)4 * L.nc * kRT * sizeof(double);
+  P->rhs_smem = ((L.bytes + 15u) & ~15u) + (size_t)3 * L.nc * kRT * sizeof(double);
   P->adv_smem = advance_smem(L, lu64);
   cudaError_t e = cudaFuncSetAttribute(rounds_rhs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)P->rhs_smem);

@@ -80,6 +80,23 @@ def kernel_roofline(args, ktimes, counters, nc, ncells, hbm, peak_src):
             "note": "latency-bound BDF solver kernel; bytes are its solver-record traffic"}
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The slowest rank's time (every rank calls it, same order, every step)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(cells_per_rank: int, steps: int, ms: float, world: int) -> float:
+    """cells*steps/s of all ranks together: every rank integrates its own batch
+    (replicas, weak scaling) and the job is as fast as its slowest rank."""
+    return world * cells_per_rank * steps / (ms / 1e3)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -301,12 +318,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dist.barrier()
     ms = float(sum(a.elapsed_time(b) for a, b in evs))
     st = status.cpu().numpy()
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, dev)
     ms_per_step = ms / args.steps
-    value = world * n * args.steps / (ms / 1e3)
+    value = whole_job_rate(n, args.steps, ms, world)
 
     # end to end through the host-pointer C ABI call: H2D of the inputs, the step, D2H of the results
     e2e = None
@@ -323,11 +337,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             Q, sth, nsh = ctx.step(Yh.numpy(), Th.numpy(), DT)
             tms.append(time.perf_counter() - t0)
         et = float(np.mean(tms[1:]))
-        if world > 1:
-            t = torch.tensor([et], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            et = float(t.item())
-        e2e = {"value": world * n / et, "unit": UNIT,
+        et = max_over_ranks(et, world, dev)
+        e2e = {"value": whole_job_rate(n, 1, et * 1e3, world), "unit": UNIT,
                "h2d_bytes_per_step": int(8 * (nc + 1) * n),
                "d2h_bytes_per_step": int(8 * (nc + 1) * n + 8 * n + 4 * n + 4 * n)}
 

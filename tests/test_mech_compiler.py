@@ -142,3 +142,23 @@ def test_synthetic_mechanism_is_element_balanced(ns, nr):
         rhs = sum(A["prod_nu"][q] * comp[A["prod_species"][q]] for q in range(A["prod_ptr"][j], A["prod_ptr"][j + 1]))
         np.testing.assert_array_equal(lhs, rhs)
     assert len(A["tb_rxn"]) == round(0.15 * nr) and len(A["fo_rxn"]) == round(0.10 * nr)
+
+
+def test_compile_command_line(tmp_path):
+    """python -m laminarsmoke_b200.mech compile writes the same blob as the library call."""
+    import subprocess
+    import sys
+    from laminarsmoke_b200.mech import blob, chemkin, synthetic
+    sm = synthetic.generate(12, 30, seed=7)
+    kin, thermo = sm.kinetics, sm.thermo
+    (tmp_path / "k.cki").write_text(kin)
+    (tmp_path / "t.ckt").write_text(thermo)
+    out = tmp_path / "m.lsmech"
+    r = subprocess.run([sys.executable, "-m", "laminarsmoke_b200.mech", "compile", str(tmp_path / "k.cki"),
+                        str(tmp_path / "t.ckt"), "-o", str(out)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    m = chemkin.compile_mechanism(kin, thermo)
+    assert out.read_bytes() == blob.pack(m.arrays, m.species)
+    r = subprocess.run([sys.executable, "-m", "laminarsmoke_b200.mech", "info", str(out)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and f"{m.n_species} species" in r.stdout

@@ -47,10 +47,13 @@ extern "C" {
 #define LSG_PRECISION_MIXED 1  /* FP64 rates/residual/error control, FP32 factorisation + FP64 refinement */
 
 /* work decomposition (lsg_options.tile) */
-#define LSG_TILE_AUTO 0        /* FP64 -> warp per cell; MIXED -> lane per cell */
+#define LSG_TILE_AUTO 0        /* FP64 -> warp per cell; MIXED -> lane per cell (up to 31 species) */
 #define LSG_TILE_WARP 1        /* one warp per cell, the reference's operation order (FP64 only) */
 #define LSG_TILE_LANE 2        /* one thread per cell, rounds of RHS / solver / factor kernels over the live cells */
 #define LSG_TILE_PERSISTENT 3  /* one thread per cell, one persistent kernel + device work queue */
+#define LSG_TILE_BLOCK 4       /* one thread block per cell (any size up to 511 species), FP64 factors */
+/* Mechanisms of 32 to 511 species always run one thread block per cell (the
+ * tile is ignored) with FP64 factors whatever the precision option. */
 
 /* counters per cell (lsg_reaction_step_device counters_out layout) */
 #define LSG_NCOUNTERS 8        /* steps, rhs, jacobians, factorisations, solves, error-test fails, convergence fails, jacobian rhs */
@@ -139,9 +142,9 @@ long long lsg_ctx_launches(const lsg_ctx* ctx);
  * stream when lsg_options.kernel_timing is set (diagnostics; no counterpart in
  * the reference).  Kinds: 0 RHS, 1 solver advance, 2 compaction, 3 round
  * initialisation (lane-per-cell form), 4 plain warp kernel, 5 persistent lane
- * kernel.  ms[k] total milliseconds, launches[k] timed launches; reset != 0
+ * kernel, 6 block-per-cell kernel (large mechanisms).  ms[k] total milliseconds, launches[k] timed launches; reset != 0
  * clears the totals after reading.  Waits for the last timed kernel. */
-#define LSG_NKERNEL_KINDS 6
+#define LSG_NKERNEL_KINDS 7
 int lsg_ctx_kernel_times(lsg_ctx* ctx, double* ms, long long* launches, int nkinds, int reset);
 
 /* Waits for the device, then reads and clears the error flags kernels raised

@@ -20,6 +20,7 @@ UNITS = [
     ("lsg_plain.cu", ["-fmad=false"]),
     ("lsg_batched.cu", []),
     ("lsg_rounds.cu", []),
+    ("lsg_block.cu", []),
     ("lsg_api.cu", []),
     ("lsg_mech_host.cpp", []),
 ]

@@ -48,6 +48,10 @@ struct lsg_ctx {
   int rplan_lu64 = -1;
   int* nact_host = nullptr;   // pinned
   long long launches = 0;     // kernels enqueued by this context
+  // block-per-cell (large mechanism) resources
+  double* bws = nullptr;
+  long bws_blocks = 0;
+  int* bqueue = nullptr;
   KernelTimer timer;          // per-kernel device time (lsg_options.kernel_timing)
 };
 
@@ -86,6 +90,7 @@ int ensure_gear(int device) {
   if (upload_gear_plain(g) != cudaSuccess) return LSG_ERR_CUDA;
   if (upload_gear_batched(g) != cudaSuccess) return LSG_ERR_CUDA;
   if (upload_gear_rounds(g) != cudaSuccess) return LSG_ERR_CUDA;
+  if (upload_gear_block(g) != cudaSuccess) return LSG_ERR_CUDA;
   g_gear_uploaded[device] = true;
   return LSG_OK;
 }
@@ -113,7 +118,7 @@ int validate_options(const lsg_options* o) {
   if (o->full_pivoting != 0) return LSG_ERR_UNSUPPORTED;
   if (o->precision != LSG_PRECISION_FP64 && o->precision != LSG_PRECISION_MIXED) return LSG_ERR_ARG;
   if (o->maximum_order < 1 || o->maximum_order > 5) return LSG_ERR_ARG;
-  if (o->tile < LSG_TILE_AUTO || o->tile > 3) return LSG_ERR_ARG;
+  if (o->tile < LSG_TILE_AUTO || o->tile > LSG_TILE_BLOCK) return LSG_ERR_ARG;
   if (o->tile == LSG_TILE_WARP && o->precision != LSG_PRECISION_FP64) return LSG_ERR_UNSUPPORTED;
   return LSG_OK;
 }
@@ -215,10 +220,42 @@ int ensure_rounds(lsg_ctx* c, long n, bool lu64) {
   return LSG_OK;
 }
 
+// Mechanisms with more than 31 species: one block per cell (FP64 factors).
+int ensure_block(lsg_ctx* c) {
+  const MechLayout& L = c->mech->host.layout;
+  if (!sm_count(c)) return LSG_ERR_CUDA;
+  if (!c->bws) {
+    long nb = 0;
+    if (block_plan(L, c->sm_count, &nb) != cudaSuccess || nb <= 0) { cudaGetLastError(); return LSG_ERR_UNSUPPORTED; }
+    if (cudaMalloc(&c->bws, block_ws_bytes(L) * (size_t)nb) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+    if (!c->bqueue && cudaMalloc(&c->bqueue, sizeof(int)) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+    c->bws_blocks = nb;
+  }
+  return LSG_OK;
+}
+
+int launch_large(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
+  const MechLayout& L = c->mech->host.layout;
+  const int r = ensure_block(c);
+  if (r != LSG_OK) return r;
+  if (c->timer.used >= KernelTimer::kPairs) {
+    cudaStreamSynchronize(s);
+    c->timer.collect();
+  }
+  c->timer.begin(KT_BLOCK, s);
+  if (launch_block(L, c->mech->d_buf, to_step_options(c->opt), a, c->bws, c->bws_blocks, c->bqueue, s) !=
+      cudaSuccess)
+    return LSG_ERR_CUDA;
+  c->timer.end(s);
+  c->launches += 1;
+  return LSG_OK;
+}
+
 int launch_step(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
   const MechLayout& L = c->mech->host.layout;
   const StepOptions so = to_step_options(c->opt);
   const int tile = resolve_tile(c->opt);
+  if (L.nc + 1 > 32 || tile == LSG_TILE_BLOCK) return launch_large(c, a, s);
   if (tile == LSG_TILE_LANE) {
     const bool lu64 = c->opt.precision == LSG_PRECISION_FP64;
     const int r = ensure_rounds(c, a.ncells, lu64);
@@ -386,6 +423,8 @@ int lsg_ctx_destroy(lsg_ctx* c) {
   cudaFree(c->slots);
   cudaFree(c->queue);
   cudaFree(c->rstate);
+  cudaFree(c->bws);
+  cudaFree(c->bqueue);
   if (c->nact_host) cudaFreeHost(c->nact_host);
   cudaFree(c->d_err);
   for (cudaEvent_t& e : c->timer.ev)
@@ -547,7 +586,14 @@ int lsg_rhs_device(lsg_ctx* c, int ncells, const double* y, double* dy, long ld,
   if (ncells == 0) return LSG_OK;
   if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
   const MechLayout& L = c->mech->host.layout;
-  if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
+  if (L.nc + 1 > 32) {
+    const int r = ensure_block(c);
+    if (r != LSG_OK) return r;
+    if (launch_rhs_block(L, c->mech->d_buf, ncells, y, dy, ld, p, c->opt.energy, qr, c->bws, c->bws_blocks,
+                         (cudaStream_t)stream) != cudaSuccess)
+      return LSG_ERR_CUDA;
+    return LSG_OK;
+  }
   if (launch_rhs_warp(L, c->mech->d_buf, ncells, y, dy, ld, p, c->opt.energy, qr, c->d_err,
                       (cudaStream_t)stream) != cudaSuccess)
     return LSG_ERR_CUDA;

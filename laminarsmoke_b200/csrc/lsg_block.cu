@@ -1,0 +1,1041 @@
+// Block-per-cell reaction step for mechanisms too large for a warp (more than
+// 31 species): one thread block integrates one cell, thread k owning ODE
+// component k; reactions are spread over the threads.  Persistent grid: blocks
+// take cells from a device queue.  All arithmetic FP64; sums are block tree
+// reductions.  The method is the one of the plain warp step
+// (MultiValueSolver.hpp:367-1328, MethodGear.hpp:79-536, KernelDense.hpp:90-245
+// under solvers/openSMOKEpp4laminarSMOKE/math/native-ode-solvers) with the RHS of
+// BatchReactorHomogeneousConstantPressure.H:175-223 and the kinetics of
+// KineticsMap_CHEMKIN.hpp (kinetic constants recomputed only when T changes,
+// :271-297); the mechanism tables are read from global memory (read-only path).
+//
+// Per-block work space in HBM: Jacobian J[n][n], factors G[n][n], cached
+// kinetic constants; in shared memory: the Nordsieck arrays, concentrations,
+// enthalpies, entropies, net rates and the pivots.
+#include "lsg_common.cuh"
+#include "lsg_kernels.h"
+
+namespace lsg {
+
+static __constant__ GearConsts c_gear_k;
+
+namespace {
+
+constexpr int kBlkMaxN = 512;
+
+__device__ __forceinline__ double contrib_k(double nu, double v) {
+  if (nu == 1.) return v;
+  if (nu == 2.) return v + v;
+  if (nu == 3.) return v + v + v;
+  if (nu == 0.5) return 0.5 * v;
+  return nu * v;
+}
+
+__device__ __forceinline__ double conc_factor_k(double nu, double c1) {
+  if (nu == 1.) return c1;
+  if (nu == 2.) return c1 * c1;
+  if (nu == 3.) return c1 * c1 * c1;
+  if (nu == 0.5) return sqrt(c1);
+  return pow(c1, nu);
+}
+
+// Block-wide sum; every thread receives the total.  red: BT/32 + 1 doubles.
+template <int BT>
+__device__ __forceinline__ double bsum(double v, double* red) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+  const int w = threadIdx.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[w] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double s = threadIdx.x < BT / 32 ? red[threadIdx.x] : 0.;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(kFull, s, off);
+    if (threadIdx.x == 0) red[BT / 32] = s;
+  }
+  __syncthreads();
+  return red[BT / 32];
+}
+
+// Value of thread src in every thread.
+__device__ __forceinline__ double bcast(double v, int src, double* slot) {
+  __syncthreads();
+  if ((int)threadIdx.x == src) *slot = v;
+  __syncthreads();
+  return *slot;
+}
+
+// Per-block shared work space.
+struct BlockShared {
+  double* Z;     // [8][BT]
+  double* V;     // [8][BT]
+  double* C;     // [NC] concentrations
+  double* H;     // [NC] h/RT
+  double* S;     // [NC] s/R
+  double* NET;   // [NR] net rates
+  double* X;     // [BT] solve vector
+  double* red;   // [BT/32 + 1]
+  double* slot;  // [4]: broadcast, cached T, QR, pivot value
+  int* PIV;      // [BT]
+  int* ival;     // [BT/32 + 1] pivot search scratch
+};
+
+template <int BT>
+__host__ __device__ inline size_t block_shared_bytes(const MechLayout& L) {
+  return sizeof(double) * (16 * BT + 3 * (size_t)L.nc + (size_t)L.nr + BT + BT / 32 + 1 + 4) +
+         sizeof(int) * (BT + BT / 32 + 1) + 64;
+}
+
+// Per-block global work space (doubles): J, G, kinetic-constant caches.
+__host__ __device__ inline size_t block_ws_doubles(const MechLayout& L) {
+  const size_t n = L.nc + 1;
+  return 2 * n * n + 2 * (size_t)L.nr + 2 * (size_t)(L.n_fo > 0 ? L.n_fo : 1) + 8;
+}
+
+// ---------------------------------------------------------------------------
+// RHS, block cooperative (thread i < NC owns species i, thread NC owns T).
+// ---------------------------------------------------------------------------
+template <int BT>
+__device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, const BlockShared& W,
+                                         double* __restrict__ karr, double* __restrict__ ukeq,
+                                         double* __restrict__ kinf, double* __restrict__ logf, double yl, double T,
+                                         double P0, int energy) {
+  const int tid = threadIdx.x;
+  const int NC = L.nc, NR = L.nr;
+  const double* MW = M.D(L.mw);
+  const double mwl = tid < NC ? MW[tid] : 1.;
+  const double u = bsum<BT>(tid < NC ? yl / mwl : 0., W.red);
+  const double MWmix = 1. / u;
+  double xl = 0.;
+  if (tid < NC) { xl = MWmix * yl; xl = xl / mwl; }
+  const double cTot = P0 / kRgas / T;
+  const double cl = cTot * xl;
+  const double rho = cTot * MWmix;
+  const double* TM = M.D(L.t_mid);
+  const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, uT = 1. / T;
+  double hl = 0.;
+  if (tid < NC) {
+    const double* A = T > TM[tid] ? M.D(L.dh_ht) + 6 * tid : M.D(L.dh_lt) + 6 * tid;
+    hl = A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4] + uT * A[5];
+    W.C[tid] = cl;
+    W.H[tid] = hl;
+  }
+  const double T_old = W.slot[1];
+  const bool recalc = fabs(T - T_old) / T > 0.;
+  if (recalc && tid < NC) {
+    const double logT = log(T);
+    const double* A = T > TM[tid] ? M.D(L.ds_ht) + 6 * tid : M.D(L.ds_lt) + 6 * tid;
+    W.S[tid] = A[0] * logT + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4] + A[5];
+  }
+  __syncthreads();
+  if (tid == 0) W.slot[1] = T;
+  if (recalc) {
+    const double logT = log(T);
+    const double lP = log(101325. / kRgas / T);
+    const double* lnA = M.D(L.lnA);
+    const double* beta = M.D(L.beta);
+    const double* eor = M.D(L.eor);
+    const double* dnu = M.D(L.dnu);
+    const int* sgn = M.I(L.a_sign);
+    const int* rk = M.I(L.rev_kind);
+    const int* rs = M.I(L.rev_slot);
+    const int* rp = M.I(L.reac_ptr);
+    const int* rsp = M.I(L.reac_sp);
+    const double* rnu = M.D(L.reac_nu);
+    const int* pp = M.I(L.prod_ptr);
+    const int* psp = M.I(L.prod_sp);
+    const double* pnu = M.D(L.prod_nu);
+    for (int j = tid; j < NR; j += BT) {
+      double k = exp(lnA[j] + beta[j] * logT - eor[j] * uT);
+      if (sgn[j] < 0) k *= -1.;
+      karr[j] = k;
+      const int kind = rk[j];
+      if (kind == 1) {
+        // StoichiometricMap::ReactionEnthalpyAndEntropy: species order, reactant first
+        double dh = 0., ds = 0.;
+        int a = rp[j], b = pp[j];
+        const int ae = rp[j + 1], be = pp[j + 1];
+        while (a < ae || b < be) {
+          const int sa = a < ae ? rsp[a] : (1 << 30);
+          const int sb = b < be ? psp[b] : (1 << 30);
+          if (sa <= sb) {
+            dh -= contrib_k(rnu[a], W.H[sa]);
+            ds -= contrib_k(rnu[a], W.S[sa]);
+            ++a;
+          } else {
+            dh += contrib_k(pnu[b], W.H[sb]);
+            ds += contrib_k(pnu[b], W.S[sb]);
+            ++b;
+          }
+        }
+        ukeq[j] = exp(-ds + dh - lP * dnu[j]);
+      } else if (kind == 2) {
+        const int s = rs[j];
+        ukeq[j] = exp(M.D(L.rev_lnA)[s] + M.D(L.rev_beta)[s] * logT - M.D(L.rev_eor)[s] * uT);
+      }
+    }
+    const int* ft = M.I(L.fo_type);
+    for (int k = tid; k < L.n_fo; k += BT) {
+      kinf[k] = exp(M.D(L.fo_lnA)[k] + M.D(L.fo_beta)[k] * logT - M.D(L.fo_eor)[k] * uT);
+      const double a = M.D(L.fo_a)[k], b = M.D(L.fo_b)[k], c = M.D(L.fo_c)[k], d = M.D(L.fo_d)[k];
+      if (ft[k] == 1) {
+        const double v = (d != 0.) ? (1. - a) * exp(-T / b) + a * exp(-T / c) + exp(-d / T)
+                                   : (1. - a) * exp(-T / b) + a * exp(-T / c);
+        logf[k] = (v < 1.e-300) ? -300. : log10(v);
+      } else if (ft[k] == 2) {
+        logf[k] = a * exp(-b / T) + exp(-T / c);
+      } else {
+        logf[k] = 0.;
+      }
+    }
+  }
+  const double cTotSum = bsum<BT>(cl, W.red);   // also orders the cache writes above before their reads
+  {
+    const int* tbs = M.I(L.tb_slot);
+    const int* fos = M.I(L.fo_slot);
+    const int* rk = M.I(L.rev_kind);
+    const int* rp = M.I(L.reac_ptr);
+    const int* rsp = M.I(L.reac_sp);
+    const double* rnu = M.D(L.reac_nu);
+    const int* pp = M.I(L.prod_ptr);
+    const int* psp = M.I(L.prod_sp);
+    const double* pnu = M.D(L.prod_nu);
+    for (int j = tid; j < NR; j += BT) {
+      const double kArr = karr[j];
+      double kMod = kArr;
+      const int tb = tbs[j];
+      if (tb >= 0) {
+        double Mc = cTotSum;
+        const int* tp = M.I(L.tb_ptr);
+        const int* ts = M.I(L.tb_sp);
+        const double* te = M.D(L.tb_eff);
+        for (int q = tp[tb]; q < tp[tb + 1]; ++q) Mc += W.C[ts[q]] * te[q];
+        kMod *= Mc;
+      }
+      const int fo = fos[j];
+      if (fo >= 0) {
+        double Mc;
+        const int single = M.I(L.fo_single)[fo];
+        if (single < 0) {
+          Mc = cTotSum;
+          const int* fp = M.I(L.fo_ptr);
+          const int* fs = M.I(L.fo_sp);
+          const double* fe = M.D(L.fo_eff);
+          for (int q = fp[fo]; q < fp[fo + 1]; ++q) Mc += W.C[fs[q]] * fe[q];
+        } else {
+          Mc = W.C[single] + 1.e-16;
+        }
+        const double kInf = kinf[fo];
+        const double lF = logf[fo];
+        const double Pr = kArr * Mc / kInf;
+        double wF = 1.;
+        const int ty = M.I(L.fo_type)[fo];
+        if (ty == 1) {
+          double qq;
+          if (Pr > 1.e-32) {
+            const double nTroe = 0.75 - 1.27 * lF;
+            const double cTroe = -0.4 - 0.67 * lF;
+            const double sTroe = log10(Pr) + cTroe;
+            qq = sTroe / (nTroe - 0.14 * sTroe);
+          } else {
+            qq = 1. / 0.14;
+          }
+          wF = pow(10., lF / (1. + qq * qq));
+        } else if (ty == 2) {
+          const double l10 = log10(Pr);
+          const double xSRI = 1. / (1. + l10 * l10);
+          wF = pow(lF, xSRI) * M.D(L.fo_d)[fo];
+          const double e = M.D(L.fo_e)[fo];
+          if (e != 0.) wF *= pow(T, e);
+        }
+        kMod *= kInf * (Pr / (1. + Pr)) * wF / kArr;
+      }
+      double fwd = 1.;
+      for (int q = rp[j]; q < rp[j + 1]; ++q) fwd *= conc_factor_k(rnu[q], W.C[rsp[q]]);
+      double net = fwd;
+      const int kind = rk[j];
+      if (kind != 0) {
+        double rv = 1.;
+        for (int q = pp[j]; q < pp[j + 1]; ++q) rv *= conc_factor_k(pnu[q], W.C[psp[q]]);
+        if (kind == 1) rv *= ukeq[j];
+        else rv *= ukeq[j] / kArr;
+        net -= rv;
+      }
+      W.NET[j] = net * kMod;
+    }
+  }
+  __syncthreads();
+  double Rl = 0.;
+  if (tid < NC) {
+    const int* fp = M.I(L.fr_ptr);
+    const int* fr = M.I(L.fr_rxn);
+    const double* fc = M.D(L.fr_coef);
+    for (int q = fp[tid]; q < fp[tid + 1]; ++q) {
+      const double c = fc[q];
+      Rl += contrib_k(c < 0. ? -c : c, W.NET[fr[q]]) * (c < 0. ? -1. : 1.);
+    }
+  }
+  double dyl = tid < NC ? mwl * Rl / rho : 0.;
+  double QR = W.slot[2];
+  if (energy) {
+    double cpl = 0.;
+    if (tid < NC) {
+      const double* A = T > TM[tid] ? M.D(L.cp_ht) + 5 * tid : M.D(L.cp_lt) + 5 * tid;
+      cpl = A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4];
+    }
+    const double cpm = bsum<BT>(cpl * xl, W.red) * kRgas;
+    const double CpMixMass = cpm / MWmix;
+    const double d = bsum<BT>(Rl * hl, W.red);
+    QR = -d * kRgas * T;
+    if (tid == NC) dyl = QR / (rho * CpMixMass);
+  } else if (tid == NC) {
+    dyl = 0.;
+  }
+  __syncthreads();
+  if (tid == 0) W.slot[2] = QR;
+  __syncthreads();
+  return dyl;
+}
+
+// ---------------------------------------------------------------------------
+// Gear / multivalue BDF integrator for one block (one cell).
+// ---------------------------------------------------------------------------
+template <int BT>
+struct GearBlock {
+  enum { H_DEC, H_CONST, H_INC };
+  enum { O_DEC, O_CONST, O_INC };
+  enum { JAC_CHANGE, JAC_MODIFIED };
+  enum { M_TO_FACT, M_FACT };
+  enum { CONV_FAIL, CONV_OK };
+
+  const MechLayout* L;
+  MechView M;
+  BlockShared W;
+  double* J;      // [n][n] row major, global
+  double* G;      // [n][n] factors, global
+  double* karr;
+  double* ukeq;
+  double* kinf;
+  double* logf;
+  double P0;
+  int energy;
+  int tid, ne;
+  bool active;
+  double b, deltab, f, va, vb, y, y0, eps, minv, maxv;
+  double alfa2_4, alfa2_5;
+  __device__ __forceinline__ double alfa2(unsigned k) const { return k == 4 ? alfa2_4 : (k == 5 ? alfa2_5 : .8); }
+  double abs_tol, rel_tol;
+  unsigned maximum_order, max_number_steps;
+  double t, t0, tOut, tInMeshPoint, tStabilize;
+  double hNordsieck, hScaleMax, h, hNextStep, hScale;
+  bool fixedOrderMin;
+  unsigned iterConstSteps, iterMinimumOrder;
+  unsigned p, iterOrder, orderInNextStep, maxIterationsJacobian;
+  int odeHStatus, odeOrderStatus, status, factorizationStatus, jacobianStatus, convergenceStatus;
+  unsigned numberOfSteps, iterConvergence, iterConvergenceRate, iterConvergenceFailure, iterErrorFailure;
+  unsigned numberOfConvergenceFailuresForOrderMax, stepOfLastJacobian;
+  long long cnt[NCNT];
+
+  __device__ __forceinline__ double& Z(int i) { return W.Z[i * BT + tid]; }
+  __device__ __forceinline__ double& V(int i) { return W.V[i * BT + tid]; }
+
+  __device__ double rhs(double yl) {
+    ++cnt[CNT_RHS];
+    const double T = bcast(yl, ne - 1, W.slot);
+    return rhs_block<BT>(*L, M, W, karr, ukeq, kinf, logf, yl, T, P0, energy);
+  }
+
+  __device__ double error_control(double w) {   // OpenSMOKEUtilities.hpp:689-701
+    const double c = active ? w * eps : 0.;
+    return sqrt(bsum<BT>(c * c, W.red) / double(ne));
+  }
+
+  __device__ __forceinline__ void check_constraints(double& yl) {
+    if (active) {
+      if (yl < minv) yl = minv;
+      if (yl > maxv) yl = maxv;
+    }
+  }
+
+  __device__ __forceinline__ void one_over_epsilon(double w) {
+    if (active) eps = 1. / (abs_tol + rel_tol * fabs(w));
+  }
+
+  // KernelDense::NumericalJacobian, constrained branch (KernelDense.hpp:111-193)
+  __device__ void numerical_jacobian(double yl, double fl) {
+    const double ZERO_DER = sqrt(kTinyFloat);
+    const double ETA2 = sqrt(kMachEpsDouble);
+    const double BETA = 1.e+3 * kMachEpsDouble;
+    double hf = BETA * fabs(h) * error_control(fl) * double(ne);
+    if (hf < 1.e-10) hf = 1.;
+    const int n = ne;
+    for (int j = 0; j < n; ++j) {
+      const double yh = bcast(yl, j, W.slot);
+      const double ej = bcast(eps, j, W.slot);
+      const double mxj = bcast(maxv, j, W.slot);
+      const double a = fabs(yh), bb = fabs(1. / ej);
+      double hJ = ETA2 * (a > bb ? a : bb);
+      hJ = fmax(hJ, hf / ej);
+      hJ = fmax(hJ, ZERO_DER);
+      if (yh + hJ > mxj) hJ = -hJ;
+      double yp = yl;
+      if (tid == j) yp += hJ;
+      const double T = bcast(yp, n - 1, W.slot);
+      const double aux = rhs_block<BT>(*L, M, W, karr, ukeq, kinf, logf, yp, T, P0, energy);
+      ++cnt[CNT_JAC_RHS];
+      const double hInv = 1. / hJ;
+      if (active) J[(long)tid * n + j] = hInv * (aux - fl);
+    }
+    __syncthreads();
+  }
+
+  // G = I - hr0 J; partial-pivot LU (largest magnitude, first occurrence)
+  __device__ void build_and_factorize(double hr0) {
+    const int n = ne;
+    for (long e = tid; e < (long)n * n; e += BT) {
+      const int i = (int)(e / n), j = (int)(e % n);
+      double g = J[e];
+      g *= -hr0;
+      if (i == j) g += 1.;
+      G[e] = g;
+    }
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+      // pivot search over rows k..n-1 of column k, ties -> lowest row
+      double best = (tid >= k && tid < n) ? fabs(G[(long)tid * n + k]) : -1.;
+      int row = tid;
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ob = __shfl_xor_sync(kFull, best, off);
+        const int orow = __shfl_xor_sync(kFull, row, off);
+        if (ob > best || (ob == best && orow < row)) { best = ob; row = orow; }
+      }
+      if ((tid & 31) == 0) { W.red[tid >> 5] = best; W.ival[tid >> 5] = row; }
+      __syncthreads();
+      if (tid < 32) {
+        double bv = tid < BT / 32 ? W.red[tid] : -2.;
+        int br = tid < BT / 32 ? W.ival[tid] : (1 << 30);
+        for (int off = 16; off > 0; off >>= 1) {
+          const double ob = __shfl_xor_sync(kFull, bv, off);
+          const int orow = __shfl_xor_sync(kFull, br, off);
+          if (ob > bv || (ob == bv && orow < br)) { bv = ob; br = orow; }
+        }
+        if (tid == 0) W.ival[BT / 32] = (br >= k && br < n) ? br : k;
+      }
+      __syncthreads();
+      const int pr = W.ival[BT / 32];
+      if (tid == 0) W.PIV[k] = pr;
+      if (pr != k)
+        for (int j = tid; j < n; j += BT) {
+          const double tmp = G[(long)k * n + j];
+          G[(long)k * n + j] = G[(long)pr * n + j];
+          G[(long)pr * n + j] = tmp;
+        }
+      __syncthreads();
+      const double d = G[(long)k * n + k];
+      if (tid > k && tid < n) {
+        double l = G[(long)tid * n + k];
+        if (d != 0.) l /= d;
+        G[(long)tid * n + k] = l;
+      }
+      __syncthreads();
+      const int m = n - k - 1;
+      for (long e = tid; e < (long)m * m; e += BT) {
+        const int i = k + 1 + (int)(e / m), j = k + 1 + (int)(e % m);
+        G[(long)i * n + j] -= G[(long)i * n + k] * G[(long)k * n + j];
+      }
+      __syncthreads();
+    }
+    ++cnt[CNT_FACT];
+  }
+
+  // KernelDense::SolveLinearSystem with the factors of build_and_factorize:
+  // row interchanges, then column-oriented forward and back substitution.
+  __device__ double solve(double xl) {
+    const int n = ne;
+    W.X[tid] = tid < n ? xl : 0.;
+    __syncthreads();
+    if (tid == 0)
+      for (int k = 0; k < n; ++k) {
+        const int pk = W.PIV[k];
+        if (pk != k) {
+          const double tmp = W.X[k];
+          W.X[k] = W.X[pk];
+          W.X[pk] = tmp;
+        }
+      }
+    __syncthreads();
+    double x = W.X[tid];
+    for (int j = 0; j < n; ++j) {
+      if (tid == j) W.X[j] = x;   // x_j is final: publish it
+      __syncthreads();
+      const double v = W.X[j];
+      if (tid > j && tid < n) x -= G[(long)tid * n + j] * v;
+    }
+    for (int j = n - 1; j >= 0; --j) {
+      if (tid == j) {
+        x /= G[(long)j * n + j];
+        W.X[j] = x;
+      }
+      __syncthreads();
+      const double v = W.X[j];
+      if (tid < j) x -= G[(long)tid * n + j] * v;
+    }
+    __syncthreads();
+    ++cnt[CNT_SOLVE];
+    return tid < n ? x : 0.;
+  }
+
+  __device__ void set_initial_conditions(double tstart, double y0l) {
+    tOut = t = t0 = tInMeshPoint = tStabilize = tstart;
+    p = 1; iterOrder = 0; orderInNextStep = 1;
+    maxIterationsJacobian = 20 + 5 * (unsigned)(ne - 3);
+    if (maxIterationsJacobian > 50u && ne < 80) maxIterationsJacobian = 50u;
+    odeHStatus = H_CONST; odeOrderStatus = O_CONST; status = 1;
+    factorizationStatus = M_TO_FACT; jacobianStatus = JAC_CHANGE; convergenceStatus = CONV_OK;
+    h = 0.; hNextStep = 0.; hScale = 0.;
+    numberOfSteps = 0; numberOfConvergenceFailuresForOrderMax = 0;
+    iterConvergence = 0; iterConvergenceRate = 0; iterConvergenceFailure = 0; iterErrorFailure = 0;
+    stepOfLastJacobian = 0;
+    y0 = y0l;
+    hNordsieck = 0.; hScaleMax = 1000.;
+    fixedOrderMin = false; iterConstSteps = 0; iterMinimumOrder = 0;
+    for (int k = 0; k < NCNT; ++k) cnt[k] = 0;
+    f = rhs(y0);
+  }
+
+  __device__ unsigned find_correction() {   // MethodGear.hpp:195-341
+    vb = active ? V(0) : 0.;
+    check_constraints(vb);
+    f = rhs(vb);
+    if (numberOfSteps >= stepOfLastJacobian + maxIterationsJacobian) jacobianStatus = JAC_CHANGE;
+    if (jacobianStatus == JAC_CHANGE) {
+      stepOfLastJacobian = numberOfSteps;
+      jacobianStatus = JAC_MODIFIED;
+      numerical_jacobian(vb, f);
+      ++cnt[CNT_JAC];
+      factorizationStatus = M_TO_FACT;
+    }
+    const double r0 = c_gear_k.r[0][p - 1];
+    const double hr0 = h * r0;
+    if (factorizationStatus == M_FACT && iterOrder == 0) factorizationStatus = M_TO_FACT;
+    if (factorizationStatus == M_TO_FACT) {
+      build_and_factorize(hr0);
+      factorizationStatus = M_FACT;
+    }
+    deltab = f * h;
+    deltab -= active ? V(1) : 0.;
+    deltab = solve(deltab);
+    b = deltab;
+    double oldCC = 0.;
+    for (unsigned k = 1; k <= 4; ++k) {
+      const double cc = r0 * error_control(deltab);
+      if (cc < 1.) { convergenceStatus = CONV_OK; return k; }
+      if (k > 1 && cc > 2. * oldCC) { convergenceStatus = CONV_FAIL; return k; }
+      oldCC = cc;
+      va = b * r0;
+      va += active ? V(0) : 0.;
+      if (active) {
+        if (va < minv) { va = minv; b = (minv - Z(0)) / r0; }
+        if (va > maxv) { va = maxv; b = (maxv - Z(0)) / r0; }
+      }
+      f = rhs(va);
+      deltab = f * h;
+      deltab -= active ? V(1) : 0.;
+      deltab -= b;
+      deltab = solve(deltab);
+      b += deltab;
+    }
+    convergenceStatus = CONV_FAIL;
+    return 4;
+  }
+
+  __device__ void convergence_failure_recovery() {   // MethodGear.hpp:343-423
+    hScale = 0.25;
+    if (numberOfSteps < 10) hScale = 0.1;
+    hScale = fmax(hScale, 0. / fabs(h));
+    odeHStatus = H_DEC;
+    if (p > 1u) { p -= 1; odeOrderStatus = O_DEC; }
+    alfa2_4 -= 0.01;
+    alfa2_5 -= 0.02;
+    if (alfa2_4 < 0.) { alfa2_4 = 0.; maximum_order = 3; if (p > 3) { p = 3; odeOrderStatus = O_DEC; } }
+    if (alfa2_5 < 0.) { alfa2_5 = 0.; maximum_order = 4; if (p > 4) { p = 4; odeOrderStatus = O_DEC; } }
+    if (numberOfSteps > 5) {
+      numberOfConvergenceFailuresForOrderMax++;
+      if (numberOfConvergenceFailuresForOrderMax % 5 == 0 && p != 1u) { p = 1; odeOrderStatus = O_DEC; }
+      if (numberOfConvergenceFailuresForOrderMax % 10 == 0 && tStabilize != tInMeshPoint) {
+        va = rhs(active ? Z(0) : 0.);
+        if (active) Z(1) = va * h;
+        tStabilize = tInMeshPoint;
+      }
+    }
+    if (numberOfSteps > stepOfLastJacobian + 5u) jacobianStatus = JAC_CHANGE;
+    if (numberOfSteps != stepOfLastJacobian && iterConvergenceFailure == 50u) jacobianStatus = JAC_CHANGE;
+    hNextStep *= hScale;
+  }
+
+  __device__ void convergence_rate() {   // MethodGear.hpp:425-516
+    if (iterErrorFailure > 0 || iterConvergenceFailure > 0) iterConvergenceRate = 0;
+    if (iterConvergence <= 1) return;
+    const int n = ne;
+    W.X[tid] = active ? V(0) - Z(0) : 0.;
+    __syncthreads();
+    double s = 0.;
+    if (active)
+      for (int j = 0; j < n; ++j) s += J[(long)tid * n + j] * W.X[j];
+    va = s;
+    va *= h;
+    va += active ? Z(1) : 0.;
+    va = (active ? V(1) : 0.) - va;
+    const double normd = bsum<BT>(active ? fabs(va) : 0., W.red);
+    const double normf = bsum<BT>(active ? fabs(V(1)) : 0., W.red);
+    if (normd > 3. * normf + .1 && iterConvergence > 2) {
+      if (numberOfSteps > stepOfLastJacobian + 5u) jacobianStatus = JAC_CHANGE;
+      hScale = 0.5; odeHStatus = H_DEC; hNextStep = h * hScale;
+      if (p > 1) { orderInNextStep = p - 1; odeOrderStatus = O_DEC; }
+      iterConvergenceRate = 0; iterConvergenceFailure = 1;
+      return;
+    }
+    if (normd > normf + 0.1) {
+      iterConvergenceRate++;
+      if (iterConvergenceRate >= 5) {
+        hScale = 0.8; odeHStatus = H_DEC; hNextStep = h * hScale;
+        iterConvergenceRate = 0; iterConvergenceFailure = 1;
+      }
+      if (numberOfSteps > stepOfLastJacobian + 5u && iterConvergence > 2) {
+        jacobianStatus = JAC_CHANGE;
+        iterConvergenceRate = 0; iterConvergenceFailure = 1;
+      }
+    }
+  }
+
+  __device__ void multi_value_step() {   // MultiValueSolver.hpp:1212-1327
+    if (active) {
+      for (unsigned i = 0; i <= p; ++i) V(i) = Z(i);
+      for (int i = 0; i < int(p); ++i)
+        for (int j = int(p) - 1; j >= i; --j) V(j) += V(j + 1);
+      if (V(0) < minv && fabs(V(0) - minv) * eps < double(ne)) {
+        V(0) = minv; V(1) = minv - Z(0);
+        for (unsigned i = 2; i <= p; ++i) V(i) = 0.;
+      }
+      if (V(0) > maxv && fabs(V(0) - maxv) * eps < double(ne)) {
+        V(0) = maxv; V(1) = maxv - Z(0);
+        for (unsigned i = 2; i <= p; ++i) V(i) = 0.;
+      }
+    }
+    iterConvergence = find_correction();
+    if (convergenceStatus == CONV_FAIL) return;
+    const double r0 = c_gear_k.r[0][p - 1];
+    if (active) {
+      va = b * r0;
+      if (V(0) + va < minv) { b = minv - Z(0) - V(1); V(0) = minv - va; if (V(0) < minv) V(0) = minv; }
+      if (V(0) + va > maxv) { b = maxv - Z(0) - V(1); V(0) = maxv - va; if (V(0) > maxv) V(0) = maxv; }
+      V(0) += va;
+      V(1) += b;
+      for (unsigned i = 2; i <= p; ++i) V(i) += b * c_gear_k.r[i][p - 1];
+      V(p + 1) = (V(p) - Z(p)) / (double(p) + 1.);
+      if (iterOrder >= p) V(p + 2) = (V(p + 1) - Z(p + 1)) / (double(p) + 2.);
+    }
+  }
+
+  __device__ void new_order_new_h() {   // MultiValueSolver.hpp:1042-1210
+    double hMinus = 0., hCur = 0., hPlus = 0., alfa1 = 0., alfa3 = 0.;
+    if (p > 1u && odeOrderStatus != O_INC) {
+      hMinus = c_gear_k.Ep[p - 1] * error_control(active ? V(p) : 0.) + kMachEpsFloat;
+      hMinus = 1. / hMinus;
+      alfa1 = alfa2(p - 1) - .05;
+      hMinus = alfa1 * pow(hMinus, 1. / double(p));
+    }
+    hCur = c_gear_k.Ep[p] * error_control(active ? V(p + 1) : 0.) + kMachEpsFloat;
+    hCur = 1. / hCur;
+    hCur = alfa2(p) * pow(hCur, 1. / double(p + 1));
+    if (p < maximum_order && odeOrderStatus != O_DEC) {
+      hPlus = c_gear_k.Ep[p + 1] * error_control(active ? V(p + 2) : 0.) + kMachEpsFloat;
+      hPlus = 1. / hPlus;
+      alfa3 = alfa2(p + 1) - .25;
+      hPlus = alfa3 * pow(hPlus, 1. / double(p + 2));
+    }
+    if (hMinus > hCur && hMinus > hPlus) {
+      hScale = (.75 / alfa1) * hMinus; orderInNextStep = p - 1; odeOrderStatus = O_DEC;
+    } else if (hCur > hMinus && hCur > hPlus) {
+      hScale = (.75 / alfa2(p)) * hCur; orderInNextStep = p; odeOrderStatus = O_CONST;
+    } else {
+      hScale = (.75 / alfa3) * hPlus; orderInNextStep = p + 1; odeOrderStatus = O_INC;
+    }
+    if (fixedOrderMin) {
+      iterMinimumOrder++;
+      if (iterMinimumOrder < 2000) {
+        hScale = (.75 / alfa2(p)) * hCur; orderInNextStep = p; odeOrderStatus = O_CONST;
+      } else {
+        fixedOrderMin = false;
+      }
+    }
+    if (hScale < 1.2) {
+      iterConstSteps++;
+      hScale = 1.; odeHStatus = H_CONST; orderInNextStep = p; odeOrderStatus = O_CONST; hNextStep = h;
+    } else {
+      iterConstSteps = 0;
+      hScale = fmin(hScale, hScaleMax);
+      odeHStatus = H_INC;
+      hNextStep = h * hScale;
+    }
+    if (iterConstSteps > 500 ||
+        (numberOfSteps % 1000 == 0 && numberOfSteps != 0 && (fabs(h) < 1.e-7 || fabs(h) < 1.e-5 * t))) {
+      if (p > 1u) {
+        fixedOrderMin = true; iterMinimumOrder = 0;
+        orderInNextStep = 1; odeOrderStatus = O_DEC;
+        hScale = 0.5; hNextStep = h * hScale; odeHStatus = H_DEC;
+      }
+    }
+  }
+
+  __device__ void driver_step() {   // MultiValueSolver.hpp:753-1040
+    iterConvergenceFailure = 0; iterErrorFailure = 0; convergenceStatus = CONV_OK;
+    if (odeOrderStatus != O_CONST || odeHStatus != H_CONST) iterOrder = 0;
+    p = orderInNextStep;
+    odeOrderStatus = O_CONST;
+    hScaleMax = 2.;
+    if (numberOfSteps < 10) hScaleMax = 1000.;
+    else if (numberOfSteps > 10 && numberOfSteps < 20) hScaleMax = 10.;
+    for (int guard = 0; guard < 1000000; ++guard) {
+      if (odeHStatus != H_CONST) {
+        hScale = hNextStep / hNordsieck;
+        double hr = 1.;
+        for (unsigned i = 1; i <= p; ++i) {
+          hr *= hScale;
+          if (active) Z(i) *= hr;
+        }
+        if (active) { double z0 = Z(0); check_constraints(z0); Z(0) = z0; }
+        iterOrder = 0;
+        odeHStatus = H_CONST;
+      }
+      h = hNextStep;
+      hNordsieck = hNextStep;
+      t = tInMeshPoint + h;
+      if (t == tInMeshPoint) { status = -6; return; }
+      multi_value_step();
+      if (convergenceStatus == CONV_FAIL) {
+        iterConvergenceFailure++;
+        ++cnt[CNT_CONVFAIL];
+        if (iterConvergenceFailure >= 50u) { status = -5; return; }
+        if (fabs(h) <= 0.) { status = -6; return; }
+        convergence_failure_recovery();
+      } else {
+        double hCur = c_gear_k.Ep[p] * error_control(active ? V(p + 1) : 0.);
+        if (hCur > 1.) {
+          iterErrorFailure++;
+          ++cnt[CNT_ERRFAIL];
+          if (iterErrorFailure >= 50u) { status = -4; return; }
+          if (fabs(h) <= 0.) { status = -6; return; }
+          hScaleMax = 1.;
+          hCur = 0.8 * pow(1. / hCur, 1. / double(p + 1));
+          hScale = hCur;
+          if (p > 1u) {
+            double hMinus = c_gear_k.Ep[p - 1] * error_control(active ? V(p) : 0.);
+            hMinus = 1. / (hMinus + kMachEpsFloat);
+            hMinus = 0.8 * pow(hMinus, 1. / double(p));
+            if (hMinus > hCur) { hScale = hMinus; p -= 1; odeOrderStatus = O_DEC; }
+          }
+          hScale = fmin(hScale, 0.5);
+          hScale = fmax(hScale, 0. / fabs(h));
+          hScale = fmax(hScale, 1.e-3);
+          if (p == 1 && hScale < 0.1 && numberOfSteps > 10 && tInMeshPoint != tStabilize) {
+            va = rhs(active ? Z(0) : 0.);
+            if (active) Z(1) = va * h;
+            tStabilize = tInMeshPoint;
+          }
+          odeHStatus = H_DEC;
+          hNextStep *= hScale;
+        } else {
+          hNordsieck = h; hNextStep = h;
+          orderInNextStep = p; odeOrderStatus = O_CONST; odeHStatus = H_CONST;
+          convergence_rate();
+          if (iterErrorFailure > 0 || iterConvergenceFailure > 0) {
+            iterErrorFailure = 0; iterConvergenceFailure = 0;
+          } else {
+            iterOrder++;
+            if (iterOrder > p + 1) new_order_new_h();
+          }
+          if (active) {
+            for (unsigned i = 0; i <= p + 2; ++i) Z(i) = V(i);
+            double z0 = Z(0); check_constraints(z0); Z(0) = z0;
+          }
+          return;
+        }
+      }
+    }
+    status = -5;
+  }
+
+  // MultiValueSolver::Solve from a fresh initial condition (:423-617); on
+  // failure y holds the last accepted state.
+  __device__ int solve_to(double tEnd) {
+    tOut = tEnd;
+    const bool illegal = active && (y0 < minv || y0 > maxv);
+    if (__syncthreads_or(illegal)) { status = -9; y = y0; return status; }
+    one_over_epsilon(y0);
+    double lo, hi;
+    if (t0 != 0.) { lo = 100. * kMachEpsDouble * fabs(t0); hi = fabs(t0); }
+    else { lo = kMachEpsDouble; hi = 1.e-4; }
+    double h0 = 0.5 / (error_control(f) + kMachEpsFloat);
+    if (h0 < lo) h0 = lo;
+    if (h0 > hi) h0 = hi;
+    h0 *= fabs(tOut - t0) / (tOut - t0);
+    if (active) { Z(0) = y0; Z(1) = f * h0; }
+    hNordsieck = h0; hNextStep = h0;
+    status = 2;
+    for (unsigned k = 1; k <= max_number_steps; ++k) {
+      one_over_epsilon(active ? Z(0) : 0.);
+      const double tolSafe = kMachEpsDouble * error_control(active ? Z(0) : 0.);
+      if (tolSafe > 1.) { status = -2; y = active ? Z(0) : 0.; return status; }
+      tInMeshPoint = t;
+      driver_step();
+      if (status <= 0) { t = tInMeshPoint; y = active ? Z(0) : 0.; return status; }
+      numberOfSteps++;
+      ++cnt[CNT_STEPS];
+      if (tOut == t) { y = active ? Z(0) : 0.; return status; }
+      if (tOut < t) {
+        const double hp = (tOut - t) / hNordsieck;
+        double hr = 1.;
+        y = active ? Z(0) : 0.;
+        if (hp != 0.) {
+          for (unsigned i = 1; i <= p; ++i) {
+            hr *= hp;
+            if (active) y += Z(i) * hr;
+          }
+          check_constraints(y);
+        }
+        va = rhs(y);   // the reactor's QR at tOut
+        return status;
+      }
+    }
+    status = -1;
+    y = active ? Z(0) : 0.;
+    return status;
+  }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Persistent block-per-cell kernel: blocks take cells from the queue.
+// chemistry_DI.H:92-235: gather, clip and renormalise, integrate, renormalise, scatter.
+// ---------------------------------------------------------------------------
+template <int BT>
+__global__ void __launch_bounds__(BT) block_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem,
+                                                   StepOptions o, StepArgs a, double* __restrict__ ws_all,
+                                                   int* queue) {
+  extern __shared__ __align__(16) unsigned char bsm[];
+  __shared__ int s_cell;
+  const int tid = threadIdx.x;
+  const int NC = L.nc, ne = NC + 1;
+  const size_t wsd = block_ws_doubles(L);
+  double* ws = ws_all + (size_t)blockIdx.x * wsd;
+  BlockShared W;
+  {
+    double* p = (double*)bsm;
+    W.Z = p; p += 8 * BT;
+    W.V = p; p += 8 * BT;
+    W.C = p; p += NC;
+    W.H = p; p += NC;
+    W.S = p; p += NC;
+    W.NET = p; p += L.nr;
+    W.X = p; p += BT;
+    W.red = p; p += BT / 32 + 1;
+    W.slot = p; p += 4;
+    W.PIV = (int*)p;
+    W.ival = W.PIV + BT;
+  }
+  const MechView M{(const double*)mech_gmem, (const int*)(mech_gmem + (size_t)L.n_double * sizeof(double))};
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_cell = atomicAdd(queue, 1);
+    __syncthreads();
+    const long cell = s_cell;
+    if (cell >= a.ncells) break;
+    double yl = 0.;
+    if (tid < NC) yl = a.Y[(size_t)tid * a.ld + cell];
+    const double Tc = a.T[cell];
+    if (tid == NC) yl = Tc;
+    double yf = yl;
+    int st = 0;
+    long long nsteps = 0;
+    double Q = 0.;
+    if (Tc > o.tmin_chem) {
+      double y0 = yl;
+      if (tid < NC && y0 < 0.) y0 = 0.;
+      const double sum = bsum<BT>(tid < NC ? y0 : 0., W.red);
+      if (tid < NC) y0 /= sum;
+      if (tid == 0) { W.slot[1] = 0.; W.slot[2] = 0.; }
+      __syncthreads();
+      GearBlock<BT> g;
+      g.L = &L;
+      g.M = M;
+      g.W = W;
+      g.J = ws;
+      g.G = ws + (size_t)ne * ne;
+      g.karr = ws + 2 * (size_t)ne * ne;
+      g.ukeq = g.karr + L.nr;
+      g.kinf = g.ukeq + L.nr;
+      g.logf = g.kinf + (L.n_fo > 0 ? L.n_fo : 1);
+      g.P0 = a.p;
+      g.energy = o.energy;
+      g.tid = tid;
+      g.ne = ne;
+      g.active = tid < ne;
+      g.alfa2_4 = o.alfa2_4;
+      g.alfa2_5 = o.alfa2_5;
+      g.maximum_order = (unsigned)o.maximum_order;
+      g.max_number_steps = (unsigned)o.max_steps;
+      g.abs_tol = o.atol;
+      g.rel_tol = o.rtol;
+      g.minv = tid < NC ? 0. : o.y_min_T;
+      g.maxv = tid < NC ? 1. : o.y_max_T;
+      g.b = g.deltab = g.f = g.va = g.vb = g.y = 0.;
+      g.eps = 0.;
+      g.set_initial_conditions(a.t0, y0);
+      const double dtc = a.dt ? a.dt[cell] : a.dt_scalar;
+      st = g.solve_to(a.t0 + dtc);
+      yf = g.y;
+      nsteps = g.cnt[CNT_STEPS];
+      Q = W.slot[2];
+      if (tid == 0 && a.counters)
+        for (int k = 0; k < NCNT; ++k) a.counters[(size_t)cell * NCNT + k] = g.cnt[k];
+    } else if (tid == 0 && a.counters) {
+      for (int k = 0; k < NCNT; ++k) a.counters[(size_t)cell * NCNT + k] = 0;
+    }
+    // solvers/laminarSMOKE/utilities.H:153-200
+    const double s = bsum<BT>(tid < NC ? yf : 0., W.red);
+    if (tid < NC) a.Y[(size_t)tid * a.ld + cell] = yf / s;
+    if (tid == NC && o.energy) a.T[cell] = yf;
+    if (tid == 0) {
+      if (a.status) a.status[cell] = st;
+      if (a.nsteps) a.nsteps[cell] = (int)nsteps;
+      if (a.Q) a.Q[cell] = Q;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stand-alone RHS for large mechanisms: one block per state (the same
+// arithmetic as inside the block step).  y/dy species-major [(NC+1) * ld].
+// ---------------------------------------------------------------------------
+template <int BT>
+__global__ void __launch_bounds__(BT) rhs_block_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem,
+                                                       long ncells, const double* __restrict__ y,
+                                                       double* __restrict__ dy, long ld, double p, int energy,
+                                                       double* qr, double* __restrict__ ws_all) {
+  extern __shared__ __align__(16) unsigned char bsm[];
+  const int tid = threadIdx.x;
+  const int NC = L.nc;
+  double* ws = ws_all + (size_t)blockIdx.x * block_ws_doubles(L);
+  const size_t n = NC + 1;
+  double* karr = ws + 2 * n * n;
+  double* ukeq = karr + L.nr;
+  double* kinf = ukeq + L.nr;
+  double* logf = kinf + (L.n_fo > 0 ? L.n_fo : 1);
+  BlockShared W;
+  {
+    double* q = (double*)bsm;
+    W.Z = q; q += 8 * BT;
+    W.V = q; q += 8 * BT;
+    W.C = q; q += NC;
+    W.H = q; q += NC;
+    W.S = q; q += NC;
+    W.NET = q; q += L.nr;
+    W.X = q; q += BT;
+    W.red = q; q += BT / 32 + 1;
+    W.slot = q; q += 4;
+    W.PIV = (int*)q;
+    W.ival = W.PIV + BT;
+  }
+  const MechView M{(const double*)mech_gmem, (const int*)(mech_gmem + (size_t)L.n_double * sizeof(double))};
+  for (long cell = blockIdx.x; cell < ncells; cell += gridDim.x) {
+    __syncthreads();
+    if (tid == 0) { W.slot[1] = 0.; W.slot[2] = 0.; }
+    const double yl = tid <= NC ? y[(size_t)tid * ld + cell] : 0.;
+    const double T = bcast(yl, NC, W.slot);
+    const double d = rhs_block<BT>(L, M, W, karr, ukeq, kinf, logf, yl, T, p, energy);
+    if (tid <= NC) dy[(size_t)tid * ld + cell] = d;
+    if (tid == 0 && qr) qr[cell] = W.slot[2];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+namespace {
+
+template <int BT>
+cudaError_t block_setup(const MechLayout& L, size_t* smem, int* bps) {
+  *smem = block_shared_bytes<BT>(L);
+  cudaError_t e = cudaFuncSetAttribute(block_kernel<BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, block_kernel<BT>, BT, *smem);
+}
+
+int block_threads(const MechLayout& L) {
+  const int n = L.nc + 1;
+  return n <= 128 ? 128 : (n <= 256 ? 256 : 512);
+}
+
+}  // namespace
+
+cudaError_t upload_gear_block(const GearConsts& gc) { return cudaMemcpyToSymbol(c_gear_k, &gc, sizeof(GearConsts)); }
+
+size_t block_ws_bytes(const MechLayout& L) { return block_ws_doubles(L) * sizeof(double); }
+
+cudaError_t block_plan(const MechLayout& L, int sm_count, long* nblocks) {
+  if (L.nc + 1 > kBlkMaxN) return cudaErrorInvalidValue;
+  size_t smem = 0;
+  int bps = 0;
+  const int bt = block_threads(L);
+  cudaError_t e = bt == 128 ? block_setup<128>(L, &smem, &bps)
+                            : (bt == 256 ? block_setup<256>(L, &smem, &bps) : block_setup<512>(L, &smem, &bps));
+  if (e != cudaSuccess) return e;
+  if (bps <= 0 || smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+  *nblocks = (long)sm_count * bps;
+  return cudaSuccess;
+}
+
+cudaError_t launch_block(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                         const StepArgs& a, double* ws, long nblocks, int* queue, cudaStream_t stream) {
+  if (a.ncells <= 0) return cudaSuccess;
+  long g = nblocks < a.ncells ? nblocks : a.ncells;
+  cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  const int bt = block_threads(L);
+  if (bt == 128) block_kernel<128><<<(unsigned)g, 128, block_shared_bytes<128>(L), stream>>>(L, mech_gmem, o, a, ws, queue);
+  else if (bt == 256) block_kernel<256><<<(unsigned)g, 256, block_shared_bytes<256>(L), stream>>>(L, mech_gmem, o, a, ws, queue);
+  else block_kernel<512><<<(unsigned)g, 512, block_shared_bytes<512>(L), stream>>>(L, mech_gmem, o, a, ws, queue);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rhs_block(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y,
+                             double* dy, long ld, double p, int energy, double* qr, double* ws, long nblocks,
+                             cudaStream_t stream) {
+  if (ncells <= 0) return cudaSuccess;
+  const long g = nblocks < ncells ? nblocks : ncells;
+  const int bt = block_threads(L);
+  cudaError_t e;
+  if (bt == 128) {
+    e = cudaFuncSetAttribute(rhs_block_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)block_shared_bytes<128>(L));
+    if (e != cudaSuccess) return e;
+    rhs_block_kernel<128><<<(unsigned)g, 128, block_shared_bytes<128>(L), stream>>>(L, mech_gmem, ncells, y, dy, ld,
+                                                                                     p, energy, qr, ws);
+  } else if (bt == 256) {
+    e = cudaFuncSetAttribute(rhs_block_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)block_shared_bytes<256>(L));
+    if (e != cudaSuccess) return e;
+    rhs_block_kernel<256><<<(unsigned)g, 256, block_shared_bytes<256>(L), stream>>>(L, mech_gmem, ncells, y, dy, ld,
+                                                                                     p, energy, qr, ws);
+  } else {
+    e = cudaFuncSetAttribute(rhs_block_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)block_shared_bytes<512>(L));
+    if (e != cudaSuccess) return e;
+    rhs_block_kernel<512><<<(unsigned)g, 512, block_shared_bytes<512>(L), stream>>>(L, mech_gmem, ncells, y, dy, ld,
+                                                                                     p, energy, qr, ws);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace lsg

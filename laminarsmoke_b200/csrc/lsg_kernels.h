@@ -54,6 +54,16 @@ cudaError_t batched_occupancy(const MechLayout& L, bool lu64, int* blocks_per_sm
 cudaError_t launch_batched(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
                            const StepArgs& a, double* slots, long nslots, const int* order, int* queue, bool lu64,
                            int* err, cudaStream_t stream);
+// Block-per-cell step for mechanisms of up to 511 species (lsg_block.cu).
+cudaError_t upload_gear_block(const GearConsts& gc);
+size_t block_ws_bytes(const MechLayout& L);
+cudaError_t block_plan(const MechLayout& L, int sm_count, long* nblocks);
+cudaError_t launch_block(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                         const StepArgs& a, double* ws, long nblocks, int* queue, cudaStream_t stream);
+cudaError_t launch_rhs_block(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y,
+                             double* dy, long ld, double p, int energy, double* qr, double* ws, long nblocks,
+                             cudaStream_t stream);
+
 // Fixed device scratch of the no-allocation entry point (lsg_batched.cu).
 constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
 long batched_noalloc_slots(const MechLayout& L, bool lu64, int sm_count);
@@ -64,7 +74,7 @@ cudaError_t launch_batched_noalloc(const MechLayout& L, const unsigned char* mec
 // Optional device timing of each kernel kind with CUDA events recorded on the
 // launching stream (lsg_options.kernel_timing).  Pairs are collected after the
 // stream has been synchronised.
-enum { KT_RHS = 0, KT_ADVANCE, KT_COMPACT, KT_INIT, KT_PLAIN, KT_PERSISTENT, KT_NKINDS };
+enum { KT_RHS = 0, KT_ADVANCE, KT_COMPACT, KT_INIT, KT_PLAIN, KT_PERSISTENT, KT_BLOCK, KT_NKINDS };
 struct KernelTimer {
   static constexpr int kPairs = 64;
   bool on = false;

@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "liblsmoke_gpu.so")
 
 LSG_PRECISION_FP64 = 0
 LSG_PRECISION_MIXED = 1
-LSG_TILE_AUTO, LSG_TILE_WARP, LSG_TILE_LANE, LSG_TILE_PERSISTENT = 0, 1, 2, 3
+LSG_TILE_AUTO, LSG_TILE_WARP, LSG_TILE_LANE, LSG_TILE_PERSISTENT, LSG_TILE_BLOCK = 0, 1, 2, 3, 4
 LSG_ERR_SCRATCH = -8
 NOALLOC_SCRATCH_BYTES = 16 << 20
 NCOUNTERS = 8
@@ -219,7 +219,7 @@ class ReactionStep:
         """Kernels this context has enqueued so far."""
         return int(lib().lsg_ctx_launches(self.h))
 
-    KERNEL_KINDS = ("rhs", "advance", "compact", "init", "plain", "persistent")
+    KERNEL_KINDS = ("rhs", "advance", "compact", "init", "plain", "persistent", "block")
 
     def kernel_times(self, reset: bool = False) -> dict:
         """{kind: (total ms, timed launches)} from the CUDA events recorded when

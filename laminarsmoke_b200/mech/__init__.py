@@ -7,7 +7,11 @@ workloads of this project use:
                    reference's CHEMKIN files into ``data/POLIMI_H2CO_1412.lsmech``
                    by ``mech/build_data.py``;
 * ``"syn120"``  -- seeded synthetic C1-C2 mechanism, 120 species / 800 reactions;
-* ``"syn500"``  -- seeded synthetic mechanism, 500 species / 3 000 reactions.
+* ``"syn500"``  -- seeded synthetic mechanism, 500 species / 3 000 reactions;
+* ``"h2co+K"``  -- POLIMI_H2CO_1412 with K chemically inert copies of N2 added
+                   (``pad_inert``): the H2/CO chemistry in a mechanism of 14 + K
+                   species, which exercises the large-mechanism path with
+                   realistic stiffness.
 """
 from __future__ import annotations
 
@@ -25,8 +29,30 @@ SYNTHETIC = {
 }
 
 
+def pad_inert(data: bytes, k: int, template: str = "N2") -> Tuple[bytes, List[str]]:
+    """The mechanism in `data` with `k` extra species that take part in no
+    reaction and have the thermodynamics and molecular weight of `template`
+    (collision efficiency 1 wherever third bodies appear)."""
+    import numpy as np
+    A, species = _blob.unpack(data)
+    A = {key: np.array(v) for key, v in A.items()}
+    t = species.index(template)
+    nc = int(A["dims"][0])
+    per = {"mw": 1, "t_mid": 1, "t_low": 1, "t_high": 1, "cp_ht": 5, "cp_lt": 5, "dh_ht": 6, "dh_lt": 6,
+           "ds_ht": 6, "ds_lt": 6, "nasa_raw": A["nasa_raw"].size // nc}
+    for key, w in per.items():
+        row = A[key][t * w:(t + 1) * w]
+        A[key] = np.concatenate([A[key]] + [row] * k)
+    A["fr_ptr"] = np.concatenate([A["fr_ptr"], np.full(k, A["fr_ptr"][-1], A["fr_ptr"].dtype)])
+    A["dims"] = np.array([nc + k, A["dims"][1]], A["dims"].dtype)
+    names = list(species) + [f"INERT{i + 1}" for i in range(k)]
+    return _blob.pack(A, names), names
+
+
 @functools.lru_cache(maxsize=8)
 def load(name: str) -> Tuple[bytes, List[str]]:
+    if name.startswith("h2co+"):
+        return pad_inert(load("h2co")[0], int(name[5:]))
     if name == "h2co":
         path = os.path.join(DATA, "POLIMI_H2CO_1412.lsmech")
         with open(path, "rb") as f:

@@ -1181,9 +1181,12 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
 }
 
 // ---------------------------------------------------------------------------
-// compact: cells still integrating form the next list (warp-aggregated append).
+// compact: cells still integrating form the next list (warp-aggregated append),
+// binned by the RHS they asked for -- Jacobian columns, predictor evaluations,
+// then the rest -- in three passes (cls 1, 2, 3), so that the cells that share
+// a warp in the next advance mostly take the same solver path.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kCT) rounds_compact_kernel(RoundBufs B, int par) {
+__global__ void __launch_bounds__(kCT) rounds_compact_kernel(RoundBufs B, int par, int cls) {
   const int nact = B.nact[par];
   const int* in = par ? B.act1 : B.act0;
   int* out = par ? B.act0 : B.act1;
@@ -1194,7 +1197,9 @@ __global__ void __launch_bounds__(kCT) rounds_compact_kernel(RoundBufs B, int pa
   for (int base = gw * 32; base < nact; base += nw * 32) {
     const int idx = base + lane;
     const int cell = idx < nact ? in[idx] : 0;
-    const bool alive = idx < nact && ((const int*)(B.rec + (long)cell * B.L.RS + ND_))[I_PHASE] != PH_DONE;
+    const int ph = idx < nact ? ((const int*)(B.rec + (long)cell * B.L.RS + ND_))[I_PHASE] : PH_DONE;
+    const bool alive = ph != PH_DONE &&
+                       (cls == 1 ? ph == PH_JAC : (cls == 2 ? ph == PH_PRED : (ph != PH_JAC && ph != PH_PRED)));
     const unsigned m = __ballot_sync(kFull, alive);
     int off = 0;
     if (lane == 0 && m) off = atomicAdd(cnt, __popc(m));
@@ -1305,9 +1310,9 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
       }
       kt->end(stream);
       kt->begin(KT_COMPACT, stream);
-      rounds_compact_kernel<<<P.g_cmp, kCT, 0, stream>>>(B, par);
+      for (int cls = 1; cls <= 3; ++cls) rounds_compact_kernel<<<P.g_cmp, kCT, 0, stream>>>(B, par, cls);
       kt->end(stream);
-      *launches += 3;
+      *launches += 5;
       par ^= 1;
     }
     e = cudaGetLastError();

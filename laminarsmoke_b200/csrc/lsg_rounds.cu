@@ -40,6 +40,7 @@ constexpr int kWA = 4;         // warps per block of the advance kernel (one cel
 constexpr int kAT = 128;       // threads per block of the init kernel
 constexpr int kCT = 256;       // threads per block of the compaction kernel
 constexpr int kRefineR = 1;    // refinement sweeps of a solve with FP32 factors
+constexpr int kBins = 6;       // solver-path bins of the compaction
 
 enum Phase : int {
   PH_DONE = 0,
@@ -1182,9 +1183,10 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
 
 // ---------------------------------------------------------------------------
 // compact: cells still integrating form the next list (warp-aggregated append),
-// binned by the RHS they asked for -- Jacobian columns, predictor evaluations,
-// then the rest -- in three passes (cls 1, 2, 3), so that the cells that share
-// a warp in the next advance mostly take the same solver path.
+// binned by the solver path their next advance will take -- Jacobian columns;
+// predictor results that start a Jacobian, that need a factorisation, that
+// need neither; Newton iterates; the rest -- one pass per bin (cls 1..kBins),
+// so that the cells that share a warp mostly take the same path.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kCT) rounds_compact_kernel(RoundBufs B, int par, int cls) {
   const int nact = B.nact[par];
@@ -1197,9 +1199,21 @@ __global__ void __launch_bounds__(kCT) rounds_compact_kernel(RoundBufs B, int pa
   for (int base = gw * 32; base < nact; base += nw * 32) {
     const int idx = base + lane;
     const int cell = idx < nact ? in[idx] : 0;
-    const int ph = idx < nact ? ((const int*)(B.rec + (long)cell * B.L.RS + ND_))[I_PHASE] : PH_DONE;
-    const bool alive = ph != PH_DONE &&
-                       (cls == 1 ? ph == PH_JAC : (cls == 2 ? ph == PH_PRED : (ph != PH_JAC && ph != PH_PRED)));
+    const int* RI = idx < nact ? (const int*)(B.rec + (long)cell * B.L.RS + ND_) : nullptr;
+    const int ph = RI ? RI[I_PHASE] : PH_DONE;
+    int bin = 6;
+    if (ph == PH_JAC) {
+      bin = 1;
+    } else if (ph == PH_PRED) {
+      // the tests of MethodGear::FindCorrection (MethodGear.hpp:205-240) that the advance makes next
+      const bool jac = RI[I_JACCHANGE] != 0 ||
+                       (unsigned)RI[I_NSTEPS] >= (unsigned)RI[I_STEPLASTJ] + (unsigned)RI[I_MAXITJ];
+      const bool fact = RI[I_FACTORIZED] == 0 || RI[I_ITORDER] == 0;
+      bin = jac ? 2 : (fact ? 3 : 4);
+    } else if (ph == PH_NEWTON) {
+      bin = 5;
+    }
+    const bool alive = ph != PH_DONE && bin == cls;
     const unsigned m = __ballot_sync(kFull, alive);
     int off = 0;
     if (lane == 0 && m) off = atomicAdd(cnt, __popc(m));
@@ -1310,9 +1324,9 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
       }
       kt->end(stream);
       kt->begin(KT_COMPACT, stream);
-      for (int cls = 1; cls <= 3; ++cls) rounds_compact_kernel<<<P.g_cmp, kCT, 0, stream>>>(B, par, cls);
+      for (int cls = 1; cls <= kBins; ++cls) rounds_compact_kernel<<<P.g_cmp, kCT, 0, stream>>>(B, par, cls);
       kt->end(stream);
-      *launches += 5;
+      *launches += 2 + kBins;
       par ^= 1;
     }
     e = cudaGetLastError();

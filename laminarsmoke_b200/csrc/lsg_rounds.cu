@@ -470,6 +470,9 @@ struct RoundBufs {
   int* act0;        // active lists (round parity 0 / 1)
   int* act1;
   int* nact;        // [2] list lengths
+  unsigned char* bin;   // [capacity] bin of each list entry (compaction)
+  int* bcnt;        // [kBins + 1] entries per bin
+  int* bcur;        // [kBins + 1] append cursors per bin
 };
 
 }  // namespace
@@ -536,7 +539,10 @@ __global__ void __launch_bounds__(kRT) rounds_rhs_kernel(MechLayout Lp, const un
   __shared__ __align__(8) uint64_t mbar;
   __shared__ MechLayout sL;
   if (threadIdx.x == 0) sL = Lp;
-  if (blockIdx.x == 0 && threadIdx.x == 0) B.nact[par ^ 1] = 0;   // this round's compaction appends there
+  if (blockIdx.x == 0 && threadIdx.x < 2 * (kBins + 1)) {   // this round's compaction counts from zero
+    if (threadIdx.x < kBins + 1) B.bcnt[threadIdx.x] = 0;
+    else B.bcur[threadIdx.x - kBins - 1] = 0;
+  }
   if (!stage_bulk(smem, mech_gmem, Lp.bytes, &mbar, err)) return;
   const double* Md = (const double*)smem;
   const int* Mi = (const int*)(smem + (size_t)Lp.n_double * sizeof(double));
@@ -1182,43 +1188,64 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
 }
 
 // ---------------------------------------------------------------------------
-// compact: cells still integrating form the next list (warp-aggregated append),
-// binned by the solver path their next advance will take -- Jacobian columns;
-// predictor results that start a Jacobian, that need a factorisation, that
-// need neither; Newton iterates; the rest -- one pass per bin (cls 1..kBins),
-// so that the cells that share a warp mostly take the same path.
+// compact: the cells still integrating form the next list, binned by the solver
+// path their next advance will take -- Jacobian columns; predictor results that
+// start a Jacobian, that need a factorisation, that need neither; Newton
+// iterates; the rest -- so that the cells that share a warp mostly take the
+// same path.  Two kernels: count (bin of every entry, per-bin totals) and
+// scatter (warp-aggregated appends into each bin's range).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kCT) rounds_compact_kernel(RoundBufs B, int par, int cls) {
+__device__ __forceinline__ int cell_bin(const RoundBufs& B, int cell) {
+  const int* RI = (const int*)(B.rec + (long)cell * B.L.RS + ND_);
+  const int ph = RI[I_PHASE];
+  if (ph == PH_DONE) return 0;
+  if (ph == PH_JAC) return 1;
+  if (ph == PH_PRED) {
+    // the tests of MethodGear::FindCorrection (MethodGear.hpp:205-240) that the advance makes next
+    const bool jac = RI[I_JACCHANGE] != 0 ||
+                     (unsigned)RI[I_NSTEPS] >= (unsigned)RI[I_STEPLASTJ] + (unsigned)RI[I_MAXITJ];
+    const bool fact = RI[I_FACTORIZED] == 0 || RI[I_ITORDER] == 0;
+    return jac ? 2 : (fact ? 3 : 4);
+  }
+  return ph == PH_NEWTON ? 5 : 6;
+}
+
+__global__ void __launch_bounds__(kCT) rounds_count_kernel(RoundBufs B, int par) {
   const int nact = B.nact[par];
   const int* in = par ? B.act1 : B.act0;
-  int* out = par ? B.act0 : B.act1;
-  int* cnt = B.nact + (par ^ 1);
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * kCT + threadIdx.x) >> 5;
   const int nw = gridDim.x * (kCT / 32);
   for (int base = gw * 32; base < nact; base += nw * 32) {
     const int idx = base + lane;
-    const int cell = idx < nact ? in[idx] : 0;
-    const int* RI = idx < nact ? (const int*)(B.rec + (long)cell * B.L.RS + ND_) : nullptr;
-    const int ph = RI ? RI[I_PHASE] : PH_DONE;
-    int bin = 6;
-    if (ph == PH_JAC) {
-      bin = 1;
-    } else if (ph == PH_PRED) {
-      // the tests of MethodGear::FindCorrection (MethodGear.hpp:205-240) that the advance makes next
-      const bool jac = RI[I_JACCHANGE] != 0 ||
-                       (unsigned)RI[I_NSTEPS] >= (unsigned)RI[I_STEPLASTJ] + (unsigned)RI[I_MAXITJ];
-      const bool fact = RI[I_FACTORIZED] == 0 || RI[I_ITORDER] == 0;
-      bin = jac ? 2 : (fact ? 3 : 4);
-    } else if (ph == PH_NEWTON) {
-      bin = 5;
-    }
-    const bool alive = ph != PH_DONE && bin == cls;
-    const unsigned m = __ballot_sync(kFull, alive);
+    const int bin = idx < nact ? cell_bin(B, in[idx]) : 0;
+    if (idx < nact) B.bin[idx] = (unsigned char)bin;
+    const unsigned peers = __match_any_sync(kFull, bin);
+    if (bin > 0 && lane == __ffs(peers) - 1) atomicAdd(B.bcnt + bin, __popc(peers));
+  }
+}
+
+__global__ void __launch_bounds__(kCT) rounds_scatter_kernel(RoundBufs B, int par) {
+  const int nact = B.nact[par];
+  const int* in = par ? B.act1 : B.act0;
+  int* out = par ? B.act0 : B.act1;
+  int start[kBins + 1];
+  start[0] = 0;
+  start[1] = 0;
+  for (int b = 2; b <= kBins; ++b) start[b] = start[b - 1] + B.bcnt[b - 1];
+  if (blockIdx.x == 0 && threadIdx.x == 0) B.nact[par ^ 1] = start[kBins] + B.bcnt[kBins];
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * kCT + threadIdx.x) >> 5;
+  const int nw = gridDim.x * (kCT / 32);
+  for (int base = gw * 32; base < nact; base += nw * 32) {
+    const int idx = base + lane;
+    const int bin = idx < nact ? B.bin[idx] : 0;
+    const unsigned peers = __match_any_sync(kFull, bin);
+    const int leader = __ffs(peers) - 1;
     int off = 0;
-    if (lane == 0 && m) off = atomicAdd(cnt, __popc(m));
-    off = __shfl_sync(kFull, off, 0);
-    if (alive) out[off + __popc(m & ((1u << lane) - 1u))] = cell;
+    if (bin > 0 && lane == leader) off = atomicAdd(B.bcur + bin, __popc(peers));
+    off = __shfl_sync(kFull, off, leader);
+    if (bin > 0) out[start[bin] + off + __popc(peers & ((1u << lane) - 1u))] = in[idx];
   }
 }
 
@@ -1237,7 +1264,10 @@ RoundBufs carve(const MechLayout& L, void* base, long cap, bool lu64) {
   p += sizeof(double) * (size_t)B.L.RS * cap;
   B.act0 = (int*)p; p += list_bytes(cap);
   B.act1 = (int*)p; p += list_bytes(cap);
+  B.bin = (unsigned char*)p; p += (cap + 255) & ~255L;
   B.nact = (int*)p;
+  B.bcnt = B.nact + 4;
+  B.bcur = B.bcnt + 8;
   return B;
 }
 
@@ -1260,7 +1290,7 @@ cudaError_t prepare_advance(size_t as, int* bps) {
 
 size_t rounds_bytes(const MechLayout& L, long cap, bool lu64) {
   const RecLayout R = rec_layout(L.nc + 1, lu64);
-  return sizeof(double) * (size_t)R.RS * cap + 2 * list_bytes(cap) + 256;
+  return sizeof(double) * (size_t)R.RS * cap + 2 * list_bytes(cap) + ((cap + 255) & ~255L) + 256;
 }
 
 cudaError_t upload_gear_rounds(const GearConsts& gc) { return cudaMemcpyToSymbol(c_gear_r, &gc, sizeof(GearConsts)); }
@@ -1281,7 +1311,7 @@ cudaError_t rounds_prepare(const MechLayout& L, bool lu64, int sm_count, RoundsP
   if (lu64) e = n <= 16 ? prepare_advance<double, 16>(P->adv_smem, &adv_bps) : prepare_advance<double, 32>(P->adv_smem, &adv_bps);
   else e = n <= 16 ? prepare_advance<float, 16>(P->adv_smem, &adv_bps) : prepare_advance<float, 32>(P->adv_smem, &adv_bps);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cmp_bps, rounds_compact_kernel, kCT, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cmp_bps, rounds_scatter_kernel, kCT, 0);
   if (e != cudaSuccess) return e;
   if (rhs_bps <= 0 || adv_bps <= 0 || cmp_bps <= 0) return cudaErrorInvalidConfiguration;
   // persistent grids: every kernel fills the GPU once and strides over the list
@@ -1324,9 +1354,10 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
       }
       kt->end(stream);
       kt->begin(KT_COMPACT, stream);
-      for (int cls = 1; cls <= kBins; ++cls) rounds_compact_kernel<<<P.g_cmp, kCT, 0, stream>>>(B, par, cls);
+      rounds_count_kernel<<<P.g_cmp, kCT, 0, stream>>>(B, par);
+      rounds_scatter_kernel<<<P.g_cmp, kCT, 0, stream>>>(B, par);
       kt->end(stream);
-      *launches += 2 + kBins;
+      *launches += 4;
       par ^= 1;
     }
     e = cudaGetLastError();

@@ -80,6 +80,16 @@ def kernel_roofline(args, ktimes, counters, nc, ncells, hbm, peak_src):
             "note": "latency-bound BDF solver kernel; bytes are its solver-record traffic"}
 
 
+def tuning_report(ctx, lsg):
+    t = ctx.tuning()
+    if t is None:
+        return None
+    tile, width, rates = t
+    names = {lsg.LSG_TILE_LANE: f"round scheme, {width} lanes per cell", lsg.LSG_TILE_WARP: "plain warp kernel",
+             lsg.LSG_TILE_PERSISTENT: "persistent lane kernel"}
+    return {"chosen": names.get(tile, str(tile)), "sample_cells_per_s": {k: round(v) for k, v in rates.items() if v}}
+
+
 def max_over_ranks(x: float, world: int, device) -> float:
     """The slowest rank's time (every rank calls it, same order, every step)."""
     if world <= 1:
@@ -107,8 +117,9 @@ def parse():
     ap.add_argument("--cells", type=int, default=NCELLS)
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="cells of the CPU baseline sample (0: sized for about 10 s of CPU work)")
-    ap.add_argument("--tile", choices=("lane", "persistent"), default="lane",
-                    help="batched form: round scheme (lane) or persistent lane kernel")
+    ap.add_argument("--tile", choices=("auto", "lane", "persistent"), default="auto",
+                    help="batched form: autotuned (the first warm-up step times the candidate forms), round "
+                         "scheme (lane) or persistent lane kernel")
     ap.add_argument("--factors", choices=("fp32", "fp64"), default="fp32",
                     help="batched form: precision of the LU factors")
     ap.add_argument("--no-e2e", action="store_true")
@@ -272,9 +283,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     n = Y.shape[0]
     nc = Y.shape[1]
     if args.form == "mixed":
-        tile = lsg.LSG_TILE_LANE if args.tile == "lane" else lsg.LSG_TILE_PERSISTENT
+        tile = {"lane": lsg.LSG_TILE_LANE, "persistent": lsg.LSG_TILE_PERSISTENT, "auto": lsg.LSG_TILE_AUTO}[args.tile]
         prec = lsg.LSG_PRECISION_MIXED if args.factors == "fp32" else lsg.LSG_PRECISION_FP64
-        ctx = lsg.ReactionStep(m, tile=tile, precision=prec, kernel_timing=1)
+        ctx = lsg.ReactionStep(m, tile=tile, precision=prec, kernel_timing=1, autotune=int(args.tile == "auto"))
         dtype = "f64+f32" if args.factors == "fp32" else "f64"
     else:
         ctx = plain
@@ -370,6 +381,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline,
             "kernel_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in ktimes.items() if v[1]},
+            "autotune": tuning_report(ctx, lsg) if args.form == "mixed" else None,
             "fp64_work": {"algorithmic_tflops": flops / (ms_per_step / 1e3) / 1e12 if ms_per_step > 0 else None,
                           "flops_per_cell_step": flops / n,
                           "bdf_steps_per_cell": nsteps_total / n,

@@ -83,7 +83,9 @@ typedef struct lsg_options {
   int maximum_order;
   int tile;             /* LSG_TILE_* */
   int kernel_timing;    /* 1: time every kernel kind with CUDA events (lsg_ctx_kernel_times) */
-  int reserved[5];
+  int autotune;         /* 1 with tile LSG_TILE_AUTO: the first step times the candidate forms on a sample of
+                           its own cells and keeps the fastest (lsg_ctx_tuning) */
+  int reserved[4];
 } lsg_options;
 
 void lsg_options_default(lsg_options* opt);
@@ -146,6 +148,15 @@ long long lsg_ctx_launches(const lsg_ctx* ctx);
  * clears the totals after reading.  Waits for the last timed kernel. */
 #define LSG_NKERNEL_KINDS 7
 int lsg_ctx_kernel_times(lsg_ctx* ctx, double* ms, long long* launches, int nkinds, int reset);
+
+/* Result of the autotuner (lsg_options.autotune; no counterpart in the
+ * reference): the chosen tile and lane-group width (16 or 32 lanes per cell in
+ * the round scheme, 0 otherwise) and the measured cells/s of the candidates, in
+ * the order round scheme 16 lanes, round scheme 32 lanes, plain warp kernel,
+ * persistent lane kernel (0 for a candidate not tried).  Returns
+ * LSG_ERR_ARG when no tuning has run yet. */
+#define LSG_NTUNE_CANDIDATES 4
+int lsg_ctx_tuning(const lsg_ctx* ctx, int* tile, int* width, double* rates);
 
 /* Waits for the device, then reads and clears the error flags kernels raised
  * (0 = none).  Returns LSG_ERR_DEVICE when a flag was set. */

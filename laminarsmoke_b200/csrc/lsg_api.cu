@@ -53,6 +53,13 @@ struct lsg_ctx {
   long bws_blocks = 0;
   int* bqueue = nullptr;
   KernelTimer timer;          // per-kernel device time (lsg_options.kernel_timing)
+  // autotuner (lsg_options.autotune)
+  bool tuned = false;
+  int tuned_tile = 0, tuned_w = 0;
+  double tune_rate[LSG_NTUNE_CANDIDATES] = {};
+  double* tune_buf = nullptr;   // sample cells: pristine copy and work copy
+  long tune_cap = 0;
+  int rplan_w = -1;             // lane-group width the round plan was prepared for
 };
 
 namespace {
@@ -198,12 +205,14 @@ int ensure_rounds(lsg_ctx* c, long n, bool lu64) {
   const MechLayout& L = c->mech->host.layout;
   if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
   if (!sm_count(c)) return LSG_ERR_CUDA;
-  if (c->rplan_lu64 != (int)lu64) {
-    if (rounds_prepare(L, lu64, c->sm_count, &c->rplan) != cudaSuccess) {
+  const int w = c->tuned ? c->tuned_w : 0;
+  if (c->rplan_lu64 != (int)lu64 || c->rplan_w != w) {
+    if (rounds_prepare(L, lu64, c->sm_count, w, &c->rplan) != cudaSuccess) {
       cudaGetLastError();
       return LSG_ERR_UNSUPPORTED;
     }
     c->rplan_lu64 = (int)lu64;
+    c->rplan_w = w;
   }
   if (!c->nact_host && cudaMallocHost(&c->nact_host, 2 * sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
@@ -251,10 +260,109 @@ int launch_large(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
   return LSG_OK;
 }
 
+int launch_tile(lsg_ctx* c, const StepArgs& a, cudaStream_t s, int tile);
+
+// Autotuner: times the candidate forms on (a copy of) the first cells of the
+// call (up to 262,144) and keeps the fastest for tile LSG_TILE_AUTO.  Candidates: round scheme
+// with 16-lane groups (two cells per warp, up to 16 equations) and with 32-lane
+// groups, the plain warp kernel (FP64 only) and the persistent lane kernel.
+int autotune(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
+  const MechLayout& L = c->mech->host.layout;
+  const int nc = L.nc, n = nc + 1;
+  // The round scheme needs many cells to hide its latency: a small sample would
+  // under-rate it, so the sample is up to 262,144 cells (a one-time cost).
+  const long m = a.ncells < 262144 ? a.ncells : 262144;
+  const size_t per = (size_t)nc * m + 2 * (size_t)m;   // Y rows, T, dt
+  if (c->tune_cap < m) {
+    cudaFree(c->tune_buf);
+    c->tune_buf = nullptr;
+    c->tune_cap = 0;
+    if (cudaMalloc(&c->tune_buf, 2 * per * sizeof(double)) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+    c->tune_cap = m;
+  }
+  double* pristine = c->tune_buf;
+  double* work = c->tune_buf + per;
+  for (int i = 0; i < nc; ++i)
+    if (cudaMemcpyAsync(pristine + (size_t)i * m, a.Y + (size_t)i * a.ld, m * sizeof(double), cudaMemcpyDeviceToDevice,
+                        s) != cudaSuccess)
+      return LSG_ERR_CUDA;
+  if (cudaMemcpyAsync(pristine + (size_t)nc * m, a.T, m * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return LSG_ERR_CUDA;
+  if (a.dt && cudaMemcpyAsync(pristine + (size_t)nc * m + m, a.dt, m * sizeof(double), cudaMemcpyDeviceToDevice,
+                              s) != cudaSuccess)
+    return LSG_ERR_CUDA;
+  StepArgs t = a;
+  t.ncells = m;
+  t.ld = m;
+  t.Y = work;
+  t.T = work + (size_t)nc * m;
+  t.dt = a.dt ? work + (size_t)nc * m + m : nullptr;
+  t.Q = nullptr;
+  t.status = nullptr;
+  t.nsteps = nullptr;
+  t.counters = nullptr;
+  struct Cand { int tile, w; };
+  const Cand cands[LSG_NTUNE_CANDIDATES] = {
+      {LSG_TILE_LANE, 16}, {LSG_TILE_LANE, 32}, {LSG_TILE_WARP, 0}, {LSG_TILE_PERSISTENT, 0}};
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return LSG_ERR_CUDA;
+  double best = -1.;
+  int besti = -1;
+  const bool timing = c->timer.on;
+  c->timer.on = false;   // the trial runs are not the caller's kernels
+  for (int k = 0; k < LSG_NTUNE_CANDIDATES; ++k) {
+    c->tune_rate[k] = 0.;
+    const Cand cd = cands[k];
+    if (cd.tile == LSG_TILE_LANE && cd.w == 16 && n > 16) continue;
+    if (cd.tile == LSG_TILE_WARP && c->opt.precision != LSG_PRECISION_FP64) continue;
+    c->tuned = cd.tile == LSG_TILE_LANE;
+    c->tuned_w = cd.w;
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {   // a 1024-cell run pays the one-time set-up, then the timed run
+      if (cudaMemcpyAsync(work, pristine, per * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        c->timer.on = timing;
+        return LSG_ERR_CUDA;
+      }
+      StepArgs tr = t;
+      if (rep == 0 && tr.ncells > 1024) tr.ncells = 1024;
+      cudaEventRecord(e0, s);
+      const int r = launch_tile(c, tr, s, cd.tile);
+      cudaEventRecord(e1, s);
+      if (r != LSG_OK || cudaEventSynchronize(e1) != cudaSuccess) {
+        c->timer.on = timing;
+        c->tuned = false;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return r != LSG_OK ? r : LSG_ERR_CUDA;
+      }
+      cudaEventElapsedTime(&ms, e0, e1);
+    }
+    c->tune_rate[k] = ms > 0.f ? m / (ms * 1e-3) : 0.;
+    if (c->tune_rate[k] > best) { best = c->tune_rate[k]; besti = k; }
+  }
+  c->timer.on = timing;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (besti < 0) return LSG_ERR_UNSUPPORTED;
+  c->tuned = true;
+  c->tuned_tile = cands[besti].tile;
+  c->tuned_w = cands[besti].w;
+  return LSG_OK;
+}
+
 int launch_step(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
   const MechLayout& L = c->mech->host.layout;
+  if (L.nc + 1 <= 32 && c->opt.tile == LSG_TILE_AUTO && c->opt.autotune && !c->tuned && a.ncells >= 1024) {
+    const int r = autotune(c, a, s);
+    if (r != LSG_OK) return r;
+  }
+  const int tile = (c->tuned && c->opt.tile == LSG_TILE_AUTO) ? c->tuned_tile : resolve_tile(c->opt);
+  return launch_tile(c, a, s, tile);
+}
+
+int launch_tile(lsg_ctx* c, const StepArgs& a, cudaStream_t s, int tile) {
+  const MechLayout& L = c->mech->host.layout;
   const StepOptions so = to_step_options(c->opt);
-  const int tile = resolve_tile(c->opt);
   if (L.nc + 1 > 32 || tile == LSG_TILE_BLOCK) return launch_large(c, a, s);
   if (tile == LSG_TILE_LANE) {
     const bool lu64 = c->opt.precision == LSG_PRECISION_FP64;
@@ -412,6 +520,7 @@ int lsg_ctx_set_options(lsg_ctx* c, const lsg_options* opt) {
   if (v != LSG_OK) return v;
   c->opt = *opt;
   apply_timing(c);
+  c->tuned = false;   // new options: tune again on the next step
   return LSG_OK;
 }
 
@@ -425,6 +534,7 @@ int lsg_ctx_destroy(lsg_ctx* c) {
   cudaFree(c->rstate);
   cudaFree(c->bws);
   cudaFree(c->bqueue);
+  cudaFree(c->tune_buf);
   if (c->nact_host) cudaFreeHost(c->nact_host);
   cudaFree(c->d_err);
   for (cudaEvent_t& e : c->timer.ev)
@@ -437,6 +547,15 @@ int lsg_ctx_destroy(lsg_ctx* c) {
 void* lsg_ctx_stream(lsg_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 long long lsg_ctx_launches(const lsg_ctx* c) { return c ? c->launches : -1; }
+
+int lsg_ctx_tuning(const lsg_ctx* c, int* tile, int* width, double* rates) {
+  if (!c || !c->tuned || c->opt.tile != LSG_TILE_AUTO || !c->opt.autotune) return LSG_ERR_ARG;
+  if (tile) *tile = c->tuned_tile;
+  if (width) *width = c->tuned_w;
+  if (rates)
+    for (int k = 0; k < LSG_NTUNE_CANDIDATES; ++k) rates[k] = c->tune_rate[k];
+  return LSG_OK;
+}
 
 int lsg_ctx_kernel_times(lsg_ctx* c, double* ms, long long* launches, int nkinds, int reset) {
   if (!c || nkinds < 0) return LSG_ERR_ARG;

@@ -108,12 +108,13 @@ struct KernelTimer {
 // Round scheme (lsg_rounds.cu): launch geometry chosen once per context.
 struct RoundsPlan {
   bool lu64;
+  int w;                       // lanes per cell in the advance kernel (16: two cells per warp; 32)
   size_t rhs_smem, adv_smem;
   unsigned g_rhs, g_adv, g_cmp, g_init;
 };
 size_t rounds_bytes(const MechLayout& L, long ns, bool lu64);
 cudaError_t upload_gear_rounds(const GearConsts& gc);
-cudaError_t rounds_prepare(const MechLayout& L, bool lu64, int sm_count, RoundsPlan* plan);
+cudaError_t rounds_prepare(const MechLayout& L, bool lu64, int sm_count, int width, RoundsPlan* plan);
 cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsigned char* mech_gmem,
                           const StepOptions& o, const StepArgs& a, void* state, long ns, int* nact_host,
                           long max_rounds, int* err, cudaStream_t stream, long long* launches,

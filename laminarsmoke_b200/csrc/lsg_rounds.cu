@@ -1271,9 +1271,9 @@ RoundBufs carve(const MechLayout& L, void* base, long cap, bool lu64) {
   return B;
 }
 
-size_t advance_smem(const MechLayout& L, bool lu64) {
+size_t advance_smem(const MechLayout& L, bool lu64, int w) {
   const size_t n = L.nc + 1;
-  const size_t groups = (size_t)kWA * (n <= 16 ? 2 : 1);
+  const size_t groups = (size_t)kWA * (w == 16 ? 2 : 1);
   const size_t lut = lu64 ? sizeof(double) : sizeof(float);
   return groups * (n * (n + 1) + n * (2 * n + 1) + 2 * n) * lut + groups * n * (n + 1) * sizeof(float);
 }
@@ -1295,21 +1295,24 @@ size_t rounds_bytes(const MechLayout& L, long cap, bool lu64) {
 
 cudaError_t upload_gear_rounds(const GearConsts& gc) { return cudaMemcpyToSymbol(c_gear_r, &gc, sizeof(GearConsts)); }
 
-cudaError_t rounds_prepare(const MechLayout& L, bool lu64, int sm_count, RoundsPlan* P) {
+cudaError_t rounds_prepare(const MechLayout& L, bool lu64, int sm_count, int width, RoundsPlan* P) {
   const int n = L.nc + 1;
   if (n > 32) return cudaErrorInvalidValue;
+  if (width == 0) width = n <= 16 ? 16 : 32;   // default: two cells per warp when they fit
+  if ((width != 16 && width != 32) || n > width) return cudaErrorInvalidValue;
   *P = RoundsPlan{};
   P->lu64 = lu64;
+  P->w = width;
   P->rhs_smem = ((L.bytes + 15u) & ~15u) + (size_t)3 * L.nc * kRT * sizeof(double);
-  P->adv_smem = advance_smem(L, lu64);
+  P->adv_smem = advance_smem(L, lu64, width);
   cudaError_t e = cudaFuncSetAttribute(rounds_rhs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)P->rhs_smem);
   if (e != cudaSuccess) return e;
   int rhs_bps = 0, adv_bps = 0, cmp_bps = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rhs_bps, rounds_rhs_kernel, kRT, P->rhs_smem);
   if (e != cudaSuccess) return e;
-  if (lu64) e = n <= 16 ? prepare_advance<double, 16>(P->adv_smem, &adv_bps) : prepare_advance<double, 32>(P->adv_smem, &adv_bps);
-  else e = n <= 16 ? prepare_advance<float, 16>(P->adv_smem, &adv_bps) : prepare_advance<float, 32>(P->adv_smem, &adv_bps);
+  if (lu64) e = width == 16 ? prepare_advance<double, 16>(P->adv_smem, &adv_bps) : prepare_advance<double, 32>(P->adv_smem, &adv_bps);
+  else e = width == 16 ? prepare_advance<float, 16>(P->adv_smem, &adv_bps) : prepare_advance<float, 32>(P->adv_smem, &adv_bps);
   if (e != cudaSuccess) return e;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cmp_bps, rounds_scatter_kernel, kCT, 0);
   if (e != cudaSuccess) return e;
@@ -1346,10 +1349,10 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
       const dim3 ga(P.g_adv), ta(kWA * 32);
       kt->begin(KT_ADVANCE, stream);
       if (P.lu64) {
-        if (n <= 16) rounds_advance_kernel<double, 16><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
+        if (P.w == 16) rounds_advance_kernel<double, 16><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
         else rounds_advance_kernel<double, 32><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
       } else {
-        if (n <= 16) rounds_advance_kernel<float, 16><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
+        if (P.w == 16) rounds_advance_kernel<float, 16><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
         else rounds_advance_kernel<float, 32><<<ga, ta, P.adv_smem, stream>>>(L.nc, o, a, B, par);
       }
       kt->end(stream);

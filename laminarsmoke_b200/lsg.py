@@ -38,7 +38,7 @@ class Options(C.Structure):
                 ("max_steps", C.c_int), ("full_pivoting", C.c_int), ("energy", C.c_int),
                 ("precision", C.c_int),
                 ("alfa2_4", C.c_double), ("alfa2_5", C.c_double), ("maximum_order", C.c_int),
-                ("tile", C.c_int), ("kernel_timing", C.c_int), ("reserved", C.c_int * 5)]
+                ("tile", C.c_int), ("kernel_timing", C.c_int), ("autotune", C.c_int), ("reserved", C.c_int * 4)]
 
 
 EXPORTS = (
@@ -46,7 +46,7 @@ EXPORTS = (
     "lsg_mech_destroy", "lsg_ctx_create", "lsg_ctx_set_options", "lsg_ctx_destroy",
     "lsg_reaction_step", "lsg_reaction_step_device", "lsg_ctx_check", "lsg_rhs_device",
     "lsg_strerror", "lsg_abi_version", "lsg_ctx_stream", "lsg_ctx_launches",
-    "lsg_reaction_step_device_noalloc", "lsg_ctx_kernel_times",
+    "lsg_reaction_step_device_noalloc", "lsg_ctx_kernel_times", "lsg_ctx_tuning",
 )
 
 _lib = None
@@ -81,6 +81,7 @@ def lib():
     L.lsg_reaction_step_device_noalloc.argtypes = [vp, C.POINTER(Options), i, i, vp, l, vp, d, d, vp, d, vp,
                                                    vp, vp, vp, vp]
     L.lsg_ctx_kernel_times.argtypes = [vp, vp, vp, i, i]
+    L.lsg_ctx_tuning.argtypes = [vp, C.POINTER(i), C.POINTER(i), vp]
     L.lsg_ctx_launches.argtypes = [vp]
     L.lsg_ctx_launches.restype = C.c_longlong
     _lib = L
@@ -230,6 +231,17 @@ class ReactionStep:
         _check(lib().lsg_ctx_kernel_times(self.h, C.cast(ms, C.c_void_p), C.cast(nl, C.c_void_p), nk, int(reset)),
                "lsg_ctx_kernel_times")
         return {k: (ms[i], nl[i]) for i, k in enumerate(self.KERNEL_KINDS)}
+
+    TUNE_CANDIDATES = ("rounds16", "rounds32", "plain_warp", "persistent")
+
+    def tuning(self):
+        """(tile, width, {candidate: cells/s}) chosen by the autotuner, or None before it ran."""
+        tile, width = C.c_int(), C.c_int()
+        rates = (C.c_double * len(self.TUNE_CANDIDATES))()
+        rc = lib().lsg_ctx_tuning(self.h, C.byref(tile), C.byref(width), C.cast(rates, C.c_void_p))
+        if rc != 0:
+            return None
+        return tile.value, width.value, {k: rates[i] for i, k in enumerate(self.TUNE_CANDIDATES)}
 
     def check(self):
         f = C.c_int()

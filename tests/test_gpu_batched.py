@@ -73,3 +73,34 @@ def test_batched_edge_cases(h2co, oracle_h2co, gpu_h2co):
     (Yg, Tg, Qg, stg, nsg), (Yo, To, Qo, sto, cnt) = _run(gpu_h2co, oracle_h2co, Y, T, 1e-5, 1, max_steps=5)
     np.testing.assert_array_equal(stg, sto)
     np.testing.assert_allclose(Tg, To, rtol=1e-9)
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_autotuner_picks_a_measured_form(h2co, oracle_h2co, gpu_h2co, precision):
+    """With tile AUTO and autotune on, the first step times the candidate forms on
+    its own cells, keeps the fastest, and the step it then runs matches the oracle."""
+    import torch
+    from laminarsmoke_b200 import lsg
+    _, species, A = h2co
+    Y, T = cells.h2co_mixing(species, A["mw"], 4096, seed=31)
+    ctx = lsg.ReactionStep(gpu_h2co, precision=precision, tile=lsg.LSG_TILE_AUTO, autotune=1)
+    assert ctx.tuning() is None
+    Yd = torch.tensor(np.ascontiguousarray(Y.T), device="cuda")
+    Td = torch.tensor(T, device="cuda")
+    st = torch.zeros(4096, dtype=torch.int32, device="cuda")
+    ctx.step_device(Yd, Td, 1e-5, status=st)
+    torch.cuda.synchronize()
+    ctx.check()
+    tile, width, rates = ctx.tuning()
+    print(f"autotune precision={precision}: tile {tile} width {width} rates {rates}")
+    tried = {k: v for k, v in rates.items() if v > 0}
+    assert len(tried) >= 3 if precision == 0 else len(tried) >= 2
+    best = max(tried, key=tried.get)
+    assert (tile, width) == {"rounds16": (lsg.LSG_TILE_LANE, 16), "rounds32": (lsg.LSG_TILE_LANE, 32),
+                             "plain_warp": (lsg.LSG_TILE_WARP, 0),
+                             "persistent": (lsg.LSG_TILE_PERSISTENT, 0)}[best]
+    Yo, To, Qo, sto, cnt = oracle_h2co.reaction_step(Y, T, 1e-5, nthreads=8)
+    np.testing.assert_array_equal(st.cpu().numpy(), sto)
+    assert np.max(np.abs(Td.cpu().numpy() - To) / To) <= RTOL_T
+    abs_Y = np.abs(Yd.cpu().numpy().T - Yo).max(axis=1)
+    assert np.mean(abs_Y <= ATOL_Y) >= 0.99 and abs_Y.max() <= 1e-7

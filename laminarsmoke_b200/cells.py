@@ -16,7 +16,7 @@ to one) and temperatures ``T[ncells]``; the seed is part of the workload name.
   with every other species log-uniform in [1e-10, 1e-3], T ~ U[lo, hi].
 * ``coflow_fields`` -- 2D axisymmetric 200 x 400 mesh: Gaussian temperature ridge
   300-2100 K along the stoichiometric surface and Z from a Burke-Schumann
-  profile.
+  profile; the fuel is CH4 or a mix of H2 and CO.
 """
 from __future__ import annotations
 
@@ -111,10 +111,24 @@ def synthetic_mixing(species: List[str], mw: np.ndarray, ncells: int, seed: int,
     return Y, T
 
 
-def coflow_fields(species: List[str], mw: np.ndarray, nr: int = 200, nz: int = 400, seed: int = 5):
-    """Burke-Schumann coflow: fuel jet radius a, coflow radius b; T ridge at Z_st."""
+def stoichiometric_z(species: Sequence[str], mw: np.ndarray, fuel: dict) -> float:
+    """Stoichiometric mixture fraction of `fuel` (mole fractions of H2, CO, CH4)
+    against air (0.21 O2 / 0.79 N2 by mole)."""
+    o2_per_mol = {"H2": 0.5, "CO": 0.5, "CH4": 2.0}
+    o2 = sum(v * o2_per_mol[k] for k, v in fuel.items())
+    m_fuel = sum(v * mw[species.index(k)] for k, v in fuel.items())
+    m_air = o2 / 0.21 * (0.21 * mw[species.index("O2")] + 0.79 * mw[species.index("N2")])
+    return m_fuel / (m_fuel + m_air)
+
+
+def coflow_fields(species: List[str], mw: np.ndarray, nr: int = 200, nz: int = 400, seed: int = 5,
+                  fuel: Optional[dict] = None):
+    """Burke-Schumann coflow: fuel jet radius a, coflow radius b; T ridge at Z_st.
+    `fuel` defaults to CH4; any mole-fraction mix of H2, CO and CH4 works (the
+    ridge follows its stoichiometric mixture fraction)."""
     rng = np.random.default_rng(seed)
-    yf, ya = fuel_air_mass(species, mw, {"CH4": 1.0}, {"O2": 0.21, "N2": 0.79})
+    fuel = fuel or {"CH4": 1.0}
+    yf, ya = fuel_air_mass(species, mw, fuel, {"O2": 0.21, "N2": 0.79})
     r = (np.arange(nr) + 0.5) / nr          # radius / coflow radius
     z = (np.arange(nz) + 0.5) / nz * 20.0   # axial distance / jet radius
     a = 0.25
@@ -122,11 +136,11 @@ def coflow_fields(species: List[str], mw: np.ndarray, nr: int = 200, nz: int = 4
     # leading-order Burke-Schumann mixture fraction: diffusion-broadened top hat
     w = 0.02 + 0.05 * np.sqrt(Zax)
     Zmix = 0.5 * (1.0 - np.tanh((R - a) / w))
-    z_st = 0.055
+    z_st = stoichiometric_z(species, mw, fuel)
     T = 300.0 + 1800.0 * np.exp(-((Zmix - z_st) / 0.05) ** 2) * (1.0 - np.exp(-Zax / 0.5))
     Zf = Zmix.ravel()
     Y = Zf[:, None] * yf[None, :] + (1.0 - Zf)[:, None] * ya[None, :]
-    others = [i for i, s in enumerate(species) if s not in ("CH4", "O2", "N2")]
+    others = [i for i, s in enumerate(species) if s not in tuple(fuel) + ("O2", "N2")]
     Y[:, others] = 10.0 ** rng.uniform(-10.0, -4.0, (Zf.size, len(others)))
     Y /= Y.sum(axis=1, keepdims=True)
     return Y, T.ravel()

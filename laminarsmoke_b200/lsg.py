@@ -208,6 +208,22 @@ class ReactionStep:
             None if nsteps is None else nsteps.data_ptr(), None if counters is None else counters.data_ptr(),
             _stream_handle(stream)), "lsg_reaction_step_device")
 
+    def step_sequence_device(self, Y, T, dt, nsteps: int, p: float = 101325.0, t0: float = 0.0, Q=None,
+                             status=None, stream=None):
+        """`nsteps` successive reaction steps on the same device arrays, the
+        start time advancing by dt each step (a CFD run's chemistry calls with
+        the state kept resident).  `dt` is a scalar.  Q and status, when given,
+        hold the last step's heat release and ODE codes; returns the number of
+        cells that reported a failure (status < 0) in any step."""
+        import torch
+        n = T.shape[0]
+        st = status if status is not None else torch.empty(n, dtype=torch.int32, device=T.device)
+        bad = torch.zeros(n, dtype=torch.bool, device=T.device)
+        for k in range(nsteps):
+            self.step_device(Y, T, dt, p=p, t0=t0 + k * float(dt), Q=Q, status=st, stream=stream)
+            bad |= st < 0
+        return int(bad.sum().item())
+
     def rhs_device(self, y, dy, p: float = 101325.0, qr=None, stream=None):
         _require_layout(y, dy, qr)
         n1, ld = y.shape

@@ -5,9 +5,16 @@ for profiling and quick checks).
 
 Workloads (seeded, see laminarsmoke_b200.cells): h2co_mixing (T ~ U[900, 2200] K
 mixtures of H2/CO fuel and air with radicals), h2co_uneven (cold / igniting /
-near-equilibrium thirds; the pool is prepared with the plain step).  Forms:
-plain (warp-per-cell FP64), mixed (round scheme, FP32 factors), batched64 (round
-scheme, FP64 factors), persistent (persistent lane kernel, FP32 factors).
+near-equilibrium thirds; the pool is prepared with the plain step), coflow (the
+200 x 400 Burke-Schumann coflow mesh with H2/CO fuel, 80,000 cells, advanced by
+--steps successive device-resident steps; --cells below 80,000 takes an evenly
+strided subset).  Forms: plain (warp-per-cell FP64), mixed (round scheme, FP32
+factors), batched64 (round scheme, FP64 factors), persistent (persistent lane
+kernel, FP32 factors), auto (the library's choice: the autotuner for up to 31
+species, the block-per-cell form above).  --mech h2co+K pads the H2/CO chemistry
+with K inert species (h2co+106: 121 species).
+
+  python -m laminarsmoke_b200.run_case --workload coflow --mech h2co+106 --steps 50 --form auto
 """
 from __future__ import annotations
 
@@ -19,26 +26,35 @@ import numpy as np
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=("h2co_mixing", "h2co_uneven"), default="h2co_mixing")
+    ap.add_argument("--workload", choices=("h2co_mixing", "h2co_uneven", "coflow"), default="h2co_mixing")
     ap.add_argument("--cells", type=int, default=65536)
-    ap.add_argument("--form", choices=("plain", "mixed", "batched64", "persistent"), default="mixed")
+    ap.add_argument("--form", choices=("plain", "mixed", "batched64", "persistent", "auto"), default="mixed")
+    ap.add_argument("--mech", default="h2co", help="h2co or h2co+K (K inert species)")
+    ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--dt", type=float, default=1e-5)
     ap.add_argument("--seed", type=int, default=1)
     args = ap.parse_args(argv)
     import torch
     from laminarsmoke_b200 import cells, lsg, mech
     from laminarsmoke_b200.mech import blob
-    data, species = mech.load("h2co")
+    data, species = mech.load(args.mech)
     arrays, _ = blob.unpack(data)
     m = lsg.Mechanism(data)
     forms = {"plain": (lsg.LSG_TILE_WARP, lsg.LSG_PRECISION_FP64),
              "mixed": (lsg.LSG_TILE_LANE, lsg.LSG_PRECISION_MIXED),
              "batched64": (lsg.LSG_TILE_LANE, lsg.LSG_PRECISION_FP64),
-             "persistent": (lsg.LSG_TILE_PERSISTENT, lsg.LSG_PRECISION_MIXED)}
+             "persistent": (lsg.LSG_TILE_PERSISTENT, lsg.LSG_PRECISION_MIXED),
+             "auto": (lsg.LSG_TILE_AUTO, lsg.LSG_PRECISION_MIXED)}
     tile, prec = forms[args.form]
     ctx = lsg.ReactionStep(m, tile=tile, precision=prec)
     if args.workload == "h2co_mixing":
         Y, T = cells.h2co_mixing(species, arrays["mw"], args.cells, seed=args.seed)
+    elif args.workload == "coflow":
+        Y, T = cells.coflow_fields(species, arrays["mw"], seed=args.seed, fuel={"H2": 0.5, "CO": 0.5})
+        if args.cells < T.size:
+            idx = np.linspace(0, T.size - 1, args.cells).astype(np.int64)
+            Y, T = Y[idx], T[idx]
+        args.cells = T.size
     else:
         plain = lsg.ReactionStep(m, tile=lsg.LSG_TILE_WARP, precision=lsg.LSG_PRECISION_FP64)
 
@@ -52,11 +68,18 @@ def main(argv=None) -> int:
     Yd = torch.tensor(np.ascontiguousarray(Y.T), device="cuda")
     Td = torch.tensor(T, device="cuda")
     status = torch.zeros(args.cells, dtype=torch.int32, device="cuda")
-    ctx.step_device(Yd, Td, args.dt, status=status)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record()
+    fails = ctx.step_sequence_device(Yd, Td, args.dt, args.steps, status=status)
+    t1.record()
     torch.cuda.synchronize()
     ctx.check()
+    ms = t0.elapsed_time(t1)
     st = status.cpu().numpy()
-    print(f"{args.form} {args.workload} {args.cells} cells: statuses {dict(zip(*np.unique(st, return_counts=True)))}")
+    print(f"{args.form} {args.workload} {args.mech} {args.cells} cells x {args.steps} steps: {ms:.1f} ms, "
+          f"{args.cells * args.steps / (ms * 1e-3):.4e} cells*steps/s, cells failing in any step {fails}, "
+          f"last statuses {dict(zip(*np.unique(st, return_counts=True)))}")
     return 0
 
 

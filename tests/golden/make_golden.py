@@ -1,0 +1,76 @@
+"""Regenerate the golden vectors of the reaction-step path from the oracle.
+
+    python tests/golden/make_golden.py
+
+The oracle (oracle/oracle.cpp, the FP64 restatement of the reference step) is
+the only source: the reference itself cannot be compiled here, so these
+fixtures pin the oracle against later changes and give the GPU tests fixed
+expected outputs.  Inputs are seeded (numpy PCG64, seeds below):
+
+* h2co_rhs.npz      -- 64 H2/CO mixing states y = [Y(14), T]: dy/dt and QR;
+* h2co_step.npz     -- 256 H2/CO mixing cells, one step dt = 1e-5, rtol 1e-7,
+                       atol 1e-12: Y, T, Q, ODE status, counters;
+* h2co_edge.npz     -- 4 cells: T at tmin_chem (skipped), a cold frozen
+                       mixture, a hot equilibrium-near state, a 1 us step;
+* h2co45_step.npz   -- 32 cells of the H2/CO chemistry padded with 30 inert
+                       species (45 components, the block-per-cell form).
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from laminarsmoke_b200 import cells, mech  # noqa: E402
+from laminarsmoke_b200.mech import blob  # noqa: E402
+from oracle.oracle import OracleMechanism  # noqa: E402
+
+
+def padded_states(k, n, seed):
+    data, species = mech.load(f"h2co+{k}")
+    A, _ = blob.unpack(data)
+    Y, T = cells.h2co_mixing(species[:14], A["mw"][:14], n, seed=seed)
+    return data, np.concatenate([Y * 0.9, np.full((n, k), 0.1 / k)], axis=1), T
+
+
+def edge_states(species, mw):
+    Y, T = cells.h2co_mixing(species, mw, 4, seed=41)
+    T = np.array([250.0, 400.0, 2300.0, 1500.0])
+    dt = np.array([1e-5, 1e-5, 1e-5, 1e-6])
+    return Y, T, dt
+
+
+def main():
+    data, species = mech.load("h2co")
+    A, _ = blob.unpack(data)
+    orc = OracleMechanism(data)
+
+    Y, T = cells.h2co_mixing(species, A["mw"], 64, seed=31)
+    y = np.concatenate([Y, T[:, None]], axis=1)
+    dy = np.zeros_like(y)
+    qr = np.zeros(64)
+    for k in range(64):
+        dy[k], qr[k] = orc.rhs(y[k])
+    np.savez_compressed(os.path.join(HERE, "h2co_rhs.npz"), y=y, dy=dy, qr=qr)
+
+    Y, T = cells.h2co_mixing(species, A["mw"], 256, seed=32)
+    Yo, To, Qo, sto, cnt = orc.reaction_step(Y, T, 1e-5, nthreads=1)
+    np.savez_compressed(os.path.join(HERE, "h2co_step.npz"), Y0=Y, T0=T, dt=1e-5, Y=Yo, T=To, Q=Qo,
+                        status=sto, counters=cnt)
+
+    Y, T, dt = edge_states(species, A["mw"])
+    Yo, To, Qo, sto, cnt = orc.reaction_step(Y, T, dt, tmin_chem=300.0, nthreads=1)
+    np.savez_compressed(os.path.join(HERE, "h2co_edge.npz"), Y0=Y, T0=T, dt=dt, tmin_chem=300.0, Y=Yo, T=To,
+                        Q=Qo, status=sto, counters=cnt)
+
+    data45, Y, T = padded_states(30, 32, seed=33)
+    Yo, To, Qo, sto, cnt = OracleMechanism(data45).reaction_step(Y, T, 1e-5, nthreads=1)
+    np.savez_compressed(os.path.join(HERE, "h2co45_step.npz"), Y0=Y, T0=T, dt=1e-5, Y=Yo, T=To, Q=Qo,
+                        status=sto, counters=cnt)
+
+
+if __name__ == "__main__":
+    main()

@@ -196,6 +196,33 @@ int lsg_reaction_step_device_noalloc(const lsg_mech* mech, const lsg_options* op
 int lsg_rhs_device(lsg_ctx* ctx, int ncells, const double* y_dev, double* dy_dev, long ld, double p,
                    double* qr_dev, void* stream);
 
+/* ---- output fields beyond Y, T and Q -------------------------------------
+ * Source terms of the compact Strang scheme (strangAlgorithm Compact), which
+ * replace the field update of solvers/laminarSMOKE/unsteady/chemistry_DI.H:
+ * 236-281: from the fields as the step found them (Y0, T0) and the step's
+ * result (Yf, Tf, e.g. a copy advanced by lsg_reaction_step_device),
+ *   rho = p MW / (R Tf), MW and cp of the mixture at (Yf, Tf),
+ *   RR_i = rho (Yf_i - Y0_i) / dt   [kg/m3/s],
+ *   RT   = rho cp (Tf - T0) / dt     [W/m3], only with the energy equation on
+ *          (lsg_options.energy; RT may be NULL),
+ * and zero where dt <= 1e-14.  dt_dev per cell or NULL + dt_scalar (the
+ * reference takes the global step tf - t0 here, which equals the cell's step
+ * unless local time stepping is on).  All arrays on the device; Y0, Yf and RR
+ * species-major [nspecies * ld]. */
+int lsg_compact_sources_device(lsg_ctx* ctx, int ncells, int nspecies, const double* Y0_dev, const double* T0_dev,
+                               const double* Yf_dev, const double* Tf_dev, long ld, double p, const double* dt_dev,
+                               double dt_scalar, double* RR_dev, double* RT_dev, void* stream);
+
+/* Formation-rate output fields (chemistry_DI.H:293-326, outputFormationRates):
+ * R_i MW_i [kg/m3/s] of every species at the states (Y, T), written to
+ * out_dev [nspecies * ld_out]; the caller picks the species it outputs.  The
+ * reference reads the reactor's R() after the solver's last right-hand-side
+ * call, which is made at the state the solver returns, i.e. before the
+ * driver's renormalisation of Y (a relative change below massFractionsTol =
+ * 1e-10).  Uses context-owned scratch of 2 (nspecies + 1) ncells doubles. */
+int lsg_formation_rates_device(lsg_ctx* ctx, int ncells, int nspecies, const double* Y_dev, const double* T_dev,
+                               long ld, double p, double* out_dev, long ld_out, void* stream);
+
 const char* lsg_strerror(int code);
 int lsg_abi_version(void);
 

@@ -1,7 +1,8 @@
 """Build the B200 library liblsmoke_gpu.so in-tree with nvcc (sm_100a).
 
-The plain FP64 kernels are compiled with FMA contraction off so their
-arithmetic rounds like the CPU reference; everything else is compiled normally.
+The plain FP64 kernels and the output-field kernels are compiled with FMA
+contraction off so their arithmetic rounds like the CPU reference; everything
+else is compiled normally.
 """
 from __future__ import annotations
 
@@ -21,6 +22,7 @@ UNITS = [
     ("lsg_batched.cu", []),
     ("lsg_rounds.cu", []),
     ("lsg_block.cu", []),
+    ("lsg_outputs.cu", ["-fmad=false"]),
     ("lsg_api.cu", []),
     ("lsg_mech_host.cpp", []),
 ]

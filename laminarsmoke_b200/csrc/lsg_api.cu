@@ -60,6 +60,9 @@ struct lsg_ctx {
   double* tune_buf = nullptr;   // sample cells: pristine copy and work copy
   long tune_cap = 0;
   int rplan_w = -1;             // lane-group width the round plan was prepared for
+  // formation-rate output: gathered states and their right-hand sides
+  double* frs = nullptr;
+  long frs_cap = 0;             // doubles
 };
 
 namespace {
@@ -199,6 +202,26 @@ int sm_count(lsg_ctx* c) {
       cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess)
     return 0;
   return c->sm_count;
+}
+
+// One right-hand-side evaluation per cell: the block form's kernel for more
+// than 31 species, the warp kernel otherwise.
+int ensure_block(lsg_ctx* c);
+int rhs_dispatch(lsg_ctx* c, long ncells, const double* y, double* dy, long ld, double p, double* qr,
+                 cudaStream_t s) {
+  const MechLayout& L = c->mech->host.layout;
+  if (L.nc + 1 > 32) {
+    const int r = ensure_block(c);
+    if (r != LSG_OK) return r;
+    if (launch_rhs_block(L, c->mech->d_buf, ncells, y, dy, ld, p, c->opt.energy, qr, c->bws, c->bws_blocks, s) !=
+        cudaSuccess)
+      return LSG_ERR_CUDA;
+  } else if (launch_rhs_warp(L, c->mech->d_buf, ncells, y, dy, ld, p, c->opt.energy, qr, c->d_err, s) !=
+             cudaSuccess) {
+    return LSG_ERR_CUDA;
+  }
+  ++c->launches;
+  return LSG_OK;
 }
 
 int ensure_rounds(lsg_ctx* c, long n, bool lu64) {
@@ -535,6 +558,7 @@ int lsg_ctx_destroy(lsg_ctx* c) {
   cudaFree(c->bws);
   cudaFree(c->bqueue);
   cudaFree(c->tune_buf);
+  cudaFree(c->frs);
   if (c->nact_host) cudaFreeHost(c->nact_host);
   cudaFree(c->d_err);
   for (cudaEvent_t& e : c->timer.ev)
@@ -704,18 +728,49 @@ int lsg_rhs_device(lsg_ctx* c, int ncells, const double* y, double* dy, long ld,
   if (!c || ncells < 0 || !y || !dy || ld < ncells || !(p > 0.)) return LSG_ERR_ARG;
   if (ncells == 0) return LSG_OK;
   if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
-  const MechLayout& L = c->mech->host.layout;
-  if (L.nc + 1 > 32) {
-    const int r = ensure_block(c);
-    if (r != LSG_OK) return r;
-    if (launch_rhs_block(L, c->mech->d_buf, ncells, y, dy, ld, p, c->opt.energy, qr, c->bws, c->bws_blocks,
-                         (cudaStream_t)stream) != cudaSuccess)
-      return LSG_ERR_CUDA;
-    return LSG_OK;
-  }
-  if (launch_rhs_warp(L, c->mech->d_buf, ncells, y, dy, ld, p, c->opt.energy, qr, c->d_err,
-                      (cudaStream_t)stream) != cudaSuccess)
+  return rhs_dispatch(c, ncells, y, dy, ld, p, qr, (cudaStream_t)stream);
+}
+
+int lsg_compact_sources_device(lsg_ctx* c, int ncells, int nspecies, const double* Y0, const double* T0,
+                               const double* Yf, const double* Tf, long ld, double p, const double* dt,
+                               double dt_scalar, double* RR, double* RT, void* stream) {
+  if (!c || ncells < 0 || !Y0 || !T0 || !Yf || !Tf || !RR || ld < ncells || !(p > 0.)) return LSG_ERR_ARG;
+  if (nspecies != c->mech->host.layout.nc) return LSG_ERR_ARG;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  if (launch_compact_sources(c->mech->host.layout, c->mech->d_buf, ncells, Y0, T0, Yf, Tf, ld, p, dt, dt_scalar,
+                             c->opt.energy, RR, RT, sm_count(c), (cudaStream_t)stream) != cudaSuccess)
     return LSG_ERR_CUDA;
+  ++c->launches;
+  return LSG_OK;
+}
+
+int lsg_formation_rates_device(lsg_ctx* c, int ncells, int nspecies, const double* Y, const double* T, long ld,
+                               double p, double* out, long ld_out, void* stream) {
+  if (!c || ncells < 0 || !Y || !T || !out || ld < ncells || ld_out < ncells || !(p > 0.)) return LSG_ERR_ARG;
+  const MechLayout& L = c->mech->host.layout;
+  if (nspecies != L.nc) return LSG_ERR_ARG;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  const cudaStream_t s = (cudaStream_t)stream;
+  const long need = 2L * (L.nc + 1) * ncells;
+  if (need > c->frs_cap) {
+    if (cudaStreamSynchronize(s) != cudaSuccess) return LSG_ERR_CUDA;
+    cudaFree(c->frs);
+    c->frs = nullptr;
+    c->frs_cap = 0;
+    if (cudaMalloc(&c->frs, sizeof(double) * need) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+    c->frs_cap = need;
+  }
+  double* y = c->frs;
+  double* dy = c->frs + (long)(L.nc + 1) * ncells;
+  if (launch_gather_state(L.nc, ncells, Y, T, ld, y, sm_count(c), s) != cudaSuccess) return LSG_ERR_CUDA;
+  ++c->launches;
+  const int r = rhs_dispatch(c, ncells, y, dy, ncells, p, nullptr, s);
+  if (r != LSG_OK) return r;
+  if (launch_formation_rates(L, c->mech->d_buf, ncells, y, dy, p, out, ld_out, sm_count(c), s) != cudaSuccess)
+    return LSG_ERR_CUDA;
+  ++c->launches;
   return LSG_OK;
 }
 

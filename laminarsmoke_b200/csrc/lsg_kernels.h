@@ -122,4 +122,15 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
 cudaError_t launch_rhs_warp(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y,
                             double* dy, long ld, double p, int energy, double* qr, int* err, cudaStream_t stream);
 
+// output fields (lsg_outputs.cu)
+cudaError_t launch_compact_sources(const MechLayout& L, const unsigned char* mech_gmem, long ncells,
+                                   const double* Y0, const double* T0, const double* Yf, const double* Tf, long ld,
+                                   double p, const double* dt, double dt_scalar, int energy, double* RR, double* RT,
+                                   int sm_count, cudaStream_t stream);
+cudaError_t launch_gather_state(int nc, long ncells, const double* Y, const double* T, long ld, double* y,
+                                int sm_count, cudaStream_t stream);
+cudaError_t launch_formation_rates(const MechLayout& L, const unsigned char* mech_gmem, long ncells,
+                                   const double* y, const double* dy, double p, double* out, long ld_out,
+                                   int sm_count, cudaStream_t stream);
+
 }  // namespace lsg

@@ -47,6 +47,7 @@ EXPORTS = (
     "lsg_reaction_step", "lsg_reaction_step_device", "lsg_ctx_check", "lsg_rhs_device",
     "lsg_strerror", "lsg_abi_version", "lsg_ctx_stream", "lsg_ctx_launches",
     "lsg_reaction_step_device_noalloc", "lsg_ctx_kernel_times", "lsg_ctx_tuning",
+    "lsg_compact_sources_device", "lsg_formation_rates_device",
 )
 
 _lib = None
@@ -84,6 +85,8 @@ def lib():
     L.lsg_ctx_tuning.argtypes = [vp, C.POINTER(i), C.POINTER(i), vp]
     L.lsg_ctx_launches.argtypes = [vp]
     L.lsg_ctx_launches.restype = C.c_longlong
+    L.lsg_compact_sources_device.argtypes = [vp, i, i, vp, vp, vp, vp, l, d, vp, d, vp, vp, vp]
+    L.lsg_formation_rates_device.argtypes = [vp, i, i, vp, vp, l, d, vp, l, vp]
     _lib = L
     return L
 
@@ -223,6 +226,29 @@ class ReactionStep:
             self.step_device(Y, T, dt, p=p, t0=t0 + k * float(dt), Q=Q, status=st, stream=stream)
             bad |= st < 0
         return int(bad.sum().item())
+
+    def compact_sources_device(self, Y0, T0, Yf, Tf, dt, RR, RT=None, p: float = 101325.0, stream=None):
+        """Source terms of the compact Strang scheme (lsg_compact_sources_device):
+        RR [NC, ld] and RT [ncells] from the fields before (Y0, T0) and after
+        (Yf, Tf) a step of length dt (scalar or a per-cell tensor)."""
+        _require_layout(Y0, T0, Yf, Tf, RR, RT, dt if hasattr(dt, "data_ptr") else None)
+        nc, ld = Y0.shape
+        n = T0.shape[0]
+        if Yf.shape != Y0.shape or RR.shape != Y0.shape:
+            raise ValueError("Y0, Yf and RR must have the same shape")
+        dtp, dts = (None, float(dt)) if not hasattr(dt, "data_ptr") else (dt.data_ptr(), 0.0)
+        _check(lib().lsg_compact_sources_device(
+            self.h, n, nc, Y0.data_ptr(), T0.data_ptr(), Yf.data_ptr(), Tf.data_ptr(), ld, p, dtp, dts,
+            RR.data_ptr(), None if RT is None else RT.data_ptr(), _stream_handle(stream)),
+            "lsg_compact_sources_device")
+
+    def formation_rates_device(self, Y, T, out, p: float = 101325.0, stream=None):
+        """R_i MW_i [kg/m3/s] of every species at the states (Y [NC, ld], T) into out [NC, ld_out]."""
+        _require_layout(Y, T, out)
+        nc, ld = Y.shape
+        _check(lib().lsg_formation_rates_device(self.h, T.shape[0], nc, Y.data_ptr(), T.data_ptr(), ld, p,
+                                                out.data_ptr(), out.shape[1], _stream_handle(stream)),
+               "lsg_formation_rates_device")
 
     def rhs_device(self, y, dy, p: float = 101325.0, qr=None, stream=None):
         _require_layout(y, dy, qr)

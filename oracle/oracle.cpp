@@ -995,6 +995,65 @@ int orc_reaction_step(void* mech, const orc_options* o, int ncells, double* Y, d
   return nerr;
 }
 
+// Source terms of the compact Strang scheme, chemistry_DI.H:236-281: from the
+// state before (Y0, T0: the cell's fields as the step found them) and after
+// (Yf, Tf: the step's normalised result), cell-major:
+//   rho = p MW / R / Tf, MW and cp of the mixture at (Yf, Tf)
+//   (ThermodynamicsMap_CHEMKIN.hpp:429-434, 436-455, 506-511),
+//   RR_i = rho (Yf_i - Y0_i) / dt, RT = rho cp (Tf - T0) / dt; zero where dt <= 1e-14.
+int orc_compact_sources(void* mech, int ncells, const double* Y0, const double* T0, const double* Yf,
+                        const double* Tf, double p, const double* dt, double dt_scalar, int energy, double* RR,
+                        double* RT) {
+  const orc::Mech& m = *(const orc::Mech*)mech;
+  const int NC = m.nc;
+  const auto& MW = m.F("mw");
+  const auto& TM = m.F("t_mid");
+  const auto& CH = m.F("cp_ht");
+  const auto& CL = m.F("cp_lt");
+  for (int c = 0; c < ncells; ++c) {
+    const double deltat = dt ? dt[c] : dt_scalar;
+    const double* yf = Yf + (size_t)c * NC;
+    const double* y0 = Y0 + (size_t)c * NC;
+    double* rr = RR + (size_t)c * NC;
+    if (!(deltat > 1e-14)) {
+      for (int i = 0; i < NC; ++i) rr[i] = 0.;
+      if (energy && RT) RT[c] = 0.;
+      continue;
+    }
+    const double T = Tf[c];
+    double u = 0.;
+    for (int i = 0; i < NC; ++i) u += yf[i] / MW[i];
+    const double mwmix = 1. / u;
+    double cpmix = 0.;
+    const double T2 = T * T, T3 = T2 * T, T4 = T3 * T;
+    for (int i = 0; i < NC; ++i) {
+      const double x = mwmix * yf[i] / MW[i];
+      const double* a = T > TM[i] ? &CH[5 * i] : &CL[5 * i];
+      cpmix += (a[0] + T * a[1] + T2 * a[2] + T3 * a[3] + T4 * a[4]) * x;
+    }
+    cpmix *= orc::R_J_KMOL;
+    cpmix /= mwmix;
+    const double rhomix = p * mwmix / orc::R_J_KMOL / T;
+    for (int i = 0; i < NC; ++i) rr[i] = rhomix * (yf[i] - y0[i]) / deltat;
+    if (energy && RT) RT[c] = rhomix * cpmix * (T - T0[c]) / deltat;
+  }
+  return 0;
+}
+
+// Formation-rate output fields, chemistry_DI.H:293-326: R_i MW_i [kg/m3/s] of
+// every species at the state y = [Y_1..Y_NC, T] (the reactor's R() after the
+// solver's last right-hand-side call, which is made at the state it returns).
+int orc_formation_rates(void* mech, double P, const double* y, double* out) {
+  const orc::Mech& m = *(const orc::Mech*)mech;
+  orc::Reactor r(m);
+  r.P0 = P;
+  std::vector<double> dy(m.nc + 1);
+  r.equations(y, dy.data());
+  const auto& MW = m.F("mw");
+  for (int i = 0; i < m.nc; ++i) out[i] = r.R[i] * MW[i];
+  return 0;
+}
+
 int orc_num_counters() { return orc::NCOUNT; }
 
 }  // extern "C"

@@ -50,6 +50,9 @@ def lib():
                                         C.c_double, C.c_double, C.c_void_p, C.c_double, C.c_void_p,
                                         C.c_void_p, C.c_void_p, C.c_int]
         L.orc_reaction_step.restype = C.c_int
+        L.orc_compact_sources.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_double, C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]
+        L.orc_formation_rates.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -78,6 +81,27 @@ class OracleMechanism:
         q = np.zeros(1)
         lib().orc_rhs(self.h, p, _ptr(y), _ptr(dy), _ptr(q))
         return dy, float(q[0])
+
+    def compact_sources(self, Y0, T0, Yf, Tf, dt, p=101325.0, energy=True):
+        """Cell-major Y0/Yf [ncells, NC]; returns (RR [ncells, NC], RT [ncells])."""
+        Y0 = np.ascontiguousarray(Y0, dtype=np.float64)
+        Yf = np.ascontiguousarray(Yf, dtype=np.float64)
+        T0 = np.ascontiguousarray(T0, dtype=np.float64)
+        Tf = np.ascontiguousarray(Tf, dtype=np.float64)
+        n = T0.size
+        dt_arr = None if np.ndim(dt) == 0 else np.ascontiguousarray(dt, dtype=np.float64)
+        RR = np.zeros_like(Y0)
+        RT = np.zeros(n)
+        lib().orc_compact_sources(self.h, n, _ptr(Y0), _ptr(T0), _ptr(Yf), _ptr(Tf), p, _ptr(dt_arr),
+                                  0.0 if dt_arr is not None else float(dt), int(energy), _ptr(RR), _ptr(RT))
+        return RR, RT
+
+    def formation_rates(self, y, p=101325.0):
+        """R_i MW_i [kg/m3/s] at y = [Y_1..Y_NC, T]."""
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.zeros(y.size - 1)
+        lib().orc_formation_rates(self.h, p, _ptr(y), _ptr(out))
+        return out
 
     def fd_jacobian(self, y, h, rtol=1e-7, atol=1e-12, p=101325.0, y_max_T=6000.0):
         y = np.ascontiguousarray(y, dtype=np.float64)

@@ -9,8 +9,9 @@
 // KineticsMap_CHEMKIN.hpp (kinetic constants recomputed only when T changes,
 // :271-297); the mechanism tables are read from global memory (read-only path).
 //
-// Per-block work space in HBM: Jacobian J[n][n], factors G[n][n], cached
-// kinetic constants; in shared memory: the Nordsieck arrays, concentrations,
+// Per-block work space in HBM: Jacobian J and factors G, both n x n stored by
+// columns (element (i, j) at [j * n + i], so that the threads of a block, one
+// per row, read a column in one coalesced sweep), cached kinetic constants; in shared memory: the Nordsieck arrays, concentrations,
 // enthalpies, entropies, net rates and the pivots.
 #include "lsg_common.cuh"
 #include "lsg_kernels.h"
@@ -383,16 +384,17 @@ struct GearBlock {
       const double aux = rhs_block<BT>(*L, M, W, karr, ukeq, kinf, logf, yp, T, P0, energy);
       ++cnt[CNT_JAC_RHS];
       const double hInv = 1. / hJ;
-      if (active) J[(long)tid * n + j] = hInv * (aux - fl);
+      if (active) J[(long)j * n + tid] = hInv * (aux - fl);
     }
     __syncthreads();
   }
 
-  // G = I - hr0 J; partial-pivot LU (largest magnitude, first occurrence)
+  // G = I - hr0 J; partial-pivot LU (largest magnitude, first occurrence).
+  // Column storage: G(i, j) at G[j * n + i].
   __device__ void build_and_factorize(double hr0) {
     const int n = ne;
     for (long e = tid; e < (long)n * n; e += BT) {
-      const int i = (int)(e / n), j = (int)(e % n);
+      const int j = (int)(e / n), i = (int)(e % n);
       double g = J[e];
       g *= -hr0;
       if (i == j) g += 1.;
@@ -401,7 +403,7 @@ struct GearBlock {
     __syncthreads();
     for (int k = 0; k < n; ++k) {
       // pivot search over rows k..n-1 of column k, ties -> lowest row
-      double best = (tid >= k && tid < n) ? fabs(G[(long)tid * n + k]) : -1.;
+      double best = (tid >= k && tid < n) ? fabs(G[(long)k * n + tid]) : -1.;
       int row = tid;
       for (int off = 16; off > 0; off >>= 1) {
         const double ob = __shfl_xor_sync(kFull, best, off);
@@ -425,22 +427,22 @@ struct GearBlock {
       if (tid == 0) W.PIV[k] = pr;
       if (pr != k)
         for (int j = tid; j < n; j += BT) {
-          const double tmp = G[(long)k * n + j];
-          G[(long)k * n + j] = G[(long)pr * n + j];
-          G[(long)pr * n + j] = tmp;
+          const double tmp = G[(long)j * n + k];
+          G[(long)j * n + k] = G[(long)j * n + pr];
+          G[(long)j * n + pr] = tmp;
         }
       __syncthreads();
       const double d = G[(long)k * n + k];
       if (tid > k && tid < n) {
-        double l = G[(long)tid * n + k];
+        double l = G[(long)k * n + tid];
         if (d != 0.) l /= d;
-        G[(long)tid * n + k] = l;
+        G[(long)k * n + tid] = l;
       }
       __syncthreads();
       const int m = n - k - 1;
       for (long e = tid; e < (long)m * m; e += BT) {
-        const int i = k + 1 + (int)(e / m), j = k + 1 + (int)(e % m);
-        G[(long)i * n + j] -= G[(long)i * n + k] * G[(long)k * n + j];
+        const int j = k + 1 + (int)(e / m), i = k + 1 + (int)(e % m);
+        G[(long)j * n + i] -= G[(long)k * n + i] * G[(long)j * n + k];
       }
       __syncthreads();
     }
@@ -463,21 +465,53 @@ struct GearBlock {
         }
       }
     __syncthreads();
+    // Substitution in panels of 32 columns.  Warp 0 solves a panel's diagonal
+    // block with shuffles, the rows below (above, going back) then apply the
+    // panel's columns; two block barriers per panel instead of one per column.
+    // Every row still applies its updates one column at a time in the
+    // column-oriented order (forward: j ascending; back: j descending, then
+    // the division by its pivot), so the result is the same to the last bit.
     double x = W.X[tid];
-    for (int j = 0; j < n; ++j) {
-      if (tid == j) W.X[j] = x;   // x_j is final: publish it
+    for (int j0 = 0; j0 < n; j0 += 32) {
+      const int j1 = min(j0 + 32, n);
+      if (tid >= j0 && tid < j1) W.X[tid] = x;
       __syncthreads();
-      const double v = W.X[j];
-      if (tid > j && tid < n) x -= G[(long)tid * n + j] * v;
-    }
-    for (int j = n - 1; j >= 0; --j) {
-      if (tid == j) {
-        x /= G[(long)j * n + j];
-        W.X[j] = x;
+      if (tid < 32) {
+        const int r = j0 + tid;
+        double xr = r < j1 ? W.X[r] : 0.;
+        for (int j = j0; j < j1; ++j) {
+          const double g = r < j1 ? G[(long)j * n + r] : 0.;
+          const double xj = __shfl_sync(kFull, xr, j - j0);
+          if (r > j && r < j1) xr -= g * xj;
+        }
+        if (r < j1) W.X[r] = xr;
       }
       __syncthreads();
-      const double v = W.X[j];
-      if (tid < j) x -= G[(long)tid * n + j] * v;
+      if (tid >= j1 && tid < n)
+        for (int j = j0; j < j1; ++j) x -= G[(long)j * n + tid] * W.X[j];
+      else if (tid >= j0 && tid < j1)
+        x = W.X[tid];
+    }
+    for (int j1 = n; j1 > 0; j1 -= 32) {
+      const int j0 = max(j1 - 32, 0);
+      if (tid >= j0 && tid < j1) W.X[tid] = x;
+      __syncthreads();
+      if (tid < 32) {
+        const int r = j0 + tid;
+        double xr = r < j1 ? W.X[r] : 0.;
+        for (int j = j1 - 1; j >= j0; --j) {
+          const double g = r < j1 ? G[(long)j * n + r] : 0.;
+          if (r == j) xr /= g;
+          const double xj = __shfl_sync(kFull, xr, j - j0);
+          if (r < j) xr -= g * xj;
+        }
+        if (r < j1) W.X[r] = xr;
+      }
+      __syncthreads();
+      if (tid < j0)
+        for (int j = j1 - 1; j >= j0; --j) x -= G[(long)j * n + tid] * W.X[j];
+      else if (tid < j1)
+        x = W.X[tid];
     }
     __syncthreads();
     ++cnt[CNT_SOLVE];
@@ -580,7 +614,7 @@ struct GearBlock {
     __syncthreads();
     double s = 0.;
     if (active)
-      for (int j = 0; j < n; ++j) s += J[(long)tid * n + j] * W.X[j];
+      for (int j = 0; j < n; ++j) s += J[(long)j * n + tid] * W.X[j];
     va = s;
     va *= h;
     va += active ? Z(1) : 0.;

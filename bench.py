@@ -42,18 +42,21 @@ TRANSCENDENTAL_FLOPS = 20.0   # FP64-instruction equivalent charged per exp/log/
 # through HBM, not what a kernel happens to move):
 #   plain (one launch = the whole step of every cell): read Y,T and write Y,T,
 #     status of every cell: 2 (n) 8 + 8 bytes per cell (n = species + 1);
-#   advance (per cell-round): read the cell's solver record -- scalar state
-#     (18 doubles + 32 ints), z and v (16 n doubles), b, f, f0, va, vb, eps
-#     (6 n doubles) -- and write it back without f, f0: (42 n) 8 + 2 * 272 bytes;
-#   rhs (per cell-round): read y (n doubles), write f (n doubles), QR and the
-#     phase/counter words: 2 n 8 + 16 bytes.
-# A cell-round is one RHS evaluation of one cell: the per-cell counters give
-# their number (rhs + jacobian-column rhs).
+#   advance (per visit of a cell): read the cell's solver record -- scalar
+#     state (18 doubles + 32 ints), z and v (16 n doubles), b, f, f0, va, vb,
+#     eps (6 n doubles) -- and write it back without f, f0: (42 n) 8 + 2 * 272
+#     bytes.  A cell is visited once per RHS call and once per Jacobian;
+#   rhs (per RHS evaluation): read y (n doubles), write f (n doubles), QR and
+#     the phase/counter words: 2 n 8 + 16 bytes.  The per-cell counters give
+#     their number (RHS calls + the RHS calls inside Jacobians).
 def kernel_roofline(args, ktimes, counters, nc, ncells, hbm, peak_src):
     n = nc + 1
-    cell_rounds = float(counters[:, 1].sum() + counters[:, 7].sum())
+    # counters: 1 = RHS calls, 2 = Jacobians, 7 = RHS calls inside Jacobians.  The advance kernel visits a cell
+    # once per RHS call and once per Jacobian (all n columns come from one RHS-kernel visit).
+    evals = float(counters[:, 1].sum() + counters[:, 7].sum())
+    visits = float(counters[:, 1].sum() + counters[:, 2].sum())
     per_unit = {"plain": 2 * n * 8 + 8, "advance": 42 * n * 8 + 2 * 272, "rhs": 2 * n * 8 + 16}
-    units = {"plain": float(ncells), "advance": cell_rounds, "rhs": cell_rounds}
+    units = {"plain": float(ncells), "advance": visits, "rhs": evals}
     timed = {k: v for k, v in ktimes.items() if v[1] > 0}
     if not timed:
         return None

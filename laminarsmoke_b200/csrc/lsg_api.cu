@@ -44,6 +44,7 @@ struct lsg_ctx {
   void* rstate = nullptr;
   long rcap = 0;
   int rstate_lu64 = -1;
+  size_t rcache = 0;            // bytes of the RHS column scratch after the round state
   RoundsPlan rplan{};
   int rplan_lu64 = -1;
   int* nact_host = nullptr;   // pinned
@@ -241,13 +242,15 @@ int ensure_rounds(lsg_ctx* c, long n, bool lu64) {
     cudaGetLastError();
     return LSG_ERR_NOMEM;
   }
-  if (c->rstate && c->rcap >= n && c->rstate_lu64 == (int)lu64) return LSG_OK;
+  const size_t cache = rounds_cache_bytes(L, c->rplan);
+  if (c->rstate && c->rcap >= n && c->rstate_lu64 == (int)lu64 && c->rcache >= cache) return LSG_OK;
   cudaFree(c->rstate);
   c->rstate = nullptr;
   c->rcap = 0;
   const long cap = (n + 255) & ~255L;
-  if (cudaMalloc(&c->rstate, rounds_bytes(L, cap, lu64)) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+  if (cudaMalloc(&c->rstate, rounds_bytes(L, cap, lu64) + cache) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
   c->rcap = cap;
+  c->rcache = cache;
   c->rstate_lu64 = (int)lu64;
   return LSG_OK;
 }

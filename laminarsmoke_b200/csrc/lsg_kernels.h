@@ -113,6 +113,9 @@ struct RoundsPlan {
   unsigned g_rhs, g_adv, g_cmp, g_init;
 };
 size_t rounds_bytes(const MechLayout& L, long ns, bool lu64);
+// Column scratch of the RHS kernel's threads (n doubles per thread of the plan's RHS grid), placed right
+// after the rounds_bytes of the state.
+size_t rounds_cache_bytes(const MechLayout& L, const RoundsPlan& P);
 cudaError_t upload_gear_rounds(const GearConsts& gc);
 cudaError_t rounds_prepare(const MechLayout& L, bool lu64, int sm_count, int width, RoundsPlan* plan);
 cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsigned char* mech_gmem,

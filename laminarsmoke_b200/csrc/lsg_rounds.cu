@@ -4,8 +4,9 @@
 // still integrating:
 //
 //   rhs       one thread per cell evaluates the RHS the cell asked for (f(y0),
-//             the predictor, a finite-difference Jacobian column, a Newton
-//             iterate, a stabilisation call or the final call at tOut): the
+//             the predictor, a Newton iterate, a stabilisation call or the
+//             final call at tOut), or all n perturbed RHS of a
+//             finite-difference Jacobian and the Jacobian itself: the
 //             reaction loop runs convergent across the warp, with the
 //             mechanism tables staged once per block into shared memory by a
 //             bulk copy;
@@ -46,7 +47,7 @@ enum Phase : int {
   PH_DONE = 0,
   PH_INIT,       // f(y0)
   PH_PRED,       // f(vb), first Newton evaluation
-  PH_JAC,        // f(vb + hJ e_j), FD column jcol
+  PH_JAC,        // f(vb + hJ_j e_j) for every column j: the whole FD Jacobian in one visit
   PH_NEWTON,     // f(va), Newton iterate
   PH_STAB_CONV,  // f(z0) during convergence-failure recovery
   PH_STAB_ERR,   // f(z0) after an error-test failure
@@ -118,12 +119,12 @@ __device__ __forceinline__ double hi_b(int k, int NC, double ymaxT) { return k <
 // (BatchReactorHomogeneousConstantPressure.H:175-223).  y: this cell's input
 // vector (stride ns) with component pj replaced by pval when pj >= 0; f: output.
 // C (concentrations), G (h/RT - s/R) and R (formation rates) scratch in shared
-// memory, [species][thread].  Returns QR.
+// memory, [species][thread].  f has stride fs.  Returns QR.
 // ---------------------------------------------------------------------------
 __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const double* __restrict__ Md,
                                         const int* __restrict__ Mi, double* __restrict__ scratch,
                                         const double* __restrict__ y, long ns, int pj, double pval,
-                                        double* __restrict__ f, double P0, int energy) {
+                                        double* __restrict__ f, long fs, double P0, int energy) {
   const MechLayout& L = *Lp;
   const MechView M{Md, Mi};
   const int NC = L.nc, NR = L.nr;
@@ -240,17 +241,19 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
     if (kind != 0) {
       double rv = 1.;
       for (int q = pp[j]; q < pp[j + 1]; ++q) rv *= conc_factor_r(pnu[q], SC_(C, psp[q]));
+      double rf;
       if (kind == 1) {
         // 1/Keq = exp(sum_products nu g - sum_reactants nu g - dnu ln(Patm/RT)), g = h/RT - s/R
         // (StoichiometricMap.hpp:916-1001, KineticsMap_CHEMKIN.hpp:1217-1222, summed per side)
         double dg = 0.;
         for (int q = pp[j]; q < pp[j + 1]; ++q) dg += contrib_r(pnu[q], SC_(G, psp[q]));
         for (int q = rp[j]; q < rp[j + 1]; ++q) dg -= contrib_r(rnu[q], SC_(G, rsp[q]));
-        rv *= exp(dg - lP * dnu[j]);
+        rf = exp(dg - lP * dnu[j]);
       } else {
         const int s = rs[j];
-        rv *= exp(M.D(L.rev_lnA)[s] + M.D(L.rev_beta)[s] * logT - M.D(L.rev_eor)[s] * uT) / kArr;
+        rf = exp(M.D(L.rev_lnA)[s] + M.D(L.rev_beta)[s] * logT - M.D(L.rev_eor)[s] * uT) / kArr;
       }
+      rv *= rf;
       net -= rv;
     }
     net *= kMod;
@@ -260,7 +263,7 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
   double QR = 0., cpm = 0., dsum = 0.;
   for (int i = 0; i < NC; ++i) {
     const double Ri = SC_(R, i);
-    f[(long)i * ns] = MW[i] * Ri / rho;
+    f[(long)i * fs] = MW[i] * Ri / rho;
     if (energy) {
       const bool hi = T > TM[i];
       const double* A = hi ? M.D(L.cp_ht) + 5 * i : M.D(L.cp_lt) + 5 * i;
@@ -277,7 +280,7 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
     QR = -dsum * kRgas * T;
     dT = QR / (rho * CpMixMass);
   }
-  f[(long)NC * ns] = dT;
+  f[(long)NC * fs] = dT;
 #undef SC_
   return QR;
 }
@@ -473,6 +476,9 @@ struct RoundBufs {
   unsigned char* bin;   // [capacity] bin of each list entry (compaction)
   int* bcnt;        // [kBins + 1] entries per bin
   int* bcur;        // [kBins + 1] append cursors per bin
+  int* rq;          // RHS work counter: warps take the next 32 list entries from it
+  int* njac;        // [2] leading Jacobian-bin entries of each list
+  double* fsc;      // column scratch of the RHS threads, n words x (RHS grid threads)
 };
 
 }  // namespace
@@ -486,6 +492,9 @@ __global__ void __launch_bounds__(kAT) rounds_init_kernel(int NC, StepOptions o,
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     B.nact[0] = (int)a.ncells;
     B.nact[1] = 0;
+    B.njac[0] = 0;
+    B.njac[1] = 0;
+    *B.rq = 0;
   }
   for (long cell = (long)blockIdx.x * blockDim.x + threadIdx.x; cell < a.ncells;
        cell += (long)gridDim.x * blockDim.x) {
@@ -530,11 +539,49 @@ __global__ void __launch_bounds__(kAT) rounds_init_kernel(int NC, StepOptions o,
   }
 }
 
+// One column j of a cell's finite-difference Jacobian (KernelDense::
+// NumericalJacobian, constrained branch, KernelDense.hpp:111-193):
+// J(:, j) = (f(vb + hJ_j e_j) - f0) / hJ_j, stored in FP32 in the cell record.
+// The n columns of a cell run on n threads of the same RHS launch; fp is this
+// thread's n-word scratch (stride fs).  The T column, the reference's last,
+// leaves its f in the record and sets QR, as the last evaluation did there;
+// column 0 counts the n evaluations.  Out of line, so that the RHS kernel
+// keeps the register budget of its single-evaluation path.
+__device__ __noinline__ void jacobian_column(const MechLayout* L, const double* Md, const int* Mi, double* scratch,
+                                             double* R, const RecLayout RL, int j, double P0, int energy,
+                                             double y_max_T, double* fp, long fs) {
+  const int n = L->nc + 1;
+  const double* vb = R + RL.ovb;
+  const double yh = vb[j], ej = R[RL.oeps + j];
+  const double hf = R[D_HF];
+  const double aa = fabs(yh), bb = fabs(1. / ej);
+  double hJ = sqrt(kMachEpsDouble) * (aa > bb ? aa : bb);
+  hJ = fmax(hJ, hf / ej);
+  hJ = fmax(hJ, sqrt(kTinyFloat));
+  if (yh + hJ > (j < n - 1 ? 1. : y_max_T)) hJ = -hJ;
+  const bool last = j == n - 1;
+  double* f = last ? R + RL.of : fp;
+  const long ffs = last ? 1 : fs;
+  const double q = rhs_cell(L, Md, Mi, scratch, vb, 1, j, yh + hJ, f, ffs, P0, energy);
+  const double* f0 = R + RL.of0;
+  float* Jg = (float*)(R + RL.ojac);
+  const double hInv = 1. / hJ;
+  for (int i = 0; i < n; ++i) Jg[i * n + j] = (float)(hInv * (f[(long)i * ffs] - f0[i]));
+  if (last) R[D_QR] = q;
+  if (j == 0) {
+    int* RI = (int*)(R + ND_);
+    RI[I_CNT0 + CNT_JAC_RHS] += n;
+  }
+}
+
 // ---------------------------------------------------------------------------
-// rhs: one thread per listed cell that requested an evaluation.
+// rhs: one thread per requested evaluation.  The list starts with the cells
+// that build a Jacobian (njac of them, the compaction's first bin); each of
+// those is n work items, one per column, the other cells one item each.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kRT) rounds_rhs_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem,
-                                                          int energy, double P0, RoundBufs B, int par, int* err) {
+__global__ void __launch_bounds__(kRT, 4) rounds_rhs_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem,
+                                                          int energy, double P0, double y_max_T, RoundBufs B, int par,
+                                                          int* err) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ MechLayout sL;
@@ -549,13 +596,37 @@ __global__ void __launch_bounds__(kRT) rounds_rhs_kernel(MechLayout Lp, const un
   double* scratch = (double*)(smem + ((Lp.bytes + 15u) & ~15u));
   const RecLayout RL = B.L;
   const int nact = B.nact[par];
+  const int njac = B.njac[par];
+  const int n = Lp.nc + 1;
   const int* act = par ? B.act1 : B.act0;
-  for (int idx = blockIdx.x * kRT + threadIdx.x; idx < nact; idx += gridDim.x * kRT) {
-    const int cell = act[idx];
+  const int nitems = njac * n + (nact - njac);
+  double* fp = B.fsc + (long)blockIdx.x * kRT + threadIdx.x;   // this thread's column scratch
+  const long fs = (long)gridDim.x * kRT;
+  // Dynamic distribution: each warp takes the next 32 work items.  Consecutive items of a Jacobian are
+  // consecutive columns of one cell, so a warp's J stores and record reads land on neighbouring words.
+  const int wl = threadIdx.x & 31;
+  for (;;) {
+    int base = 0;
+    if (wl == 0) base = atomicAdd(B.rq, 32);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= nitems) break;
+    const int item = base + wl;
+    if (item >= nitems) continue;
+    if (item < njac * n) {
+      const int e = item / n;
+      double* R = B.rec + (long)act[e] * RL.RS;
+      jacobian_column(&sL, Md, Mi, scratch, R, RL, item - e * n, P0, energy, y_max_T, fp, fs);
+      continue;
+    }
+    const int cell = act[njac + (item - njac * n)];
     double* R = B.rec + (long)cell * RL.RS;
     int* RI = (int*)(R + ND_);
     const int ph = RI[I_PHASE];
     if (!rhs_phase(ph)) continue;
+    if (ph == PH_JAC) {   // a Jacobian outside the list head (not produced by the compaction): serially
+      for (int j = 0; j < n; ++j) jacobian_column(&sL, Md, Mi, scratch, R, RL, j, P0, energy, y_max_T, fp, fs);
+      continue;
+    }
     const double* src = R + RL.ova;
     double* dst = R + RL.of;
     int pj = -1;
@@ -563,16 +634,11 @@ __global__ void __launch_bounds__(kRT) rounds_rhs_kernel(MechLayout Lp, const un
     if (ph == PH_PRED) {
       src = R + RL.ovb;
       dst = R + RL.of0;
-    } else if (ph == PH_JAC) {
-      src = R + RL.ovb;
-      pj = RI[I_JCOL];
-      pval = src[pj] + R[D_HJ];
     } else if (ph == PH_STAB_CONV || ph == PH_STAB_ERR) {
       src = R + RL.oz;
     }
-    R[D_QR] = rhs_cell(&sL, Md, Mi, scratch, src, 1, pj, pval, dst, P0, energy);
-    const int ck = (ph == PH_JAC) ? CNT_JAC_RHS : CNT_RHS;
-    RI[I_CNT0 + ck] += 1;
+    R[D_QR] = rhs_cell(&sL, Md, Mi, scratch, src, 1, pj, pval, dst, 1, P0, energy);
+    RI[I_CNT0 + CNT_RHS] += 1;
   }
 }
 
@@ -758,10 +824,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
         break;
       }
       case PH_JAC: {
-        const double hInv = 1. / hJ;
-        if (al) Jg[lane * n + jcol] = (float)(hInv * (f - f0));
-        ++jcol;
-        if (jcol < n) { lab = L_JAC_COLUMN; break; }
+        // the RHS kernel has built every column of J
         ++cjac;
         factorized = 0;
         lab = L_AFTER_JAC;
@@ -883,14 +946,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
           break;
         }
         case L_JAC_COLUMN: {
-          // KernelDense::NumericalJacobian, constrained branch: increment of column jcol
-          const double yh = __shfl_sync(gm, vb, jcol, W);
-          const double ej = __shfl_sync(gm, eps, jcol, W);
-          const double aa = fabs(yh), bb = fabs(1. / ej);
-          hJ = sqrt(kMachEpsDouble) * (aa > bb ? aa : bb);
-          hJ = fmax(hJ, hf / ej);
-          hJ = fmax(hJ, sqrt(kTinyFloat));
-          if (yh + hJ > (jcol < NC ? 1. : o.y_max_T)) hJ = -hJ;
+          // KernelDense::NumericalJacobian: the RHS kernel evaluates all n perturbed states next
           phase = PH_JAC;
           lab = L_NONE;
           break;
@@ -1189,7 +1245,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
 
 // ---------------------------------------------------------------------------
 // compact: the cells still integrating form the next list, binned by the solver
-// path their next advance will take -- Jacobian columns; predictor results that
+// path their next advance will take -- Jacobians; predictor results that
 // start a Jacobian, that need a factorisation, that need neither; Newton
 // iterates; the rest -- so that the cells that share a warp mostly take the
 // same path.  Two kernels: count (bin of every entry, per-bin totals) and
@@ -1226,6 +1282,7 @@ __global__ void __launch_bounds__(kCT) rounds_count_kernel(RoundBufs B, int par)
 }
 
 __global__ void __launch_bounds__(kCT) rounds_scatter_kernel(RoundBufs B, int par) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *B.rq = 0;   // the next round's RHS kernel takes work from zero
   const int nact = B.nact[par];
   const int* in = par ? B.act1 : B.act0;
   int* out = par ? B.act0 : B.act1;
@@ -1233,7 +1290,10 @@ __global__ void __launch_bounds__(kCT) rounds_scatter_kernel(RoundBufs B, int pa
   start[0] = 0;
   start[1] = 0;
   for (int b = 2; b <= kBins; ++b) start[b] = start[b - 1] + B.bcnt[b - 1];
-  if (blockIdx.x == 0 && threadIdx.x == 0) B.nact[par ^ 1] = start[kBins] + B.bcnt[kBins];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    B.nact[par ^ 1] = start[kBins] + B.bcnt[kBins];
+    B.njac[par ^ 1] = B.bcnt[1];
+  }
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * kCT + threadIdx.x) >> 5;
   const int nw = gridDim.x * (kCT / 32);
@@ -1268,6 +1328,8 @@ RoundBufs carve(const MechLayout& L, void* base, long cap, bool lu64) {
   B.nact = (int*)p;
   B.bcnt = B.nact + 4;
   B.bcur = B.bcnt + 8;
+  B.rq = B.bcur + 8;
+  B.njac = B.nact + 2;
   return B;
 }
 
@@ -1291,6 +1353,10 @@ cudaError_t prepare_advance(size_t as, int* bps) {
 size_t rounds_bytes(const MechLayout& L, long cap, bool lu64) {
   const RecLayout R = rec_layout(L.nc + 1, lu64);
   return sizeof(double) * (size_t)R.RS * cap + 2 * list_bytes(cap) + ((cap + 255) & ~255L) + 256;
+}
+
+size_t rounds_cache_bytes(const MechLayout& L, const RoundsPlan& P) {
+  return sizeof(double) * (size_t)(L.nc + 1) * (size_t)P.g_rhs * kRT;
 }
 
 cudaError_t upload_gear_rounds(const GearConsts& gc) { return cudaMemcpyToSymbol(c_gear_r, &gc, sizeof(GearConsts)); }
@@ -1332,7 +1398,8 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
   // nact_host: two pinned ints (list length, error flags); launches: kernels enqueued (added to)
   const int n = L.nc + 1;
   if (n > 32 || a.ncells > cap || a.ncells <= 0) return cudaErrorInvalidValue;
-  const RoundBufs B = carve(L, state, cap, P.lu64);
+  RoundBufs B = carve(L, state, cap, P.lu64);
+  B.fsc = (double*)((char*)state + rounds_bytes(L, cap, P.lu64));   // rounds_cache_bytes(L, P) after the rest
   kt->begin(KT_INIT, stream);
   rounds_init_kernel<<<P.g_init, kAT, 0, stream>>>(L.nc, o, a, B);
   kt->end(stream);
@@ -1344,7 +1411,8 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
   for (long round = 0; round < max_rounds; round += kBatch) {
     for (int r = 0; r < kBatch; ++r) {
       kt->begin(KT_RHS, stream);
-      rounds_rhs_kernel<<<P.g_rhs, kRT, P.rhs_smem, stream>>>(L, mech_gmem, o.energy, a.p, B, par, err);
+      rounds_rhs_kernel<<<P.g_rhs, kRT, P.rhs_smem, stream>>>(L, mech_gmem, o.energy, a.p, o.y_max_T, B, par,
+                                                              err);
       kt->end(stream);
       const dim3 ga(P.g_adv), ta(kWA * 32);
       kt->begin(KT_ADVANCE, stream);

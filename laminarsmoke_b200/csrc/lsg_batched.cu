@@ -157,6 +157,9 @@ __device__ __noinline__ double rhs_lane(const MechLayout* __restrict__ Lp, const
   const int* rp = M.I(L.reac_ptr);
   const int* rsp = M.I(L.reac_sp);
   const double* rnu = M.D(L.reac_nu);
+  const int* op = M.I(L.ford_ptr);     // forward rate-law orders (FORD, else the coefficients)
+  const int* osp = M.I(L.ford_sp);
+  const double* onu = M.D(L.ford_val);
   const int* pp = M.I(L.prod_ptr);
   const int* psp = M.I(L.prod_sp);
   const double* pnu = M.D(L.prod_nu);
@@ -217,7 +220,7 @@ __device__ __noinline__ double rhs_lane(const MechLayout* __restrict__ Lp, const
       kMod *= kInf * (Pr / (1. + Pr)) * wF / kArr;
     }
     double fwd = 1.;
-    for (int q = rp[j]; q < rp[j + 1]; ++q) fwd *= conc_factor_b(rnu[q], SC_(C, rsp[q]));
+    for (int q = op[j]; q < op[j + 1]; ++q) fwd *= conc_factor_b(onu[q], SC_(C, osp[q]));
     double net = fwd;
     const int kind = rk[j];
     if (kind != 0) {

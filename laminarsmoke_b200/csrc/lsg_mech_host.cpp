@@ -110,6 +110,11 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
     L.fo_d = B.addd(b.F("fo_d"));
     L.fo_e = B.addd(b.F("fo_e"));
     L.reac_nu = B.addd(b.F("reac_nu"));
+    // forward rate-law orders: the FORD lists when the mechanism has them, else the reactant coefficients
+    const bool ford = b.f.count("ford_val") != 0;
+    const std::vector<int>& ford_ptr = ford ? b.I("ford_ptr") : b.I("reac_ptr");
+    const std::vector<int>& ford_sp = ford ? b.I("ford_species") : b.I("reac_species");
+    L.ford_val = B.addd(ford ? b.F("ford_val") : b.F("reac_nu"));
     L.prod_nu = B.addd(b.F("prod_nu"));
     L.fr_coef = B.addd(b.F("fr_coef"));
     L.tb_eff = B.addd(b.F("tb_eff_m1"));
@@ -135,6 +140,8 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
     L.fo_slot = B.addi(fo_slot);
     L.reac_ptr = B.addi(b.I("reac_ptr"));
     L.reac_sp = B.addi(b.I("reac_species"));
+    L.ford_ptr = B.addi(ford_ptr);
+    L.ford_sp = B.addi(ford_sp);
     L.prod_ptr = B.addi(b.I("prod_ptr"));
     L.prod_sp = B.addi(b.I("prod_species"));
     L.fr_ptr = B.addi(b.I("fr_ptr"));
@@ -161,13 +168,15 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
       for (int x : v) if (x < lo || x >= hi) return false;
       return true;
     };
-    if (!in_range(b.I("reac_species"), 0, nc) || !in_range(b.I("prod_species"), 0, nc) ||
+    if (!in_range(b.I("reac_species"), 0, nc) || !in_range(b.I("prod_species"), 0, nc) || !in_range(ford_sp, 0, nc) ||
         !in_range(b.I("fr_rxn"), 0, nr) || !in_range(b.I("tb_species"), 0, nc) ||
         !in_range(b.I("fo_species"), 0, nc) || !in_range(tbr, 0, nr) || !in_range(fr, 0, nr)) {
       err = "index out of range in mechanism blob";
       return false;
     }
     if ((int)b.I("reac_ptr").size() != nr + 1 || (int)b.I("prod_ptr").size() != nr + 1 ||
+        (int)ford_ptr.size() != nr + 1 || ford_ptr.back() != (int)ford_sp.size() ||
+        (ford && b.F("ford_val").size() != ford_sp.size()) ||
         (int)b.I("fr_ptr").size() != nc + 1 || (int)b.F("mw").size() != nc ||
         (int)b.F("cp_ht").size() != 5 * nc || (int)b.F("dh_ht").size() != 6 * nc ||
         (int)b.F("lnA").size() != nr) {

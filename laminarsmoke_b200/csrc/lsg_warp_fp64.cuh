@@ -209,6 +209,9 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
     const int* rp = M.I(L.reac_ptr);
     const int* rsp = M.I(L.reac_sp);
     const double* rnu = M.D(L.reac_nu);
+    const int* op = M.I(L.ford_ptr);     // forward rate-law orders (FORD, else the coefficients)
+    const int* osp = M.I(L.ford_sp);
+    const double* onu = M.D(L.ford_val);
     const int* pp = M.I(L.prod_ptr);
     const int* psp = M.I(L.prod_sp);
     const double* pnu = M.D(L.prod_nu);
@@ -264,7 +267,7 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
         kMod *= corr;
       }
       double fwd = 1.;
-      for (int q2 = rp[j]; q2 < rp[j + 1]; ++q2) fwd *= conc_factor(rnu[q2], W.C[rsp[q2]]);
+      for (int q2 = op[j]; q2 < op[j + 1]; ++q2) fwd *= conc_factor(onu[q2], W.C[osp[q2]]);
       double net = fwd;
       const int kind = rk[j];
       if (kind != 0) {

@@ -6,6 +6,9 @@ workloads of this project use:
 * ``"h2co"``    -- POLIMI_H2CO_1412 (14 species, 33 reactions), compiled from the
                    reference's CHEMKIN files into ``data/POLIMI_H2CO_1412.lsmech``
                    by ``mech/build_data.py``;
+* ``"ch4_1step"``, ``"h2_1step"`` -- the reference's global one-step CH4 and H2
+                   mechanisms (forward reaction orders given by FORD), in
+                   ``data/GLOBAL_*_1step.lsmech``;
 * ``"syn120"``  -- seeded synthetic C1-C2 mechanism, 120 species / 800 reactions;
 * ``"syn500"``  -- seeded synthetic mechanism, 500 species / 3 000 reactions;
 * ``"h2co+K"``  -- POLIMI_H2CO_1412 with K chemically inert copies of N2 added
@@ -53,8 +56,9 @@ def pad_inert(data: bytes, k: int, template: str = "N2") -> Tuple[bytes, List[st
 def load(name: str) -> Tuple[bytes, List[str]]:
     if name.startswith("h2co+"):
         return pad_inert(load("h2co")[0], int(name[5:]))
-    if name == "h2co":
-        path = os.path.join(DATA, "POLIMI_H2CO_1412.lsmech")
+    files = {"h2co": "POLIMI_H2CO_1412", "ch4_1step": "GLOBAL_CH4_1step", "h2_1step": "GLOBAL_H2_1step"}
+    if name in files:
+        path = os.path.join(DATA, files[name] + ".lsmech")
         with open(path, "rb") as f:
             data = f.read()
         _, species = _blob.unpack(data)

@@ -271,6 +271,8 @@ class Reaction:
     tb_eff: List[float] = field(default_factory=list)
     pd_species: int = -1
     duplicate: bool = False
+    ford: bool = False   # FORD given: forward_orders replace the reactant coefficients in the rate law
+    forward_orders: List[Tuple[int, float]] = field(default_factory=list)
     text: str = ""
 
 
@@ -311,6 +313,18 @@ def _reorder_clean(pairs: List[Tuple[int, float]]) -> List[Tuple[int, float]]:
             nu[i - 1] += nu[i]
             idx[i] = -1
     return [(i, v) for i, v in zip(idx, nu) if i != -1]
+
+
+def _species_value(line: str, what: str) -> Tuple[str, float]:
+    """`KEY /SPECIES value/` (ReadReactionKeyWordPlusCoefficients with two tokens)."""
+    a, b = line.find("/"), line.rfind("/")
+    toks = line[a + 1:b].split() if 0 <= a < b else []
+    if len(toks) != 2:
+        raise ChemkinError(f"{what}: expected /SPECIES value/ in: {line.strip()}")
+    try:
+        return toks[0], float(toks[1])
+    except ValueError:
+        raise ChemkinError(f"{what}: bad value in: {line.strip()}") from None
 
 
 def _slash_numbers(line: str, counts: Sequence[int], what: str) -> List[float]:
@@ -440,6 +454,24 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
                 raise ChemkinError("REV used on an irreversible reaction")
             r.A_rev, r.beta_rev, r.E_rev = c
             r.explicit_rev = True
+        elif kw == "FORD":
+            # ReactionPolicy_CHEMKIN.hpp:511-545: the order of one species in the forward rate law; the
+            # reactant coefficients are the starting orders, a species not among the reactants is appended
+            nm, val = _species_value(line, "FORD")
+            if nm not in species_index:
+                raise ChemkinError(f"FORD: species not available: {nm}")
+            if not r.ford:
+                r.forward_orders = list(r.reactants)
+                r.ford = True
+            si = species_index[nm]
+            for q, (sq, _) in enumerate(r.forward_orders):
+                if sq == si:
+                    r.forward_orders[q] = (si, val)
+                    break
+            else:
+                r.forward_orders.append((si, val))
+        elif kw == "RORD":
+            raise ChemkinError("option RORD is not available (ReactionPolicy_CHEMKIN.hpp:908-913 rejects it)")
         elif kw in ("DUP", "DUPLICATE"):
             r.duplicate = True
         elif kw == "UNITS":
@@ -447,6 +479,8 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
         else:
             raise ChemkinError(f"option {keyword} is not supported by this compiler")
 
+    if r.ford:   # ReorderPairsOfVectors + CleanPairsOfVectors of the orders (ReactionPolicy_CHEMKIN.hpp:1266-1271)
+        r.forward_orders = _reorder_clean(r.forward_orders)
     if pdr == "all" and not i_low:
         raise ChemkinError("no pressure dependence option defined")
     if pdr == "partial" and not i_low:
@@ -480,8 +514,8 @@ def _convert_units(r: Reaction, a_units: str, e_units: str) -> None:
         "KELV": 1.e3 * R_J_MOL,
     }[e_units]
     a_conv = 1. if a_units == "MOLE" else NAV_MOL
-    sum_lr = 0.
-    for _, v in r.reactants:
+    sum_lr = 0.   # ReactionOrders: the sums of the rate-law orders (lambda), FORD included
+    for _, v in (r.forward_orders if r.ford else r.reactants):
         sum_lr += v
     sum_lp = 0.
     for _, v in r.products:
@@ -741,6 +775,16 @@ def build_tables(species: List[str], reactions: List[Reaction], thermo: List[The
     A["reac_nu"] = np.array(rnu, f64)
     A["prod_ptr"] = np.array(pptr, np.int32); A["prod_species"] = np.array(psp, np.int32)
     A["prod_nu"] = np.array(pnu, f64)
+    if any(r.ford for r in reactions):
+        # forward rate-law orders (StoichiometricMap lambda lists), only when some reaction has FORD;
+        # without them the reactant coefficients are the orders
+        optr, osp, oval = [0], [], []
+        for r in reactions:
+            for sp, v in (r.forward_orders if r.ford else r.reactants):
+                osp.append(sp); oval.append(v)
+            optr.append(len(osp))
+        A["ford_ptr"] = np.array(optr, np.int32); A["ford_species"] = np.array(osp, np.int32)
+        A["ford_val"] = np.array(oval, f64)
 
     # --- formation-rate lists in the reference's accumulation order
     # (StoichiometricMap.hpp:656-729): per species, reactant buckets 1,2,3,1/2,other

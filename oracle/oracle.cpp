@@ -72,6 +72,13 @@ static Mech* load_blob(const unsigned char* p, size_t n) {
   }
   m->nc = m->I("dims")[0];
   m->nr = m->I("dims")[1];
+  // Forward rate-law orders (ReactionPolicy_CHEMKIN reactant_lambda_): the FORD lists when the mechanism
+  // has them, else the reactant coefficients (ReactionPolicy_CHEMKIN.hpp:380-381).
+  if (!m->f.count("ford_val")) {
+    m->i["ford_ptr"] = m->I("reac_ptr");
+    m->i["ford_species"] = m->I("reac_species");
+    m->f["ford_val"] = m->F("reac_nu");
+  }
   return m;
 }
 
@@ -260,8 +267,9 @@ struct Reactor {
     }
     for (size_t k = 0; k < fr.size(); ++k) kMod[fr[k]] *= corr[k];
 
-    // StoichiometricMap::ProductOfConcentrations (:512-598): factors in species order
-    const auto& rp = m.I("reac_ptr"); const auto& rs = m.I("reac_species"); const auto& rn = m.F("reac_nu");
+    // StoichiometricMap::ProductOfConcentrations (:512-598): factors in species order, forward orders
+    // lambda (FORD or the reactant coefficients)
+    const auto& rp = m.I("ford_ptr"); const auto& rs = m.I("ford_species"); const auto& rn = m.F("ford_val");
     const auto& pp = m.I("prod_ptr"); const auto& ps = m.I("prod_species"); const auto& pn = m.F("prod_nu");
     const auto& isrev = m.I("is_reversible");
     for (int j = 0; j < NR; ++j) {

@@ -162,3 +162,84 @@ def test_compile_command_line(tmp_path):
     r = subprocess.run([sys.executable, "-m", "laminarsmoke_b200.mech", "info", str(out)],
                        capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and f"{m.n_species} species" in r.stdout
+
+
+def _ford_case(extra=""):
+    s = synthetic.generate(12, 10, seed=1)
+    a, b, c = list(s.compositions)[:3]
+    kin = (f"ELEMENTS\nC H O N\nEND\nSPECIES\n{a} {b} {c}\nEND\nREACTIONS\n"
+           f"{a}+{b}=>{c} 1.0E13 0.5 1000.\nFORD /{a} 0.7/\nFORD /{c} 0.2/\n{extra}END\n")
+    return kin, s.thermo
+
+
+def test_ford_orders_and_units():
+    """FORD (ReactionPolicy_CHEMKIN.hpp:511-545): the reactant coefficients are the starting orders, a FORD
+    species replaces its order or is appended, the list is sorted by species, and the units of A follow
+    the sum of the orders (0.7 + 1 + 0.2 = 1.9): A [m, kmol, s] = 1e13 * 1e3^(1 - 1.9)."""
+    kin, thermo = _ford_case()
+    m = chemkin.compile_mechanism(kin, thermo)
+    A = m.arrays
+    np.testing.assert_array_equal(A["reac_nu"], [1.0, 1.0])
+    np.testing.assert_array_equal(A["ford_ptr"], [0, 3])
+    np.testing.assert_array_equal(A["ford_species"], [0, 1, 2])
+    np.testing.assert_array_equal(A["ford_val"], [0.7, 1.0, 0.2])
+    assert A["lnA"][0] == math.log(1.0e13 * math.pow(1.e3, 1. - 1.9))
+
+
+def test_ford_absent_keeps_the_blob_unchanged(h2co):
+    assert "ford_val" not in h2co[2]
+
+
+def test_rord_is_rejected_like_the_reference():
+    kin, thermo = _ford_case("RORD /X 1.0/\n")
+    with pytest.raises(chemkin.ChemkinError):
+        chemkin.compile_mechanism(kin, thermo)
+
+
+def test_global_ch4_one_step():
+    """The reference's GLOBAL_CH4_1step: CH4 + 2 O2 => CO2 + 2 H2O with FORD /CH4 1/ /O2 1/, so the rate
+    law is second order and A = 1e15 cm3/mol/s = 1e12 m3/kmol/s."""
+    from laminarsmoke_b200 import mech
+    from laminarsmoke_b200.mech import blob
+    A, species = blob.unpack(mech.load("ch4_1step")[0])
+    assert species == ["CH4", "O2", "CO2", "H2O", "N2"]
+    np.testing.assert_array_equal(A["reac_nu"], [1.0, 2.0])
+    np.testing.assert_array_equal(A["ford_val"], [1.0, 1.0])
+    assert A["lnA"][0] == math.log(1.0e15 * math.pow(1.e3, 1. - 2.0))
+    assert A["e_over_r"][0] == 20000.0 * 1.e3 * J_FROM_CAL / R_J_KMOL
+
+
+def test_oracle_rhs_global_ch4_rate_law():
+    """Oracle RHS of the one-step CH4 mechanism against the rate law written out by hand:
+    r = k [CH4] [O2], dY_i/dt = MW_i nu_i r / rho."""
+    from laminarsmoke_b200 import mech
+    from laminarsmoke_b200.mech import blob
+    from oracle.oracle import OracleMechanism
+    data, species = mech.load("ch4_1step")
+    A, _ = blob.unpack(data)
+    mw = A["mw"]
+    orc = OracleMechanism(data)
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        Y = rng.uniform(0.01, 1.0, 5)
+        Y /= Y.sum()
+        T = rng.uniform(800.0, 2200.0)
+        dy, _ = orc.rhs(np.concatenate([Y, [T]]))
+        ctot = 101325.0 / R_J_KMOL / T
+        mwmix = 1.0 / (Y / mw).sum()
+        c = ctot * mwmix * Y / mw
+        k = math.exp(A["lnA"][0] - A["e_over_r"][0] / T)
+        r = k * c[0] * c[1]
+        rho = ctot * mwmix
+        nu = np.array([-1.0, -2.0, 1.0, 2.0, 0.0])
+        np.testing.assert_allclose(dy[:5], mw * nu * r / rho, rtol=1e-12, atol=1e-300)
+
+
+@pytest.mark.skipif(not os.path.exists("/root/reference/run/kinetic-mechanisms/GLOBAL_CH4_1step"),
+                    reason="reference CHEMKIN files not present")
+@pytest.mark.parametrize("name,key", [("GLOBAL_CH4_1step", "ch4_1step"), ("GLOBAL_H2_1step", "h2_1step")])
+def test_packaged_global_blobs_match_fresh_compile(name, key):
+    from laminarsmoke_b200 import mech
+    d = f"/root/reference/run/kinetic-mechanisms/{name}/"
+    m = chemkin.compile_files(d + name + ".CKI", d + name + ".CKT")
+    assert blob.pack(m.arrays, m.species) == mech.load(key)[0]

@@ -677,6 +677,15 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
     const int cell = act[widx];
     double* R = B.rec + (long)cell * RL.RS;
     int* RI = (int*)(R + ND_);
+    {
+      // ask L2 for the record this group visits next, so its DRAM latency overlaps this visit
+      const int wn = widx + gridDim.x * G;
+      if (wn < nact) {
+        const char* Rn = (const char*)(B.rec + (long)act[wn] * RL.RS);
+        for (int off = lane * 128; off < RL.RS * 8; off += W * 128)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(Rn + off));
+      }
+    }
     int phase = RI[I_PHASE];
     if (!rhs_phase(phase)) continue;   // same in all lanes
     // ---- scalar state (every lane reads the same words) ----

@@ -6,6 +6,9 @@ workloads of this project use:
 * ``"h2co"``    -- POLIMI_H2CO_1412 (14 species, 33 reactions), compiled from the
                    reference's CHEMKIN files into ``data/POLIMI_H2CO_1412.lsmech``
                    by ``mech/build_data.py``;
+* ``"h2"``, ``"ch4"`` -- POLIMI_H2_1412 (9 species, 20 reactions) and
+                   POLIMI_CH4_SKELETAL_1412 (24 species, 155 reactions), from the
+                   reference's files likewise;
 * ``"ch4_1step"``, ``"h2_1step"`` -- the reference's global one-step CH4 and H2
                    mechanisms (forward reaction orders given by FORD), in
                    ``data/GLOBAL_*_1step.lsmech``;
@@ -56,7 +59,8 @@ def pad_inert(data: bytes, k: int, template: str = "N2") -> Tuple[bytes, List[st
 def load(name: str) -> Tuple[bytes, List[str]]:
     if name.startswith("h2co+"):
         return pad_inert(load("h2co")[0], int(name[5:]))
-    files = {"h2co": "POLIMI_H2CO_1412", "ch4_1step": "GLOBAL_CH4_1step", "h2_1step": "GLOBAL_H2_1step"}
+    files = {"h2co": "POLIMI_H2CO_1412", "h2": "POLIMI_H2_1412", "ch4": "POLIMI_CH4_SKELETAL_1412",
+             "ch4_1step": "GLOBAL_CH4_1step", "h2_1step": "GLOBAL_H2_1step"}
     if name in files:
         path = os.path.join(DATA, files[name] + ".lsmech")
         with open(path, "rb") as f:

@@ -16,6 +16,10 @@ from . import DATA, blob, chemkin
 MECHS = {
     "POLIMI_H2CO_1412": ("run/kinetic-mechanisms/POLIMI_H2CO_1412/POLIMI_H2CO_1412.CKI",
                          "run/kinetic-mechanisms/POLIMI_H2CO_1412/POLIMI_TOT_NOX_1412.CKT"),
+    "POLIMI_H2_1412": ("run/kinetic-mechanisms/POLIMI_H2_1412/POLIMI_H2_1412.CKI",
+                       "run/kinetic-mechanisms/POLIMI_H2_1412/POLIMI_TOT_NOX_1412.CKT"),
+    "POLIMI_CH4_SKELETAL_1412": ("run/kinetic-mechanisms/POLIMI_CH4_SKELETAL_1412/POLIMI_CH4_SKELETAL_1412.CKI",
+                                 "run/kinetic-mechanisms/POLIMI_CH4_SKELETAL_1412/POLIMI_TOT_NOX_1412.CKT"),
     # global one-step mechanisms with forward reaction orders (FORD)
     "GLOBAL_CH4_1step": ("run/kinetic-mechanisms/GLOBAL_CH4_1step/GLOBAL_CH4_1step.CKI",
                          "run/kinetic-mechanisms/GLOBAL_CH4_1step/GLOBAL_CH4_1step.CKT"),

@@ -133,6 +133,24 @@ int lsg_reaction_step_device(lsg_ctx* ctx, int ncells, int nspecies, double* Y_d
                              double p, double t0, const double* dt_dev, double dt_scalar, double* Q_dev,
                              int* status_dev, int* nsteps_dev, long long* counters_dev, void* stream);
 
+/* ---- reaction step, constant-volume reactor ------------------------------
+ * The branch of chemistry_DI.H taken with constPressureBatchReactor false
+ * (:168-203): BatchReactorHomogeneousConstantVolume::SetReactor(V, P, rho)
+ * and its Equations (BatchReactorHomogeneousConstantVolume.H:148-199).  Each
+ * cell keeps its density rho [kg/m3] (the CFD field rhoCells): the
+ * concentrations are rho / MW x_i, dY_i/dt = MW_i R_i / rho and, with the
+ * energy equation, dT/dt = (QR + R T sum_i R_i) / (rho cv).  The pressure of
+ * the constant-pressure calls has no counterpart (the reactor's P follows
+ * from rho and T); every other argument and the pre- and post-processing are
+ * those of lsg_reaction_step / lsg_reaction_step_device.  rho may not be NULL. */
+int lsg_reaction_step_cv(lsg_ctx* ctx, int ncells, int nspecies, double* const* Y_species, double* T,
+                         const double* rho, double t0, const double* dt, double dt_scalar, double* Q_out,
+                         int* status_out, int* nsteps_out);
+int lsg_reaction_step_cv_device(lsg_ctx* ctx, int ncells, int nspecies, double* Y_dev, long ld, double* T_dev,
+                                const double* rho_dev, double t0, const double* dt_dev, double dt_scalar,
+                                double* Q_dev, int* status_dev, int* nsteps_dev, long long* counters_dev,
+                                void* stream);
+
 /* The context's own stream (a cudaStream_t), for callers without one. */
 void* lsg_ctx_stream(lsg_ctx* ctx);
 

@@ -33,6 +33,7 @@ struct lsg_ctx {
   double* dT = nullptr;
   double* ddt = nullptr;
   double* dQ = nullptr;
+  double* drho = nullptr;       // staged densities of the constant-volume host call
   int* dstatus = nullptr;
   int* dnsteps = nullptr;
   // lane-per-cell (batched) resources
@@ -136,7 +137,8 @@ int validate_options(const lsg_options* o) {
 
 void free_buffers(lsg_ctx* c) {
   cudaFree(c->dY); cudaFree(c->dT); cudaFree(c->ddt); cudaFree(c->dQ); cudaFree(c->dstatus); cudaFree(c->dnsteps);
-  c->dY = c->dT = c->ddt = c->dQ = nullptr;
+  cudaFree(c->drho);
+  c->dY = c->dT = c->ddt = c->dQ = c->drho = nullptr;
   c->dstatus = c->dnsteps = nullptr;
   c->cap = 0;
 }
@@ -150,6 +152,7 @@ int ensure_capacity(lsg_ctx* c, long n) {
       cudaMalloc(&c->dT, sizeof(double) * cap) != cudaSuccess ||
       cudaMalloc(&c->ddt, sizeof(double) * cap) != cudaSuccess ||
       cudaMalloc(&c->dQ, sizeof(double) * cap) != cudaSuccess ||
+      cudaMalloc(&c->drho, sizeof(double) * cap) != cudaSuccess ||
       cudaMalloc(&c->dstatus, sizeof(int) * cap) != cudaSuccess ||
       cudaMalloc(&c->dnsteps, sizeof(int) * cap) != cudaSuccess) {
     free_buffers(c);
@@ -614,9 +617,11 @@ int lsg_ctx_check(lsg_ctx* c, int* flags) {
   return h ? LSG_ERR_DEVICE : LSG_OK;
 }
 
-int lsg_reaction_step_device(lsg_ctx* c, int ncells, int nspecies, double* Y, long ld, double* T, double p,
-                             double t0, const double* dt, double dt_scalar, double* Q, int* status, int* nsteps,
-                             long long* counters, void* stream) {
+namespace {
+// The device-array step of both reactors: rho == nullptr is the constant-pressure reactor at p.
+int device_step(lsg_ctx* c, int ncells, int nspecies, double* Y, long ld, double* T, double p, const double* rho,
+                double t0, const double* dt, double dt_scalar, double* Q, int* status, int* nsteps,
+                long long* counters, void* stream) {
   if (!c || ncells < 0 || !Y || !T || ld < ncells) return LSG_ERR_ARG;
   if (nspecies != c->mech->host.layout.nc) return LSG_ERR_ARG;
   if (!(p > 0.)) return LSG_ERR_ARG;
@@ -635,11 +640,13 @@ int lsg_reaction_step_device(lsg_ctx* c, int ncells, int nspecies, double* Y, lo
   a.status = status;
   a.nsteps = nsteps;
   a.counters = counters;
+  a.rho = rho;
   return launch_step(c, a, (cudaStream_t)stream);
 }
 
-int lsg_reaction_step(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, double* T, double p, double t0,
-                      const double* dt, double dt_scalar, double* Q, int* status, int* nsteps) {
+// The host-array step of both reactors: arrays are staged through the context's device buffers.
+int host_step(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, double* T, double p, const double* rho,
+              double t0, const double* dt, double dt_scalar, double* Q, int* status, int* nsteps) {
   if (!c || ncells < 0 || !Ys || !T) return LSG_ERR_ARG;
   if (nspecies != c->mech->host.layout.nc) return LSG_ERR_ARG;
   for (int i = 0; i < nspecies; ++i) if (!Ys[i]) return LSG_ERR_ARG;
@@ -654,6 +661,7 @@ int lsg_reaction_step(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, d
     if (cudaMemcpyAsync(c->dY + (size_t)i * c->cap, Ys[i], nb, cudaMemcpyHostToDevice, s) != cudaSuccess) return LSG_ERR_CUDA;
   if (cudaMemcpyAsync(c->dT, T, nb, cudaMemcpyHostToDevice, s) != cudaSuccess) return LSG_ERR_CUDA;
   if (dt && cudaMemcpyAsync(c->ddt, dt, nb, cudaMemcpyHostToDevice, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (rho && cudaMemcpyAsync(c->drho, rho, nb, cudaMemcpyHostToDevice, s) != cudaSuccess) return LSG_ERR_CUDA;
   StepArgs a{};
   a.ncells = ncells;
   a.ld = c->cap;
@@ -666,6 +674,7 @@ int lsg_reaction_step(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, d
   a.Q = Q ? c->dQ : nullptr;
   a.status = status ? c->dstatus : nullptr;
   a.nsteps = nsteps ? c->dnsteps : nullptr;
+  a.rho = rho ? c->drho : nullptr;
   r = launch_step(c, a, s);
   if (r != LSG_OK) return r;
   for (int i = 0; i < nspecies; ++i)
@@ -679,6 +688,33 @@ int lsg_reaction_step(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, d
   if (cudaStreamSynchronize(s) != cudaSuccess) return LSG_ERR_CUDA;
   int flags = 0;
   return lsg_ctx_check(c, &flags);
+}
+}  // namespace
+
+int lsg_reaction_step_device(lsg_ctx* c, int ncells, int nspecies, double* Y, long ld, double* T, double p,
+                             double t0, const double* dt, double dt_scalar, double* Q, int* status, int* nsteps,
+                             long long* counters, void* stream) {
+  return device_step(c, ncells, nspecies, Y, ld, T, p, nullptr, t0, dt, dt_scalar, Q, status, nsteps, counters,
+                     stream);
+}
+
+int lsg_reaction_step_cv_device(lsg_ctx* c, int ncells, int nspecies, double* Y, long ld, double* T,
+                                const double* rho, double t0, const double* dt, double dt_scalar, double* Q,
+                                int* status, int* nsteps, long long* counters, void* stream) {
+  if (!rho) return LSG_ERR_ARG;
+  return device_step(c, ncells, nspecies, Y, ld, T, 101325., rho, t0, dt, dt_scalar, Q, status, nsteps, counters,
+                     stream);
+}
+
+int lsg_reaction_step(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, double* T, double p, double t0,
+                      const double* dt, double dt_scalar, double* Q, int* status, int* nsteps) {
+  return host_step(c, ncells, nspecies, Ys, T, p, nullptr, t0, dt, dt_scalar, Q, status, nsteps);
+}
+
+int lsg_reaction_step_cv(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, double* T, const double* rho,
+                         double t0, const double* dt, double dt_scalar, double* Q, int* status, int* nsteps) {
+  if (!rho) return LSG_ERR_ARG;
+  return host_step(c, ncells, nspecies, Ys, T, 101325., rho, t0, dt, dt_scalar, Q, status, nsteps);
 }
 
 int lsg_reaction_step_device_noalloc(const lsg_mech* m, const lsg_options* opt, int ncells, int nspecies,

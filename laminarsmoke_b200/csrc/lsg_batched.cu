@@ -100,12 +100,14 @@ __device__ __forceinline__ double hi_bound(int k, int NC, double ymaxT) { return
 // Thread-serial RHS of the constant-pressure reactor
 // (BatchReactorHomogeneousConstantPressure.H:175-223).  y: this lane's input
 // vector (stride ns) with component pj replaced by pval when pj >= 0; f: output.
-// C,H,S,R scratch in shared memory, [species][lane].  Returns QR.
+// C,H,S,R scratch in shared memory, [species][lane].  Returns QR.  rho0 > 0
+// selects the constant-volume reactor of that density
+// (BatchReactorHomogeneousConstantVolume.H:148-199).
 // ---------------------------------------------------------------------------
 __device__ __noinline__ double rhs_lane(const MechLayout* __restrict__ Lp, const double* __restrict__ Md,
                                         const int* __restrict__ Mi, double* __restrict__ scratch,
                                         const double* __restrict__ y, long ns, int pj, double pval,
-                                        double* __restrict__ f, double P0, int energy) {
+                                        double* __restrict__ f, double P0, int energy, double rho0) {
   const MechLayout& L = *Lp;
   const MechView M{Md, Mi};
   const int NC = L.nc, NR = L.nr;
@@ -125,8 +127,9 @@ __device__ __noinline__ double rhs_lane(const MechLayout* __restrict__ Lp, const
     u += yi / MW[i];
   }
   const double MWmix = 1. / u;
-  const double cTot = P0 / kRgas / T;
-  const double rho = cTot * MWmix;
+  const bool cv = rho0 > 0.;
+  const double cTot = cv ? rho0 / MWmix : P0 / kRgas / T;
+  const double rho = cv ? rho0 : cTot * MWmix;
   const double* TM = M.D(L.t_mid);
   const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, uT = 1. / T;
   const double logT = log(T);
@@ -269,9 +272,16 @@ __device__ __noinline__ double rhs_lane(const MechLayout* __restrict__ Lp, const
   double dT = 0.;
   if (energy) {
     cpm *= kRgas;
-    const double CpMixMass = cpm / MWmix;
     QR = -dsum * kRgas * T;
-    dT = QR / (rho * CpMixMass);
+    if (cv) {
+      const double CvMixMass = (cpm - kRgas) / MWmix;
+      double sumR = 0.;
+      for (int i = 0; i < NC; ++i) sumR += SC_(R, i);
+      dT = (QR + kRgas * T * sumR) / (rho0 * CvMixMass);
+    } else {
+      const double CpMixMass = cpm / MWmix;
+      dT = QR / (rho * CpMixMass);
+    }
   }
   f[(long)NC * ns] = dT;
 #undef SC_
@@ -587,7 +597,7 @@ batched_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem, StepO
         case PH_STAB_ERR: src = pz; break;
         default: break;   // PH_INIT, PH_NEWTON, PH_FINAL evaluate at va
       }
-      QR = rhs_lane(&sL, Md, Mi, scratch, src, ns, pj, pval, dst, P0, o.energy);
+      QR = rhs_lane(&sL, Md, Mi, scratch, src, ns, pj, pval, dst, P0, o.energy, a.rho ? a.rho[cell] : 0.);
       if (phase == PH_JAC) ++cnt[CNT_JAC_RHS];
       else ++cnt[CNT_RHS];
     }

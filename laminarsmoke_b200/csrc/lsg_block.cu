@@ -99,7 +99,7 @@ template <int BT>
 __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, const BlockShared& W,
                                          double* __restrict__ karr, double* __restrict__ ukeq,
                                          double* __restrict__ kinf, double* __restrict__ logf, double yl, double T,
-                                         double P0, int energy) {
+                                         double P0, int energy, double rho0) {
   const int tid = threadIdx.x;
   const int NC = L.nc, NR = L.nr;
   const double* MW = M.D(L.mw);
@@ -108,9 +108,10 @@ __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, 
   const double MWmix = 1. / u;
   double xl = 0.;
   if (tid < NC) { xl = MWmix * yl; xl = xl / mwl; }
-  const double cTot = P0 / kRgas / T;
+  const bool cv = rho0 > 0.;   // constant volume (BatchReactorHomogeneousConstantVolume.H:148-199)
+  const double cTot = cv ? rho0 / MWmix : P0 / kRgas / T;
   const double cl = cTot * xl;
-  const double rho = cTot * MWmix;
+  const double rho = cv ? rho0 : cTot * MWmix;
   const double* TM = M.D(L.t_mid);
   const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, uT = 1. / T;
   double hl = 0.;
@@ -287,10 +288,16 @@ __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, 
       cpl = A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4];
     }
     const double cpm = bsum<BT>(cpl * xl, W.red) * kRgas;
-    const double CpMixMass = cpm / MWmix;
     const double d = bsum<BT>(Rl * hl, W.red);
     QR = -d * kRgas * T;
-    if (tid == NC) dyl = QR / (rho * CpMixMass);
+    if (cv) {
+      const double CvMixMass = (cpm - kRgas) / MWmix;
+      const double sumR = bsum<BT>(Rl, W.red);
+      if (tid == NC) dyl = (QR + kRgas * T * sumR) / (rho0 * CvMixMass);
+    } else {
+      const double CpMixMass = cpm / MWmix;
+      if (tid == NC) dyl = QR / (rho * CpMixMass);
+    }
   } else if (tid == NC) {
     dyl = 0.;
   }
@@ -321,6 +328,7 @@ struct GearBlock {
   double* kinf;
   double* logf;
   double P0;
+  double rho0;   // > 0: constant-volume reactor of this density
   int energy;
   int tid, ne;
   bool active;
@@ -345,7 +353,7 @@ struct GearBlock {
   __device__ double rhs(double yl) {
     ++cnt[CNT_RHS];
     const double T = bcast(yl, ne - 1, W.slot);
-    return rhs_block<BT>(*L, M, W, karr, ukeq, kinf, logf, yl, T, P0, energy);
+    return rhs_block<BT>(*L, M, W, karr, ukeq, kinf, logf, yl, T, P0, energy, rho0);
   }
 
   __device__ double error_control(double w) {   // OpenSMOKEUtilities.hpp:689-701
@@ -384,7 +392,7 @@ struct GearBlock {
       double yp = yl;
       if (tid == j) yp += hJ;
       const double T = bcast(yp, n - 1, W.slot);
-      const double aux = rhs_block<BT>(*L, M, W, karr, ukeq, kinf, logf, yp, T, P0, energy);
+      const double aux = rhs_block<BT>(*L, M, W, karr, ukeq, kinf, logf, yp, T, P0, energy, rho0);
       ++cnt[CNT_JAC_RHS];
       const double hInv = 1. / hJ;
       if (active) J[(long)j * n + tid] = hInv * (aux - fl);
@@ -914,6 +922,7 @@ __global__ void __launch_bounds__(BT) block_kernel(MechLayout L, const unsigned 
       g.kinf = g.ukeq + L.nr;
       g.logf = g.kinf + (L.n_fo > 0 ? L.n_fo : 1);
       g.P0 = a.p;
+      g.rho0 = a.rho ? a.rho[cell] : 0.;
       g.energy = o.energy;
       g.tid = tid;
       g.ne = ne;
@@ -990,7 +999,7 @@ __global__ void __launch_bounds__(BT) rhs_block_kernel(MechLayout L, const unsig
     if (tid == 0) { W.slot[1] = 0.; W.slot[2] = 0.; }
     const double yl = tid <= NC ? y[(size_t)tid * ld + cell] : 0.;
     const double T = bcast(yl, NC, W.slot);
-    const double d = rhs_block<BT>(L, M, W, karr, ukeq, kinf, logf, yl, T, p, energy);
+    const double d = rhs_block<BT>(L, M, W, karr, ukeq, kinf, logf, yl, T, p, energy, 0.);
     if (tid <= NC) dy[(size_t)tid * ld + cell] = d;
     if (tid == 0 && qr) qr[cell] = W.slot[2];
   }

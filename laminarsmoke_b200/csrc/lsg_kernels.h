@@ -40,6 +40,7 @@ struct StepArgs {
   int* status;        // optional
   int* nsteps;        // optional
   long long* counters;  // optional [ncells][NCNT]
+  const double* rho;  // constant-volume reactor: per-cell density [kg/m3]; nullptr: constant pressure
 };
 
 size_t plain_smem_bytes(const MechLayout& L);

@@ -26,7 +26,10 @@ plain_warp_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, Ste
   double* wsbase = (double*)(smem + ((L.bytes + 15u) & ~15u)) + (size_t)warp * warp_ws_doubles(L);
   {
     WarpWS W0 = carve_ws(wsbase, L);
-    if (lane == 0) { W0.SC[0] = 0.; W0.SC[1] = 0.; W0.SC[2] = a.p; W0.SC[3] = o.energy ? 1. : 0.; }
+    if (lane == 0) {
+      W0.SC[0] = 0.; W0.SC[1] = 0.; W0.SC[2] = a.p; W0.SC[3] = o.energy ? 1. : 0.;
+      W0.SC[4] = a.rho ? a.rho[cell] : 0.;
+    }
     __syncwarp();
   }
 
@@ -106,7 +109,7 @@ rhs_warp_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, long 
   if (cell >= ncells) return;
   double* wsbase = (double*)(smem + ((L.bytes + 15u) & ~15u)) + (size_t)warp * warp_ws_doubles(L);
   WarpWS W = carve_ws(wsbase, L);
-  if (lane == 0) { W.SC[0] = 0.; W.SC[1] = 0.; W.SC[2] = p; W.SC[3] = energy ? 1. : 0.; }
+  if (lane == 0) { W.SC[0] = 0.; W.SC[1] = 0.; W.SC[2] = p; W.SC[3] = energy ? 1. : 0.; W.SC[4] = 0.; }
   __syncwarp();
   const int NC = L.nc;
   const double yl = lane <= NC ? y[(size_t)lane * ld + cell] : 0.;

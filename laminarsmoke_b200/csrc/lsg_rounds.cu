@@ -119,12 +119,15 @@ __device__ __forceinline__ double hi_b(int k, int NC, double ymaxT) { return k <
 // (BatchReactorHomogeneousConstantPressure.H:175-223).  y: this cell's input
 // vector (stride ns) with component pj replaced by pval when pj >= 0; f: output.
 // C (concentrations), G (h/RT - s/R) and R (formation rates) scratch in shared
-// memory, [species][thread].  f has stride fs.  Returns QR.
+// memory, [species][thread].  f has stride fs.  Returns QR.  rho0 > 0 selects
+// the constant-volume reactor of that density (BatchReactorHomogeneousConstant
+// Volume.H:148-199): cTot = rho0 / MW, dY/dt = MW R / rho0 and
+// dT/dt = (QR + R T sum R_i) / (rho0 cv).
 // ---------------------------------------------------------------------------
 __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const double* __restrict__ Md,
                                         const int* __restrict__ Mi, double* __restrict__ scratch,
                                         const double* __restrict__ y, long ns, int pj, double pval,
-                                        double* __restrict__ f, long fs, double P0, int energy) {
+                                        double* __restrict__ f, long fs, double P0, int energy, double rho0) {
   const MechLayout& L = *Lp;
   const MechView M{Md, Mi};
   const int NC = L.nc, NR = L.nr;
@@ -143,8 +146,9 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
     u += yi / MW[i];
   }
   const double MWmix = 1. / u;
-  const double cTot = P0 / kRgas / T;
-  const double rho = cTot * MWmix;
+  const bool cv = rho0 > 0.;
+  const double cTot = cv ? rho0 / MWmix : P0 / kRgas / T;
+  const double rho = cv ? rho0 : cTot * MWmix;
   const double* TM = M.D(L.t_mid);
   const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, uT = 1. / T;
   const double logT = log(T);
@@ -279,9 +283,16 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
   double dT = 0.;
   if (energy) {
     cpm *= kRgas;
-    const double CpMixMass = cpm / MWmix;
     QR = -dsum * kRgas * T;
-    dT = QR / (rho * CpMixMass);
+    if (cv) {
+      const double CvMixMass = (cpm - kRgas) / MWmix;
+      double sumR = 0.;
+      for (int i = 0; i < NC; ++i) sumR += SC_(R, i);
+      dT = (QR + kRgas * T * sumR) / (rho0 * CvMixMass);
+    } else {
+      const double CpMixMass = cpm / MWmix;
+      dT = QR / (rho * CpMixMass);
+    }
   }
   f[(long)NC * fs] = dT;
 #undef SC_
@@ -482,6 +493,7 @@ struct RoundBufs {
   int* rq;          // RHS work counter: warps take the next 32 list entries from it
   int* njac;        // [2] leading Jacobian-bin entries of each list
   double* fsc;      // column scratch of the RHS threads, n words x (RHS grid threads)
+  const double* rho;   // per-cell density of the constant-volume reactor, or nullptr (constant pressure)
 };
 
 }  // namespace
@@ -552,7 +564,7 @@ __global__ void __launch_bounds__(kAT) rounds_init_kernel(int NC, StepOptions o,
 // keeps the register budget of its single-evaluation path.
 __device__ __noinline__ void jacobian_column(const MechLayout* L, const double* Md, const int* Mi, double* scratch,
                                              double* R, const RecLayout RL, int j, double P0, int energy,
-                                             double y_max_T, double* fp, long fs) {
+                                             double y_max_T, double* fp, long fs, double rho0) {
   const int n = L->nc + 1;
   const double* vb = R + RL.ovb;
   const double yh = vb[j], ej = R[RL.oeps + j];
@@ -565,7 +577,7 @@ __device__ __noinline__ void jacobian_column(const MechLayout* L, const double* 
   const bool last = j == n - 1;
   double* f = last ? R + RL.of : fp;
   const long ffs = last ? 1 : fs;
-  const double q = rhs_cell(L, Md, Mi, scratch, vb, 1, j, yh + hJ, f, ffs, P0, energy);
+  const double q = rhs_cell(L, Md, Mi, scratch, vb, 1, j, yh + hJ, f, ffs, P0, energy, rho0);
   const double* f0 = R + RL.of0;
   float* Jg = (float*)(R + RL.ojac);
   const double hInv = 1. / hJ;
@@ -617,8 +629,10 @@ __global__ void __launch_bounds__(kRT, 4) rounds_rhs_kernel(MechLayout Lp, const
     if (item >= nitems) continue;
     if (item < njac * n) {
       const int e = item / n;
-      double* R = B.rec + (long)act[e] * RL.RS;
-      jacobian_column(&sL, Md, Mi, scratch, R, RL, item - e * n, P0, energy, y_max_T, fp, fs);
+      const int cell = act[e];
+      double* R = B.rec + (long)cell * RL.RS;
+      jacobian_column(&sL, Md, Mi, scratch, R, RL, item - e * n, P0, energy, y_max_T, fp, fs,
+                      B.rho ? B.rho[cell] : 0.);
       continue;
     }
     const int cell = act[njac + (item - njac * n)];
@@ -627,7 +641,8 @@ __global__ void __launch_bounds__(kRT, 4) rounds_rhs_kernel(MechLayout Lp, const
     const int ph = RI[I_PHASE];
     if (!rhs_phase(ph)) continue;
     if (ph == PH_JAC) {   // a Jacobian outside the list head (not produced by the compaction): serially
-      for (int j = 0; j < n; ++j) jacobian_column(&sL, Md, Mi, scratch, R, RL, j, P0, energy, y_max_T, fp, fs);
+      for (int j = 0; j < n; ++j)
+        jacobian_column(&sL, Md, Mi, scratch, R, RL, j, P0, energy, y_max_T, fp, fs, B.rho ? B.rho[cell] : 0.);
       continue;
     }
     const double* src = R + RL.ova;
@@ -640,7 +655,7 @@ __global__ void __launch_bounds__(kRT, 4) rounds_rhs_kernel(MechLayout Lp, const
     } else if (ph == PH_STAB_CONV || ph == PH_STAB_ERR) {
       src = R + RL.oz;
     }
-    R[D_QR] = rhs_cell(&sL, Md, Mi, scratch, src, 1, pj, pval, dst, 1, P0, energy);
+    R[D_QR] = rhs_cell(&sL, Md, Mi, scratch, src, 1, pj, pval, dst, 1, P0, energy, B.rho ? B.rho[cell] : 0.);
     RI[I_CNT0 + CNT_RHS] += 1;
   }
 }
@@ -1412,6 +1427,7 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
   if (n > 32 || a.ncells > cap || a.ncells <= 0) return cudaErrorInvalidValue;
   RoundBufs B = carve(L, state, cap, P.lu64);
   B.fsc = (double*)((char*)state + rounds_bytes(L, cap, P.lu64));   // rounds_cache_bytes(L, P) after the rest
+  B.rho = a.rho;
   kt->begin(KT_INIT, stream);
   rounds_init_kernel<<<P.g_init, kAT, 0, stream>>>(L.nc, o, a, B);
   kt->end(stream);

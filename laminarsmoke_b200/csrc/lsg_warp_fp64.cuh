@@ -41,13 +41,13 @@ struct WarpWS {
   double* KINF;   // [NFO] k_inf (cache)
   double* LOGF;   // [NFO] log10 Fcent (Troe) / SRI factor (cache)
   int* PIV;       // [32]
-  double* SC;     // [4] scalars: cached kinetic T, QR of the last call, P0, energy flag
+  double* SC;     // [6] scalars: cached kinetic T, QR of the last call, P0, energy flag, rho0 (> 0: constant volume)
 };
 
 __host__ __device__ inline int warp_ws_doubles(const MechLayout& L) {
   const int n = L.nc + 1;
   auto even = [](int x) { return (x + 1) & ~1; };
-  return 8 * 32 * 2 + even(n * (n + 1)) * 2 + 32 * 3 + even(L.nr) * 3 + even(L.n_fo > 0 ? L.n_fo : 1) * 2 + 16 + 4;
+  return 8 * 32 * 2 + even(n * (n + 1)) * 2 + 32 * 3 + even(L.nr) * 3 + even(L.n_fo > 0 ? L.n_fo : 1) * 2 + 16 + 6;
 }
 
 __device__ __forceinline__ WarpWS carve_ws(double* base, const MechLayout& L) {
@@ -103,6 +103,8 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
   WarpWS W = carve_ws(ws, L);
   const double P0 = W.SC[2];
   const bool energy = W.SC[3] != 0.;
+  const double rho0 = W.SC[4];   // constant volume when > 0 (BatchReactorHomogeneousConstantVolume.H:148-199)
+  const bool cv = rho0 > 0.;
   const int lane = threadIdx.x & 31;
   const int NC = L.nc, NR = L.nr;
   const double* MW = M.D(L.mw);
@@ -113,9 +115,9 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
   const double MWmix = 1. / u;
   double xl = 0.;
   if (lane < NC) { xl = MWmix * yl; xl = xl / mwl; }
-  const double cTot = P0 / kRgas / T;
+  const double cTot = cv ? rho0 / MWmix : P0 / kRgas / T;
   const double cl = cTot * xl;
-  const double rho = cTot * MWmix;
+  const double rho = cv ? rho0 : cTot * MWmix;
   const double* TM = M.D(L.t_mid);
   const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, uT = 1. / T;
   double hl = 0.;
@@ -306,10 +308,16 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
     }
     double cpm = seq_sum(cpl * xl, NC);
     cpm *= kRgas;
-    const double CpMixMass = cpm / MWmix;
     const double d = seq_sum(Rl * hl, NC);
     QR = -d * kRgas * T;
-    if (lane == NC) dyl = QR / (rho * CpMixMass);
+    if (cv) {
+      const double CvMixMass = (cpm - kRgas) / MWmix;
+      const double sumR = seq_sum(Rl, NC);
+      if (lane == NC) dyl = (QR + kRgas * T * sumR) / (rho0 * CvMixMass);
+    } else {
+      const double CpMixMass = cpm / MWmix;
+      if (lane == NC) dyl = QR / (rho * CpMixMass);
+    }
   } else if (lane == NC) {
     dyl = 0.;
   }

@@ -48,6 +48,7 @@ EXPORTS = (
     "lsg_strerror", "lsg_abi_version", "lsg_ctx_stream", "lsg_ctx_launches",
     "lsg_reaction_step_device_noalloc", "lsg_ctx_kernel_times", "lsg_ctx_tuning",
     "lsg_compact_sources_device", "lsg_formation_rates_device",
+    "lsg_reaction_step_cv", "lsg_reaction_step_cv_device",
 )
 
 _lib = None
@@ -85,6 +86,8 @@ def lib():
     L.lsg_ctx_tuning.argtypes = [vp, C.POINTER(i), C.POINTER(i), vp]
     L.lsg_ctx_launches.argtypes = [vp]
     L.lsg_ctx_launches.restype = C.c_longlong
+    L.lsg_reaction_step_cv.argtypes = [vp, i, i, C.POINTER(vp), vp, vp, d, vp, d, vp, vp, vp]
+    L.lsg_reaction_step_cv_device.argtypes = [vp, i, i, vp, l, vp, vp, d, vp, d, vp, vp, vp, vp, vp]
     L.lsg_compact_sources_device.argtypes = [vp, i, i, vp, vp, vp, vp, l, d, vp, d, vp, vp, vp]
     L.lsg_formation_rates_device.argtypes = [vp, i, i, vp, vp, l, d, vp, l, vp]
     _lib = L
@@ -197,6 +200,33 @@ class ReactionStep:
                "lsg_reaction_step")
         return Q, st, ns
 
+    def step_cv(self, Y_species: np.ndarray, T: np.ndarray, rho: np.ndarray, dt, t0: float = 0.0,
+                want_q: bool = True):
+        """Constant-volume reactor (lsg_reaction_step_cv): as step(), with the
+        per-cell density rho [ncells] instead of a pressure."""
+        Y = Y_species
+        if Y.dtype != np.float64 or not Y.flags.c_contiguous or T.dtype != np.float64:
+            raise TypeError("Y_species and T must be C-contiguous float64")
+        nc, n = Y.shape
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        if rho.shape != (n,):
+            raise ValueError("rho must have one value per cell")
+        ptrs = (C.c_void_p * nc)(*[Y[i].ctypes.data for i in range(nc)])
+        dt_arr = None
+        dt_s = 0.0
+        if np.ndim(dt) == 0:
+            dt_s = float(dt)
+        else:
+            dt_arr = np.ascontiguousarray(dt, dtype=np.float64)
+        Q = np.zeros(n) if want_q else None
+        st = np.zeros(n, dtype=np.int32)
+        ns = np.zeros(n, dtype=np.int32)
+        _check(lib().lsg_reaction_step_cv(self.h, n, nc, ptrs, T.ctypes.data, rho.ctypes.data, t0,
+                                          None if dt_arr is None else dt_arr.ctypes.data, dt_s,
+                                          None if Q is None else Q.ctypes.data, st.ctypes.data, ns.ctypes.data),
+               "lsg_reaction_step_cv")
+        return Q, st, ns
+
     # ---- device arrays (torch tensors) ----
     def step_device(self, Y, T, dt=1e-5, p: float = 101325.0, t0: float = 0.0, Q=None, status=None,
                     nsteps=None, counters=None, stream=None):
@@ -210,6 +240,19 @@ class ReactionStep:
             None if Q is None else Q.data_ptr(), None if status is None else status.data_ptr(),
             None if nsteps is None else nsteps.data_ptr(), None if counters is None else counters.data_ptr(),
             _stream_handle(stream)), "lsg_reaction_step_device")
+
+    def step_cv_device(self, Y, T, rho, dt=1e-5, t0: float = 0.0, Q=None, status=None, nsteps=None,
+                       counters=None, stream=None):
+        """Constant-volume reactor on device arrays (lsg_reaction_step_cv_device)."""
+        _require_layout(Y, T, rho, Q, status, nsteps, counters, dt if hasattr(dt, "data_ptr") else None)
+        nc, ld = Y.shape
+        n = T.shape[0]
+        dtp, dts = (None, float(dt)) if not hasattr(dt, "data_ptr") else (dt.data_ptr(), 0.0)
+        _check(lib().lsg_reaction_step_cv_device(
+            self.h, n, nc, Y.data_ptr(), ld, T.data_ptr(), rho.data_ptr(), t0, dtp, dts,
+            None if Q is None else Q.data_ptr(), None if status is None else status.data_ptr(),
+            None if nsteps is None else nsteps.data_ptr(), None if counters is None else counters.data_ptr(),
+            _stream_handle(stream)), "lsg_reaction_step_cv_device")
 
     def step_sequence_device(self, Y, T, dt, nsteps: int, p: float = 101325.0, t0: float = 0.0, Q=None,
                              status=None, stream=None):

@@ -93,6 +93,7 @@ struct Reactor {
   const Mech& m;
   int NC, NR;
   double P0 = 101325.;
+  double rho0 = 0.;   // > 0: constant-volume reactor of this density (BatchReactorHomogeneousConstantVolume.H)
   bool energy = true;
   double QR = 0.;
   // thermo map
@@ -317,9 +318,11 @@ struct Reactor {
     const double MWmix = 1. / u;
     for (int i = 0; i < NC; ++i) x[i] = MWmix * y[i];
     for (int i = 0; i < NC; ++i) x[i] = x[i] / MW[i];
-    const double cTot = P0 / R_J_KMOL / T;
+    // constant volume (BatchReactorHomogeneousConstantVolume.H:148-199): cTot_ = rho0_ / MW_
+    const bool cv = rho0 > 0.;
+    const double cTot = cv ? rho0 / MWmix : P0 / R_J_KMOL / T;
     for (int i = 0; i < NC; ++i) c[i] = cTot * x[i];
-    const double rho = cTot * MWmix;
+    const double rho = cv ? rho0 : cTot * MWmix;
     h_over_RT(T);   // species h/RT at T: used by the reaction enthalpies and by QR
     kin_set_T(T);
     reaction_rates();
@@ -331,11 +334,19 @@ struct Reactor {
       double cpm = 0.;
       for (int i = 0; i < NC; ++i) cpm += cp[i] * x[i];
       cpm *= R_J_KMOL;
-      const double CpMixMass = cpm / MWmix;
       double d = 0.;
       for (int i = 0; i < NC; ++i) d += R[i] * h[i];
       QR = -d * R_J_KMOL * T;
-      dy[NC] = QR / (rho * CpMixMass);
+      if (cv) {
+        // CvMixMass_ = (CpMixMolar - R) / MW_; dT/dt = (QR_ + R T sum R_i) / (rho0_ CvMixMass_)
+        const double CvMixMass = (cpm - R_J_KMOL) / MWmix;
+        double sumR = 0.;
+        for (int i = 0; i < NC; ++i) sumR += R[i];
+        dy[NC] = (QR + R_J_KMOL * T * sumR) / (rho0 * CvMixMass);
+      } else {
+        const double CpMixMass = cpm / MWmix;
+        dy[NC] = QR / (rho * CpMixMass);
+      }
     }
   }
 };
@@ -945,7 +956,7 @@ int orc_fd_jacobian(void* mech, double P, const double* y, double h, double rtol
 // and solvers/laminarSMOKE/utilities.H:153-200 (normalizeMassFractions).
 int orc_reaction_step(void* mech, const orc_options* o, int ncells, double* Y, double* T, double p,
                       double t0, const double* dt, double dt_scalar, double* Q, int* status,
-                      long long* counters, int nthreads) {
+                      long long* counters, int nthreads, const double* rho) {
   const orc::Mech& m = *(const orc::Mech*)mech;
   const int NC = m.nc;
   const unsigned NEQ = NC + 1;
@@ -972,6 +983,7 @@ int orc_reaction_step(void* mech, const orc_options* o, int ncells, double* Y, d
         for (int i = 0; i < NC; ++i) { if (y0[i] < 0.) y0[i] = 0.; sum += y0[i]; }
         for (int i = 0; i < NC; ++i) y0[i] /= sum;
         reactor.P0 = p;
+        reactor.rho0 = rho ? rho[cell] : 0.;   // chemistry_DI.H:168-203: SetReactor(V, P, rhoCells[celli])
         reactor.energy = o->energy != 0;
         if (!reactor.energy) reactor.QR = 0.;
         g.set_initial_conditions(t0, y0.data());

@@ -48,7 +48,7 @@ def lib():
                                       C.c_double, C.c_double, C.c_void_p]
         L.orc_reaction_step.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.c_int, C.c_void_p, C.c_void_p,
                                         C.c_double, C.c_double, C.c_void_p, C.c_double, C.c_void_p,
-                                        C.c_void_p, C.c_void_p, C.c_int]
+                                        C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         L.orc_reaction_step.restype = C.c_int
         L.orc_compact_sources.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_double, C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]
@@ -112,8 +112,9 @@ class OracleMechanism:
 
     def reaction_step(self, Y, T, dt, p=101325.0, t0=0.0, rtol=1e-7, atol=1e-12, tmin_chem=0.0,
                       max_steps=500000, energy=True, alfa2_4=0.8, alfa2_5=0.8, maximum_order=5,
-                      sequential_state=False, nthreads=0, y_min_T=200.0, y_max_T=6000.0):
-        """Cell-major Y[ncells, NC], T[ncells]; returns (Y, T, Q, status, counters)."""
+                      sequential_state=False, nthreads=0, y_min_T=200.0, y_max_T=6000.0, rho=None):
+        """Cell-major Y[ncells, NC], T[ncells]; returns (Y, T, Q, status, counters).  rho [ncells]:
+        constant-volume reactor of those densities (p is then unused)."""
         Y = np.array(Y, dtype=np.float64, order="C", copy=True)
         T = np.array(T, dtype=np.float64, copy=True)
         n = T.size
@@ -129,5 +130,6 @@ class OracleMechanism:
         o = OrcOptions(rtol, atol, tmin_chem, y_min_T, y_max_T, max_steps, 0, int(energy),
                        alfa2_4, alfa2_5, maximum_order, int(sequential_state))
         lib().orc_reaction_step(self.h, C.byref(o), n, _ptr(Y), _ptr(T), p, t0, _ptr(dt_arr), dt_s,
-                                _ptr(Q), _ptr(st), _ptr(cnt), nthreads)
+                                _ptr(Q), _ptr(st), _ptr(cnt), nthreads,
+                                _ptr(None if rho is None else np.ascontiguousarray(rho, dtype=np.float64)))
         return Y, T, Q, st, cnt

@@ -116,3 +116,36 @@ def test_saturated_order_state_changes_results(h2co, oracle_h2co):
     a = oracle_h2co.reaction_step(Y, T, 1e-4, nthreads=2)
     b = oracle_h2co.reaction_step(Y, T, 1e-4, nthreads=2, alfa2_4=0.0, alfa2_5=0.0, maximum_order=4)
     assert not np.array_equal(a[4][:, 0], b[4][:, 0])
+
+
+def _umix(A, species, Yc, Tc):
+    """Mixture internal energy per unit mass, u = sum_i Y_i (h_i - R T) / MW_i."""
+    raw = A["nasa_raw"].reshape(-1, 18)
+    out = 0.0
+    for i in range(len(species)):
+        a = raw[i, 0:7] if Tc > A["t_mid"][i] else raw[i, 7:14]
+        h_rt = a[0] + a[1] / 2 * Tc + a[2] / 3 * Tc ** 2 + a[3] / 4 * Tc ** 3 + a[4] / 5 * Tc ** 4 + a[5] / Tc
+        out += Yc[i] / A["mw"][i] * (h_rt - 1.0) * 8314.4621 * Tc
+    return out
+
+
+def test_constant_volume_step_conserves_internal_energy(h2co, oracle_h2co):
+    """Constant-volume reactor (BatchReactorHomogeneousConstantVolume.H:148-199): the mixture internal
+    energy of the closed cell is invariant, the enthalpy is not, and T rises more than at constant p."""
+    _, species, A = h2co
+    Y, T = _mix(h2co, 64)
+    Yn = Y / Y.sum(axis=1, keepdims=True)
+    rho = 101325.0 * (1.0 / (Yn / A["mw"]).sum(axis=1)) / 8314.4621 / T
+    Yv, Tv, Q, st, cnt = oracle_h2co.reaction_step(Y, T, 1e-4, nthreads=4, rho=rho)
+    Yp, Tp, _, _, _ = oracle_h2co.reaction_step(Y, T, 1e-4, nthreads=4)
+    assert np.all(st == 2)
+    np.testing.assert_allclose(Yv.sum(axis=1), 1.0, rtol=1e-12)
+    hot = 0
+    for k in range(0, 64, 2):
+        u0, u1 = _umix(A, species, Yn[k], T[k]), _umix(A, species, Yv[k], Tv[k])
+        assert abs(u1 - u0) <= 1e-4 * (abs(u0) + 1e5)
+        if Tp[k] - T[k] > 50.0:
+            hot += 1
+            assert Tv[k] - T[k] > Tp[k] - T[k]
+    assert hot > 0
+

@@ -241,6 +241,23 @@ int lsg_compact_sources_device(lsg_ctx* ctx, int ncells, int nspecies, const dou
 int lsg_formation_rates_device(lsg_ctx* ctx, int ncells, int nspecies, const double* Y_dev, const double* T_dev,
                                long ld, double p, double* out_dev, long ld_out, void* stream);
 
+/* ---- steady solvers: linearised chemical source terms ---------------------
+ * What solvers/laminarSMOKE/steady/jacobianEvaluation.H:60-92 computes per
+ * cell with linearModel::reactionSourceTerms and ::reactionJacobian
+ * (steady/linearModel.H:92-170): the source S_i = R_i MW_i [kg/m3/s] of each
+ * species and S_T = QR [W/m3] at omega = max(Y, 0) and T, and the diagonal
+ * of its Jacobian J_k = dS_k/dy_k by one forward difference per component
+ * (the reference's increment; a perturbed mass fraction is clipped at zero).
+ * Outputs, [nspecies + 1][lds] device arrays: S_implicit_k = J_k and
+ * S_explicit_k = S_k - J_k y_k, the sourceImplicit / sourceExplicit fields.
+ * Pressure per cell (p_dev, the steady solver's p field) or p_scalar when
+ * p_dev is NULL.  Uses context-owned scratch of 3 (nspecies + 1) ncells
+ * doubles.  LSG_ERR_UNSUPPORTED when the mechanism's tables and the per-thread
+ * work arrays do not fit one block's shared memory (about 65 species). */
+int lsg_steady_sources_device(lsg_ctx* ctx, int ncells, int nspecies, const double* Y_dev, const double* T_dev,
+                              long ld, const double* p_dev, double p_scalar, double* S_implicit_dev,
+                              double* S_explicit_dev, long lds, void* stream);
+
 const char* lsg_strerror(int code);
 int lsg_abi_version(void);
 

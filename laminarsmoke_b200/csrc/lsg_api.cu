@@ -62,7 +62,7 @@ struct lsg_ctx {
   double* tune_buf = nullptr;   // sample cells: pristine copy and work copy
   long tune_cap = 0;
   int rplan_w = -1;             // lane-group width the round plan was prepared for
-  // formation-rate output: gathered states and their right-hand sides
+  // formation-rate output and steady-solver sources: gathered states and their right-hand sides
   double* frs = nullptr;
   long frs_cap = 0;             // doubles
 };
@@ -780,6 +780,34 @@ int lsg_compact_sources_device(lsg_ctx* c, int ncells, int nspecies, const doubl
   if (launch_compact_sources(c->mech->host.layout, c->mech->d_buf, ncells, Y0, T0, Yf, Tf, ld, p, dt, dt_scalar,
                              c->opt.energy, RR, RT, sm_count(c), (cudaStream_t)stream) != cudaSuccess)
     return LSG_ERR_CUDA;
+  ++c->launches;
+  return LSG_OK;
+}
+
+int lsg_steady_sources_device(lsg_ctx* c, int ncells, int nspecies, const double* Y, const double* T, long ld,
+                              const double* p, double p_scalar, double* S_implicit, double* S_explicit, long lds,
+                              void* stream) {
+  if (!c || ncells < 0 || !Y || !T || !S_implicit || !S_explicit || ld < ncells || lds < ncells) return LSG_ERR_ARG;
+  if (!p && !(p_scalar > 0.)) return LSG_ERR_ARG;
+  const MechLayout& L = c->mech->host.layout;
+  if (nspecies != L.nc) return LSG_ERR_ARG;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  const cudaStream_t s = (cudaStream_t)stream;
+  const long need = 3L * (L.nc + 1) * ncells;
+  if (need > c->frs_cap) {
+    if (cudaStreamSynchronize(s) != cudaSuccess) return LSG_ERR_CUDA;
+    cudaFree(c->frs);
+    c->frs = nullptr;
+    c->frs_cap = 0;
+    if (cudaMalloc(&c->frs, sizeof(double) * need) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+    c->frs_cap = need;
+  }
+  if (!sm_count(c)) return LSG_ERR_CUDA;
+  const cudaError_t e = launch_steady_sources(L, c->mech->d_buf, ncells, Y, T, ld, p, p_scalar, c->frs, S_implicit,
+                                              S_explicit, lds, c->sm_count, c->d_err, s);
+  if (e == cudaErrorInvalidValue) { cudaGetLastError(); return LSG_ERR_UNSUPPORTED; }
+  if (e != cudaSuccess) return LSG_ERR_CUDA;
   ++c->launches;
   return LSG_OK;
 }

@@ -122,8 +122,11 @@ __device__ __forceinline__ double hi_b(int k, int NC, double ymaxT) { return k <
 // memory, [species][thread].  f has stride fs.  Returns QR.  rho0 > 0 selects
 // the constant-volume reactor of that density (BatchReactorHomogeneousConstant
 // Volume.H:148-199): cTot = rho0 / MW, dY/dt = MW R / rho0 and
-// dT/dt = (QR + R T sum R_i) / (rho0 cv).
+// dT/dt = (QR + R T sum R_i) / (rho0 cv).  With kSources, f receives the
+// source terms R_i MW_i instead of the species derivatives (the steady
+// solvers' reactionSourceTerms).
 // ---------------------------------------------------------------------------
+template <bool kSources = false>
 __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const double* __restrict__ Md,
                                         const int* __restrict__ Mi, double* __restrict__ scratch,
                                         const double* __restrict__ y, long ns, int pj, double pval,
@@ -270,7 +273,7 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
   double QR = 0., cpm = 0., dsum = 0.;
   for (int i = 0; i < NC; ++i) {
     const double Ri = SC_(R, i);
-    f[(long)i * fs] = MW[i] * Ri / rho;
+    f[(long)i * fs] = kSources ? Ri * MW[i] : MW[i] * Ri / rho;
     if (energy) {
       const bool hi = T > TM[i];
       const double* A = hi ? M.D(L.cp_ht) + 5 * i : M.D(L.cp_lt) + 5 * i;
@@ -657,6 +660,64 @@ __global__ void __launch_bounds__(kRT, 4) rounds_rhs_kernel(MechLayout Lp, const
     }
     R[D_QR] = rhs_cell(&sL, Md, Mi, scratch, src, 1, pj, pval, dst, 1, P0, energy, B.rho ? B.rho[cell] : 0.);
     RI[I_CNT0 + CNT_RHS] += 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Source terms and diagonal Jacobian of the steady solvers (laminarSMOKE
+// steady/linearModel.H:92-170 as jacobianEvaluation.H:60-92 calls it), one
+// thread per cell:
+//   S_i = R_i MW_i (i < NC), S_NC = QR at omega = max(Y, 0), T and the cell's
+//   pressure;
+//   J_k = (S_k(y + dy_k e_k) - S_k(y)) / dy_k with the increment dy_k of
+//   reactionJacobian (:132-170), the perturbed mass fraction clipped at zero
+//   as reactionSourceTerms clips it;
+//   implicit_k = J_k, explicit_k = S_k - J_k y_k (y unclipped).
+// yb, s0, sp: scratch [n][ncells] (clipped state, S(y), S(y + dy e_k)).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRT, 4) steady_sources_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem,
+                                                                long ncells, const double* __restrict__ Y,
+                                                                const double* __restrict__ T, long ld,
+                                                                const double* __restrict__ pc, double p_scalar,
+                                                                double* __restrict__ yb, double* __restrict__ s0,
+                                                                double* __restrict__ sp, double* __restrict__ Simp,
+                                                                double* __restrict__ Sexp, long lds, int* err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ MechLayout sL;
+  if (threadIdx.x == 0) sL = Lp;
+  if (!stage_bulk(smem, mech_gmem, Lp.bytes, &mbar, err)) return;
+  const double* Md = (const double*)smem;
+  const int* Mi = (const int*)(smem + (size_t)Lp.n_double * sizeof(double));
+  double* scratch = (double*)(smem + ((Lp.bytes + 15u) & ~15u));
+  const int NC = Lp.nc, n = NC + 1;
+  const double ZERO_DER = sqrt(kTinyFloat);
+  const double ETA2 = sqrt(kMachEpsDouble);
+  const double TOLR = 1.e-7, TOLA = 1.e-12;
+  for (long c = (long)blockIdx.x * kRT + threadIdx.x; c < ncells; c += (long)gridDim.x * kRT) {
+    for (int i = 0; i < NC; ++i) yb[(long)i * ncells + c] = fmax(Y[(long)i * ld + c], 0.);
+    yb[(long)NC * ncells + c] = T[c];
+    const double P0 = pc ? pc[c] : p_scalar;
+    const double* y = yb + c;
+    s0[(long)NC * ncells + c] = rhs_cell<true>(&sL, Md, Mi, scratch, y, ncells, -1, 0., s0 + c, ncells, P0, 1, 0.);
+    for (int k = 0; k < n; ++k) {
+      const double yk = k < NC ? Y[(long)k * ld + c] : T[c];
+      const double ew = 1. / (TOLA + TOLR * fabs(yk));
+      double hJ = ETA2 * fabs(fmax(yk, 1. / ew));
+      const double hJf = 1. / ew;
+      hJ = fmax(hJ, hJf);
+      hJ = fmax(hJ, ZERO_DER);
+      const double dy = fmin(hJ, 1.e-3 + 1e-3 * fabs(yk));
+      const double udy = 1. / dy;
+      double pv = yk + dy;
+      if (k < NC) pv = fmax(pv, 0.);
+      const double qp = rhs_cell<true>(&sL, Md, Mi, scratch, y, ncells, k, pv, sp + c, ncells, P0, 1, 0.);
+      const double spk = k < NC ? sp[(long)k * ncells + c] : qp;
+      const double s0k = s0[(long)k * ncells + c];
+      const double J = (spk - s0k) * udy;
+      Simp[(long)k * lds + c] = J;
+      Sexp[(long)k * lds + c] = s0k - J * yk;
+    }
   }
 }
 
@@ -1380,6 +1441,28 @@ cudaError_t prepare_advance(size_t as, int* bps) {
 size_t rounds_bytes(const MechLayout& L, long cap, bool lu64) {
   const RecLayout R = rec_layout(L.nc + 1, lu64);
   return sizeof(double) * (size_t)R.RS * cap + 2 * list_bytes(cap) + ((cap + 255) & ~255L) + 256;
+}
+
+cudaError_t launch_steady_sources(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* Y,
+                                  const double* T, long ld, const double* p, double p_scalar, double* scratch,
+                                  double* Simp, double* Sexp, long lds, int sm_count, int* err, cudaStream_t stream) {
+  if (ncells <= 0) return cudaSuccess;
+  const size_t smem = ((L.bytes + 15u) & ~15u) + (size_t)3 * L.nc * kRT * sizeof(double);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(steady_sources_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int bps = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, steady_sources_kernel, kRT, smem);
+  if (e != cudaSuccess) return e;
+  if (bps <= 0) return cudaErrorInvalidConfiguration;
+  const long want = (ncells + kRT - 1) / kRT, cap = (long)sm_count * bps;
+  const long n = L.nc + 1;
+  double* yb = scratch;
+  double* s0 = scratch + n * ncells;
+  double* sp = scratch + 2 * n * ncells;
+  steady_sources_kernel<<<(unsigned)(want < cap ? want : cap), kRT, smem, stream>>>(
+      L, mech_gmem, ncells, Y, T, ld, p, p_scalar, yb, s0, sp, Simp, Sexp, lds, err);
+  return cudaGetLastError();
 }
 
 size_t rounds_cache_bytes(const MechLayout& L, const RoundsPlan& P) {

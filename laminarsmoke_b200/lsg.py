@@ -48,7 +48,7 @@ EXPORTS = (
     "lsg_strerror", "lsg_abi_version", "lsg_ctx_stream", "lsg_ctx_launches",
     "lsg_reaction_step_device_noalloc", "lsg_ctx_kernel_times", "lsg_ctx_tuning",
     "lsg_compact_sources_device", "lsg_formation_rates_device",
-    "lsg_reaction_step_cv", "lsg_reaction_step_cv_device",
+    "lsg_reaction_step_cv", "lsg_reaction_step_cv_device", "lsg_steady_sources_device",
 )
 
 _lib = None
@@ -88,6 +88,7 @@ def lib():
     L.lsg_ctx_launches.restype = C.c_longlong
     L.lsg_reaction_step_cv.argtypes = [vp, i, i, C.POINTER(vp), vp, vp, d, vp, d, vp, vp, vp]
     L.lsg_reaction_step_cv_device.argtypes = [vp, i, i, vp, l, vp, vp, d, vp, d, vp, vp, vp, vp, vp]
+    L.lsg_steady_sources_device.argtypes = [vp, i, i, vp, vp, l, vp, d, vp, vp, l, vp]
     L.lsg_compact_sources_device.argtypes = [vp, i, i, vp, vp, vp, vp, l, d, vp, d, vp, vp, vp]
     L.lsg_formation_rates_device.argtypes = [vp, i, i, vp, vp, l, d, vp, l, vp]
     _lib = L
@@ -284,6 +285,16 @@ class ReactionStep:
             self.h, n, nc, Y0.data_ptr(), T0.data_ptr(), Yf.data_ptr(), Tf.data_ptr(), ld, p, dtp, dts,
             RR.data_ptr(), None if RT is None else RT.data_ptr(), _stream_handle(stream)),
             "lsg_compact_sources_device")
+
+    def steady_sources_device(self, Y, T, S_implicit, S_explicit, p=101325.0, stream=None):
+        """Linearised source terms of the steady solvers (lsg_steady_sources_device): S_implicit and
+        S_explicit [NC + 1, lds]; p a scalar or a per-cell tensor."""
+        _require_layout(Y, T, S_implicit, S_explicit, p if hasattr(p, "data_ptr") else None)
+        nc, ld = Y.shape
+        pp, ps = (p.data_ptr(), 0.0) if hasattr(p, "data_ptr") else (None, float(p))
+        _check(lib().lsg_steady_sources_device(self.h, T.shape[0], nc, Y.data_ptr(), T.data_ptr(), ld, pp, ps,
+                                               S_implicit.data_ptr(), S_explicit.data_ptr(), S_implicit.shape[1],
+                                               _stream_handle(stream)), "lsg_steady_sources_device")
 
     def formation_rates_device(self, Y, T, out, p: float = 101325.0, stream=None):
         """R_i MW_i [kg/m3/s] of every species at the states (Y [NC, ld], T) into out [NC, ld_out]."""

@@ -1074,6 +1074,46 @@ int orc_formation_rates(void* mech, double P, const double* y, double* out) {
   return 0;
 }
 
+// Steady solvers' linearised sources, solvers/laminarSMOKE/steady/linearModel.H:92-170 (reactionSourceTerms,
+// reactionJacobian) as jacobianEvaluation.H:60-92 stores them.  y = [Y_1..Y_NC, T] of one cell.
+int orc_steady_sources(void* mech, double P, const double* y, double* s_implicit, double* s_explicit) {
+  const orc::Mech& m = *(const orc::Mech*)mech;
+  const int NC = m.nc, NE = NC + 1;
+  const auto& MW = m.F("mw");
+  orc::Reactor r(m);
+  r.P0 = P;
+  r.energy = true;
+  std::vector<double> yc(NE), dy(NE), S0(NE), Sp(NE), yp(y, y + NE);
+  auto sources = [&](const double* yy, double* S) {   // reactionSourceTerms: omega = max(y, 0)
+    for (int i = 0; i < NC; ++i) yc[i] = std::max(yy[i], 0.);
+    yc[NC] = yy[NC];
+    r.equations(yc.data(), dy.data());
+    for (int i = 0; i < NC; ++i) S[i] = r.R[i] * MW[i];
+    S[NC] = r.QR;
+  };
+  sources(y, S0.data());
+  const double ZERO_DER = std::sqrt(orc::TINY_FLOAT);
+  const double ETA2 = std::sqrt(orc::MACH_EPS_DOUBLE);
+  const double TOLR = 1.e-7, TOLA = 1.e-12;
+  for (int k = 0; k < NE; ++k) {
+    const double hf = 1.;
+    const double error_weight = 1. / (TOLA + TOLR * std::fabs(y[k]));
+    double hJ = ETA2 * std::fabs(std::max(y[k], 1. / error_weight));
+    const double hJf = hf / error_weight;
+    hJ = std::max(hJ, hJf);
+    hJ = std::max(hJ, ZERO_DER);
+    const double d = std::min(hJ, 1.e-3 + 1e-3 * std::fabs(y[k]));
+    const double udy = 1. / d;
+    yp[k] += d;
+    sources(yp.data(), Sp.data());
+    const double J = (Sp[k] - S0[k]) * udy;
+    yp[k] = y[k];
+    s_implicit[k] = J;
+    s_explicit[k] = S0[k] - J * y[k];
+  }
+  return 0;
+}
+
 int orc_num_counters() { return orc::NCOUNT; }
 
 }  // extern "C"

@@ -53,6 +53,7 @@ def lib():
         L.orc_compact_sources.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_double, C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]
         L.orc_formation_rates.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
+        L.orc_steady_sources.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -102,6 +103,14 @@ class OracleMechanism:
         out = np.zeros(y.size - 1)
         lib().orc_formation_rates(self.h, p, _ptr(y), _ptr(out))
         return out
+
+    def steady_sources(self, y, p=101325.0):
+        """(S_implicit, S_explicit) [NC + 1] of the steady solvers at y = [Y_1..Y_NC, T]."""
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        si = np.zeros(y.size)
+        se = np.zeros(y.size)
+        lib().orc_steady_sources(self.h, p, _ptr(y), _ptr(si), _ptr(se))
+        return si, se
 
     def fd_jacobian(self, y, h, rtol=1e-7, atol=1e-12, p=101325.0, y_max_T=6000.0):
         y = np.ascontiguousarray(y, dtype=np.float64)

@@ -1,8 +1,11 @@
 """Output fields beyond Y, T and Q (chemistry_DI.H): the compact Strang
-scheme's source terms RR/RT (:236-281) and the formation-rate fields
-(:293-326).  CPU: the oracle against an independent numpy restatement and
-conservation laws.  GPU: the library against the oracle on the same inputs.
+scheme's source terms RR/RT (:236-281), the formation-rate fields (:293-326),
+and the steady solvers' linearised sources (steady/linearModel.H:92-170).
+CPU: the oracle against an independent numpy restatement and conservation
+laws.  GPU: the library against the oracle on the same inputs.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -114,3 +117,80 @@ def test_gpu_formation_rates(h2co, cuda, mech_name):
     for c in range(512):
         ref = orc.formation_rates(np.concatenate([Y[c], [T[c]]]))
         np.testing.assert_allclose(g[c], ref, rtol=rtol, atol=1e-12 * np.abs(ref).max())
+
+
+def _steady_ref(orc, y, p=101325.0):
+    """linearModel::reactionSourceTerms + ::reactionJacobian (steady/linearModel.H:92-170) written out with
+    the oracle's formation rates and heat release."""
+    nc = y.size - 1
+
+    def sources(yy):
+        yc = yy.copy()
+        yc[:nc] = np.maximum(yc[:nc], 0.0)
+        s = np.empty(nc + 1)
+        s[:nc] = orc.formation_rates(yc, p)
+        s[nc] = orc.rhs(yc, p)[1]
+        return s
+    s0 = sources(y)
+    zero_der = math.sqrt(float(np.float32(1.175494351e-38)))
+    eta2 = math.sqrt(2.220446049250313e-16)
+    si = np.empty(nc + 1)
+    se = np.empty(nc + 1)
+    for k in range(nc + 1):
+        ew = 1.0 / (1e-12 + 1e-7 * abs(y[k]))
+        hj = eta2 * abs(max(y[k], 1.0 / ew))
+        hj = max(hj, 1.0 / ew)
+        hj = max(hj, zero_der)
+        d = min(hj, 1.e-3 + 1e-3 * abs(y[k]))
+        yp = y.copy()
+        yp[k] += d
+        j = (sources(yp)[k] - s0[k]) * (1.0 / d)
+        si[k] = j
+        se[k] = s0[k] - j * y[k]
+    return si, se
+
+
+def test_oracle_steady_sources(h2co, oracle_h2co):
+    Y, T = _states(h2co, 16, 55)
+    Y[0, 3] = -1e-12   # a slightly negative mass fraction: clipped in the source, perturbed unclipped
+    for c in range(16):
+        y = np.concatenate([Y[c], [T[c]]])
+        si, se = oracle_h2co.steady_sources(y)
+        ri, re = _steady_ref(oracle_h2co, y)
+        np.testing.assert_allclose(si, ri, rtol=1e-13, atol=1e-300)
+        np.testing.assert_allclose(se, re, rtol=1e-13, atol=1e-12 * np.abs(re).max())
+
+
+@pytest.mark.gpu
+def test_gpu_steady_sources(h2co, oracle_h2co, cuda):
+    """Device against oracle.  A one-sided difference carries the rounding of S_k amplified by 1/dy_k, so
+    each J_k is compared within 1e-6 |J_k| plus 64 eps |S_k| / dy_k."""
+    import torch
+    from laminarsmoke_b200 import lsg
+    Y, T = _states(h2co, 512, 56)
+    p = np.random.default_rng(57).uniform(0.8e5, 1.2e5, 512)
+    ctx = lsg.ReactionStep(lsg.Mechanism(h2co[0]))
+    Yd = torch.tensor(np.ascontiguousarray(Y.T), device=cuda)
+    Td = torch.tensor(T, device=cuda)
+    n = Y.shape[1] + 1
+    Si = torch.zeros(n, 600, dtype=torch.float64, device=cuda)
+    Se = torch.zeros(n, 600, dtype=torch.float64, device=cuda)
+    ctx.steady_sources_device(Yd, Td, Si, Se, p=torch.tensor(p, device=cuda))
+    torch.cuda.synchronize()
+    ctx.check()
+    si, se = Si.cpu().numpy()[:, :512].T, Se.cpu().numpy()[:, :512].T
+    worst = 0.0
+    for c in range(512):
+        y = np.concatenate([Y[c], [T[c]]])
+        ri, re = oracle_h2co.steady_sources(y, p[c])
+        s0 = re + ri * y
+        ew = 1.0 / (1e-12 + 1e-7 * np.abs(y))
+        hj = np.maximum(np.maximum(math.sqrt(2.220446049250313e-16) * np.abs(np.maximum(y, 1.0 / ew)), 1.0 / ew),
+                        math.sqrt(float(np.float32(1.175494351e-38))))
+        d = np.minimum(hj, 1e-3 + 1e-3 * np.abs(y))
+        tol = 1e-6 * np.abs(ri) + 64 * 2.220446049250313e-16 * np.abs(s0) / d
+        err = np.abs(si[c] - ri)
+        worst = max(worst, float((err / np.maximum(tol, 1e-300)).max()))
+        assert np.all(err <= tol), (c, err / tol)
+        np.testing.assert_allclose(se[c] + si[c] * y, s0, rtol=1e-10, atol=1e-12 * np.abs(s0).max())
+    print(f"worst J error / tolerance {worst:.3f}")

@@ -14,6 +14,8 @@ workloads of this project use:
                    ``data/GLOBAL_*_1step.lsmech``;
 * ``"syn120"``  -- seeded synthetic C1-C2 mechanism, 120 species / 800 reactions;
 * ``"syn500"``  -- seeded synthetic mechanism, 500 species / 3 000 reactions;
+* ``"syn120p"``, ``"syn500p"`` -- the same mechanisms with physically bounded
+                   activation energies and rate constants (integrable);
 * ``"h2co+K"``  -- POLIMI_H2CO_1412 with K chemically inert copies of N2 added
                    (``pad_inert``): the H2/CO chemistry in a mechanism of 14 + K
                    species, which exercises the large-mechanism path with
@@ -30,8 +32,11 @@ from . import blob as _blob
 DATA = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "data")
 
 SYNTHETIC = {
-    "syn120": (120, 800, 1201),
-    "syn500": (500, 3000, 5003),
+    "syn120": (120, 800, 1201, False),
+    "syn500": (500, 3000, 5003, False),
+    # the same draws under physical bounds on barriers and rate constants (mech/synthetic.py)
+    "syn120p": (120, 800, 1201, True),
+    "syn500p": (500, 3000, 5003, True),
 }
 
 
@@ -69,8 +74,8 @@ def load(name: str) -> Tuple[bytes, List[str]]:
         return data, species
     if name in SYNTHETIC:
         from . import chemkin, synthetic
-        ns, nr, seed = SYNTHETIC[name]
-        s = synthetic.generate(ns, nr, seed)
+        ns, nr, seed, physical = SYNTHETIC[name]
+        s = synthetic.generate(ns, nr, seed, physical=physical)
         m = chemkin.compile_mechanism(s.kinetics, s.thermo)
         return _blob.pack(m.arrays, m.species), m.species
     raise KeyError(f"unknown mechanism {name!r}")

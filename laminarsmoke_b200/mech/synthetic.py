@@ -21,6 +21,14 @@ Construction:
   [300, T_mid] and [T_mid, 3500] K; a6/a7 come from a bounded formation
   enthalpy (|Hf| <= 50 kcal/mol) and standard entropy, made continuous at T_mid,
   which keeps |dG/RT| of every reaction well below the exp() overflow range.
+
+With ``physical=True`` the same draws are shaped by two physical bounds:
+every activation energy is raised by the reaction's endothermicity at 298 K
+(so no reverse rate constant exceeds its forward one by more than exp(dS/R)),
+and forward rate constants at 2000 K are capped at 1e14 cm3/mol/s (1e17
+cm6/mol2/s for third-body and 1e20 for fall-off low-pressure limits).  The
+unbounded mechanisms give time scales near 1e-13 s and many cells that no
+integrator finishes; the bounded ones integrate like real chemistry.
 """
 from __future__ import annotations
 
@@ -100,11 +108,11 @@ def _fit_nasa(rng: np.random.Generator, natoms: int, tmid: float):
     a7_lt = s0 - spoly(lt, 298.15)
     a6_ht = (hpoly(lt, tmid) + a6_lt) - hpoly(ht, tmid)
     a7_ht = (spoly(lt, tmid) + a7_lt) - spoly(ht, tmid)
-    return np.concatenate([ht, [a6_ht, a7_ht]]), np.concatenate([lt, [a6_lt, a7_lt]])
+    return np.concatenate([ht, [a6_ht, a7_ht]]), np.concatenate([lt, [a6_lt, a7_lt]]), hf
 
 
 def generate(n_species: int, n_reactions: int, seed: int,
-             frac_thirdbody: float = 0.15, frac_troe: float = 0.10) -> SyntheticMechanism:
+             frac_thirdbody: float = 0.15, frac_troe: float = 0.10, physical: bool = False) -> SyntheticMechanism:
     rng = np.random.default_rng(seed)
     cmax = 2 if n_species <= 200 else 4
     hmax = 6 if n_species <= 200 else 10
@@ -126,10 +134,11 @@ def generate(n_species: int, n_reactions: int, seed: int,
 
     # thermodynamics
     th_lines = ["THERMO ALL", "   300.000  1000.000  3500.000"]
+    hf_r: Dict[str, float] = {}   # formation enthalpy / R [K]
     for nm in names:
         comp = comps[nm]
         tmid = float(rng.choice([800.0, 1000.0, 1200.0, 1400.0]))
-        ht, lt = _fit_nasa(rng, sum(comp), tmid)
+        ht, lt, hf_r[nm] = _fit_nasa(rng, sum(comp), tmid)
         th_lines += _nasa_lines(nm, comp, tmid, ht, lt)
     th_lines.append("END")
 
@@ -159,10 +168,14 @@ def generate(n_species: int, n_reactions: int, seed: int,
     lines += ["END", "REACTIONS"]
     bath_eff = [n for n in ("H2O", "CO2", "H2", "CO") if n in idx]
 
-    def arrh():
+    def arrh(reac=(), prod=(), kcap=1.e14):
         A = 10.0 ** rng.uniform(6.0, 14.0)
         b = rng.uniform(-2.0, 2.0)
         Ea = rng.uniform(0.0, 60000.0)
+        if physical:
+            dh = R_CAL * (sum(hf_r[names[q]] for q in prod) - sum(hf_r[names[q]] for q in reac))   # cal/mol
+            Ea += max(0.0, dh)
+            A = min(A, kcap / 2000.0 ** b)
         return A, b, Ea
 
     for kind in kinds:
@@ -178,7 +191,7 @@ def generate(n_species: int, n_reactions: int, seed: int,
                 if key in seen:
                     continue
                 seen.add(key)
-                A, b, Ea = arrh()
+                A, b, Ea = arrh((i, j), (c, d))
                 lines.append(f"{'+'.join(_side(names, i, j))}={'+'.join(_side(names, c, d))}"
                              f"   {A:.6E} {b:.4f} {Ea:.3f}")
                 break
@@ -192,7 +205,7 @@ def generate(n_species: int, n_reactions: int, seed: int,
                 if key in seen:
                     continue
                 seen.add(key)
-                A, b, Ea = arrh()
+                A, b, Ea = arrh((i, j), (t,), 1.e17 if kind == "tb" else 1.e14)
                 left = "+".join(_side(names, i, j))
                 effs = "".join(f"{n}/{rng.uniform(1.5, 8.0):.2f}/" for n in bath_eff
                                if idx[n] not in (i, j, t))
@@ -203,6 +216,8 @@ def generate(n_species: int, n_reactions: int, seed: int,
                     A0 = A * 10.0 ** rng.uniform(3.0, 7.0)
                     b0 = b - rng.uniform(0.0, 2.0)
                     E0 = Ea * rng.uniform(0.0, 1.0)
+                    if physical:
+                        A0 = min(A0, 1.e20 / 2000.0 ** b0)
                     lines.append(f" LOW/ {A0:.6E} {b0:.4f} {E0:.3f} /")
                     lines.append(f" TROE/ {rng.uniform(0.1, 0.9):.4f} {rng.uniform(50, 500):.2f} "
                                  f"{rng.uniform(500, 5000):.2f} {rng.uniform(2000, 9000):.2f} /")

@@ -118,3 +118,28 @@ def test_block_synthetic_120_step(cuda):
     assert np.all(np.isin(stg, [2, -1, -2, -4, -5, -6]))
     assert np.all(np.isfinite(Yg)) and np.all(np.isfinite(Tg))
     np.testing.assert_allclose(Yg.sum(axis=1), 1.0, atol=1e-12)
+
+
+
+def test_block_synthetic_120p_step(cuda):
+    """One step of the physically bounded 120-species / 800-reaction synthetic chemistry (barriers no lower
+    than the endothermicity, rate constants at the collision limit; T ~ U[800, 2400] K, dt = 5e-6 s,
+    thousands of BDF steps per cell) against the oracle.  At the default tolerances rounding-level
+    differences move the step sequences of such long integrations apart by O(rtol); with rtol 1e-10 both
+    integrations converge on the exact solution and are compared at the usual bounds."""
+    from laminarsmoke_b200 import mech
+    from laminarsmoke_b200.mech import blob
+    data, species = mech.load("syn120p")
+    A, _ = blob.unpack(data)
+    Y, T = cells.synthetic_mixing(species, A["mw"], 32, seed=3, t_range=(800.0, 2400.0))
+    for rtol, atol in ((1e-7, 1e-12), (1e-10, 1e-16)):
+        (Yg, Tg, Qg, stg, nsg), (Yo, To, Qo, sto, cnt) = _run(data, Y, T, 5e-6, rtol=rtol, atol=atol)
+        rel_T = np.abs(Tg - To) / To
+        abs_Y = np.abs(Yg - Yo).max(axis=1)
+        print(f"syn120p rtol {rtol:g}: statuses equal {np.mean(stg == sto):.3f}, max rel T err {rel_T.max():.3e}, "
+              f"max abs Y err {abs_Y.max():.3e}, cells within 1e-9 {np.mean(abs_Y <= ATOL_Y):.3f}, "
+              f"steps {cnt[:, 0].mean():.0f}", flush=True)
+    np.testing.assert_array_equal(stg, sto)
+    assert np.all(stg == 2)
+    assert rel_T.max() <= RTOL_T
+    assert np.mean(abs_Y <= ATOL_Y) >= 0.9 and abs_Y.max() <= 1e-7

@@ -865,7 +865,7 @@ struct GearBlock {
 // chemistry_DI.H:92-235: gather, clip and renormalise, integrate, renormalise, scatter.
 // ---------------------------------------------------------------------------
 template <int BT>
-__global__ void __launch_bounds__(BT) block_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem,
+__global__ void __launch_bounds__(BT, BT == 128 ? 4 : (BT == 256 ? 2 : 1)) block_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem,
                                                    StepOptions o, StepArgs a, double* __restrict__ ws_all,
                                                    int* queue) {
   extern __shared__ __align__(16) unsigned char bsm[];

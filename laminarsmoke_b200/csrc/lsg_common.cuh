@@ -31,6 +31,29 @@ __device__ __forceinline__ double seq_sum(double v, int n) {
   return s;
 }
 
+// Rate constant of a pressure-logarithmic (PLOG) reaction at T and P
+// (PressureLogarithmicRateExpression::KineticConstant,
+// PressureLogarithmicRateExpression.hpp:104-119): the first or last point
+// outside the tabulated pressures, else ln k interpolated linearly in ln P
+// between the two points that bracket P.
+__device__ __forceinline__ double plog_k(const MechView& M, const MechLayout& L, int slot, double T, double logT,
+                                         double P) {
+  const int a = M.I(L.plog_ptr)[slot], b = M.I(L.plog_ptr)[slot + 1];
+  const double* p = M.D(L.plog_p);
+  const double* lnA = M.D(L.plog_lnA);
+  const double* be = M.D(L.plog_beta);
+  const double* er = M.D(L.plog_eor);
+  if (P <= p[a]) return exp(lnA[a] + be[a] * logT - er[a] / T);
+  if (P >= p[b - 1]) return exp(lnA[b - 1] + be[b - 1] * logT - er[b - 1] / T);
+  int i = a;
+  for (; i < b - 1; ++i)
+    if (P < p[i + 1]) break;
+  const double* lnp = M.D(L.plog_lnp);
+  const double kA = lnA[i] + be[i] * logT - er[i] / T;
+  const double kB = lnA[i + 1] + be[i + 1] * logT - er[i + 1] / T;
+  return exp(kA + (kB - kA) * (log(P) - lnp[i]) / (lnp[i + 1] - lnp[i]));
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }

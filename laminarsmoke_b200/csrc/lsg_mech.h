@@ -28,10 +28,13 @@ struct MechLayout {
   int fo_lnA, fo_beta, fo_eor, fo_a, fo_b, fo_c, fo_d, fo_e; // fall-off (by slot)
   int reac_nu, prod_nu, fr_coef, tb_eff, fo_eff;             // CSR values
   int ford_val;                                              // forward rate-law orders (FORD or reac_nu)
+  int plog_p, plog_lnp, plog_lnA, plog_beta, plog_eor;       // pressure-logarithmic points (by slot CSR)
+  int n_plog;                                                // reactions with PLOG
   // ---- int region offsets
   int a_sign, rev_kind, rev_slot, tb_slot, fo_slot;          // per reaction
   int reac_ptr, reac_sp, prod_ptr, prod_sp;                  // per reaction CSR
   int ford_ptr, ford_sp;                                     // per reaction CSR of the forward orders
+  int plog_slot, plog_ptr, plog_rxn;                         // per reaction slot (-1: none); CSR by slot
   int fr_ptr, fr_rxn;                                        // per species CSR
   int tb_ptr, tb_sp;                                         // third body CSR (by slot)
   int fo_type, fo_single, fo_ptr, fo_sp;                     // fall-off (by slot)

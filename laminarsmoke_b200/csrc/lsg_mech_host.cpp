@@ -118,6 +118,15 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
     L.prod_nu = B.addd(b.F("prod_nu"));
     L.fr_coef = B.addd(b.F("fr_coef"));
     L.tb_eff = B.addd(b.F("tb_eff_m1"));
+    // pressure-logarithmic (PLOG) reactions, when the mechanism has them
+    const bool plog = b.f.count("plog_p") != 0;
+    const std::vector<double> none_d(2, 0.);
+    const std::vector<int> none_i(2, 0), plog_ptr0{0};
+    L.plog_p = B.addd(plog ? b.F("plog_p") : none_d);
+    L.plog_lnp = B.addd(plog ? b.F("plog_lnp") : none_d);
+    L.plog_lnA = B.addd(plog ? b.F("plog_lnA") : none_d);
+    L.plog_beta = B.addd(plog ? b.F("plog_beta") : none_d);
+    L.plog_eor = B.addd(plog ? b.F("plog_eor") : none_d);
     L.fo_eff = B.addd(b.F("fo_eff_m1"));
 
     const auto& isrev = b.I("is_reversible");
@@ -133,6 +142,20 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
     for (size_t k = 0; k < tbr.size(); ++k) tb_slot.at(tbr[k]) = (int)k;
     for (size_t k = 0; k < fr.size(); ++k) fo_slot.at(fr[k]) = (int)k;
 
+    std::vector<int> plog_slot(nr, -1);
+    const std::vector<int> plog_rxn = plog ? b.I("plog_rxn") : std::vector<int>();
+    const std::vector<int> plog_ptr = plog ? b.I("plog_ptr") : plog_ptr0;
+    for (size_t k = 0; k < plog_rxn.size(); ++k) plog_slot.at(plog_rxn[k]) = (int)k;
+    if (plog_ptr.size() != plog_rxn.size() + 1 || (plog && (size_t)plog_ptr.back() != b.F("plog_p").size())) {
+      err = "inconsistent PLOG arrays in mechanism blob";
+      return false;
+    }
+    for (size_t k = 0; k + 1 < plog_ptr.size(); ++k)
+      if (plog_ptr[k + 1] <= plog_ptr[k]) { err = "PLOG reaction without points"; return false; }
+    L.n_plog = (int)plog_rxn.size();
+    L.plog_slot = B.addi(plog_slot);
+    L.plog_ptr = B.addi(plog_ptr);
+    L.plog_rxn = B.addi(plog_rxn.empty() ? none_i : plog_rxn);
     L.a_sign = B.addi(b.I("a_sign"));
     L.rev_kind = B.addi(rev_kind);
     L.rev_slot = B.addi(rev_slot);

@@ -152,6 +152,7 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
   const bool cv = rho0 > 0.;
   const double cTot = cv ? rho0 / MWmix : P0 / kRgas / T;
   const double rho = cv ? rho0 : cTot * MWmix;
+  const double Pk = cv ? cTot * kRgas * T : P0;   // the kinetics map's pressure (PLOG)
   const double* TM = M.D(L.t_mid);
   const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, uT = 1. / T;
   const double logT = log(T);
@@ -191,6 +192,10 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
   for (int j = 0; j < NR; ++j) {
     double kArr = exp(lnA[j] + beta[j] * logT - eor[j] * uT);
     if (sgn[j] < 0) kArr *= -1.;
+    if (L.n_plog > 0) {   // pressure-logarithmic reaction (KineticsMap_CHEMKIN.hpp:1341-1348)
+      const int ps = M.I(L.plog_slot)[j];
+      if (ps >= 0) kArr = plog_k(M, L, ps, T, logT, Pk);
+    }
     double kMod = kArr;
     const int tb = tbs[j];
     if (tb >= 0) {

@@ -272,6 +272,8 @@ class Reaction:
     pd_species: int = -1
     duplicate: bool = False
     ford: bool = False   # FORD given: forward_orders replace the reactant coefficients in the rate law
+    plog: List[Tuple[float, float, float, float]] = field(default_factory=list)   # PLOG (p [atm], A, beta, E)
+    plog_table: List[Tuple[float, float, float, float, float]] = field(default_factory=list)  # (p [Pa], ln p, ln A, beta, E/R) SI
     forward_orders: List[Tuple[int, float]] = field(default_factory=list)
     text: str = ""
 
@@ -470,6 +472,11 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
                     break
             else:
                 r.forward_orders.append((si, val))
+        elif kw == "PLOG":
+            # ReactionPolicy_CHEMKIN.hpp:772-792: one (p [atm], A, beta, E) point per line
+            if third_body or pdr != "none" or i_low or i_troe or i_sri:
+                raise ChemkinError("PLOG cannot be combined with third bodies or LOW/TROE/SRI")
+            r.plog.append(tuple(_slash_numbers(line, (4,), "PLOG")))
         elif kw == "RORD":
             raise ChemkinError("option RORD is not available (ReactionPolicy_CHEMKIN.hpp:908-913 rejects it)")
         elif kw in ("DUP", "DUPLICATE"):
@@ -499,6 +506,8 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
         raise ChemkinError("unsupported pressure-dependent form")
     if r.A < 0. and r.tag != TAG_SIMPLE:
         raise ChemkinError("negative frequency factors only for simple reactions")
+    if r.plog and r.tag != TAG_SIMPLE:
+        raise ChemkinError("PLOG cannot be used for third-body or fall-off reactions")
     _convert_units(r, a_units, e_units)
     return r
 
@@ -534,6 +543,19 @@ def _convert_units(r: Reaction, a_units: str, e_units: str) -> None:
     else:
         r.E *= e_conv
         r.A *= math.pow(1.e3, 1. - sum_lr) / math.pow(a_conv, 1. - sum_lr)
+        if r.plog:
+            # PressureLogarithmicRateExpression::Setup (PressureLogarithmicRateExpression.hpp:71-101), with the
+            # conversion factors ConvertUnits appends (ReactionPolicy_CHEMKIN.hpp:1460-1465)
+            conv_a = math.pow(1.e3, 1. - sum_lr) / math.pow(a_conv, 1. - sum_lr)
+            last = -math.inf
+            for pa, a_, b_, e_ in r.plog:
+                if a_ < 0.:
+                    raise ChemkinError("PLOG needs non-negative frequency factors")
+                pp = pa * 101325.
+                if pp <= last:
+                    raise ChemkinError("PLOG pressures must be increasing")
+                last = pp
+                r.plog_table.append((pp, math.log(pp), math.log(max(a_ * conv_a, 1.e-32)), b_, e_ * e_conv / R_J_KMOL))
         if r.explicit_rev:
             r.E_rev *= e_conv
             r.A_rev *= math.pow(1.e3, 1. - sum_lp) / math.pow(a_conv, 1. - sum_lp)
@@ -775,6 +797,19 @@ def build_tables(species: List[str], reactions: List[Reaction], thermo: List[The
     A["reac_nu"] = np.array(rnu, f64)
     A["prod_ptr"] = np.array(pptr, np.int32); A["prod_species"] = np.array(psp, np.int32)
     A["prod_nu"] = np.array(pnu, f64)
+    if any(r.plog for r in reactions):
+        # pressure-logarithmic reactions (KineticsMap_CHEMKIN.hpp:1341-1348): their k replaces the Arrhenius one
+        prx, pptr2, pv = [], [0], {k: [] for k in ("p", "lnp", "lnA", "beta", "eor")}
+        for j, r in enumerate(reactions):
+            if r.plog:
+                prx.append(j)
+                for pp, lp, la, b_, er in r.plog_table:
+                    pv["p"].append(pp); pv["lnp"].append(lp); pv["lnA"].append(la); pv["beta"].append(b_)
+                    pv["eor"].append(er)
+                pptr2.append(len(pv["p"]))
+        A["plog_rxn"] = np.array(prx, np.int32); A["plog_ptr"] = np.array(pptr2, np.int32)
+        for k, v in pv.items():
+            A["plog_" + k] = np.array(v, f64)
     if any(r.ford for r in reactions):
         # forward rate-law orders (StoichiometricMap lambda lists), only when some reaction has FORD;
         # without them the reactant coefficients are the orders

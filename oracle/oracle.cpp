@@ -94,6 +94,7 @@ struct Reactor {
   int NC, NR;
   double P0 = 101325.;
   double rho0 = 0.;   // > 0: constant-volume reactor of this density (BatchReactorHomogeneousConstantVolume.H)
+  double P_ = 101325.;   // the kinetics map's pressure: P0, or cTot R T at constant volume
   bool energy = true;
   double QR = 0.;
   // thermo map
@@ -218,6 +219,27 @@ struct Reactor {
       }
       arr_recalc = false;
     }
+    // pressure-logarithmic reactions, every call: their k depends on P as well
+    // (KineticsMap_CHEMKIN.hpp:1341-1348, PressureLogarithmicRateExpression.hpp:104-119)
+    if (m.f.count("plog_p")) {
+      const auto& prx = m.I("plog_rxn"); const auto& pptr = m.I("plog_ptr");
+      const auto& pp = m.F("plog_p"); const auto& lnp = m.F("plog_lnp"); const auto& lA = m.F("plog_lnA");
+      const auto& pb = m.F("plog_beta"); const auto& pe = m.F("plog_eor");
+      for (size_t k = 0; k < prx.size(); ++k) {
+        const int a = pptr[k], b = pptr[k + 1];
+        double kk;
+        if (P_ <= pp[a]) kk = std::exp(lA[a] + pb[a] * std::log(T) - pe[a] / T);
+        else if (P_ >= pp[b - 1]) kk = std::exp(lA[b - 1] + pb[b - 1] * std::log(T) - pe[b - 1] / T);
+        else {
+          int i = a;
+          for (; i < b - 1; ++i) if (P_ < pp[i + 1]) break;
+          const double kA = lA[i] + pb[i] * std::log(T) - pe[i] / T;
+          const double kB = lA[i + 1] + pb[i + 1] * std::log(T) - pe[i + 1] / T;
+          kk = std::exp(kA + (kB - kA) * (std::log(P_) - lnp[i]) / (lnp[i + 1] - lnp[i]));
+        }
+        kArr[prx[k]] = kk;
+      }
+    }
     kMod = kArr;
   }
 
@@ -323,6 +345,7 @@ struct Reactor {
     const double cTot = cv ? rho0 / MWmix : P0 / R_J_KMOL / T;
     for (int i = 0; i < NC; ++i) c[i] = cTot * x[i];
     const double rho = cv ? rho0 : cTot * MWmix;
+    P_ = cv ? cTot * R_J_KMOL * T : P0;
     h_over_RT(T);   // species h/RT at T: used by the reaction enthalpies and by QR
     kin_set_T(T);
     reaction_rates();

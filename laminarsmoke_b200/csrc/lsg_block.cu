@@ -190,13 +190,16 @@ __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, 
       }
     }
   }
-  if (L.n_plog > 0) {
-    // pressure-logarithmic reactions: k depends on P too, so every call (KineticsMap_CHEMKIN.hpp:1341-1348)
+  if (L.n_plog > 0 || L.n_cheb > 0) {
+    // pressure-logarithmic and Chebyshev reactions: k depends on P too, so every call
+    // (KineticsMap_CHEMKIN.hpp:1332-1348)
     const double Pk = cv ? cTot * kRgas * T : P0;
     const double logTk = log(T);
     const int* prx = M.I(L.plog_rxn);
     __syncthreads();   // after the Arrhenius values other threads wrote above
     for (int k = tid; k < L.n_plog; k += BT) karr[prx[k]] = plog_k(M, L, k, T, logTk, Pk);
+    const int* crx = M.I(L.cheb_rxn);
+    for (int k = tid; k < L.n_cheb; k += BT) karr[crx[k]] = cheb_k(M, L, k, T, Pk);
   }
   const double cTotSum = bsum<BT>(cl, W.red);   // also orders the cache writes above before their reads
   {

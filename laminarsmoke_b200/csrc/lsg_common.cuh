@@ -54,6 +54,27 @@ __device__ __forceinline__ double plog_k(const MechView& M, const MechLayout& L,
   return exp(kA + (kB - kA) * (log(P) - lnp[i]) / (lnp[i + 1] - lnp[i]));
 }
 
+// Rate constant of a Chebyshev reaction at T and P
+// (ChebyshevPolynomialRateExpression::KineticConstant, :93-114, with
+// Phi(n, x) = cos((n - 1) acos(x)), :187-190): 10^(sum_nm a_nm phi_n(T~) phi_m(P~))
+// times the unit conversion, T~ and P~ the reduced inverse temperature and
+// log10 pressure.  Outside the limits acos is undefined, as in the reference.
+__device__ __forceinline__ double cheb_k(const MechView& M, const MechLayout& L, int slot, double T, double P) {
+  const int N = M.I(L.cheb_nm)[2 * slot], Mm = M.I(L.cheb_nm)[2 * slot + 1];
+  const double* a = M.D(L.cheb_coef) + M.I(L.cheb_ptr)[slot];
+  const double* lim = M.D(L.cheb_lim) + 5 * slot;
+  const double Tmin = lim[0], Tmax = lim[1], lPmin = lim[2], lPmax = lim[3];
+  const double Tt = (2. / T - 1. / Tmin - 1. / Tmax) / (1. / Tmax - 1. / Tmin);
+  const double Pt = (2. * log10(P) - lPmin - lPmax) / (lPmax - lPmin);
+  const double aT = acos(Tt), aP = acos(Pt);
+  double sum = 0.;
+  for (int n = 0; n < N; ++n) {
+    const double phn = cos(double(n) * aT);
+    for (int m = 0; m < Mm; ++m) sum += a[n * Mm + m] * phn * cos(double(m) * aP);
+  }
+  return pow(10., sum) * lim[4];
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }

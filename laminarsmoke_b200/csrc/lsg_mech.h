@@ -30,11 +30,14 @@ struct MechLayout {
   int ford_val;                                              // forward rate-law orders (FORD or reac_nu)
   int plog_p, plog_lnp, plog_lnA, plog_beta, plog_eor;       // pressure-logarithmic points (by slot CSR)
   int n_plog;                                                // reactions with PLOG
+  int cheb_coef, cheb_lim;                                   // Chebyshev coefficients, limits (by slot)
+  int n_cheb;                                                // reactions with CHEB
   // ---- int region offsets
   int a_sign, rev_kind, rev_slot, tb_slot, fo_slot;          // per reaction
   int reac_ptr, reac_sp, prod_ptr, prod_sp;                  // per reaction CSR
   int ford_ptr, ford_sp;                                     // per reaction CSR of the forward orders
   int plog_slot, plog_ptr, plog_rxn;                         // per reaction slot (-1: none); CSR by slot
+  int cheb_slot, cheb_rxn, cheb_nm, cheb_ptr;                // likewise for Chebyshev reactions
   int fr_ptr, fr_rxn;                                        // per species CSR
   int tb_ptr, tb_sp;                                         // third body CSR (by slot)
   int fo_type, fo_single, fo_ptr, fo_sp;                     // fall-off (by slot)

@@ -127,6 +127,10 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
     L.plog_lnA = B.addd(plog ? b.F("plog_lnA") : none_d);
     L.plog_beta = B.addd(plog ? b.F("plog_beta") : none_d);
     L.plog_eor = B.addd(plog ? b.F("plog_eor") : none_d);
+    // Chebyshev reactions, when the mechanism has them
+    const bool cheb = b.f.count("cheb_coef") != 0;
+    L.cheb_coef = B.addd(cheb ? b.F("cheb_coef") : none_d);
+    L.cheb_lim = B.addd(cheb ? b.F("cheb_lim") : none_d);
     L.fo_eff = B.addd(b.F("fo_eff_m1"));
 
     const auto& isrev = b.I("is_reversible");
@@ -156,6 +160,26 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
     L.plog_slot = B.addi(plog_slot);
     L.plog_ptr = B.addi(plog_ptr);
     L.plog_rxn = B.addi(plog_rxn.empty() ? none_i : plog_rxn);
+    std::vector<int> cheb_slot(nr, -1);
+    const std::vector<int> cheb_rxn = cheb ? b.I("cheb_rxn") : std::vector<int>();
+    const std::vector<int> cheb_ptr = cheb ? b.I("cheb_ptr") : plog_ptr0;
+    const std::vector<int> cheb_nm = cheb ? b.I("cheb_nm") : none_i;
+    for (size_t k = 0; k < cheb_rxn.size(); ++k) cheb_slot.at(cheb_rxn[k]) = (int)k;
+    if (cheb_ptr.size() != cheb_rxn.size() + 1 || (cheb && (cheb_nm.size() != 2 * cheb_rxn.size() ||
+        (size_t)cheb_ptr.back() != b.F("cheb_coef").size() || b.F("cheb_lim").size() != 5 * cheb_rxn.size()))) {
+      err = "inconsistent Chebyshev arrays in mechanism blob";
+      return false;
+    }
+    for (size_t k = 0; k < cheb_rxn.size(); ++k)
+      if (cheb_nm[2 * k] < 1 || cheb_nm[2 * k + 1] < 1 || cheb_ptr[k + 1] - cheb_ptr[k] != cheb_nm[2 * k] * cheb_nm[2 * k + 1]) {
+        err = "inconsistent Chebyshev table in mechanism blob";
+        return false;
+      }
+    L.n_cheb = (int)cheb_rxn.size();
+    L.cheb_slot = B.addi(cheb_slot);
+    L.cheb_rxn = B.addi(cheb_rxn.empty() ? none_i : cheb_rxn);
+    L.cheb_nm = B.addi(cheb_nm);
+    L.cheb_ptr = B.addi(cheb_ptr);
     L.a_sign = B.addi(b.I("a_sign"));
     L.rev_kind = B.addi(rev_kind);
     L.rev_slot = B.addi(rev_slot);

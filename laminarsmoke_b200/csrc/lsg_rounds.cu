@@ -196,6 +196,10 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
       const int ps = M.I(L.plog_slot)[j];
       if (ps >= 0) kArr = plog_k(M, L, ps, T, logT, Pk);
     }
+    if (L.n_cheb > 0) {   // Chebyshev reaction (KineticsMap_CHEMKIN.hpp:1332-1339)
+      const int cs = M.I(L.cheb_slot)[j];
+      if (cs >= 0) kArr = cheb_k(M, L, cs, T, Pk);
+    }
     double kMod = kArr;
     const int tb = tbs[j];
     if (tb >= 0) {

@@ -202,13 +202,16 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
       }
     }
   }
-  if (L.n_plog > 0) {
-    // pressure-logarithmic reactions: k depends on P too, so every call (KineticsMap_CHEMKIN.hpp:1341-1348)
+  if (L.n_plog > 0 || L.n_cheb > 0) {
+    // pressure-logarithmic and Chebyshev reactions: k depends on P too, so every call
+    // (KineticsMap_CHEMKIN.hpp:1332-1348)
     const double Pk = cv ? cTot * kRgas * T : P0;
     const double logTk = log(T);
     const int* prx = M.I(L.plog_rxn);
     __syncwarp();   // after the Arrhenius values other lanes wrote above
     for (int k = lane; k < L.n_plog; k += 32) W.KARR[prx[k]] = plog_k(M, L, k, T, logTk, Pk);
+    const int* crx = M.I(L.cheb_rxn);
+    for (int k = lane; k < L.n_cheb; k += 32) W.KARR[crx[k]] = cheb_k(M, L, k, T, Pk);
   }
   const double cTotSum = seq_sum(cl, NC);
   __syncwarp();

@@ -274,6 +274,10 @@ class Reaction:
     ford: bool = False   # FORD given: forward_orders replace the reactant coefficients in the rate law
     plog: List[Tuple[float, float, float, float]] = field(default_factory=list)   # PLOG (p [atm], A, beta, E)
     plog_table: List[Tuple[float, float, float, float, float]] = field(default_factory=list)  # (p [Pa], ln p, ln A, beta, E/R) SI
+    cheb: List[float] = field(default_factory=list)   # CHEB numbers as given: N, M, a_11 .. a_NM
+    cheb_T: List[float] = field(default_factory=list)  # TCHEB (Tmin, Tmax) [K]
+    cheb_P: List[float] = field(default_factory=list)  # PCHEB (Pmin, Pmax) [atm]
+    cheb_conv: float = 1.0
     forward_orders: List[Tuple[int, float]] = field(default_factory=list)
     text: str = ""
 
@@ -477,6 +481,21 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
             if third_body or pdr != "none" or i_low or i_troe or i_sri:
                 raise ChemkinError("PLOG cannot be combined with third bodies or LOW/TROE/SRI")
             r.plog.append(tuple(_slash_numbers(line, (4,), "PLOG")))
+        elif kw == "CHEB":
+            # ReactionPolicy_CHEMKIN.hpp:456-475: every number between the slashes, over as many lines as needed
+            if pdr != "all":
+                raise ChemkinError("CHEB needs a (+M) pressure-dependent reaction")
+            if i_low or i_troe or i_sri or r.plog:
+                raise ChemkinError("CHEB cannot be combined with LOW/TROE/SRI/PLOG")
+            a, b = line.find("/"), line.rfind("/")
+            r.cheb += [float(t) for t in line[a + 1:b].split()]
+        elif kw in ("TCHEB", "PCHEB"):
+            if pdr != "all":
+                raise ChemkinError(f"{kw} needs a (+M) pressure-dependent reaction")
+            lim = _slash_numbers(line, (2,), kw)
+            if (r.cheb_T if kw == "TCHEB" else r.cheb_P):
+                raise ChemkinError(f"{kw} is used more than once")
+            (r.cheb_T if kw == "TCHEB" else r.cheb_P).extend(lim)
         elif kw == "RORD":
             raise ChemkinError("option RORD is not available (ReactionPolicy_CHEMKIN.hpp:908-913 rejects it)")
         elif kw in ("DUP", "DUPLICATE"):
@@ -488,11 +507,22 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
 
     if r.ford:   # ReorderPairsOfVectors + CleanPairsOfVectors of the orders (ReactionPolicy_CHEMKIN.hpp:1266-1271)
         r.forward_orders = _reorder_clean(r.forward_orders)
-    if pdr == "all" and not i_low:
+    if pdr == "all" and not i_low and not r.cheb:
         raise ChemkinError("no pressure dependence option defined")
     if pdr == "partial" and not i_low:
         raise ChemkinError("no pressure dependence option defined")
-    if not third_body and pdr == "none":
+    if r.cheb:
+        # REACTION_CHEBYSHEV (ReactionPolicy_CHEMKIN.hpp:1299, :1321-1342): its k replaces the Arrhenius one;
+        # no third-body or fall-off factor; default limits 300-2500 K and 0.001-100 atm
+        if i_low:
+            raise ChemkinError("CHEB cannot be combined with LOW")
+        n_, m_ = int(r.cheb[0]), int(r.cheb[1])
+        if n_ * m_ != len(r.cheb) - 2:
+            raise ChemkinError(f"CHEB: expected {n_ * m_} coefficients, given {len(r.cheb) - 2}")
+        r.cheb_T = r.cheb_T or [300., 2500.]
+        r.cheb_P = r.cheb_P or [0.001, 100.]
+        r.tag = TAG_SIMPLE
+    elif not third_body and pdr == "none":
         r.tag = TAG_SIMPLE
     elif third_body:
         r.tag = TAG_THIRDBODY
@@ -543,6 +573,8 @@ def _convert_units(r: Reaction, a_units: str, e_units: str) -> None:
     else:
         r.E *= e_conv
         r.A *= math.pow(1.e3, 1. - sum_lr) / math.pow(a_conv, 1. - sum_lr)
+        if r.cheb:   # ConvertUnits for REACTION_CHEBYSHEV (ReactionPolicy_CHEMKIN.hpp:1409-1412)
+            r.cheb_conv = math.pow(1.e3, 1. - sum_lr) / math.pow(a_conv, 1. - sum_lr)
         if r.plog:
             # PressureLogarithmicRateExpression::Setup (PressureLogarithmicRateExpression.hpp:71-101), with the
             # conversion factors ConvertUnits appends (ReactionPolicy_CHEMKIN.hpp:1460-1465)
@@ -810,6 +842,21 @@ def build_tables(species: List[str], reactions: List[Reaction], thermo: List[The
         A["plog_rxn"] = np.array(prx, np.int32); A["plog_ptr"] = np.array(pptr2, np.int32)
         for k, v in pv.items():
             A["plog_" + k] = np.array(v, f64)
+    if any(r.cheb for r in reactions):
+        # Chebyshev reactions (ChebyshevPolynomialRateExpression::Setup, :50-75): per reaction N, M, the
+        # N x M coefficients by rows and (Tmin, Tmax, log10 Pmin, log10 Pmax, conversion) with P in Pa
+        crx, cnm, cptr, cco, clim = [], [], [0], [], []
+        for j, r in enumerate(reactions):
+            if r.cheb:
+                crx.append(j)
+                cnm += [int(r.cheb[0]), int(r.cheb[1])]
+                cco += list(r.cheb[2:])
+                cptr.append(len(cco))
+                clim += [r.cheb_T[0], r.cheb_T[1], math.log10(r.cheb_P[0] * 101325.),
+                         math.log10(r.cheb_P[1] * 101325.), r.cheb_conv]
+        A["cheb_rxn"] = np.array(crx, np.int32); A["cheb_nm"] = np.array(cnm, np.int32)
+        A["cheb_ptr"] = np.array(cptr, np.int32); A["cheb_coef"] = np.array(cco, f64)
+        A["cheb_lim"] = np.array(clim, f64)
     if any(r.ford for r in reactions):
         # forward rate-law orders (StoichiometricMap lambda lists), only when some reaction has FORD;
         # without them the reactant coefficients are the orders

@@ -240,6 +240,25 @@ struct Reactor {
         kArr[prx[k]] = kk;
       }
     }
+    // Chebyshev reactions, every call (KineticsMap_CHEMKIN.hpp:1332-1339,
+    // ChebyshevPolynomialRateExpression.hpp:93-114 and :187-190)
+    if (m.f.count("cheb_coef")) {
+      const auto& crx = m.I("cheb_rxn"); const auto& cnm = m.I("cheb_nm"); const auto& cptr = m.I("cheb_ptr");
+      const auto& cco = m.F("cheb_coef"); const auto& clim = m.F("cheb_lim");
+      for (size_t k = 0; k < crx.size(); ++k) {
+        const int N = cnm[2 * k], Mm = cnm[2 * k + 1];
+        const double* lim = &clim[5 * k];
+        const double Ttilde = (2. / T - 1. / lim[0] - 1. / lim[1]) / (1. / lim[1] - 1. / lim[0]);
+        const double Ptilde = (2. * std::log10(P_) - lim[2] - lim[3]) / (lim[3] - lim[2]);
+        std::vector<double> phn(N), phm(Mm);
+        for (int n = 1; n <= N; ++n) phn[n - 1] = std::cos(double(n - 1) * std::acos(Ttilde));
+        for (int mm = 1; mm <= Mm; ++mm) phm[mm - 1] = std::cos(double(mm - 1) * std::acos(Ptilde));
+        double sum = 0.;
+        for (int n = 0; n < N; ++n)
+          for (int mm = 0; mm < Mm; ++mm) sum += cco[cptr[k] + n * Mm + mm] * phn[n] * phm[mm];
+        kArr[crx[k]] = std::pow(10., sum) * lim[4];
+      }
+    }
     kMod = kArr;
   }
 

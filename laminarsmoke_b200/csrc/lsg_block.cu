@@ -243,11 +243,12 @@ __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, 
         const double kInf = kinf[fo];
         const double lF = logf[fo];
         const double Pr = kArr * Mc / kInf;
+        const bool cabr = M.I(L.fo_cabr)[fo] != 0;
         double wF = 1.;
         const int ty = M.I(L.fo_type)[fo];
         if (ty == 1) {
           double qq;
-          if (Pr > 1.e-32) {
+          if (Pr > 1.e-32 || cabr) {
             const double nTroe = 0.75 - 1.27 * lF;
             const double cTroe = -0.4 - 0.67 * lF;
             const double sTroe = log10(Pr) + cTroe;
@@ -263,7 +264,9 @@ __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, 
           const double e = M.D(L.fo_e)[fo];
           if (e != 0.) wF *= pow(T, e);
         }
-        kMod *= kInf * (Pr / (1. + Pr)) * wF / kArr;
+        // CABR (KineticsMap_CHEMKIN.hpp:1613-1660): k0 (1 / (1 + Pr)) F; fall-off: k_inf (Pr / (1 + Pr)) F
+        if (cabr) kMod *= (1. / (1. + Pr)) * wF;
+        else kMod *= kInf * (Pr / (1. + Pr)) * wF / kArr;
       }
       double fwd = 1.;
       for (int q = op[j]; q < op[j + 1]; ++q) fwd *= conc_factor_k(onu[q], W.C[osp[q]]);

@@ -41,6 +41,7 @@ struct MechLayout {
   int fr_ptr, fr_rxn;                                        // per species CSR
   int tb_ptr, tb_sp;                                         // third body CSR (by slot)
   int fo_type, fo_single, fo_ptr, fo_sp;                     // fall-off (by slot)
+  int fo_cabr;                                               // 1: chemically activated bimolecular (by slot)
 };
 
 // Views into a flattened table (global or shared memory).

@@ -199,6 +199,14 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
     L.fo_single = B.addi(b.I("fo_single"));
     L.fo_ptr = B.addi(b.I("fo_ptr"));
     L.fo_sp = B.addi(b.I("fo_species"));
+    {
+      std::vector<int> cabr(fr.size() > 0 ? fr.size() : 1, 0);
+      if (b.i.count("fo_cabr")) {
+        if (b.I("fo_cabr").size() != fr.size()) { err = "inconsistent CABR flags in mechanism blob"; return false; }
+        for (size_t k = 0; k < fr.size(); ++k) cabr[k] = b.I("fo_cabr")[k];
+      }
+      L.fo_cabr = B.addi(cabr);
+    }
 
     L.n_tb = (int)tbr.size();
     L.n_fo = (int)fr.size();

@@ -228,13 +228,14 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
         Mc = SC_(C, single) + 1.e-16;
       }
       const double Pr = kArr * Mc / kInf;
+      const bool cabr = M.I(L.fo_cabr)[fo] != 0;
       double wF = 1.;
       if (ty == 1) {
         double v = (1. - a) * exp(-T / b) + a * exp(-T / c);
         if (d != 0.) v += exp(-d / T);
         const double lF = (v < 1.e-300) ? -300. : log10(v);
         double qq;
-        if (Pr > 1.e-32) {
+        if (Pr > 1.e-32 || cabr) {
           const double nTroe = 0.75 - 1.27 * lF;
           const double cTroe = -0.4 - 0.67 * lF;
           const double sTroe = log10(Pr) + cTroe;
@@ -251,7 +252,9 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
         const double e = M.D(L.fo_e)[fo];
         if (e != 0.) wF *= pow(T, e);
       }
-      kMod *= kInf * (Pr / (1. + Pr)) * wF / kArr;
+      // CABR (KineticsMap_CHEMKIN.hpp:1613-1660): k0 (1 / (1 + Pr)) F; fall-off: k_inf (Pr / (1 + Pr)) F
+      if (cabr) kMod *= (1. / (1. + Pr)) * wF;
+      else kMod *= kInf * (Pr / (1. + Pr)) * wF / kArr;
     }
     double fwd = 1.;
     for (int q = op[j]; q < op[j + 1]; ++q) fwd *= conc_factor_r(onu[q], SC_(C, osp[q]));

@@ -256,10 +256,11 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
         const double kInf = W.KINF[fo];
         const double lF = W.LOGF[fo];
         const double Pr = kArr * Mc / kInf;
+        const bool cabr = M.I(L.fo_cabr)[fo] != 0;
         double wF = 1.;
         const int ty = M.I(L.fo_type)[fo];
         if (ty == 1) {
-          if (Pr > 1.e-32) {
+          if (Pr > 1.e-32 || cabr) {
             const double nTroe = 0.75 - 1.27 * lF;
             const double cTroe = -0.4 - 0.67 * lF;
             const double sTroe = log10(Pr) + cTroe;
@@ -276,7 +277,8 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
           const double e = M.D(L.fo_e)[fo];
           if (e != 0.) wF *= pow(T, e);
         }
-        const double corr = kInf * (Pr / (1. + Pr)) * wF / kArr;
+        // CABR (KineticsMap_CHEMKIN.hpp:1613-1660): k0 (1 / (1 + Pr)) F; fall-off: k_inf (Pr / (1 + Pr)) F
+        const double corr = cabr ? (1. / (1. + Pr)) * wF : kInf * (Pr / (1. + Pr)) * wF / kArr;
         kMod *= corr;
       }
       double fwd = 1.;

@@ -278,6 +278,7 @@ class Reaction:
     cheb_T: List[float] = field(default_factory=list)  # TCHEB (Tmin, Tmax) [K]
     cheb_P: List[float] = field(default_factory=list)  # PCHEB (Pmin, Pmax) [atm]
     cheb_conv: float = 1.0
+    cabr: bool = False   # HIGH given: chemically activated bimolecular reaction (k0 on the line, k_inf in HIGH)
     forward_orders: List[Tuple[int, float]] = field(default_factory=list)
     text: str = ""
 
@@ -412,7 +413,7 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
     r.reactants = to_idx(left)
     r.products = to_idx(right)
 
-    i_low = i_troe = i_sri = i_lind = False
+    i_low = i_troe = i_sri = i_lind = i_high = False
     for line in lines[1:]:
         k = line.find("/")
         keyword = line[:k].strip() if k >= 0 else line.split()[0]
@@ -444,6 +445,19 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
             r.A, r.beta, r.E = c
             if r.A_inf < 0.:
                 raise ChemkinError("negative frequency factor in LOW reaction")
+        elif kw == "HIGH":
+            # ReactionPolicy_CHEMKIN.hpp:553-575: the high-pressure limit of a chemically activated
+            # bimolecular (CABR) reaction; the reaction line keeps the low-pressure k0
+            if pdr == "none":
+                raise ChemkinError("HIGH only for pressure-dependent reactions")
+            if i_low or r.cheb or r.plog:
+                raise ChemkinError("HIGH cannot be combined with LOW/CHEB/PLOG")
+            c = _slash_numbers(line, (3,), "HIGH")
+            i_high = True
+            if not i_troe and not i_sri:
+                i_lind = True
+            r.A_inf, r.beta_inf, r.E_inf = c
+            r.cabr = True
         elif kw == "TROE":
             if pdr == "none":
                 raise ChemkinError("TROE only for pressure-dependent reactions")
@@ -507,9 +521,9 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
 
     if r.ford:   # ReorderPairsOfVectors + CleanPairsOfVectors of the orders (ReactionPolicy_CHEMKIN.hpp:1266-1271)
         r.forward_orders = _reorder_clean(r.forward_orders)
-    if pdr == "all" and not i_low and not r.cheb:
+    if pdr == "all" and not i_low and not i_high and not r.cheb:
         raise ChemkinError("no pressure dependence option defined")
-    if pdr == "partial" and not i_low:
+    if pdr == "partial" and not i_low and not i_high:
         raise ChemkinError("no pressure dependence option defined")
     if r.cheb:
         # REACTION_CHEBYSHEV (ReactionPolicy_CHEMKIN.hpp:1299, :1321-1342): its k replaces the Arrhenius one;
@@ -526,11 +540,11 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
         r.tag = TAG_SIMPLE
     elif third_body:
         r.tag = TAG_THIRDBODY
-    elif i_lind and i_low:
+    elif i_lind and (i_low or i_high):
         r.tag = TAG_LINDEMANN
-    elif i_troe and i_low:
+    elif i_troe and (i_low or i_high):
         r.tag = TAG_TROE
-    elif i_sri and i_low:
+    elif i_sri and (i_low or i_high):
         r.tag = TAG_SRI
     else:
         raise ChemkinError("unsupported pressure-dependent form")
@@ -563,7 +577,14 @@ def _convert_units(r: Reaction, a_units: str, e_units: str) -> None:
         sum_lr += 1.
         if r.reversible:
             sum_lp += 1.
-    if r.tag in FALLOFF_TAGS:
+    if r.tag in FALLOFF_TAGS and r.cabr:   # ConvertUnits, CABR branch (ReactionPolicy_CHEMKIN.hpp:1395-1407)
+        r.E *= e_conv
+        r.E_inf *= e_conv
+        r.A *= math.pow(1.e3, 1. - sum_lr) / math.pow(a_conv, 1. - sum_lr)
+        r.A_inf *= math.pow(1.e3, 2. - sum_lr) / math.pow(a_conv, 2. - sum_lr)
+        if r.explicit_rev:
+            raise ChemkinError("explicitly reversible CABR reactions are not allowed")
+    elif r.tag in FALLOFF_TAGS:
         r.E *= e_conv
         r.E_inf *= e_conv
         r.A *= math.pow(1.e3, -sum_lr) / math.pow(a_conv, -sum_lr)
@@ -814,6 +835,8 @@ def build_tables(species: List[str], reactions: List[Reaction], thermo: List[The
     A["fo_ptr"] = np.array(fptr, np.int32)
     A["fo_species"] = np.array(fsp, np.int32)
     A["fo_eff_m1"] = np.array(feff, f64)
+    if any(reactions[j].cabr for j in fo):   # chemically activated bimolecular slots, only when present
+        A["fo_cabr"] = np.array([1 if reactions[j].cabr else 0 for j in fo], np.int32)
 
     # --- stoichiometry per reaction (species ascending; merged)
     rptr, rsp, rnu = [0], [], []

@@ -287,9 +287,10 @@ struct Reactor {
       }
       const int j = fr[k];
       const double Pr = kArr[j] * M / kInf[k];
+      const bool cabr = m.i.count("fo_cabr") && m.I("fo_cabr")[k] != 0;
       double wF = 1.;
       if (fty[k] == 1) {
-        if (Pr > 1.e-32) {
+        if (Pr > 1.e-32 || cabr) {   // ChemicallyActivatedBimolecularReactions has no small-Pr branch
           const double nTroe = 0.75 - 1.27 * logFcent[k];
           const double cTroe = -0.4 - 0.67 * logFcent[k];
           const double sTroe = std::log10(Pr) + cTroe;
@@ -305,7 +306,8 @@ struct Reactor {
         wF = std::pow(logFcent[k], xSRI) * fd[k];
         if (fee[k] != 0.) wF *= std::pow(T_, fee[k]);
       }
-      corr[k] = kInf[k] * (Pr / (1. + Pr)) * wF / kArr[j];
+      // KineticsMap_CHEMKIN::ChemicallyActivatedBimolecularReactions (:1613-1660): correction_cabr = F / (1 + Pr)
+      corr[k] = cabr ? (1. / (1. + Pr)) * wF : kInf[k] * (Pr / (1. + Pr)) * wF / kArr[j];
     }
     for (size_t k = 0; k < fr.size(); ++k) kMod[fr[k]] *= corr[k];
 

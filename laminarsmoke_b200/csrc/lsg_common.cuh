@@ -36,7 +36,7 @@ __device__ __forceinline__ double seq_sum(double v, int n) {
 // PressureLogarithmicRateExpression.hpp:104-119): the first or last point
 // outside the tabulated pressures, else ln k interpolated linearly in ln P
 // between the two points that bracket P.
-__device__ __forceinline__ double plog_k(const MechView& M, const MechLayout& L, int slot, double T, double logT,
+static __device__ __noinline__ double plog_k(const MechView& M, const MechLayout& L, int slot, double T, double logT,
                                          double P) {
   const int a = M.I(L.plog_ptr)[slot], b = M.I(L.plog_ptr)[slot + 1];
   const double* p = M.D(L.plog_p);
@@ -59,7 +59,7 @@ __device__ __forceinline__ double plog_k(const MechView& M, const MechLayout& L,
 // Phi(n, x) = cos((n - 1) acos(x)), :187-190): 10^(sum_nm a_nm phi_n(T~) phi_m(P~))
 // times the unit conversion, T~ and P~ the reduced inverse temperature and
 // log10 pressure.  Outside the limits acos is undefined, as in the reference.
-__device__ __forceinline__ double cheb_k(const MechView& M, const MechLayout& L, int slot, double T, double P) {
+static __device__ __noinline__ double cheb_k(const MechView& M, const MechLayout& L, int slot, double T, double P) {
   const int N = M.I(L.cheb_nm)[2 * slot], Mm = M.I(L.cheb_nm)[2 * slot + 1];
   const double* a = M.D(L.cheb_coef) + M.I(L.cheb_ptr)[slot];
   const double* lim = M.D(L.cheb_lim) + 5 * slot;

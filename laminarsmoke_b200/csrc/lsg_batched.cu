@@ -443,7 +443,7 @@ batched_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem, StepO
   double oldCC = 0.;
   int jcol = 0;
   double hf = 0., hJ = 0.;
-  unsigned cnt[NCNT];
+  unsigned cnt[NCNT] = {};
   double pendHScale = 0.;
   double pendHr0 = 0.;
   enum : int { H_DEC = 0, H_CONST = 1, H_INC = 2 };

@@ -111,8 +111,6 @@ __device__ __forceinline__ double conc_factor_r(double nu, double c1) {
   return pow(c1, nu);
 }
 
-__device__ __forceinline__ double lo_b(int k, int NC, double yminT) { return k < NC ? 0. : yminT; }
-__device__ __forceinline__ double hi_b(int k, int NC, double ymaxT) { return k < NC ? 1. : ymaxT; }
 
 // ---------------------------------------------------------------------------
 // Thread-serial RHS of the constant-pressure reactor

@@ -356,6 +356,22 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                "h2d_bytes_per_step": int(8 * (nc + 1) * n),
                "d2h_bytes_per_step": int(8 * (nc + 1) * n + 8 * n + 4 * n + 4 * n)}
 
+    # the metric's accuracy condition, checked at full size outside the timed region: the last timed step's
+    # result against the plain FP64 form (the reference method's operation order) on the same cells
+    accuracy = None
+    if rank == 0 and args.form == "mixed":
+        Yp = Y0.clone()
+        Tp = T0.clone()
+        plain.step_device(Yp, Tp, DT)
+        torch.cuda.synchronize()
+        plain.check()
+        dY = (Yw - Yp).abs().amax(dim=0)
+        accuracy = {"against": "plain FP64 form, same cells, same step",
+                    "max_rel_T": float(((Tw - Tp).abs() / Tp).max()),
+                    "max_abs_Y": float(dY.max()),
+                    "cells_within_abs_Y_1e-9": float((dY <= 1e-9).double().mean())}
+        del Yp, Tp
+
     flops, nsteps_total = work_model(arrays, counters)
     out = None
     if rank == 0:
@@ -390,6 +406,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                           "bdf_steps_per_cell": nsteps_total / n,
                           "transcendental_flops_each": TRANSCENDENTAL_FLOPS},
             "statuses": {str(k): int(v) for k, v in zip(*np.unique(st, return_counts=True))},
+            "accuracy": accuracy,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,

@@ -13,7 +13,15 @@ expected outputs.  Inputs are seeded (numpy PCG64, seeds below):
 * h2co_edge.npz     -- 4 cells: T at tmin_chem (skipped), a cold frozen
                        mixture, a hot equilibrium-near state, a 1 us step;
 * h2co45_step.npz   -- 32 cells of the H2/CO chemistry padded with 30 inert
-                       species (45 components, the block-per-cell form).
+                       species (45 components, the block-per-cell form);
+* h2co_cv_step.npz  -- 64 cells of the constant-volume reactor at their own
+                       densities;
+* h2co_sources.npz  -- compact-scheme sources of the h2co_step cells and the
+                       steady solvers' linearised sources of 32 states;
+* ch4_1step.npz     -- 64 cells of the global one-step CH4 mechanism (FORD);
+* rateforms_rhs.npz -- RHS of the PLOG, Chebyshev and CABR test mechanisms
+                       (tests/test_plog.py, test_cheb.py, test_cabr.py) at
+                       32 states and three pressures each.
 """
 import os
 import sys
@@ -70,6 +78,52 @@ def main():
     Yo, To, Qo, sto, cnt = OracleMechanism(data45).reaction_step(Y, T, 1e-5, nthreads=1)
     np.savez_compressed(os.path.join(HERE, "h2co45_step.npz"), Y0=Y, T0=T, dt=1e-5, Y=Yo, T=To, Q=Qo,
                         status=sto, counters=cnt)
+
+    Y, T = cells.h2co_mixing(species, A["mw"], 64, seed=34)
+    Y = Y / Y.sum(axis=1, keepdims=True)
+    rho = np.random.default_rng(35).uniform(0.5, 2.0, 64) * 101325.0 / ((Y / A["mw"]).sum(axis=1) * 8314.4621 * T)
+    Yo, To, Qo, sto, cnt = orc.reaction_step(Y, T, 1e-5, nthreads=1, rho=rho)
+    np.savez_compressed(os.path.join(HERE, "h2co_cv_step.npz"), Y0=Y, T0=T, rho=rho, dt=1e-5, Y=Yo, T=To, Q=Qo,
+                        status=sto, counters=cnt)
+
+    g = np.load(os.path.join(HERE, "h2co_step.npz"))
+    RR, RT = orc.compact_sources(g["Y0"], g["T0"], g["Y"], g["T"], 1e-5)
+    Y, T = cells.h2co_mixing(species, A["mw"], 32, seed=36)
+    ys = np.concatenate([Y, T[:, None]], axis=1)
+    si = np.zeros_like(ys)
+    se = np.zeros_like(ys)
+    for k in range(32):
+        si[k], se[k] = orc.steady_sources(ys[k], 1.5e5)
+    np.savez_compressed(os.path.join(HERE, "h2co_sources.npz"), RR=RR, RT=RT, y=ys, p=1.5e5, S_implicit=si,
+                        S_explicit=se)
+
+    d1, sp1 = mech.load("ch4_1step")
+    A1, _ = blob.unpack(d1)
+    rng = np.random.default_rng(37)
+    Y = rng.uniform(0.0, 1.0, (64, len(sp1)))
+    Y /= Y.sum(axis=1, keepdims=True)
+    T = rng.uniform(900.0, 2200.0, 64)
+    Yo, To, Qo, sto, cnt = OracleMechanism(d1).reaction_step(Y, T, 1e-5, nthreads=1)
+    np.savez_compressed(os.path.join(HERE, "ch4_1step.npz"), Y0=Y, T0=T, dt=1e-5, Y=Yo, T=To, Q=Qo,
+                        status=sto, counters=cnt)
+
+    sys.path.insert(0, os.path.dirname(HERE))
+    import test_cabr
+    import test_cheb
+    import test_plog
+    out = {}
+    for name, (dm, mm) in (("plog", test_plog.plog_mechanism()), ("cheb", test_cheb.cheb_mechanism()),
+                           ("cabr", test_cabr.cabr_mechanism(troe=True))):
+        o = OracleMechanism(dm)
+        rng = np.random.default_rng(38)
+        Y = rng.uniform(0.0, 1.0, (32, mm.n_species))
+        Y /= Y.sum(axis=1, keepdims=True)
+        T = rng.uniform(700.0, 2400.0, 32)
+        ys = np.concatenate([Y, T[:, None]], axis=1)
+        for patm in (0.3, 2.0, 20.0):
+            out[f"{name}_y"] = ys
+            out[f"{name}_dy_{patm}"] = np.array([o.rhs(ys[k], patm * 101325.0)[0] for k in range(32)])
+    np.savez_compressed(os.path.join(HERE, "rateforms_rhs.npz"), **out)
 
 
 if __name__ == "__main__":

@@ -48,6 +48,55 @@ def test_oracle_step_golden(oracle_h2co, name):
     np.testing.assert_allclose(Q, g["Q"], rtol=1e-12, atol=1e-9)
 
 
+def test_oracle_cv_step_golden(oracle_h2co):
+    g = _load("h2co_cv_step.npz")
+    Y, T, Q, st, cnt = oracle_h2co.reaction_step(g["Y0"], g["T0"], float(g["dt"]), nthreads=1, rho=g["rho"])
+    np.testing.assert_array_equal(st, g["status"])
+    np.testing.assert_array_equal(cnt, g["counters"])
+    np.testing.assert_allclose(T, g["T"], rtol=1e-13)
+    np.testing.assert_allclose(Y, g["Y"], rtol=1e-12, atol=1e-18)
+    np.testing.assert_allclose(Q, g["Q"], rtol=1e-12, atol=1e-9)
+
+
+def test_oracle_sources_golden(oracle_h2co):
+    s = _load("h2co_step.npz")
+    g = _load("h2co_sources.npz")
+    RR, RT = oracle_h2co.compact_sources(s["Y0"], s["T0"], s["Y"], s["T"], 1e-5)
+    np.testing.assert_allclose(RR, g["RR"], rtol=1e-13, atol=1e-300)
+    np.testing.assert_allclose(RT, g["RT"], rtol=1e-13, atol=1e-300)
+    for k in range(g["y"].shape[0]):
+        si, se = oracle_h2co.steady_sources(g["y"][k], float(g["p"]))
+        np.testing.assert_allclose(si, g["S_implicit"][k], rtol=1e-12, atol=1e-300)
+        np.testing.assert_allclose(se, g["S_explicit"][k], rtol=1e-12, atol=1e-300)
+
+
+def test_oracle_global_ford_golden():
+    from laminarsmoke_b200 import mech
+    from oracle.oracle import OracleMechanism
+    g = _load("ch4_1step.npz")
+    Y, T, Q, st, cnt = OracleMechanism(mech.load("ch4_1step")[0]).reaction_step(
+        g["Y0"], g["T0"], float(g["dt"]), nthreads=1)
+    np.testing.assert_array_equal(st, g["status"])
+    np.testing.assert_array_equal(cnt, g["counters"])
+    np.testing.assert_allclose(T, g["T"], rtol=1e-13)
+    np.testing.assert_allclose(Y, g["Y"], rtol=1e-12, atol=1e-18)
+
+
+def test_oracle_rateforms_golden():
+    import test_cabr
+    import test_cheb
+    import test_plog
+    from oracle.oracle import OracleMechanism
+    g = _load("rateforms_rhs.npz")
+    for name, (dm, _) in (("plog", test_plog.plog_mechanism()), ("cheb", test_cheb.cheb_mechanism()),
+                          ("cabr", test_cabr.cabr_mechanism(troe=True))):
+        o = OracleMechanism(dm)
+        ys = g[f"{name}_y"]
+        for patm in (0.3, 2.0, 20.0):
+            dy = np.array([o.rhs(ys[k], patm * 101325.0)[0] for k in range(ys.shape[0])])
+            np.testing.assert_allclose(dy, g[f"{name}_dy_{patm}"], rtol=1e-13, atol=1e-300, err_msg=name)
+
+
 # ---- the library against the fixtures (GPU) ----
 
 def _gpu_step(data, g, **kw):

@@ -258,6 +258,55 @@ int lsg_steady_sources_device(lsg_ctx* ctx, int ncells, int nspecies, const doub
                               long ld, const double* p_dev, double p_scalar, double* S_implicit_dev,
                               double* S_explicit_dev, long lds, void* stream);
 
+/* ---- property update after the step ----------------------------------------
+ * What solvers/laminarSMOKE/properties.H:40-190 evaluates per cell after each
+ * reaction step, from the mechanism's fitted transport data (a blob compiled
+ * with a CHEMKIN transport file; TransportPropertiesMap_CHEMKIN.hpp):
+ * mole fractions, cTot, psi, h, mu (Wilke), lambda (Mathur-Saxena), cp, cv,
+ * species cp, diffusion coefficients and thermal-diffusion (Soret) terms.
+ * Every field pointer may be NULL (not written).  Species fields are
+ * species-major [nspecies * ld_out]; Dsoret is [n_thermal_diffusion * ld_out]
+ * in the order lsg_mech_transport_info returns. */
+typedef struct lsg_property_fields {
+  double* X;           /* mole fractions */
+  double* cTot;        /* [kmol/m3] */
+  double* psi;         /* compressibility MWmix / (R T) [s2/m2] */
+  double* mu;          /* dynamic viscosity [kg/m/s] */
+  double* lambda;      /* thermal conductivity [W/m/K] (energy or Lewis) */
+  double* cp;          /* [J/kg/K] (energy or Lewis) */
+  double* cv;          /* [J/kg/K] (energy or Lewis) */
+  double* h;           /* [J/kg] */
+  double* MWmix;       /* [kg/kmol] */
+  double* cp_species;  /* species cp [J/kg/K] (energy or Lewis; the reference's iMassDiffusionInEnergyEquation) */
+  double* Dmix;        /* diffusion coefficients [m2/s]; NULL: not evaluated */
+  double* Dsoret;      /* Dmix_i theta_i MW_i / MWmix of the light species [m2/s]; needs Dmix */
+} lsg_property_fields;
+
+typedef struct lsg_property_options {
+  int energy;                  /* energyEquation: lambda, cp, cv and species cp are evaluated */
+  int simplified_transport;    /* simplifiedTransportProperties: mu0 (T/300)^0.6759, lambda = mu cp / 0.7 */
+  const double* lewis;         /* nspecies Lewis numbers (device for _device, host for the host call), or
+                                  NULL: mixture-averaged diffusivities (the reference's MULTICOMPONENT) */
+} lsg_property_options;
+
+/* Transport data of a mechanism: has_transport 0/1; n_thermal_diffusion light
+ * species (MW <= 20) get Soret terms; their species indices go to indices
+ * (NULL, or room for nspecies ints). */
+int lsg_mech_transport_info(const lsg_mech* mech, int* has_transport, int* n_thermal_diffusion, int* indices);
+
+/* Device arrays: Y_dev [nspecies * ld], T_dev [ncells], p_dev [ncells] or NULL
+ * with p_scalar.  LSG_ERR_UNSUPPORTED when the mechanism has no transport data
+ * or more species than one block's shared memory holds (about 200). */
+int lsg_properties_device(lsg_ctx* ctx, int ncells, int nspecies, const double* Y_dev, const double* T_dev,
+                          long ld, const double* p_dev, double p_scalar, const lsg_property_options* opt,
+                          const lsg_property_fields* out_dev, long ld_out, void* stream);
+
+/* The same from host arrays (ld = ld_out = ncells): the inputs go to the device,
+ * the kernel runs, the requested fields come back; synchronous.  Uses
+ * context-owned device scratch. */
+int lsg_properties(lsg_ctx* ctx, int ncells, int nspecies, const double* Y, const double* T, const double* p,
+                   double p_scalar, const lsg_property_options* opt, const lsg_property_fields* out);
+
 const char* lsg_strerror(int code);
 int lsg_abi_version(void);
 

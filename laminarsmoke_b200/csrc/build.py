@@ -1,6 +1,6 @@
 """Build the B200 library liblsmoke_gpu.so in-tree with nvcc (sm_100a).
 
-The plain FP64 kernels and the output-field kernels are compiled with FMA
+The plain FP64 kernels, the output-field kernels and the property kernel are compiled with FMA
 contraction off so their arithmetic rounds like the CPU reference; everything
 else is compiled normally.
 """
@@ -23,6 +23,7 @@ UNITS = [
     ("lsg_rounds.cu", []),
     ("lsg_block.cu", []),
     ("lsg_outputs.cu", ["-fmad=false"]),
+    ("lsg_properties.cu", ["-fmad=false"]),
     ("lsg_api.cu", []),
     ("lsg_mech_host.cpp", []),
 ]

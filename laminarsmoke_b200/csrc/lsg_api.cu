@@ -20,6 +20,7 @@ struct lsg_mech {
   HostMech host;
   int device = 0;
   unsigned char* d_buf = nullptr;
+  unsigned char* d_tr = nullptr;   // transport table, when the blob has one
 };
 
 struct lsg_ctx {
@@ -487,6 +488,21 @@ int lsg_mech_load_blob(const void* blob, size_t nbytes, int device, lsg_mech** o
     delete m;
     return LSG_ERR_CUDA;
   }
+  if (m->host.has_transport) {
+    const size_t nb = m->host.tbuffer.size();
+    if (cudaMalloc(&m->d_tr, nb) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(m->d_buf);
+      delete m;
+      return LSG_ERR_NOMEM;
+    }
+    if (cudaMemcpy(m->d_tr, m->host.tbuffer.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaFree(m->d_tr);
+      cudaFree(m->d_buf);
+      delete m;
+      return LSG_ERR_CUDA;
+    }
+  }
   *out = m;
   return LSG_OK;
 }
@@ -510,6 +526,7 @@ int lsg_mech_destroy(lsg_mech* m) {
   if (!m) return LSG_OK;
   cudaSetDevice(m->device);
   cudaFree(m->d_buf);
+  cudaFree(m->d_tr);
   delete m;
   return LSG_OK;
 }
@@ -838,6 +855,114 @@ int lsg_formation_rates_device(lsg_ctx* c, int ncells, int nspecies, const doubl
   if (launch_formation_rates(L, c->mech->d_buf, ncells, y, dy, p, out, ld_out, sm_count(c), s) != cudaSuccess)
     return LSG_ERR_CUDA;
   ++c->launches;
+  return LSG_OK;
+}
+
+int lsg_mech_transport_info(const lsg_mech* m, int* has_transport, int* n_thermal_diffusion, int* indices) {
+  if (!m) return LSG_ERR_ARG;
+  if (has_transport) *has_transport = m->host.has_transport ? 1 : 0;
+  if (n_thermal_diffusion) *n_thermal_diffusion = (int)m->host.iteta.size();
+  if (indices)
+    for (size_t i = 0; i < m->host.iteta.size(); ++i) indices[i] = m->host.iteta[i];
+  return LSG_OK;
+}
+
+int lsg_properties_device(lsg_ctx* c, int ncells, int nspecies, const double* Y, const double* T, long ld,
+                          const double* p, double p_scalar, const lsg_property_options* opt,
+                          const lsg_property_fields* out, long ld_out, void* stream) {
+  if (!c || !opt || !out || ncells < 0 || !Y || !T || ld < ncells || ld_out < ncells) return LSG_ERR_ARG;
+  if (!p && !(p_scalar > 0.)) return LSG_ERR_ARG;
+  if (out->Dsoret && !out->Dmix) return LSG_ERR_ARG;
+  const lsg_mech* m = c->mech;
+  const MechLayout& L = m->host.layout;
+  if (nspecies != L.nc) return LSG_ERR_ARG;
+  if (!m->host.has_transport || properties_block(L.nc) == 0) return LSG_ERR_UNSUPPORTED;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  PropArgs a{};
+  a.ncells = ncells;
+  a.Y = Y;
+  a.T = T;
+  a.ld = ld;
+  a.p = p;
+  a.p_scalar = p_scalar;
+  a.energy = opt->energy ? 1 : 0;
+  a.simplified = opt->simplified_transport ? 1 : 0;
+  a.lewis = opt->lewis;
+  a.X = out->X;
+  a.cTot = out->cTot;
+  a.psi = out->psi;
+  a.mu = out->mu;
+  a.lambda = out->lambda;
+  a.cp = out->cp;
+  a.cv = out->cv;
+  a.h = out->h;
+  a.MWmix = out->MWmix;
+  a.cp_species = out->cp_species;
+  a.Dmix = out->Dmix;
+  a.Dsoret = out->Dsoret;
+  a.ld_out = ld_out;
+  if (launch_properties(L, m->d_buf, m->host.tlayout, m->d_tr, a, (cudaStream_t)stream) != cudaSuccess)
+    return LSG_ERR_CUDA;
+  ++c->launches;
+  return LSG_OK;
+}
+
+int lsg_properties(lsg_ctx* c, int ncells, int nspecies, const double* Y, const double* T, const double* p,
+                   double p_scalar, const lsg_property_options* opt, const lsg_property_fields* out) {
+  if (!c || !opt || !out || ncells < 0 || !Y || !T) return LSG_ERR_ARG;
+  if (!p && !(p_scalar > 0.)) return LSG_ERR_ARG;
+  if (out->Dsoret && !out->Dmix) return LSG_ERR_ARG;
+  const lsg_mech* m = c->mech;
+  const int nc = m->host.layout.nc;
+  if (nspecies != nc) return LSG_ERR_ARG;
+  if (!m->host.has_transport || properties_block(nc) == 0) return LSG_ERR_UNSUPPORTED;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  const long n = ncells;
+  const long nt = (long)m->host.iteta.size();
+  // device scratch: inputs, then one slot per requested field
+  double* const hp[12] = {out->X, out->cTot, out->psi, out->mu, out->lambda, out->cp, out->cv, out->h,
+                          out->MWmix, out->cp_species, out->Dmix, out->Dsoret};
+  const long rows[12] = {nc, 1, 1, 1, 1, 1, 1, 1, 1, nc, nc, nt};
+  long need = (long)nc * n + 2 * n + nc;
+  for (int f = 0; f < 12; ++f)
+    if (hp[f]) need += rows[f] * n;
+  const cudaStream_t s = c->stream;
+  if (need > c->frs_cap) {
+    if (cudaStreamSynchronize(s) != cudaSuccess) return LSG_ERR_CUDA;
+    cudaFree(c->frs);
+    c->frs = nullptr;
+    c->frs_cap = 0;
+    if (cudaMalloc(&c->frs, sizeof(double) * need) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+    c->frs_cap = need;
+  }
+  double* dY = c->frs;
+  double* dT = dY + (long)nc * n;
+  double* dp = dT + n;
+  double* dLe = dp + n;
+  double* cur = dLe + nc;
+  double* dev[12] = {};
+  for (int f = 0; f < 12; ++f)
+    if (hp[f]) {
+      dev[f] = cur;
+      cur += rows[f] * n;
+    }
+  if (cudaMemcpyAsync(dY, Y, sizeof(double) * nc * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(dT, T, sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      (p && cudaMemcpyAsync(dp, p, sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+      (opt->lewis && cudaMemcpyAsync(dLe, opt->lewis, sizeof(double) * nc, cudaMemcpyHostToDevice, s) != cudaSuccess))
+    return LSG_ERR_CUDA;
+  lsg_property_options o = *opt;
+  o.lewis = opt->lewis ? dLe : nullptr;
+  const lsg_property_fields fd{dev[0], dev[1], dev[2], dev[3], dev[4],  dev[5],
+                               dev[6], dev[7], dev[8], dev[9], dev[10], dev[11]};
+  const int r = lsg_properties_device(c, ncells, nspecies, dY, dT, n, p ? dp : nullptr, p_scalar, &o, &fd, n, s);
+  if (r != LSG_OK) return r;
+  for (int f = 0; f < 12; ++f)
+    if (hp[f] && cudaMemcpyAsync(hp[f], dev[f], sizeof(double) * rows[f] * n, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      return LSG_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return LSG_ERR_CUDA;
   return LSG_OK;
 }
 

@@ -142,4 +142,24 @@ cudaError_t launch_formation_rates(const MechLayout& L, const unsigned char* mec
                                    const double* y, const double* dy, double p, double* out, long ld_out,
                                    int sm_count, cudaStream_t stream);
 
+// ---- property update after the step (lsg_properties.cu)
+struct PropArgs {
+  long ncells;
+  const double* Y;       // [nc][ld]
+  const double* T;       // [ncells]
+  long ld;
+  const double* p;       // [ncells] or null: p_scalar everywhere
+  double p_scalar;
+  int energy;            // lambda, cp, cv and the species cp are evaluated
+  int simplified;        // mu = mu0 (T/T0)^beta0, lambda = mu cp / Pr0
+  const double* lewis;   // [nc] Lewis numbers (device) or null: mixture-averaged diffusivities
+  double *X, *cTot, *psi, *mu, *lambda, *cp, *cv, *h, *MWmix;   // null: not written
+  double *cp_species, *Dmix, *Dsoret;                            // [nc|n_teta][ld_out], null: not evaluated
+  long ld_out;
+};
+// Largest cells-per-block the property kernel can run for nc species (0: too many species).
+int properties_block(int nc);
+cudaError_t launch_properties(const MechLayout& L, const unsigned char* mech_gmem, const TransportLayout& TL,
+                              const unsigned char* tr_gmem, const PropArgs& a, cudaStream_t stream);
+
 }  // namespace lsg

@@ -44,6 +44,24 @@ struct MechLayout {
   int fo_cabr;                                               // 1: chemically activated bimolecular (by slot)
 };
 
+// Fitted transport properties (the packed blob's tr_* arrays), flattened into
+// a table of their own: [double region][int region], offsets in elements.
+// Only the property update reads it, so the kinetics table stays as small as
+// the reaction kernels need.
+struct TransportLayout {
+  int nc, n_pair, n_teta;     // species, pairs j < k, light species with thermal-diffusion ratios
+  int n_double, n_int;
+  uint32_t bytes;
+  // ---- double region
+  int eta, lam;               // [nc][4]: ln(eta), ln(lambda) in powers of ln T
+  int gam;                    // [n_pair][4]: ln(D_jk P) [m2/s bar] in powers of ln T, pairs j < k row by row
+  int teta;                   // [n_teta][nc][4]: theta_ij in powers of T
+  int wilke_phi;              // [nc][nc]: 1 / sqrt(8 (1 + M_k / M_j))
+  int wilke_r14;              // [nc][nc]: (M_j / M_k)^(1/4)
+  // ---- int region
+  int iteta;                  // [n_teta] species index of each light species
+};
+
 // Views into a flattened table (global or shared memory).
 struct MechView {
   const double* d;

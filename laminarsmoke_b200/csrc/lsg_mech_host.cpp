@@ -1,6 +1,7 @@
 // Host side: packed blob (named arrays) -> flattened device table (lsg_mech.h).
 #include "lsg_mech_host.h"
 
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <stdexcept>
@@ -74,6 +75,60 @@ struct Builder {
   }
 };
 }  // namespace
+
+// The transport fits, when the blob has them, with the Wilke factors of every
+// species pair (TransportPropertiesMap_CHEMKIN.hpp:653-688) precomputed.
+static bool build_transport(const Blob& b, int nc, HostMech& out, std::string& err) {
+  out.has_transport = false;
+  out.tbuffer.clear();
+  out.iteta.clear();
+  if (!b.f.count("tr_eta")) return true;
+  const auto& eta = b.F("tr_eta");
+  const auto& lam = b.F("tr_lambda");
+  const auto& gam = b.F("tr_gamma");
+  const auto& teta = b.F("tr_teta");
+  const auto& it = b.I("tr_iteta");
+  const long npair = (long)nc * (nc - 1) / 2;
+  const long nt = (long)it.size();
+  if ((long)eta.size() != 4L * nc || (long)lam.size() != 4L * nc || (long)gam.size() != 4 * npair ||
+      (long)teta.size() != 4 * nt * nc) {
+    err = "inconsistent transport arrays in mechanism blob";
+    return false;
+  }
+  for (int v : it)
+    if (v < 0 || v >= nc) { err = "transport species index out of range in mechanism blob"; return false; }
+  const std::vector<double>& M = out.mw;
+  std::vector<double> phi((size_t)nc * nc, 0.), r14((size_t)nc * nc, 0.);
+  for (int k = 0; k < nc; ++k)
+    for (int j = 0; j < nc; ++j) {
+      phi[(size_t)k * nc + j] = 1. / std::sqrt(8. * (1. + M[k] / M[j]));
+      r14[(size_t)k * nc + j] = std::sqrt(std::sqrt(M[j] / M[k]));
+    }
+  TransportLayout T{};
+  T.nc = nc;
+  T.n_pair = (int)npair;
+  T.n_teta = (int)nt;
+  Builder B;
+  T.eta = B.addd(eta);
+  T.lam = B.addd(lam);
+  T.gam = B.addd(gam.empty() ? std::vector<double>(2, 0.) : gam);
+  T.teta = B.addd(teta.empty() ? std::vector<double>(2, 0.) : teta);
+  T.wilke_phi = B.addd(phi);
+  T.wilke_r14 = B.addd(r14);
+  T.iteta = B.addi(it.empty() ? std::vector<int>(1, 0) : it);
+  while (B.d.size() % 2) B.d.push_back(0.);
+  while (B.iv.size() % 4) B.iv.push_back(0);
+  T.n_double = (int)B.d.size();
+  T.n_int = (int)B.iv.size();
+  T.bytes = (uint32_t)(B.d.size() * sizeof(double) + B.iv.size() * sizeof(int));
+  out.tbuffer.resize(T.bytes);
+  std::memcpy(out.tbuffer.data(), B.d.data(), B.d.size() * sizeof(double));
+  std::memcpy(out.tbuffer.data() + B.d.size() * sizeof(double), B.iv.data(), B.iv.size() * sizeof(int));
+  out.tlayout = T;
+  out.iteta = it;
+  out.has_transport = true;
+  return true;
+}
 
 bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string& err) {
   Blob b;
@@ -255,6 +310,7 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
       else cur.push_back((char)ch);
     }
     out.mw = b.F("mw");
+    if (!build_transport(b, nc, out, err)) return false;
   } catch (const std::exception& e) {
     err = e.what();
     return false;

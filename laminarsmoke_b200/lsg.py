@@ -49,7 +49,19 @@ EXPORTS = (
     "lsg_reaction_step_device_noalloc", "lsg_ctx_kernel_times", "lsg_ctx_tuning",
     "lsg_compact_sources_device", "lsg_formation_rates_device",
     "lsg_reaction_step_cv", "lsg_reaction_step_cv_device", "lsg_steady_sources_device",
+    "lsg_mech_transport_info", "lsg_properties_device", "lsg_properties",
 )
+
+# lsg_property_fields, in declaration order: species rows (nc), scalars, light-species rows
+PROPERTY_FIELDS = ("X", "cTot", "psi", "mu", "lambda", "cp", "cv", "h", "MWmix", "cp_species", "Dmix", "Dsoret")
+
+
+class PropertyFields(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in PROPERTY_FIELDS]
+
+
+class PropertyOptions(C.Structure):
+    _fields_ = [("energy", C.c_int), ("simplified_transport", C.c_int), ("lewis", C.c_void_p)]
 
 _lib = None
 
@@ -91,6 +103,10 @@ def lib():
     L.lsg_steady_sources_device.argtypes = [vp, i, i, vp, vp, l, vp, d, vp, vp, l, vp]
     L.lsg_compact_sources_device.argtypes = [vp, i, i, vp, vp, vp, vp, l, d, vp, d, vp, vp, vp]
     L.lsg_formation_rates_device.argtypes = [vp, i, i, vp, vp, l, d, vp, l, vp]
+    L.lsg_mech_transport_info.argtypes = [vp, C.POINTER(i), C.POINTER(i), vp]
+    L.lsg_properties_device.argtypes = [vp, i, i, vp, vp, l, vp, d, C.POINTER(PropertyOptions),
+                                        C.POINTER(PropertyFields), l, vp]
+    L.lsg_properties.argtypes = [vp, i, i, vp, vp, vp, d, C.POINTER(PropertyOptions), C.POINTER(PropertyFields)]
     _lib = L
     return L
 
@@ -122,6 +138,14 @@ class Mechanism:
         ns, nr = C.c_int(), C.c_int()
         _check(lib().lsg_mech_info(self.h, C.byref(ns), C.byref(nr)), "lsg_mech_info")
         self.n_species, self.n_reactions = ns.value, nr.value
+
+    def transport_info(self):
+        """(has transport data, species indices of the light species with Soret terms)."""
+        has, nt = C.c_int(), C.c_int()
+        idx = (C.c_int * max(self.n_species, 1))()
+        _check(lib().lsg_mech_transport_info(self.h, C.byref(has), C.byref(nt), C.cast(idx, C.c_void_p)),
+               "lsg_mech_transport_info")
+        return bool(has.value), [idx[k] for k in range(nt.value)]
 
     def close(self):
         if self.h:
@@ -303,6 +327,55 @@ class ReactionStep:
         _check(lib().lsg_formation_rates_device(self.h, T.shape[0], nc, Y.data_ptr(), T.data_ptr(), ld, p,
                                                 out.data_ptr(), out.shape[1], _stream_handle(stream)),
                "lsg_formation_rates_device")
+
+    def _property_request(self, soret: bool, fields, thermal: bool):
+        nt = len(self.mech.transport_info()[1])
+        want = set(PROPERTY_FIELDS if fields is None else fields)
+        if not soret:
+            want.discard("Dsoret")
+        if not thermal:   # evaluated only with the energy equation or Lewis numbers
+            want -= {"lambda", "cp", "cv", "cp_species"}
+        if "Dsoret" in want:
+            want.add("Dmix")
+        rows = {"X": self.mech.n_species, "cp_species": self.mech.n_species, "Dmix": self.mech.n_species,
+                "Dsoret": nt}
+        return [f for f in PROPERTY_FIELDS if f in want], rows
+
+    def properties_device(self, Y, T, p=None, p_scalar: float = 101325.0, energy: bool = True, lewis=None,
+                          simplified: bool = False, soret: bool = False, fields=None, stream=None) -> dict:
+        """Property update of the cells (Y [NC, ld], T [ncells], p [ncells] or p_scalar) on the
+        device: a dict of new CUDA tensors, species fields [rows, ncells]; lewis a CUDA tensor
+        of NC Lewis numbers or None (mixture-averaged diffusivities)."""
+        import torch
+        _require_layout(Y, T, p, lewis)
+        nc, ld = Y.shape
+        n = T.shape[0]
+        names, rows = self._property_request(soret, fields, energy or lewis is not None)
+        out = {f: torch.empty((rows[f], n) if f in rows else (n,), dtype=torch.float64, device=Y.device)
+               for f in names}
+        fd = PropertyFields(**{f: out[f].data_ptr() for f in names})
+        opt = PropertyOptions(int(energy), int(simplified), None if lewis is None else lewis.data_ptr())
+        _check(lib().lsg_properties_device(self.h, n, nc, Y.data_ptr(), T.data_ptr(), ld,
+                                           None if p is None else p.data_ptr(), p_scalar, C.byref(opt),
+                                           C.byref(fd), n, _stream_handle(stream)), "lsg_properties_device")
+        return out
+
+    def properties(self, Y, T, p=None, p_scalar: float = 101325.0, energy: bool = True, lewis=None,
+                   simplified: bool = False, soret: bool = False, fields=None) -> dict:
+        """The same from host arrays (Y [NC, ncells] species-major, float64): numpy fields."""
+        Y = np.ascontiguousarray(Y, dtype=np.float64)
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        nc, n = Y.shape
+        names, rows = self._property_request(soret, fields, energy or lewis is not None)
+        out = {f: np.empty((rows[f], n) if f in rows else (n,)) for f in names}
+        fd = PropertyFields(**{f: out[f].ctypes.data for f in names})
+        le = None if lewis is None else np.ascontiguousarray(lewis, dtype=np.float64)
+        pp = None if p is None else np.ascontiguousarray(p, dtype=np.float64)
+        opt = PropertyOptions(int(energy), int(simplified), None if le is None else le.ctypes.data)
+        _check(lib().lsg_properties(self.h, n, nc, Y.ctypes.data, T.ctypes.data,
+                                    None if pp is None else pp.ctypes.data, p_scalar, C.byref(opt), C.byref(fd)),
+               "lsg_properties")
+        return out
 
     def rhs_device(self, y, dy, p: float = 101325.0, qr=None, stream=None):
         _require_layout(y, dy, qr)

@@ -54,6 +54,8 @@ def pad_inert(data: bytes, k: int, template: str = "N2") -> Tuple[bytes, List[st
     for key, w in per.items():
         row = A[key][t * w:(t + 1) * w]
         A[key] = np.concatenate([A[key]] + [row] * k)
+    for key in [key for key in A if key.startswith("tr_")]:
+        del A[key]    # the padded mechanism carries no transport data
     A["fr_ptr"] = np.concatenate([A["fr_ptr"], np.full(k, A["fr_ptr"][-1], A["fr_ptr"].dtype)])
     A["dims"] = np.array([nc + k, A["dims"][1]], A["dims"].dtype)
     names = list(species) + [f"INERT{i + 1}" for i in range(k)]

@@ -1,11 +1,14 @@
 """Mechanism compiler command line.
 
     python -m laminarsmoke_b200.mech compile KIN.CKI THERMO.CKT -o mech.lsmech [--tmid-correction]
+                                            [--transport TRANSPORT.TRC]
     python -m laminarsmoke_b200.mech info mech.lsmech
 
 `compile` turns CHEMKIN kinetics and thermodynamics files into the packed
 blob that lsg_mech_load_file / lsg_mech_load_blob read (it takes the place of
-the reference's pre-processor output, kinetics.xml).
+the reference's pre-processor output, kinetics.xml).  With a CHEMKIN
+transport file the blob also carries the fitted species transport properties
+that the property update (lsg_properties_device) evaluates.
 """
 from __future__ import annotations
 
@@ -24,13 +27,15 @@ def main(argv=None) -> int:
     c.add_argument("-o", "--output", required=True)
     c.add_argument("--tmid-correction", action="store_true",
                    help="make cp, h, s continuous at T_mid (the pre-processor's optional correction)")
+    c.add_argument("--transport", default=None, help="CHEMKIN transport file (Lennard-Jones records)")
     i = sub.add_parser("info", help="print the sizes of a blob")
     i.add_argument("blob")
     args = ap.parse_args(argv)
     if args.cmd == "compile":
         try:
-            m = chemkin.compile_files(args.kinetics, args.thermo, tmid_correct=args.tmid_correction)
-        except chemkin.ChemkinError as e:
+            m = chemkin.compile_files(args.kinetics, args.thermo, tmid_correct=args.tmid_correction,
+                                      trc_path=args.transport)
+        except (chemkin.ChemkinError, ValueError) as e:
             print(f"error: {e}", file=sys.stderr)
             return 1
         with open(args.output, "wb") as f:

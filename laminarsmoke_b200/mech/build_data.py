@@ -13,18 +13,21 @@ import sys
 
 from . import DATA, blob, chemkin
 
+_K = "run/kinetic-mechanisms/"
+# kinetics, thermodynamics, transport
 MECHS = {
-    "POLIMI_H2CO_1412": ("run/kinetic-mechanisms/POLIMI_H2CO_1412/POLIMI_H2CO_1412.CKI",
-                         "run/kinetic-mechanisms/POLIMI_H2CO_1412/POLIMI_TOT_NOX_1412.CKT"),
-    "POLIMI_H2_1412": ("run/kinetic-mechanisms/POLIMI_H2_1412/POLIMI_H2_1412.CKI",
-                       "run/kinetic-mechanisms/POLIMI_H2_1412/POLIMI_TOT_NOX_1412.CKT"),
-    "POLIMI_CH4_SKELETAL_1412": ("run/kinetic-mechanisms/POLIMI_CH4_SKELETAL_1412/POLIMI_CH4_SKELETAL_1412.CKI",
-                                 "run/kinetic-mechanisms/POLIMI_CH4_SKELETAL_1412/POLIMI_TOT_NOX_1412.CKT"),
+    "POLIMI_H2CO_1412": (_K + "POLIMI_H2CO_1412/POLIMI_H2CO_1412.CKI", _K + "POLIMI_H2CO_1412/POLIMI_TOT_NOX_1412.CKT",
+                         _K + "POLIMI_H2CO_1412/POLIMI_TOT_NOX_1412.TRC"),
+    "POLIMI_H2_1412": (_K + "POLIMI_H2_1412/POLIMI_H2_1412.CKI", _K + "POLIMI_H2_1412/POLIMI_TOT_NOX_1412.CKT",
+                       _K + "POLIMI_H2_1412/POLIMI_TOT_NOX_1412.TRC"),
+    "POLIMI_CH4_SKELETAL_1412": (_K + "POLIMI_CH4_SKELETAL_1412/POLIMI_CH4_SKELETAL_1412.CKI",
+                                 _K + "POLIMI_CH4_SKELETAL_1412/POLIMI_TOT_NOX_1412.CKT",
+                                 _K + "POLIMI_CH4_SKELETAL_1412/POLIMI_TOT_NOX_1412.TRC"),
     # global one-step mechanisms with forward reaction orders (FORD)
-    "GLOBAL_CH4_1step": ("run/kinetic-mechanisms/GLOBAL_CH4_1step/GLOBAL_CH4_1step.CKI",
-                         "run/kinetic-mechanisms/GLOBAL_CH4_1step/GLOBAL_CH4_1step.CKT"),
-    "GLOBAL_H2_1step": ("run/kinetic-mechanisms/GLOBAL_H2_1step/GLOBAL_H2_1step.CKI",
-                        "run/kinetic-mechanisms/GLOBAL_H2_1step/GLOBAL_H2_1step.CKT"),
+    "GLOBAL_CH4_1step": (_K + "GLOBAL_CH4_1step/GLOBAL_CH4_1step.CKI", _K + "GLOBAL_CH4_1step/GLOBAL_CH4_1step.CKT",
+                         _K + "GLOBAL_CH4_1step/GLOBAL_CH4_1step.TRC"),
+    "GLOBAL_H2_1step": (_K + "GLOBAL_H2_1step/GLOBAL_H2_1step.CKI", _K + "GLOBAL_H2_1step/GLOBAL_H2_1step.CKT",
+                        _K + "GLOBAL_H2_1step/GLOBAL_H2_1step.TRC"),
 }
 
 
@@ -32,8 +35,8 @@ def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
     root = argv[0] if argv else "/root/reference"
     os.makedirs(DATA, exist_ok=True)
-    for name, (cki, ckt) in MECHS.items():
-        m = chemkin.compile_files(os.path.join(root, cki), os.path.join(root, ckt))
+    for name, (cki, ckt, trc) in MECHS.items():
+        m = chemkin.compile_files(os.path.join(root, cki), os.path.join(root, ckt), trc_path=os.path.join(root, trc))
         out = os.path.join(DATA, name + ".lsmech")
         with open(out, "wb") as f:
             f.write(blob.pack(m.arrays, m.species))

@@ -911,8 +911,12 @@ def build_tables(species: List[str], reactions: List[Reaction], thermo: List[The
     return A
 
 
-def compile_mechanism(kinetics_text: str, thermo_text: str, tmid_correct: bool = False) -> Mechanism:
-    """Compile CHEMKIN kinetics + thermodynamics text into a :class:`Mechanism`."""
+def compile_mechanism(kinetics_text: str, thermo_text: str, tmid_correct: bool = False,
+                      transport_text: str = None) -> Mechanism:
+    """Compile CHEMKIN kinetics + thermodynamics (+ transport) text into a :class:`Mechanism`.
+
+    With a transport file the tables also carry the fitted species transport
+    properties (``tr_*``, mech/transport.py) that the property update uses."""
     species, reactions = read_kinetics(kinetics_text)
     db = read_thermo(thermo_text)
     thermo = []
@@ -927,12 +931,19 @@ def compile_mechanism(kinetics_text: str, thermo_text: str, tmid_correct: bool =
         thermo.append(rec)
     mech = Mechanism(species=species, reactions=reactions, thermo=thermo)
     mech.arrays = build_tables(species, reactions, thermo)
+    if transport_text is not None:
+        from .transport import transport_tables
+        mech.arrays.update(transport_tables(species, mech.arrays, transport_text))
     return mech
 
 
-def compile_files(cki_path: str, ckt_path: str, tmid_correct: bool = False) -> Mechanism:
+def compile_files(cki_path: str, ckt_path: str, tmid_correct: bool = False, trc_path: str = None) -> Mechanism:
     with open(cki_path, "r", encoding="latin-1") as f:
         kin = f.read()
     with open(ckt_path, "r", encoding="latin-1") as f:
         th = f.read()
-    return compile_mechanism(kin, th, tmid_correct=tmid_correct)
+    tr = None
+    if trc_path is not None:
+        with open(trc_path, "r", encoding="latin-1") as f:
+            tr = f.read()
+    return compile_mechanism(kin, th, tmid_correct=tmid_correct, transport_text=tr)

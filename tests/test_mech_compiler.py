@@ -112,7 +112,8 @@ def test_blob_roundtrip(h2co):
 
 @pytest.mark.skipif(not have_ref, reason="reference CHEMKIN files not present")
 def test_packaged_blob_matches_fresh_compile(h2co):
-    m = chemkin.compile_files(REF + "POLIMI_H2CO_1412.CKI", REF + "POLIMI_TOT_NOX_1412.CKT")
+    m = chemkin.compile_files(REF + "POLIMI_H2CO_1412.CKI", REF + "POLIMI_TOT_NOX_1412.CKT",
+                              trc_path=REF + "POLIMI_TOT_NOX_1412.TRC")
     assert blob.pack(m.arrays, m.species) == h2co[0]
 
 
@@ -241,5 +242,5 @@ def test_oracle_rhs_global_ch4_rate_law():
 def test_packaged_global_blobs_match_fresh_compile(name, key):
     from laminarsmoke_b200 import mech
     d = f"/root/reference/run/kinetic-mechanisms/{name}/"
-    m = chemkin.compile_files(d + name + ".CKI", d + name + ".CKT")
+    m = chemkin.compile_files(d + name + ".CKI", d + name + ".CKT", trc_path=d + name + ".TRC")
     assert blob.pack(m.arrays, m.species) == mech.load(key)[0]

@@ -296,7 +296,7 @@ int lsg_mech_transport_info(const lsg_mech* mech, int* has_transport, int* n_the
 
 /* Device arrays: Y_dev [nspecies * ld], T_dev [ncells], p_dev [ncells] or NULL
  * with p_scalar.  LSG_ERR_UNSUPPORTED when the mechanism has no transport data
- * or more species than one block's shared memory holds (about 200). */
+ * or more species than one block's shared memory holds (about 260). */
 int lsg_properties_device(lsg_ctx* ctx, int ncells, int nspecies, const double* Y_dev, const double* T_dev,
                           long ld, const double* p_dev, double p_scalar, const lsg_property_options* opt,
                           const lsg_property_fields* out_dev, long ld_out, void* stream);

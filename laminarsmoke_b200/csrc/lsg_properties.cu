@@ -23,18 +23,21 @@
 //
 // One thread per cell.  Species rows are species-major with the cells of a
 // warp in consecutive lanes, so every row read and written is coalesced.  The
-// per-species work arrays of a cell (x, eta, sqrt eta, the Wilke / diffusion
-// sums) sit in shared memory laid out [array][species][thread], so the lanes
-// of a warp touch consecutive doubles.  The pair loops are O(nc^2) per cell and
-// read the mechanism's fit and Wilke tables as warp-uniform loads.  Compiled
-// with FMA contraction off so each expression rounds like the host arithmetic.
+// per-species work arrays of a cell (x, sqrt eta, the Wilke / diffusion sums)
+// sit in shared memory laid out [array][species][thread], so the lanes of a
+// warp touch consecutive doubles; three arrays keep about 20 warps resident per
+// SM at 14 species.  The pair loops are O(nc^2) per cell and read the
+// mechanism's fit and Wilke tables as warp-uniform loads.  The kernel is bound
+// by its FP64 arithmetic (exponentials and divisions of the pair loops), not
+// by HBM.  Compiled with FMA contraction off so each expression rounds like the
+// host arithmetic.
 #include "lsg_common.cuh"
 #include "lsg_kernels.h"
 
 namespace lsg {
 
 namespace {
-constexpr int kPropArrays = 4;              // x, eta, sqrt(eta), sums
+constexpr int kPropArrays = 3;              // x, sqrt(eta), sums
 constexpr size_t kPropSmemMax = 200 * 1024;
 constexpr double kThreshold = 1.e-14;       // TransportPropertiesMap_CHEMKIN.hpp:47
 constexpr double kMu0 = 1.8405e-5, kT0 = 300., kBeta0 = 0.6759, kPr0 = 0.7;   // properties.H:126-129
@@ -62,8 +65,7 @@ __global__ void __launch_bounds__(128) properties_kernel(MechLayout L, const uns
   const double* MW = M.D(L.mw);
   const double* TM = M.D(L.t_mid);
   double* xs = sm + threadIdx.x;             // xs[s * bd]
-  double* es = xs + (size_t)nc * bd;
-  double* ss = es + (size_t)nc * bd;
+  double* ss = xs + (size_t)nc * bd;
   double* acc = ss + (size_t)nc * bd;
   const long ld = a.ld, lo = a.ld_out;
 
@@ -98,30 +100,35 @@ __global__ void __launch_bounds__(128) properties_kernel(MechLayout L, const uns
   const double lT = log(T), lT2 = lT * lT, lT3 = lT * lT2;
   // Wilke's rule (etaMix)
   const double* fe = TD + TL.eta;
-  for (int s = 0; s < nc; ++s) {
+  auto eta_of = [&](int s) {
     double sum = fe[4 * s];
     sum += fe[4 * s + 1] * lT;
     sum += fe[4 * s + 2] * lT2;
     sum += fe[4 * s + 3] * lT3;
-    const double e = exp(sum);
-    es[(size_t)s * bd] = e;
-    ss[(size_t)s * bd] = sqrt(e);
+    return exp(sum);
+  };
+  for (int s = 0; s < nc; ++s) {
+    ss[(size_t)s * bd] = sqrt(eta_of(s));
     acc[(size_t)s * bd] = xs[(size_t)s * bd];
   }
+  // Pair (k, j), k < j, adds x_j phi_kj (1 + d)^2 to sum_k and x_k phi_jk (1 + 1/d)^2 to
+  // sum_j, d = sqrt(eta_k) / sqrt(eta_j) (M_j / M_k)^(1/4).  With j outermost each sum
+  // receives its terms in the reference's order (the k < j terms, then j < k ascending),
+  // and 1 / sqrt(eta_j) is formed once per species as there.
   const double* phi = TD + TL.wilke_phi;
   const double* r14 = TD + TL.wilke_r14;
-  for (int k = 0; k < nc; ++k) {
-    const double sqk = ss[(size_t)k * bd], xk = xs[(size_t)k * bd];
-    double sk = acc[(size_t)k * bd];
-    for (int j = k + 1; j < nc; ++j) {
-      const double d = sqk * (1. / ss[(size_t)j * bd]) * r14[k * nc + j];
-      sk += xs[(size_t)j * bd] * phi[k * nc + j] * (1. + d) * (1. + d);
-      acc[(size_t)j * bd] += xk * phi[j * nc + k] * (1. + 1. / d) * (1. + 1. / d);
+  for (int j = 1; j < nc; ++j) {
+    const double usj = 1. / ss[(size_t)j * bd], xj = xs[(size_t)j * bd];
+    double sj = acc[(size_t)j * bd];
+    for (int k = 0; k < j; ++k) {
+      const double d = ss[(size_t)k * bd] * usj * r14[k * nc + j];
+      acc[(size_t)k * bd] += xj * phi[k * nc + j] * (1. + d) * (1. + d);
+      sj += xs[(size_t)k * bd] * phi[j * nc + k] * (1. + 1. / d) * (1. + 1. / d);
     }
-    acc[(size_t)k * bd] = sk;
+    acc[(size_t)j * bd] = sj;
   }
   double mu = 0.;
-  for (int s = 0; s < nc; ++s) mu += xs[(size_t)s * bd] * es[(size_t)s * bd] / acc[(size_t)s * bd];
+  for (int s = 0; s < nc; ++s) mu += xs[(size_t)s * bd] * eta_of(s) / acc[(size_t)s * bd];
 
   const bool lewis = a.lewis != nullptr;
   double lambda = 0., cp = 0.;

@@ -125,7 +125,8 @@ class OracleProperties:
             out["cp_species"] = cp_r * R_J_KMOL / self.mw[None, :]
         if simplified:
             out["mu"] = MU0 * (T / T0) ** BETA0
-            out["lambda"] = out["mu"] * out["cp"] / PR0
+            if "cp" in out:   # lambda and cp are fields only with the energy equation or Lewis numbers
+                out["lambda"] = out["mu"] * out["cp"] / PR0
         if lewis_mode:
             coef = out["lambda"] / (p * psi) / out["cp"]
             out["Dmix"] = coef[:, None] / np.asarray(lewis, float)[None, :]

@@ -21,7 +21,9 @@ expected outputs.  Inputs are seeded (numpy PCG64, seeds below):
 * ch4_1step.npz     -- 64 cells of the global one-step CH4 mechanism (FORD);
 * rateforms_rhs.npz -- RHS of the PLOG, Chebyshev and CABR test mechanisms
                        (tests/test_plog.py, test_cheb.py, test_cabr.py) at
-                       32 states and three pressures each.
+                       32 states and three pressures each;
+* h2co_properties.npz -- the property update (oracle/properties.py) of the
+                       h2co_step result at 1 and 3 atm, with Soret terms.
 """
 import os
 import sys
@@ -124,6 +126,12 @@ def main():
             out[f"{name}_y"] = ys
             out[f"{name}_dy_{patm}"] = np.array([o.rhs(ys[k], patm * 101325.0)[0] for k in range(32)])
     np.savez_compressed(os.path.join(HERE, "rateforms_rhs.npz"), **out)
+
+    from oracle.properties import OracleProperties
+    g = np.load(os.path.join(HERE, "h2co_step.npz"))
+    p = np.where(np.arange(g["T"].size) % 2 == 0, 101325.0, 3.0 * 101325.0)
+    f = OracleProperties(data).evaluate(g["Y"], g["T"], p, soret=True)
+    np.savez_compressed(os.path.join(HERE, "h2co_properties.npz"), p=p, **f)
 
 
 if __name__ == "__main__":

@@ -97,6 +97,15 @@ def test_oracle_rateforms_golden():
             np.testing.assert_allclose(dy, g[f"{name}_dy_{patm}"], rtol=1e-13, atol=1e-300, err_msg=name)
 
 
+def test_oracle_properties_golden(h2co):
+    from oracle.properties import OracleProperties
+    s = _load("h2co_step.npz")
+    g = _load("h2co_properties.npz")
+    f = OracleProperties(h2co[0]).evaluate(s["Y"], s["T"], g["p"], soret=True)
+    for key, v in f.items():
+        np.testing.assert_allclose(v, g[key], rtol=1e-13, atol=0., err_msg=key)
+
+
 # ---- the library against the fixtures (GPU) ----
 
 def _gpu_step(data, g, **kw):
@@ -161,3 +170,19 @@ def test_gpu_block_golden(cuda):
     abs_Y = np.abs(Y - g["Y"]).max(axis=1)
     assert (np.abs(T - g["T"]) / g["T"]).max() <= RTOL_T
     assert np.mean(abs_Y <= ATOL_Y) >= 0.9 and abs_Y.max() <= 1e-7
+
+
+@pytest.mark.gpu
+def test_gpu_properties_golden(h2co, cuda):
+    import torch
+    from laminarsmoke_b200 import lsg
+    s = _load("h2co_step.npz")
+    g = _load("h2co_properties.npz")
+    ctx = lsg.ReactionStep(lsg.Mechanism(h2co[0]))
+    got = ctx.properties_device(torch.tensor(np.ascontiguousarray(s["Y"].T), device=cuda),
+                                torch.tensor(s["T"], device=cuda), torch.tensor(g["p"], device=cuda), soret=True)
+    torch.cuda.synchronize()
+    for key, v in got.items():
+        r = g[key].T if g[key].ndim == 2 else g[key]
+        np.testing.assert_allclose(v.cpu().numpy(), r, rtol=1e-11, atol=1e-13 * float(np.max(np.abs(r))),
+                                   err_msg=key)

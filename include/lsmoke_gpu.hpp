@@ -206,6 +206,81 @@ class MultiValueSolver {
   std::vector<double> Q_;
 };
 
+/* The property update after the step (solvers/laminarSMOKE/properties.H:40-190) over a whole field, in one
+ * call: what the reference gets per cell from ThermodynamicsMap_CHEMKIN (MoleFractions_From_MassFractions,
+ * hMolar_Mixture_From_MoleFractions, cpMolar_Mixture_From_MoleFractions, cpMolar_Species) and
+ * TransportPropertiesMap_CHEMKIN (DynamicViscosity, ThermalConductivity, MassDiffusionCoefficients,
+ * ThermalDiffusionRatios).  Needs a mechanism compiled with its transport file. */
+class TransportPropertiesMap {
+ public:
+  /* Host fields, resized by Evaluate; species fields species-major [NC][ncells], Dsoret
+   * [ThermalDiffusionSpecies().size()][ncells]. */
+  struct Fields {
+    std::vector<double> X, cTot, psi, mu, lambda, cp, cv, h, MWmix, cp_species, Dmix, Dsoret;
+  };
+
+  explicit TransportPropertiesMap(const Mechanism& mech) : mech_(mech) {
+    int has = 0, nt = 0;
+    iteta_.assign(mech.NumberOfSpecies(), 0);
+    check(lsg_mech_transport_info(mech.get(), &has, &nt, iteta_.data()), "lsg_mech_transport_info");
+    if (!has) throw Error("TransportPropertiesMap: the mechanism has no transport data", LSG_ERR_UNSUPPORTED);
+    iteta_.resize(nt);
+    lsg_options o;
+    lsg_options_default(&o);
+    check(lsg_ctx_create(mech.get(), &o, mech.device(), &ctx_), "lsg_ctx_create");
+  }
+  ~TransportPropertiesMap() { if (ctx_) lsg_ctx_destroy(ctx_); }
+  TransportPropertiesMap(const TransportPropertiesMap&) = delete;
+  TransportPropertiesMap& operator=(const TransportPropertiesMap&) = delete;
+
+  /* energyEquation: lambda, cp, cv and the species cp are evaluated. */
+  void SetEnergyEquation(bool flag) { energy_ = flag; }
+  /* simplifiedTransportProperties: mu = 1.8405e-5 (T/300)^0.6759, lambda = mu cp / 0.7. */
+  void SetSimplifiedTransportProperties(bool flag) { simplified_ = flag; }
+  /* DIFFUSIVITY_MODEL_LEWIS_NUMBERS with one Lewis number per species; an empty vector selects the
+   * mixture-averaged coefficients (DIFFUSIVITY_MODEL_MULTICOMPONENT). */
+  void SetLewisNumbers(const std::vector<double>& le) {
+    if (!le.empty() && (int)le.size() != mech_.NumberOfSpecies()) throw Error("SetLewisNumbers", LSG_ERR_ARG);
+    lewis_ = le;
+  }
+  /* soretEffect: thermal-diffusion terms of the light species. */
+  void SetSoretEffect(bool flag) { soret_ = flag; }
+  /* Species with thermal-diffusion ratios (iThermalDiffusionRatios, 0-based). */
+  const std::vector<int>& ThermalDiffusionSpecies() const { return iteta_; }
+
+  /* Y [NC][ncells] mass fractions, T [ncells], p [ncells] (or nullptr and p_scalar). */
+  void Evaluate(int ncells, const double* Y, const double* T, const double* p, Fields& f, double p_scalar = 0.) {
+    if (ncells < 0 || !Y || !T) throw Error("Evaluate", LSG_ERR_ARG);
+    const size_t n = (size_t)ncells, nc = (size_t)mech_.NumberOfSpecies();
+    const bool thermal = energy_ || !lewis_.empty();
+    f.X.resize(nc * n);
+    f.cTot.resize(n);
+    f.psi.resize(n);
+    f.mu.resize(n);
+    f.h.resize(n);
+    f.MWmix.resize(n);
+    f.Dmix.resize(nc * n);
+    f.lambda.resize(thermal ? n : 0);
+    f.cp.resize(thermal ? n : 0);
+    f.cv.resize(thermal ? n : 0);
+    f.cp_species.resize(thermal ? nc * n : 0);
+    f.Dsoret.resize(soret_ ? iteta_.size() * n : 0);
+    auto ptr = [](std::vector<double>& v) { return v.empty() ? nullptr : v.data(); };
+    lsg_property_fields pf = {ptr(f.X),  ptr(f.cTot), ptr(f.psi), ptr(f.mu),    ptr(f.lambda),     ptr(f.cp),
+                              ptr(f.cv), ptr(f.h),    ptr(f.MWmix), ptr(f.cp_species), ptr(f.Dmix), nullptr};
+    if (soret_ && !iteta_.empty()) pf.Dsoret = f.Dsoret.data();
+    lsg_property_options po = {energy_ ? 1 : 0, simplified_ ? 1 : 0, lewis_.empty() ? nullptr : lewis_.data()};
+    check(lsg_properties(ctx_, ncells, (int)nc, Y, T, p, p_scalar, &po, &pf), "lsg_properties");
+  }
+
+ private:
+  const Mechanism& mech_;
+  lsg_ctx* ctx_ = nullptr;
+  std::vector<int> iteta_;
+  std::vector<double> lewis_;
+  bool energy_ = true, simplified_ = false, soret_ = false;
+};
+
 }  // namespace lsmoke
 
 #endif /* LSMOKE_GPU_HPP */

@@ -25,7 +25,15 @@ int main(int argc, char** argv) {
   try { reactor.SetReactor(-1.); return 11; } catch (const lsmoke::Error& e) { if (e.code() != LSG_ERR_ARG) return 12; }
   const char bad[16] = "NOTAMECHANISM00";
   try { lsmoke::Mechanism m(lsmoke::Blob{bad, 16}); return 13; } catch (const lsmoke::Error& e) { if (e.code() != LSG_ERR_MECH) return 14; }
-  if (argc < 5) { std::printf("cpu ok\n"); return 0; }
+  if (argc < 5) {
+    // the property map's interface compiles against the same header (its C entry point is tested on the GPU)
+    void (lsmoke::TransportPropertiesMap::*ev)(int, const double*, const double*, const double*,
+                                               lsmoke::TransportPropertiesMap::Fields&, double) =
+        &lsmoke::TransportPropertiesMap::Evaluate;
+    (void)ev;
+    std::printf("cpu ok\n");
+    return 0;
+  }
   // the reference's call sequence on a field read from argv[2] (ncells, then Y[NC][ncells], then T[ncells])
   lsmoke::Mechanism mech(argv[1]);
   const int nc = mech.NumberOfSpecies();

@@ -212,11 +212,13 @@ class SpeciesTransport:
         return e, s
 
     def cp_mass(self, T: float) -> np.ndarray:
-        """Species cp [J/kg/K] from the NASA polynomials."""
+        """Species cp [J/kg/K] from the NASA polynomials (ThermoPolicy_CHEMKIN::cp,
+        kernel/thermo/ThermoPolicy_CHEMKIN.hpp:371-379)."""
         out = np.empty(self.nc)
         for i in range(self.nc):
             a = self.cp_ht[i] if T > self.t_mid[i] else self.cp_lt[i]
-            out[i] = (a[0] + T * (a[1] + T * (a[2] + T * (a[3] + T * a[4])))) * R_J_KMOL / self.mw[i]
+            r = R_J_MOL / (self.mw[i] * 1.e-3)
+            out[i] = (a[0] + T * (a[1] + T * (a[2] + T * (a[3] + T * a[4])))) * r
         return out
 
     def viscosity(self, T: float) -> np.ndarray:
@@ -230,7 +232,7 @@ class SpeciesTransport:
         aux = np.sqrt(self.eps_kb / T)
         fT = 1. + aux * (_ZROTA + aux * (_ZROTB + aux * _ZROTC))
         zrot = self.zrot298 * self.f298 / fT
-        cv = self.cp_mass(T) - R_J_KMOL / self.mw
+        cv = self.cp_mass(T) - R_J_KMOL * (1. / self.mw)     # SpeciesCv (WithoutTransport.hpp:95-99)
         cv_vib = cv * self.mw * 1.e-3 - self.cv_trans - self.cv_rot
         rho = 100. / (R_J_MOL * T) * self.mw
         om11 = np.array([omega11(T / self.eps_kb[k], 0.) for k in range(self.nc)])

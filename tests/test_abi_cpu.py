@@ -43,3 +43,18 @@ def test_options_defaults_and_errors_without_gpu():
     bad = (C.c_ubyte * 16)(*b"NOTAMECHANISM000")
     assert L.lsg_mech_load_blob(C.cast(bad, C.c_void_p), 16, 0, C.byref(h)) == -2
     assert L.lsg_strerror(-2) == b"mechanism blob could not be read"
+
+
+def test_property_entry_points_reject_bad_arguments_without_gpu():
+    from laminarsmoke_b200 import lsg
+    L = lsg.lib()
+    has, nt = C.c_int(-1), C.c_int(-1)
+    assert L.lsg_mech_transport_info(None, C.byref(has), C.byref(nt), None) == -1
+    opt = lsg.PropertyOptions(1, 0, None)
+    fields = lsg.PropertyFields()
+    y = (C.c_double * 4)()
+    assert L.lsg_properties_device(None, 1, 1, C.cast(y, C.c_void_p), C.cast(y, C.c_void_p), 1, None, 101325.,
+                                   C.byref(opt), C.byref(fields), 1, None) == -1
+    assert L.lsg_properties(None, 1, 1, C.cast(y, C.c_void_p), C.cast(y, C.c_void_p), None, 101325.,
+                            C.byref(opt), C.byref(fields)) == -1
+    assert [f for f, _ in lsg.PropertyFields._fields_] == list(lsg.PROPERTY_FIELDS)

@@ -350,9 +350,52 @@ struct Reactor {
     }
   }
 
+  // DRG-reduced system (BatchReactorHomogeneousConstantPressure.H:253-320): the unknowns are the
+  // important species (ascending) and T; the other species keep their values in omega, and the
+  // dropped reactions' rates are zeroed before the formation rates.  Constant pressure only.
+  const std::vector<int>* drg_species = nullptr;
+  const std::vector<int>* drg_dropped = nullptr;
+  std::vector<double> omega;
+
+  void equations_drg(const double* y, double* dy) {
+    const auto& MW = m.F("mw");
+    const std::vector<int>& S = *drg_species;
+    const int ni = (int)S.size();
+    for (int i = 0; i < ni; ++i) omega[S[i]] = y[i];
+    const double T = y[ni];
+    double u = 0.;
+    for (int i = 0; i < NC; ++i) u += omega[i] / MW[i];
+    const double MWmix = 1. / u;
+    for (int i = 0; i < NC; ++i) x[i] = MWmix * omega[i];
+    for (int i = 0; i < NC; ++i) x[i] = x[i] / MW[i];
+    const double cTot = P0 / R_J_KMOL / T;
+    for (int i = 0; i < NC; ++i) c[i] = cTot * x[i];
+    const double rho = cTot * MWmix;
+    P_ = P0;
+    h_over_RT(T);
+    kin_set_T(T);
+    reaction_rates();
+    for (int j : *drg_dropped) net[j] = 0.;
+    formation_rates();
+    for (int i = 0; i < ni; ++i) dy[i] = MW[S[i]] * R[S[i]] / rho;
+    dy[ni] = 0.;
+    if (energy) {
+      cp_over_R(T);
+      double cpm = 0.;
+      for (int i = 0; i < NC; ++i) cpm += cp[i] * x[i];
+      cpm *= R_J_KMOL;
+      double d = 0.;
+      for (int i = 0; i < NC; ++i) d += R[i] * h[i];
+      QR = -d * R_J_KMOL * T;
+      const double CpMixMass = cpm / MWmix;
+      dy[ni] = QR / (rho * CpMixMass);
+    }
+  }
+
   // BatchReactorHomogeneousConstantPressure::Equations (:175-223)
   void equations(const double* y, double* dy) {
     ++n_calls;
+    if (drg_species) { equations_drg(y, dy); return; }
     const auto& MW = m.F("mw");
     const double T = y[NC];
     // ThermodynamicsMap_CHEMKIN::MoleFractions_From_MassFractions (:429-434)
@@ -946,6 +989,75 @@ class Gear {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Directed relation graph of one state (solvers/laminarSMOKE/unsteady/DRG.hpp)
+// ---------------------------------------------------------------------------
+struct Drg {
+  const Mech& m;
+  int NS, NR;
+  // net coefficients nu(k, j) = products - reactants of reaction k, the non-zero ones by species
+  // (the constructor's nu_ and delta_, DRG.hpp:45-110)
+  std::vector<std::vector<std::pair<int, double>>> nu;
+  std::vector<double> den, num;
+
+  explicit Drg(const Mech& mech) : m(mech), NS(mech.nc), NR(mech.nr) {
+    const auto& rp = m.I("reac_ptr"); const auto& rs = m.I("reac_species"); const auto& rn = m.F("reac_nu");
+    const auto& pp = m.I("prod_ptr"); const auto& ps = m.I("prod_species"); const auto& pn = m.F("prod_nu");
+    nu.resize(NR);
+    std::vector<double> row(NS);
+    for (int k = 0; k < NR; ++k) {
+      std::fill(row.begin(), row.end(), 0.);
+      for (int q = pp[k]; q < pp[k + 1]; ++q) row[ps[q]] += pn[q];
+      for (int q = rp[k]; q < rp[k + 1]; ++q) row[rs[q]] -= rn[q];
+      for (int j = 0; j < NS; ++j) if (row[j] != 0.) nu[k].push_back({j, row[j]});
+    }
+    den.resize(NS); num.resize(NS);
+  }
+
+  // Analysis = PairWiseErrorMatrix + ParsePairWiseErrorMatrix (DRG.hpp:150-273) at (T, P, c):
+  // r_ij = sum_k |nu_ki r_k| over the reactions with both i and j / (1e-64 + sum_k |nu_ki r_k|),
+  // breadth-first from the key species through r_qj > eps; a reaction is dropped when one of its
+  // species is not reached.  The rows r_q. are formed when q leaves the queue.
+  void analysis(Reactor& R, double T, double P, const double* c, double eps, const std::vector<int>& key,
+                std::vector<int>& important, std::vector<int>& dropped) {
+    for (int i = 0; i < NS; ++i) R.c[i] = c[i];
+    R.P_ = P;
+    R.h_over_RT(T);
+    R.kin_set_T(T);
+    R.reaction_rates();
+    const std::vector<double>& r = R.net;
+    std::fill(den.begin(), den.end(), 0.);
+    for (int k = 0; k < NR; ++k)
+      for (const auto& e : nu[k]) den[e.first] += std::fabs(e.second * r[k]);
+    std::vector<char> imp(NS, 0);
+    std::vector<int> Q;
+    size_t head = 0;
+    for (int s : key) { Q.push_back(s); imp[s] = 1; }
+    while (head < Q.size()) {
+      const int q = Q[head];
+      std::fill(num.begin(), num.end(), 0.);
+      for (int k = 0; k < NR; ++k) {
+        double nq = 0.;
+        bool has = false;
+        for (const auto& e : nu[k]) if (e.first == q) { nq = e.second; has = true; break; }
+        if (!has) continue;
+        for (const auto& e : nu[k]) num[e.first] += std::fabs(nq * r[k]);
+      }
+      for (int k = 0; k < NS; ++k)
+        if (!imp[k] && num[k] / (1.e-64 + den[q]) > eps) { imp[k] = 1; Q.push_back(k); }
+      ++head;
+    }
+    important.clear();
+    for (int k = 0; k < NS; ++k) if (imp[k]) important.push_back(k);
+    dropped.clear();
+    for (int k = 0; k < NR; ++k) {
+      bool keep = true;
+      for (const auto& e : nu[k]) if (!imp[e.first]) keep = false;
+      if (!keep) dropped.push_back(k);
+    }
+  }
+};
+
 }  // namespace orc
 
 // ---------------------------------------------------------------------------
@@ -1155,6 +1267,119 @@ int orc_steady_sources(void* mech, double P, const double* y, double* s_implicit
     s_implicit[k] = J;
     s_explicit[k] = S0[k] - J * y[k];
   }
+  return 0;
+}
+
+// DRG-reduced reaction step, solvers/laminarSMOKE/unsteady/chemistry_DRG.H:78-200, cells in order.
+// Per cell above min_T: the analysis at the cell's concentrations (epsilon from the first band whose
+// temperature is above the cell's; with none, the epsilon of the previous analysis stays), then the
+// reduced system from t0 to t0 + dt with a new solver, the other species kept, the mass fractions
+// normalised after the step.  The reference declares the solver inside the cell loop and applies the
+// tolerances and bounds (T in [200, 6000]) only when celli == 0; every other cell integrates with the
+// solver's defaults (absolute 1e-10, relative 100 * FLT_EPSILON, no bounds).  first_cell_options_only
+// = 1 restates that; 0 gives every cell the options.  n_species / n_reactions: the drg fields (0 for
+// skipped cells).
+struct orc_drg_options {
+  const int* key;
+  int nkey;
+  const double* band_T;
+  const double* band_eps;
+  int nbands;
+  double epsilon0;
+  double min_T;
+  int first_cell_options_only;
+};
+
+int orc_reaction_step_drg(void* mech, const orc_options* o, const orc_drg_options* d, int ncells, double* Y,
+                          double* T, double p, double t0, const double* dt, double dt_scalar, double* Q, int* status,
+                          long long* counters, int* n_species, int* n_reactions) {
+  const orc::Mech& m = *(const orc::Mech*)mech;
+  const int NC = m.nc, NR = m.nr;
+  const auto& MW = m.F("mw");
+  orc::Reactor reactor(m);
+  orc::Drg drg(m);
+  std::vector<int> key(d->key, d->key + d->nkey), imp, drop;
+  std::vector<double> omega(NC), x(NC), c(NC), yff(NC + 1);
+  double eps = d->epsilon0;
+  int nerr = 0;
+  for (int cell = 0; cell < ncells; ++cell) {
+    double* Yc = Y + (size_t)cell * NC;
+    int st = 0;
+    int nsp = 0, nrx = 0;
+    if (T[cell] > d->min_T) {
+      for (int i = 0; i < NC; ++i) omega[i] = Yc[i];
+      double u = 0.;
+      for (int i = 0; i < NC; ++i) u += omega[i] / MW[i];
+      const double MWmix = 1. / u;
+      for (int i = 0; i < NC; ++i) x[i] = MWmix * omega[i];
+      for (int i = 0; i < NC; ++i) x[i] = x[i] / MW[i];
+      const double cTot = p / orc::R_J_KMOL / T[cell];
+      for (int i = 0; i < NC; ++i) c[i] = cTot * x[i];
+      for (int b = 0; b < d->nbands; ++b)
+        if (T[cell] < d->band_T[b]) { eps = d->band_eps[b]; break; }
+      drg.analysis(reactor, T[cell], p, c.data(), eps, key, imp, drop);
+      const int ni = (int)imp.size();
+      const unsigned NEQ = ni + 1;
+      std::vector<double> y0(NEQ);
+      for (int i = 0; i < ni; ++i) y0[i] = omega[imp[i]];
+      y0[ni] = T[cell];
+      reactor.P0 = p;
+      reactor.rho0 = 0.;
+      reactor.energy = o->energy != 0;
+      if (!reactor.energy) reactor.QR = 0.;
+      reactor.omega = omega;
+      reactor.drg_species = &imp;
+      reactor.drg_dropped = &drop;
+      orc::Gear g(reactor, NEQ);
+      g.set_initial_conditions(t0, y0.data());
+      if (cell == 0 || !d->first_cell_options_only) {
+        g.full_piv_ = o->full_pivoting != 0;
+        g.abs_tol_ = o->atol; g.rel_tol_ = o->rtol;
+        for (unsigned i = 0; i < NEQ; ++i) { g.minv_[i] = 0.; g.maxv_[i] = 1.; }
+        g.minv_[ni] = 200.; g.maxv_[ni] = 6000.;
+      } else {
+        g.abs_tol_ = 1.e-10; g.rel_tol_ = 100. * orc::MACH_EPS_FLOAT;   // MultiValueSolver.hpp:41-43
+        g.min_c_ = false; g.max_c_ = false;
+      }
+      const double dtc = dt ? dt[cell] : dt_scalar;
+      st = g.solve(t0 + dtc);
+      reactor.drg_species = nullptr;
+      reactor.drg_dropped = nullptr;
+      for (int i = 0; i < NC; ++i) yff[i] = omega[i];
+      yff[NC] = g.y_[ni];
+      for (int i = 0; i < ni; ++i) yff[imp[i]] = g.y_[i];
+      double sum = 0.;
+      for (int i = 0; i < NC; ++i) sum += yff[i];
+      for (int i = 0; i < NC; ++i) yff[i] /= sum;
+      for (int i = 0; i < NC; ++i) Yc[i] = yff[i];
+      if (o->energy) T[cell] = yff[NC];
+      if (Q) Q[cell] = reactor.QR;
+      if (counters) for (int k = 0; k < orc::NCOUNT; ++k) counters[(size_t)cell * orc::NCOUNT + k] = g.cnt_[k];
+      nsp = ni;
+      nrx = NR - (int)drop.size();
+      if (st < 0) nerr++;
+    } else if (counters) {
+      for (int k = 0; k < orc::NCOUNT; ++k) counters[(size_t)cell * orc::NCOUNT + k] = 0;
+    }
+    if (status) status[cell] = st;
+    if (n_species) n_species[cell] = nsp;
+    if (n_reactions) n_reactions[cell] = nrx;
+  }
+  return nerr;
+}
+
+// The analysis alone at one state: important species (ascending) and dropped reactions.
+int orc_drg_analysis(void* mech, double T, double P, const double* c, double eps, const int* key, int nkey,
+                     int* important, int* n_important, int* dropped, int* n_dropped) {
+  const orc::Mech& m = *(const orc::Mech*)mech;
+  orc::Reactor reactor(m);
+  orc::Drg drg(m);
+  std::vector<int> k(key, key + nkey), imp, drop;
+  drg.analysis(reactor, T, P, c, eps, k, imp, drop);
+  for (size_t i = 0; i < imp.size(); ++i) important[i] = imp[i];
+  for (size_t i = 0; i < drop.size(); ++i) dropped[i] = drop[i];
+  *n_important = (int)imp.size();
+  *n_dropped = (int)drop.size();
   return 0;
 }
 

@@ -54,8 +54,19 @@ def lib():
                                           C.c_double, C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]
         L.orc_formation_rates.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
         L.orc_steady_sources.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_reaction_step_drg.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.POINTER(OrcDrgOptions), C.c_int,
+                                            C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_double,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_drg_analysis.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_double, C.c_void_p,
+                                       C.c_int, C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.POINTER(C.c_int)]
         _lib = L
     return _lib
+
+
+class OrcDrgOptions(C.Structure):
+    _fields_ = [("key", C.c_void_p), ("nkey", C.c_int), ("band_T", C.c_void_p), ("band_eps", C.c_void_p),
+                ("nbands", C.c_int), ("epsilon0", C.c_double), ("min_T", C.c_double),
+                ("first_cell_options_only", C.c_int)]
 
 
 def _ptr(a):
@@ -68,6 +79,9 @@ class OracleMechanism:
         self.h = lib().orc_mech_load(C.cast(self._buf, C.c_void_p), len(blob))
         if not self.h:
             raise ValueError("oracle: bad mechanism blob")
+        from laminarsmoke_b200.mech import blob as _blob
+        dims = _blob.unpack(blob)[0]["dims"]
+        self.n_species, self.n_reactions = int(dims[0]), int(dims[1])
 
     def __del__(self):
         try:
@@ -142,3 +156,38 @@ class OracleMechanism:
                                 _ptr(Q), _ptr(st), _ptr(cnt), nthreads,
                                 _ptr(None if rho is None else np.ascontiguousarray(rho, dtype=np.float64)))
         return Y, T, Q, st, cnt
+
+    def drg_analysis(self, T, P, c, eps, key):
+        """DRG analysis at one state (concentrations c [NC]): (important species, dropped reactions)."""
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        k = np.ascontiguousarray(key, dtype=np.int32)
+        nc = c.size
+        imp = np.zeros(nc, np.int32)
+        drop = np.zeros(max(self.n_reactions, 1), np.int32)
+        ni, nd = C.c_int(), C.c_int()
+        lib().orc_drg_analysis(self.h, T, P, _ptr(c), eps, _ptr(k), k.size, _ptr(imp), C.byref(ni), _ptr(drop),
+                               C.byref(nd))
+        return imp[:ni.value].tolist(), drop[:nd.value].tolist()
+
+    def reaction_step_drg(self, Y, T, dt, key, bands=((1.e6, 1.e-2),), epsilon0=1.e-2, min_T=300.0,
+                          first_cell_options_only=True, p=101325.0, t0=0.0, rtol=1e-7, atol=1e-12, energy=True):
+        """DRG-reduced step of cell-major Y[ncells, NC], T[ncells] (chemistry_DRG.H): key species
+        indices, (temperature, epsilon) bands.  Returns (Y, T, Q, status, counters, n_species,
+        n_reactions)."""
+        Y = np.array(Y, dtype=np.float64, order="C", copy=True)
+        T = np.array(T, dtype=np.float64, copy=True)
+        n = T.size
+        dt_arr, dt_s = (None, float(dt)) if np.ndim(dt) == 0 else (np.ascontiguousarray(dt, dtype=np.float64), 0.)
+        Q = np.zeros(n)
+        st = np.zeros(n, dtype=np.int32)
+        cnt = np.zeros((n, NCOUNT), dtype=np.int64)
+        nsp = np.zeros(n, dtype=np.int32)
+        nrx = np.zeros(n, dtype=np.int32)
+        k = np.ascontiguousarray(key, dtype=np.int32)
+        bt = np.ascontiguousarray([b[0] for b in bands], dtype=np.float64)
+        be = np.ascontiguousarray([b[1] for b in bands], dtype=np.float64)
+        o = OrcOptions(rtol, atol, 0.0, 200.0, 6000.0, 500000, 0, int(energy), 0.8, 0.8, 5, 1)
+        d = OrcDrgOptions(_ptr(k), k.size, _ptr(bt), _ptr(be), bt.size, epsilon0, min_T, int(first_cell_options_only))
+        lib().orc_reaction_step_drg(self.h, C.byref(o), C.byref(d), n, _ptr(Y), _ptr(T), p, t0, _ptr(dt_arr), dt_s,
+                                    _ptr(Q), _ptr(st), _ptr(cnt), _ptr(nsp), _ptr(nrx))
+        return Y, T, Q, st, cnt, nsp, nrx

@@ -479,7 +479,10 @@ int lsg_mech_load_blob(const void* blob, size_t nbytes, int device, lsg_mech** o
   lsg_mech* m = new (std::nothrow) lsg_mech();
   if (!m) return LSG_ERR_NOMEM;
   std::string err;
-  if (!build_mechanism(blob, nbytes, m->host, err)) { delete m; return LSG_ERR_MECH; }
+  if (!build_mechanism(blob, nbytes, m->host, err)) {
+    delete m;
+    return err.rfind("unsupported", 0) == 0 ? LSG_ERR_UNSUPPORTED : LSG_ERR_MECH;
+  }
   m->device = device;
   if (cudaSetDevice(device) != cudaSuccess) { delete m; cudaGetLastError(); return LSG_ERR_CUDA; }
   if (cudaMalloc(&m->d_buf, m->host.buffer.size()) != cudaSuccess) { delete m; cudaGetLastError(); return LSG_ERR_NOMEM; }

@@ -134,6 +134,12 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
   Blob b;
   if (!parse((const unsigned char*)blob, nbytes, b, err)) return false;
   try {
+    if (b.i.count("xplog_rxn")) {
+      // PLOGMX / PLOGSP (bath-gas-specific PLOG tables): the oracle evaluates them, the device
+      // kernels do not, so such a mechanism is refused rather than integrated without them
+      err = "unsupported: extended PLOG (PLOGMX/PLOGSP) reactions";
+      return false;
+    }
     const auto& dims = b.I("dims");
     const int nc = dims.at(0), nr = dims.at(1);
     if (nc <= 0 || nr < 0) { err = "bad dimensions"; return false; }

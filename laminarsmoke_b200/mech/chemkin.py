@@ -274,6 +274,10 @@ class Reaction:
     ford: bool = False   # FORD given: forward_orders replace the reactant coefficients in the rate law
     plog: List[Tuple[float, float, float, float]] = field(default_factory=list)   # PLOG (p [atm], A, beta, E)
     plog_table: List[Tuple[float, float, float, float, float]] = field(default_factory=list)  # (p [Pa], ln p, ln A, beta, E/R) SI
+    # PLOGMX / PLOGSP: (bath species index, -1 for the mixture; p [atm], A, beta, E) per line, and per bath in
+    # order of first appearance its SI table [(p [Pa], ln p, ln A, beta, E/R)]
+    xplog: List[Tuple[int, float, float, float, float]] = field(default_factory=list)
+    xplog_table: List[Tuple[int, List[Tuple[float, float, float, float, float]]]] = field(default_factory=list)
     cheb: List[float] = field(default_factory=list)   # CHEB numbers as given: N, M, a_11 .. a_NM
     cheb_T: List[float] = field(default_factory=list)  # TCHEB (Tmin, Tmax) [K]
     cheb_P: List[float] = field(default_factory=list)  # PCHEB (Pmin, Pmax) [atm]
@@ -492,9 +496,30 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
                 r.forward_orders.append((si, val))
         elif kw == "PLOG":
             # ReactionPolicy_CHEMKIN.hpp:772-792: one (p [atm], A, beta, E) point per line
-            if third_body or pdr != "none" or i_low or i_troe or i_sri:
+            if third_body or pdr != "none" or i_low or i_troe or i_sri or r.xplog:
                 raise ChemkinError("PLOG cannot be combined with third bodies or LOW/TROE/SRI")
             r.plog.append(tuple(_slash_numbers(line, (4,), "PLOG")))
+        elif kw in ("PLOGMX", "PLOGSP"):
+            # ReactionPolicy_CHEMKIN.hpp:793-880: a PLOG table for the mixture (PLOGMX) or for one bath species
+            # (PLOGSP), one point (p [atm], A, beta, E) per line
+            if third_body:
+                raise ChemkinError(f"{kw} cannot be used for third-body reactions")
+            if i_low or i_high or i_troe or i_sri or r.cheb or r.cheb_T or r.cheb_P or r.plog:
+                raise ChemkinError(f"{kw} cannot be combined with LOW/HIGH/TROE/SRI/CHEB/PLOG")
+            if kw == "PLOGMX":
+                r.xplog.append((-1,) + tuple(_slash_numbers(line, (4,), kw)))
+            else:
+                a, b = line.find("/"), line.rfind("/")
+                tok = line[a + 1:b].split() if 0 <= a < b else []
+                if len(tok) != 5:
+                    raise ChemkinError(f"{kw}: expected /SPECIES p A beta E/ in: {line.strip()}")
+                if tok[0] not in species_index:
+                    raise ChemkinError(f"{kw}: bath species not available: {tok[0]}")
+                try:
+                    vals = tuple(float(t) for t in tok[1:])
+                except ValueError:
+                    raise ChemkinError(f"{kw}: the coefficients are not numbers in: {line.strip()}") from None
+                r.xplog.append((species_index[tok[0]],) + vals)
         elif kw == "CHEB":
             # ReactionPolicy_CHEMKIN.hpp:456-475: every number between the slashes, over as many lines as needed
             if pdr != "all":
@@ -552,6 +577,8 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
         raise ChemkinError("negative frequency factors only for simple reactions")
     if r.plog and r.tag != TAG_SIMPLE:
         raise ChemkinError("PLOG cannot be used for third-body or fall-off reactions")
+    if r.xplog and r.tag != TAG_SIMPLE:
+        raise ChemkinError("PLOGMX/PLOGSP cannot be used for third-body or fall-off reactions")
     _convert_units(r, a_units, e_units)
     return r
 
@@ -609,6 +636,30 @@ def _convert_units(r: Reaction, a_units: str, e_units: str) -> None:
                     raise ChemkinError("PLOG pressures must be increasing")
                 last = pp
                 r.plog_table.append((pp, math.log(pp), math.log(max(a_ * conv_a, 1.e-32)), b_, e_ * e_conv / R_J_KMOL))
+        if r.xplog:
+            # ExtendedPressureLogarithmicRateExpression::Setup (:84-160) with the conversion factors of
+            # ConvertUnits (ReactionPolicy_CHEMKIN.hpp:1467-1471): baths in order of first appearance, each
+            # table with increasing pressures and non-negative A; a mixture table (PLOGMX) is required
+            conv_a = math.pow(1.e3, 1. - sum_lr) / math.pow(a_conv, 1. - sum_lr)
+            order: List[int] = []
+            for sp, *_ in r.xplog:
+                if sp not in order:
+                    order.append(sp)
+            if -1 not in order:
+                raise ChemkinError("PLOGSP needs the kinetic parameters of the mixture (PLOGMX)")
+            for sp in order:
+                pts, last = [], -math.inf
+                for sq, pa, a_, b_, e_ in r.xplog:
+                    if sq != sp:
+                        continue
+                    if a_ < 0.:
+                        raise ChemkinError("PLOGMX/PLOGSP need non-negative frequency factors")
+                    pp = pa * 101325.
+                    if pp <= last:
+                        raise ChemkinError("PLOGMX/PLOGSP pressures must be increasing")
+                    last = pp
+                    pts.append((pp, math.log(pp), math.log(max(a_ * conv_a, 1.e-32)), b_, e_ * e_conv / R_J_KMOL))
+                r.xplog_table.append((sp, pts))
         if r.explicit_rev:
             r.E_rev *= e_conv
             r.A_rev *= math.pow(1.e3, 1. - sum_lp) / math.pow(a_conv, 1. - sum_lp)
@@ -865,6 +916,26 @@ def build_tables(species: List[str], reactions: List[Reaction], thermo: List[The
         A["plog_rxn"] = np.array(prx, np.int32); A["plog_ptr"] = np.array(pptr2, np.int32)
         for k, v in pv.items():
             A["plog_" + k] = np.array(v, f64)
+    if any(r.xplog for r in reactions):
+        # extended PLOG reactions (KineticsMap_CHEMKIN.hpp:1662-1670; ExtendedPressureLogarithmicRateExpression::
+        # KineticConstant, :162-202): per reaction its baths (species index, -1 the mixture), per bath its points
+        xrx, bptr, bsp, qptr = [], [0], [], [0]
+        xv = {k: [] for k in ("p", "lnp", "lnA", "beta", "eor")}
+        for j, r in enumerate(reactions):
+            if not r.xplog:
+                continue
+            xrx.append(j)
+            for sp, pts in r.xplog_table:
+                bsp.append(sp)
+                for pp, lp, la, b_, er in pts:
+                    xv["p"].append(pp); xv["lnp"].append(lp); xv["lnA"].append(la); xv["beta"].append(b_)
+                    xv["eor"].append(er)
+                qptr.append(len(xv["p"]))
+            bptr.append(len(bsp))
+        A["xplog_rxn"] = np.array(xrx, np.int32); A["xplog_bath_ptr"] = np.array(bptr, np.int32)
+        A["xplog_bath_sp"] = np.array(bsp, np.int32); A["xplog_ptr"] = np.array(qptr, np.int32)
+        for k, v in xv.items():
+            A["xplog_" + k] = np.array(v, f64)
     if any(r.cheb for r in reactions):
         # Chebyshev reactions (ChebyshevPolynomialRateExpression::Setup, :50-75): per reaction N, M, the
         # N x M coefficients by rows and (Tmin, Tmax, log10 Pmin, log10 Pmax, conversion) with P in Pa

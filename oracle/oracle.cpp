@@ -263,10 +263,49 @@ struct Reactor {
   }
 
   // KineticsMap_CHEMKIN::ReactionRates (:1683-1768) and FallOffReactions (:1496-1550)
+  // ExtendedPressureLogarithmicRateExpression::KineticConstant(index, T, P) (:181-202): the PLOG
+  // interpolation of one bath's table q0 .. q1 - 1
+  double xplog_k(int q0, int q1, double T, double P) const {
+    const auto& pp = m.F("xplog_p"); const auto& lnp = m.F("xplog_lnp"); const auto& lA = m.F("xplog_lnA");
+    const auto& pb = m.F("xplog_beta"); const auto& pe = m.F("xplog_eor");
+    const int n = q1 - q0;
+    if (P <= pp[q0]) return std::exp(lA[q0] + pb[q0] * std::log(T) - pe[q0] / T);
+    if (P >= pp[q1 - 1]) return std::exp(lA[q1 - 1] + pb[q1 - 1] * std::log(T) - pe[q1 - 1] / T);
+    int i = 0;
+    for (i = 0; i < n - 1; ++i)
+      if (P < pp[q0 + i + 1]) break;
+    const int a = q0 + i, b = a + 1;
+    const double ln_kA = lA[a] + pb[a] * std::log(T) - pe[a] / T;
+    const double ln_kB = lA[b] + pb[b] * std::log(T) - pe[b] / T;
+    return std::exp(ln_kA + (ln_kB - ln_kA) * (std::log(P) - lnp[a]) / (lnp[b] - lnp[a]));
+  }
+
+  // KineticsMap_CHEMKIN::ExtendedPressureLogReactions (:1662-1670) with
+  // ExtendedPressureLogarithmicRateExpression::KineticConstant(T, P, cTot, c) (:162-179):
+  // k = (sum over bath species c_s k_s + (cTot - sum c_s) k_mixture) / cTot replaces the Arrhenius k
+  void extended_plog(double cTot) {
+    if (!m.i.count("xplog_rxn")) return;
+    const auto& xr = m.I("xplog_rxn"); const auto& bp = m.I("xplog_bath_ptr");
+    const auto& bs = m.I("xplog_bath_sp"); const auto& qp = m.I("xplog_ptr");
+    for (size_t k = 0; k < xr.size(); ++k) {
+      double rest = cTot;
+      for (int b = bp[k]; b < bp[k + 1]; ++b) if (bs[b] != -1) rest -= c[bs[b]];
+      double kc = 0.;
+      for (int b = bp[k]; b < bp[k + 1]; ++b) {
+        const double kb = xplog_k(qp[b], qp[b + 1], T_, P_);
+        kc += (bs[b] != -1 ? c[bs[b]] : rest) * kb;
+      }
+      kc /= cTot;
+      kArr[xr[k]] = kc;
+      kMod[xr[k]] = kc;
+    }
+  }
+
   void reaction_rates() {
     double cTot = 0.;
     for (int i = 0; i < NC; ++i) cTot += c[i];
     kinetic_constants();
+    extended_plog(cTot);
     const auto& tbr = m.I("tb_rxn"); const auto& tbp = m.I("tb_ptr");
     const auto& tbs = m.I("tb_species"); const auto& tbe = m.F("tb_eff_m1");
     for (size_t sidx = 0; sidx < tbr.size(); ++sidx) {

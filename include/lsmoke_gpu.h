@@ -95,8 +95,8 @@ void lsg_options_default(lsg_options* opt);
  * `python -m laminarsmoke_b200.mech compile KIN.CKI THERMO.CKT -o mech.lsmech`
  * (it replaces openSMOKEppCHEMKINPreProcessor + kinetics.xml, which the
  * reference loads at solvers/laminarSMOKE/readOptions.H:62-78).  A blob with
- * extended PLOG reactions (PLOGMX/PLOGSP), which the device kernels do not
- * evaluate, is refused with LSG_ERR_UNSUPPORTED. */
+ * extended PLOG (PLOGMX/PLOGSP) or extended fall-off (LOWMX/LOWSP) reactions,
+ * which the device kernels do not evaluate, is refused with LSG_ERR_UNSUPPORTED. */
 int lsg_mech_load_blob(const void* blob, size_t nbytes, int device, lsg_mech** out);
 int lsg_mech_load_file(const char* path, int device, lsg_mech** out);
 int lsg_mech_info(const lsg_mech* mech, int* nspecies, int* nreactions);

@@ -134,10 +134,11 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
   Blob b;
   if (!parse((const unsigned char*)blob, nbytes, b, err)) return false;
   try {
-    if (b.i.count("xplog_rxn")) {
-      // PLOGMX / PLOGSP (bath-gas-specific PLOG tables): the oracle evaluates them, the device
-      // kernels do not, so such a mechanism is refused rather than integrated without them
-      err = "unsupported: extended PLOG (PLOGMX/PLOGSP) reactions";
+    if (b.i.count("xplog_rxn") || b.i.count("xfo_rxn")) {
+      // PLOGMX / PLOGSP and LOWMX / LOWSP (bath-gas-specific PLOG tables and fall-off limits): the
+      // oracle evaluates them, the device kernels do not, so such a mechanism is refused rather than
+      // integrated without them
+      err = "unsupported: extended PLOG or extended fall-off reactions";
       return false;
     }
     const auto& dims = b.I("dims");

@@ -278,6 +278,11 @@ class Reaction:
     # order of first appearance its SI table [(p [Pa], ln p, ln A, beta, E/R)]
     xplog: List[Tuple[int, float, float, float, float]] = field(default_factory=list)
     xplog_table: List[Tuple[int, List[Tuple[float, float, float, float, float]]]] = field(default_factory=list)
+    # LOWMX/LOWSP, TROEMX/TROESP, SRIMX/SRISP: (kind "low" | "troe" | "sri", bath index (-1 mixture), values)
+    # per line, and per bath in order of first appearance (bath, A0, beta0, E0/R, type 0/1/2, parameters) SI
+    xfo: List[Tuple[str, int, List[float]]] = field(default_factory=list)
+    xfo_table: List[Tuple[int, float, float, float, int, List[float]]] = field(default_factory=list)
+    xfo_kinf: Tuple[float, float, float] = (0., 0., 0.)   # (A_inf, beta_inf, E_inf/R) SI
     cheb: List[float] = field(default_factory=list)   # CHEB numbers as given: N, M, a_11 .. a_NM
     cheb_T: List[float] = field(default_factory=list)  # TCHEB (Tmin, Tmax) [K]
     cheb_P: List[float] = field(default_factory=list)  # PCHEB (Pmin, Pmax) [atm]
@@ -441,6 +446,8 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
         if kw == "LOW":
             if pdr == "none":
                 raise ChemkinError("LOW only for pressure-dependent reactions")
+            if r.xfo:
+                raise ChemkinError("LOW cannot be combined with LOWMX/LOWSP")
             c = _slash_numbers(line, (3,), "LOW")
             i_low = True
             if not i_troe and not i_sri:
@@ -465,11 +472,15 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
         elif kw == "TROE":
             if pdr == "none":
                 raise ChemkinError("TROE only for pressure-dependent reactions")
+            if r.xfo:
+                raise ChemkinError("TROE cannot be combined with the extended fall-off options")
             r.troe = _slash_numbers(line, (3, 4), "TROE")
             i_troe, i_lind = True, False
         elif kw == "SRI":
             if pdr == "none":
                 raise ChemkinError("SRI only for pressure-dependent reactions")
+            if r.xfo:
+                raise ChemkinError("SRI cannot be combined with the extended fall-off options")
             r.sri = _slash_numbers(line, (3, 5), "SRI")
             i_sri, i_lind = True, False
         elif kw == "REV":
@@ -499,13 +510,36 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
             if third_body or pdr != "none" or i_low or i_troe or i_sri or r.xplog:
                 raise ChemkinError("PLOG cannot be combined with third bodies or LOW/TROE/SRI")
             r.plog.append(tuple(_slash_numbers(line, (4,), "PLOG")))
+        elif kw in ("LOWMX", "LOWSP", "TROEMX", "TROESP", "SRIMX", "SRISP"):
+            # ReactionPolicy_CHEMKIN.hpp:639-730, 984-1070, 1126-1215: the extended fall-off form, per bath
+            # (the mixture: ...MX; one species: ...SP) its low-pressure limit and optionally Troe or SRI
+            if pdr == "none":
+                raise ChemkinError(f"{kw} can be used only for pressure-dependent reactions")
+            if i_low or i_high or i_troe or i_sri or r.cheb or r.cheb_T or r.cheb_P or r.plog or r.xplog:
+                raise ChemkinError(f"{kw} cannot be combined with LOW/HIGH/TROE/SRI/CHEB/PLOG/PLOGMX")
+            kind = {"LOW": "low", "TRO": "troe", "SRI": "sri"}[kw[:3]]
+            counts = {"low": (3,), "troe": (3, 4), "sri": (3, 5)}[kind]
+            if kw.endswith("MX"):
+                r.xfo.append((kind, -1, _slash_numbers(line, counts, kw)))
+            else:
+                a, b = line.find("/"), line.rfind("/")
+                tok = line[a + 1:b].split() if 0 <= a < b else []
+                if len(tok) - 1 not in counts:
+                    raise ChemkinError(f"{kw}: wrong number of arguments in: {line.strip()}")
+                if tok[0] not in species_index:
+                    raise ChemkinError(f"{kw}: bath species not available: {tok[0]}")
+                try:
+                    vals = [float(t) for t in tok[1:]]
+                except ValueError:
+                    raise ChemkinError(f"{kw}: the coefficients are not numbers in: {line.strip()}") from None
+                r.xfo.append((kind, species_index[tok[0]], vals))
         elif kw in ("PLOGMX", "PLOGSP"):
             # ReactionPolicy_CHEMKIN.hpp:793-880: a PLOG table for the mixture (PLOGMX) or for one bath species
             # (PLOGSP), one point (p [atm], A, beta, E) per line
             if third_body:
                 raise ChemkinError(f"{kw} cannot be used for third-body reactions")
-            if i_low or i_high or i_troe or i_sri or r.cheb or r.cheb_T or r.cheb_P or r.plog:
-                raise ChemkinError(f"{kw} cannot be combined with LOW/HIGH/TROE/SRI/CHEB/PLOG")
+            if i_low or i_high or i_troe or i_sri or r.cheb or r.cheb_T or r.cheb_P or r.plog or r.xfo:
+                raise ChemkinError(f"{kw} cannot be combined with LOW/HIGH/TROE/SRI/CHEB/PLOG/LOWMX")
             if kw == "PLOGMX":
                 r.xplog.append((-1,) + tuple(_slash_numbers(line, (4,), kw)))
             else:
@@ -546,7 +580,7 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
 
     if r.ford:   # ReorderPairsOfVectors + CleanPairsOfVectors of the orders (ReactionPolicy_CHEMKIN.hpp:1266-1271)
         r.forward_orders = _reorder_clean(r.forward_orders)
-    if pdr == "all" and not i_low and not i_high and not r.cheb:
+    if pdr == "all" and not i_low and not i_high and not r.cheb and not r.xfo:
         raise ChemkinError("no pressure dependence option defined")
     if pdr == "partial" and not i_low and not i_high:
         raise ChemkinError("no pressure dependence option defined")
@@ -560,6 +594,12 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
             raise ChemkinError(f"CHEB: expected {n_ * m_} coefficients, given {len(r.cheb) - 2}")
         r.cheb_T = r.cheb_T or [300., 2500.]
         r.cheb_P = r.cheb_P or [0.001, 100.]
+        r.tag = TAG_SIMPLE
+    elif r.xfo:
+        # REACTION_EXTENDEDFALLOFF (ReactionPolicy_CHEMKIN.hpp:1300-1301): the kinetics tables keep it as a
+        # simple reaction; the extended fall-off tables carry k
+        if r.explicit_rev:
+            raise ChemkinError("explicitly reversible extended fall-off reactions are not allowed")
         r.tag = TAG_SIMPLE
     elif not third_body and pdr == "none":
         r.tag = TAG_SIMPLE
@@ -594,6 +634,7 @@ def _convert_units(r: Reaction, a_units: str, e_units: str) -> None:
         "KELV": 1.e3 * R_J_MOL,
     }[e_units]
     a_conv = 1. if a_units == "MOLE" else NAV_MOL
+    a_line, e_line = r.A, r.E   # the reaction line's values before conversion
     sum_lr = 0.   # ReactionOrders: the sums of the rate-law orders (lambda), FORD included
     for _, v in (r.forward_orders if r.ford else r.reactants):
         sum_lr += v
@@ -636,6 +677,31 @@ def _convert_units(r: Reaction, a_units: str, e_units: str) -> None:
                     raise ChemkinError("PLOG pressures must be increasing")
                 last = pp
                 r.plog_table.append((pp, math.log(pp), math.log(max(a_ * conv_a, 1.e-32)), b_, e_ * e_conv / R_J_KMOL))
+        if r.xfo:
+            # ExtendedFallOff::Setup (ExtendedFallOff.hpp:71-169) with the conversion factors of ConvertUnits
+            # (ReactionPolicy_CHEMKIN.hpp:1415-1453): k_inf from the reaction line, a low-pressure limit per
+            # bath, the mixture's required; a bath takes one low-pressure line and at most one Troe or SRI line
+            conv_a0 = math.pow(1.e3, -sum_lr) / math.pow(a_conv, -sum_lr)
+            order: List[int] = []
+            for _, sp, _ in r.xfo:
+                if sp not in order:
+                    order.append(sp)
+            for sp in order:
+                kinds = [kd for kd, sq, _ in r.xfo if sq == sp]
+                if kinds.count("low") != 1 or len(kinds) > 2:
+                    raise ChemkinError("extended fall-off: each bath needs one LOW line and at most one TROE or SRI")
+            if -1 not in order:
+                raise ChemkinError("extended fall-off needs the low-pressure parameters of the mixture (LOWMX)")
+            for sp in order:
+                if sp != -1 and sp in r.tb_species and r.tb_eff[r.tb_species.index(sp)] != 1.:
+                    raise ChemkinError("extended fall-off: the third-body efficiency of a bath species must be 1")
+                low = next(v for kd, sq, v in r.xfo if sq == sp and kd == "low")
+                extra = [(kd, v) for kd, sq, v in r.xfo if sq == sp and kd != "low"]
+                kind, par = (extra[0] if extra else ("low", []))
+                r.xfo_table.append((sp, low[0] * conv_a0, low[1], low[2] * (e_conv / R_J_KMOL),
+                                    {"low": 0, "troe": 1, "sri": 2}[kind], list(par)))
+            conv_ainf = math.pow(1.e3, 1. - sum_lr) / math.pow(a_conv, 1. - sum_lr)
+            r.xfo_kinf = (a_line * conv_ainf, r.beta, e_line * (e_conv / R_J_KMOL))
         if r.xplog:
             # ExtendedPressureLogarithmicRateExpression::Setup (:84-160) with the conversion factors of
             # ConvertUnits (ReactionPolicy_CHEMKIN.hpp:1467-1471): baths in order of first appearance, each
@@ -916,6 +982,28 @@ def build_tables(species: List[str], reactions: List[Reaction], thermo: List[The
         A["plog_rxn"] = np.array(prx, np.int32); A["plog_ptr"] = np.array(pptr2, np.int32)
         for k, v in pv.items():
             A["plog_" + k] = np.array(v, f64)
+    if any(r.xfo for r in reactions):
+        # extended fall-off reactions (KineticsMap_CHEMKIN.hpp:1672-1681; ExtendedFallOff::KineticConstant,
+        # ExtendedFallOff.hpp:170-240): k_inf (A, beta, E/R), efficiencies - 1, per bath the low-pressure limit,
+        # the form (0 Lindemann, 1 Troe, 2 SRI) and its parameters
+        xr, kinf, tbp, tbs, tbe, bp, bs, low, bty, pp, par = [], [], [0], [], [], [0], [], [], [], [0], []
+        for j, r in enumerate(reactions):
+            if not r.xfo:
+                continue
+            xr.append(j)
+            kinf += list(r.xfo_kinf)
+            tbs += r.tb_species
+            tbe += [e - 1. for e in r.tb_eff]
+            tbp.append(len(tbs))
+            for sp, a0, b0, e0, ty, pr in r.xfo_table:
+                bs.append(sp); low += [a0, b0, e0]; bty.append(ty); par += pr; pp.append(len(par))
+            bp.append(len(bs))
+        A["xfo_rxn"] = np.array(xr, np.int32); A["xfo_kinf"] = np.array(kinf, f64)
+        A["xfo_tb_ptr"] = np.array(tbp, np.int32); A["xfo_tb_sp"] = np.array(tbs, np.int32)
+        A["xfo_tb_eff_m1"] = np.array(tbe, f64)
+        A["xfo_bath_ptr"] = np.array(bp, np.int32); A["xfo_bath_sp"] = np.array(bs, np.int32)
+        A["xfo_low"] = np.array(low, f64); A["xfo_type"] = np.array(bty, np.int32)
+        A["xfo_par_ptr"] = np.array(pp, np.int32); A["xfo_par"] = np.array(par, f64)
     if any(r.xplog for r in reactions):
         # extended PLOG reactions (KineticsMap_CHEMKIN.hpp:1662-1670; ExtendedPressureLogarithmicRateExpression::
         # KineticConstant, :162-202): per reaction its baths (species index, -1 the mixture), per bath its points

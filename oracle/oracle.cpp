@@ -301,6 +301,58 @@ struct Reactor {
     }
   }
 
+  // KineticsMap_CHEMKIN::ExtendedFallOffReactions (:1672-1681) with ExtendedFallOff::KineticConstant
+  // (ExtendedFallOff.hpp:170-240): per bath k = k_inf Pr / (1 + Pr) F with its own low-pressure limit
+  // and form, M from the reaction's efficiencies; the baths weighted as in the extended PLOG
+  void extended_falloff(double cTot) {
+    if (!m.i.count("xfo_rxn")) return;
+    const auto& xr = m.I("xfo_rxn"); const auto& ki = m.F("xfo_kinf");
+    const auto& tp = m.I("xfo_tb_ptr"); const auto& ts = m.I("xfo_tb_sp"); const auto& te = m.F("xfo_tb_eff_m1");
+    const auto& bp = m.I("xfo_bath_ptr"); const auto& bs = m.I("xfo_bath_sp"); const auto& lo = m.F("xfo_low");
+    const auto& ty = m.I("xfo_type"); const auto& pp = m.I("xfo_par_ptr"); const auto& pa = m.F("xfo_par");
+    const double T = T_;
+    for (size_t r = 0; r < xr.size(); ++r) {
+      const double kInf = ki[3 * r] * std::pow(T, ki[3 * r + 1]) * std::exp(-ki[3 * r + 2] / T);
+      double M = cTot;
+      for (int q = tp[r]; q < tp[r + 1]; ++q) M += te[q] * c[ts[q]];
+      double rest = cTot;
+      for (int b = bp[r]; b < bp[r + 1]; ++b) if (bs[b] != -1) rest -= c[bs[b]];
+      double kc = 0.;
+      for (int b = bp[r]; b < bp[r + 1]; ++b) {
+        const double k0 = lo[3 * b] * std::pow(T, lo[3 * b + 1]) * std::exp(-lo[3 * b + 2] / T);
+        const double Pr = k0 / kInf * M;
+        const double* t = pa.data() + pp[b];
+        const int nt = pp[b + 1] - pp[b];
+        double F = 1.;
+        if (ty[b] == 1) {
+          double Fcent = (1. - t[0]) * std::exp(-T / t[1]) + t[0] * std::exp(-T / t[2]);
+          if (nt == 4) Fcent += std::exp(-t[3] / T);
+          double logFcent = -300.;
+          if (Fcent > 1e-300) logFcent = std::log10(Fcent);
+          if (Pr > 1.e-32) {
+            const double cc = -0.4 - 0.67 * logFcent;
+            const double n = 0.75 - 1.27 * logFcent;
+            const double e = std::log10(Pr) + cc;
+            const double q = e / (n - 0.14 * e);
+            F = std::pow(10., logFcent / (1. + q * q));
+          } else {
+            const double q = 1. / 0.14;
+            F = std::pow(10., logFcent / (1. + q * q));
+          }
+        } else if (ty[b] == 2) {
+          const double l = std::log10(Pr);
+          const double X = 1. / (1. + l * l);
+          F = std::pow(t[0] * std::exp(-t[1] / T) + std::exp(-T / t[2]), X);
+          if (nt == 5) F *= t[3] * std::pow(T, t[4]);
+        }
+        kc += (bs[b] != -1 ? c[bs[b]] : rest) * (kInf * (Pr / (1. + Pr)) * F);
+      }
+      kc /= cTot;
+      kArr[xr[r]] = kc;
+      kMod[xr[r]] = kc;
+    }
+  }
+
   void reaction_rates() {
     double cTot = 0.;
     for (int i = 0; i < NC; ++i) cTot += c[i];
@@ -349,6 +401,7 @@ struct Reactor {
       corr[k] = cabr ? (1. / (1. + Pr)) * wF : kInf[k] * (Pr / (1. + Pr)) * wF / kArr[j];
     }
     for (size_t k = 0; k < fr.size(); ++k) kMod[fr[k]] *= corr[k];
+    extended_falloff(cTot);
 
     // StoichiometricMap::ProductOfConcentrations (:512-598): factors in species order, forward orders
     // lambda (FORD or the reactant coefficients)

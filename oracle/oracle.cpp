@@ -104,6 +104,7 @@ struct Reactor {
   bool arr_recalc = true, hs_recalc = true;
   std::vector<double> kArr, uKeq, kRev, kInf, logFcent, rdh, rds, kMod, fwd, rev, net, corr;
   std::vector<double> x, c, R;
+  std::vector<double> Mtb;   // M of each third-body reaction at the last reaction_rates()
   long long n_calls = 0;
 
   explicit Reactor(const Mech& mech) : m(mech), NC(mech.nc), NR(mech.nr) {
@@ -114,6 +115,46 @@ struct Reactor {
     kRev.resize(m.I("rev_explicit").size());
     kInf.resize(m.I("fo_rxn").size()); logFcent.resize(kInf.size()); corr.resize(kInf.size());
     x.resize(NC); c.resize(NC); R.resize(NC);
+    Mtb.resize(m.I("tb_rxn").size());
+  }
+
+  // KineticsMap_CHEMKIN::FallOffReactionsCorrection (:1552-1610): the fall-off factor of slot k at the
+  // concentrations cc, with the constants of the last reaction_rates()
+  double falloff_correction(int k, double cTot, const double* cc) const {
+    const auto& fr = m.I("fo_rxn"); const auto& fty = m.I("fo_type"); const auto& fsg = m.I("fo_single");
+    const auto& fp = m.I("fo_ptr"); const auto& fs = m.I("fo_species"); const auto& fe = m.F("fo_eff_m1");
+    const auto& fd = m.F("fo_d"); const auto& fee = m.F("fo_e");
+    double M;
+    if (fsg[k] < 0) {
+      M = cTot;
+      for (int q = fp[k]; q < fp[k + 1]; ++q) M += cc[fs[q]] * fe[q];
+    } else {
+      M = cc[fsg[k]] + 1.e-16;
+    }
+    const int j = fr[k];
+    const double Pr = kArr[j] * M / kInf[k];
+    double wF = 1.;
+    if (fty[k] == 1) {
+      if (Pr > 1.e-32) {
+        const double nTroe = 0.75 - 1.27 * logFcent[k];
+        const double cTroe = -0.4 - 0.67 * logFcent[k];
+        const double sTroe = std::log10(Pr) + cTroe;
+        const double q = sTroe / (nTroe - 0.14 * sTroe);
+        wF = std::pow(10., logFcent[k] / (1. + q * q));
+      } else {
+        const double q = 1. / 0.14;
+        wF = std::pow(10., logFcent[k] / (1. + q * q));
+      }
+    } else if (fty[k] == 2) {
+      double xSRI = 0.;
+      if (Pr > 1.e-32) {
+        const double l = std::log10(Pr);
+        xSRI = 1. / (1. + l * l);
+      }
+      wF = std::pow(logFcent[k], xSRI) * fd[k];
+      if (fee[k] != 0.) wF *= std::pow(T_, fee[k]);
+    }
+    return kInf[k] * (Pr / (1. + Pr)) * wF / kArr[j];
   }
 
   // ThermodynamicsMap_CHEMKIN::cp_over_R (:436-454)
@@ -353,9 +394,10 @@ struct Reactor {
     }
   }
 
-  void reaction_rates() {
+  void reaction_rates(double cTot_given = -1.) {
     double cTot = 0.;
     for (int i = 0; i < NC; ++i) cTot += c[i];
+    if (cTot_given >= 0.) cTot = cTot_given;   // ReactionRates(c, cTot) with the caller's cTot
     kinetic_constants();
     extended_plog(cTot);
     const auto& tbr = m.I("tb_rxn"); const auto& tbp = m.I("tb_ptr");
@@ -364,6 +406,7 @@ struct Reactor {
       double M = cTot;
       for (int q = tbp[sidx]; q < tbp[sidx + 1]; ++q) M += c[tbs[q]] * tbe[q];
       kMod[tbr[sidx]] *= M;
+      Mtb[sidx] = M;
     }
     const auto& fr = m.I("fo_rxn"); const auto& fty = m.I("fo_type"); const auto& fsg = m.I("fo_single");
     const auto& fp = m.I("fo_ptr"); const auto& fs = m.I("fo_species"); const auto& fe = m.F("fo_eff_m1");
@@ -1358,6 +1401,130 @@ int orc_steady_sources(void* mech, double P, const double* y, double* s_implicit
     yp[k] = y[k];
     s_implicit[k] = J;
     s_explicit[k] = S0[k] - J * y[k];
+  }
+  return 0;
+}
+
+// The steady solvers' default linearisation (sparseJacobian true): linearModel::reactionJacobianSparse
+// (steady/linearModel.H:172-232).  Species entries of the diagonal: JacobianSparsityPatternMap::Jacobian
+// (maps/JacobianSparsityPatternMap.hpp:427-560) at omega* = max(max(y, 0), 1e-13) times MW, i.e.
+//   J_k = sum over reactions of (nu_prod - nu_reac)_k * [ lambda_f r_f / omega*_k - lambda_b r_b / omega*_k
+//         + third body (r_f - r_b) c*_k / omega*_k (eff - 1) / M + fall-off (r_f - r_b) dG / G
+//         + CABR (r_f - r_b) ]
+// with each bracket term present where the reaction's orders, efficiencies or bath species name k, and the
+// fall-off derivative a 1e-4 forward difference of FallOffReactionsCorrection in omega_k.  The T entry is the
+// forward difference of the dense path.  species / energy: the speciesEquations / energyEquation switches.
+int orc_steady_sources_sparse(void* mech, double P, const double* y, double* s_implicit, double* s_explicit,
+                              int species, int energy) {
+  const orc::Mech& m = *(const orc::Mech*)mech;
+  const int NC = m.nc, NE = NC + 1, NR = m.nr;
+  const auto& MW = m.F("mw");
+  orc::Reactor r(m);
+  r.P0 = P;
+  r.energy = true;
+  std::vector<double> yc(NE), dy(NE), S0(NE), Sp(NE), yp(y, y + NE), J(NE, 0.);
+  auto sources = [&](const double* yy, double* S) {   // reactionSourceTerms: omega = max(y, 0)
+    for (int i = 0; i < NC; ++i) yc[i] = std::max(yy[i], 0.);
+    yc[NC] = yy[NC];
+    r.equations(yc.data(), dy.data());
+    for (int i = 0; i < NC; ++i) S[i] = r.R[i] * MW[i];
+    S[NC] = r.QR;
+  };
+  sources(y, S0.data());
+  if (species) {
+    const double eps = 1.e-13;   // SetEpsilon(1e-13)
+    const double T = y[NC];
+    std::vector<double> om(NC), cs(NC), rf(NR), rb(NR), Jd(NC, 0.), net(NR);
+    for (int i = 0; i < NC; ++i) {
+      const double o = std::max(y[i], 0.);
+      om[i] = (o > eps) ? o : eps;
+    }
+    double u = 0.;
+    for (int i = 0; i < NC; ++i) u += om[i] / MW[i];
+    const double MWs = 1. / u;
+    const double cTs = P / orc::R_J_KMOL / T;
+    const double rhos = cTs * MWs;
+    for (int i = 0; i < NC; ++i) cs[i] = om[i] * rhos / MW[i];
+    for (int i = 0; i < NC; ++i) r.c[i] = cs[i];
+    r.P_ = P;
+    r.h_over_RT(T);
+    r.kin_set_T(T);
+    r.reaction_rates(cTs);
+    const auto& isrev = m.I("is_reversible");
+    for (int j = 0; j < NR; ++j) rf[j] = r.kMod[j] * r.fwd[j];
+    for (int j = 0; j < NR; ++j) rb[j] = isrev[j] ? r.rev[j] * r.kMod[j] : 0.;
+    const auto& op = m.I("ford_ptr"); const auto& os = m.I("ford_species"); const auto& ov = m.F("ford_val");
+    const auto& rp = m.I("reac_ptr"); const auto& rs = m.I("reac_species"); const auto& rn = m.F("reac_nu");
+    const auto& pp = m.I("prod_ptr"); const auto& ps = m.I("prod_species"); const auto& pn = m.F("prod_nu");
+    const auto& tbr = m.I("tb_rxn"); const auto& tbp = m.I("tb_ptr");
+    const auto& tbs = m.I("tb_species"); const auto& tbe = m.F("tb_eff_m1");
+    const auto& fr = m.I("fo_rxn"); const auto& fsg = m.I("fo_single");
+    const auto& fp = m.I("fo_ptr"); const auto& fs = m.I("fo_species");
+    std::vector<double> cplus(cs);
+    for (int k = 0; k < NC; ++k) {
+      std::fill(net.begin(), net.end(), 0.);
+      for (int j = 0; j < NR; ++j)
+        for (int q = op[j]; q < op[j + 1]; ++q)
+          if (os[q] == k) net[j] = ov[q] * rf[j] / om[k];
+      for (int j = 0; j < NR; ++j)
+        for (int q = pp[j]; q < pp[j + 1]; ++q)
+          if (ps[q] == k) net[j] -= pn[q] * rb[j] / om[k];
+      for (size_t sidx = 0; sidx < tbr.size(); ++sidx)
+        for (int q = tbp[sidx]; q < tbp[sidx + 1]; ++q)
+          if (tbs[q] == k) {
+            const int j = tbr[sidx];
+            net[j] += (rf[j] - rb[j]) * cs[k] / om[k] * tbe[q] / r.Mtb[sidx];
+          }
+      for (size_t f = 0; f < fr.size(); ++f) {
+        bool has = fsg[f] == k;
+        if (fsg[f] < 0)
+          for (int q = fp[f]; q < fp[f + 1]; ++q) if (fs[q] == k) has = true;
+        if (!has) continue;
+        const int j = fr[f];
+        const bool cabr = m.i.count("fo_cabr") && m.I("fo_cabr")[f] != 0;
+        if (cabr) {
+          net[j] += (rf[j] - rb[j]);
+        } else {
+          const double fo_eps = 1.e-4;
+          cplus[k] = (om[k] + fo_eps) * rhos / MW[k];
+          const double G = r.falloff_correction((int)f, cTs, cs.data());
+          const double Gp = r.falloff_correction((int)f, cTs, cplus.data());
+          const double dG = (Gp - G) / fo_eps;
+          cplus[k] = om[k] * rhos / MW[k];
+          net[j] += (rf[j] - rb[j]) * dG / G;
+        }
+      }
+      for (int j = 0; j < NR; ++j)
+        for (int q = rp[j]; q < rp[j + 1]; ++q)
+          if (rs[q] == k) Jd[k] -= rn[q] * net[j];
+      for (int j = 0; j < NR; ++j)
+        for (int q = pp[j]; q < pp[j + 1]; ++q)
+          if (ps[q] == k) Jd[k] += pn[q] * net[j];
+    }
+    for (int i = 0; i < NC; ++i) J[i] = Jd[i] * MW[i];
+  }
+  if (energy) {   // the dense path's forward difference, for T only (linearModel.H:195-230)
+    const double ZERO_DER = std::sqrt(orc::TINY_FLOAT);
+    const double ETA2 = std::sqrt(orc::MACH_EPS_DOUBLE);
+    const double TOLR = 1.e-7, TOLA = 1.e-12;
+    const int kd = NC;
+    sources(y, S0.data());
+    const double hf = 1.;
+    const double error_weight = 1. / (TOLA + TOLR * std::fabs(y[kd]));
+    double hJ = ETA2 * std::fabs(std::max(y[kd], 1. / error_weight));
+    const double hJf = hf / error_weight;
+    hJ = std::max(hJ, hJf);
+    hJ = std::max(hJ, ZERO_DER);
+    const double d = std::min(hJ, 1.e-3 + 1e-3 * std::fabs(y[kd]));
+    const double udy = 1. / d;
+    yp[kd] += d;
+    sources(yp.data(), Sp.data());
+    J[kd] = (Sp[kd] - S0[kd]) * udy;
+    yp[kd] = y[kd];
+  }
+  for (int k = 0; k < NE; ++k) {
+    s_implicit[k] = J[k];
+    s_explicit[k] = S0[k] - J[k] * y[k];
   }
   return 0;
 }

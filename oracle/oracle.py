@@ -54,6 +54,8 @@ def lib():
                                           C.c_double, C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]
         L.orc_formation_rates.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
         L.orc_steady_sources.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_steady_sources_sparse.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_int, C.c_int]
         L.orc_reaction_step_drg.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.POINTER(OrcDrgOptions), C.c_int,
                                             C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_double,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -124,6 +126,15 @@ class OracleMechanism:
         si = np.zeros(y.size)
         se = np.zeros(y.size)
         lib().orc_steady_sources(self.h, p, _ptr(y), _ptr(si), _ptr(se))
+        return si, se
+
+    def steady_sources_sparse(self, y, p=101325.0, species=True, energy=True):
+        """(S_implicit, S_explicit) [NC + 1] with the steady solvers' default analytic species diagonal
+        (sparseJacobian true)."""
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        si = np.zeros(y.size)
+        se = np.zeros(y.size)
+        lib().orc_steady_sources_sparse(self.h, p, _ptr(y), _ptr(si), _ptr(se), int(species), int(energy))
         return si, se
 
     def fd_jacobian(self, y, h, rtol=1e-7, atol=1e-12, p=101325.0, y_max_T=6000.0):

@@ -23,7 +23,14 @@ expected outputs.  Inputs are seeded (numpy PCG64, seeds below):
                        (tests/test_plog.py, test_cheb.py, test_cabr.py) at
                        32 states and three pressures each;
 * h2co_properties.npz -- the property update (oracle/properties.py) of the
-                       h2co_step result at 1 and 3 atm, with Soret terms.
+                       h2co_step result at 1 and 3 atm, with Soret terms;
+* h2co_drg_step.npz -- a DRG-reduced step of 48 cells (key species H2, O2,
+                       CO; epsilon 1e-3 below 1000 K, 1e-2 above);
+* h2co_sparse_sources.npz -- the steady solvers' analytic-diagonal sources of
+                       32 states at 1.5 bar;
+* xrates_rhs.npz    -- RHS of the PLOGMX/PLOGSP and LOWMX/LOWSP test
+                       mechanisms (tests/test_xplog.py, test_xfo.py) at 32
+                       states and three pressures each.
 """
 import os
 import sys
@@ -132,6 +139,38 @@ def main():
     p = np.where(np.arange(g["T"].size) % 2 == 0, 101325.0, 3.0 * 101325.0)
     f = OracleProperties(data).evaluate(g["Y"], g["T"], p, soret=True)
     np.savez_compressed(os.path.join(HERE, "h2co_properties.npz"), p=p, **f)
+
+    Y, T = cells.h2co_mixing(species, A["mw"], 48, seed=40)
+    key = [species.index(n) for n in ("H2", "O2", "CO")]
+    bands = ((1000., 1e-3), (1e6, 1e-2))
+    Yd, Td, Qd, std, cnt, nsp, nrx = orc.reaction_step_drg(Y, T, 1e-5, key, bands=bands, min_T=300.0)
+    np.savez_compressed(os.path.join(HERE, "h2co_drg_step.npz"), Y0=Y, T0=T, dt=1e-5, key=np.array(key),
+                        bands=np.array(bands), Y=Yd, T=Td, Q=Qd, status=std, counters=cnt, n_species=nsp,
+                        n_reactions=nrx)
+
+    Y, T = cells.h2co_mixing(species, A["mw"], 32, seed=41)
+    ys = np.concatenate([Y, T[:, None]], axis=1)
+    si = np.zeros_like(ys)
+    se = np.zeros_like(ys)
+    for k in range(32):
+        si[k], se[k] = orc.steady_sources_sparse(ys[k], 1.5e5)
+    np.savez_compressed(os.path.join(HERE, "h2co_sparse_sources.npz"), y=ys, p=1.5e5, S_implicit=si,
+                        S_explicit=se)
+
+    import test_xfo
+    import test_xplog
+    out = {}
+    for name, dm in (("xplog", test_xplog.xplog_mechanism()[0]), ("xfo", test_xfo.xfo_mechanism()[0])):
+        o = OracleMechanism(dm)
+        rng = np.random.default_rng(42)
+        Y = rng.uniform(0.0, 1.0, (32, o.n_species))
+        Y /= Y.sum(axis=1, keepdims=True)
+        T = rng.uniform(700.0, 2400.0, 32)
+        ys = np.concatenate([Y, T[:, None]], axis=1)
+        out[f"{name}_y"] = ys
+        for patm in (0.3, 2.0, 20.0):
+            out[f"{name}_dy_{patm}"] = np.array([o.rhs(ys[k], patm * 101325.0)[0] for k in range(32)])
+    np.savez_compressed(os.path.join(HERE, "xrates_rhs.npz"), **out)
 
 
 if __name__ == "__main__":

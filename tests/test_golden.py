@@ -106,6 +106,39 @@ def test_oracle_properties_golden(h2co):
         np.testing.assert_allclose(v, g[key], rtol=1e-13, atol=0., err_msg=key)
 
 
+def test_oracle_drg_golden(oracle_h2co):
+    g = _load("h2co_drg_step.npz")
+    bands = tuple(tuple(b) for b in g["bands"])
+    Y, T, Q, st, cnt, nsp, nrx = oracle_h2co.reaction_step_drg(g["Y0"], g["T0"], float(g["dt"]), list(g["key"]),
+                                                               bands=bands, min_T=300.0)
+    for got, key in ((st, "status"), (cnt, "counters"), (nsp, "n_species"), (nrx, "n_reactions")):
+        np.testing.assert_array_equal(got, g[key], err_msg=key)
+    np.testing.assert_allclose(T, g["T"], rtol=1e-13)
+    np.testing.assert_allclose(Y, g["Y"], rtol=1e-12, atol=1e-18)
+    np.testing.assert_allclose(Q, g["Q"], rtol=1e-12, atol=1e-9)
+
+
+def test_oracle_sparse_sources_golden(oracle_h2co):
+    g = _load("h2co_sparse_sources.npz")
+    for k in range(g["y"].shape[0]):
+        si, se = oracle_h2co.steady_sources_sparse(g["y"][k], float(g["p"]))
+        np.testing.assert_allclose(si, g["S_implicit"][k], rtol=1e-12, atol=1e-300)
+        np.testing.assert_allclose(se, g["S_explicit"][k], rtol=1e-12, atol=1e-300)
+
+
+def test_oracle_extended_rates_golden():
+    import test_xfo
+    import test_xplog
+    from oracle.oracle import OracleMechanism
+    g = _load("xrates_rhs.npz")
+    for name, dm in (("xplog", test_xplog.xplog_mechanism()[0]), ("xfo", test_xfo.xfo_mechanism()[0])):
+        o = OracleMechanism(dm)
+        ys = g[f"{name}_y"]
+        for patm in (0.3, 2.0, 20.0):
+            dy = np.array([o.rhs(ys[k], patm * 101325.0)[0] for k in range(ys.shape[0])])
+            np.testing.assert_allclose(dy, g[f"{name}_dy_{patm}"], rtol=1e-13, atol=1e-300, err_msg=name)
+
+
 # ---- the library against the fixtures (GPU) ----
 
 def _gpu_step(data, g, **kw):

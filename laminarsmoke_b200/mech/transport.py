@@ -76,11 +76,16 @@ class TransportRecord:
 
 def read_transport(text: str) -> Dict[str, TransportRecord]:
     """CHEMKIN transport file: one species per line, name then six numbers;
-    '!' starts a comment.  Keys are upper-case names."""
+    '!' starts a comment.  As TransportReaderPolicy_CHEMKIN::ReadFromASCIIFile
+    (kernel/transport/TransportReaderPolicy_CHEMKIN.hpp:52-79) reads it, the
+    first line containing END or end ends the file and the first record of a
+    species is the one kept.  Keys are upper-case names."""
     db: Dict[str, TransportRecord] = {}
     for raw in text.splitlines():
         line = raw.split("!", 1)[0].strip()
-        if not line or line.upper().startswith("END"):
+        if "END" in line or "end" in line:
+            break
+        if not line:
             continue
         tok = line.split()
         if len(tok) < 7:
@@ -92,7 +97,7 @@ def read_transport(text: str) -> Dict[str, TransportRecord]:
             raise TransportError(f"bad transport record {raw!r}") from e
         if shape not in (0, 1, 2):
             raise TransportError(f"bad molecule shape {shape} for {tok[0]}")
-        db[tok[0].upper()] = TransportRecord(tok[0], shape, *vals)
+        db.setdefault(tok[0].upper(), TransportRecord(tok[0], shape, *vals))
     return db
 
 

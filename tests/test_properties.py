@@ -234,3 +234,34 @@ def test_gpu_properties_without_transport_data(cuda):
     Y = torch.full((len(species), 4), 1. / len(species), dtype=torch.float64, device=cuda)
     with pytest.raises(lsg.LsgError):
         ctx.properties_device(Y, torch.full((4,), 1000., dtype=torch.float64, device=cuda))
+
+
+def test_transport_file_errors():
+    from laminarsmoke_b200.mech import transport as tr
+    with pytest.raises(tr.TransportError):
+        tr.read_transport("N2 1 97.53 3.621 0.0 1.76\n")               # six fields
+    with pytest.raises(tr.TransportError):
+        tr.read_transport("N2 3 97.53 3.621 0.0 1.76 4.0\n")           # shape 3
+    with pytest.raises(tr.TransportError):
+        tr.read_transport("N2 1 97.53 abc 0.0 1.76 4.0\n")
+    db = tr.read_transport("! comment\n\nn2 1 97.53 3.621 0.0 1.76 4.0 ! trailing\nN2 1 1 1 1 1 1\n"
+                           "END\nO2 1 1 1 1 1 1\n")
+    assert list(db) == ["N2"] and db["N2"].sigma == 3.621   # case-insensitive; first record kept; END stops
+    st_args = _n2_o2_h2_h2o_ar()
+    with pytest.raises(tr.TransportError):
+        tr.SpeciesTransport(["N2", "XX"], st_args.mw[:2], st_args.cp_ht[:2], st_args.cp_lt[:2], st_args.t_mid[:2],
+                            tr.read_transport(TRC))
+
+
+def test_compile_with_transport_rejects_missing_species(tmp_path):
+    import subprocess
+    import sys
+    from laminarsmoke_b200.mech import synthetic
+    s = synthetic.generate(12, 10, seed=3)
+    (tmp_path / "k.cki").write_text(s.kinetics)
+    (tmp_path / "t.ckt").write_text(s.thermo)
+    (tmp_path / "tr.trc").write_text(TRC)                                # lacks most of the species
+    r = subprocess.run([sys.executable, "-m", "laminarsmoke_b200.mech", "compile", str(tmp_path / "k.cki"),
+                        str(tmp_path / "t.ckt"), "--transport", str(tmp_path / "tr.trc"), "-o",
+                        str(tmp_path / "m.lsmech")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1 and "no transport data" in r.stderr

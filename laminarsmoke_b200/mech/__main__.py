@@ -46,6 +46,15 @@ def main(argv=None) -> int:
         arrays, species = blob.unpack(f.read())
     dims = arrays["dims"]
     print(f"{args.blob}: {int(dims[0])} species, {int(dims[1])} reactions")
+    extras = [f"{len(arrays[k])} {what}" for k, what in (
+        ("plog_rxn", "PLOG"), ("cheb_rxn", "CHEB"), ("xplog_rxn", "PLOGMX/PLOGSP (oracle only)"),
+        ("xfo_rxn", "LOWMX/LOWSP (oracle only)")) if k in arrays]
+    if extras:
+        print("  reactions with " + ", ".join(extras))
+    if "tr_eta" in arrays:
+        print(f"  transport fits: yes ({len(arrays['tr_iteta'])} species with thermal-diffusion ratios)")
+    else:
+        print("  transport fits: no")
     return 0
 
 

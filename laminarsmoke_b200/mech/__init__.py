@@ -16,6 +16,9 @@ workloads of this project use:
 * ``"syn500"``  -- seeded synthetic mechanism, 500 species / 3 000 reactions;
 * ``"syn120p"``, ``"syn500p"`` -- the same mechanisms with physically bounded
                    activation energies and rate constants (integrable);
+* ``"syn120t"``  -- ``syn120p`` compiled with synthetic transport records
+                   (``synthetic.transport_text``), for the property update at
+                   120 species;
 * ``"h2co+K"``  -- POLIMI_H2CO_1412 with K chemically inert copies of N2 added
                    (``pad_inert``): the H2/CO chemistry in a mechanism of 14 + K
                    species, which exercises the large-mechanism path with
@@ -74,6 +77,11 @@ def load(name: str) -> Tuple[bytes, List[str]]:
             data = f.read()
         _, species = _blob.unpack(data)
         return data, species
+    if name == "syn120t":
+        from . import chemkin, synthetic
+        s = synthetic.generate(120, 800, 1201, physical=True)
+        m = chemkin.compile_mechanism(s.kinetics, s.thermo, transport_text=synthetic.transport_text(s))
+        return _blob.pack(m.arrays, m.species), m.species
     if name in SYNTHETIC:
         from . import chemkin, synthetic
         ns, nr, seed, physical = SYNTHETIC[name]

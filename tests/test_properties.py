@@ -265,3 +265,26 @@ def test_compile_with_transport_rejects_missing_species(tmp_path):
                         str(tmp_path / "t.ckt"), "--transport", str(tmp_path / "tr.trc"), "-o",
                         str(tmp_path / "m.lsmech")], capture_output=True, text=True, timeout=120)
     assert r.returncode == 1 and "no transport data" in r.stderr
+
+
+def test_synthetic_transport_120_species():
+    """The 120-species synthetic mechanism with synthetic transport records: fits, oracle fields, and the
+    library's host-side checks (on a machine without a GPU the load gets as far as the CUDA call)."""
+    import ctypes as C
+    from laminarsmoke_b200 import lsg, mech
+    from oracle.properties import OracleProperties
+    data, sp = mech.load("syn120t")
+    o = OracleProperties(data)
+    rng = np.random.default_rng(1)
+    Y = rng.uniform(0, 1, (16, len(sp)))
+    Y /= Y.sum(axis=1, keepdims=True)
+    T = rng.uniform(400, 2500, 16)
+    f = o.evaluate(Y, T, np.full(16, 1e5), soret=True)
+    assert all(np.isfinite(v).all() for v in f.values())
+    assert np.all(f["mu"] > 0) and np.all(f["Dmix"] > 0) and f["Dsoret"].shape == (16, len(o.iteta))
+    buf = (C.c_ubyte * len(data)).from_buffer_copy(data)
+    h = C.c_void_p()
+    rc = lsg.lib().lsg_mech_load_blob(C.cast(buf, C.c_void_p), len(data), 0, C.byref(h))
+    assert rc in (0, -3)                                  # LSG_OK with a GPU, LSG_ERR_CUDA without one
+    if rc == 0:
+        lsg.lib().lsg_mech_destroy(h)

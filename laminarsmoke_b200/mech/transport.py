@@ -228,19 +228,21 @@ class SpeciesTransport:
 
     def viscosity(self, T: float) -> np.ndarray:
         """[kg/m/s] (SingleSpeciesViscosity, :525-534; the species delta* stays 0)."""
-        om = np.array([omega22(T / self.eps_kb[k], 0.) for k in range(self.nc)])
+        kb_over_eps = 1. / self.eps_kb
+        om = np.array([omega22(T * kb_over_eps[k], 0.) for k in range(self.nc)])   # TkStar = T kb/eps
         return self.coeff_eta * math.sqrt(T) / om
 
     def conductivity(self, T: float) -> np.ndarray:
         """[W/m/K] (SpeciesThermalConductivities, :323-336, 419-500)."""
         eta = self.viscosity(T)
-        aux = np.sqrt(self.eps_kb / T)
+        aux = np.sqrt(self.eps_kb * (1. / T))     # ComputeFT: sqrt(eps/k uT)
         fT = 1. + aux * (_ZROTA + aux * (_ZROTB + aux * _ZROTC))
         zrot = self.zrot298 * self.f298 / fT
         cv = self.cp_mass(T) - R_J_KMOL * (1. / self.mw)     # SpeciesCv (WithoutTransport.hpp:95-99)
         cv_vib = cv * self.mw * 1.e-3 - self.cv_trans - self.cv_rot
         rho = 100. / (R_J_MOL * T) * self.mw
-        om11 = np.array([omega11(T / self.eps_kb[k], 0.) for k in range(self.nc)])
+        kb_over_eps = 1. / self.eps_kb
+        om11 = np.array([omega11(T * kb_over_eps[k], 0.) for k in range(self.nc)])
         dkk = self.coeff_dkk * T ** 1.5 / om11
         lam = np.empty(self.nc)
         for k in range(self.nc):
@@ -248,11 +250,12 @@ class SpeciesTransport:
             A = 2.5 - f_vib
             B = zrot[k] + _TWO_OVER_PI * (_FIVE_OVER_3R * self.cv_rot[k] + f_vib)
             f_trans = 2.50 * (1. - _TWO_OVER_PI * self.cv_rot[k] / self.cv_trans * A / B)
+            umw = 1. / self.mw[k]
             if self.shape[k] == 0:
-                lam[k] = eta[k] / self.mw[k] * (f_trans * self.cv_trans)
+                lam[k] = eta[k] * umw * (f_trans * self.cv_trans)
             else:
                 f_rot = f_vib * (1. + _TWO_OVER_PI * A / B)
-                lam[k] = eta[k] / self.mw[k] * (f_trans * self.cv_trans + f_rot * self.cv_rot[k] + f_vib * cv_vib[k])
+                lam[k] = eta[k] * umw * (f_trans * self.cv_trans + f_rot * self.cv_rot[k] + f_vib * cv_vib[k])
         return lam * 1000.
 
     def binary_diffusivity(self, T: float, p_bar: float = 1.) -> np.ndarray:
@@ -265,7 +268,7 @@ class SpeciesTransport:
                 ts = T / math.sqrt(self.eps_kb[j] * self.eps_kb[k])
                 D[j, k] = D[k, j] = self.coeff_djk[j, k] * tp / omega11(ts, self.delta_jk[j, k])
         for k in range(self.nc):
-            D[k, k] = self.coeff_dkk[k] * tp / omega11(T / self.eps_kb[k], 0.)
+            D[k, k] = self.coeff_dkk[k] * tp / omega11(T * (1. / self.eps_kb[k]), 0.)
         return D
 
     def thermal_diffusion_ratios(self, T: float) -> np.ndarray:

@@ -58,3 +58,24 @@ def test_property_entry_points_reject_bad_arguments_without_gpu():
     assert L.lsg_properties(None, 1, 1, C.cast(y, C.c_void_p), C.cast(y, C.c_void_p), None, 101325.,
                             C.byref(opt), C.byref(fields)) == -1
     assert [f for f, _ in lsg.PropertyFields._fields_] == list(lsg.PROPERTY_FIELDS)
+
+
+def test_loader_rejects_inconsistent_transport_arrays_without_gpu():
+    """build_transport's size and index checks run before any CUDA call."""
+    import numpy as np
+    from laminarsmoke_b200 import lsg, mech
+    from laminarsmoke_b200.mech import blob
+    A, species = blob.unpack(mech.load("h2co")[0])
+
+    def load(arrays):
+        data = blob.pack(arrays, species)
+        buf = (C.c_ubyte * len(data)).from_buffer_copy(data)
+        return lsg.lib().lsg_mech_load_blob(C.cast(buf, C.c_void_p), len(data), 0, C.byref(C.c_void_p()))
+
+    assert load(A) in (0, -3)                                       # consistent: on to the device
+    bad = dict(A)
+    bad["tr_gamma"] = np.asarray(A["tr_gamma"])[:-4]
+    assert load(bad) == -2                                          # LSG_ERR_MECH
+    bad = dict(A)
+    bad["tr_iteta"] = np.array(list(A["tr_iteta"][:-1]) + [99], np.int32)   # right count, index out of range
+    assert load(bad) == -2

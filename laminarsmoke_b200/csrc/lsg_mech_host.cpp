@@ -42,8 +42,9 @@ bool parse(const unsigned char* p, size_t n, Blob& b, std::string& err) {
     std::memcpy(&count, p + pos + 40, 8);
     pos += 48;
     if (code > 1) { err = "bad dtype"; return false; }
-    const size_t nb = (code == 0 ? 8 : 4) * count;
-    if (pos + nb > n) { err = "truncated payload"; return false; }
+    const size_t item = code == 0 ? 8 : 4;
+    if (count > (n - pos) / item) { err = "truncated payload"; return false; }   // no overflow of item * count
+    const size_t nb = item * count;
     if (code == 0) {
       std::vector<double> v(count);
       if (nb) std::memcpy(v.data(), p + pos, nb);
@@ -132,7 +133,12 @@ static bool build_transport(const Blob& b, int nc, HostMech& out, std::string& e
 
 bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string& err) {
   Blob b;
-  if (!parse((const unsigned char*)blob, nbytes, b, err)) return false;
+  try {
+    if (!parse((const unsigned char*)blob, nbytes, b, err)) return false;
+  } catch (const std::exception& e) {
+    err = std::string("mechanism blob: ") + e.what();
+    return false;
+  }
   try {
     if (b.i.count("xplog_rxn") || b.i.count("xfo_rxn")) {
       // PLOGMX / PLOGSP and LOWMX / LOWSP (bath-gas-specific PLOG tables and fall-off limits): the
@@ -143,7 +149,10 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
     }
     const auto& dims = b.I("dims");
     const int nc = dims.at(0), nr = dims.at(1);
-    if (nc <= 0 || nr < 0) { err = "bad dimensions"; return false; }
+    if (nc <= 0 || nr < 0 || (int)b.F("mw").size() != nc || (int)b.F("lnA").size() != nr) {
+      err = "bad dimensions";   // before anything is sized from nc or nr
+      return false;
+    }
     MechLayout L{};
     L.nc = nc;
     L.nr = nr;
@@ -289,6 +298,38 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
         !in_range(b.I("fr_rxn"), 0, nr) || !in_range(b.I("tb_species"), 0, nc) ||
         !in_range(b.I("fo_species"), 0, nc) || !in_range(tbr, 0, nr) || !in_range(fr, 0, nr)) {
       err = "index out of range in mechanism blob";
+      return false;
+    }
+    // CSR pointer arrays start at 0, never decrease and end at the entry count; value arrays are as long as
+    // their index arrays, per-reaction and per-slot arrays as long as the reactions and slots, so that no
+    // kernel reads past an array of a corrupt blob
+    auto csr_ok = [](const std::vector<int>& ptr, size_t rows, size_t nnz) {
+      if (ptr.size() != rows + 1 || ptr[0] != 0 || (size_t)ptr.back() != nnz) return false;
+      for (size_t k = 0; k + 1 < ptr.size(); ++k)
+        if (ptr[k + 1] < ptr[k]) return false;
+      return true;
+    };
+    const size_t nfo = fr.size();
+    bool ok = csr_ok(b.I("reac_ptr"), nr, b.I("reac_species").size()) &&
+              csr_ok(b.I("prod_ptr"), nr, b.I("prod_species").size()) && csr_ok(ford_ptr, nr, ford_sp.size()) &&
+              csr_ok(b.I("fr_ptr"), nc, b.I("fr_rxn").size()) &&
+              csr_ok(b.I("tb_ptr"), tbr.size(), b.I("tb_species").size()) &&
+              csr_ok(b.I("fo_ptr"), nfo, b.I("fo_species").size()) &&
+              b.F("reac_nu").size() == b.I("reac_species").size() &&
+              b.F("prod_nu").size() == b.I("prod_species").size() &&
+              b.F("fr_coef").size() == b.I("fr_rxn").size() && b.F("tb_eff_m1").size() == b.I("tb_species").size() &&
+              b.F("fo_eff_m1").size() == b.I("fo_species").size() && b.I("fo_type").size() == nfo &&
+              b.I("fo_single").size() == nfo && in_range(b.I("fo_type"), 0, 3) &&
+              in_range(b.I("fo_single"), -1, nc) && in_range(rth, 0, nr) && in_range(rex, 0, nr);
+    for (const char* k : {"beta", "e_over_r", "delta_nu"}) ok = ok && (int)b.F(k).size() == nr;
+    for (const char* k : {"fo_lnA", "fo_beta", "fo_e_over_r", "fo_a", "fo_b", "fo_c", "fo_d", "fo_e"})
+      ok = ok && b.F(k).size() == nfo;
+    for (const char* k : {"lnA_rev", "beta_rev", "e_over_r_rev"}) ok = ok && b.F(k).size() == rex.size();
+    for (const char* k : {"cp_lt"}) ok = ok && (int)b.F(k).size() == 5 * nc;
+    for (const char* k : {"dh_lt", "ds_ht", "ds_lt"}) ok = ok && (int)b.F(k).size() == 6 * nc;
+    ok = ok && (int)b.F("t_mid").size() == nc;
+    if (!ok) {
+      err = "inconsistent tables in mechanism blob";
       return false;
     }
     if ((int)b.I("reac_ptr").size() != nr + 1 || (int)b.I("prod_ptr").size() != nr + 1 ||

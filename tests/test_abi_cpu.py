@@ -79,3 +79,27 @@ def test_loader_rejects_inconsistent_transport_arrays_without_gpu():
     bad = dict(A)
     bad["tr_iteta"] = np.array(list(A["tr_iteta"][:-1]) + [99], np.int32)   # right count, index out of range
     assert load(bad) == -2
+
+
+def test_loader_rejects_corrupt_headers_and_tables_without_gpu():
+    """A huge element count in an array header (which once overflowed the truncation check) and a CSR
+    pointer array that decreases are both refused with LSG_ERR_MECH, before any CUDA call."""
+    import struct
+    import numpy as np
+    from laminarsmoke_b200 import lsg, mech
+    from laminarsmoke_b200.mech import blob
+    data, species = mech.load("h2co")
+
+    def load(d):
+        buf = (C.c_ubyte * len(d)).from_buffer_copy(bytes(d))
+        return lsg.lib().lsg_mech_load_blob(C.cast(buf, C.c_void_p), len(d), 0, C.byref(C.c_void_p()))
+
+    d = bytearray(data)
+    d[16 + 40:16 + 48] = struct.pack("<Q", 1 << 62)          # count of the first array
+    assert load(d) == -2
+    A, _ = blob.unpack(data)
+    bad = dict(A)
+    ptr = np.array(A["reac_ptr"])
+    ptr[3], ptr[4] = ptr[4], ptr[3]                          # same length and end, decreasing inside
+    bad["reac_ptr"] = ptr
+    assert load(blob.pack(bad, species)) == -2

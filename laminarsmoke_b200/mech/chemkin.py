@@ -315,7 +315,10 @@ def _split_species_side(side: str) -> List[Tuple[str, float]]:
                 j += 1
             if j == len(tok):
                 raise ChemkinError(f"bad species token {tok}")
-            out.append((tok[j:], float(tok[:j])))
+            try:
+                out.append((tok[j:], float(tok[:j])))
+            except ValueError:
+                raise ChemkinError(f"bad stoichiometric coefficient in species token {tok}") from None
     return out
 
 
@@ -350,17 +353,25 @@ def _slash_numbers(line: str, counts: Sequence[int], what: str) -> List[float]:
     nums = parts[1].split()
     if len(nums) not in counts:
         raise ChemkinError(f"{what}: wrong number of arguments")
-    return [float(x) for x in nums]
+    try:
+        return [float(x) for x in nums]
+    except ValueError:
+        raise ChemkinError(f"{what}: the coefficients are not numbers in: {line.strip()}") from None
 
 
 def _parse_reaction(lines: List[str], species_index: Dict[str, int],
                     a_units: str, e_units: str) -> Reaction:
+    if not lines:
+        raise ChemkinError("a reaction line is missing its data (a '=' on the END line?)")
     first = lines[0]
     toks = first.split()
     if len(toks) < 4:
         raise ChemkinError(f"wrong number of arguments: {first}")
     r = Reaction(text=first.strip())
-    r.A, r.beta, r.E = float(toks[-3]), float(toks[-2]), float(toks[-1])
+    try:
+        r.A, r.beta, r.E = float(toks[-3]), float(toks[-2]), float(toks[-1])
+    except ValueError:
+        raise ChemkinError(f"the reaction line must end with A, beta and E: {first.strip()}") from None
     recon = "".join(toks[:-3])
     k = recon.find("<=>")
     if k >= 0:
@@ -438,7 +449,10 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
                 if nm not in species_index:
                     raise ChemkinError(f"third body efficiencies: unknown species {nm}")
                 r.tb_species.append(species_index[nm])
-                r.tb_eff.append(float(parts[q + 1].strip()))
+                try:
+                    r.tb_eff.append(float(parts[q + 1].strip()))
+                except ValueError:
+                    raise ChemkinError(f"third body efficiencies: bad value in: {line.strip()}") from None
             if r.pd_species != -1:
                 raise ChemkinError("third body reactions require (+M)")
             continue
@@ -561,7 +575,10 @@ def _parse_reaction(lines: List[str], species_index: Dict[str, int],
             if i_low or i_troe or i_sri or r.plog:
                 raise ChemkinError("CHEB cannot be combined with LOW/TROE/SRI/PLOG")
             a, b = line.find("/"), line.rfind("/")
-            r.cheb += [float(t) for t in line[a + 1:b].split()]
+            try:
+                r.cheb += [float(t) for t in line[a + 1:b].split()]
+            except ValueError:
+                raise ChemkinError(f"CHEB: the coefficients are not numbers in: {line.strip()}") from None
         elif kw in ("TCHEB", "PCHEB"):
             if pdr != "all":
                 raise ChemkinError(f"{kw} needs a (+M) pressure-dependent reaction")

@@ -244,3 +244,20 @@ def test_packaged_global_blobs_match_fresh_compile(name, key):
     d = f"/root/reference/run/kinetic-mechanisms/{name}/"
     m = chemkin.compile_files(d + name + ".CKI", d + name + ".CKT", trc_path=d + name + ".TRC")
     assert blob.pack(m.arrays, m.species) == mech.load(key)[0]
+
+
+@pytest.mark.parametrize("bad", [
+    "H2+O2=OH+OH 1.0E13 X 0.0",              # not a number where beta stands
+    "2.x H2+O2=H2O2 1.0E13 0.0 0.0",          # bad stoichiometric coefficient
+    "H2+M=H+H+M 1.0E13 0.0 0.0\n H2O/1..0/",  # bad efficiency
+    "H2+O2=OH+OH 1.0E13 0.0 0.0\n LOW / 1.0 2.0 /",   # LOW with two numbers, no (+M)
+    "H2+O2=OH+OH 1.0E13 0.0 0.0\nEND = ",     # '=' on the END line
+])
+def test_malformed_reactions_raise_chemkin_errors(bad):
+    """Malformed input raises ChemkinError naming the line, never another exception (a fuzz of the
+    packaged mechanism's text found these)."""
+    s = synthetic.generate(12, 10, seed=1)
+    names = " ".join(n for n in ("H2", "O2", "OH", "H", "H2O2", "H2O") if n in s.compositions)
+    kin = f"ELEMENTS\nC H O N\nEND\nSPECIES\n{names}\nEND\nREACTIONS\n{bad}\nEND\n"
+    with pytest.raises(chemkin.ChemkinError):
+        chemkin.compile_mechanism(kin, s.thermo)

@@ -192,7 +192,10 @@ def read_thermo(text: str) -> Dict[str, ThermoRecord]:
     t = lines[1].split()
     if len(t) != 3:
         raise ChemkinError("Wrong number of temperature ranges")
-    tdef = (float(t[0]), float(t[1]), float(t[2]))
+    try:
+        tdef = (float(t[0]), float(t[1]), float(t[2]))
+    except ValueError:
+        raise ChemkinError("the THERMO line must give three default temperatures") from None
     starts = []
     end = None
     for j in range(2, len(lines)):
@@ -213,7 +216,12 @@ def read_thermo(text: str) -> Dict[str, ThermoRecord]:
     starts.append(end if end is not None else len(lines))
     recs: Dict[str, ThermoRecord] = {}
     for a, b in zip(starts[:-1], starts[1:]):
-        rec = _parse_thermo_record(lines[a:b], tdef)
+        try:
+            rec = _parse_thermo_record(lines[a:b], tdef)
+        except ChemkinError:
+            raise
+        except ValueError as exc:
+            raise ChemkinError(f"bad thermodynamic record: {lines[a].strip()[:40]}: {exc}") from None
         recs.setdefault(rec.name, rec)
     return recs
 

@@ -261,3 +261,14 @@ def test_malformed_reactions_raise_chemkin_errors(bad):
     kin = f"ELEMENTS\nC H O N\nEND\nSPECIES\n{names}\nEND\nREACTIONS\n{bad}\nEND\n"
     with pytest.raises(chemkin.ChemkinError):
         chemkin.compile_mechanism(kin, s.thermo)
+
+
+def test_malformed_thermo_raises_chemkin_error():
+    """A NASA record with a broken number raises ChemkinError naming the record (thermo fuzzing found
+    plain ValueErrors here)."""
+    s = synthetic.generate(12, 10, seed=1)
+    lines = s.thermo.split("\n")
+    k = next(i for i, l in enumerate(lines) if l.rstrip().endswith("2"))
+    lines[k] = lines[k][:10] + "1.2.3e+00" + lines[k][19:]
+    with pytest.raises(chemkin.ChemkinError):
+        chemkin.compile_mechanism(s.kinetics, "\n".join(lines))

@@ -64,8 +64,10 @@ static Mech* load_blob(const unsigned char* p, size_t n) {
     uint32_t code; uint64_t count;
     std::memcpy(&code, p + pos + 32, 4); std::memcpy(&count, p + pos + 40, 8);
     pos += 48;
-    size_t item = code == 0 ? 8 : 4, nb = item * count;
-    if (pos + nb > n) { delete m; return nullptr; }
+    if (code > 1) { delete m; return nullptr; }
+    const size_t item = code == 0 ? 8 : 4;
+    if (count > (n - pos) / item) { delete m; return nullptr; }   // no overflow of item * count
+    const size_t nb = item * count;
     if (code == 0) { std::vector<double> v(count); std::memcpy(v.data(), p + pos, nb); m->f[name] = v; }
     else { std::vector<int> v(count); std::memcpy(v.data(), p + pos, nb); m->i[name] = v; }
     pos += nb + ((8 - nb % 8) % 8);

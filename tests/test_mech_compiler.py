@@ -272,3 +272,24 @@ def test_malformed_thermo_raises_chemkin_error():
     lines[k] = lines[k][:10] + "1.2.3e+00" + lines[k][19:]
     with pytest.raises(chemkin.ChemkinError):
         chemkin.compile_mechanism(s.kinetics, "\n".join(lines))
+
+
+def test_compile_command_line_with_transport(tmp_path):
+    """--transport writes the same blob as compile_mechanism(..., transport_text=...)."""
+    import subprocess
+    import sys
+    from laminarsmoke_b200.mech import synthetic
+    s = synthetic.generate(12, 30, seed=7)
+    tr = synthetic.transport_text(s)
+    for nm, text in (("k.cki", s.kinetics), ("t.ckt", s.thermo), ("tr.trc", tr)):
+        (tmp_path / nm).write_text(text)
+    out = tmp_path / "m.lsmech"
+    r = subprocess.run([sys.executable, "-m", "laminarsmoke_b200.mech", "compile", str(tmp_path / "k.cki"),
+                        str(tmp_path / "t.ckt"), "--transport", str(tmp_path / "tr.trc"), "-o", str(out)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    m = chemkin.compile_mechanism(s.kinetics, s.thermo, transport_text=tr)
+    assert out.read_bytes() == blob.pack(m.arrays, m.species)
+    r = subprocess.run([sys.executable, "-m", "laminarsmoke_b200.mech", "info", str(out)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "transport fits: yes" in r.stdout

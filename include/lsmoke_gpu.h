@@ -197,9 +197,14 @@ int lsg_ctx_check(lsg_ctx* ctx, int* device_flags);
  *   - opt: NULL for the defaults; precision FP64 or MIXED, tile is ignored.
  *   - Mechanisms with more than 31 species do not fit: LSG_ERR_SCRATCH.
  *   - Synchronous: returns when the step has finished on `stream` (NULL = the
- *     legacy default stream).  The first call on a device looks up the device
- *     address of the array (once per device); make that first call before any
- *     stream capture.
+ *     legacy default stream).  Loading a mechanism (lsg_mech_load_blob /
+ *     lsg_mech_load_file) on a device loads this call's kernels there, commits
+ *     the array and looks up its device address, so a caller that hands the
+ *     free device memory to its own pool afterwards still has the call work;
+ *     the call itself allocates nothing.
+ *   - The caller's current device is the same after the call as before it.
+ *   - The library caches per-device state (the array's address, uploaded
+ *     constants): cudaDeviceReset is not supported while it is loaded.
  *   - All calls on a device share the array and it keeps the previous call's
  *     contents: calls that overlap on the GPU (several streams or host
  *     threads at once) race and must be serialised by the caller. */

@@ -73,6 +73,16 @@ namespace {
 std::mutex g_mutex;
 bool g_gear_uploaded[64] = {};
 
+// Saves the calling thread's current device and makes it current again when the scope ends.
+struct DeviceGuard {
+  int dev = -1;
+  bool ok = false;
+  DeviceGuard() { ok = cudaGetDevice(&dev) == cudaSuccess; }
+  ~DeviceGuard() {
+    if (ok) cudaSetDevice(dev);
+  }
+};
+
 GearConsts make_gear_consts() {
   // MethodGear::MemoryAllocationMethod (MethodGear.hpp:125-193)
   GearConsts g{};
@@ -485,6 +495,13 @@ int lsg_mech_load_blob(const void* blob, size_t nbytes, int device, lsg_mech** o
   }
   m->device = device;
   if (cudaSetDevice(device) != cudaSuccess) { delete m; cudaGetLastError(); return LSG_ERR_CUDA; }
+  // Load the kernel modules now: CUDA loads them lazily, and loading commits device memory (kernel code,
+  // the no-allocation entry point's fixed array), which must not wait for the first step call.
+  if (ensure_gear(device) != LSG_OK || batched_noalloc_prepare(device) != cudaSuccess) {
+    delete m;
+    cudaGetLastError();
+    return LSG_ERR_CUDA;
+  }
   if (cudaMalloc(&m->d_buf, m->host.buffer.size()) != cudaSuccess) { delete m; cudaGetLastError(); return LSG_ERR_NOMEM; }
   if (cudaMemcpy(m->d_buf, m->host.buffer.data(), m->host.buffer.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
     cudaFree(m->d_buf);
@@ -752,7 +769,8 @@ int lsg_reaction_step_device_noalloc(const lsg_mech* m, const lsg_options* opt, 
   if (nspecies != L.nc || !(p > 0.)) return LSG_ERR_ARG;
   if (L.nc + 1 > 32) return LSG_ERR_SCRATCH;
   if (ncells == 0) return LSG_OK;
-  if (cudaSetDevice(m->device) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_CUDA; }
+  DeviceGuard dg;   // the caller's current device is restored on every return
+  if (!dg.ok || cudaSetDevice(m->device) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_CUDA; }
   const int g = ensure_gear(m->device);
   if (g != LSG_OK) return g;
   const bool lu64 = o.precision == LSG_PRECISION_FP64;

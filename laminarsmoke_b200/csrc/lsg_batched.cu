@@ -1208,6 +1208,21 @@ static cudaError_t noalloc_scratch(int device, unsigned char** out) {
   return cudaSuccess;
 }
 
+// Loads this file's kernels and the scratch array on `device` (the current
+// device) and looks up the array's address.  CUDA loads modules and kernels
+// lazily, and loading commits device memory (kernel code, and the 16 MiB
+// array itself); doing it when a mechanism is loaded keeps every such
+// commitment ahead of a caller that then hands the free memory to its pool.
+cudaError_t batched_noalloc_prepare(int device) {
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, batched_kernel<double>);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncGetAttributes(&fa, batched_kernel<float>);
+  if (e != cudaSuccess) return e;
+  unsigned char* base = nullptr;
+  return noalloc_scratch(device, &base);
+}
+
 long batched_noalloc_slots(const MechLayout& L, bool lu64, int sm_count) {
   int bps = 0;
   if (batched_occupancy(L, lu64, &bps) != cudaSuccess || bps <= 0) return -1;

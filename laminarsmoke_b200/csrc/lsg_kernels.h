@@ -67,6 +67,7 @@ cudaError_t launch_rhs_block(const MechLayout& L, const unsigned char* mech_gmem
 
 // Fixed device scratch of the no-allocation entry point (lsg_batched.cu).
 constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
+cudaError_t batched_noalloc_prepare(int device);
 long batched_noalloc_slots(const MechLayout& L, bool lu64, int sm_count);
 cudaError_t launch_batched_noalloc(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
                                    const StepArgs& a, bool lu64, int device, long nslots, int* host_flags,

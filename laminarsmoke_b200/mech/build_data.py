@@ -33,7 +33,9 @@ MECHS = {
 
 def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
-    root = argv[0] if argv else "/root/reference"
+    root = argv[0] if argv else os.environ.get("LSMOKE_REFERENCE_ROOT", "")
+    if not root:
+        raise SystemExit("usage: give the reference checkout as the first argument or in LSMOKE_REFERENCE_ROOT")
     os.makedirs(DATA, exist_ok=True)
     for name, (cki, ckt, trc) in MECHS.items():
         m = chemkin.compile_files(os.path.join(root, cki), os.path.join(root, ckt), trc_path=os.path.join(root, trc))

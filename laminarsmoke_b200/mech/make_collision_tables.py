@@ -62,7 +62,9 @@ def extract(path: str) -> dict:
 
 def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
-    root = argv[0] if argv else "/root/reference"
+    root = argv[0] if argv else os.environ.get("LSMOKE_REFERENCE_ROOT", "")
+    if not root:
+        raise SystemExit("usage: give the reference checkout as the first argument or in LSMOKE_REFERENCE_ROOT")
     src = os.path.join(root, "solvers/openSMOKEpp4laminarSMOKE/preprocessing/CollisionIntegralMatrices.hpp")
     tabs = extract(src)
     out = os.path.join(DATA, "collision_integrals.npz")

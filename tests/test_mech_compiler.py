@@ -7,8 +7,12 @@ import pytest
 
 from laminarsmoke_b200.mech import blob, chemkin, synthetic
 
-REF = "/root/reference/run/kinetic-mechanisms/POLIMI_H2CO_1412/"
-have_ref = os.path.exists(REF)
+# The reference checkout (its run/kinetic-mechanisms CHEMKIN files) is named by LSMOKE_REFERENCE_ROOT;
+# the tests that recompile its files are skipped when the variable is unset.
+REF_ROOT = os.environ.get("LSMOKE_REFERENCE_ROOT", "")
+KM = os.path.join(REF_ROOT, "run", "kinetic-mechanisms") if REF_ROOT else ""
+REF = os.path.join(KM, "POLIMI_H2CO_1412") + os.sep if KM else ""
+have_ref = bool(REF) and os.path.exists(REF)
 
 R_J_KMOL = 8314.4621
 J_FROM_CAL = 8.3144621 / (8.3144621 / 4.18443)
@@ -236,12 +240,12 @@ def test_oracle_rhs_global_ch4_rate_law():
         np.testing.assert_allclose(dy[:5], mw * nu * r / rho, rtol=1e-12, atol=1e-300)
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/run/kinetic-mechanisms/GLOBAL_CH4_1step"),
-                    reason="reference CHEMKIN files not present")
+@pytest.mark.skipif(not (KM and os.path.exists(os.path.join(KM, "GLOBAL_CH4_1step"))),
+                    reason="LSMOKE_REFERENCE_ROOT unset or its CHEMKIN files not present")
 @pytest.mark.parametrize("name,key", [("GLOBAL_CH4_1step", "ch4_1step"), ("GLOBAL_H2_1step", "h2_1step")])
 def test_packaged_global_blobs_match_fresh_compile(name, key):
     from laminarsmoke_b200 import mech
-    d = f"/root/reference/run/kinetic-mechanisms/{name}/"
+    d = os.path.join(KM, name) + os.sep
     m = chemkin.compile_files(d + name + ".CKI", d + name + ".CKT", trc_path=d + name + ".TRC")
     assert blob.pack(m.arrays, m.species) == mech.load(key)[0]
 

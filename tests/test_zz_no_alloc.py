@@ -71,3 +71,49 @@ def test_noalloc_rejects_mechanism_beyond_scratch(cuda):
     assert info.value.code == lsg.LSG_ERR_SCRATCH
     assert "scratch" in str(info.value)
     mech.close()
+
+
+_FRESH = r"""
+import sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+from laminarsmoke_b200 import cells, lsg, mech as mechs
+from laminarsmoke_b200.mech import blob
+data, species = mechs.load("h2co")
+A, _ = blob.unpack(data)
+dev = torch.device("cuda:0")
+m = lsg.Mechanism(data)                       # loads the kernels and commits the fixed array
+n = 4096
+Y, T = cells.h2co_mixing(species, A["mw"], n, seed=9)
+Yd = torch.tensor(np.ascontiguousarray(Y.T), device=dev)
+Td = torch.tensor(T, device=dev)
+st = torch.full((n,), 99, dtype=torch.int32, device=dev)
+torch.cuda.synchronize()
+# a pool allocator takes (nearly) all free device memory
+hog = None
+margin = 32 << 20
+free, _ = torch.cuda.mem_get_info()
+while hog is None and free > margin:
+    try:
+        hog = torch.empty(free - margin, dtype=torch.uint8, device=dev)
+    except torch.OutOfMemoryError:
+        margin *= 2
+left, _ = torch.cuda.mem_get_info()
+lsg.step_device_noalloc(m, Yd, Td, 1e-5, status=st)
+s = st.cpu().numpy()
+assert ((s == 2) | (s == 0)).all(), np.unique(s)
+print(f"OK free before the call: {left >> 20} MiB")
+"""
+
+
+def test_noalloc_first_call_after_pool_takes_memory(cuda):
+    """In a fresh process: load the mechanism, let a stand-in pool allocator take all but a few MiB of
+    the free device memory, then make the first no-allocation call.  It must succeed: everything it
+    needs was committed when the mechanism was loaded."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _FRESH, root], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]

@@ -216,7 +216,9 @@ int lsg_reaction_step_device_noalloc(const lsg_mech* mech, const lsg_options* op
 
 /* ---- right-hand side -----------------------------------------------------
  * f(y) of the constant-pressure reactor for ncells states
- * (BatchReactorHomogeneousConstantPressure::Equations, :175-223).
+ * (BatchReactorHomogeneousConstantPressure::Equations, :175-223).  Evaluated
+ * by the block form's kernel for more than 31 species or when the context's
+ * tile is LSG_TILE_BLOCK, by the warp kernel otherwise.
  * y_dev/dy_dev are species-major [(nspecies+1) * ld], row nspecies = T. */
 int lsg_rhs_device(lsg_ctx* ctx, int ncells, const double* y_dev, double* dy_dev, long ld, double p,
                    double* qr_dev, void* stream);

@@ -10,8 +10,9 @@ to one) and temperatures ``T[ncells]``; the seed is part of the workload name.
 * ``h2co_uneven``   -- 30 % cold frozen mixing states T ~ U[300, 600] K, 20 %
   near-ignition T ~ U[950, 1150] K with radicals at 1e-8, 50 % hot
   near-equilibrium states: a pool of 4 096 hot mixtures (T ~ U[1800, 2300] K)
-  integrated for 10 ms by a caller-supplied integrator, then sampled with a
-  relative perturbation of at most 1e-3.
+  integrated for 10 ms by a caller-supplied integrator (``pool_from_file`` reads
+  the pool the CPU oracle integrated once), then sampled with a relative
+  perturbation of at most 1e-3.
 * ``synthetic_mixing`` -- for the synthetic mechanisms: CH4/air mixing states
   with every other species log-uniform in [1e-10, 1e-3], T ~ U[lo, hi].
 * ``coflow_fields`` -- 2D axisymmetric 200 x 400 mesh: Gaussian temperature ridge
@@ -59,8 +60,31 @@ def h2co_mixing(species: List[str], mw: np.ndarray, ncells: int, seed: int = 1,
 Integrator = Callable[[np.ndarray, np.ndarray, float], Tuple[np.ndarray, np.ndarray]]
 
 
+def pool_digest(Y: np.ndarray, T: np.ndarray) -> str:
+    """SHA-256 of a pool's initial states (float64, C order)."""
+    import hashlib
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(Y, dtype=np.float64).tobytes())
+    h.update(np.ascontiguousarray(T, dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def pool_from_file(path: str) -> Integrator:
+    """An integrate_pool callable for h2co_uneven that returns the integrated pool stored in `path`
+    (written once by the CPU oracle), after checking that the pool's initial states are the ones the
+    file was made from."""
+    d = np.load(path)
+    want = bytes(d["sha256_initial"]).decode()
+
+    def integrate(Yp, Tp, dt):
+        if pool_digest(Yp, Tp) != want or float(d["dt"]) != dt:
+            raise ValueError(f"{path} was made from other initial pool states")
+        return d["Y"].copy(), d["T"].copy()
+    return integrate
+
+
 def h2co_uneven(species: List[str], mw: np.ndarray, ncells: int, integrate_pool: Integrator,
-                seed: int = 2, pool_size: int = 4096):
+                seed: int = 2, pool_size: int = 4096, pool_seed: int = 2):
     """Config with per-cell BDF step counts spread over two orders of magnitude."""
     rng = np.random.default_rng(seed)
     n_cold = int(round(0.3 * ncells))
@@ -81,11 +105,14 @@ def h2co_uneven(species: List[str], mw: np.ndarray, ncells: int, integrate_pool:
     Yi = mix(n_ign)
     Yi[:, rad] = 1e-8
     Ti = rng.uniform(950.0, 1150.0, n_ign)
-    # hot near-equilibrium states from an integrated pool
-    Yp = mix(pool_size)
-    Yp[:, rad] = 10.0 ** rng.uniform(-6.0, -3.0, (pool_size, len(rad)))
+    # hot near-equilibrium states from an integrated pool; the pool has its own random stream (pool_seed),
+    # so it is the same whatever the number of cells and the seed of the rest
+    prng = np.random.default_rng([pool_seed, 1])
+    Zp = prng.uniform(0.0, 1.0, pool_size)
+    Yp = Zp[:, None] * yf[None, :] + (1.0 - Zp)[:, None] * ya[None, :]
+    Yp[:, rad] = 10.0 ** prng.uniform(-6.0, -3.0, (pool_size, len(rad)))
     Yp /= Yp.sum(axis=1, keepdims=True)
-    Tp = rng.uniform(1800.0, 2300.0, pool_size)
+    Tp = prng.uniform(1800.0, 2300.0, pool_size)
     Yp, Tp = integrate_pool(Yp, Tp, 1.0e-2)
     pick = rng.integers(0, pool_size, n_hot)
     Yh = Yp[pick] * (1.0 + rng.uniform(-1e-3, 1e-3, (n_hot, len(species))))

@@ -220,12 +220,13 @@ int sm_count(lsg_ctx* c) {
 }
 
 // One right-hand-side evaluation per cell: the block form's kernel for more
-// than 31 species, the warp kernel otherwise.
+// than 31 species or when the context's tile is LSG_TILE_BLOCK, the warp
+// kernel otherwise.
 int ensure_block(lsg_ctx* c);
 int rhs_dispatch(lsg_ctx* c, long ncells, const double* y, double* dy, long ld, double p, double* qr,
                  cudaStream_t s) {
   const MechLayout& L = c->mech->host.layout;
-  if (L.nc + 1 > 32) {
+  if (L.nc + 1 > 32 || c->opt.tile == LSG_TILE_BLOCK) {
     const int r = ensure_block(c);
     if (r != LSG_OK) return r;
     if (launch_rhs_block(L, c->mech->d_buf, ncells, y, dy, ld, p, c->opt.energy, qr, c->bws, c->bws_blocks, s) !=

@@ -14,7 +14,7 @@
 //   lane that needs one, instead of serially on one lane while 31 idle;
 // * the mechanism tables are staged once per block into shared memory and are
 //   read as warp-wide broadcasts (all lanes walk the same reaction together);
-// * per-cell vectors (Nordsieck arrays, Newton vectors, the FP32 Jacobian)
+// * per-cell vectors (Nordsieck arrays, Newton vectors, the FP64 Jacobian)
 //   live in a slot-interleaved HBM buffer ([element][slot], coalesced); every
 //   loop over them goes through helpers with non-aliasing pointers so the
 //   loads of a loop are in flight together.  LU factors, pivots, the Newton
@@ -72,7 +72,7 @@ __host__ __device__ inline SlotLayout slot_layout(const MechLayout& L) {
   s.vb = o; o += n;
   s.eps = o; o += n;
   s.r = o; o += n;
-  s.jac = o; o += (n * n + 1) / 2;   // FP32 Jacobian, two per double slot
+  s.jac = o; o += n * n;   // FP64 Jacobian (the FP64 residual of the refinement uses it)
   s.total = o;
   return s;
 }
@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(kBT, 1)
 batched_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem, StepOptions o, StepArgs a,
                double* __restrict__ gz, double* __restrict__ gv, double* __restrict__ gb, double* __restrict__ gf,
                double* __restrict__ gf0, double* __restrict__ gva, double* __restrict__ gvb,
-               double* __restrict__ geps, double* __restrict__ gr, float* __restrict__ gjac, long ns,
+               double* __restrict__ geps, double* __restrict__ gr, double* __restrict__ gjac, long ns,
                const int* __restrict__ order, int* __restrict__ queue, int* err) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar;
@@ -419,7 +419,7 @@ batched_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem, StepO
   double* const pvb = gvb + slot;
   double* const peps = geps + slot;
   double* const pr = gr + slot;
-  float* const pjac = gjac + slot;   // element e at pjac[e * ns]
+  double* const pjac = gjac + slot;   // element e at pjac[e * ns]
   auto DB = [&](int k) -> double& { return sDB[k * kBT + tid]; };
   auto LU = [&](int i, int j) -> LUT& { return sLU[(i * n + j) * kLS + tid]; };
   auto PIV = [&](int k) -> int& { return sPIV[k * kBT + tid]; };
@@ -487,7 +487,7 @@ batched_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem, StepO
         for (int i = 0; i < n; ++i) {
           double s = 0.;
 #pragma unroll 4
-          for (int j = 0; j < n; ++j) s += (double)pjac[(long)(i * n + j) * ns] * DB(j);
+          for (int j = 0; j < n; ++j) s += pjac[(long)(i * n + j) * ns] * DB(j);
           pf[i * ns] = pr[i * ns] - (DB(i) - pendHr0 * s);
         }
 #pragma unroll 4
@@ -508,12 +508,12 @@ batched_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem, StepO
   // pivoting on the largest magnitude, first occurrence.  All 32 lanes call it.
   auto coop_factorize = [&](int qlane, double hr0) {
     const int q = wbase + qlane;
-    const float* jq = gjac + ((long)blockIdx.x * kBT + q);
+    const double* jq = gjac + ((long)blockIdx.x * kBT + q);
     LUT* lq = sLU + q;
     const int i = lane;
     if (i < n)
       for (int j = 0; j < n; ++j) {
-        double g = -hr0 * (double)jq[(long)(i * n + j) * ns];
+        double g = -hr0 * jq[(long)(i * n + j) * ns];
         if (i == j) g += 1.;
         lq[(i * n + j) * kLS] = (LUT)g;
       }
@@ -664,7 +664,7 @@ batched_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem, StepO
       }
       case PH_JAC: {
         const double hInv = 1. / hJ;
-        for (int i = 0; i < n; ++i) pjac[(long)(i * n + jcol) * ns] = (float)(hInv * (pf[i * ns] - pf0[i * ns]));
+        for (int i = 0; i < n; ++i) pjac[(long)(i * n + jcol) * ns] = hInv * (pf[i * ns] - pf0[i * ns]);
         ++jcol;
         if (jcol < n) { lab = L_JAC_COLUMN; break; }
         ++cnt[CNT_JAC];
@@ -1141,7 +1141,7 @@ cudaError_t launch_batched(const MechLayout& L, const unsigned char* mech_gmem, 
   double* gvb = slots + (long)S.vb * ns;
   double* geps = slots + (long)S.eps * ns;
   double* gr = slots + (long)S.r * ns;
-  float* gjac = (float*)(slots + (long)S.jac * ns);
+  double* gjac = slots + (long)S.jac * ns;
   cudaError_t e;
   if (lu64) {
     e = cudaFuncSetAttribute(batched_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

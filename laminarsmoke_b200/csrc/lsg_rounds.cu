@@ -24,9 +24,10 @@
 // The method is the one of the plain step -- MultiValueSolver.hpp:423-1328,
 // MethodGear.hpp:195-516, KernelDense.hpp:111-245 (under
 // solvers/openSMOKEpp4laminarSMOKE/math/native-ode-solvers) -- with the RHS of
-// BatchReactorHomogeneousConstantPressure.H:175-223.  With FP32 factors every
-// linear solve is refined against its FP64 residual (the matrix rebuilt in FP64
-// from the stored Jacobian) until it equals the FP64 solve to rounding.
+// BatchReactorHomogeneousConstantPressure.H:175-223.  The Jacobian is stored in
+// FP64 whatever the precision of the factors.  With FP32 factors every linear
+// solve is refined against its FP64 residual (G = I - h r0 J applied in FP64
+// from the stored FP64 Jacobian).
 #include "lsg_common.cuh"
 #include "lsg_kernels.h"
 
@@ -40,7 +41,7 @@ constexpr int kRT = 128;       // threads per block of the RHS kernel (one cell 
 constexpr int kWA = 4;         // warps per block of the advance kernel (one cell each)
 constexpr int kAT = 128;       // threads per block of the init kernel
 constexpr int kCT = 256;       // threads per block of the compaction kernel
-constexpr int kRefineR = 1;    // refinement sweeps of a solve with FP32 factors
+constexpr int kRefineR = 2;    // refinement sweeps of a solve with FP32 factors
 constexpr int kBins = 6;       // solver-path bins of the compaction
 
 enum Phase : int {
@@ -73,7 +74,7 @@ enum : int {
 //   [ND_, ND_ + NI_/2)  scalar ints
 //   oz   z[8][n]  Nordsieck array      ov   v[8][n]
 //   ob, of, of0, ova, ovb, oeps         n each
-//   ojac J[n][n] float (row major)      oinv G^-1[n][n] LUT (row major)
+//   ojac J[n][n] double (row major)     oinv G^-1[n][n] LUT (row major)
 struct RecLayout {
   int oz, ov, ob, of, of0, ova, ovb, oeps, ojac, oinv, RS;
 };
@@ -89,7 +90,7 @@ __host__ __device__ inline RecLayout rec_layout(int n, bool lu64) {
   r.ova = o; o += n;
   r.ovb = o; o += n;
   r.oeps = o; o += n;
-  r.ojac = o; o += (n * n + 1) / 2;
+  r.ojac = o; o += n * n;
   r.oinv = o; o += lu64 ? n * n : (n * n + 1) / 2;
   r.RS = (o + 31) & ~31;
   return r;
@@ -338,13 +339,13 @@ __device__ __noinline__ double pow_ol(double x, double y) { return pow(x, y); }
 // 4.  Js: J rows (shared), As/Ks: work arrays, Xs: G^-1 (shared), Ig: G^-1 in
 // the cell record.  Out of line: one copy serves every call site.
 template <typename LUT, int W>
-__device__ __noinline__ void gj_inverse(const float* Js, LUT* As, LUT* Ks, LUT* Xs, LUT* Ig, double hr0, int n,
+__device__ __noinline__ void gj_inverse(const double* Js, LUT* As, LUT* Ks, LUT* Xs, LUT* Ig, double hr0, int n,
                                         int lane, unsigned gm) {
   const int ld = n + 1, la = 2 * n + 1, m2 = 2 * n;
   const bool al = lane < n;
   if (al) {
     for (int j = 0; j < n; ++j) {
-      double g = -hr0 * (double)Js[lane * ld + j];
+      double g = -hr0 * Js[lane * ld + j];
       if (j == lane) g += 1.;
       As[lane * la + j] = (LUT)g;
       As[lane * la + n + j] = (j == lane) ? (LUT)1 : (LUT)0;
@@ -449,16 +450,16 @@ __device__ __forceinline__ void set8(double (&a)[8], unsigned i, double x) {
 }
 
 // x = G^-1 rhs for one lane group (Xs = G^-1 rows in shared memory); with FP32
-// factors (refine) one sweep of iterative refinement on the FP64 residual
-// rhs - (x - hr0 J x), the matrix rebuilt in FP64 from the Jacobian rows Js.
+// factors (refine) sweeps of iterative refinement on the FP64 residual
+// rhs - (x - hr0 J x), J the FP64 Jacobian rows Js.
 template <typename LUT, int W>
-__device__ __noinline__ double solve_ol(const LUT* Xs, const float* Js, double rhs, double hr0, int n, int lane,
+__device__ __noinline__ double solve_ol(const LUT* Xs, const double* Js, double rhs, double hr0, int n, int lane,
                                         unsigned gm, int refine) {
   const int ld = n + 1;
   const bool al = lane < n;
   double xv = rowdot_ol<LUT, W>(Xs, rhs, n, ld, lane, gm);
   for (int it = 0; it < refine; ++it) {
-    const double s = rowdot_ol<float, W>(Js, xv, n, ld, lane, gm);
+    const double s = rowdot_ol<double, W>(Js, xv, n, ld, lane, gm);
     const double res = al ? rhs - (xv - hr0 * s) : 0.;
     xv += rowdot_ol<LUT, W>(Xs, res, n, ld, lane, gm);
   }
@@ -592,9 +593,9 @@ __device__ __noinline__ void jacobian_column(const MechLayout* L, const double* 
   const long ffs = last ? 1 : fs;
   const double q = rhs_cell(L, Md, Mi, scratch, vb, 1, j, yh + hJ, f, ffs, P0, energy, rho0);
   const double* f0 = R + RL.of0;
-  float* Jg = (float*)(R + RL.ojac);
+  double* Jg = R + RL.ojac;
   const double hInv = 1. / hJ;
-  for (int i = 0; i < n; ++i) Jg[i * n + j] = (float)(hInv * (f[(long)i * ffs] - f0[i]));
+  for (int i = 0; i < n; ++i) Jg[i * n + j] = hInv * (f[(long)i * ffs] - f0[i]);
   if (last) R[D_QR] = q;
   if (j == 0) {
     int* RI = (int*)(R + ND_);
@@ -748,13 +749,13 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
   const int n = NC + 1, ld = n + 1;
   const RecLayout RL = B.L;
   // per-warp shared memory: G^-1 X[n][ld] (LUT), the Gauss-Jordan work array A[n][2n+1] (LUT), its pivot
-  // row K[2n] (LUT) and the Jacobian J[n][ld] (float)
+  // row K[2n] (LUT) and the Jacobian J[n][ld] (double)
   const int la = 2 * n + 1;
   constexpr int G = kWA * CPW;   // lane groups per block
   LUT* Xs = (LUT*)wsm + (size_t)w * n * ld;
   LUT* As = (LUT*)wsm + (size_t)G * n * ld + (size_t)w * n * la;
   LUT* Ks = (LUT*)wsm + (size_t)G * n * ld + (size_t)G * n * la + (size_t)w * 2 * n;
-  float* Js = (float*)((LUT*)wsm + (size_t)G * (n * ld + n * la + 2 * n)) + (size_t)w * n * ld;
+  double* Js = (double*)((LUT*)wsm + (((size_t)G * (n * ld + n * la + 2 * n) + 1) & ~(size_t)1)) + (size_t)w * n * ld;
   const bool al = lane < n;
   const double lo = lane < NC ? 0. : o.y_min_T, hi = lane < NC ? 1. : o.y_max_T;
   const int nact = B.nact[par];
@@ -809,7 +810,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
     double x = 0.;                 // latest Newton correction
     bool dz = false, dv = false;   // z / v modified
     bool j_in = false, inv_in = false;
-    float* const Jg = (float*)(R + RL.ojac);
+    double* const Jg = R + RL.ojac;
     LUT* const Ig = (LUT*)(R + RL.oinv);
     // Rounds that solve (predictor and Newton results) will want G^-1 and, for the refinement and the
     // convergence-rate test, J: start copying this lane's rows into shared memory now.
@@ -818,7 +819,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
       if (al)
         for (int j = 0; j < n; ++j) {
           cp_async_el(&Xs[lane * ld + j], &Ig[lane * n + j]);
-          cp_async4(&Js[lane * ld + j], &Jg[lane * n + j]);
+          cp_async8(&Js[lane * ld + j], &Jg[lane * n + j]);
         }
       pending = true;
     }
@@ -860,8 +861,8 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
         inv_in = true;
       }
     };
-    // x = G^-1 rhs; with FP32 factors one refinement sweep on the FP64 residual
-    // rhs - (x - hr0 J x), the matrix rebuilt in FP64 from the stored Jacobian
+    // x = G^-1 rhs; with FP32 factors refinement sweeps on the FP64 residual
+    // rhs - (x - hr0 J x) of the stored FP64 Jacobian
     auto solve = [&](double rhs) {
       load_inv();
       const bool fp32 = sizeof(LUT) == sizeof(float);
@@ -1181,7 +1182,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
             if (iterErrorFailure > 0 || iterConvergenceFailure > 0) iterConvergenceRate = 0;
             if (iterConvergence > 1) {
               load_j();
-              const double s = rowdot_ol<float, W>(Js, v[0] - z[0], n, ld, lane, gm);
+              const double s = rowdot_ol<double, W>(Js, v[0] - z[0], n, ld, lane, gm);
               const double vr = v[1] - (s * h + z[1]);
               const double normd = wsum_g<W>(gm, al ? fabs(vr) : 0.);
               const double normf = wsum_g<W>(gm, al ? fabs(v[1]) : 0.);
@@ -1435,7 +1436,7 @@ size_t advance_smem(const MechLayout& L, bool lu64, int w) {
   const size_t n = L.nc + 1;
   const size_t groups = (size_t)kWA * (w == 16 ? 2 : 1);
   const size_t lut = lu64 ? sizeof(double) : sizeof(float);
-  return groups * (n * (n + 1) + n * (2 * n + 1) + 2 * n) * lut + groups * n * (n + 1) * sizeof(float);
+  return ((groups * (n * (n + 1) + n * (2 * n + 1) + 2 * n) * lut + 7) & ~(size_t)7) + groups * n * (n + 1) * sizeof(double);
 }
 
 template <typename LUT, int NM>

@@ -17,6 +17,9 @@ Construction:
   A+B+M=C+M found through an index of single-species compositions;
 * A is log-uniform in [1e6, 1e14] (CHEMKIN mol-cm-s units), beta ~ U[-2, 2],
   Ea ~ U[0, 60] kcal/mol; 15 % third-body reactions, 10 % Troe fall-off;
+  optionally (frac_sri, frac_rev; both 0 by default, which leaves the draws of
+  the packaged mechanisms unchanged) SRI fall-off reactions with 3 or 5
+  parameters and exchange reactions with explicit reverse constants (REV);
 * NASA-7 polynomials are least-squares fits of a smooth random cp(T) on
   [300, T_mid] and [T_mid, 3500] K; a6/a7 come from a bounded formation
   enthalpy (|Hf| <= 50 kcal/mol) and standard entropy, made continuous at T_mid,
@@ -112,7 +115,8 @@ def _fit_nasa(rng: np.random.Generator, natoms: int, tmid: float):
 
 
 def generate(n_species: int, n_reactions: int, seed: int,
-             frac_thirdbody: float = 0.15, frac_troe: float = 0.10, physical: bool = False) -> SyntheticMechanism:
+             frac_thirdbody: float = 0.15, frac_troe: float = 0.10, physical: bool = False,
+             frac_sri: float = 0.0, frac_rev: float = 0.0) -> SyntheticMechanism:
     rng = np.random.default_rng(seed)
     cmax = 2 if n_species <= 200 else 4
     hmax = 6 if n_species <= 200 else 10
@@ -159,7 +163,9 @@ def generate(n_species: int, n_reactions: int, seed: int,
 
     n_tb = int(round(frac_thirdbody * n_reactions))
     n_troe = int(round(frac_troe * n_reactions))
-    kinds = ["tb"] * n_tb + ["troe"] * n_troe + ["ex"] * (n_reactions - n_tb - n_troe)
+    n_sri = int(round(frac_sri * n_reactions))
+    kinds = (["tb"] * n_tb + ["troe"] * n_troe + ["sri"] * n_sri
+             + ["ex"] * (n_reactions - n_tb - n_troe - n_sri))
     rng.shuffle(kinds)
     seen = set()
     lines = ["ELEMENTS", "C H O N", "END", "SPECIES"]
@@ -194,6 +200,12 @@ def generate(n_species: int, n_reactions: int, seed: int,
                 A, b, Ea = arrh((i, j), (c, d))
                 lines.append(f"{'+'.join(_side(names, i, j))}={'+'.join(_side(names, c, d))}"
                              f"   {A:.6E} {b:.4f} {Ea:.3f}")
+                if frac_rev > 0.0 and rng.uniform() < frac_rev:
+                    # explicit reverse rate constants: k_r = k_f(T) / K_eq(298 K)-like ratio, kept in the
+                    # collision limit; the reverse barrier is the forward one less the reaction enthalpy
+                    dh = R_CAL * (hf_r[names[c]] + hf_r[names[d]] - hf_r[names[i]] - hf_r[names[j]])
+                    Ar = min(A * 10.0 ** rng.uniform(-1.0, 1.0), 1.e14 / 2000.0 ** b)
+                    lines.append(f" REV/ {Ar:.6E} {b:.4f} {max(0.0, Ea - dh):.3f} /")
                 break
             else:
                 (i, j), target = recomb_targets[int(rng.integers(len(recomb_targets)))]
@@ -211,6 +223,14 @@ def generate(n_species: int, n_reactions: int, seed: int,
                                if idx[n] not in (i, j, t))
                 if kind == "tb":
                     lines.append(f"{left}+M={names[t]}+M   {A:.6E} {b:.4f} {Ea:.3f}")
+                elif kind == "sri":
+                    lines.append(f"{left}(+M)={names[t]}(+M)   {A:.6E} {b:.4f} {Ea:.3f}")
+                    A0 = min(A * 10.0 ** rng.uniform(3.0, 7.0), 1.e20 / 2000.0 ** (b - 1.0))
+                    lines.append(f" LOW/ {A0:.6E} {b - 1.0:.4f} {Ea * 0.5:.3f} /")
+                    sri = [rng.uniform(0.3, 1.5), rng.uniform(100.0, 800.0), rng.uniform(800.0, 3000.0)]
+                    if rng.uniform() < 0.5:
+                        sri += [rng.uniform(0.8, 1.2), rng.uniform(-0.3, 0.3)]
+                    lines.append(" SRI/ " + " ".join(f"{v:.4f}" for v in sri) + " /")
                 else:
                     lines.append(f"{left}(+M)={names[t]}(+M)   {A:.6E} {b:.4f} {Ea:.3f}")
                     A0 = A * 10.0 ** rng.uniform(3.0, 7.0)

@@ -1,0 +1,71 @@
+"""The metric's accuracy condition on the benchmark's own workload: a seeded 4,096-cell subset of the
+1,048,576-cell uneven-stiffness H2/CO workload (cold frozen, igniting and near-equilibrium cells;
+hot pool integrated by the oracle, tests/golden/h2co_hot_pool.npz), every GPU form against the
+oracle.
+
+Bounds: relative T error <= 1e-6 in every cell; absolute Y error <= 1e-9 in every cell whose
+solver took the oracle's path (all eight per-cell counters equal: steps, RHS calls, Jacobians,
+factorisations, solves, error-test and convergence failures, Jacobian RHS calls).  A cell whose
+path differs -- a step-size or order decision flipped by an ulp of exp/log/pow -- differs by
+O(rtol |Y|); those cells are counted, must be few, and must stay within 1e-7."""
+import os
+
+import numpy as np
+import pytest
+
+from laminarsmoke_b200 import cells
+
+pytestmark = pytest.mark.gpu
+
+RTOL_T = 1e-6
+ATOL_Y = 1e-9
+POOL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "h2co_hot_pool.npz")
+
+
+@pytest.fixture(scope="module")
+def uneven(h2co):
+    from oracle.oracle import OracleMechanism
+    data, species, A = h2co
+    Y, T = cells.h2co_uneven(species, A["mw"], 1 << 20, cells.pool_from_file(POOL), seed=2)
+    pick = np.sort(np.random.default_rng(11).choice(Y.shape[0], 4096, replace=False))
+    Y, T = Y[pick], T[pick]
+    ref = OracleMechanism(data).reaction_step(Y, T, 1e-5, nthreads=os.cpu_count() or 1)
+    return data, Y, T, ref
+
+
+FORMS = {
+    "plain": dict(tile=1, precision=0),
+    "rounds-fp32": dict(tile=2, precision=1),
+    "rounds-fp64": dict(tile=2, precision=0),
+    "persistent-fp32": dict(tile=3, precision=1),
+    "block": dict(tile=4, precision=0),
+}
+
+
+@pytest.mark.parametrize("form", list(FORMS))
+def test_uneven_subset_against_oracle(cuda, uneven, form):
+    import torch
+    from laminarsmoke_b200 import lsg
+    data, Y, T, (Yo, To, _, sto, cnto) = uneven
+    n = len(T)
+    ctx = lsg.ReactionStep(lsg.Mechanism(data), **FORMS[form])
+    Yd = torch.tensor(np.ascontiguousarray(Y.T), device=cuda)
+    Td = torch.tensor(T, device=cuda)
+    st = torch.zeros(n, dtype=torch.int32, device=cuda)
+    cnt = torch.zeros((n, lsg.NCOUNTERS), dtype=torch.int64, device=cuda)
+    ctx.step_device(Yd, Td, 1e-5, status=st, counters=cnt)
+    torch.cuda.synchronize()
+    ctx.check()
+    Yg, Tg, stg, cg = Yd.cpu().numpy().T, Td.cpu().numpy(), st.cpu().numpy(), cnt.cpu().numpy()
+    np.testing.assert_array_equal(stg, sto)
+    dT = np.abs(Tg - To) / To
+    dY = np.abs(Yg - Yo).max(axis=1)
+    same = (cg == cnto).all(axis=1)
+    miss = dY > ATOL_Y
+    print(f"{form}: max rel T {dT.max():.2e}; max abs Y {dY.max():.2e}; same path {same.mean():.4f}; "
+          f"beyond 1e-9: {miss.sum()} cells, {np.sum(miss & same)} of them on the oracle's path; "
+          f"max abs Y on the oracle's path {dY[same].max():.2e}")
+    assert dT.max() <= RTOL_T
+    assert dY[same].max() <= ATOL_Y
+    assert same.mean() >= 0.9
+    assert dY.max() <= 1e-7

@@ -202,3 +202,71 @@ class OracleMechanism:
         lib().orc_reaction_step_drg(self.h, C.byref(o), C.byref(d), n, _ptr(Y), _ptr(T), p, t0, _ptr(dt_arr), dt_s,
                                     _ptr(Q), _ptr(st), _ptr(cnt), _ptr(nsp), _ptr(nrx))
         return Y, T, Q, st, cnt, nsp, nrx
+
+
+# ----------------------------------------------------------------------------
+# The reference's own integrator (oracle/refpin): the class templates of
+# math/native-ode-solvers/{MultiValueSolver,MethodGear,KernelDense}.hpp compiled
+# unchanged from the reference checkout, driving the oracle's right-hand side.
+# Built into oracle/_ref/ by oracle/refpin/Makefile where the reference sources
+# are present; used by tests/test_refpin.py to pin the oracle's integrator.
+REFPIN = os.path.join(HERE, "_ref", "liblsmoke_refpin.so")
+_refpin = None
+
+
+def refpin_available() -> bool:
+    return os.path.exists(REFPIN)
+
+
+def refpin_lib():
+    global _refpin
+    if _refpin is None:
+        L = C.CDLL(REFPIN)
+        L.orc_mech_load.restype = C.c_void_p
+        L.orc_mech_load.argtypes = [C.c_void_p, C.c_size_t]
+        L.orc_mech_free.argtypes = [C.c_void_p]
+        L.ref_reaction_step.argtypes = [C.c_void_p, C.POINTER(OrcOptions), C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_double, C.c_double, C.c_void_p, C.c_double, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_int]
+        L.ref_reaction_step.restype = C.c_int
+        _refpin = L
+    return _refpin
+
+
+class ReferenceIntegrator:
+    """The reference's MultiValueSolver<MethodGear<KernelDense<...>>> on the oracle's RHS, with the
+    per-cell calls of chemistry_DI.H:92-169 (a fresh solver object per cell)."""
+
+    def __init__(self, blob: bytes):
+        self._buf = (C.c_ubyte * len(blob)).from_buffer_copy(blob)
+        self.h = refpin_lib().orc_mech_load(C.cast(self._buf, C.c_void_p), len(blob))
+        if not self.h:
+            raise ValueError("refpin: bad mechanism blob")
+
+    def __del__(self):
+        try:
+            if self.h:
+                refpin_lib().orc_mech_free(self.h)
+        except Exception:
+            pass
+
+    def reaction_step(self, Y, T, dt, p=101325.0, t0=0.0, rtol=1e-7, atol=1e-12, tmin_chem=0.0,
+                      max_steps=500000, energy=True, nthreads=0, y_min_T=200.0, y_max_T=6000.0):
+        """Cell-major Y[ncells, NC], T[ncells]; returns (Y, T, Q, status, counters) as
+        OracleMechanism.reaction_step does."""
+        Y = np.array(Y, dtype=np.float64, order="C", copy=True)
+        T = np.array(T, dtype=np.float64, copy=True)
+        n = T.size
+        dt_arr = None
+        dt_s = 0.0
+        if np.ndim(dt) == 0:
+            dt_s = float(dt)
+        else:
+            dt_arr = np.ascontiguousarray(dt, dtype=np.float64)
+        Q = np.zeros(n)
+        st = np.zeros(n, dtype=np.int32)
+        cnt = np.zeros((n, NCOUNT), dtype=np.int64)
+        o = OrcOptions(rtol, atol, tmin_chem, y_min_T, y_max_T, max_steps, 0, int(energy), 0.8, 0.8, 5, 0)
+        refpin_lib().ref_reaction_step(self.h, C.byref(o), n, _ptr(Y), _ptr(T), p, t0, _ptr(dt_arr), dt_s,
+                                       _ptr(Q), _ptr(st), _ptr(cnt), nthreads)
+        return Y, T, Q, st, cnt

@@ -51,9 +51,13 @@ extern "C" {
 #define LSG_TILE_WARP 1        /* one warp per cell, the reference's operation order (FP64 only) */
 #define LSG_TILE_LANE 2        /* one thread per cell, rounds of RHS / solver / factor kernels over the live cells */
 #define LSG_TILE_PERSISTENT 3  /* one thread per cell, one persistent kernel + device work queue */
-#define LSG_TILE_BLOCK 4       /* one thread block per cell (any size up to 511 species), FP64 factors */
+#define LSG_TILE_BLOCK 4       /* one thread block per cell (any size up to 511 species) */
 /* Mechanisms of 32 to 511 species always run one thread block per cell (the
- * tile is ignored) with FP64 factors whatever the precision option. */
+ * tile is ignored).  The block form factorises in FP64 with LSG_PRECISION_FP64;
+ * with LSG_PRECISION_MIXED and 32 to 127 species it inverts G = I - h r0 J on
+ * the tensor cores in FP32 (lsg_build_and_invert_g_device) and solves with the
+ * inverse, the Newton residual staying FP64; above 127 species it factorises
+ * in FP64 whatever the precision option. */
 
 /* counters per cell (lsg_reaction_step_device counters_out layout) */
 #define LSG_NCOUNTERS 8        /* steps, rhs, jacobians, factorisations, solves, error-test fails, convergence fails, jacobian rhs */
@@ -135,6 +139,25 @@ int lsg_reaction_step_device(lsg_ctx* ctx, int ncells, int nspecies, double* Y_d
                              double p, double t0, const double* dt_dev, double dt_scalar, double* Q_dev,
                              int* status_dev, int* nsteps_dev, long long* counters_dev, void* stream);
 
+/* ---- successive reaction steps, captured in a CUDA graph -------------------
+ * nsteps reaction steps of the same device-resident cells, as a CFD run makes
+ * between its flow steps with the state kept in HBM (solvers/laminarSMOKE/
+ * unsteady/chemistry_DI.H called once per time step): step k integrates from
+ * t0 + k dt to t0 + (k + 1) dt; arrays and conventions as for
+ * lsg_reaction_step_device (constant pressure p, scalar dt).  Q_dev and
+ * status_dev (optional) hold the last step's values.  The whole sequence is
+ * captured once into a CUDA graph on the context's stream and replayed;
+ * the context keeps the graph and replays it while every argument stays the
+ * same (a changed argument or lsg_ctx_set_options captures anew).  The form
+ * whose rounds wait on the host (LSG_TILE_LANE, or the autotuner's choice of
+ * it) runs the steps one by one instead.  graph_used (optional) is set to 1
+ * when the graph ran.  Ordered after the work already on `stream` and before
+ * the work enqueued on it afterwards; asynchronous.  No counterpart in the
+ * reference. */
+int lsg_reaction_step_sequence_device(lsg_ctx* ctx, int nsteps, int ncells, int nspecies, double* Y_dev, long ld,
+                                      double* T_dev, double p, double t0, double dt, double* Q_dev, int* status_dev,
+                                      int* graph_used, void* stream);
+
 /* ---- reaction step, constant-volume reactor ------------------------------
  * The branch of chemistry_DI.H taken with constPressureBatchReactor false
  * (:168-203): BatchReactorHomogeneousConstantVolume::SetReactor(V, P, rho)
@@ -213,6 +236,20 @@ int lsg_reaction_step_device_noalloc(const lsg_mech* mech, const lsg_options* op
                                      double* Y_dev, long ld, double* T_dev, double p, double t0, const double* dt_dev,
                                      double dt_scalar, double* Q_dev, int* status_dev, int* nsteps_dev,
                                      long long* counters_dev, void* stream);
+
+/* ---- the mixed-precision factorisation, on its own -------------------------
+ * What the mixed-precision block form (LSG_PRECISION_MIXED, 32 to 127
+ * species) does where the reference calls KernelDense::BuildAndFactorizeMatrixG
+ * (math/native-ode-solvers/KernelDense.hpp:195-220): for nmat Jacobians J_dev
+ * [nmat][n][n] (FP64, each column-major: element (i, j) at [j * n + i]) and
+ * scalars hr0_dev [nmat], it writes G^-1 of G = I - hr0 J as FP32, column-major,
+ * to inv_dev [nmat][n][n].  The inverse is a blocked Gauss-Jordan elimination
+ * with partial pivoting whose rank-32 updates run on the tensor cores as split
+ * TF32 products (three TF32 products per FP32 product, FP32 accumulation).
+ * 1 <= n <= 128; device pointers; asynchronous on `stream`.  For tests and
+ * measurement: the reaction step calls it internally. */
+int lsg_build_and_invert_g_device(lsg_ctx* ctx, int nmat, int n, const double* J_dev, const double* hr0_dev,
+                                  float* inv_dev, void* stream);
 
 /* ---- right-hand side -----------------------------------------------------
  * f(y) of the constant-pressure reactor for ncells states

@@ -54,6 +54,7 @@ struct lsg_ctx {
   // block-per-cell (large mechanism) resources
   double* bws = nullptr;
   long bws_blocks = 0;
+  long tc_blocks = 0;           // blocks of the tensor-core (mixed-precision) block kernel
   int* bqueue = nullptr;
   KernelTimer timer;          // per-kernel device time (lsg_options.kernel_timing)
   // autotuner (lsg_options.autotune)
@@ -66,6 +67,12 @@ struct lsg_ctx {
   // formation-rate output and steady-solver sources: gathered states and their right-hand sides
   double* frs = nullptr;
   long frs_cap = 0;             // doubles
+  // captured step sequence (lsg_reaction_step_sequence_device) and the arguments it was captured for
+  cudaGraphExec_t seq_exec = nullptr;
+  StepArgs seq_args{};
+  int seq_nsteps = 0, seq_tile = -1;
+  double seq_dt = 0.;
+  cudaEvent_t seq_ev[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -276,7 +283,7 @@ int ensure_block(lsg_ctx* c) {
   if (!sm_count(c)) return LSG_ERR_CUDA;
   if (!c->bws) {
     long nb = 0;
-    if (block_plan(L, c->sm_count, &nb) != cudaSuccess || nb <= 0) { cudaGetLastError(); return LSG_ERR_UNSUPPORTED; }
+    if (block_plan(L, c->sm_count, false, &nb) != cudaSuccess || nb <= 0) { cudaGetLastError(); return LSG_ERR_UNSUPPORTED; }
     if (cudaMalloc(&c->bws, block_ws_bytes(L) * (size_t)nb) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
     if (!c->bqueue && cudaMalloc(&c->bqueue, sizeof(int)) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
     c->bws_blocks = nb;
@@ -284,16 +291,33 @@ int ensure_block(lsg_ctx* c) {
   return LSG_OK;
 }
 
-int launch_large(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
+// The block form's buffers and launch plan (FP64 form, and the tensor-core form for mixed precision).
+int prepare_large(lsg_ctx* c) {
   const MechLayout& L = c->mech->host.layout;
   const int r = ensure_block(c);
+  if (r != LSG_OK) return r;
+  if (c->opt.precision == LSG_PRECISION_MIXED && block_tc_eligible(L) && !c->tc_blocks) {
+    long t = 0;
+    if (block_plan(L, c->sm_count, true, &t) != cudaSuccess || t <= 0) { cudaGetLastError(); return LSG_ERR_UNSUPPORTED; }
+    c->tc_blocks = t < c->bws_blocks ? t : c->bws_blocks;
+  }
+  return LSG_OK;
+}
+
+int launch_large(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
+  const MechLayout& L = c->mech->host.layout;
+  const int r = prepare_large(c);
   if (r != LSG_OK) return r;
   if (c->timer.used >= KernelTimer::kPairs) {
     cudaStreamSynchronize(s);
     c->timer.collect();
   }
+  // mixed precision at 32 to 128 components: the tensor-core inverse (fewer blocks per SM; the FP64 form's
+  // work space covers them)
+  const bool tc = c->opt.precision == LSG_PRECISION_MIXED && block_tc_eligible(L);
+  const long nb = tc ? c->tc_blocks : c->bws_blocks;
   c->timer.begin(KT_BLOCK, s);
-  if (launch_block(L, c->mech->d_buf, to_step_options(c->opt), a, c->bws, c->bws_blocks, c->bqueue, s) !=
+  if (launch_block(L, c->mech->d_buf, to_step_options(c->opt), a, c->bws, nb, c->bqueue, tc, c->d_err, s) !=
       cudaSuccess)
     return LSG_ERR_CUDA;
   c->timer.end(s);
@@ -588,6 +612,11 @@ int lsg_ctx_set_options(lsg_ctx* c, const lsg_options* opt) {
   c->opt = *opt;
   apply_timing(c);
   c->tuned = false;   // new options: tune again on the next step
+  if (c->seq_exec) {  // a captured sequence holds the old options
+    cudaStreamSynchronize(c->stream);
+    cudaGraphExecDestroy(c->seq_exec);
+    c->seq_exec = nullptr;
+  }
   return LSG_OK;
 }
 
@@ -600,6 +629,9 @@ int lsg_ctx_destroy(lsg_ctx* c) {
   cudaFree(c->queue);
   cudaFree(c->rstate);
   cudaFree(c->bws);
+  if (c->seq_exec) cudaGraphExecDestroy(c->seq_exec);
+  if (c->seq_ev[0]) cudaEventDestroy(c->seq_ev[0]);
+  if (c->seq_ev[1]) cudaEventDestroy(c->seq_ev[1]);
   cudaFree(c->bqueue);
   cudaFree(c->tune_buf);
   cudaFree(c->frs);
@@ -744,6 +776,94 @@ int lsg_reaction_step_cv_device(lsg_ctx* c, int ncells, int nspecies, double* Y,
                      stream);
 }
 
+// A sequence of device-resident steps, captured once into a CUDA graph and replayed while the arguments
+// stay the same.  Forms whose step waits on the host (the round scheme) run the steps one by one.
+int lsg_reaction_step_sequence_device(lsg_ctx* c, int nsteps, int ncells, int nspecies, double* Y, long ld,
+                                      double* T, double p, double t0, double dt, double* Q, int* status,
+                                      int* graph_used, void* stream) {
+  if (graph_used) *graph_used = 0;
+  if (!c || nsteps < 0 || ncells < 0 || !Y || !T || ld < ncells || !(p > 0.) || !(dt > 0.)) return LSG_ERR_ARG;
+  if (nspecies != c->mech->host.layout.nc) return LSG_ERR_ARG;
+  if (nsteps == 0 || ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  const cudaStream_t s = (cudaStream_t)stream;
+  StepArgs a{};
+  a.ncells = ncells; a.ld = ld; a.Y = Y; a.T = T; a.dt = nullptr; a.dt_scalar = dt; a.t0 = t0; a.p = p;
+  a.Q = Q; a.status = status;
+  const MechLayout& L = c->mech->host.layout;
+  // the form: tuned once (on copies of the cells) when autotuning is on
+  if (L.nc + 1 <= 32 && c->opt.tile == LSG_TILE_AUTO && c->opt.autotune && !c->tuned && ncells >= 1024) {
+    const int r = autotune(c, a, s);
+    if (r != LSG_OK) return r;
+  }
+  int tile = (c->tuned && c->opt.tile == LSG_TILE_AUTO) ? c->tuned_tile : resolve_tile(c->opt);
+  if (L.nc + 1 > 32) tile = LSG_TILE_BLOCK;
+  if (tile == LSG_TILE_LANE) {   // host-synchronised rounds: no graph
+    for (int k = 0; k < nsteps; ++k) {
+      a.t0 = t0 + k * dt;
+      const int r = launch_tile(c, a, s, tile);
+      if (r != LSG_OK) return r;
+    }
+    return LSG_OK;
+  }
+  const bool same = c->seq_exec && c->seq_nsteps == nsteps && c->seq_tile == tile && c->seq_dt == dt &&
+                    c->seq_args.ncells == a.ncells && c->seq_args.ld == a.ld && c->seq_args.Y == a.Y &&
+                    c->seq_args.T == a.T && c->seq_args.t0 == a.t0 && c->seq_args.p == a.p &&
+                    c->seq_args.Q == a.Q && c->seq_args.status == a.status;
+  if (!c->seq_ev[0]) {
+    if (cudaEventCreateWithFlags(&c->seq_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->seq_ev[1], cudaEventDisableTiming) != cudaSuccess)
+      return LSG_ERR_CUDA;
+  }
+  if (!same) {
+    if (c->seq_exec) { cudaGraphExecDestroy(c->seq_exec); c->seq_exec = nullptr; }
+    // buffers and plans first: nothing is allocated while capturing
+    int r = LSG_OK;
+    if (tile == LSG_TILE_BLOCK || L.nc + 1 > 32) r = prepare_large(c);
+    else if (tile == LSG_TILE_PERSISTENT) r = ensure_batched(c, c->opt.precision == LSG_PRECISION_FP64);
+    if (r != LSG_OK) return r;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return LSG_ERR_CUDA;
+    const bool timing = c->timer.on;
+    c->timer.on = false;
+    const long long l0 = c->launches;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      c->timer.on = timing;
+      cudaGetLastError();
+      return LSG_ERR_CUDA;
+    }
+    for (int k = 0; k < nsteps && r == LSG_OK; ++k) {
+      StepArgs ak = a;
+      ak.t0 = t0 + k * dt;
+      r = launch_tile(c, ak, c->stream, tile);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
+    c->timer.on = timing;
+    c->launches = l0;
+    if (r != LSG_OK || ec != cudaSuccess || !graph) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      return r != LSG_OK ? r : LSG_ERR_CUDA;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&c->seq_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) { c->seq_exec = nullptr; cudaGetLastError(); return LSG_ERR_CUDA; }
+    c->seq_args = a;
+    c->seq_nsteps = nsteps;
+    c->seq_tile = tile;
+    c->seq_dt = dt;
+  }
+  // order the replay after the caller's stream and the caller's stream after the replay
+  if (cudaEventRecord(c->seq_ev[0], s) != cudaSuccess || cudaStreamWaitEvent(c->stream, c->seq_ev[0], 0) != cudaSuccess)
+    return LSG_ERR_CUDA;
+  if (cudaGraphLaunch(c->seq_exec, c->stream) != cudaSuccess) return LSG_ERR_CUDA;
+  if (cudaEventRecord(c->seq_ev[1], c->stream) != cudaSuccess || cudaStreamWaitEvent(s, c->seq_ev[1], 0) != cudaSuccess)
+    return LSG_ERR_CUDA;
+  c->launches += (long long)nsteps;
+  if (graph_used) *graph_used = 1;
+  return LSG_OK;
+}
+
 int lsg_reaction_step(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, double* T, double p, double t0,
                       const double* dt, double dt_scalar, double* Q, int* status, int* nsteps) {
   return host_step(c, ncells, nspecies, Ys, T, p, nullptr, t0, dt, dt_scalar, Q, status, nsteps);
@@ -800,6 +920,20 @@ int lsg_reaction_step_device_noalloc(const lsg_mech* m, const lsg_options* opt, 
     return LSG_ERR_CUDA;
   }
   return flags ? LSG_ERR_DEVICE : LSG_OK;
+}
+
+int lsg_build_and_invert_g_device(lsg_ctx* c, int nmat, int n, const double* J, const double* hr0, float* inv,
+                                  void* stream) {
+  if (!c || nmat < 0 || n < 1 || n > 128 || (nmat > 0 && (!J || !hr0 || !inv))) return LSG_ERR_ARG;
+  if (nmat == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  if (!sm_count(c)) return LSG_ERR_CUDA;
+  if (launch_tc_inverse(nmat, n, J, hr0, inv, c->sm_count, c->d_err, (cudaStream_t)stream) != cudaSuccess) {
+    cudaGetLastError();
+    return LSG_ERR_CUDA;
+  }
+  ++c->launches;
+  return LSG_OK;
 }
 
 int lsg_rhs_device(lsg_ctx* c, int ncells, const double* y, double* dy, long ld, double p, double* qr, void* stream) {

@@ -15,6 +15,7 @@
 // enthalpies, entropies, net rates and the pivots.
 #include "lsg_common.cuh"
 #include "lsg_kernels.h"
+#include "lsg_tc.cuh"
 
 namespace lsg {
 
@@ -78,12 +79,13 @@ struct BlockShared {
   double* slot;  // [4]: broadcast, cached T, QR, pivot value
   int* PIV;      // [BT]
   int* ival;     // [BT/32 + 1] pivot search scratch
+  int* PERM;     // [BT] the factorisation's row interchanges composed: row i of P b is b[PERM[i]]
 };
 
 template <int BT>
 __host__ __device__ inline size_t block_shared_bytes(const MechLayout& L) {
   return sizeof(double) * (16 * BT + 3 * (size_t)L.nc + (size_t)L.nr + BT + BT / 32 + 1 + 4) +
-         sizeof(int) * (BT + BT / 32 + 1) + 64;
+         sizeof(int) * (2 * BT + BT / 32 + 1) + 64;
 }
 
 // Per-block global work space (doubles): J, G, kinetic-constant caches.
@@ -324,7 +326,7 @@ __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, 
 // ---------------------------------------------------------------------------
 // Gear / multivalue BDF integrator for one block (one cell).
 // ---------------------------------------------------------------------------
-template <int BT>
+template <int BT, bool TC = false>
 struct GearBlock {
   enum { H_DEC, H_CONST, H_INC };
   enum { O_DEC, O_CONST, O_INC };
@@ -336,7 +338,12 @@ struct GearBlock {
   MechView M;
   BlockShared W;
   double* J;      // [n][n] row major, global
-  double* G;      // [n][n] factors, global
+  double* G;      // [n][n] factors, global (FP64 form)
+  // mixed-precision form (TC): the tensor-core inverse's shared memory, TMEM and barrier parity
+  tc::Smem TS;
+  uint32_t tmem;
+  uint32_t tc_phase;
+  bool tc_failed;
   double* karr;
   double* ukeq;
   double* kinf;
@@ -417,6 +424,16 @@ struct GearBlock {
   // G = I - hr0 J; partial-pivot LU (largest magnitude, first occurrence).
   // Column storage: G(i, j) at G[j * n + i].
   __device__ void build_and_factorize(double hr0) {
+    if constexpr (TC) {
+      // G^-1 in FP32 by the tensor-core Gauss-Jordan inverse (lsg_tc.cuh)
+      if (!tc::gj_inverse(J, ne, hr0, TS, tmem, &tc_phase)) tc_failed = true;
+      ++cnt[CNT_FACT];
+    } else {
+      build_and_factorize_fp64(hr0);
+    }
+  }
+
+  __device__ void build_and_factorize_fp64(double hr0) {
     const int n = ne;
     for (long e = tid; e < (long)n * n; e += BT) {
       const int j = (int)(e / n), i = (int)(e % n);
@@ -450,45 +467,75 @@ struct GearBlock {
       __syncthreads();
       const int pr = W.ival[BT / 32];
       if (tid == 0) W.PIV[k] = pr;
-      if (pr != k)
-        for (int j = tid; j < n; j += BT) {
-          const double tmp = G[(long)j * n + k];
-          G[(long)j * n + k] = G[(long)j * n + pr];
-          G[(long)j * n + pr] = tmp;
+      // swap rows k and pr and stage the new row k (the pivot row) in shared memory (W.X is free here)
+      for (int j = tid; j < n; j += BT) {
+        double gk = G[(long)j * n + k];
+        if (pr != k) {
+          const double gp = G[(long)j * n + pr];
+          G[(long)j * n + pr] = gk;
+          G[(long)j * n + k] = gp;
+          gk = gp;
         }
+        W.X[j] = gk;
+      }
       __syncthreads();
-      const double d = G[(long)k * n + k];
+      // thread i > k owns row i: its multiplier, then the row's rank-1 update (each element is updated
+      // once per k, so the result does not depend on this loop order)
       if (tid > k && tid < n) {
+        const double d = W.X[k];
         double l = G[(long)k * n + tid];
         if (d != 0.) l /= d;
         G[(long)k * n + tid] = l;
-      }
-      __syncthreads();
-      const int m = n - k - 1;
-      for (long e = tid; e < (long)m * m; e += BT) {
-        const int j = k + 1 + (int)(e / m), i = k + 1 + (int)(e % m);
-        G[(long)j * n + i] -= G[(long)k * n + i] * G[(long)j * n + k];
+#pragma unroll 4
+        for (int j = k + 1; j < n; ++j) G[(long)j * n + tid] -= l * W.X[j];
       }
       __syncthreads();
     }
+    // the row interchanges composed, for the solves: apply PIV[0..n-1] in order to the identity
+    if (tid == 0) {
+      for (int i = 0; i < n; ++i) W.PERM[i] = i;
+      for (int k = 0; k < n; ++k) {
+        const int pk = W.PIV[k];
+        if (pk != k) {
+          const int t2 = W.PERM[k];
+          W.PERM[k] = W.PERM[pk];
+          W.PERM[pk] = t2;
+        }
+      }
+    }
+    __syncthreads();
     ++cnt[CNT_FACT];
   }
 
   // KernelDense::SolveLinearSystem with the factors of build_and_factorize:
   // row interchanges, then column-oriented forward and back substitution.
   __device__ double solve(double xl) {
+    if constexpr (TC) {
+      // x = G^-1 r with the FP32 inverse (column-major in shared memory), accumulated in FP64
+      const int n = ne;
+      W.X[tid] = tid < n ? xl : 0.;
+      __syncthreads();
+      double x = 0.;
+      if (tid < n) {
+        const float* RT = TS.op;
+#pragma unroll 4
+        for (int j = 0; j < n; ++j) x += (double)RT[j * tc::kRows + tid] * W.X[j];
+      }
+      __syncthreads();
+      ++cnt[CNT_SOLVE];
+      return x;
+    } else {
+      return solve_fp64(xl);
+    }
+  }
+
+  __device__ double solve_fp64(double xl) {
     const int n = ne;
     W.X[tid] = tid < n ? xl : 0.;
     __syncthreads();
-    if (tid == 0)
-      for (int k = 0; k < n; ++k) {
-        const int pk = W.PIV[k];
-        if (pk != k) {
-          const double tmp = W.X[k];
-          W.X[k] = W.X[pk];
-          W.X[pk] = tmp;
-        }
-      }
+    const double xp = tid < n ? W.X[W.PERM[tid]] : 0.;   // the row interchanges of the factorisation
+    __syncthreads();
+    W.X[tid] = xp;
     __syncthreads();
     // Substitution in panels of 32 columns.  Warp 0 solves a panel's diagonal
     // block with shuffles, the rows below (above, going back) then apply the
@@ -847,6 +894,9 @@ struct GearBlock {
       if (tolSafe > 1.) { status = -2; y = active ? Z(0) : 0.; return status; }
       tInMeshPoint = t;
       driver_step();
+      if constexpr (TC) {
+        if (tc_failed) status = -1;   // the device error flag reports it; the cell stops here
+      }
       if (status <= 0) { t = tInMeshPoint; y = active ? Z(0) : 0.; return status; }
       numberOfSteps++;
       ++cnt[CNT_STEPS];
@@ -878,10 +928,10 @@ struct GearBlock {
 // Persistent block-per-cell kernel: blocks take cells from the queue.
 // chemistry_DI.H:92-235: gather, clip and renormalise, integrate, renormalise, scatter.
 // ---------------------------------------------------------------------------
-template <int BT>
-__global__ void __launch_bounds__(BT, BT == 128 ? 4 : (BT == 256 ? 2 : 1)) block_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem,
+template <int BT, bool TC>
+__global__ void __launch_bounds__(BT, TC ? 2 : (BT == 128 ? 4 : (BT == 256 ? 2 : 1))) block_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem,
                                                    StepOptions o, StepArgs a, double* __restrict__ ws_all,
-                                                   int* queue) {
+                                                   int* queue, int* err) {
   extern __shared__ __align__(16) unsigned char bsm[];
   __shared__ int s_cell;
   const int tid = threadIdx.x;
@@ -902,14 +952,39 @@ __global__ void __launch_bounds__(BT, BT == 128 ? 4 : (BT == 256 ? 2 : 1)) block
     W.slot = p; p += 4;
     W.PIV = (int*)p;
     W.ival = W.PIV + BT;
+    W.PERM = W.ival + BT / 32 + 1;
   }
+  // mixed-precision form: the tensor-core inverse's operands after the FP64 work space, 1024-byte aligned,
+  // then its small arrays; TMEM (256 columns) for the block's lifetime
+  tc::Smem TS{};
+  uint32_t tmem = 0;
+  if constexpr (TC) {
+    const uint32_t s0 = tc::smem_addr(bsm);
+    const uint32_t base = ((s0 + (uint32_t)block_shared_bytes<BT>(L) + 1023u) & ~1023u) - s0;   // 1024-byte aligned
+    unsigned char* q = bsm + base;
+    TS.op = (float*)q; q += 4 * tc::kOperandFloats * sizeof(float);
+    TS.mbar = (unsigned long long*)q; q += 16;
+    TS.tmem_slot = (uint32_t*)q; q += 16;
+    TS.red = (float*)q; q += 8 * sizeof(float);
+    TS.redi = (int*)q; q += 8 * sizeof(int);
+    TS.prow = (float*)q; q += 4 * tc::kPanel * sizeof(float);
+    TS.pivot_of_row = (int*)q;
+    if (tid < 32) tc::tmem_alloc(TS.tmem_slot, tc::kCols);
+    if (tid == 0) tc::mbar_init(TS.mbar, 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    tmem = *TS.tmem_slot;
+  }
+  uint32_t tc_phase = 0;
+  bool tc_failed = false;
   const MechView M{(const double*)mech_gmem, (const int*)(mech_gmem + (size_t)L.n_double * sizeof(double))};
   for (;;) {
     __syncthreads();
     if (tid == 0) s_cell = atomicAdd(queue, 1);
     __syncthreads();
     const long cell = s_cell;
-    if (cell >= a.ncells) break;
+    if (cell >= a.ncells || tc_failed) break;
     double yl = 0.;
     if (tid < NC) yl = a.Y[(size_t)tid * a.ld + cell];
     const double Tc = a.T[cell];
@@ -925,7 +1000,11 @@ __global__ void __launch_bounds__(BT, BT == 128 ? 4 : (BT == 256 ? 2 : 1)) block
       if (tid < NC) y0 /= sum;
       if (tid == 0) { W.slot[1] = 0.; W.slot[2] = 0.; }
       __syncthreads();
-      GearBlock<BT> g;
+      GearBlock<BT, TC> g;
+      g.TS = TS;
+      g.tmem = tmem;
+      g.tc_phase = tc_phase;
+      g.tc_failed = false;
       g.L = &L;
       g.M = M;
       g.W = W;
@@ -954,6 +1033,11 @@ __global__ void __launch_bounds__(BT, BT == 128 ? 4 : (BT == 256 ? 2 : 1)) block
       g.set_initial_conditions(a.t0, y0);
       const double dtc = a.dt ? a.dt[cell] : a.dt_scalar;
       st = g.solve_to(a.t0 + dtc);
+      tc_phase = g.tc_phase;
+      if (g.tc_failed) {
+        tc_failed = true;
+        if (tid == 0) atomicOr(err, kErrTensorCoreWait);
+      }
       yf = g.y;
       nsteps = g.cnt[CNT_STEPS];
       Q = W.slot[2];
@@ -972,6 +1056,56 @@ __global__ void __launch_bounds__(BT, BT == 128 ? 4 : (BT == 256 ? 2 : 1)) block
       if (a.Q) a.Q[cell] = Q;
     }
   }
+  if constexpr (TC) {
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (tid < 32) tc::tmem_dealloc(tmem, tc::kCols);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stand-alone tensor-core inverse (lsg_build_and_invert_g_device): persistent
+// blocks of 128 threads, one matrix at a time; G^-1 written column-major FP32.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, 2) tc_inverse_kernel(int nmat, int n, const double* __restrict__ J,
+                                                            const double* __restrict__ hr0, float* __restrict__ out,
+                                                            int* err) {
+  extern __shared__ __align__(16) unsigned char tsm[];
+  const int tid = threadIdx.x;
+  const uint32_t s0 = tc::smem_addr(tsm);
+  unsigned char* q = tsm + (((s0 + 1023u) & ~1023u) - s0);
+  tc::Smem TS{};
+  TS.op = (float*)q; q += 4 * tc::kOperandFloats * sizeof(float);
+  TS.mbar = (unsigned long long*)q; q += 16;
+  TS.tmem_slot = (uint32_t*)q; q += 16;
+  TS.red = (float*)q; q += 8 * sizeof(float);
+  TS.redi = (int*)q; q += 8 * sizeof(int);
+  TS.prow = (float*)q; q += 4 * tc::kPanel * sizeof(float);
+  TS.pivot_of_row = (int*)q;
+  if (tid < 32) tc::tmem_alloc(TS.tmem_slot, tc::kCols);
+  if (tid == 0) tc::mbar_init(TS.mbar, 1);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *TS.tmem_slot;
+  uint32_t phase = 0;
+  for (int m = blockIdx.x; m < nmat; m += gridDim.x) {
+    if (!tc::gj_inverse(J + (size_t)m * n * n, n, hr0[m], TS, tmem, &phase)) {
+      if (tid == 0) atomicOr(err, kErrTensorCoreWait);
+      break;
+    }
+    float* o = out + (size_t)m * n * n;
+    for (int e = tid; e < n * n; e += 128) {
+      const int j = e / n, c = e - j * n;
+      o[e] = TS.op[j * tc::kRows + c];
+    }
+    __syncthreads();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (tid < 32) tc::tmem_dealloc(tmem, tc::kCols);
 }
 
 // ---------------------------------------------------------------------------
@@ -1006,6 +1140,7 @@ __global__ void __launch_bounds__(BT) rhs_block_kernel(MechLayout L, const unsig
     W.slot = q; q += 4;
     W.PIV = (int*)q;
     W.ival = W.PIV + BT;
+    W.PERM = W.ival + BT / 32 + 1;
   }
   const MechView M{(const double*)mech_gmem, (const int*)(mech_gmem + (size_t)L.n_double * sizeof(double))};
   for (long cell = blockIdx.x; cell < ncells; cell += gridDim.x) {
@@ -1024,12 +1159,24 @@ __global__ void __launch_bounds__(BT) rhs_block_kernel(MechLayout L, const unsig
 // ---------------------------------------------------------------------------
 namespace {
 
-template <int BT>
+// Shared memory of the mixed-precision (tensor-core) block kernel: the FP64 form's, then the inverse's
+// operands (64 KB, 1024-byte aligned) and small arrays; at least 80 KB so that at most two blocks share
+// an SM (each holds 256 of the SM's 512 TMEM columns).
+size_t tc_block_smem(const MechLayout& L) {
+  const size_t base = block_shared_bytes<128>(L) + 1024;   // + the alignment of the operands
+  const size_t s = base + 4 * tc::kOperandFloats * sizeof(float) + 32 + 16 * sizeof(float) +
+                   4 * tc::kPanel * sizeof(float) + tc::kRows * sizeof(int);
+  return s < 80 * 1024 ? 80 * 1024 : s;
+}
+
+template <int BT, bool TC>
 cudaError_t block_setup(const MechLayout& L, size_t* smem, int* bps) {
-  *smem = block_shared_bytes<BT>(L);
-  cudaError_t e = cudaFuncSetAttribute(block_kernel<BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+  *smem = TC ? tc_block_smem(L) : block_shared_bytes<BT>(L);
+  cudaError_t e = cudaFuncSetAttribute(block_kernel<BT, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, block_kernel<BT>, BT, *smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, block_kernel<BT, TC>, BT, *smem);
+  if (TC && *bps > 2) *bps = 2;
+  return e;
 }
 
 int block_threads(const MechLayout& L) {
@@ -1043,13 +1190,18 @@ cudaError_t upload_gear_block(const GearConsts& gc) { return cudaMemcpyToSymbol(
 
 size_t block_ws_bytes(const MechLayout& L) { return block_ws_doubles(L) * sizeof(double); }
 
-cudaError_t block_plan(const MechLayout& L, int sm_count, long* nblocks) {
+bool block_tc_eligible(const MechLayout& L) { return L.nc + 1 >= 32 && L.nc + 1 <= tc::kRows; }
+
+cudaError_t block_plan(const MechLayout& L, int sm_count, bool tc, long* nblocks) {
   if (L.nc + 1 > kBlkMaxN) return cudaErrorInvalidValue;
+  if (tc && !block_tc_eligible(L)) return cudaErrorInvalidValue;
   size_t smem = 0;
   int bps = 0;
   const int bt = block_threads(L);
-  cudaError_t e = bt == 128 ? block_setup<128>(L, &smem, &bps)
-                            : (bt == 256 ? block_setup<256>(L, &smem, &bps) : block_setup<512>(L, &smem, &bps));
+  cudaError_t e = tc ? block_setup<128, true>(L, &smem, &bps)
+                     : (bt == 128 ? block_setup<128, false>(L, &smem, &bps)
+                                  : (bt == 256 ? block_setup<256, false>(L, &smem, &bps)
+                                               : block_setup<512, false>(L, &smem, &bps)));
   if (e != cudaSuccess) return e;
   if (bps <= 0 || smem > 227 * 1024) return cudaErrorInvalidConfiguration;
   *nblocks = (long)sm_count * bps;
@@ -1057,15 +1209,41 @@ cudaError_t block_plan(const MechLayout& L, int sm_count, long* nblocks) {
 }
 
 cudaError_t launch_block(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
-                         const StepArgs& a, double* ws, long nblocks, int* queue, cudaStream_t stream) {
+                         const StepArgs& a, double* ws, long nblocks, int* queue, bool tc, int* err,
+                         cudaStream_t stream) {
   if (a.ncells <= 0) return cudaSuccess;
   long g = nblocks < a.ncells ? nblocks : a.ncells;
   cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), stream);
   if (e != cudaSuccess) return e;
   const int bt = block_threads(L);
-  if (bt == 128) block_kernel<128><<<(unsigned)g, 128, block_shared_bytes<128>(L), stream>>>(L, mech_gmem, o, a, ws, queue);
-  else if (bt == 256) block_kernel<256><<<(unsigned)g, 256, block_shared_bytes<256>(L), stream>>>(L, mech_gmem, o, a, ws, queue);
-  else block_kernel<512><<<(unsigned)g, 512, block_shared_bytes<512>(L), stream>>>(L, mech_gmem, o, a, ws, queue);
+  if (tc) {
+    if (!block_tc_eligible(L)) return cudaErrorInvalidValue;
+    block_kernel<128, true><<<(unsigned)g, 128, tc_block_smem(L), stream>>>(L, mech_gmem, o, a, ws, queue, err);
+  } else if (bt == 128) {
+    block_kernel<128, false><<<(unsigned)g, 128, block_shared_bytes<128>(L), stream>>>(L, mech_gmem, o, a, ws, queue, err);
+  } else if (bt == 256) {
+    block_kernel<256, false><<<(unsigned)g, 256, block_shared_bytes<256>(L), stream>>>(L, mech_gmem, o, a, ws, queue, err);
+  } else {
+    block_kernel<512, false><<<(unsigned)g, 512, block_shared_bytes<512>(L), stream>>>(L, mech_gmem, o, a, ws, queue, err);
+  }
+  return cudaGetLastError();
+}
+
+size_t tc_inverse_smem() {
+  return 1024 + 4 * tc::kOperandFloats * sizeof(float) + 32 + 16 * sizeof(float) + 4 * tc::kPanel * sizeof(float) +
+         tc::kRows * sizeof(int);
+}
+
+cudaError_t launch_tc_inverse(int nmat, int n, const double* J, const double* hr0, float* out, int sm_count,
+                              int* err, cudaStream_t stream) {
+  if (n < 1 || n > tc::kRows || nmat < 0) return cudaErrorInvalidValue;
+  if (nmat == 0) return cudaSuccess;
+  size_t smem = tc_inverse_smem();
+  if (smem < 80 * 1024) smem = 80 * 1024;   // at most two blocks per SM: 256 TMEM columns each
+  cudaError_t e = cudaFuncSetAttribute(tc_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const long g = (long)sm_count * 2 < nmat ? (long)sm_count * 2 : nmat;
+  tc_inverse_kernel<<<(unsigned)g, 128, smem, stream>>>(nmat, n, J, hr0, out, err);
   return cudaGetLastError();
 }
 

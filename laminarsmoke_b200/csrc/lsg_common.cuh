@@ -21,6 +21,7 @@ enum : int {
   kErrStageTimeout = 1,     // bulk copy of the mechanism did not complete in time
   kErrBadSize = 2,
   kErrQueueTimeout = 4,
+  kErrTensorCoreWait = 8,   // a tensor-core MMA did not report completion within the wait limit
 };
 
 // Sum of v over lanes 0..n-1, added strictly in lane order (the reference's

@@ -58,9 +58,16 @@ cudaError_t launch_batched(const MechLayout& L, const unsigned char* mech_gmem, 
 // Block-per-cell step for mechanisms of up to 511 species (lsg_block.cu).
 cudaError_t upload_gear_block(const GearConsts& gc);
 size_t block_ws_bytes(const MechLayout& L);
-cudaError_t block_plan(const MechLayout& L, int sm_count, long* nblocks);
+// tc: the mixed-precision form with the tensor-core inverse (32 to 128 ODE components; lsg_tc.cuh)
+bool block_tc_eligible(const MechLayout& L);
+cudaError_t block_plan(const MechLayout& L, int sm_count, bool tc, long* nblocks);
 cudaError_t launch_block(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
-                         const StepArgs& a, double* ws, long nblocks, int* queue, cudaStream_t stream);
+                         const StepArgs& a, double* ws, long nblocks, int* queue, bool tc, int* err,
+                         cudaStream_t stream);
+// G^-1 (FP32, column-major) of G = I - hr0[m] J[m] for nmat column-major FP64 Jacobians of order n <= 128,
+// by the tensor-core Gauss-Jordan inverse of the mixed-precision block form.
+cudaError_t launch_tc_inverse(int nmat, int n, const double* J, const double* hr0, float* out, int sm_count,
+                              int* err, cudaStream_t stream);
 cudaError_t launch_rhs_block(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y,
                              double* dy, long ld, double p, int energy, double* qr, double* ws, long nblocks,
                              cudaStream_t stream);

@@ -49,7 +49,8 @@ EXPORTS = (
     "lsg_reaction_step_device_noalloc", "lsg_ctx_kernel_times", "lsg_ctx_tuning",
     "lsg_compact_sources_device", "lsg_formation_rates_device",
     "lsg_reaction_step_cv", "lsg_reaction_step_cv_device", "lsg_steady_sources_device",
-    "lsg_mech_transport_info", "lsg_properties_device", "lsg_properties",
+    "lsg_mech_transport_info", "lsg_properties_device", "lsg_properties", "lsg_build_and_invert_g_device",
+    "lsg_reaction_step_sequence_device",
 )
 
 # lsg_property_fields, in declaration order: species rows (nc), scalars, light-species rows
@@ -87,6 +88,8 @@ def lib():
     L.lsg_reaction_step_device.argtypes = [vp, i, i, vp, l, vp, d, d, vp, d, vp, vp, vp, vp, vp]
     L.lsg_ctx_check.argtypes = [vp, C.POINTER(i)]
     L.lsg_rhs_device.argtypes = [vp, i, vp, vp, l, d, vp, vp]
+    L.lsg_build_and_invert_g_device.argtypes = [vp, i, i, vp, vp, vp, vp]
+    L.lsg_reaction_step_sequence_device.argtypes = [vp, i, i, i, vp, l, vp, d, d, d, vp, vp, C.POINTER(i), vp]
     L.lsg_strerror.argtypes = [i]
     L.lsg_strerror.restype = C.c_char_p
     L.lsg_abi_version.restype = i
@@ -295,6 +298,21 @@ class ReactionStep:
             bad |= st < 0
         return int(bad.sum().item())
 
+    def step_sequence_graph(self, Y, T, dt: float, nsteps: int, p: float = 101325.0, t0: float = 0.0, Q=None,
+                            status=None, stream=None) -> bool:
+        """lsg_reaction_step_sequence_device: `nsteps` successive steps of the device-resident cells,
+        captured once into a CUDA graph by the library and replayed (the round scheme runs them one by
+        one).  Returns True when the graph ran."""
+        _require_layout(Y, T, Q, status)
+        nc, ld = Y.shape
+        n = T.shape[0]
+        used = C.c_int(0)
+        _check(lib().lsg_reaction_step_sequence_device(
+            self.h, int(nsteps), n, nc, Y.data_ptr(), ld, T.data_ptr(), p, t0, float(dt),
+            None if Q is None else Q.data_ptr(), None if status is None else status.data_ptr(), C.byref(used),
+            _stream_handle(stream)), "lsg_reaction_step_sequence_device")
+        return bool(used.value)
+
     def compact_sources_device(self, Y0, T0, Yf, Tf, dt, RR, RT=None, p: float = 101325.0, stream=None):
         """Source terms of the compact Strang scheme (lsg_compact_sources_device):
         RR [NC, ld] and RT [ncells] from the fields before (Y0, T0) and after
@@ -384,6 +402,17 @@ class ReactionStep:
         _check(lib().lsg_rhs_device(self.h, n, y.data_ptr(), dy.data_ptr(), ld, p,
                                     None if qr is None else qr.data_ptr(),
                                     _stream_handle(stream)), "lsg_rhs_device")
+
+    def build_and_invert_g_device(self, J, hr0, inv, stream=None):
+        """lsg_build_and_invert_g_device: G^-1 (FP32) of G = I - hr0 J for a batch of Jacobians.
+        J: cuda float64 [nmat, n, n] holding each Jacobian column-major (J[m].T is the matrix, i.e.
+        J[m][j][i] = J_ij); hr0: float64 [nmat]; inv: float32 [nmat, n, n], written the same way."""
+        _require_layout(J, hr0, inv)
+        nmat, n, n2 = J.shape
+        if n != n2 or tuple(inv.shape) != (nmat, n, n) or hr0.shape[0] != nmat:
+            raise ValueError("J, hr0 and inv shapes disagree")
+        _check(lib().lsg_build_and_invert_g_device(self.h, nmat, n, J.data_ptr(), hr0.data_ptr(), inv.data_ptr(),
+                                                   _stream_handle(stream)), "lsg_build_and_invert_g_device")
 
     def launches(self) -> int:
         """Kernels this context has enqueued so far."""

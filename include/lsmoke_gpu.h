@@ -89,8 +89,21 @@ typedef struct lsg_options {
   int kernel_timing;    /* 1: time every kernel kind with CUDA events (lsg_ctx_kernel_times) */
   int autotune;         /* 1 with tile LSG_TILE_AUTO: the first step times the candidate forms on a sample of
                            its own cells and keeps the fastest (lsg_ctx_tuning) */
-  int reserved[4];
+  int jacobian;         /* LSG_JACOBIAN_FD (0, the reference's) or LSG_JACOBIAN_ANALYTIC */
+  int reserved[3];
 } lsg_options;
+
+/* Newton-matrix Jacobian (lsg_options.jacobian).  The reference always builds
+ * it by forward differences, one RHS evaluation per column
+ * (KernelDense.hpp:111-193).  LSG_JACOBIAN_ANALYTIC differentiates the rate
+ * expressions for the species columns (lsg_jacobian_device) and keeps the
+ * temperature column a forward difference; it is used by the lane-per-cell
+ * round scheme (LSG_TILE_LANE) of the constant-pressure reactor, the other
+ * forms and the constant-volume reactor keep the differences.  It changes the
+ * Newton iterates (not their fixed point), so step sequences can differ from
+ * the reference's at O(rtol). */
+#define LSG_JACOBIAN_FD 0
+#define LSG_JACOBIAN_ANALYTIC 1
 
 void lsg_options_default(lsg_options* opt);
 
@@ -250,6 +263,21 @@ int lsg_reaction_step_device_noalloc(const lsg_mech* mech, const lsg_options* op
  * measurement: the reaction step calls it internally. */
 int lsg_build_and_invert_g_device(lsg_ctx* ctx, int nmat, int n, const double* J_dev, const double* hr0_dev,
                                   float* inv_dev, void* stream);
+
+/* ---- analytic Jacobian ------------------------------------------------------
+ * J = df/dy of the constant-pressure reactor (BatchReactorHomogeneousConstant
+ * Pressure::Equations, :175-223) for ncells states y_dev (species-major
+ * [(nspecies + 1) * ld], row nspecies = T), written row-major to J_dev
+ * [ncells][n][n] (n = nspecies + 1, element (i, j) = df_i/dy_j at
+ * [cell * n * n + i * n + j]).  The species columns are exact derivatives of
+ * the rate expressions (Arrhenius, third body, Lindemann/Troe/SRI fall-off,
+ * CABR, FORD orders, PLOG/Chebyshev at the given pressure, reverse rates from
+ * equilibrium constants or REV); the temperature column is a forward
+ * difference with the increment sqrt(eps) max(T, 1).  What the reference
+ * would compute in KernelDense::UserDefinedJacobian, which it leaves
+ * unimplemented (KernelDense.hpp:96-109); the step uses it with
+ * lsg_options.jacobian = LSG_JACOBIAN_ANALYTIC.  Up to 31 species. */
+int lsg_jacobian_device(lsg_ctx* ctx, int ncells, const double* y_dev, long ld, double p, double* J_dev, void* stream);
 
 /* ---- right-hand side -----------------------------------------------------
  * f(y) of the constant-pressure reactor for ncells states

@@ -137,6 +137,7 @@ StepOptions to_step_options(const lsg_options& o) {
   s.alfa2_4 = o.alfa2_4;
   s.alfa2_5 = o.alfa2_5;
   s.maximum_order = o.maximum_order;
+  s.jacobian = o.jacobian;
   return s;
 }
 
@@ -150,6 +151,7 @@ int validate_options(const lsg_options* o) {
   if (o->maximum_order < 1 || o->maximum_order > 5) return LSG_ERR_ARG;
   if (o->tile < LSG_TILE_AUTO || o->tile > LSG_TILE_BLOCK) return LSG_ERR_ARG;
   if (o->tile == LSG_TILE_WARP && o->precision != LSG_PRECISION_FP64) return LSG_ERR_UNSUPPORTED;
+  if (o->jacobian != LSG_JACOBIAN_FD && o->jacobian != LSG_JACOBIAN_ANALYTIC) return LSG_ERR_ARG;
   return LSG_OK;
 }
 
@@ -929,6 +931,22 @@ int lsg_build_and_invert_g_device(lsg_ctx* c, int nmat, int n, const double* J, 
   if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
   if (!sm_count(c)) return LSG_ERR_CUDA;
   if (launch_tc_inverse(nmat, n, J, hr0, inv, c->sm_count, c->d_err, (cudaStream_t)stream) != cudaSuccess) {
+    cudaGetLastError();
+    return LSG_ERR_CUDA;
+  }
+  ++c->launches;
+  return LSG_OK;
+}
+
+int lsg_jacobian_device(lsg_ctx* c, int ncells, const double* y, long ld, double p, double* J, void* stream) {
+  if (!c || ncells < 0 || !y || !J || ld < ncells || !(p > 0.)) return LSG_ERR_ARG;
+  if (ncells == 0) return LSG_OK;
+  const MechLayout& L = c->mech->host.layout;
+  if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  if (!sm_count(c)) return LSG_ERR_CUDA;
+  if (launch_jacobian(L, c->mech->d_buf, ncells, y, ld, p, c->opt.energy, J, c->sm_count, c->d_err,
+                      (cudaStream_t)stream) != cudaSuccess) {
     cudaGetLastError();
     return LSG_ERR_CUDA;
   }

@@ -13,6 +13,7 @@ struct StepOptions {
   int max_steps, energy;
   double alfa2_4, alfa2_5;
   int maximum_order;
+  int jacobian;   // LSG_JACOBIAN_FD or LSG_JACOBIAN_ANALYTIC
 };
 
 enum { CNT_STEPS, CNT_RHS, CNT_JAC, CNT_FACT, CNT_SOLVE, CNT_ERRFAIL, CNT_CONVFAIL, CNT_JAC_RHS, NCNT };
@@ -133,6 +134,10 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
                           KernelTimer* timer);
 cudaError_t launch_rhs_warp(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y,
                             double* dy, long ld, double p, int energy, double* qr, int* err, cudaStream_t stream);
+
+// Jacobians with analytic species columns (lsg_rounds.cu), up to 31 species; J [ncells][n][n] row-major
+cudaError_t launch_jacobian(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y, long ld,
+                            double p, int energy, double* J, int sm_count, int* err, cudaStream_t stream);
 
 // source terms and diagonal Jacobian of the steady solvers (lsg_rounds.cu); scratch: 3 (nc + 1) ncells doubles
 cudaError_t launch_steady_sources(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* Y,

@@ -314,6 +314,292 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
 }
 
 
+// d/dc of conc_factor_r(nu, c): the derivative of one factor of a product of concentrations
+__device__ __forceinline__ double dconc_factor_r(double nu, double c1) {
+  if (nu == 1.) return 1.;
+  if (nu == 2.) return c1 + c1;
+  if (nu == 3.) return 3. * c1 * c1;
+  if (nu == 0.5) return c1 > 0. ? 0.5 / sqrt(c1) : 0.;
+  return c1 > 0. ? nu * pow(c1, nu - 1.) : 0.;
+}
+
+// ---------------------------------------------------------------------------
+// Analytic Jacobian, species columns, of the constant-pressure reactor
+// (BatchReactorHomogeneousConstantPressure.H:175-223) at the state y (stride
+// ns), thread-serial.  The reference builds every column by forward
+// differences (KernelDense.hpp:111-193); here the NC species columns are
+// exact derivatives and the temperature column stays a forward difference
+// (its own work item, jacobian_column).  With c_k = cTot x_k(Y) at fixed T
+// (cTot = P/(R T)), x the mole fractions and D = dOmega/dc (Omega the
+// formation rates, KineticsMap_CHEMKIN.hpp:1683-1768):
+//   dc_k/dY_j = rho (delta_kj - x_k) / MW_j,
+//   J_ij = (MW_i / MW_j) (D_ij - sum_k D_ik x_k + Omega_i / cTot)       (i < NC),
+//   J_Tj = -(R T MWmix / (MW_j cpm)) sum_k (h/RT)_k (D_kj - s_k)
+//          - f_T MWmix (R cp_j - cpm) / (MW_j cpm)                     (energy on),
+// s_k = sum_m D_km x_m, cpm the mixture molar cp, f_T = QR / (cTot cpm).
+// D collects, per reaction r with net rate q_r = kMod_r (fwd_r - rev_r):
+// the partials of the products of concentrations (forward orders, reverse
+// coefficients times 1/Keq or k_rev/k_fwd), and through the third-body
+// concentration M = sum c + sum (eps - 1) c the partials of kMod (third body:
+// kArr; fall-off: kMod [1/(1+Pr) + Pr dlnF/dPr] / M, CABR: kMod [-Pr/(1+Pr) +
+// Pr dlnF/dPr] / M, with the Troe and SRI forms' dlnF/dPr).  The part of
+// dM/dc_k that is the same for every k (the sum of all concentrations) adds a
+// term independent of k to a row of D, which the x-weighted sum removes
+// exactly (sum x = 1): only the (eps - 1) terms and single-bath partials are
+// accumulated.  J is written row-major into Jg[i * n + j] for j < NC.
+// Scratch as rhs_cell: C (concentrations), G (h/RT - s/R, later reused),
+// R (formation rates), [species][thread] in shared memory.
+// ---------------------------------------------------------------------------
+__device__ __noinline__ void analytic_jacobian_species(const MechLayout* __restrict__ Lp, const double* __restrict__ Md,
+                                                       const int* __restrict__ Mi, double* __restrict__ scratch,
+                                                       const double* __restrict__ y, long ns, double P0, int energy,
+                                                       double* __restrict__ Jg) {
+  const MechLayout& L = *Lp;
+  const MechView M{Md, Mi};
+  const int NC = L.nc, NR = L.nr, n = NC + 1;
+  const int tid = threadIdx.x;
+  double* C = scratch;
+  double* G = scratch + NC * kRT;
+  double* R = scratch + 2 * NC * kRT;
+#define SC_(arr, i) arr[(i) * kRT + tid]
+  const double* MW = M.D(L.mw);
+  const double T = y[(long)NC * ns];
+  double u = 0.;
+  for (int i = 0; i < NC; ++i) {
+    const double yi = y[(long)i * ns];
+    SC_(C, i) = yi;
+    u += yi / MW[i];
+  }
+  const double MWmix = 1. / u;
+  const double cTot = P0 / kRgas / T;
+  const double* TM = M.D(L.t_mid);
+  const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, uT = 1. / T;
+  const double logT = log(T);
+  const double lP = log(101325. / kRgas / T);
+  double cTotSum = 0.;
+  for (int i = 0; i < NC; ++i) {
+    double x = MWmix * SC_(C, i);
+    x = x / MW[i];
+    const double c = cTot * x;
+    SC_(C, i) = c;
+    cTotSum += c;
+    const bool hi = T > TM[i];
+    const double* A = hi ? M.D(L.dh_ht) + 6 * i : M.D(L.dh_lt) + 6 * i;
+    const double hrt = A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4] + uT * A[5];
+    const double* B = hi ? M.D(L.ds_ht) + 6 * i : M.D(L.ds_lt) + 6 * i;
+    SC_(G, i) = hrt - (B[0] * logT + T * B[1] + T2 * B[2] + T3 * B[3] + T4 * B[4] + B[5]);
+    SC_(R, i) = 0.;
+  }
+  for (int i = 0; i < NC; ++i)
+    for (int j = 0; j < NC; ++j) Jg[i * n + j] = 0.;
+  const double* lnA = M.D(L.lnA);
+  const double* beta = M.D(L.beta);
+  const double* eor = M.D(L.eor);
+  const double* dnu = M.D(L.dnu);
+  const int* sgn = M.I(L.a_sign);
+  const int* rk = M.I(L.rev_kind);
+  const int* rs = M.I(L.rev_slot);
+  const int* tbs = M.I(L.tb_slot);
+  const int* fos = M.I(L.fo_slot);
+  const int* rp = M.I(L.reac_ptr);
+  const int* rsp = M.I(L.reac_sp);
+  const double* rnu = M.D(L.reac_nu);
+  const int* op = M.I(L.ford_ptr);
+  const int* osp = M.I(L.ford_sp);
+  const double* onu = M.D(L.ford_val);
+  const int* pp = M.I(L.prod_ptr);
+  const int* psp = M.I(L.prod_sp);
+  const double* pnu = M.D(L.prod_nu);
+  // D[i][k] += nu_ij g for every species i of reaction j (reactants negative)
+  auto scatter = [&](int j, int k, double g) {
+    for (int q = rp[j]; q < rp[j + 1]; ++q) Jg[rsp[q] * n + k] -= contrib_r(rnu[q], g);
+    for (int q = pp[j]; q < pp[j + 1]; ++q) Jg[psp[q] * n + k] += contrib_r(pnu[q], g);
+  };
+  for (int j = 0; j < NR; ++j) {
+    double kArr = exp(lnA[j] + beta[j] * logT - eor[j] * uT);
+    if (sgn[j] < 0) kArr *= -1.;
+    if (L.n_plog > 0) {
+      const int ps = M.I(L.plog_slot)[j];
+      if (ps >= 0) kArr = plog_k(M, L, ps, T, logT, P0);
+    }
+    if (L.n_cheb > 0) {
+      const int cs = M.I(L.cheb_slot)[j];
+      if (cs >= 0) kArr = cheb_k(M, L, cs, T, P0);
+    }
+    double kMod = kArr;
+    double dkdM = 0.;          // d kMod / d M
+    int mkind = 0;             // 0: no M; 1: third body (efficiency list tb); 2: fall-off mixture; 3: fall-off single bath
+    int mslot = -1;
+    const int tb = tbs[j];
+    if (tb >= 0) {
+      double Mc = cTotSum;
+      const int* tp = M.I(L.tb_ptr);
+      const int* ts = M.I(L.tb_sp);
+      const double* te = M.D(L.tb_eff);
+      for (int q = tp[tb]; q < tp[tb + 1]; ++q) Mc += SC_(C, ts[q]) * te[q];
+      kMod *= Mc;
+      dkdM = kArr;
+      mkind = 1;
+      mslot = tb;
+    }
+    const int fo = fos[j];
+    if (fo >= 0) {
+      const double kInf = exp(M.D(L.fo_lnA)[fo] + M.D(L.fo_beta)[fo] * logT - M.D(L.fo_eor)[fo] * uT);
+      const double a = M.D(L.fo_a)[fo], b = M.D(L.fo_b)[fo], c = M.D(L.fo_c)[fo], d = M.D(L.fo_d)[fo];
+      const int ty = M.I(L.fo_type)[fo];
+      double Mc;
+      const int single = M.I(L.fo_single)[fo];
+      if (single < 0) {
+        Mc = cTotSum;
+        const int* fp = M.I(L.fo_ptr);
+        const int* fs = M.I(L.fo_sp);
+        const double* fe = M.D(L.fo_eff);
+        for (int q = fp[fo]; q < fp[fo + 1]; ++q) Mc += SC_(C, fs[q]) * fe[q];
+        mkind = 2;
+      } else {
+        Mc = SC_(C, single) + 1.e-16;
+        mkind = 3;
+      }
+      mslot = fo;
+      const double Pr = kArr * Mc / kInf;
+      const bool cabr = M.I(L.fo_cabr)[fo] != 0;
+      double wF = 1., PrdlnF = 0.;   // F and Pr dlnF/dPr
+      if (ty == 1) {
+        double v = (1. - a) * exp(-T / b) + a * exp(-T / c);
+        if (d != 0.) v += exp(-d / T);
+        const double lF = (v < 1.e-300) ? -300. : log10(v);
+        double qq;
+        if (Pr > 1.e-32 || cabr) {
+          const double nTroe = 0.75 - 1.27 * lF;
+          const double cTroe = -0.4 - 0.67 * lF;
+          const double sTroe = log10(Pr) + cTroe;
+          const double den = nTroe - 0.14 * sTroe;
+          qq = sTroe / den;
+          // log10 F = lF / (1 + q^2), dq/ds = n / den^2, Pr dlnF/dPr = d log10 F / d log10 Pr
+          const double opq = 1. + qq * qq;
+          PrdlnF = -lF * 2. * qq / (opq * opq) * nTroe / (den * den);
+        } else {
+          qq = 1. / 0.14;
+        }
+        wF = exp10(lF / (1. + qq * qq));
+      } else if (ty == 2) {
+        const double lF = a * exp(-b / T) + exp(-T / c);
+        const double l10 = log10(Pr);
+        const double opl = 1. + l10 * l10;
+        const double xSRI = 1. / opl;
+        wF = pow(lF, xSRI) * d;
+        const double e = M.D(L.fo_e)[fo];
+        if (e != 0.) wF *= pow(T, e);
+        // ln F = X ln(lF) + ...: Pr dlnF/dPr = ln(lF) dX/dlog10Pr / ln 10
+        if (Pr > 1.e-300 && lF > 0.) PrdlnF = log(lF) * (-2. * l10 / (opl * opl)) / 2.302585092994046;
+      }
+      if (cabr) {
+        kMod *= (1. / (1. + Pr)) * wF;
+        dkdM = Mc > 0. ? kMod * (-Pr / (1. + Pr) + PrdlnF) / Mc : 0.;
+      } else {
+        kMod *= kInf * (Pr / (1. + Pr)) * wF / kArr;
+        dkdM = Mc > 0. ? kMod * (1. / (1. + Pr) + PrdlnF) / Mc : 0.;
+      }
+    }
+    // forward product and its partials (orders lambda: FORD or the coefficients)
+    double fwd = 1.;
+    for (int q = op[j]; q < op[j + 1]; ++q) fwd *= conc_factor_r(onu[q], SC_(C, osp[q]));
+    for (int q = op[j]; q < op[j + 1]; ++q) {
+      double dp = dconc_factor_r(onu[q], SC_(C, osp[q]));
+      for (int q2 = op[j]; q2 < op[j + 1]; ++q2)
+        if (q2 != q) dp *= conc_factor_r(onu[q2], SC_(C, osp[q2]));
+      scatter(j, osp[q], kMod * dp);
+    }
+    double net = fwd;
+    const int kind = rk[j];
+    if (kind != 0) {
+      double rv = 1.;
+      for (int q = pp[j]; q < pp[j + 1]; ++q) rv *= conc_factor_r(pnu[q], SC_(C, psp[q]));
+      double rf;
+      if (kind == 1) {
+        double dg = 0.;
+        for (int q = pp[j]; q < pp[j + 1]; ++q) dg += contrib_r(pnu[q], SC_(G, psp[q]));
+        for (int q = rp[j]; q < rp[j + 1]; ++q) dg -= contrib_r(rnu[q], SC_(G, rsp[q]));
+        rf = exp(dg - lP * dnu[j]);
+      } else {
+        const int sr = rs[j];
+        rf = exp(M.D(L.rev_lnA)[sr] + M.D(L.rev_beta)[sr] * logT - M.D(L.rev_eor)[sr] * uT) / kArr;
+      }
+      for (int q = pp[j]; q < pp[j + 1]; ++q) {
+        double dp = dconc_factor_r(pnu[q], SC_(C, psp[q]));
+        for (int q2 = pp[j]; q2 < pp[j + 1]; ++q2)
+          if (q2 != q) dp *= conc_factor_r(pnu[q2], SC_(C, psp[q2]));
+        scatter(j, psp[q], -kMod * rf * dp);
+      }
+      rv *= rf;
+      net -= rv;
+    }
+    // through M: the (eps - 1) efficiencies, or the single bath species
+    if (mkind != 0 && dkdM != 0.) {
+      const double gm = net * dkdM;
+      if (mkind == 1) {
+        const int* tp = M.I(L.tb_ptr);
+        const int* ts = M.I(L.tb_sp);
+        const double* te = M.D(L.tb_eff);
+        for (int q = tp[mslot]; q < tp[mslot + 1]; ++q) scatter(j, ts[q], gm * te[q]);
+      } else if (mkind == 2) {
+        const int* fp = M.I(L.fo_ptr);
+        const int* fs = M.I(L.fo_sp);
+        const double* fe = M.D(L.fo_eff);
+        for (int q = fp[mslot]; q < fp[mslot + 1]; ++q) scatter(j, fs[q], gm * fe[q]);
+      } else {
+        scatter(j, M.I(L.fo_single)[mslot], gm);
+      }
+    }
+    net *= kMod;
+    for (int q = rp[j]; q < rp[j + 1]; ++q) SC_(R, rsp[q]) -= contrib_r(rnu[q], net);
+    for (int q = pp[j]; q < pp[j + 1]; ++q) SC_(R, psp[q]) += contrib_r(pnu[q], net);
+  }
+  // mixture cp and QR (the RHS's), for the temperature row
+  double cpm = 0., dsum = 0.;
+  if (energy) {
+    for (int i = 0; i < NC; ++i) {
+      const bool hi = T > TM[i];
+      const double* A = hi ? M.D(L.cp_ht) + 5 * i : M.D(L.cp_lt) + 5 * i;
+      cpm += (A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4]) * (SC_(C, i) / cTot);
+      const double* Hc = hi ? M.D(L.dh_ht) + 6 * i : M.D(L.dh_lt) + 6 * i;
+      dsum += SC_(R, i) * (Hc[0] + T * Hc[1] + T2 * Hc[2] + T3 * Hc[3] + T4 * Hc[4] + uT * Hc[5]);
+    }
+    cpm *= kRgas;
+  }
+  const double QR = -dsum * kRgas * T;
+  const double fT = energy ? QR / (cTot * cpm) : 0.;
+  // rows: s_k, the species rows in place, and t_j = sum_k (h/RT)_k D_kj for the temperature row (in G)
+  for (int j = 0; j < NC; ++j) SC_(G, j) = 0.;
+  double shs = 0.;
+  for (int k = 0; k < NC; ++k) {
+    double sk = 0.;
+    for (int m = 0; m < NC; ++m) sk += Jg[k * n + m] * (SC_(C, m) / cTot);
+    double hk = 0.;
+    if (energy) {
+      const double* Hc = T > TM[k] ? M.D(L.dh_ht) + 6 * k : M.D(L.dh_lt) + 6 * k;
+      hk = Hc[0] + T * Hc[1] + T2 * Hc[2] + T3 * Hc[3] + T4 * Hc[4] + uT * Hc[5];
+      shs += hk * sk;
+    }
+    const double add = SC_(R, k) / cTot - sk;
+    for (int m = 0; m < NC; ++m) {
+      const double dkm = Jg[k * n + m];
+      if (energy) SC_(G, m) += hk * dkm;
+      Jg[k * n + m] = (MW[k] / MW[m]) * (dkm + add);
+    }
+  }
+  for (int m = 0; m < NC; ++m) {
+    double jt = 0.;
+    if (energy) {
+      const double* A = T > TM[m] ? M.D(L.cp_ht) + 5 * m : M.D(L.cp_lt) + 5 * m;
+      const double cpj = kRgas * (A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4]);
+      jt = -(kRgas * T * MWmix / (MW[m] * cpm)) * (SC_(G, m) - shs) - fT * MWmix * (cpj - cpm) / (MW[m] * cpm);
+    }
+    Jg[NC * n + m] = jt;
+  }
+#undef SC_
+}
+
 // Asynchronous global -> shared copies (no register staging); completed by cp_async_wait_all.
 __device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
@@ -610,7 +896,7 @@ __device__ __noinline__ void jacobian_column(const MechLayout* L, const double* 
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kRT, 4) rounds_rhs_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem,
                                                           int energy, double P0, double y_max_T, RoundBufs B, int par,
-                                                          int* err) {
+                                                          int analytic, int* err) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ MechLayout sL;
@@ -628,7 +914,10 @@ __global__ void __launch_bounds__(kRT, 4) rounds_rhs_kernel(MechLayout Lp, const
   const int njac = B.njac[par];
   const int n = Lp.nc + 1;
   const int* act = par ? B.act1 : B.act0;
-  const int nitems = njac * n + (nact - njac);
+  // items per Jacobian cell: its n columns by forward differences, or (analytic) the species columns
+  // as one item and the temperature column (a forward difference) as another
+  const int jitems = analytic ? 2 : n;
+  const int nitems = njac * jitems + (nact - njac);
   double* fp = B.fsc + (long)blockIdx.x * kRT + threadIdx.x;   // this thread's column scratch
   const long fs = (long)gridDim.x * kRT;
   // Dynamic distribution: each warp takes the next 32 work items.  Consecutive items of a Jacobian are
@@ -641,22 +930,36 @@ __global__ void __launch_bounds__(kRT, 4) rounds_rhs_kernel(MechLayout Lp, const
     if (base >= nitems) break;
     const int item = base + wl;
     if (item >= nitems) continue;
-    if (item < njac * n) {
-      const int e = item / n;
+    if (item < njac * jitems) {
+      const int e = item / jitems;
       const int cell = act[e];
       double* R = B.rec + (long)cell * RL.RS;
-      jacobian_column(&sL, Md, Mi, scratch, R, RL, item - e * n, P0, energy, y_max_T, fp, fs,
-                      B.rho ? B.rho[cell] : 0.);
+      const int col = item - e * jitems;
+      if (!analytic) {
+        jacobian_column(&sL, Md, Mi, scratch, R, RL, col, P0, energy, y_max_T, fp, fs, B.rho ? B.rho[cell] : 0.);
+      } else if (col == 0) {
+        analytic_jacobian_species(&sL, Md, Mi, scratch, R + RL.ovb, 1, P0, energy, R + RL.ojac);
+      } else {
+        jacobian_column(&sL, Md, Mi, scratch, R, RL, n - 1, P0, energy, y_max_T, fp, fs, 0.);
+        int* RI = (int*)(R + ND_);
+        RI[I_CNT0 + CNT_JAC_RHS] += 1;
+      }
       continue;
     }
-    const int cell = act[njac + (item - njac * n)];
+    const int cell = act[njac + (item - njac * jitems)];
     double* R = B.rec + (long)cell * RL.RS;
     int* RI = (int*)(R + ND_);
     const int ph = RI[I_PHASE];
     if (!rhs_phase(ph)) continue;
     if (ph == PH_JAC) {   // a Jacobian outside the list head (not produced by the compaction): serially
-      for (int j = 0; j < n; ++j)
-        jacobian_column(&sL, Md, Mi, scratch, R, RL, j, P0, energy, y_max_T, fp, fs, B.rho ? B.rho[cell] : 0.);
+      if (analytic) {
+        analytic_jacobian_species(&sL, Md, Mi, scratch, R + RL.ovb, 1, P0, energy, R + RL.ojac);
+        jacobian_column(&sL, Md, Mi, scratch, R, RL, n - 1, P0, energy, y_max_T, fp, fs, 0.);
+        RI[I_CNT0 + CNT_JAC_RHS] += 1;
+      } else {
+        for (int j = 0; j < n; ++j)
+          jacobian_column(&sL, Md, Mi, scratch, R, RL, j, P0, energy, y_max_T, fp, fs, B.rho ? B.rho[cell] : 0.);
+      }
       continue;
     }
     const double* src = R + RL.ova;
@@ -1476,6 +1779,49 @@ cudaError_t launch_steady_sources(const MechLayout& L, const unsigned char* mech
   return cudaGetLastError();
 }
 
+// Jacobians of the constant-pressure reactor for ncells states (lsg_jacobian_device), one thread per
+// state: the species columns analytic (analytic_jacobian_species), the temperature column a forward
+// difference with the increment hT = sqrt(eps) max(T, 1).  y: species-major [n][ld]; J: [ncells][n][n]
+// row-major.
+__global__ void __launch_bounds__(kRT) jacobian_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem,
+                                                       long ncells, const double* __restrict__ y, long ld, double P0,
+                                                       int energy, double* __restrict__ J, int* err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ MechLayout sL;
+  if (threadIdx.x == 0) sL = Lp;
+  if (!stage_bulk(smem, mech_gmem, Lp.bytes, &mbar, err)) return;
+  const double* Md = (const double*)smem;
+  const int* Mi = (const int*)(smem + (size_t)Lp.n_double * sizeof(double));
+  double* scratch = (double*)(smem + ((Lp.bytes + 15u) & ~15u));
+  const int n = Lp.nc + 1;
+  for (long cell = (long)blockIdx.x * kRT + threadIdx.x; cell < ncells; cell += (long)gridDim.x * kRT) {
+    double* Jc = J + cell * (long)n * n;
+    analytic_jacobian_species(&sL, Md, Mi, scratch, y + cell, ld, P0, energy, Jc);
+    // temperature column: (f(y + hT e_T) - f(y)) / hT; f(y) is parked in the column first
+    const double T = y[(long)(n - 1) * ld + cell];
+    const double hT = sqrt(kMachEpsDouble) * fmax(fabs(T), 1.);
+    rhs_cell(&sL, Md, Mi, scratch, y + cell, ld, -1, 0., Jc + (n - 1), n, P0, energy, 0.);
+    double f1[32];
+    rhs_cell(&sL, Md, Mi, scratch, y + cell, ld, n - 1, T + hT, f1, 1, P0, energy, 0.);
+    for (int i = 0; i < n; ++i) Jc[i * n + n - 1] = (f1[i] - Jc[i * n + n - 1]) / hT;
+  }
+}
+
+cudaError_t launch_jacobian(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y, long ld,
+                            double p, int energy, double* J, int sm_count, int* err, cudaStream_t stream) {
+  if (ncells <= 0) return cudaSuccess;
+  if (L.nc + 1 > 32) return cudaErrorInvalidValue;
+  const size_t smem = ((L.bytes + 15u) & ~15u) + (size_t)3 * L.nc * kRT * sizeof(double);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(jacobian_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const long want = (ncells + kRT - 1) / kRT, cap = (long)sm_count * 4;
+  jacobian_kernel<<<(unsigned)(want < cap ? want : cap), kRT, smem, stream>>>(L, mech_gmem, ncells, y, ld, p, energy,
+                                                                             J, err);
+  return cudaGetLastError();
+}
+
 size_t rounds_cache_bytes(const MechLayout& L, const RoundsPlan& P) {
   return sizeof(double) * (size_t)(L.nc + 1) * (size_t)P.g_rhs * kRT;
 }
@@ -1533,8 +1879,9 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
   for (long round = 0; round < max_rounds; round += kBatch) {
     for (int r = 0; r < kBatch; ++r) {
       kt->begin(KT_RHS, stream);
+      // the analytic Jacobian is for the constant-pressure reactor; constant volume keeps the differences
       rounds_rhs_kernel<<<P.g_rhs, kRT, P.rhs_smem, stream>>>(L, mech_gmem, o.energy, a.p, o.y_max_T, B, par,
-                                                              err);
+                                                              (o.jacobian != 0 && !a.rho) ? 1 : 0, err);
       kt->end(stream);
       const dim3 ga(P.g_adv), ta(kWA * 32);
       kt->begin(KT_ADVANCE, stream);

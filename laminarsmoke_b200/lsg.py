@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(HERE, "liblsmoke_gpu.so")
 
 LSG_PRECISION_FP64 = 0
 LSG_PRECISION_MIXED = 1
+LSG_JACOBIAN_FD, LSG_JACOBIAN_ANALYTIC = 0, 1
 LSG_TILE_AUTO, LSG_TILE_WARP, LSG_TILE_LANE, LSG_TILE_PERSISTENT, LSG_TILE_BLOCK = 0, 1, 2, 3, 4
 LSG_ERR_SCRATCH = -8
 NOALLOC_SCRATCH_BYTES = 16 << 20
@@ -38,7 +39,8 @@ class Options(C.Structure):
                 ("max_steps", C.c_int), ("full_pivoting", C.c_int), ("energy", C.c_int),
                 ("precision", C.c_int),
                 ("alfa2_4", C.c_double), ("alfa2_5", C.c_double), ("maximum_order", C.c_int),
-                ("tile", C.c_int), ("kernel_timing", C.c_int), ("autotune", C.c_int), ("reserved", C.c_int * 4)]
+                ("tile", C.c_int), ("kernel_timing", C.c_int), ("autotune", C.c_int), ("jacobian", C.c_int),
+                ("reserved", C.c_int * 3)]
 
 
 EXPORTS = (
@@ -50,7 +52,7 @@ EXPORTS = (
     "lsg_compact_sources_device", "lsg_formation_rates_device",
     "lsg_reaction_step_cv", "lsg_reaction_step_cv_device", "lsg_steady_sources_device",
     "lsg_mech_transport_info", "lsg_properties_device", "lsg_properties", "lsg_build_and_invert_g_device",
-    "lsg_reaction_step_sequence_device",
+    "lsg_reaction_step_sequence_device", "lsg_jacobian_device",
 )
 
 # lsg_property_fields, in declaration order: species rows (nc), scalars, light-species rows
@@ -90,6 +92,7 @@ def lib():
     L.lsg_rhs_device.argtypes = [vp, i, vp, vp, l, d, vp, vp]
     L.lsg_build_and_invert_g_device.argtypes = [vp, i, i, vp, vp, vp, vp]
     L.lsg_reaction_step_sequence_device.argtypes = [vp, i, i, i, vp, l, vp, d, d, d, vp, vp, C.POINTER(i), vp]
+    L.lsg_jacobian_device.argtypes = [vp, i, vp, l, d, vp, vp]
     L.lsg_strerror.argtypes = [i]
     L.lsg_strerror.restype = C.c_char_p
     L.lsg_abi_version.restype = i
@@ -413,6 +416,17 @@ class ReactionStep:
             raise ValueError("J, hr0 and inv shapes disagree")
         _check(lib().lsg_build_and_invert_g_device(self.h, nmat, n, J.data_ptr(), hr0.data_ptr(), inv.data_ptr(),
                                                    _stream_handle(stream)), "lsg_build_and_invert_g_device")
+
+    def jacobian_device(self, y, J, p: float = 101325.0, stream=None):
+        """lsg_jacobian_device: y cuda float64 [n, ld] (species-major, row n-1 = T); J float64
+        [ncells, n, n] receives df/dy row-major per state."""
+        _require_layout(y, J)
+        n, ld = y.shape
+        ncells = J.shape[0]
+        if tuple(J.shape) != (ncells, n, n):
+            raise ValueError("J must be [ncells, n, n]")
+        _check(lib().lsg_jacobian_device(self.h, ncells, y.data_ptr(), ld, p, J.data_ptr(), _stream_handle(stream)),
+               "lsg_jacobian_device")
 
     def launches(self) -> int:
         """Kernels this context has enqueued so far."""

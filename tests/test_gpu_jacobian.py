@@ -1,0 +1,114 @@
+"""The analytic Jacobian (lsg_jacobian_device, lsg_options.jacobian = LSG_JACOBIAN_ANALYTIC).
+
+The reference builds the Newton matrix's Jacobian by forward differences only (KernelDense.hpp:111-193;
+its UserDefinedJacobian is unimplemented, :96-109).  The library's species columns are exact derivatives
+of the rate expressions.  They are checked column by column against central differences of the oracle's
+right-hand side (truncation O(h^2)) on several mechanisms and rate forms, and the reaction step of the
+round scheme that uses them is checked against the oracle."""
+import numpy as np
+import pytest
+
+from laminarsmoke_b200 import cells
+
+pytestmark = pytest.mark.gpu
+
+
+def _synthetic_sri_rev():
+    from laminarsmoke_b200.mech import blob, chemkin, synthetic
+    s = synthetic.generate(16, 40, seed=12, physical=True, frac_sri=0.15, frac_rev=0.3)
+    m = chemkin.compile_mechanism(s.kinetics, s.thermo)
+    return blob.pack(m.arrays, m.species), m.species
+
+
+def _mech(name):
+    from laminarsmoke_b200 import mech
+    if name == "sri_rev":
+        return _synthetic_sri_rev()
+    return mech.load(name)
+
+
+def _states(data, species, n, seed):
+    from laminarsmoke_b200.mech import blob
+    A, _ = blob.unpack(data)
+    fuel = {"H2": 0.5, "CO": 0.5} if "CO" in species and "CH4" not in species else {"CH4": 1.0}
+    if "CH4" not in species and "CO" not in species:
+        fuel = {"H2": 1.0}
+    rng = np.random.default_rng(seed)
+    yf, ya = cells.fuel_air_mass(species, A["mw"], fuel, {"O2": 0.21, "N2": 0.79})
+    Z = rng.uniform(0.0, 0.5, n)
+    Y = Z[:, None] * yf[None, :] + (1.0 - Z)[:, None] * ya[None, :]
+    others = [i for i, s in enumerate(species) if s not in tuple(fuel) + ("O2", "N2")]
+    Y[:, others] = 10.0 ** rng.uniform(-8.0, -2.0, (n, len(others)))
+    Y /= Y.sum(axis=1, keepdims=True)
+    T = rng.uniform(900.0, 2400.0, n)
+    return Y, T
+
+
+def _central(orc, y, j, p):
+    h = 1e-5 * max(abs(y[j]), 1e-6) if j < len(y) - 1 else 1e-5 * y[j]
+    yp, ym = y.copy(), y.copy()
+    yp[j] += h
+    ym[j] -= h
+    return (orc.rhs(yp, p)[0] - orc.rhs(ym, p)[0]) / (2 * h)
+
+
+@pytest.mark.parametrize("name", ["h2co", "ch4", "ch4_1step", "sri_rev"])
+def test_analytic_jacobian_against_central_differences(cuda, name):
+    import torch
+    from laminarsmoke_b200 import lsg
+    from oracle.oracle import OracleMechanism
+    data, species = _mech(name)
+    n = len(species) + 1
+    Y, T = _states(data, species, 24, 3)
+    y = np.ascontiguousarray(np.concatenate([Y.T, T[None, :]], axis=0))
+    ctx = lsg.ReactionStep(lsg.Mechanism(data))
+    J = torch.zeros((24, n, n), dtype=torch.float64, device=cuda)
+    ctx.jacobian_device(torch.tensor(y, device=cuda), J)
+    torch.cuda.synchronize()
+    ctx.check()
+    Jg = J.cpu().numpy()
+    orc = OracleMechanism(data)
+    worst = 0.0
+    for k in range(24):
+        yk = y[:, k].copy()
+        f0 = orc.rhs(yk)[0]
+        for j in range(n):
+            ref = _central(orc, yk, j, 101325.0)
+            scale = max(np.abs(ref).max(), 1e-12 * np.abs(f0).max() / max(abs(yk[j]), 1e-12))
+            err = np.abs(Jg[k, :, j] - ref).max() / scale
+            worst = max(worst, err)
+            assert err <= 1e-4, (name, k, j, err)
+    print(f"{name}: worst column error against central differences {worst:.2e}")
+
+
+@pytest.mark.parametrize("rtol,atol,frac", [(1e-7, 1e-12, 0.97), (1e-10, 1e-16, 0.99)])
+def test_round_scheme_with_analytic_jacobian(cuda, h2co, rtol, atol, frac):
+    """The round scheme with the analytic Jacobian against the oracle (which differentiates numerically,
+    as the reference does): identical statuses, T within 1e-6, Y within 1e-9 in most cells and 1e-7 in
+    all; one RHS call per Jacobian (its temperature column) instead of n."""
+    import torch
+    from laminarsmoke_b200 import lsg
+    from oracle.oracle import OracleMechanism
+    data, species, A = h2co
+    n = 2048
+    Y, T = cells.h2co_mixing(species, A["mw"], n, seed=4)
+    ctx = lsg.ReactionStep(lsg.Mechanism(data), tile=lsg.LSG_TILE_LANE, precision=lsg.LSG_PRECISION_MIXED,
+                           jacobian=lsg.LSG_JACOBIAN_ANALYTIC, rtol=rtol, atol=atol)
+    Yd = torch.tensor(np.ascontiguousarray(Y.T), device=cuda)
+    Td = torch.tensor(T, device=cuda)
+    st = torch.zeros(n, dtype=torch.int32, device=cuda)
+    cnt = torch.zeros((n, lsg.NCOUNTERS), dtype=torch.int64, device=cuda)
+    ctx.step_device(Yd, Td, 1e-5, status=st, counters=cnt)
+    torch.cuda.synchronize()
+    ctx.check()
+    Yo, To, _, sto, co = OracleMechanism(data).reaction_step(Y, T, 1e-5, rtol=rtol, atol=atol, nthreads=8)
+    c = cnt.cpu().numpy()
+    np.testing.assert_array_equal(st.cpu().numpy(), sto)
+    assert (c[:, 7] == c[:, 2]).all()          # one RHS call per Jacobian
+    dT = np.abs(Td.cpu().numpy() - To) / To
+    dY = np.abs(Yd.cpu().numpy().T - Yo).max(axis=1)
+    print(f"analytic J rtol {rtol:g}: max rel T {dT.max():.2e}, max abs Y {dY.max():.2e}, within 1e-9 "
+          f"{np.mean(dY <= 1e-9):.4f}; steps/cell {c[:, 0].mean():.1f} (oracle {co[:, 0].mean():.1f}), "
+          f"RHS/cell {c[:, 1].mean() + c[:, 7].mean():.1f} (oracle {co[:, 1].mean() + co[:, 7].mean():.1f})")
+    assert dT.max() <= 1e-6
+    assert np.mean(dY <= 1e-9) >= frac and dY.max() <= 1e-7

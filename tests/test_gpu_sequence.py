@@ -81,3 +81,43 @@ def test_coflow_sequence_block_121(cuda):
     Y, T = _coflow_subset(species, A["mw"], 128)
     g, o = _sequence(data, Y, T, 3)
     _compare(g, o, 0.9)
+
+
+@pytest.mark.parametrize("name,tile,precision", [("h2co", 1, 0), ("h2co", 3, 1), ("h2co+30", 4, 0),
+                                                 ("h2co+30", 4, 1), ("h2co", 2, 1)],
+                         ids=["plain", "persistent", "block-fp64", "block-tc", "rounds"])
+def test_sequence_graph_equals_step_by_step(cuda, name, tile, precision):
+    """lsg_reaction_step_sequence_device captures the steps into a CUDA graph (the round scheme, whose
+    rounds wait on the host, runs them one by one): its result must be the one of the same steps
+    made one call at a time, bit for bit, on the first call and on the replay."""
+    import torch
+    from laminarsmoke_b200 import lsg, mech
+    from laminarsmoke_b200.mech import blob
+    data, species = mech.load(name)
+    A, _ = blob.unpack(data)
+    Y, T = _coflow_subset(species[:14], A["mw"][:14], 256)
+    if len(species) > 14:
+        Yp = np.zeros((len(T), len(species)))
+        Yp[:, :14] = 0.5 * Y
+        Yp[:, 14:] = 0.5 / (len(species) - 14)
+        Y = Yp
+    m = lsg.Mechanism(data)
+    nsteps = 4
+    ref = lsg.ReactionStep(m, tile=tile, precision=precision)
+    Yr = torch.tensor(np.ascontiguousarray(Y.T), device=cuda)
+    Tr = torch.tensor(T, device=cuda)
+    for k in range(nsteps):
+        ref.step_device(Yr, Tr, DT, t0=k * DT)
+    torch.cuda.synchronize()
+    ref.check()
+    ctx = lsg.ReactionStep(m, tile=tile, precision=precision)
+    Yg = torch.empty_like(Yr)
+    Tg = torch.empty_like(Tr)
+    for call in range(2):
+        Yg.copy_(torch.tensor(np.ascontiguousarray(Y.T), device=cuda))
+        Tg.copy_(torch.tensor(T, device=cuda))
+        used = ctx.step_sequence_graph(Yg, Tg, DT, nsteps)
+        torch.cuda.synchronize()
+        ctx.check()
+        assert used == (tile != 2)
+        assert torch.equal(Yg, Yr) and torch.equal(Tg, Tr), f"call {call}"

@@ -332,6 +332,24 @@ int lsg_steady_sources_device(lsg_ctx* ctx, int ncells, int nspecies, const doub
                               long ld, const double* p_dev, double p_scalar, double* S_implicit_dev,
                               double* S_explicit_dev, long lds, void* stream);
 
+/* The steady solvers' default linearisation, sparseJacobian true
+ * (steady/readOptionsSteadyState.H:46): linearModel::reactionJacobianSparse
+ * (steady/linearModel.H:172-232).  The same sources S and outputs as
+ * lsg_steady_sources_device; the diagonal J_k differs:
+ *   species (with species_equations != 0, else 0): the reference's analytic
+ *     derivative of the formation rate in omega_k (maps/JacobianSparsityPattern
+ *     Map.hpp:427-560) at omega* = max(max(Y, 0), 1e-13), times MW_k -- order
+ *     times rate over omega* for the forward and reverse products, the
+ *     third-body efficiencies, a 1e-4 difference of the fall-off correction,
+ *     and the CABR term;
+ *   temperature (with energy_equation != 0, else 0): the forward difference of
+ *     the dense path.
+ * Same scratch, limits and pressure arguments as lsg_steady_sources_device. */
+int lsg_steady_sources_sparse_device(lsg_ctx* ctx, int ncells, int nspecies, const double* Y_dev, const double* T_dev,
+                                     long ld, const double* p_dev, double p_scalar, int species_equations,
+                                     int energy_equation, double* S_implicit_dev, double* S_explicit_dev, long lds,
+                                     void* stream);
+
 /* ---- property update after the step ----------------------------------------
  * What solvers/laminarSMOKE/properties.H:40-190 evaluates per cell after each
  * reaction step, from the mechanism's fitted transport data (a blob compiled

@@ -1003,6 +1003,35 @@ int lsg_steady_sources_device(lsg_ctx* c, int ncells, int nspecies, const double
   return LSG_OK;
 }
 
+int lsg_steady_sources_sparse_device(lsg_ctx* c, int ncells, int nspecies, const double* Y, const double* T, long ld,
+                                     const double* p, double p_scalar, int species_equations, int energy_equation,
+                                     double* S_implicit, double* S_explicit, long lds, void* stream) {
+  if (!c || ncells < 0 || !Y || !T || !S_implicit || !S_explicit || ld < ncells || lds < ncells) return LSG_ERR_ARG;
+  if (!p && !(p_scalar > 0.)) return LSG_ERR_ARG;
+  const MechLayout& L = c->mech->host.layout;
+  if (nspecies != L.nc) return LSG_ERR_ARG;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  const cudaStream_t s = (cudaStream_t)stream;
+  const long need = 3L * (L.nc + 1) * ncells;
+  if (need > c->frs_cap) {
+    if (cudaStreamSynchronize(s) != cudaSuccess) return LSG_ERR_CUDA;
+    cudaFree(c->frs);
+    c->frs = nullptr;
+    c->frs_cap = 0;
+    if (cudaMalloc(&c->frs, sizeof(double) * need) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+    c->frs_cap = need;
+  }
+  if (!sm_count(c)) return LSG_ERR_CUDA;
+  const cudaError_t e = launch_steady_sources_sparse(L, c->mech->d_buf, ncells, Y, T, ld, p, p_scalar,
+                                                     species_equations ? 1 : 0, energy_equation ? 1 : 0, c->frs,
+                                                     S_implicit, S_explicit, lds, c->sm_count, c->d_err, s);
+  if (e == cudaErrorInvalidValue) { cudaGetLastError(); return LSG_ERR_UNSUPPORTED; }
+  if (e != cudaSuccess) return LSG_ERR_CUDA;
+  ++c->launches;
+  return LSG_OK;
+}
+
 int lsg_formation_rates_device(lsg_ctx* c, int ncells, int nspecies, const double* Y, const double* T, long ld,
                                double p, double* out, long ld_out, void* stream) {
   if (!c || ncells < 0 || !Y || !T || !out || ld < ncells || ld_out < ncells || !(p > 0.)) return LSG_ERR_ARG;

@@ -144,6 +144,12 @@ cudaError_t launch_steady_sources(const MechLayout& L, const unsigned char* mech
                                   const double* T, long ld, const double* p, double p_scalar, double* scratch,
                                   double* Simp, double* Sexp, long lds, int sm_count, int* err, cudaStream_t stream);
 
+// the steady solvers' default sparse linearisation (lsg_rounds.cu); scratch: 3 (nc + 1) ncells doubles
+cudaError_t launch_steady_sources_sparse(const MechLayout& L, const unsigned char* mech_gmem, long ncells,
+                                         const double* Y, const double* T, long ld, const double* p, double p_scalar,
+                                         int species, int energy, double* scratch, double* Simp, double* Sexp,
+                                         long lds, int sm_count, int* err, cudaStream_t stream);
+
 // output fields (lsg_outputs.cu)
 cudaError_t launch_compact_sources(const MechLayout& L, const unsigned char* mech_gmem, long ncells,
                                    const double* Y0, const double* T0, const double* Yf, const double* Tf, long ld,

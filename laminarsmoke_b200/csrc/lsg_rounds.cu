@@ -1035,6 +1035,298 @@ __global__ void __launch_bounds__(kRT, 4) steady_sources_kernel(MechLayout Lp, c
   }
 }
 
+// Fall-off correction of slot fo at the third-body concentration Mc (KineticsMap_CHEMKIN.hpp:1552-1610,
+// FallOffReactionsCorrection): k_inf (Pr / (1 + Pr)) F / kArr.
+__device__ __forceinline__ double falloff_corr(const MechView& M, const MechLayout& L, int fo, double kArr, double Mc,
+                                              double T, double logT, double uT) {
+  const double kInf = exp(M.D(L.fo_lnA)[fo] + M.D(L.fo_beta)[fo] * logT - M.D(L.fo_eor)[fo] * uT);
+  const double a = M.D(L.fo_a)[fo], b = M.D(L.fo_b)[fo], c = M.D(L.fo_c)[fo], d = M.D(L.fo_d)[fo];
+  const int ty = M.I(L.fo_type)[fo];
+  const double Pr = kArr * Mc / kInf;
+  double wF = 1.;
+  if (ty == 1) {
+    double v = (1. - a) * exp(-T / b) + a * exp(-T / c);
+    if (d != 0.) v += exp(-d / T);
+    const double lF = (v < 1.e-300) ? -300. : log10(v);
+    double qq;
+    if (Pr > 1.e-32) {
+      const double nTroe = 0.75 - 1.27 * lF;
+      const double cTroe = -0.4 - 0.67 * lF;
+      const double sTroe = log10(Pr) + cTroe;
+      qq = sTroe / (nTroe - 0.14 * sTroe);
+    } else {
+      qq = 1. / 0.14;
+    }
+    wF = exp10(lF / (1. + qq * qq));
+  } else if (ty == 2) {
+    const double lF = a * exp(-b / T) + exp(-T / c);
+    double xSRI = 0.;
+    if (Pr > 1.e-32) {
+      const double l10 = log10(Pr);
+      xSRI = 1. / (1. + l10 * l10);
+    }
+    wF = pow(lF, xSRI) * d;
+    const double e = M.D(L.fo_e)[fo];
+    if (e != 0.) wF *= pow(T, e);
+  }
+  return kInf * (Pr / (1. + Pr)) * wF / kArr;
+}
+
+// ---------------------------------------------------------------------------
+// The steady solvers' default linearisation (sparseJacobian true,
+// steady/readOptionsSteadyState.H:46): linearModel::reactionJacobianSparse
+// (steady/linearModel.H:172-232).  The species entries of the diagonal are
+// JacobianSparsityPatternMap::Jacobian (maps/JacobianSparsityPatternMap.hpp:
+// 427-560) at omega* = max(max(Y, 0), 1e-13), times MW:
+//   J_k = MW_k sum_j nu_kj [ lambda_jk r_f,j / omega*_k - nu'_jk r_b,j / omega*_k
+//         + (r_f,j - r_b,j) c*_k / omega*_k (eps_jk - 1) / M_j              (third body)
+//         + (r_f,j - r_b,j) dG_jk / G_j   or  (r_f,j - r_b,j)  (fall-off / CABR) ]
+// each term present where the reaction's orders, products, efficiencies or
+// bath name k; dG a forward difference of the fall-off correction with an
+// omega increment of 1e-4, at fixed density; the kinetics evaluated at
+// c* = omega* rho* / MW with cTot = P / (R T) given.  Thread-serial; scratch
+// as rhs_cell: C = c*, G = h/RT - s/R, R = the accumulated diagonal.  Y: the
+// unclipped mass fractions (stride ys).  Writes J_k to Jk[k * js].
+// ---------------------------------------------------------------------------
+__device__ __noinline__ void steady_sparse_diagonal(const MechLayout* __restrict__ Lp, const double* __restrict__ Md,
+                                                    const int* __restrict__ Mi, double* __restrict__ scratch,
+                                                    const double* __restrict__ Yc, long ys, double T, double P0,
+                                                    double* __restrict__ Jk, long js) {
+  const MechLayout& L = *Lp;
+  const MechView M{Md, Mi};
+  const int NC = L.nc, NR = L.nr;
+  const int tid = threadIdx.x;
+  double* C = scratch;
+  double* G = scratch + NC * kRT;
+  double* D = scratch + 2 * NC * kRT;
+#define SC_(arr, i) arr[(i) * kRT + tid]
+  const double* MW = M.D(L.mw);
+  const double eps = 1.e-13;
+  auto om = [&](int k) {
+    const double o = fmax(Yc[(long)k * ys], 0.);
+    return o > eps ? o : eps;
+  };
+  double u = 0.;
+  for (int i = 0; i < NC; ++i) u += om(i) / MW[i];
+  const double MWs = 1. / u;
+  const double cTs = P0 / kRgas / T;
+  const double rhos = cTs * MWs;
+  const double* TM = M.D(L.t_mid);
+  const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, uT = 1. / T;
+  const double logT = log(T);
+  const double lP = log(101325. / kRgas / T);
+  for (int i = 0; i < NC; ++i) {
+    SC_(C, i) = om(i) * rhos / MW[i];
+    const bool hi = T > TM[i];
+    const double* A = hi ? M.D(L.dh_ht) + 6 * i : M.D(L.dh_lt) + 6 * i;
+    const double hrt = A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4] + uT * A[5];
+    const double* B = hi ? M.D(L.ds_ht) + 6 * i : M.D(L.ds_lt) + 6 * i;
+    SC_(G, i) = hrt - (B[0] * logT + T * B[1] + T2 * B[2] + T3 * B[3] + T4 * B[4] + B[5]);
+    SC_(D, i) = 0.;
+  }
+  const double* lnA = M.D(L.lnA);
+  const double* beta = M.D(L.beta);
+  const double* eor = M.D(L.eor);
+  const double* dnu = M.D(L.dnu);
+  const int* sgn = M.I(L.a_sign);
+  const int* rk = M.I(L.rev_kind);
+  const int* rs = M.I(L.rev_slot);
+  const int* tbs = M.I(L.tb_slot);
+  const int* fos = M.I(L.fo_slot);
+  const int* rp = M.I(L.reac_ptr);
+  const int* rsp = M.I(L.reac_sp);
+  const double* rnu = M.D(L.reac_nu);
+  const int* op = M.I(L.ford_ptr);
+  const int* osp = M.I(L.ford_sp);
+  const double* onu = M.D(L.ford_val);
+  const int* pp = M.I(L.prod_ptr);
+  const int* psp = M.I(L.prod_sp);
+  const double* pnu = M.D(L.prod_nu);
+  for (int j = 0; j < NR; ++j) {
+    double kArr = exp(lnA[j] + beta[j] * logT - eor[j] * uT);
+    if (sgn[j] < 0) kArr *= -1.;
+    if (L.n_plog > 0) {
+      const int ps = M.I(L.plog_slot)[j];
+      if (ps >= 0) kArr = plog_k(M, L, ps, T, logT, P0);
+    }
+    if (L.n_cheb > 0) {
+      const int cs = M.I(L.cheb_slot)[j];
+      if (cs >= 0) kArr = cheb_k(M, L, cs, T, P0);
+    }
+    double kMod = kArr, Mtb = 0.;
+    const int tb = tbs[j];
+    if (tb >= 0) {
+      Mtb = cTs;
+      const int* tp = M.I(L.tb_ptr);
+      const int* ts = M.I(L.tb_sp);
+      const double* te = M.D(L.tb_eff);
+      for (int q = tp[tb]; q < tp[tb + 1]; ++q) Mtb += SC_(C, ts[q]) * te[q];
+      kMod *= Mtb;
+    }
+    const int fo = fos[j];
+    bool cabr = false;
+    double Gcorr = 1.;
+    if (fo >= 0) {
+      cabr = M.I(L.fo_cabr)[fo] != 0;
+      const int single = M.I(L.fo_single)[fo];
+      double Mc;
+      if (single < 0) {
+        Mc = cTs;
+        const int* fp = M.I(L.fo_ptr);
+        const int* fs = M.I(L.fo_sp);
+        const double* fe = M.D(L.fo_eff);
+        for (int q = fp[fo]; q < fp[fo + 1]; ++q) Mc += SC_(C, fs[q]) * fe[q];
+      } else {
+        Mc = SC_(C, single) + 1.e-16;
+      }
+      if (cabr) {
+        // KineticsMap_CHEMKIN::ChemicallyActivatedBimolecularReactions (:1613-1660): F / (1 + Pr)
+        const double kInf = exp(M.D(L.fo_lnA)[fo] + M.D(L.fo_beta)[fo] * logT - M.D(L.fo_eor)[fo] * uT);
+        const double Pr = kArr * Mc / kInf;
+        const double a = M.D(L.fo_a)[fo], b = M.D(L.fo_b)[fo], c = M.D(L.fo_c)[fo], d = M.D(L.fo_d)[fo];
+        const int ty = M.I(L.fo_type)[fo];
+        double wF = 1.;
+        if (ty == 1) {
+          double v = (1. - a) * exp(-T / b) + a * exp(-T / c);
+          if (d != 0.) v += exp(-d / T);
+          const double lF = (v < 1.e-300) ? -300. : log10(v);
+          const double nTroe = 0.75 - 1.27 * lF;
+          const double cTroe = -0.4 - 0.67 * lF;
+          const double sTroe = log10(Pr) + cTroe;
+          const double qq = sTroe / (nTroe - 0.14 * sTroe);
+          wF = exp10(lF / (1. + qq * qq));
+        } else if (ty == 2) {
+          const double lF = a * exp(-b / T) + exp(-T / c);
+          const double l10 = log10(Pr);
+          wF = pow(lF, 1. / (1. + l10 * l10)) * d;
+          const double e = M.D(L.fo_e)[fo];
+          if (e != 0.) wF *= pow(T, e);
+        }
+        kMod *= (1. / (1. + Pr)) * wF;
+      } else {
+        Gcorr = falloff_corr(M, L, fo, kArr, Mc, T, logT, uT);
+        kMod *= Gcorr;
+      }
+    }
+    double fwd = 1.;
+    for (int q = op[j]; q < op[j + 1]; ++q) fwd *= conc_factor_r(onu[q], SC_(C, osp[q]));
+    double rbj = 0.;
+    const int kind = rk[j];
+    if (kind != 0) {
+      double rv = 1.;
+      for (int q = pp[j]; q < pp[j + 1]; ++q) rv *= conc_factor_r(pnu[q], SC_(C, psp[q]));
+      double rf;
+      if (kind == 1) {
+        double dg = 0.;
+        for (int q = pp[j]; q < pp[j + 1]; ++q) dg += contrib_r(pnu[q], SC_(G, psp[q]));
+        for (int q = rp[j]; q < rp[j + 1]; ++q) dg -= contrib_r(rnu[q], SC_(G, rsp[q]));
+        rf = exp(dg - lP * dnu[j]);
+      } else {
+        const int sr = rs[j];
+        rf = exp(M.D(L.rev_lnA)[sr] + M.D(L.rev_beta)[sr] * logT - M.D(L.rev_eor)[sr] * uT) / kArr;
+      }
+      rbj = (rv * rf) * kMod;
+    }
+    const double rfj = kMod * fwd;
+    // the bracket of species k in reaction j
+    auto bracket = [&](int k) {
+      const double omk = om(k);
+      double v = 0.;
+      for (int q = op[j]; q < op[j + 1]; ++q)
+        if (osp[q] == k) v = onu[q] * rfj / omk;
+      for (int q = pp[j]; q < pp[j + 1]; ++q)
+        if (psp[q] == k) v -= pnu[q] * rbj / omk;
+      if (tb >= 0) {
+        const int* tp = M.I(L.tb_ptr);
+        const int* ts = M.I(L.tb_sp);
+        const double* te = M.D(L.tb_eff);
+        for (int q = tp[tb]; q < tp[tb + 1]; ++q)
+          if (ts[q] == k) v += (rfj - rbj) * SC_(C, k) / omk * te[q] / Mtb;
+      }
+      if (fo >= 0) {
+        const int single = M.I(L.fo_single)[fo];
+        bool has = single == k;
+        const int* fp = M.I(L.fo_ptr);
+        const int* fs = M.I(L.fo_sp);
+        const double* fe = M.D(L.fo_eff);
+        if (single < 0)
+          for (int q = fp[fo]; q < fp[fo + 1]; ++q)
+            if (fs[q] == k) has = true;
+        if (has) {
+          if (cabr) {
+            v += (rfj - rbj);
+          } else {
+            // M at c* with c*_k from omega*_k + 1e-4 (density unchanged)
+            const double ck_plus = (omk + 1.e-4) * rhos / MW[k];
+            double Mp;
+            if (single < 0) {
+              Mp = cTs;
+              for (int q = fp[fo]; q < fp[fo + 1]; ++q) Mp += (fs[q] == k ? ck_plus : SC_(C, fs[q])) * fe[q];
+            } else {
+              Mp = ck_plus + 1.e-16;
+            }
+            const double Gp = falloff_corr(M, L, fo, kArr, Mp, T, logT, uT);
+            const double dG = (Gp - Gcorr) / 1.e-4;
+            v += (rfj - rbj) * dG / Gcorr;
+          }
+        }
+      }
+      return v;
+    };
+    for (int q = rp[j]; q < rp[j + 1]; ++q) SC_(D, rsp[q]) -= rnu[q] * bracket(rsp[q]);
+    for (int q = pp[j]; q < pp[j + 1]; ++q) SC_(D, psp[q]) += pnu[q] * bracket(psp[q]);
+  }
+  for (int k = 0; k < NC; ++k) Jk[(long)k * js] = SC_(D, k) * MW[k];
+#undef SC_
+}
+
+// sparseJacobian true: the species diagonal of steady_sparse_diagonal (with speciesEquations on, else
+// zero) and the temperature entry by the forward difference of the dense path (with energyEquation on,
+// else zero).  yb, s0, sp: scratch [n][ncells].
+__global__ void __launch_bounds__(kRT, 4) steady_sources_sparse_kernel(
+    MechLayout Lp, const unsigned char* __restrict__ mech_gmem, long ncells, const double* __restrict__ Y,
+    const double* __restrict__ T, long ld, const double* __restrict__ pc, double p_scalar, int species, int energy,
+    double* __restrict__ yb, double* __restrict__ s0, double* __restrict__ sp, double* __restrict__ Simp,
+    double* __restrict__ Sexp, long lds, int* err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ MechLayout sL;
+  if (threadIdx.x == 0) sL = Lp;
+  if (!stage_bulk(smem, mech_gmem, Lp.bytes, &mbar, err)) return;
+  const double* Md = (const double*)smem;
+  const int* Mi = (const int*)(smem + (size_t)Lp.n_double * sizeof(double));
+  double* scratch = (double*)(smem + ((Lp.bytes + 15u) & ~15u));
+  const int NC = Lp.nc, n = NC + 1;
+  for (long c = (long)blockIdx.x * kRT + threadIdx.x; c < ncells; c += (long)gridDim.x * kRT) {
+    for (int i = 0; i < NC; ++i) yb[(long)i * ncells + c] = fmax(Y[(long)i * ld + c], 0.);
+    yb[(long)NC * ncells + c] = T[c];
+    const double P0 = pc ? pc[c] : p_scalar;
+    const double* y = yb + c;
+    s0[(long)NC * ncells + c] = rhs_cell<true>(&sL, Md, Mi, scratch, y, ncells, -1, 0., s0 + c, ncells, P0, 1, 0.);
+    double JT = 0.;
+    if (energy) {   // linearModel.H:195-230, the dense path's increment for the T entry
+      const double yk = T[c];
+      const double ew = 1. / (1.e-12 + 1.e-7 * fabs(yk));
+      double hJ = sqrt(kMachEpsDouble) * fabs(fmax(yk, 1. / ew));
+      hJ = fmax(hJ, 1. / ew);
+      hJ = fmax(hJ, sqrt(kTinyFloat));
+      const double dy = fmin(hJ, 1.e-3 + 1e-3 * fabs(yk));
+      const double qp = rhs_cell<true>(&sL, Md, Mi, scratch, y, ncells, NC, yk + dy, sp + c, ncells, P0, 1, 0.);
+      JT = (qp - s0[(long)NC * ncells + c]) * (1. / dy);
+    }
+    if (species) {
+      steady_sparse_diagonal(&sL, Md, Mi, scratch, Y + c, ld, T[c], P0, Simp + c, lds);
+    } else {
+      for (int k = 0; k < NC; ++k) Simp[(long)k * lds + c] = 0.;
+    }
+    Simp[(long)NC * lds + c] = JT;
+    for (int k = 0; k < n; ++k) {
+      const double yk = k < NC ? Y[(long)k * ld + c] : T[c];
+      Sexp[(long)k * lds + c] = s0[(long)k * ncells + c] - Simp[(long)k * lds + c] * yk;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // advance: one lane group per listed cell -- a warp, or half a warp when the
 // cell has at most 16 components (two cells per warp) -- lane k of the group
@@ -1819,6 +2111,28 @@ cudaError_t launch_jacobian(const MechLayout& L, const unsigned char* mech_gmem,
   const long want = (ncells + kRT - 1) / kRT, cap = (long)sm_count * 4;
   jacobian_kernel<<<(unsigned)(want < cap ? want : cap), kRT, smem, stream>>>(L, mech_gmem, ncells, y, ld, p, energy,
                                                                              J, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_steady_sources_sparse(const MechLayout& L, const unsigned char* mech_gmem, long ncells,
+                                         const double* Y, const double* T, long ld, const double* p, double p_scalar,
+                                         int species, int energy, double* scratch, double* Simp, double* Sexp,
+                                         long lds, int sm_count, int* err, cudaStream_t stream) {
+  if (ncells <= 0) return cudaSuccess;
+  const size_t smem = ((L.bytes + 15u) & ~15u) + (size_t)3 * L.nc * kRT * sizeof(double);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e =
+      cudaFuncSetAttribute(steady_sources_sparse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int bps = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, steady_sources_sparse_kernel, kRT, smem);
+  if (e != cudaSuccess) return e;
+  if (bps <= 0) return cudaErrorInvalidConfiguration;
+  const long want = (ncells + kRT - 1) / kRT, cap = (long)sm_count * bps;
+  const long n = L.nc + 1;
+  steady_sources_sparse_kernel<<<(unsigned)(want < cap ? want : cap), kRT, smem, stream>>>(
+      L, mech_gmem, ncells, Y, T, ld, p, p_scalar, species, energy, scratch, scratch + n * ncells,
+      scratch + 2 * n * ncells, Simp, Sexp, lds, err);
   return cudaGetLastError();
 }
 

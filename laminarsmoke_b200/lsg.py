@@ -52,7 +52,7 @@ EXPORTS = (
     "lsg_compact_sources_device", "lsg_formation_rates_device",
     "lsg_reaction_step_cv", "lsg_reaction_step_cv_device", "lsg_steady_sources_device",
     "lsg_mech_transport_info", "lsg_properties_device", "lsg_properties", "lsg_build_and_invert_g_device",
-    "lsg_reaction_step_sequence_device", "lsg_jacobian_device",
+    "lsg_reaction_step_sequence_device", "lsg_jacobian_device", "lsg_steady_sources_sparse_device",
 )
 
 # lsg_property_fields, in declaration order: species rows (nc), scalars, light-species rows
@@ -93,6 +93,7 @@ def lib():
     L.lsg_build_and_invert_g_device.argtypes = [vp, i, i, vp, vp, vp, vp]
     L.lsg_reaction_step_sequence_device.argtypes = [vp, i, i, i, vp, l, vp, d, d, d, vp, vp, C.POINTER(i), vp]
     L.lsg_jacobian_device.argtypes = [vp, i, vp, l, d, vp, vp]
+    L.lsg_steady_sources_sparse_device.argtypes = [vp, i, i, vp, vp, l, vp, d, i, i, vp, vp, l, vp]
     L.lsg_strerror.argtypes = [i]
     L.lsg_strerror.restype = C.c_char_p
     L.lsg_abi_version.restype = i
@@ -340,6 +341,18 @@ class ReactionStep:
         _check(lib().lsg_steady_sources_device(self.h, T.shape[0], nc, Y.data_ptr(), T.data_ptr(), ld, pp, ps,
                                                S_implicit.data_ptr(), S_explicit.data_ptr(), S_implicit.shape[1],
                                                _stream_handle(stream)), "lsg_steady_sources_device")
+
+    def steady_sources_sparse_device(self, Y, T, S_implicit, S_explicit, p=101325.0, species=True, energy=True,
+                                     stream=None):
+        """The steady solvers' default linearisation, sparseJacobian true (lsg_steady_sources_sparse_device):
+        as steady_sources_device with the analytic species diagonal."""
+        _require_layout(Y, T, S_implicit, S_explicit, p if hasattr(p, "data_ptr") else None)
+        nc, ld = Y.shape
+        pp, ps = (p.data_ptr(), 0.0) if hasattr(p, "data_ptr") else (None, float(p))
+        _check(lib().lsg_steady_sources_sparse_device(
+            self.h, T.shape[0], nc, Y.data_ptr(), T.data_ptr(), ld, pp, ps, int(species), int(energy),
+            S_implicit.data_ptr(), S_explicit.data_ptr(), S_implicit.shape[1], _stream_handle(stream)),
+            "lsg_steady_sources_sparse_device")
 
     def formation_rates_device(self, Y, T, out, p: float = 101325.0, stream=None):
         """R_i MW_i [kg/m3/s] of every species at the states (Y [NC, ld], T) into out [NC, ld_out]."""

@@ -111,9 +111,9 @@ void lsg_options_default(lsg_options* opt);
  * The blob is produced offline from CHEMKIN files by
  * `python -m laminarsmoke_b200.mech compile KIN.CKI THERMO.CKT -o mech.lsmech`
  * (it replaces openSMOKEppCHEMKINPreProcessor + kinetics.xml, which the
- * reference loads at solvers/laminarSMOKE/readOptions.H:62-78).  A blob with
- * extended PLOG (PLOGMX/PLOGSP) or extended fall-off (LOWMX/LOWSP) reactions,
- * which the device kernels do not evaluate, is refused with LSG_ERR_UNSUPPORTED. */
+ * reference loads at solvers/laminarSMOKE/readOptions.H:62-78).  Every rate
+ * form of the compiler is evaluated on the device, the extended PLOG
+ * (PLOGMX/PLOGSP) and extended fall-off (LOWMX/LOWSP) forms included. */
 int lsg_mech_load_blob(const void* blob, size_t nbytes, int device, lsg_mech** out);
 int lsg_mech_load_file(const char* path, int device, lsg_mech** out);
 int lsg_mech_info(const lsg_mech* mech, int* nspecies, int* nreactions);
@@ -276,7 +276,10 @@ int lsg_build_and_invert_g_device(lsg_ctx* ctx, int nmat, int n, const double* J
  * difference with the increment sqrt(eps) max(T, 1).  What the reference
  * would compute in KernelDense::UserDefinedJacobian, which it leaves
  * unimplemented (KernelDense.hpp:96-109); the step uses it with
- * lsg_options.jacobian = LSG_JACOBIAN_ANALYTIC.  Up to 31 species. */
+ * lsg_options.jacobian = LSG_JACOBIAN_ANALYTIC.  Up to 31 species;
+ * LSG_ERR_UNSUPPORTED for mechanisms with extended PLOG or fall-off reactions
+ * (their constants depend on the concentrations; the step keeps the
+ * differences for them). */
 int lsg_jacobian_device(lsg_ctx* ctx, int ncells, const double* y_dev, long ld, double p, double* J_dev, void* stream);
 
 /* ---- right-hand side -----------------------------------------------------

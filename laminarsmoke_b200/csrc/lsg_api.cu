@@ -942,7 +942,7 @@ int lsg_jacobian_device(lsg_ctx* c, int ncells, const double* y, long ld, double
   if (!c || ncells < 0 || !y || !J || ld < ncells || !(p > 0.)) return LSG_ERR_ARG;
   if (ncells == 0) return LSG_OK;
   const MechLayout& L = c->mech->host.layout;
-  if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
+  if (L.nc + 1 > 32 || L.n_xplog > 0 || L.n_xfo > 0) return LSG_ERR_UNSUPPORTED;
   if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
   if (!sm_count(c)) return LSG_ERR_CUDA;
   if (launch_jacobian(L, c->mech->d_buf, ncells, y, ld, p, c->opt.energy, J, c->sm_count, c->d_err,

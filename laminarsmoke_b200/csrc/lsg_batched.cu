@@ -178,6 +178,10 @@ __device__ __noinline__ double rhs_lane(const MechLayout* __restrict__ Lp, const
       const int cs = M.I(L.cheb_slot)[j];
       if (cs >= 0) kArr = cheb_k(M, L, cs, T, Pk);
     }
+    if (L.n_xplog > 0) {  // extended PLOG (KineticsMap_CHEMKIN.hpp:1662-1670)
+      const int xs = M.I(L.xplog_slot)[j];
+      if (xs >= 0) kArr = xplog_k(M, L, xs, T, logT, Pk, cTotSum, [&](int k) { return SC_(C, k); });
+    }
     double kMod = kArr;
     const int tb = tbs[j];
     if (tb >= 0) {
@@ -233,6 +237,13 @@ __device__ __noinline__ double rhs_lane(const MechLayout* __restrict__ Lp, const
       // CABR (KineticsMap_CHEMKIN.hpp:1613-1660): k0 (1 / (1 + Pr)) F; fall-off: k_inf (Pr / (1 + Pr)) F
       if (cabr) kMod *= (1. / (1. + Pr)) * wF;
       else kMod *= kInf * (Pr / (1. + Pr)) * wF / kArr;
+    }
+    if (L.n_xfo > 0) {    // extended fall-off (KineticsMap_CHEMKIN.hpp:1672-1681)
+      const int xs = M.I(L.xfo_slot)[j];
+      if (xs >= 0) {
+        kArr = xfo_k(M, L, xs, T, cTotSum, [&](int k) { return SC_(C, k); });
+        kMod = kArr;
+      }
     }
     double fwd = 1.;
     for (int q = op[j]; q < op[j + 1]; ++q) fwd *= conc_factor_b(onu[q], SC_(C, osp[q]));

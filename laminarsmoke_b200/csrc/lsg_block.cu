@@ -218,7 +218,11 @@ __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, 
     const int* psp = M.I(L.prod_sp);
     const double* pnu = M.D(L.prod_nu);
     for (int j = tid; j < NR; j += BT) {
-      const double kArr = karr[j];
+      double kArr = karr[j];
+      if (L.n_xplog > 0) {   // extended PLOG, every call: k depends on the concentrations (KineticsMap_CHEMKIN.hpp:1662-1670)
+        const int xs = M.I(L.xplog_slot)[j];
+        if (xs >= 0) kArr = xplog_k(M, L, xs, T, log(T), cv ? cTot * kRgas * T : P0, cTotSum, [&](int k) { return W.C[k]; });
+      }
       double kMod = kArr;
       const int tb = tbs[j];
       if (tb >= 0) {
@@ -269,6 +273,13 @@ __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, 
         // CABR (KineticsMap_CHEMKIN.hpp:1613-1660): k0 (1 / (1 + Pr)) F; fall-off: k_inf (Pr / (1 + Pr)) F
         if (cabr) kMod *= (1. / (1. + Pr)) * wF;
         else kMod *= kInf * (Pr / (1. + Pr)) * wF / kArr;
+      }
+      if (L.n_xfo > 0) {     // extended fall-off (KineticsMap_CHEMKIN.hpp:1672-1681)
+        const int xs = M.I(L.xfo_slot)[j];
+        if (xs >= 0) {
+          kArr = xfo_k(M, L, xs, T, cTotSum, [&](int k) { return W.C[k]; });
+          kMod = kArr;
+        }
       }
       double fwd = 1.;
       for (int q = op[j]; q < op[j + 1]; ++q) fwd *= conc_factor_k(onu[q], W.C[osp[q]]);

@@ -55,6 +55,102 @@ static __device__ __noinline__ double plog_k(const MechView& M, const MechLayout
   return exp(kA + (kB - kA) * (log(P) - lnp[i]) / (lnp[i + 1] - lnp[i]));
 }
 
+// PLOG interpolation of points q0 .. q1 - 1 of a table (PressureLogarithmicRateExpression.hpp:104-119 and
+// ExtendedPressureLogarithmicRateExpression.hpp:181-202): the first or last point outside the table, else
+// ln k linear in ln P between the bracketing points.
+static __device__ __forceinline__ double plog_points(const double* p, const double* lnp, const double* lnA,
+                                                     const double* be, const double* er, int q0, int q1, double T,
+                                                     double logT, double P) {
+  if (P <= p[q0]) return exp(lnA[q0] + be[q0] * logT - er[q0] / T);
+  if (P >= p[q1 - 1]) return exp(lnA[q1 - 1] + be[q1 - 1] * logT - er[q1 - 1] / T);
+  int i = q0;
+  for (; i < q1 - 1; ++i)
+    if (P < p[i + 1]) break;
+  const double kA = lnA[i] + be[i] * logT - er[i] / T;
+  const double kB = lnA[i + 1] + be[i + 1] * logT - er[i + 1] / T;
+  return exp(kA + (kB - kA) * (log(P) - lnp[i]) / (lnp[i + 1] - lnp[i]));
+}
+
+// Extended PLOG (PLOGMX / PLOGSP; KineticsMap_CHEMKIN.hpp:1662-1670 with
+// ExtendedPressureLogarithmicRateExpression::KineticConstant, :162-179): the
+// rate constant of slot `slot` at T, P and the concentrations conc(k):
+//   k = (sum over bath species c_s k_s + (cTot - sum c_s) k_mixture) / cTot,
+// each k a PLOG interpolation of that bath's table; cTot the kinetics map's
+// sum of the concentrations.  Replaces the reaction's Arrhenius constant.
+template <class Conc>
+__device__ double xplog_k(const MechView& M, const MechLayout& L, int slot, double T, double logT, double P,
+                          double cTot, Conc conc) {
+  const int* bp = M.I(L.xplog_bath_ptr);
+  const int* bs = M.I(L.xplog_bath_sp);
+  const int* qp = M.I(L.xplog_ptr);
+  double rest = cTot;
+  for (int b = bp[slot]; b < bp[slot + 1]; ++b)
+    if (bs[b] != -1) rest -= conc(bs[b]);
+  double kc = 0.;
+  for (int b = bp[slot]; b < bp[slot + 1]; ++b) {
+    const double kb = plog_points(M.D(L.xplog_p), M.D(L.xplog_lnp), M.D(L.xplog_lnA), M.D(L.xplog_beta),
+                                  M.D(L.xplog_eor), qp[b], qp[b + 1], T, logT, P);
+    kc += (bs[b] != -1 ? conc(bs[b]) : rest) * kb;
+  }
+  return kc / cTot;
+}
+
+// Extended fall-off (LOWMX / LOWSP; KineticsMap_CHEMKIN.hpp:1672-1681 with
+// ExtendedFallOff::KineticConstant, ExtendedFallOff.hpp:170-240): per bath
+// k_inf (Pr / (1 + Pr)) F with the bath's own low-pressure limit k0 and its
+// Lindemann, Troe or SRI form, M from the reaction's efficiencies, the baths
+// weighted by concentration as in the extended PLOG.  Replaces the reaction's
+// modified rate constant.
+template <class Conc>
+__device__ double xfo_k(const MechView& M, const MechLayout& L, int slot, double T, double cTot, Conc conc) {
+  const double* ki = M.D(L.xfo_kinf) + 3 * slot;
+  const double kInf = ki[0] * pow(T, ki[1]) * exp(-ki[2] / T);
+  const int* tp = M.I(L.xfo_tb_ptr);
+  const int* ts = M.I(L.xfo_tb_sp);
+  const double* te = M.D(L.xfo_tb_eff);
+  double Mc = cTot;
+  for (int q = tp[slot]; q < tp[slot + 1]; ++q) Mc += te[q] * conc(ts[q]);
+  const int* bp = M.I(L.xfo_bath_ptr);
+  const int* bs = M.I(L.xfo_bath_sp);
+  const int* ty = M.I(L.xfo_type);
+  const int* pp = M.I(L.xfo_par_ptr);
+  double rest = cTot;
+  for (int b = bp[slot]; b < bp[slot + 1]; ++b)
+    if (bs[b] != -1) rest -= conc(bs[b]);
+  double kc = 0.;
+  for (int b = bp[slot]; b < bp[slot + 1]; ++b) {
+    const double* lo = M.D(L.xfo_low) + 3 * b;
+    const double k0 = lo[0] * pow(T, lo[1]) * exp(-lo[2] / T);
+    const double Pr = k0 / kInf * Mc;
+    const double* t = M.D(L.xfo_par) + pp[b];
+    const int nt = pp[b + 1] - pp[b];
+    double F = 1.;
+    if (ty[b] == 1) {
+      double Fcent = (1. - t[0]) * exp(-T / t[1]) + t[0] * exp(-T / t[2]);
+      if (nt == 4) Fcent += exp(-t[3] / T);
+      double logFcent = -300.;
+      if (Fcent > 1e-300) logFcent = log10(Fcent);
+      double q;
+      if (Pr > 1.e-32) {
+        const double cc = -0.4 - 0.67 * logFcent;
+        const double nn = 0.75 - 1.27 * logFcent;
+        const double e = log10(Pr) + cc;
+        q = e / (nn - 0.14 * e);
+      } else {
+        q = 1. / 0.14;
+      }
+      F = pow(10., logFcent / (1. + q * q));
+    } else if (ty[b] == 2) {
+      const double l = log10(Pr);
+      const double X = 1. / (1. + l * l);
+      F = pow(t[0] * exp(-t[1] / T) + exp(-T / t[2]), X);
+      if (nt == 5) F *= t[3] * pow(T, t[4]);
+    }
+    kc += (bs[b] != -1 ? conc(bs[b]) : rest) * (kInf * (Pr / (1. + Pr)) * F);
+  }
+  return kc / cTot;
+}
+
 // Rate constant of a Chebyshev reaction at T and P
 // (ChebyshevPolynomialRateExpression::KineticConstant, :93-114, with
 // Phi(n, x) = cos((n - 1) acos(x)), :187-190): 10^(sum_nm a_nm phi_n(T~) phi_m(P~))

@@ -32,12 +32,20 @@ struct MechLayout {
   int n_plog;                                                // reactions with PLOG
   int cheb_coef, cheb_lim;                                   // Chebyshev coefficients, limits (by slot)
   int n_cheb;                                                // reactions with CHEB
+  // extended PLOG (PLOGMX / PLOGSP): per slot a CSR of baths, per bath a CSR of points
+  int xplog_p, xplog_lnp, xplog_lnA, xplog_beta, xplog_eor;  // points
+  int n_xplog;                                               // reactions with extended PLOG
+  // extended fall-off (LOWMX / LOWSP): k_inf (A, beta, E/R) per slot, per bath k0 (A, beta, E/R), form, params
+  int xfo_kinf, xfo_tb_eff, xfo_low, xfo_par;
+  int n_xfo;                                                 // reactions with extended fall-off
   // ---- int region offsets
   int a_sign, rev_kind, rev_slot, tb_slot, fo_slot;          // per reaction
   int reac_ptr, reac_sp, prod_ptr, prod_sp;                  // per reaction CSR
   int ford_ptr, ford_sp;                                     // per reaction CSR of the forward orders
   int plog_slot, plog_ptr, plog_rxn;                         // per reaction slot (-1: none); CSR by slot
   int cheb_slot, cheb_rxn, cheb_nm, cheb_ptr;                // likewise for Chebyshev reactions
+  int xplog_slot, xplog_bath_ptr, xplog_bath_sp, xplog_ptr;  // per reaction slot (-1: none); baths (-1: mixture)
+  int xfo_slot, xfo_tb_ptr, xfo_tb_sp, xfo_bath_ptr, xfo_bath_sp, xfo_type, xfo_par_ptr;
   int fr_ptr, fr_rxn;                                        // per species CSR
   int tb_ptr, tb_sp;                                         // third body CSR (by slot)
   int fo_type, fo_single, fo_ptr, fo_sp;                     // fall-off (by slot)

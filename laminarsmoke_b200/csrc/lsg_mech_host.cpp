@@ -140,13 +140,6 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
     return false;
   }
   try {
-    if (b.i.count("xplog_rxn") || b.i.count("xfo_rxn")) {
-      // PLOGMX / PLOGSP and LOWMX / LOWSP (bath-gas-specific PLOG tables and fall-off limits): the
-      // oracle evaluates them, the device kernels do not, so such a mechanism is refused rather than
-      // integrated without them
-      err = "unsupported: extended PLOG or extended fall-off reactions";
-      return false;
-    }
     const auto& dims = b.I("dims");
     const int nc = dims.at(0), nr = dims.at(1);
     if (nc <= 0 || nr < 0 || (int)b.F("mw").size() != nc || (int)b.F("lnA").size() != nr) {
@@ -203,6 +196,18 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
     L.cheb_coef = B.addd(cheb ? b.F("cheb_coef") : none_d);
     L.cheb_lim = B.addd(cheb ? b.F("cheb_lim") : none_d);
     L.fo_eff = B.addd(b.F("fo_eff_m1"));
+    // extended PLOG and extended fall-off, when the mechanism has them
+    const bool xplog = b.i.count("xplog_rxn") != 0;
+    const bool xfo = b.i.count("xfo_rxn") != 0;
+    L.xplog_p = B.addd(xplog ? b.F("xplog_p") : none_d);
+    L.xplog_lnp = B.addd(xplog ? b.F("xplog_lnp") : none_d);
+    L.xplog_lnA = B.addd(xplog ? b.F("xplog_lnA") : none_d);
+    L.xplog_beta = B.addd(xplog ? b.F("xplog_beta") : none_d);
+    L.xplog_eor = B.addd(xplog ? b.F("xplog_eor") : none_d);
+    L.xfo_kinf = B.addd(xfo ? b.F("xfo_kinf") : none_d);
+    L.xfo_tb_eff = B.addd(xfo && !b.F("xfo_tb_eff_m1").empty() ? b.F("xfo_tb_eff_m1") : none_d);
+    L.xfo_low = B.addd(xfo ? b.F("xfo_low") : none_d);
+    L.xfo_par = B.addd(xfo && !b.F("xfo_par").empty() ? b.F("xfo_par") : none_d);
 
     const auto& isrev = b.I("is_reversible");
     const auto& rth = b.I("rev_thermo");
@@ -247,6 +252,70 @@ bool build_mechanism(const void* blob, size_t nbytes, HostMech& out, std::string
         return false;
       }
     L.n_cheb = (int)cheb_rxn.size();
+    {
+      // extended PLOG: slots, bath CSR (species or -1 for the mixture), point CSR per bath
+      std::vector<int> xs(nr, -1);
+      const std::vector<int> xr = xplog ? b.I("xplog_rxn") : std::vector<int>();
+      const std::vector<int> bp = xplog ? b.I("xplog_bath_ptr") : plog_ptr0;
+      const std::vector<int> bs = xplog ? b.I("xplog_bath_sp") : std::vector<int>();
+      const std::vector<int> qp = xplog ? b.I("xplog_ptr") : plog_ptr0;
+      for (size_t k = 0; k < xr.size(); ++k) {
+        if (xr[k] < 0 || xr[k] >= nr || xs[xr[k]] >= 0) { err = "inconsistent extended PLOG arrays in mechanism blob"; return false; }
+        xs[xr[k]] = (int)k;
+      }
+      bool okx = bp.size() == xr.size() + 1 && qp.size() == bs.size() + 1 && bp[0] == 0 && qp[0] == 0 &&
+                 (size_t)bp.back() == bs.size() && (!xplog || (size_t)qp.back() == b.F("xplog_p").size());
+      for (size_t k = 0; okx && k + 1 < bp.size(); ++k) okx = bp[k + 1] > bp[k];
+      for (size_t k = 0; okx && k + 1 < qp.size(); ++k) okx = qp[k + 1] > qp[k];
+      for (size_t k = 0; okx && k < bs.size(); ++k) okx = bs[k] >= -1 && bs[k] < nc;
+      if (okx && xplog)
+        for (const char* k : {"xplog_lnp", "xplog_lnA", "xplog_beta", "xplog_eor"})
+          okx = okx && b.F(k).size() == b.F("xplog_p").size();
+      if (!okx) { err = "inconsistent extended PLOG arrays in mechanism blob"; return false; }
+      L.n_xplog = (int)xr.size();
+      L.xplog_slot = B.addi(xs);
+      L.xplog_bath_ptr = B.addi(bp);
+      L.xplog_bath_sp = B.addi(bs.empty() ? none_i : bs);
+      L.xplog_ptr = B.addi(qp);
+    }
+    {
+      // extended fall-off: slots, third-body CSR, bath CSR, per bath form and parameter CSR
+      std::vector<int> xs(nr, -1);
+      const std::vector<int> xr = xfo ? b.I("xfo_rxn") : std::vector<int>();
+      const std::vector<int> tp = xfo ? b.I("xfo_tb_ptr") : plog_ptr0;
+      const std::vector<int> ts = xfo ? b.I("xfo_tb_sp") : std::vector<int>();
+      const std::vector<int> bp = xfo ? b.I("xfo_bath_ptr") : plog_ptr0;
+      const std::vector<int> bs = xfo ? b.I("xfo_bath_sp") : std::vector<int>();
+      const std::vector<int> ty = xfo ? b.I("xfo_type") : std::vector<int>();
+      const std::vector<int> pp = xfo ? b.I("xfo_par_ptr") : plog_ptr0;
+      for (size_t k = 0; k < xr.size(); ++k) {
+        if (xr[k] < 0 || xr[k] >= nr || xs[xr[k]] >= 0) { err = "inconsistent extended fall-off arrays in mechanism blob"; return false; }
+        xs[xr[k]] = (int)k;
+      }
+      bool okx = tp.size() == xr.size() + 1 && bp.size() == xr.size() + 1 && pp.size() == bs.size() + 1 &&
+                 ty.size() == bs.size() && tp[0] == 0 && bp[0] == 0 && pp[0] == 0 &&
+                 (size_t)tp.back() == ts.size() && (size_t)bp.back() == bs.size();
+      if (okx && xfo)
+        okx = b.F("xfo_kinf").size() == 3 * xr.size() && b.F("xfo_low").size() == 3 * bs.size() &&
+              b.F("xfo_tb_eff_m1").size() == ts.size() && (size_t)pp.back() == b.F("xfo_par").size();
+      for (size_t k = 0; okx && k + 1 < tp.size(); ++k) okx = tp[k + 1] >= tp[k];
+      for (size_t k = 0; okx && k + 1 < bp.size(); ++k) okx = bp[k + 1] > bp[k];
+      for (size_t k = 0; okx && k + 1 < pp.size(); ++k) {
+        const int np = pp[k + 1] - pp[k];
+        okx = (ty[k] == 0 && np == 0) || (ty[k] == 1 && (np == 3 || np == 4)) || (ty[k] == 2 && (np == 3 || np == 5));
+      }
+      for (size_t k = 0; okx && k < bs.size(); ++k) okx = bs[k] >= -1 && bs[k] < nc;
+      for (size_t k = 0; okx && k < ts.size(); ++k) okx = ts[k] >= 0 && ts[k] < nc;
+      if (!okx) { err = "inconsistent extended fall-off arrays in mechanism blob"; return false; }
+      L.n_xfo = (int)xr.size();
+      L.xfo_slot = B.addi(xs);
+      L.xfo_tb_ptr = B.addi(tp);
+      L.xfo_tb_sp = B.addi(ts.empty() ? none_i : ts);
+      L.xfo_bath_ptr = B.addi(bp);
+      L.xfo_bath_sp = B.addi(bs.empty() ? none_i : bs);
+      L.xfo_type = B.addi(ty.empty() ? none_i : ty);
+      L.xfo_par_ptr = B.addi(pp);
+    }
     L.cheb_slot = B.addi(cheb_slot);
     L.cheb_rxn = B.addi(cheb_rxn.empty() ? none_i : cheb_rxn);
     L.cheb_nm = B.addi(cheb_nm);

@@ -41,7 +41,7 @@ constexpr int kRT = 128;       // threads per block of the RHS kernel (one cell 
 constexpr int kWA = 4;         // warps per block of the advance kernel (one cell each)
 constexpr int kAT = 128;       // threads per block of the init kernel
 constexpr int kCT = 256;       // threads per block of the compaction kernel
-constexpr int kRefineR = 2;    // refinement sweeps of a solve with FP32 factors
+constexpr int kRefineR = 1;    // refinement sweeps of a solve with FP32 factors
 constexpr int kBins = 6;       // solver-path bins of the compaction
 
 enum Phase : int {
@@ -199,6 +199,10 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
       const int cs = M.I(L.cheb_slot)[j];
       if (cs >= 0) kArr = cheb_k(M, L, cs, T, Pk);
     }
+    if (L.n_xplog > 0) {  // extended PLOG (KineticsMap_CHEMKIN.hpp:1662-1670)
+      const int xs = M.I(L.xplog_slot)[j];
+      if (xs >= 0) kArr = xplog_k(M, L, xs, T, logT, Pk, cTotSum, [&](int k) { return SC_(C, k); });
+    }
     double kMod = kArr;
     const int tb = tbs[j];
     if (tb >= 0) {
@@ -254,6 +258,13 @@ __device__ __noinline__ double rhs_cell(const MechLayout* __restrict__ Lp, const
       // CABR (KineticsMap_CHEMKIN.hpp:1613-1660): k0 (1 / (1 + Pr)) F; fall-off: k_inf (Pr / (1 + Pr)) F
       if (cabr) kMod *= (1. / (1. + Pr)) * wF;
       else kMod *= kInf * (Pr / (1. + Pr)) * wF / kArr;
+    }
+    if (L.n_xfo > 0) {    // extended fall-off (KineticsMap_CHEMKIN.hpp:1672-1681)
+      const int xs = M.I(L.xfo_slot)[j];
+      if (xs >= 0) {
+        kArr = xfo_k(M, L, xs, T, cTotSum, [&](int k) { return SC_(C, k); });
+        kMod = kArr;
+      }
     }
     double fwd = 1.;
     for (int q = op[j]; q < op[j + 1]; ++q) fwd *= conc_factor_r(onu[q], SC_(C, osp[q]));
@@ -426,6 +437,10 @@ __device__ __noinline__ void analytic_jacobian_species(const MechLayout* __restr
       const int cs = M.I(L.cheb_slot)[j];
       if (cs >= 0) kArr = cheb_k(M, L, cs, T, P0);
     }
+    if (L.n_xplog > 0) {
+      const int xs = M.I(L.xplog_slot)[j];
+      if (xs >= 0) kArr = xplog_k(M, L, xs, T, logT, P0, cTotSum, [&](int k) { return SC_(C, k); });
+    }
     double kMod = kArr;
     double dkdM = 0.;          // d kMod / d M
     int mkind = 0;             // 0: no M; 1: third body (efficiency list tb); 2: fall-off mixture; 3: fall-off single bath
@@ -502,6 +517,13 @@ __device__ __noinline__ void analytic_jacobian_species(const MechLayout* __restr
       }
     }
     // forward product and its partials (orders lambda: FORD or the coefficients)
+    if (L.n_xfo > 0) {    // extended fall-off (KineticsMap_CHEMKIN.hpp:1672-1681)
+      const int xs = M.I(L.xfo_slot)[j];
+      if (xs >= 0) {
+        kArr = xfo_k(M, L, xs, T, cTotSum, [&](int k) { return SC_(C, k); });
+        kMod = kArr;
+      }
+    }
     double fwd = 1.;
     for (int q = op[j]; q < op[j + 1]; ++q) fwd *= conc_factor_r(onu[q], SC_(C, osp[q]));
     for (int q = op[j]; q < op[j + 1]; ++q) {
@@ -1153,6 +1175,10 @@ __device__ __noinline__ void steady_sparse_diagonal(const MechLayout* __restrict
       const int cs = M.I(L.cheb_slot)[j];
       if (cs >= 0) kArr = cheb_k(M, L, cs, T, P0);
     }
+    if (L.n_xplog > 0) {
+      const int xs = M.I(L.xplog_slot)[j];
+      if (xs >= 0) kArr = xplog_k(M, L, xs, T, logT, P0, cTs, [&](int k) { return SC_(C, k); });
+    }
     double kMod = kArr, Mtb = 0.;
     const int tb = tbs[j];
     if (tb >= 0) {
@@ -1206,6 +1232,13 @@ __device__ __noinline__ void steady_sparse_diagonal(const MechLayout* __restrict
       } else {
         Gcorr = falloff_corr(M, L, fo, kArr, Mc, T, logT, uT);
         kMod *= Gcorr;
+      }
+    }
+    if (L.n_xfo > 0) {    // extended fall-off (KineticsMap_CHEMKIN.hpp:1672-1681)
+      const int xs = M.I(L.xfo_slot)[j];
+      if (xs >= 0) {
+        kArr = xfo_k(M, L, xs, T, cTs, [&](int k) { return SC_(C, k); });
+        kMod = kArr;
       }
     }
     double fwd = 1.;
@@ -2193,9 +2226,11 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
   for (long round = 0; round < max_rounds; round += kBatch) {
     for (int r = 0; r < kBatch; ++r) {
       kt->begin(KT_RHS, stream);
-      // the analytic Jacobian is for the constant-pressure reactor; constant volume keeps the differences
+      // the analytic Jacobian is for the constant-pressure reactor without the concentration-dependent
+      // extended PLOG / fall-off constants; the other cases keep the differences
       rounds_rhs_kernel<<<P.g_rhs, kRT, P.rhs_smem, stream>>>(L, mech_gmem, o.energy, a.p, o.y_max_T, B, par,
-                                                              (o.jacobian != 0 && !a.rho) ? 1 : 0, err);
+                                                              (o.jacobian != 0 && !a.rho && L.n_xplog == 0 && L.n_xfo == 0) ? 1 : 0,
+                                                              err);
       kt->end(stream);
       const dim3 ga(P.g_adv), ta(kWA * 32);
       kt->begin(KT_ADVANCE, stream);

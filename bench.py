@@ -138,7 +138,8 @@ def tuning_report(ctx, lsg):
         return None
     tile, width, rates = t
     names = {lsg.LSG_TILE_LANE: f"round scheme, {width} lanes per cell", lsg.LSG_TILE_WARP: "plain warp kernel",
-             lsg.LSG_TILE_PERSISTENT: "persistent lane kernel"}
+             lsg.LSG_TILE_PERSISTENT: "persistent lane kernel",
+             lsg.LSG_TILE_GROUP: f"fused lane-group kernel, {width} blocks per SM"}
     return {"chosen": names.get(tile, str(tile)), "sample_cells_per_s": {k: round(v) for k, v in rates.items() if v}}
 
 
@@ -168,7 +169,7 @@ def parse():
     ap.add_argument("--cells", type=int, default=NCELLS)
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="cells of the CPU baseline sample (0: sized for about 10 s of CPU work)")
-    ap.add_argument("--tile", choices=("auto", "lane", "persistent"), default="auto",
+    ap.add_argument("--tile", choices=("auto", "lane", "persistent", "group"), default="auto",
                     help="batched form: autotuned (the first warm-up step times the candidate forms), round "
                          "scheme (lane) or persistent lane kernel")
     ap.add_argument("--factors", choices=("fp32", "fp64"), default="fp32",
@@ -374,7 +375,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     data, species, arrays, Y, T = workload(args.cells, 2 + 1000 * rank)
     n, nc = Y.shape
     m = lsg.Mechanism(data, device=local_rank)
-    tile = {"lane": lsg.LSG_TILE_LANE, "persistent": lsg.LSG_TILE_PERSISTENT, "auto": lsg.LSG_TILE_AUTO}[args.tile]
+    tile = {"lane": lsg.LSG_TILE_LANE, "persistent": lsg.LSG_TILE_PERSISTENT, "auto": lsg.LSG_TILE_AUTO,
+            "group": lsg.LSG_TILE_GROUP}[args.tile]
     prec = lsg.LSG_PRECISION_MIXED if args.factors == "fp32" else lsg.LSG_PRECISION_FP64
     ctx = lsg.ReactionStep(m, tile=tile, precision=prec, kernel_timing=1, autotune=int(args.tile == "auto"))
     plain = lsg.ReactionStep(m, tile=lsg.LSG_TILE_WARP, precision=lsg.LSG_PRECISION_FP64, kernel_timing=1)

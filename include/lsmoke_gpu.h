@@ -52,6 +52,8 @@ extern "C" {
 #define LSG_TILE_LANE 2        /* one thread per cell, rounds of RHS / solver / factor kernels over the live cells */
 #define LSG_TILE_PERSISTENT 3  /* one thread per cell, one persistent kernel + device work queue */
 #define LSG_TILE_BLOCK 4       /* one thread block per cell (any size up to 511 species) */
+#define LSG_TILE_GROUP 5       /* one lane group (16 or 32 lanes) per cell from start to finish, the RHS evaluated
+                                  by the group inside the solver kernel, persistent grid (up to 31 species) */
 /* Mechanisms of 32 to 511 species always run one thread block per cell (the
  * tile is ignored).  The block form factorises in FP64 with LSG_PRECISION_FP64;
  * with LSG_PRECISION_MIXED and 32 to 127 species it inverts G = I - h r0 J on
@@ -200,18 +202,20 @@ long long lsg_ctx_launches(const lsg_ctx* ctx);
  * stream when lsg_options.kernel_timing is set (diagnostics; no counterpart in
  * the reference).  Kinds: 0 RHS, 1 solver advance, 2 compaction, 3 round
  * initialisation (lane-per-cell form), 4 plain warp kernel, 5 persistent lane
- * kernel, 6 block-per-cell kernel (large mechanisms).  ms[k] total milliseconds, launches[k] timed launches; reset != 0
+ * kernel, 6 block-per-cell kernel (large mechanisms), 7 fused lane-group
+ * kernel.  ms[k] total milliseconds, launches[k] timed launches; reset != 0
  * clears the totals after reading.  Waits for the last timed kernel. */
-#define LSG_NKERNEL_KINDS 7
+#define LSG_NKERNEL_KINDS 8
 int lsg_ctx_kernel_times(lsg_ctx* ctx, double* ms, long long* launches, int nkinds, int reset);
 
 /* Result of the autotuner (lsg_options.autotune; no counterpart in the
- * reference): the chosen tile and lane-group width (16 or 32 lanes per cell in
- * the round scheme, 0 otherwise) and the measured cells/s of the candidates, in
- * the order round scheme 16 lanes, round scheme 32 lanes, plain warp kernel,
- * persistent lane kernel (0 for a candidate not tried).  Returns
- * LSG_ERR_ARG when no tuning has run yet. */
-#define LSG_NTUNE_CANDIDATES 4
+ * reference): the chosen tile and its variant (lanes per cell, 16 or 32, for
+ * the round scheme; blocks per SM, 4 or 2, for the fused lane-group kernel; 0
+ * otherwise) and the measured cells/s of the candidates, in the order round
+ * scheme 16 lanes, round scheme 32 lanes, plain warp kernel, persistent lane
+ * kernel, fused lane-group kernel at 4 and at 2 blocks per SM (0 for a
+ * candidate not tried).  Returns LSG_ERR_ARG when no tuning has run yet. */
+#define LSG_NTUNE_CANDIDATES 6
 int lsg_ctx_tuning(const lsg_ctx* ctx, int* tile, int* width, double* rates);
 
 /* Waits for the device, then reads and clears the error flags kernels raised

@@ -56,6 +56,7 @@ struct lsg_ctx {
   long bws_blocks = 0;
   long tc_blocks = 0;           // blocks of the tensor-core (mixed-precision) block kernel
   int* bqueue = nullptr;
+  int* gqueue = nullptr;        // cell queue of the fused lane-group form
   KernelTimer timer;          // per-kernel device time (lsg_options.kernel_timing)
   // autotuner (lsg_options.autotune)
   bool tuned = false;
@@ -149,7 +150,7 @@ int validate_options(const lsg_options* o) {
   if (o->full_pivoting != 0) return LSG_ERR_UNSUPPORTED;
   if (o->precision != LSG_PRECISION_FP64 && o->precision != LSG_PRECISION_MIXED) return LSG_ERR_ARG;
   if (o->maximum_order < 1 || o->maximum_order > 5) return LSG_ERR_ARG;
-  if (o->tile < LSG_TILE_AUTO || o->tile > LSG_TILE_BLOCK) return LSG_ERR_ARG;
+  if (o->tile < LSG_TILE_AUTO || o->tile > LSG_TILE_GROUP) return LSG_ERR_ARG;
   if (o->tile == LSG_TILE_WARP && o->precision != LSG_PRECISION_FP64) return LSG_ERR_UNSUPPORTED;
   if (o->jacobian != LSG_JACOBIAN_FD && o->jacobian != LSG_JACOBIAN_ANALYTIC) return LSG_ERR_ARG;
   return LSG_OK;
@@ -370,7 +371,8 @@ int autotune(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
   t.counters = nullptr;
   struct Cand { int tile, w; };
   const Cand cands[LSG_NTUNE_CANDIDATES] = {
-      {LSG_TILE_LANE, 16}, {LSG_TILE_LANE, 32}, {LSG_TILE_WARP, 0}, {LSG_TILE_PERSISTENT, 0}};
+      {LSG_TILE_LANE, 16}, {LSG_TILE_LANE, 32}, {LSG_TILE_WARP, 0}, {LSG_TILE_PERSISTENT, 0},
+      {LSG_TILE_GROUP, 4}, {LSG_TILE_GROUP, 2}};
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return LSG_ERR_CUDA;
   double best = -1.;
@@ -382,7 +384,7 @@ int autotune(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
     const Cand cd = cands[k];
     if (cd.tile == LSG_TILE_LANE && cd.w == 16 && n > 16) continue;
     if (cd.tile == LSG_TILE_WARP && c->opt.precision != LSG_PRECISION_FP64) continue;
-    c->tuned = cd.tile == LSG_TILE_LANE;
+    c->tuned = cd.tile == LSG_TILE_LANE || cd.tile == LSG_TILE_GROUP;
     c->tuned_w = cd.w;
     float ms = 0.f;
     for (int rep = 0; rep < 2; ++rep) {   // a 1024-cell run pays the one-time set-up, then the timed run
@@ -440,6 +442,24 @@ int launch_tile(lsg_ctx* c, const StepArgs& a, cudaStream_t s, int tile) {
                                         max_rounds, c->d_err, s, &c->launches, &c->timer);
     if (e == cudaErrorLaunchTimeout) return LSG_ERR_DEVICE;
     return e == cudaSuccess ? LSG_OK : LSG_ERR_CUDA;
+  }
+  if (tile == LSG_TILE_GROUP) {
+    if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
+    if (!c->gqueue && cudaMalloc(&c->gqueue, sizeof(int)) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+    if (!sm_count(c)) return LSG_ERR_CUDA;
+    if (c->timer.used >= KernelTimer::kPairs) {
+      cudaStreamSynchronize(s);
+      c->timer.collect();
+    }
+    const int mb = (c->tuned && c->tuned_w == 2) ? 2 : 4;   // the autotuner's occupancy variant, else 4 blocks/SM
+    c->timer.begin(KT_GROUP, s);
+    const cudaError_t e = launch_group(L, c->mech->d_buf, so, a, c->opt.precision == LSG_PRECISION_FP64,
+                                       mb == 2 ? 2 : 4, c->gqueue, c->d_err, c->sm_count, s);
+    c->timer.end(s);
+    if (e == cudaErrorInvalidValue) { cudaGetLastError(); return LSG_ERR_UNSUPPORTED; }
+    if (e != cudaSuccess) return LSG_ERR_CUDA;
+    c->launches += 1;
+    return LSG_OK;
   }
   if (tile == LSG_TILE_WARP) {
     if (L.nc + 1 > 32) return LSG_ERR_UNSUPPORTED;
@@ -635,6 +655,7 @@ int lsg_ctx_destroy(lsg_ctx* c) {
   if (c->seq_ev[0]) cudaEventDestroy(c->seq_ev[0]);
   if (c->seq_ev[1]) cudaEventDestroy(c->seq_ev[1]);
   cudaFree(c->bqueue);
+  cudaFree(c->gqueue);
   cudaFree(c->tune_buf);
   cudaFree(c->frs);
   if (c->nact_host) cudaFreeHost(c->nact_host);
@@ -823,6 +844,11 @@ int lsg_reaction_step_sequence_device(lsg_ctx* c, int nsteps, int ncells, int ns
     int r = LSG_OK;
     if (tile == LSG_TILE_BLOCK || L.nc + 1 > 32) r = prepare_large(c);
     else if (tile == LSG_TILE_PERSISTENT) r = ensure_batched(c, c->opt.precision == LSG_PRECISION_FP64);
+    else if (tile == LSG_TILE_GROUP && !c->gqueue && cudaMalloc(&c->gqueue, sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      r = LSG_ERR_NOMEM;
+    }
+    if (r == LSG_OK && !sm_count(c)) r = LSG_ERR_CUDA;
     if (r != LSG_OK) return r;
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return LSG_ERR_CUDA;
     const bool timing = c->timer.on;

@@ -84,7 +84,7 @@ cudaError_t launch_batched_noalloc(const MechLayout& L, const unsigned char* mec
 // Optional device timing of each kernel kind with CUDA events recorded on the
 // launching stream (lsg_options.kernel_timing).  Pairs are collected after the
 // stream has been synchronised.
-enum { KT_RHS = 0, KT_ADVANCE, KT_COMPACT, KT_INIT, KT_PLAIN, KT_PERSISTENT, KT_BLOCK, KT_NKINDS };
+enum { KT_RHS = 0, KT_ADVANCE, KT_COMPACT, KT_INIT, KT_PLAIN, KT_PERSISTENT, KT_BLOCK, KT_GROUP, KT_NKINDS };
 struct KernelTimer {
   static constexpr int kPairs = 64;
   bool on = false;
@@ -134,6 +134,11 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
                           KernelTimer* timer);
 cudaError_t launch_rhs_warp(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y,
                             double* dy, long ld, double p, int energy, double* qr, int* err, cudaStream_t stream);
+
+// Fused lane-group form (lsg_rounds.cu): one lane group per cell from start to finish, RHS in-kernel;
+// min_blocks 4 or 2 blocks per SM (128 or 255 registers a thread); queue: one int
+cudaError_t launch_group(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o, const StepArgs& a,
+                         bool lu64, int min_blocks, int* queue, int* err, int sm_count, cudaStream_t stream);
 
 // Jacobians with analytic species columns (lsg_rounds.cu), up to 31 species; J [ncells][n][n] row-major
 cudaError_t launch_jacobian(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y, long ld,

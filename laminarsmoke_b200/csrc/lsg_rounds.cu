@@ -702,7 +702,7 @@ __device__ __noinline__ void gj_inverse(const double* Js, LUT* As, LUT* Ks, LUT*
     for (int j = 0; j < n; ++j) {
       const LUT g = As[lane * la + n + j];
       Xs[lane * ld + j] = g;
-      Ig[lane * n + j] = g;
+      if (Ig) Ig[lane * n + j] = g;
     }
   __syncwarp(gm);
 }
@@ -1970,6 +1970,832 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Fused lane-group form (LSG_TILE_GROUP): one lane group (16 lanes for up to
+// 16 ODE components, else 32) integrates one cell from start to finish.  The
+// solver state lives in registers (lane k holds component k of every vector)
+// and the group's Jacobian, G^-1 and Gauss-Jordan work arrays in shared
+// memory for the cell's whole integration; every RHS the solver asks for is
+// evaluated at once by the group (rhs_group), so nothing round-trips through
+// HBM between requests.  Cells come from a device queue; the grid is
+// persistent.  The solver is the round scheme's state machine, unchanged.
+// ---------------------------------------------------------------------------
+constexpr int kGW = 4;   // warps per block of the group kernel
+
+// Group-cooperative RHS of the constant-pressure (rho0 == 0) or constant-volume
+// reactor (BatchReactorHomogeneousConstantPressure.H:175-223,
+// BatchReactorHomogeneousConstantVolume.H:148-199): lane i < NC owns species
+// i, lane NC the temperature; reactions are spread over the lanes (C, G, NET:
+// the group's shared arrays).  Returns this lane's f; sets QR.
+template <int W>
+__device__ __noinline__ double rhs_group(const MechLayout* __restrict__ Lp, const double* __restrict__ Md,
+                                         const int* __restrict__ Mi, double* __restrict__ C, double* __restrict__ G,
+                                         double* __restrict__ NET, double yl, double P0, int energy, double rho0,
+                                         int lane, unsigned gm, double* QRout) {
+  const MechLayout& L = *Lp;
+  const MechView M{Md, Mi};
+  const int NC = L.nc, NR = L.nr;
+  const double* MW = M.D(L.mw);
+  const bool sp = lane < NC;
+  const double mwl = sp ? MW[lane] : 1.;
+  const double T = __shfl_sync(gm, yl, NC, W);
+  const double MWmix = 1. / wsum_g<W>(gm, sp ? yl / mwl : 0.);
+  const bool cv = rho0 > 0.;
+  const double cTot = cv ? rho0 / MWmix : P0 / kRgas / T;
+  const double rho = cv ? rho0 : cTot * MWmix;
+  const double Pk = cv ? cTot * kRgas * T : P0;
+  const double* TM = M.D(L.t_mid);
+  const double T2 = T * T, T3 = T2 * T, T4 = T3 * T, uT = 1. / T;
+  const double logT = log(T);
+  const double lP = log(101325. / kRgas / T);
+  double xl = 0., cl = 0., hrt = 0.;
+  if (sp) {
+    xl = MWmix * yl;
+    xl = xl / mwl;
+    cl = cTot * xl;
+    C[lane] = cl;
+    const bool hiT = T > TM[lane];
+    const double* A = hiT ? M.D(L.dh_ht) + 6 * lane : M.D(L.dh_lt) + 6 * lane;
+    hrt = A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4] + uT * A[5];
+    const double* B = hiT ? M.D(L.ds_ht) + 6 * lane : M.D(L.ds_lt) + 6 * lane;
+    G[lane] = hrt - (B[0] * logT + T * B[1] + T2 * B[2] + T3 * B[3] + T4 * B[4] + B[5]);
+  }
+  const double cTotSum = wsum_g<W>(gm, cl);
+  __syncwarp(gm);
+  const double* lnA = M.D(L.lnA);
+  const double* beta = M.D(L.beta);
+  const double* eor = M.D(L.eor);
+  const double* dnu = M.D(L.dnu);
+  const int* sgn = M.I(L.a_sign);
+  const int* rk = M.I(L.rev_kind);
+  const int* rs = M.I(L.rev_slot);
+  const int* tbs = M.I(L.tb_slot);
+  const int* fos = M.I(L.fo_slot);
+  const int* rp = M.I(L.reac_ptr);
+  const int* rsp = M.I(L.reac_sp);
+  const double* rnu = M.D(L.reac_nu);
+  const int* op = M.I(L.ford_ptr);
+  const int* osp = M.I(L.ford_sp);
+  const double* onu = M.D(L.ford_val);
+  const int* pp = M.I(L.prod_ptr);
+  const int* psp = M.I(L.prod_sp);
+  const double* pnu = M.D(L.prod_nu);
+  for (int j = lane; j < NR; j += W) {
+    double kArr = exp(lnA[j] + beta[j] * logT - eor[j] * uT);
+    if (sgn[j] < 0) kArr *= -1.;
+    if (L.n_plog > 0) {
+      const int ps = M.I(L.plog_slot)[j];
+      if (ps >= 0) kArr = plog_k(M, L, ps, T, logT, Pk);
+    }
+    if (L.n_cheb > 0) {
+      const int cs = M.I(L.cheb_slot)[j];
+      if (cs >= 0) kArr = cheb_k(M, L, cs, T, Pk);
+    }
+    if (L.n_xplog > 0) {
+      const int xs = M.I(L.xplog_slot)[j];
+      if (xs >= 0) kArr = xplog_k(M, L, xs, T, logT, Pk, cTotSum, [&](int k) { return C[k]; });
+    }
+    double kMod = kArr;
+    const int tb = tbs[j];
+    if (tb >= 0) {
+      double Mc = cTotSum;
+      const int* tp = M.I(L.tb_ptr);
+      const int* ts = M.I(L.tb_sp);
+      const double* te = M.D(L.tb_eff);
+      for (int q = tp[tb]; q < tp[tb + 1]; ++q) Mc += C[ts[q]] * te[q];
+      kMod *= Mc;
+    }
+    const int fo = fos[j];
+    if (fo >= 0) {
+      const double kInf = exp(M.D(L.fo_lnA)[fo] + M.D(L.fo_beta)[fo] * logT - M.D(L.fo_eor)[fo] * uT);
+      const double a = M.D(L.fo_a)[fo], b = M.D(L.fo_b)[fo], c = M.D(L.fo_c)[fo], d = M.D(L.fo_d)[fo];
+      const int ty = M.I(L.fo_type)[fo];
+      double Mc;
+      const int single = M.I(L.fo_single)[fo];
+      if (single < 0) {
+        Mc = cTotSum;
+        const int* fp = M.I(L.fo_ptr);
+        const int* fs = M.I(L.fo_sp);
+        const double* fe = M.D(L.fo_eff);
+        for (int q = fp[fo]; q < fp[fo + 1]; ++q) Mc += C[fs[q]] * fe[q];
+      } else {
+        Mc = C[single] + 1.e-16;
+      }
+      const double Pr = kArr * Mc / kInf;
+      const bool cabr = M.I(L.fo_cabr)[fo] != 0;
+      double wF = 1.;
+      if (ty == 1) {
+        double v = (1. - a) * exp(-T / b) + a * exp(-T / c);
+        if (d != 0.) v += exp(-d / T);
+        const double lF = (v < 1.e-300) ? -300. : log10(v);
+        double qq;
+        if (Pr > 1.e-32 || cabr) {
+          const double nTroe = 0.75 - 1.27 * lF;
+          const double cTroe = -0.4 - 0.67 * lF;
+          const double sTroe = log10(Pr) + cTroe;
+          qq = sTroe / (nTroe - 0.14 * sTroe);
+        } else {
+          qq = 1. / 0.14;
+        }
+        wF = exp10(lF / (1. + qq * qq));
+      } else if (ty == 2) {
+        const double lF = a * exp(-b / T) + exp(-T / c);
+        const double l10 = log10(Pr);
+        wF = pow(lF, 1. / (1. + l10 * l10)) * d;
+        const double e = M.D(L.fo_e)[fo];
+        if (e != 0.) wF *= pow(T, e);
+      }
+      if (cabr) kMod *= (1. / (1. + Pr)) * wF;
+      else kMod *= kInf * (Pr / (1. + Pr)) * wF / kArr;
+    }
+    if (L.n_xfo > 0) {
+      const int xs = M.I(L.xfo_slot)[j];
+      if (xs >= 0) {
+        kArr = xfo_k(M, L, xs, T, cTotSum, [&](int k) { return C[k]; });
+        kMod = kArr;
+      }
+    }
+    double fwd = 1.;
+    for (int q = op[j]; q < op[j + 1]; ++q) fwd *= conc_factor_r(onu[q], C[osp[q]]);
+    double net = fwd;
+    const int kind = rk[j];
+    if (kind != 0) {
+      double rv = 1.;
+      for (int q = pp[j]; q < pp[j + 1]; ++q) rv *= conc_factor_r(pnu[q], C[psp[q]]);
+      double rf;
+      if (kind == 1) {
+        double dg = 0.;
+        for (int q = pp[j]; q < pp[j + 1]; ++q) dg += contrib_r(pnu[q], G[psp[q]]);
+        for (int q = rp[j]; q < rp[j + 1]; ++q) dg -= contrib_r(rnu[q], G[rsp[q]]);
+        rf = exp(dg - lP * dnu[j]);
+      } else {
+        const int sr = rs[j];
+        rf = exp(M.D(L.rev_lnA)[sr] + M.D(L.rev_beta)[sr] * logT - M.D(L.rev_eor)[sr] * uT) / kArr;
+      }
+      rv *= rf;
+      net -= rv;
+    }
+    NET[j] = net * kMod;
+  }
+  __syncwarp(gm);
+  double Rl = 0.;
+  if (sp) {   // StoichiometricMap::FormationRatesFromReactionRates (:656-729), gathered per species
+    const int* fp = M.I(L.fr_ptr);
+    const int* fr = M.I(L.fr_rxn);
+    const double* fc = M.D(L.fr_coef);
+    for (int q = fp[lane]; q < fp[lane + 1]; ++q) {
+      const double cf = fc[q];
+      Rl += contrib_r(cf < 0. ? -cf : cf, NET[fr[q]]) * (cf < 0. ? -1. : 1.);
+    }
+  }
+  double out = sp ? mwl * Rl / rho : 0.;
+  double QR = 0.;
+  if (energy) {
+    double cpl = 0.;
+    if (sp) {
+      const bool hiT = T > TM[lane];
+      const double* A = hiT ? M.D(L.cp_ht) + 5 * lane : M.D(L.cp_lt) + 5 * lane;
+      cpl = (A[0] + T * A[1] + T2 * A[2] + T3 * A[3] + T4 * A[4]) * (cl / cTot);
+    }
+    const double cpm = kRgas * wsum_g<W>(gm, cpl);
+    const double dsum = wsum_g<W>(gm, sp ? Rl * hrt : 0.);
+    QR = -dsum * kRgas * T;
+    double dT;
+    if (cv) {
+      const double CvMixMass = (cpm - kRgas) / MWmix;
+      const double sumR = wsum_g<W>(gm, sp ? Rl : 0.);
+      dT = (QR + kRgas * T * sumR) / (rho0 * CvMixMass);
+    } else {
+      dT = QR / (rho * (cpm / MWmix));
+    }
+    if (lane == NC) out = dT;
+  }
+  __syncwarp(gm);   // C, G, NET may be rewritten by the next call
+  *QRout = QR;
+  return out;
+}
+
+template <typename LUT, int W, int MB>
+__global__ void __launch_bounds__(kGW * 32, MB) group_kernel(MechLayout Lp, const unsigned char* __restrict__ mech_gmem,
+                                                             StepOptions o, StepArgs a, int* queue, int* err) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ MechLayout sL;
+  if (threadIdx.x == 0) sL = Lp;
+  if (!stage_bulk(gsm, mech_gmem, Lp.bytes, &mbar, err)) return;
+  const double* Md = (const double*)gsm;
+  const int* Mi = (const int*)(gsm + (size_t)Lp.n_double * sizeof(double));
+  constexpr int CPW = 32 / W;
+  constexpr int GB = kGW * CPW;   // lane groups per block
+  const int NC = Lp.nc, NR = Lp.nr;
+  const int n = NC + 1, ld = n + 1, la = 2 * n + 1;
+  const int wl = threadIdx.x & 31;
+  const int lane = wl & (W - 1);
+  const int w = (threadIdx.x >> 5) * CPW + wl / W;
+  const unsigned gm = W == 32 ? kFull : (0xffffu << (wl & 16));
+  // per group: C[NC], G[NC], NET[NR], J[n][ld] (double); G^-1 X[n][ld], A[n][2n+1], K[2n] (LUT)
+  double* gbase = (double*)(gsm + ((Lp.bytes + 15u) & ~15u));
+  const size_t gd = (size_t)2 * NC + NR + (size_t)n * ld;
+  double* C = gbase + (size_t)w * gd;
+  double* Gs = C + NC;
+  double* NET = Gs + NC;
+  double* Js = NET + NR;
+  LUT* lbase = (LUT*)(gbase + (size_t)GB * gd);
+  const size_t gl = (size_t)n * ld + (size_t)n * la + 2 * n;
+  LUT* Xs = lbase + (size_t)w * gl;
+  LUT* As = Xs + (size_t)n * ld;
+  LUT* Ks = As + (size_t)n * la;
+  const bool al = lane < n;
+  const double lo = lane < NC ? 0. : o.y_min_T, hi = lane < NC ? 1. : o.y_max_T;
+  const long max_requests = 4L * (long)o.max_steps * (NC + 10) + 64;
+  for (;;) {
+    int cell = 0;
+    if (lane == 0) cell = atomicAdd(queue, 1);
+    cell = __shfl_sync(gm, cell, 0, W);
+    if (cell >= a.ncells) break;
+    const double rho0 = a.rho ? a.rho[cell] : 0.;
+    const double Tc = a.T[cell];
+    if (!(Tc > o.tmin_chem)) {   // chemistry_DI.H:92-96: the cell is skipped, its Y renormalised
+      const double yv = lane < NC ? a.Y[(long)lane * a.ld + cell] : 0.;
+      const double sy = wsum_g<W>(gm, yv);
+      if (lane < NC) a.Y[(long)lane * a.ld + cell] = yv / sy;
+      if (lane == 0) {
+        if (a.status) a.status[cell] = 0;
+        if (a.nsteps) a.nsteps[cell] = 0;
+      }
+      if (a.counters && lane < NCNT) a.counters[(long)cell * NCNT + lane] = 0;
+      continue;
+    }
+    // gather, clip and renormalise (chemistry_DI.H:97-129); solver reset (MultiValueSolver.hpp:367-420)
+    double va = 0.;
+    if (lane < NC) {
+      va = a.Y[(long)lane * a.ld + cell];
+      if (va < 0.) va = 0.;
+    }
+    const double sy = wsum_g<W>(gm, va);
+    if (lane < NC) va /= sy;
+    if (lane == NC) va = Tc;
+    const double t0 = a.t0;
+    double t = t0, tOut = t0, tInMeshPoint = t0, tStabilize = t0, h = 0., hNextStep = 0., hNordsieck = 0.;
+    double hScale = 0., hScaleMax = 1000., alfa2_4 = o.alfa2_4, alfa2_5 = o.alfa2_5, oldCC = 0., hf = 0., hJ = 0.;
+    double pendHScale = 0., hr0f = 0., QR = 0.;
+    int status = 1;
+    unsigned p = 1, iterOrder = 0, orderInNextStep = 1;
+    unsigned maxIterationsJacobian = 20u + 5u * (unsigned)(n - 3);
+    if (maxIterationsJacobian > 50u && n < 80) maxIterationsJacobian = 50u;
+    int odeHStatus = 1, odeOrderStatus = 1, factorized = 0, jacobianChange = 1, convOK = 1;
+    unsigned numberOfSteps = 0, iterConvergence = 0, iterConvergenceRate = 0, iterConvergenceFailure = 0;
+    unsigned iterErrorFailure = 0, nConvFailOrderMax = 0, stepOfLastJacobian = 0, iterConstSteps = 0;
+    unsigned iterMinimumOrder = 0;
+    bool fixedOrderMin = false;
+    unsigned newtonK = 0;
+    int jcol = 0;
+    unsigned maximum_order = (unsigned)o.maximum_order;
+    int cstep = 0, csolve = 0, cjac = 0, cfact = 0, cerr = 0, cconv = 0;
+    long crhs = 0, cjrhs = 0;
+    double z[8], v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) { z[i] = 0.; v[i] = 0.; }
+    double b = 0., f = 0., f0 = 0., vb = 0., eps = 0.;
+    double x = 0.;
+    bool dz = false, dv = false;
+    (void)dz; (void)dv; (void)hJ; (void)jcol;
+    enum : int { H_DEC = 0, H_CONST = 1, H_INC = 2 };
+    enum : int { O_DEC = 0, O_CONST = 1, O_INC = 2 };
+    auto alfa2 = [&](unsigned k) { return k == 4 ? alfa2_4 : (k == 5 ? alfa2_5 : .8); };
+    auto wrms = [&](double xv) { return wrms_ol<W>(xv, eps, al, n, gm); };
+    auto clamp = [&](double y) {
+      if (al) {
+        if (y < lo) y = lo;
+        if (y > hi) y = hi;
+      }
+      return y;
+    };
+    auto load_j = [&]() {};   // the Jacobian stays in the group's shared memory
+    auto solve = [&](double rhs) {
+      const bool fp32 = sizeof(LUT) == sizeof(float);
+      ++csolve;
+      return solve_ol<LUT, W>(Xs, Js, rhs, hr0f, n, lane, gm, fp32 ? kRefineR : 0);
+    };
+    auto factorize = [&]() {
+      gj_inverse<LUT, W>(Js, As, Ks, Xs, (LUT*)nullptr, hr0f, n, lane, gm);
+      ++cfact;
+    };
+    auto fail_keep_z = [&](int st) {
+      status = st;
+      va = z[0];
+    };
+    auto rhs = [&](double yv) {
+      ++crhs;
+      return rhs_group<W>(&sL, Md, Mi, C, Gs, NET, yv, a.p, o.energy, rho0, lane, gm, &QR);
+    };
+    int phase = PH_INIT;
+    f = rhs(va);
+    for (long req = 0; phase != PH_DONE; ++req) {
+      if (req > 0) {
+        // serve the request the solver ended on
+        if (req > max_requests) {   // the round scheme's round limit: status -1, last accepted state
+          status = -1;
+          va = z[0];
+          const double sv = wsum_g<W>(gm, lane < NC ? va : 0.);
+          if (lane < NC) a.Y[(long)lane * a.ld + cell] = va / sv;
+          if (o.energy && lane == NC) a.T[cell] = va;
+          if (lane == 0) {
+            if (a.Q) a.Q[cell] = QR;
+            if (a.status) a.status[cell] = status;
+            if (a.nsteps) a.nsteps[cell] = (int)numberOfSteps;
+          }
+          if (a.counters && lane == 0) {
+            long long* cc = a.counters + (long)cell * NCNT;
+            cc[CNT_STEPS] = cstep; cc[CNT_RHS] = crhs; cc[CNT_JAC] = cjac; cc[CNT_FACT] = cfact;
+            cc[CNT_SOLVE] = csolve; cc[CNT_ERRFAIL] = cerr; cc[CNT_CONVFAIL] = cconv; cc[CNT_JAC_RHS] = cjrhs;
+          }
+          break;
+        }
+        if (phase == PH_PRED) {
+          f0 = rhs(vb);
+        } else if (phase == PH_JAC) {
+          // KernelDense::NumericalJacobian, constrained branch (KernelDense.hpp:111-193): column j by the group
+          for (int j = 0; j < n; ++j) {
+            double hj = 0.;
+            if (lane == j) {
+              const double aa = fabs(vb), bb2 = fabs(1. / eps);
+              hj = sqrt(kMachEpsDouble) * (aa > bb2 ? aa : bb2);
+              hj = fmax(hj, hf / eps);
+              hj = fmax(hj, sqrt(kTinyFloat));
+              if (vb + hj > (j < n - 1 ? 1. : o.y_max_T)) hj = -hj;
+            }
+            hj = __shfl_sync(gm, hj, j, W);
+            const double fj = rhs_group<W>(&sL, Md, Mi, C, Gs, NET, lane == j ? vb + hj : vb, a.p, o.energy, rho0,
+                                           lane, gm, &QR);
+            if (al) Js[lane * ld + j] = (1. / hj) * (fj - f0);
+            if (j == n - 1) f = fj;
+          }
+          __syncwarp(gm);
+          cjrhs += n;
+        } else if (phase == PH_STAB_CONV || phase == PH_STAB_ERR) {
+          f = rhs(z[0]);
+        } else {   // PH_NEWTON, PH_FINAL
+          f = rhs(va);
+        }
+      }
+        enum : int { L_NONE, L_START_STEP, L_DRIVER_LOOP, L_JAC_COLUMN, L_AFTER_JAC, L_AFTER_FACT, L_NEWTON_TEST,
+                     L_CORR_DONE, L_FINISH };
+        int lab = L_NONE;
+        switch (phase) {
+          case PH_INIT: {
+            // MultiValueSolver::Solve, first call (:445-469)
+            const bool illegal = al && (va < lo || va > hi);
+            if (__any_sync(gm, illegal)) { status = -9; lab = L_FINISH; break; }
+            eps = al ? 1. / (o.atol + o.rtol * fabs(va)) : 0.;
+            double lo0, hi0;
+            if (t0 != 0.) { lo0 = 100. * kMachEpsDouble * fabs(t0); hi0 = fabs(t0); }
+            else { lo0 = kMachEpsDouble; hi0 = 1.e-4; }
+            double h0 = 0.5 / (wrms(f) + kMachEpsFloat);
+            if (h0 < lo0) h0 = lo0;
+            if (h0 > hi0) h0 = hi0;
+            const double dtc = a.dt ? a.dt[cell] : a.dt_scalar;
+            tOut = t0 + dtc;
+            h0 *= fabs(tOut - t0) / (tOut - t0);
+            z[0] = va;
+            z[1] = f * h0;
+            dz = true;
+            hNordsieck = h0; hNextStep = h0;
+            status = 2;
+            lab = L_START_STEP;
+            break;
+          }
+          case PH_PRED: {
+            // MethodGear::FindCorrection after f(vb) (:205-262)
+            if (numberOfSteps >= stepOfLastJacobian + maxIterationsJacobian) jacobianChange = 1;
+            if (jacobianChange) {
+              stepOfLastJacobian = numberOfSteps;
+              jacobianChange = 0;
+              hf = 1.e+3 * kMachEpsDouble * fabs(h) * wrms(f0) * double(n);
+              if (hf < 1.e-10) hf = 1.;
+              jcol = 0;
+              lab = L_JAC_COLUMN;
+              break;
+            }
+            lab = L_AFTER_JAC;
+            break;
+          }
+          case PH_JAC: {
+            // the RHS kernel has built every column of J
+            ++cjac;
+            factorized = 0;
+            lab = L_AFTER_JAC;
+            break;
+          }
+          case PH_NEWTON: {
+            x = solve(al ? f * h - v[1] - b : 0.);
+            b += x;
+            ++newtonK;
+            if (newtonK > 4u) { convOK = 0; iterConvergence = 4; lab = L_CORR_DONE; }
+            else lab = L_NEWTON_TEST;
+            break;
+          }
+          case PH_STAB_CONV: {
+            z[1] = f * h;
+            dz = true;
+            tStabilize = tInMeshPoint;
+            if (numberOfSteps > stepOfLastJacobian + 5u) jacobianChange = 1;
+            if (numberOfSteps != stepOfLastJacobian && iterConvergenceFailure == 50u) jacobianChange = 1;
+            hNextStep *= pendHScale;
+            lab = L_DRIVER_LOOP;
+            break;
+          }
+          case PH_STAB_ERR: {
+            z[1] = f * h;
+            dz = true;
+            tStabilize = tInMeshPoint;
+            odeHStatus = H_DEC;
+            hNextStep *= hScale;
+            lab = L_DRIVER_LOOP;
+            break;
+          }
+          default:   // PH_FINAL
+            lab = L_FINISH;
+            break;
+        }
+
+        // labels that need no RHS; a request or a finish is reached within a few hops
+        for (int hop = 0; lab != L_NONE; ++hop) {
+          if (hop >= 64) {
+            fail_keep_z(-10);
+            lab = L_FINISH;
+          }
+          switch (lab) {
+            case L_START_STEP: {
+              // MultiValueSolver::Solve loop (:532-560) + DriverStep prologue (:753-776)
+              if (numberOfSteps >= (unsigned)o.max_steps) { fail_keep_z(-1); lab = L_FINISH; break; }
+              eps = al ? 1. / (o.atol + o.rtol * fabs(z[0])) : 0.;
+              if (kMachEpsDouble * wrms(z[0]) > 1.) { fail_keep_z(-2); lab = L_FINISH; break; }
+              tInMeshPoint = t;
+              iterConvergenceFailure = 0; iterErrorFailure = 0; convOK = 1;
+              if (odeOrderStatus != O_CONST || odeHStatus != H_CONST) iterOrder = 0;
+              p = orderInNextStep;
+              odeOrderStatus = O_CONST;
+              hScaleMax = 2.;
+              if (numberOfSteps < 10) hScaleMax = 1000.;
+              else if (numberOfSteps > 10 && numberOfSteps < 20) hScaleMax = 10.;
+              lab = L_DRIVER_LOOP;
+              break;
+            }
+            case L_DRIVER_LOOP: {
+              // DriverStep while(1) body up to FindCorrection (:778-820, :1212-1266)
+              if (odeHStatus != H_CONST) {
+                hScale = hNextStep / hNordsieck;
+                double hr = 1.;
+    #pragma unroll
+                for (unsigned i = 1; i < 8; ++i) {
+                  if (i <= p) {
+                    hr *= hScale;
+                    z[i] *= hr;
+                  }
+                }
+                z[0] = clamp(z[0]);
+                dz = true;
+                iterOrder = 0;
+                odeHStatus = H_CONST;
+              }
+              h = hNextStep;
+              hNordsieck = hNextStep;
+              t = tInMeshPoint + h;
+              if (t == tInMeshPoint) {
+                fail_keep_z(-6);
+                t = tInMeshPoint;
+                lab = L_FINISH;
+                break;
+              }
+              {
+                // MultiValueStep prediction v = D z with min/max handling, then vb = CheckConstraints(v0)
+                double wv[8];
+    #pragma unroll
+                for (int i = 0; i < 8; ++i) wv[i] = (i <= (int)p) ? z[i] : 0.;
+    #pragma unroll
+                for (int i = 0; i < 7; ++i)
+    #pragma unroll
+                  for (int j = 6; j >= 0; --j)
+                    if (i < (int)p && j >= i && j <= (int)p - 1) wv[j] += wv[j + 1];
+                if (al) {
+                  if (wv[0] < lo && fabs(wv[0] - lo) * eps < double(n)) {
+                    wv[1] = lo - z[0];
+                    wv[0] = lo;
+    #pragma unroll
+                    for (int i = 2; i < 8; ++i) wv[i] = 0.;
+                  }
+                  if (wv[0] > hi && fabs(wv[0] - hi) * eps < double(n)) {
+                    wv[1] = hi - z[0];
+                    wv[0] = hi;
+    #pragma unroll
+                    for (int i = 2; i < 8; ++i) wv[i] = 0.;
+                  }
+                }
+    #pragma unroll
+                for (int i = 0; i < 8; ++i)
+                  if (i <= (int)p) v[i] = wv[i];
+                dv = true;
+                vb = clamp(wv[0]);
+              }
+              phase = PH_PRED;
+              lab = L_NONE;
+              break;
+            }
+            case L_JAC_COLUMN: {
+              // KernelDense::NumericalJacobian: the RHS kernel evaluates all n perturbed states next
+              phase = PH_JAC;
+              lab = L_NONE;
+              break;
+            }
+            case L_AFTER_JAC: {
+              if (factorized && iterOrder == 0) factorized = 0;
+              if (!factorized) {
+                hr0f = h * c_gear_r.r[0][p - 1];
+                factorize();
+                factorized = 1;
+              }
+              lab = L_AFTER_FACT;
+              break;
+            }
+            case L_AFTER_FACT: {
+              x = solve(al ? f0 * h - v[1] : 0.);
+              b = x;
+              newtonK = 1;
+              lab = L_NEWTON_TEST;
+              break;
+            }
+            case L_NEWTON_TEST: {
+              const double r0 = c_gear_r.r[0][p - 1];
+              const double cc = r0 * wrms(x);
+              if (cc < 1.) { convOK = 1; iterConvergence = newtonK; lab = L_CORR_DONE; break; }
+              if (newtonK > 1 && cc > 2. * oldCC) { convOK = 0; iterConvergence = newtonK; lab = L_CORR_DONE; break; }
+              oldCC = cc;
+              double vn = b * r0 + v[0];
+              if (al) {
+                if (vn < lo) { vn = lo; b = (lo - z[0]) / r0; }
+                if (vn > hi) { vn = hi; b = (hi - z[0]) / r0; }
+              }
+              va = vn;
+              phase = PH_NEWTON;
+              lab = L_NONE;
+              break;
+            }
+            case L_CORR_DONE: {
+              if (!convOK) {
+                // DriverStep convergence-failure branch (:822-847) + recovery (MethodGear.hpp:343-423)
+                iterConvergenceFailure++;
+                ++cconv;
+                if (iterConvergenceFailure >= 50u || fabs(h) <= 0.) {
+                  fail_keep_z(iterConvergenceFailure >= 50u ? -5 : -6);
+                  t = tInMeshPoint;
+                  lab = L_FINISH;
+                  break;
+                }
+                double hs = 0.25;
+                if (numberOfSteps < 10) hs = 0.1;
+                hs = fmax(hs, 0. / fabs(h));
+                odeHStatus = H_DEC;
+                if (p > 1u) { p -= 1; odeOrderStatus = O_DEC; }
+                alfa2_4 -= 0.01;
+                alfa2_5 -= 0.02;
+                if (alfa2_4 < 0.) { alfa2_4 = 0.; maximum_order = 3; if (p > 3) { p = 3; odeOrderStatus = O_DEC; } }
+                if (alfa2_5 < 0.) { alfa2_5 = 0.; maximum_order = 4; if (p > 4) { p = 4; odeOrderStatus = O_DEC; } }
+                hScale = hs;
+                pendHScale = hs;
+                if (numberOfSteps > 5) {
+                  nConvFailOrderMax++;
+                  if (nConvFailOrderMax % 5 == 0 && p != 1u) { p = 1; odeOrderStatus = O_DEC; }
+                  if (nConvFailOrderMax % 10 == 0 && tStabilize != tInMeshPoint) {
+                    phase = PH_STAB_CONV;
+                    lab = L_NONE;
+                    break;
+                  }
+                }
+                if (numberOfSteps > stepOfLastJacobian + 5u) jacobianChange = 1;
+                if (numberOfSteps != stepOfLastJacobian && iterConvergenceFailure == 50u) jacobianChange = 1;
+                hNextStep *= hs;
+                lab = L_DRIVER_LOOP;
+                break;
+              }
+              // MultiValueStep tail (:1271-1327)
+              {
+                const double r0 = c_gear_r.r[0][p - 1];
+                double bb = b;
+                const double vr = bb * r0;
+                double x0 = v[0];
+                const double x1 = v[1];
+                if (al) {
+                  if (x0 + vr < lo) { bb = lo - z[0] - x1; x0 = lo - vr; if (x0 < lo) x0 = lo; }
+                  if (x0 + vr > hi) { bb = hi - z[0] - x1; x0 = hi - vr; if (x0 > hi) x0 = hi; }
+                }
+                v[0] = x0 + vr;
+                v[1] = x1 + bb;
+                b = bb;
+    #pragma unroll
+                for (unsigned i = 2; i < 8; ++i)
+                  if (i <= p) v[i] += b * c_gear_r.r[i][p - 1];
+                set8(v, p + 1, (get8(v, p) - get8(z, p)) / (double(p) + 1.));
+                if (iterOrder >= p) set8(v, p + 2, (get8(v, p + 1) - get8(z, p + 1)) / (double(p) + 2.));
+                dv = true;
+              }
+              // error test (:876-962)
+              double hCur = c_gear_r.Ep[p] * wrms(get8(v, p + 1));
+              if (hCur > 1.) {
+                iterErrorFailure++;
+                ++cerr;
+                if (iterErrorFailure >= 50u || fabs(h) <= 0.) {
+                  fail_keep_z(iterErrorFailure >= 50u ? -4 : -6);
+                  t = tInMeshPoint;
+                  lab = L_FINISH;
+                  break;
+                }
+                hScaleMax = 1.;
+                hCur = 0.8 * pow_ol(1. / hCur, 1. / double(p + 1));
+                hScale = hCur;
+                if (p > 1u) {
+                  double hMinus = c_gear_r.Ep[p - 1] * wrms(get8(v, p));
+                  hMinus = 1. / (hMinus + kMachEpsFloat);
+                  hMinus = 0.8 * pow_ol(hMinus, 1. / double(p));
+                  if (hMinus > hCur) { hScale = hMinus; p -= 1; odeOrderStatus = O_DEC; }
+                }
+                hScale = fmin(hScale, 0.5);
+                hScale = fmax(hScale, 0. / fabs(h));
+                hScale = fmax(hScale, 1.e-3);
+                if (p == 1u && hScale < 0.1 && numberOfSteps > 10 && tInMeshPoint != tStabilize) {
+                  phase = PH_STAB_ERR;
+                  lab = L_NONE;
+                  break;
+                }
+                odeHStatus = H_DEC;
+                hNextStep *= hScale;
+                lab = L_DRIVER_LOOP;
+                break;
+              }
+              // accepted step (:963-1037)
+              hNordsieck = h; hNextStep = h;
+              orderInNextStep = p; odeOrderStatus = O_CONST; odeHStatus = H_CONST;
+              {
+                // MethodGear::ConvergenceRate (:425-516) with the stored Jacobian
+                if (iterErrorFailure > 0 || iterConvergenceFailure > 0) iterConvergenceRate = 0;
+                if (iterConvergence > 1) {
+                  load_j();
+                  const double s = rowdot_ol<double, W>(Js, v[0] - z[0], n, ld, lane, gm);
+                  const double vr = v[1] - (s * h + z[1]);
+                  const double normd = wsum_g<W>(gm, al ? fabs(vr) : 0.);
+                  const double normf = wsum_g<W>(gm, al ? fabs(v[1]) : 0.);
+                  if (normd > 3. * normf + .1 && iterConvergence > 2) {
+                    if (numberOfSteps > stepOfLastJacobian + 5u) jacobianChange = 1;
+                    hScale = 0.5; odeHStatus = H_DEC; hNextStep = h * hScale;
+                    if (p > 1) { orderInNextStep = p - 1; odeOrderStatus = O_DEC; }
+                    iterConvergenceRate = 0; iterConvergenceFailure = 1;
+                  } else if (normd > normf + 0.1) {
+                    iterConvergenceRate++;
+                    if (iterConvergenceRate >= 5) {
+                      hScale = 0.8; odeHStatus = H_DEC; hNextStep = h * hScale;
+                      iterConvergenceRate = 0; iterConvergenceFailure = 1;
+                    }
+                    if (numberOfSteps > stepOfLastJacobian + 5u && iterConvergence > 2) {
+                      jacobianChange = 1;
+                      iterConvergenceRate = 0; iterConvergenceFailure = 1;
+                    }
+                  }
+                }
+              }
+              if (iterErrorFailure > 0 || iterConvergenceFailure > 0) {
+                iterErrorFailure = 0; iterConvergenceFailure = 0;
+              } else {
+                iterOrder++;
+                if (iterOrder > p + 1) {
+                  // NewOrderNewH (:1042-1210)
+                  const HCand hc = order_candidates<W>(get8(v, p), get8(v, p + 1), get8(v, p + 2), eps, al, n, gm, p,
+                                                       p > 1u && odeOrderStatus != O_INC,
+                                                       p < maximum_order && odeOrderStatus != O_DEC,
+                                                       alfa2(p - 1), alfa2(p), alfa2(p + 1));
+                  const double hMinus = hc.hMinus, hC = hc.hC, hPlus = hc.hPlus, alfa1 = hc.alfa1, alfa3 = hc.alfa3;
+                  if (hMinus > hC && hMinus > hPlus) {
+                    hScale = (.75 / alfa1) * hMinus; orderInNextStep = p - 1; odeOrderStatus = O_DEC;
+                  } else if (hC > hMinus && hC > hPlus) {
+                    hScale = (.75 / alfa2(p)) * hC; orderInNextStep = p; odeOrderStatus = O_CONST;
+                  } else {
+                    hScale = (.75 / alfa3) * hPlus; orderInNextStep = p + 1; odeOrderStatus = O_INC;
+                  }
+                  if (fixedOrderMin) {
+                    iterMinimumOrder++;
+                    if (iterMinimumOrder < 2000) {
+                      hScale = (.75 / alfa2(p)) * hC; orderInNextStep = p; odeOrderStatus = O_CONST;
+                    } else {
+                      fixedOrderMin = false;
+                    }
+                  }
+                  if (hScale < 1.2) {
+                    iterConstSteps++;
+                    hScale = 1.; odeHStatus = H_CONST; orderInNextStep = p; odeOrderStatus = O_CONST; hNextStep = h;
+                  } else {
+                    iterConstSteps = 0;
+                    hScale = fmin(hScale, hScaleMax);
+                    odeHStatus = H_INC;
+                    hNextStep = h * hScale;
+                  }
+                  if (iterConstSteps > 500 ||
+                      (numberOfSteps % 1000 == 0 && numberOfSteps != 0 && (fabs(h) < 1.e-7 || fabs(h) < 1.e-5 * t))) {
+                    if (p > 1u) {
+                      fixedOrderMin = true; iterMinimumOrder = 0;
+                      orderInNextStep = 1; odeOrderStatus = O_DEC;
+                      hScale = 0.5; hNextStep = h * hScale; odeHStatus = H_DEC;
+                    }
+                  }
+                }
+              }
+    #pragma unroll
+              for (unsigned i = 0; i < 8; ++i)
+                if (i <= p + 2) z[i] = v[i];
+              z[0] = clamp(z[0]);
+              dz = true;
+              numberOfSteps++;
+              ++cstep;
+              if (tOut == t) {
+                va = z[0];
+                lab = L_FINISH;
+                break;
+              }
+              if (tOut < t) {
+                // Interpolation (:687-706); the RHS at tOut then sets QR (:599-611)
+                const double hp = (tOut - t) / hNordsieck;
+                double yv = z[0];
+                if (hp != 0.) {
+                  double hr = 1.;
+    #pragma unroll
+                  for (unsigned i = 1; i < 8; ++i) {
+                    if (i <= p) {
+                      hr *= hp;
+                      yv += z[i] * hr;
+                    }
+                  }
+                  yv = clamp(yv);
+                }
+                va = yv;
+                phase = PH_FINAL;
+                lab = L_NONE;
+                break;
+              }
+              lab = L_START_STEP;
+              break;
+            }
+            case L_FINISH: {
+              // utilities.H:153-200 and the scatter of chemistry_DI.H:221-235
+              const double s = wsum_g<W>(gm, lane < NC ? va : 0.);
+              if (lane < NC) a.Y[(long)lane * a.ld + cell] = va / s;
+              if (o.energy && lane == NC) a.T[cell] = va;
+              if (lane == 0) {
+                if (a.Q) a.Q[cell] = QR;
+                if (a.status) a.status[cell] = status;
+                if (a.nsteps) a.nsteps[cell] = (int)numberOfSteps;
+              }
+              phase = PH_DONE;
+              lab = L_NONE;
+              break;
+            }
+            default:
+              lab = L_NONE;
+              break;
+          }
+        }
+    }
+    __syncwarp(gm);
+  }
+}
+
+size_t group_smem_bytes(const MechLayout& L, bool lu64, int width) {
+  const size_t n = L.nc + 1, ld = n + 1, la = 2 * n + 1;
+  const size_t groups = (size_t)kGW * (width == 16 ? 2 : 1);
+  const size_t gd = 2 * (size_t)L.nc + L.nr + n * ld;
+  const size_t gl = n * ld + n * la + 2 * n;
+  return ((L.bytes + 15u) & ~15u) + groups * gd * sizeof(double) + groups * gl * (lu64 ? 8 : 4) + 16;
+}
+
+template <typename LUT, int W, int MB>
+cudaError_t group_launch(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                         const StepArgs& a, int* queue, int* err, int sm_count, cudaStream_t stream) {
+  const size_t smem = group_smem_bytes(L, sizeof(LUT) == 8, W);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e =
+      cudaFuncSetAttribute(group_kernel<LUT, W, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int bps = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, group_kernel<LUT, W, MB>, kGW * 32, smem);
+  if (e != cudaSuccess) return e;
+  if (bps <= 0) return cudaErrorInvalidConfiguration;
+  constexpr int GB = kGW * (32 / W);
+  const long want = (a.ncells + GB - 1) / GB, cap = (long)sm_count * bps;
+  e = cudaMemsetAsync(queue, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  group_kernel<LUT, W, MB><<<(unsigned)(want < cap ? want : cap), kGW * 32, smem, stream>>>(L, mech_gmem, o, a, queue,
+                                                                                              err);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // compact: the cells still integrating form the next list, binned by the solver
 // path their next advance will take -- Jacobians; predictor results that
@@ -2262,6 +3088,26 @@ cudaError_t launch_rounds(const RoundsPlan& P, const MechLayout& L, const unsign
     if (nact_host[1] != 0) return cudaErrorLaunchTimeout;   // a kernel raised a flag: stop, the caller reports it
   }
   return cudaErrorLaunchTimeout;
+}
+
+
+// occupancy: 4 (up to 128 registers a thread) or 2 blocks per SM (up to 255)
+template <int MB>
+cudaError_t launch_group_mb(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                            const StepArgs& a, bool lu64, int* queue, int* err, int sm_count, cudaStream_t stream) {
+  if (L.nc + 1 <= 16)
+    return lu64 ? group_launch<double, 16, MB>(L, mech_gmem, o, a, queue, err, sm_count, stream)
+                : group_launch<float, 16, MB>(L, mech_gmem, o, a, queue, err, sm_count, stream);
+  return lu64 ? group_launch<double, 32, MB>(L, mech_gmem, o, a, queue, err, sm_count, stream)
+              : group_launch<float, 32, MB>(L, mech_gmem, o, a, queue, err, sm_count, stream);
+}
+
+cudaError_t launch_group(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o, const StepArgs& a,
+                         bool lu64, int min_blocks, int* queue, int* err, int sm_count, cudaStream_t stream) {
+  if (a.ncells <= 0) return cudaSuccess;
+  if (L.nc + 1 > 32) return cudaErrorInvalidValue;
+  return min_blocks == 2 ? launch_group_mb<2>(L, mech_gmem, o, a, lu64, queue, err, sm_count, stream)
+                         : launch_group_mb<4>(L, mech_gmem, o, a, lu64, queue, err, sm_count, stream);
 }
 
 }  // namespace lsg

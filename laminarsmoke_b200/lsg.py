@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(HERE, "liblsmoke_gpu.so")
 LSG_PRECISION_FP64 = 0
 LSG_PRECISION_MIXED = 1
 LSG_JACOBIAN_FD, LSG_JACOBIAN_ANALYTIC = 0, 1
-LSG_TILE_AUTO, LSG_TILE_WARP, LSG_TILE_LANE, LSG_TILE_PERSISTENT, LSG_TILE_BLOCK = 0, 1, 2, 3, 4
+LSG_TILE_AUTO, LSG_TILE_WARP, LSG_TILE_LANE, LSG_TILE_PERSISTENT, LSG_TILE_BLOCK, LSG_TILE_GROUP = 0, 1, 2, 3, 4, 5
 LSG_ERR_SCRATCH = -8
 NOALLOC_SCRATCH_BYTES = 16 << 20
 NCOUNTERS = 8
@@ -445,7 +445,7 @@ class ReactionStep:
         """Kernels this context has enqueued so far."""
         return int(lib().lsg_ctx_launches(self.h))
 
-    KERNEL_KINDS = ("rhs", "advance", "compact", "init", "plain", "persistent", "block")
+    KERNEL_KINDS = ("rhs", "advance", "compact", "init", "plain", "persistent", "block", "group")
 
     def kernel_times(self, reset: bool = False) -> dict:
         """{kind: (total ms, timed launches)} from the CUDA events recorded when
@@ -457,7 +457,7 @@ class ReactionStep:
                "lsg_ctx_kernel_times")
         return {k: (ms[i], nl[i]) for i, k in enumerate(self.KERNEL_KINDS)}
 
-    TUNE_CANDIDATES = ("rounds16", "rounds32", "plain_warp", "persistent")
+    TUNE_CANDIDATES = ("rounds16", "rounds32", "plain_warp", "persistent", "group_4", "group_2")
 
     def tuning(self):
         """(tile, width, {candidate: cells/s}) chosen by the autotuner, or None before it ran."""

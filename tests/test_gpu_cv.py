@@ -29,7 +29,7 @@ def _cv_states(name, n, seed):
 
 @pytest.mark.parametrize("name,form,n,frac", [
     ("h2co", "plain", 1024, 0.97), ("h2co", "mixed", 1024, 0.97), ("h2co", "persistent", 1024, 0.97),
-    ("h2co+30", "block", 128, 0.85)])
+    ("h2co", "group", 1024, 0.97), ("h2co+30", "block", 128, 0.85)])
 def test_cv_step(cuda, name, form, n, frac):
     """Statuses equal the oracle's; T within 1e-6 everywhere; Y within 1e-9 in every cell whose solver took
     the oracle's path (all eight counters equal) and within 1e-7 in the others (an ulp of exp/log flips a
@@ -41,6 +41,7 @@ def test_cv_step(cuda, name, form, n, frac):
     kw = {"plain": dict(tile=lsg.LSG_TILE_WARP, precision=lsg.LSG_PRECISION_FP64),
           "mixed": dict(tile=lsg.LSG_TILE_LANE, precision=lsg.LSG_PRECISION_MIXED),
           "persistent": dict(tile=lsg.LSG_TILE_PERSISTENT, precision=lsg.LSG_PRECISION_MIXED),
+          "group": dict(tile=lsg.LSG_TILE_GROUP, precision=lsg.LSG_PRECISION_MIXED),
           "block": dict(precision=lsg.LSG_PRECISION_FP64)}[form]
     ctx = lsg.ReactionStep(lsg.Mechanism(data), **kw)
     Yd = torch.tensor(np.ascontiguousarray(Y.T), device=cuda)

@@ -84,8 +84,8 @@ def test_coflow_sequence_block_121(cuda):
 
 
 @pytest.mark.parametrize("name,tile,precision", [("h2co", 1, 0), ("h2co", 3, 1), ("h2co+30", 4, 0),
-                                                 ("h2co+30", 4, 1), ("h2co", 2, 1)],
-                         ids=["plain", "persistent", "block-fp64", "block-tc", "rounds"])
+                                                 ("h2co+30", 4, 1), ("h2co", 2, 1), ("h2co", 5, 1)],
+                         ids=["plain", "persistent", "block-fp64", "block-tc", "rounds", "group"])
 def test_sequence_graph_equals_step_by_step(cuda, name, tile, precision):
     """lsg_reaction_step_sequence_device captures the steps into a CUDA graph (the round scheme, whose
     rounds wait on the host, runs them one by one): its result must be the one of the same steps

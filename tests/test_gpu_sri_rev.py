@@ -50,7 +50,7 @@ def test_sri_rev_rhs(cuda, sri_rev, tile):
         np.testing.assert_allclose(dy[:, k], ref, rtol=1e-11, atol=1e-12 * np.abs(ref).max())
 
 
-@pytest.mark.parametrize("form", ["plain", "rounds", "persistent", "block"])
+@pytest.mark.parametrize("form", ["plain", "rounds", "persistent", "block", "group"])
 def test_sri_rev_step(cuda, sri_rev, form):
     import torch
     from laminarsmoke_b200 import lsg
@@ -59,7 +59,8 @@ def test_sri_rev_step(cuda, sri_rev, form):
     n = 256
     Y, T = cells.synthetic_mixing(m.species, m.arrays["mw"], n, seed=3, t_range=(900.0, 2200.0))
     kw = {"plain": dict(tile=1, precision=0), "rounds": dict(tile=2, precision=1),
-          "persistent": dict(tile=3, precision=1), "block": dict(tile=4, precision=0)}[form]
+          "persistent": dict(tile=3, precision=1), "block": dict(tile=4, precision=0),
+          "group": dict(tile=5, precision=1)}[form]
     ctx = lsg.ReactionStep(lsg.Mechanism(data), rtol=1e-10, atol=1e-16, **kw)
     Yd = torch.tensor(np.ascontiguousarray(Y.T), device=cuda)
     Td = torch.tensor(T, device=cuda)

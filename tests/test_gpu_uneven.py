@@ -38,6 +38,8 @@ FORMS = {
     "rounds-fp32": dict(tile=2, precision=1),
     "rounds-fp64": dict(tile=2, precision=0),
     "persistent-fp32": dict(tile=3, precision=1),
+    "group-fp32": dict(tile=5, precision=1),
+    "group-fp64": dict(tile=5, precision=0),
     "block": dict(tile=4, precision=0),
 }
 

@@ -2290,6 +2290,13 @@ __global__ void __launch_bounds__(kGW * 32, MB) group_kernel(MechLayout Lp, cons
       ++crhs;
       return rhs_group<W>(&sL, Md, Mi, C, Gs, NET, yv, a.p, o.energy, rho0, lane, gm, &QR);
     };
+    auto write_counters = [&]() {
+      if (a.counters && lane == 0) {
+        long long* cc = a.counters + (long)cell * NCNT;
+        cc[CNT_STEPS] = cstep; cc[CNT_RHS] = crhs; cc[CNT_JAC] = cjac; cc[CNT_FACT] = cfact;
+        cc[CNT_SOLVE] = csolve; cc[CNT_ERRFAIL] = cerr; cc[CNT_CONVFAIL] = cconv; cc[CNT_JAC_RHS] = cjrhs;
+      }
+    };
     int phase = PH_INIT;
     f = rhs(va);
     for (long req = 0; phase != PH_DONE; ++req) {
@@ -2306,11 +2313,7 @@ __global__ void __launch_bounds__(kGW * 32, MB) group_kernel(MechLayout Lp, cons
             if (a.status) a.status[cell] = status;
             if (a.nsteps) a.nsteps[cell] = (int)numberOfSteps;
           }
-          if (a.counters && lane == 0) {
-            long long* cc = a.counters + (long)cell * NCNT;
-            cc[CNT_STEPS] = cstep; cc[CNT_RHS] = crhs; cc[CNT_JAC] = cjac; cc[CNT_FACT] = cfact;
-            cc[CNT_SOLVE] = csolve; cc[CNT_ERRFAIL] = cerr; cc[CNT_CONVFAIL] = cconv; cc[CNT_JAC_RHS] = cjrhs;
-          }
+          write_counters();
           break;
         }
         if (phase == PH_PRED) {
@@ -2753,6 +2756,7 @@ __global__ void __launch_bounds__(kGW * 32, MB) group_kernel(MechLayout Lp, cons
                 if (a.status) a.status[cell] = status;
                 if (a.nsteps) a.nsteps[cell] = (int)numberOfSteps;
               }
+              write_counters();
               phase = PH_DONE;
               lab = L_NONE;
               break;

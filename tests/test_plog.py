@@ -139,18 +139,20 @@ def test_gpu_plog_step(cuda, form):
     orc = OracleMechanism(data)
     if form == "cv":
         rho = P / R_J_KMOL / T / (Y / m.arrays["mw"]).sum(axis=1)
-        _, st, _ = ctx.step_cv(Ys, Tg, rho, 1e-5)
+        _, st, ns = ctx.step_cv(Ys, Tg, rho, 1e-5)
         Yo, To, _, sto, cnt = orc.reaction_step(Y, T, 1e-5, nthreads=8, rho=rho, **tol)
     else:
-        _, st, _ = ctx.step(Ys, Tg, 1e-5, p=P)
+        _, st, ns = ctx.step(Ys, Tg, 1e-5, p=P)
         Yo, To, _, sto, cnt = orc.reaction_step(Y, T, 1e-5, p=P, nthreads=8, **tol)
     ctx.check()
     abs_Y = np.abs(Ys.T - Yo).max(axis=1)
     rel_T = np.abs(Tg - To) / To
+    same = ns == cnt[:, 0]
     print(f"plog {form}: statuses equal {np.mean(st == sto):.3f}, max rel T {rel_T.max():.3e}, "
-          f"max abs Y {abs_Y.max():.3e}, within 1e-9 {np.mean(abs_Y <= 1e-9):.3f}, steps {cnt[:, 0].mean():.0f}")
+          f"max abs Y {abs_Y.max():.3e}, within 1e-9 {np.mean(abs_Y <= 1e-9):.3f}, "
+          f"same step count {same.mean():.3f}, max abs Y there {abs_Y[same].max():.3e}, steps {cnt[:, 0].mean():.0f}")
     np.testing.assert_array_equal(st, sto)
     assert rel_T.max() <= 1e-6
-    # at constant volume the pressure, and with it every PLOG rate, follows the state: measured 97.7 % of
-    # the cells within 1e-9 (99.2 % at constant pressure), max 2.1e-8
-    assert np.mean(abs_Y <= 1e-9) >= (0.95 if form == "cv" else 0.99) and abs_Y.max() <= 1e-7
+    # cells taking the oracle's number of steps meet 1e-9; in the others a last-ulp difference of exp/log
+    # moved a step-size decision (measured 97.7 % to 99.2 % of all cells within 1e-9, max 2.1e-8)
+    assert same.mean() >= 0.9 and abs_Y[same].max() <= 1e-9 and abs_Y.max() <= 1e-7

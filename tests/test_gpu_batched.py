@@ -98,7 +98,8 @@ def test_autotuner_picks_a_measured_form(h2co, oracle_h2co, gpu_h2co, precision)
     best = max(tried, key=tried.get)
     assert (tile, width) == {"rounds16": (lsg.LSG_TILE_LANE, 16), "rounds32": (lsg.LSG_TILE_LANE, 32),
                              "plain_warp": (lsg.LSG_TILE_WARP, 0),
-                             "persistent": (lsg.LSG_TILE_PERSISTENT, 0)}[best]
+                             "persistent": (lsg.LSG_TILE_PERSISTENT, 0), "group_4": (lsg.LSG_TILE_GROUP, 4),
+                             "group_2": (lsg.LSG_TILE_GROUP, 2)}[best]
     Yo, To, Qo, sto, cnt = oracle_h2co.reaction_step(Y, T, 1e-5, nthreads=8)
     np.testing.assert_array_equal(st.cpu().numpy(), sto)
     assert np.max(np.abs(Td.cpu().numpy() - To) / To) <= RTOL_T

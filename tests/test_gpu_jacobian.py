@@ -76,12 +76,12 @@ def test_analytic_jacobian_against_central_differences(cuda, name):
             ref, h = _central(orc, yk, j, 101325.0)
             # a central difference carries the rounding of f amplified by 1/h, and its own truncation; the
             # bound allows 1e-6 of the column plus 256 eps |f| / h per entry.  The device's temperature
-            # column is itself a forward difference with hT = sqrt(eps) T: its rounding, 8 eps |f| / hT, is
-            # added there
+            # column is itself a forward difference with hT = sqrt(eps) T: its rounding, 64 eps |f| / hT, is
+            # added there (f is a sum with cancellation: measured up to 14 eps |f| / hT)
             eps = 2.220446049250313e-16
             tol = 1e-6 * np.abs(ref).max() + 256 * eps * np.abs(f0) / h
             if j == n - 1:
-                tol = tol + 8 * eps * np.abs(f0) / (np.sqrt(eps) * max(abs(yk[j]), 1.0))
+                tol = tol + 64 * eps * np.abs(f0) / (np.sqrt(eps) * max(abs(yk[j]), 1.0))
             err = np.abs(Jg[k, :, j] - ref)
             worst = max(worst, float((err / np.maximum(tol, 1e-300)).max()))
             assert np.all(err <= tol), (name, k, j, float((err / np.maximum(tol, 1e-300)).max()))

@@ -153,6 +153,8 @@ def test_gpu_plog_step(cuda, form):
           f"same step count {same.mean():.3f}, max abs Y there {abs_Y[same].max():.3e}, steps {cnt[:, 0].mean():.0f}")
     np.testing.assert_array_equal(st, sto)
     assert rel_T.max() <= 1e-6
-    # cells taking the oracle's number of steps meet 1e-9; in the others a last-ulp difference of exp/log
-    # moved a step-size decision (measured 97.7 % to 99.2 % of all cells within 1e-9, max 2.1e-8)
-    assert same.mean() >= 0.9 and abs_Y[same].max() <= 1e-9 and abs_Y.max() <= 1e-7
+    # about 8,500 BDF steps a cell: cells taking the oracle's number of steps meet 1e-9; in the others a
+    # last-ulp difference of exp/log moved step-size decisions (measured 97.3 % to 99.2 % of all cells
+    # within 1e-9, max 2.1e-8)
+    assert (not same.any() or abs_Y[same].max() <= 1e-9)
+    assert np.mean(abs_Y <= 1e-9) >= 0.95 and abs_Y.max() <= 1e-7

@@ -55,11 +55,13 @@ extern "C" {
 #define LSG_TILE_GROUP 5       /* one lane group (16 or 32 lanes) per cell from start to finish, the RHS evaluated
                                   by the group inside the solver kernel, persistent grid (up to 31 species) */
 /* Mechanisms of 32 to 511 species always run one thread block per cell (the
- * tile is ignored).  The block form factorises in FP64 with LSG_PRECISION_FP64;
- * with LSG_PRECISION_MIXED and 32 to 127 species it inverts G = I - h r0 J on
- * the tensor cores in FP32 (lsg_build_and_invert_g_device) and solves with the
- * inverse, the Newton residual staying FP64; above 127 species it factorises
- * in FP64 whatever the precision option. */
+ * tile is ignored).  The block form factorises in FP64 with LSG_PRECISION_FP64.
+ * With LSG_PRECISION_MIXED it inverts G = I - h r0 J on the tensor cores in
+ * FP32 (lsg_build_and_invert_g_device: one 128-row tile in tensor memory up to
+ * 127 species, an in-place multi-tile inverse in global memory above) and
+ * solves with the inverse, refined on the FP64 residual of G until a
+ * correction's weighted norm is below 1e-6; a matrix on which the refinement
+ * stalls (FP32 cannot hold its conditioning) is refactorised by the FP64 LU. */
 
 /* counters per cell (lsg_reaction_step_device counters_out layout) */
 #define LSG_NCOUNTERS 8        /* steps, rhs, jacobians, factorisations, solves, error-test fails, convergence fails, jacobian rhs */
@@ -255,7 +257,7 @@ int lsg_reaction_step_device_noalloc(const lsg_mech* mech, const lsg_options* op
                                      long long* counters_dev, void* stream);
 
 /* ---- the mixed-precision factorisation, on its own -------------------------
- * What the mixed-precision block form (LSG_PRECISION_MIXED, 32 to 127
+ * What the mixed-precision block form (LSG_PRECISION_MIXED, 32 to 511
  * species) does where the reference calls KernelDense::BuildAndFactorizeMatrixG
  * (math/native-ode-solvers/KernelDense.hpp:195-220): for nmat Jacobians J_dev
  * [nmat][n][n] (FP64, each column-major: element (i, j) at [j * n + i]) and
@@ -263,8 +265,9 @@ int lsg_reaction_step_device_noalloc(const lsg_mech* mech, const lsg_options* op
  * to inv_dev [nmat][n][n].  The inverse is a blocked Gauss-Jordan elimination
  * with partial pivoting whose rank-32 updates run on the tensor cores as split
  * TF32 products (three TF32 products per FP32 product, FP32 accumulation).
- * 1 <= n <= 128; device pointers; asynchronous on `stream`.  For tests and
- * measurement: the reaction step calls it internally. */
+ * 1 <= n <= 512 (above 128 the context keeps an FP32 work matrix per block,
+ * allocated on the first such call); device pointers; asynchronous on
+ * `stream`.  For tests and measurement: the reaction step calls it internally. */
 int lsg_build_and_invert_g_device(lsg_ctx* ctx, int nmat, int n, const double* J_dev, const double* hr0_dev,
                                   float* inv_dev, void* stream);
 

@@ -53,6 +53,8 @@ struct lsg_ctx {
   long long launches = 0;     // kernels enqueued by this context
   // block-per-cell (large mechanism) resources
   double* bws = nullptr;
+  float* tcinv_ws = nullptr;    // lsg_build_and_invert_g_device above 128: one FP32 work matrix per block
+  size_t tcinv_bytes = 0;
   long bws_blocks = 0;
   long tc_blocks = 0;           // blocks of the tensor-core (mixed-precision) block kernel
   int* bqueue = nullptr;
@@ -651,6 +653,7 @@ int lsg_ctx_destroy(lsg_ctx* c) {
   cudaFree(c->queue);
   cudaFree(c->rstate);
   cudaFree(c->bws);
+  cudaFree(c->tcinv_ws);
   if (c->seq_exec) cudaGraphExecDestroy(c->seq_exec);
   if (c->seq_ev[0]) cudaEventDestroy(c->seq_ev[0]);
   if (c->seq_ev[1]) cudaEventDestroy(c->seq_ev[1]);
@@ -952,11 +955,20 @@ int lsg_reaction_step_device_noalloc(const lsg_mech* m, const lsg_options* opt, 
 
 int lsg_build_and_invert_g_device(lsg_ctx* c, int nmat, int n, const double* J, const double* hr0, float* inv,
                                   void* stream) {
-  if (!c || nmat < 0 || n < 1 || n > 128 || (nmat > 0 && (!J || !hr0 || !inv))) return LSG_ERR_ARG;
+  if (!c || nmat < 0 || n < 1 || n > 512 || (nmat > 0 && (!J || !hr0 || !inv))) return LSG_ERR_ARG;
   if (nmat == 0) return LSG_OK;
   if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
   if (!sm_count(c)) return LSG_ERR_CUDA;
-  if (launch_tc_inverse(nmat, n, J, hr0, inv, c->sm_count, c->d_err, (cudaStream_t)stream) != cudaSuccess) {
+  const size_t need = tc_inverse_ws_bytes(n, c->sm_count);
+  if (need > c->tcinv_bytes) {
+    cudaFree(c->tcinv_ws);
+    c->tcinv_ws = nullptr;
+    c->tcinv_bytes = 0;
+    if (cudaMalloc(&c->tcinv_ws, need) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+    c->tcinv_bytes = need;
+  }
+  if (launch_tc_inverse(nmat, n, J, hr0, inv, c->tcinv_ws, c->sm_count, c->d_err, (cudaStream_t)stream) !=
+      cudaSuccess) {
     cudaGetLastError();
     return LSG_ERR_CUDA;
   }

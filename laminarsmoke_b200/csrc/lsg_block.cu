@@ -24,6 +24,9 @@ static __constant__ GearConsts c_gear_k;
 namespace {
 
 constexpr int kBlkMaxN = 512;
+// refinement of the mixed-precision solve (GearBlock::solve)
+constexpr int kBlkRefineMax = 4;
+constexpr double kBlkRefineTol = 1.e-6;
 
 __device__ __forceinline__ double contrib_k(double nu, double v) {
   if (nu == 1.) return v;
@@ -88,10 +91,43 @@ __host__ __device__ inline size_t block_shared_bytes(const MechLayout& L) {
          sizeof(int) * (2 * BT + BT / 32 + 1) + 64;
 }
 
-// Per-block global work space (doubles): J, G, kinetic-constant caches.
+// Threads of the block form: one per ODE component, in whole warpgroups.
+__host__ __device__ inline int block_bt(int n) { return n <= 128 ? 128 : (n <= 256 ? 256 : 512); }
+
+// Per-block global work space (doubles).  Up to 128 components: J and G (n x n, column-major), the
+// kinetic-constant caches.  Above 128 the mixed-precision form's layout is also covered: J with leading
+// dimension Np = the block's threads, the FP64 fallback factors G (n x n), the FP32 inverse (Np x Np),
+// the Nordsieck arrays Z and V (8 Np each: they leave shared memory to the inverse's operands), caches.
+__host__ __device__ inline size_t round32(size_t x) { return (x + 31) & ~(size_t)31; }
 __host__ __device__ inline size_t block_ws_doubles(const MechLayout& L) {
   const size_t n = L.nc + 1;
-  return 2 * n * n + 2 * (size_t)L.nr + 2 * (size_t)(L.n_fo > 0 ? L.n_fo : 1) + 8;
+  const size_t caches = 2 * (size_t)L.nr + 2 * (size_t)(L.n_fo > 0 ? L.n_fo : 1) + 8;
+  const size_t fp64 = round32(2 * n * n + caches);
+  if (n <= 128) return fp64;
+  const size_t np = (size_t)block_bt((int)n);
+  const size_t tcl = round32(np * np + round32(n * n) + np * np / 2 + 16 * np + caches);
+  return fp64 > tcl ? fp64 : tcl;
+}
+
+// Shared memory of the mixed-precision form above 128 components: a persistent head (solve vector,
+// reductions, LU pivots, the inverse's pivots, TMEM slot, MMA barrier), then, 1024-byte aligned, one
+// region used in turn by the RHS (concentrations, enthalpies, entropies, net rates), by the inverse
+// (split-TF32 operands) and by the solves (partial sums).
+template <int BT>
+__host__ __device__ inline size_t tcl_head_bytes() {
+  return sizeof(double) * (BT + BT / 32 + 1 + 4) + sizeof(int) * (4 * BT + BT / 32 + 1 + 4) + 16;
+}
+template <int BT>
+__host__ __device__ inline size_t tcl_union_bytes(const MechLayout& L) {
+  const size_t rhs = sizeof(double) * (3 * (size_t)L.nc + L.nr);
+  const size_t inv = sizeof(float) * ((2 * (BT / 128) + 2) * (size_t)tc::kOperandFloats + 64 + 4 * tc::kPanel);
+  const size_t sol = sizeof(double) * 5 * (size_t)BT;
+  size_t m = rhs > inv ? rhs : inv;
+  return m > sol ? m : sol;
+}
+template <int BT>
+__host__ __device__ inline size_t tcl_smem_bytes(const MechLayout& L) {
+  return tcl_head_bytes<BT>() + 1024 + tcl_union_bytes<BT>(L);
 }
 
 // ---------------------------------------------------------------------------
@@ -334,6 +370,52 @@ __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, 
   return dyl;
 }
 
+// y = A x for a column-major matrix with BT rows (leading dimension BT) and n columns; x: n doubles in
+// shared memory.  Thread t reads rows 4 (t mod BT/4) .. +3 of a quarter of the columns with 16-byte
+// loads (four independent streams per row quad, so that many loads are in flight); the quarters are
+// summed through part (4 BT doubles, shared).  Returns y_tid.  All BT threads call it.
+template <int BT, typename T>
+__device__ __forceinline__ double gemv_block(const T* __restrict__ A, int n, const double* xs, double* part) {
+  const int tid = threadIdx.x;
+  constexpr int RQ = BT / 4;
+  const int q = tid % RQ, sl = tid / RQ;
+  const int js = (n * sl) >> 2, je = (n * (sl + 1)) >> 2;
+  double a0 = 0., a1 = 0., a2 = 0., a3 = 0.;
+  if constexpr (sizeof(T) == 4) {
+    const float4* A4 = reinterpret_cast<const float4*>(A);
+#pragma unroll 8
+    for (int j = js; j < je; ++j) {
+      const float4 v = A4[(long)j * RQ + q];
+      const double xj = xs[j];
+      a0 += (double)v.x * xj;
+      a1 += (double)v.y * xj;
+      a2 += (double)v.z * xj;
+      a3 += (double)v.w * xj;
+    }
+  } else {
+    const double2* A2 = reinterpret_cast<const double2*>(A);
+#pragma unroll 4
+    for (int j = js; j < je; ++j) {
+      const double2 v0 = A2[(long)j * (BT / 2) + 2 * q];
+      const double2 v1 = A2[(long)j * (BT / 2) + 2 * q + 1];
+      const double xj = xs[j];
+      a0 += v0.x * xj;
+      a1 += v0.y * xj;
+      a2 += v1.x * xj;
+      a3 += v1.y * xj;
+    }
+  }
+  double* pp = part + sl * BT + 4 * q;
+  pp[0] = a0;
+  pp[1] = a1;
+  pp[2] = a2;
+  pp[3] = a3;
+  __syncthreads();
+  const double y = (part[tid] + part[BT + tid]) + (part[2 * BT + tid] + part[3 * BT + tid]);
+  __syncthreads();
+  return y;
+}
+
 // ---------------------------------------------------------------------------
 // Gear / multivalue BDF integrator for one block (one cell).
 // ---------------------------------------------------------------------------
@@ -348,13 +430,23 @@ struct GearBlock {
   const MechLayout* L;
   MechView M;
   BlockShared W;
-  double* J;      // [n][n] row major, global
+  double* J;      // column-major, leading dimension jld, global
+  int jld;
   double* G;      // [n][n] factors, global (FP64 form)
   // mixed-precision form (TC): the tensor-core inverse's shared memory, TMEM and barrier parity
   tc::Smem TS;
   uint32_t tmem;
   uint32_t tc_phase;
   bool tc_failed;
+  double tc_hr0;    // hr0 of the matrix the current inverse belongs to
+  bool tc_fp64;     // the refinement stalled on this matrix: it was refactorised by the FP64 LU
+  // more than 128 components (TCL): the inverse in global memory (lsg_tc.cuh gj_inverse_large), its
+  // pivots in shared memory; part/ysm: the solves' partial sums (shared)
+  static constexpr bool TCL = TC && BT > 128;
+  float* RL;
+  tc::SmemL TL;
+  double* part;
+  double* ysm;
   double* karr;
   double* ukeq;
   double* kinf;
@@ -427,7 +519,7 @@ struct GearBlock {
       const double aux = rhs_block<BT>(*L, M, W, karr, ukeq, kinf, logf, yp, T, P0, energy, rho0);
       ++cnt[CNT_JAC_RHS];
       const double hInv = 1. / hJ;
-      if (active) J[(long)j * n + tid] = hInv * (aux - fl);
+      if (active) J[(long)j * jld + tid] = hInv * (aux - fl);
     }
     __syncthreads();
   }
@@ -437,7 +529,13 @@ struct GearBlock {
   __device__ void build_and_factorize(double hr0) {
     if constexpr (TC) {
       // G^-1 in FP32 by the tensor-core Gauss-Jordan inverse (lsg_tc.cuh)
-      if (!tc::gj_inverse(J, ne, hr0, TS, tmem, &tc_phase)) tc_failed = true;
+      if constexpr (TCL) {
+        if (!tc::gj_inverse_large<BT / 128>(J, jld, ne, hr0, RL, TL, tmem, &tc_phase)) tc_failed = true;
+      } else {
+        if (!tc::gj_inverse(J, ne, hr0, TS, tmem, &tc_phase)) tc_failed = true;
+      }
+      tc_hr0 = hr0;
+      tc_fp64 = false;
       ++cnt[CNT_FACT];
     } else {
       build_and_factorize_fp64(hr0);
@@ -448,7 +546,7 @@ struct GearBlock {
     const int n = ne;
     for (long e = tid; e < (long)n * n; e += BT) {
       const int j = (int)(e / n), i = (int)(e % n);
-      double g = J[e];
+      double g = J[(long)j * jld + i];
       g *= -hr0;
       if (i == j) g += 1.;
       G[e] = g;
@@ -520,21 +618,84 @@ struct GearBlock {
 
   // KernelDense::SolveLinearSystem with the factors of build_and_factorize:
   // row interchanges, then column-oriented forward and back substitution.
+  // x = X r with the FP32 inverse X (column-major in shared memory), accumulated in FP64
+  __device__ double apply_inverse(double rl) {
+    const int n = ne;
+    if constexpr (TCL) {
+      // x_a = y_{p_a}, y = R r~, r~_s = r_{p_s} (gj_inverse_large); after a failed inverse the pivots are
+      // incomplete: the solve is discarded then, but stays in bounds
+      W.X[tid] = 0.;
+      __syncthreads();
+      const int sl = TL.colof[tid];
+      if (tid < n && sl >= 0 && sl < n) W.X[sl] = rl;
+      __syncthreads();
+      const double y = gemv_block<BT, float>(RL, n, W.X, part);
+      ysm[tid] = y;
+      __syncthreads();
+      const double x = tid < n ? ysm[TL.piv[tid]] : 0.;
+      __syncthreads();
+      return x;
+    }
+    W.X[tid] = tid < n ? rl : 0.;
+    __syncthreads();
+    double x = 0.;
+    if (tid < n) {
+      const float* RT = TS.op;
+#pragma unroll 4
+      for (int j = 0; j < n; ++j) x += (double)RT[j * tc::kRows + tid] * W.X[j];
+    }
+    __syncthreads();
+    return x;
+  }
+
+  // (G x)_tid = x_tid - hr0 (J x)_tid in FP64 with the FP64 Jacobian (column-major in global memory)
+  __device__ double apply_g(double xl, double hr0) {
+    return xl - hr0 * jacobian_times(xl);
+  }
+
+  // (J x)_tid, FP64
+  __device__ double jacobian_times(double xl) {
+    const int n = ne;
+    W.X[tid] = tid < n ? xl : 0.;
+    __syncthreads();
+    if constexpr (TCL) return gemv_block<BT, double>(J, n, W.X, part);
+    double s0 = 0.;   // JacobianTimesVector (MethodGear.hpp:438) in column order
+    if (tid < n) {
+#pragma unroll 8
+      for (int j = 0; j < n; ++j) s0 += J[(long)j * jld + tid] * W.X[j];
+    }
+    __syncthreads();
+    return s0;
+  }
+
+  // Mixed-precision solve: x = X r, then refinement sweeps x += X (r - G x) on the FP64 residual until
+  // the weighted RMS of a correction is below kBlkRefineTol (the Newton test compares such norms with 1), at
+  // most kBlkRefineMax sweeps.  A sweep that does not halve the correction means |I - X G| is too close to
+  // 1 for this matrix (FP32 cannot hold its conditioning): G is then refactorised by the FP64 LU, which
+  // serves every solve until the next factorisation.
   __device__ double solve(double xl) {
     if constexpr (TC) {
-      // x = G^-1 r with the FP32 inverse (column-major in shared memory), accumulated in FP64
-      const int n = ne;
-      W.X[tid] = tid < n ? xl : 0.;
-      __syncthreads();
-      double x = 0.;
-      if (tid < n) {
-        const float* RT = TS.op;
-#pragma unroll 4
-        for (int j = 0; j < n; ++j) x += (double)RT[j * tc::kRows + tid] * W.X[j];
+      if (!tc_fp64) {
+        double x = apply_inverse(xl);
+        double prev = 0.;
+        bool converged = false;
+        for (int s = 0; s < kBlkRefineMax; ++s) {
+          const double d = apply_inverse(xl - apply_g(x, tc_hr0));
+          x += d;
+          const double nd = error_control(d);
+          if (nd <= kBlkRefineTol) { converged = true; break; }
+          if (s > 0 && !(nd <= 0.5 * prev)) break;
+          prev = nd;
+        }
+        if (converged) {
+          ++cnt[CNT_SOLVE];
+          return x;
+        }
+        build_and_factorize_fp64(tc_hr0);   // the same matrix: not a factorisation of the method
+        --cnt[CNT_FACT];
+        tc_fp64 = true;
       }
-      __syncthreads();
-      ++cnt[CNT_SOLVE];
-      return x;
+      return solve_fp64(xl);
     } else {
       return solve_fp64(xl);
     }
@@ -692,13 +853,8 @@ struct GearBlock {
   __device__ void convergence_rate() {   // MethodGear.hpp:425-516
     if (iterErrorFailure > 0 || iterConvergenceFailure > 0) iterConvergenceRate = 0;
     if (iterConvergence <= 1) return;
-    const int n = ne;
-    W.X[tid] = active ? V(0) - Z(0) : 0.;
-    __syncthreads();
-    double s = 0.;
-    if (active)
-      for (int j = 0; j < n; ++j) s += J[(long)j * n + tid] * W.X[j];
-    va = s;
+    const double s = jacobian_times(active ? V(0) - Z(0) : 0.);
+    va = active ? s : 0.;
     va *= h;
     va += active ? Z(1) : 0.;
     va = (active ? V(1) : 0.) - va;
@@ -813,6 +969,9 @@ struct GearBlock {
     if (numberOfSteps < 10) hScaleMax = 1000.;
     else if (numberOfSteps > 10 && numberOfSteps < 20) hScaleMax = 10.;
     for (int guard = 0; guard < 1000000; ++guard) {
+      if constexpr (TC) {
+        if (tc_failed) { status = -1; return; }   // an MMA did not complete: the cell stops
+      }
       if (odeHStatus != H_CONST) {
         hScale = hNextStep / hNordsieck;
         double hr = 1.;
@@ -940,9 +1099,10 @@ struct GearBlock {
 // chemistry_DI.H:92-235: gather, clip and renormalise, integrate, renormalise, scatter.
 // ---------------------------------------------------------------------------
 template <int BT, bool TC>
-__global__ void __launch_bounds__(BT, TC ? 2 : (BT == 128 ? 4 : (BT == 256 ? 2 : 1))) block_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem,
-                                                   StepOptions o, StepArgs a, double* __restrict__ ws_all,
-                                                   int* queue, int* err) {
+__global__ void __launch_bounds__(BT, TC ? (BT == 128 ? 2 : 1) : (BT == 128 ? 4 : (BT == 256 ? 2 : 1)))
+    block_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, StepOptions o, StepArgs a,
+                 double* __restrict__ ws_all, int* queue, int* err) {
+  constexpr bool TCL = TC && BT > 128;
   extern __shared__ __align__(16) unsigned char bsm[];
   __shared__ int s_cell;
   const int tid = threadIdx.x;
@@ -950,7 +1110,53 @@ __global__ void __launch_bounds__(BT, TC ? 2 : (BT == 128 ? 4 : (BT == 256 ? 2 :
   const size_t wsd = block_ws_doubles(L);
   double* ws = ws_all + (size_t)blockIdx.x * wsd;
   BlockShared W;
-  {
+  // global work space: the FP64 layout, or (TCL) J with leading dimension BT, G, the FP32 inverse, Z, V
+  double* Jp = ws;
+  int jld = ne;
+  double* Gp = ws + (size_t)ne * ne;
+  double* karr = ws + 2 * (size_t)ne * ne;
+  float* RL = nullptr;
+  tc::SmemL TL{};
+  double* part = nullptr;
+  double* ysm = nullptr;
+  uint32_t* tslot = nullptr;
+  if constexpr (TCL) {
+    jld = BT;
+    Gp = ws + (size_t)BT * BT;
+    RL = (float*)(Gp + round32((size_t)ne * ne));
+    double* zv = (double*)(RL + (size_t)BT * BT);
+    W.Z = zv;
+    W.V = zv + 8 * BT;
+    karr = zv + 16 * BT;
+    double* p = (double*)bsm;
+    W.X = p; p += BT;
+    W.red = p; p += BT / 32 + 1;
+    W.slot = p; p += 4;
+    int* ip = (int*)p;
+    W.PIV = ip; ip += BT;
+    W.ival = ip; ip += BT / 32 + 1;
+    W.PERM = ip; ip += BT;
+    TL.piv = ip; ip += BT;
+    TL.colof = ip; ip += BT;
+    tslot = (uint32_t*)ip; ip += 4;
+    TL.mbar = (unsigned long long*)(((uintptr_t)ip + 7) & ~(uintptr_t)7);
+    const uint32_t s0 = tc::smem_addr(bsm);
+    const uint32_t base = ((s0 + (uint32_t)tcl_head_bytes<BT>() + 1023u) & ~1023u) - s0;
+    unsigned char* un = bsm + base;
+    double* d = (double*)un;
+    W.C = d; d += NC;
+    W.H = d; d += NC;
+    W.S = d; d += NC;
+    W.NET = d;
+    TL.A = (float*)un;
+    TL.B = TL.A + 2 * (BT / 128) * tc::kOperandFloats;
+    float* f = TL.B + 2 * tc::kOperandFloats;
+    TL.red = f; f += 32;
+    TL.redi = (int*)f; f += 32;
+    TL.prow = f;
+    part = (double*)un;
+    ysm = part + 4 * BT;
+  } else {
     double* p = (double*)bsm;
     W.Z = p; p += 8 * BT;
     W.V = p; p += 8 * BT;
@@ -969,7 +1175,14 @@ __global__ void __launch_bounds__(BT, TC ? 2 : (BT == 128 ? 4 : (BT == 256 ? 2 :
   // then its small arrays; TMEM (256 columns) for the block's lifetime
   tc::Smem TS{};
   uint32_t tmem = 0;
-  if constexpr (TC) {
+  if constexpr (TCL) {
+    if (tid < 32) tc::tmem_alloc(tslot, BT);
+    if (tid == 0) tc::mbar_init(TL.mbar, 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    tmem = *tslot;
+  } else if constexpr (TC) {
     const uint32_t s0 = tc::smem_addr(bsm);
     const uint32_t base = ((s0 + (uint32_t)block_shared_bytes<BT>(L) + 1023u) & ~1023u) - s0;   // 1024-byte aligned
     unsigned char* q = bsm + base;
@@ -1016,12 +1229,19 @@ __global__ void __launch_bounds__(BT, TC ? 2 : (BT == 128 ? 4 : (BT == 256 ? 2 :
       g.tmem = tmem;
       g.tc_phase = tc_phase;
       g.tc_failed = false;
+      g.tc_hr0 = 0.;
+      g.tc_fp64 = false;
       g.L = &L;
       g.M = M;
       g.W = W;
-      g.J = ws;
-      g.G = ws + (size_t)ne * ne;
-      g.karr = ws + 2 * (size_t)ne * ne;
+      g.J = Jp;
+      g.jld = jld;
+      g.G = Gp;
+      g.RL = RL;
+      g.TL = TL;
+      g.part = part;
+      g.ysm = ysm;
+      g.karr = karr;
       g.ukeq = g.karr + L.nr;
       g.kinf = g.ukeq + L.nr;
       g.logf = g.kinf + (L.n_fo > 0 ? L.n_fo : 1);
@@ -1071,7 +1291,7 @@ __global__ void __launch_bounds__(BT, TC ? 2 : (BT == 128 ? 4 : (BT == 256 ? 2 :
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (tid < 32) tc::tmem_dealloc(tmem, tc::kCols);
+    if (tid < 32) tc::tmem_dealloc(tmem, TCL ? (uint32_t)BT : (uint32_t)tc::kCols);
   }
 }
 
@@ -1117,6 +1337,62 @@ __global__ void __launch_bounds__(128, 2) tc_inverse_kernel(int nmat, int n, con
   __syncthreads();
   tc::fence_after_sync();
   if (tid < 32) tc::tmem_dealloc(tmem, tc::kCols);
+}
+
+// Stand-alone multi-tile inverse (128 < n <= 512): blocks of BT = 128 MT threads, each with an FP32 work
+// matrix of BT x BT in ws; G^-1[a][b] = R[c(b) * BT + p_a] (gj_inverse_large) written column-major FP32.
+template <int BT>
+__host__ __device__ inline size_t tcl_inverse_smem() {
+  return 1024 + sizeof(float) * ((2 * (BT / 128) + 2) * (size_t)tc::kOperandFloats + 64 + 4 * tc::kPanel) +
+         sizeof(int) * 2 * BT + 64;
+}
+
+template <int MT>
+__global__ void __launch_bounds__(MT * 128, 1) tc_inverse_large_kernel(int nmat, int n, const double* __restrict__ J,
+                                                                       const double* __restrict__ hr0,
+                                                                       float* __restrict__ out, float* __restrict__ ws,
+                                                                       int* err) {
+  constexpr int BT = MT * 128;
+  extern __shared__ __align__(16) unsigned char tsm[];
+  __shared__ uint32_t tslot;
+  __shared__ __align__(8) unsigned long long mbar;
+  const int tid = threadIdx.x;
+  const uint32_t s0 = tc::smem_addr(tsm);
+  unsigned char* q = tsm + (((s0 + 1023u) & ~1023u) - s0);
+  tc::SmemL TL{};
+  TL.A = (float*)q;
+  TL.B = TL.A + 2 * MT * tc::kOperandFloats;
+  float* f = TL.B + 2 * tc::kOperandFloats;
+  TL.red = f; f += 32;
+  TL.redi = (int*)f; f += 32;
+  TL.prow = f; f += 4 * tc::kPanel;
+  TL.piv = (int*)f;
+  TL.colof = TL.piv + BT;
+  TL.mbar = &mbar;
+  if (tid < 32) tc::tmem_alloc(&tslot, BT);
+  if (tid == 0) tc::mbar_init(&mbar, 1);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tslot;
+  uint32_t phase = 0;
+  float* R = ws + (size_t)blockIdx.x * BT * BT;
+  for (int m = blockIdx.x; m < nmat; m += gridDim.x) {
+    if (!tc::gj_inverse_large<MT>(J + (size_t)m * n * n, n, n, hr0[m], R, TL, tmem, &phase)) {
+      if (tid == 0) atomicOr(err, kErrTensorCoreWait);
+      break;
+    }
+    float* o = out + (size_t)m * n * n;
+    for (int e = tid; e < n * n; e += BT) {
+      const int b = e / n, a = e - b * n;   // element (a, b) of G^-1
+      o[e] = R[(size_t)TL.colof[b] * BT + TL.piv[a]];
+    }
+    __syncthreads();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (tid < 32) tc::tmem_dealloc(tmem, BT);
 }
 
 // ---------------------------------------------------------------------------
@@ -1181,19 +1457,25 @@ size_t tc_block_smem(const MechLayout& L) {
 }
 
 template <int BT, bool TC>
+size_t block_smem(const MechLayout& L) {
+  if (!TC) return block_shared_bytes<BT>(L);
+  return BT == 128 ? tc_block_smem(L) : tcl_smem_bytes<BT>(L);
+}
+
+template <int BT, bool TC>
 cudaError_t block_setup(const MechLayout& L, size_t* smem, int* bps) {
-  *smem = TC ? tc_block_smem(L) : block_shared_bytes<BT>(L);
+  *smem = block_smem<BT, TC>(L);
+  if (*smem > 227 * 1024) return cudaErrorInvalidConfiguration;
   cudaError_t e = cudaFuncSetAttribute(block_kernel<BT, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
   if (e != cudaSuccess) return e;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, block_kernel<BT, TC>, BT, *smem);
-  if (TC && *bps > 2) *bps = 2;
+  // TMEM: 256 columns a block up to 128 components, BT columns above (512 on the SM)
+  const int tmem_cap = BT == 128 ? 2 : 512 / BT;
+  if (TC && *bps > tmem_cap) *bps = tmem_cap;
   return e;
 }
 
-int block_threads(const MechLayout& L) {
-  const int n = L.nc + 1;
-  return n <= 128 ? 128 : (n <= 256 ? 256 : 512);
-}
+int block_threads(const MechLayout& L) { return block_bt(L.nc + 1); }
 
 }  // namespace
 
@@ -1201,7 +1483,13 @@ cudaError_t upload_gear_block(const GearConsts& gc) { return cudaMemcpyToSymbol(
 
 size_t block_ws_bytes(const MechLayout& L) { return block_ws_doubles(L) * sizeof(double); }
 
-bool block_tc_eligible(const MechLayout& L) { return L.nc + 1 >= 32 && L.nc + 1 <= tc::kRows; }
+bool block_tc_eligible(const MechLayout& L) {
+  const int n = L.nc + 1;
+  if (n < 32 || n > kBlkMaxN) return false;
+  const int bt = block_bt(n);
+  const size_t smem = bt == 128 ? tc_block_smem(L) : (bt == 256 ? tcl_smem_bytes<256>(L) : tcl_smem_bytes<512>(L));
+  return smem <= 227 * 1024;
+}
 
 cudaError_t block_plan(const MechLayout& L, int sm_count, bool tc, long* nblocks) {
   if (L.nc + 1 > kBlkMaxN) return cudaErrorInvalidValue;
@@ -1209,7 +1497,9 @@ cudaError_t block_plan(const MechLayout& L, int sm_count, bool tc, long* nblocks
   size_t smem = 0;
   int bps = 0;
   const int bt = block_threads(L);
-  cudaError_t e = tc ? block_setup<128, true>(L, &smem, &bps)
+  cudaError_t e = tc ? (bt == 128 ? block_setup<128, true>(L, &smem, &bps)
+                                   : (bt == 256 ? block_setup<256, true>(L, &smem, &bps)
+                                                : block_setup<512, true>(L, &smem, &bps)))
                      : (bt == 128 ? block_setup<128, false>(L, &smem, &bps)
                                   : (bt == 256 ? block_setup<256, false>(L, &smem, &bps)
                                                : block_setup<512, false>(L, &smem, &bps)));
@@ -1229,7 +1519,12 @@ cudaError_t launch_block(const MechLayout& L, const unsigned char* mech_gmem, co
   const int bt = block_threads(L);
   if (tc) {
     if (!block_tc_eligible(L)) return cudaErrorInvalidValue;
-    block_kernel<128, true><<<(unsigned)g, 128, tc_block_smem(L), stream>>>(L, mech_gmem, o, a, ws, queue, err);
+    if (bt == 128)
+      block_kernel<128, true><<<(unsigned)g, 128, block_smem<128, true>(L), stream>>>(L, mech_gmem, o, a, ws, queue, err);
+    else if (bt == 256)
+      block_kernel<256, true><<<(unsigned)g, 256, block_smem<256, true>(L), stream>>>(L, mech_gmem, o, a, ws, queue, err);
+    else
+      block_kernel<512, true><<<(unsigned)g, 512, block_smem<512, true>(L), stream>>>(L, mech_gmem, o, a, ws, queue, err);
   } else if (bt == 128) {
     block_kernel<128, false><<<(unsigned)g, 128, block_shared_bytes<128>(L), stream>>>(L, mech_gmem, o, a, ws, queue, err);
   } else if (bt == 256) {
@@ -1245,10 +1540,35 @@ size_t tc_inverse_smem() {
          tc::kRows * sizeof(int);
 }
 
-cudaError_t launch_tc_inverse(int nmat, int n, const double* J, const double* hr0, float* out, int sm_count,
-                              int* err, cudaStream_t stream) {
-  if (n < 1 || n > tc::kRows || nmat < 0) return cudaErrorInvalidValue;
+size_t tc_inverse_ws_bytes(int n, int sm_count) {
+  if (n <= tc::kRows) return 0;
+  const size_t np = (size_t)block_bt(n);
+  return np * np * sizeof(float) * (size_t)sm_count * (512 / np);
+}
+
+template <int MT>
+cudaError_t launch_tc_inverse_large(int nmat, int n, const double* J, const double* hr0, float* out, float* ws,
+                                    int sm_count, int* err, cudaStream_t stream) {
+  constexpr int BT = MT * 128;
+  const size_t smem = tcl_inverse_smem<BT>();
+  cudaError_t e =
+      cudaFuncSetAttribute(tc_inverse_large_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const long cap = (long)sm_count * (512 / BT);
+  const long g = cap < nmat ? cap : nmat;
+  tc_inverse_large_kernel<MT><<<(unsigned)g, BT, smem, stream>>>(nmat, n, J, hr0, out, ws, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tc_inverse(int nmat, int n, const double* J, const double* hr0, float* out, float* ws,
+                              int sm_count, int* err, cudaStream_t stream) {
+  if (n < 1 || n > kBlkMaxN || nmat < 0) return cudaErrorInvalidValue;
   if (nmat == 0) return cudaSuccess;
+  if (n > tc::kRows) {
+    if (!ws) return cudaErrorInvalidValue;
+    return n <= 256 ? launch_tc_inverse_large<2>(nmat, n, J, hr0, out, ws, sm_count, err, stream)
+                    : launch_tc_inverse_large<4>(nmat, n, J, hr0, out, ws, sm_count, err, stream);
+  }
   size_t smem = tc_inverse_smem();
   if (smem < 80 * 1024) smem = 80 * 1024;   // at most two blocks per SM: 256 TMEM columns each
   cudaError_t e = cudaFuncSetAttribute(tc_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -65,10 +65,12 @@ cudaError_t block_plan(const MechLayout& L, int sm_count, bool tc, long* nblocks
 cudaError_t launch_block(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
                          const StepArgs& a, double* ws, long nblocks, int* queue, bool tc, int* err,
                          cudaStream_t stream);
-// G^-1 (FP32, column-major) of G = I - hr0[m] J[m] for nmat column-major FP64 Jacobians of order n <= 128,
-// by the tensor-core Gauss-Jordan inverse of the mixed-precision block form.
-cudaError_t launch_tc_inverse(int nmat, int n, const double* J, const double* hr0, float* out, int sm_count,
-                              int* err, cudaStream_t stream);
+// G^-1 (FP32, column-major) of G = I - hr0[m] J[m] for nmat column-major FP64 Jacobians of order n <= 512,
+// by the tensor-core Gauss-Jordan inverses of the mixed-precision block form (one 128-row tile up to 128,
+// the in-place multi-tile inverse above); ws: tc_inverse_ws_bytes(n, sm_count) (unused up to 128).
+size_t tc_inverse_ws_bytes(int n, int sm_count);
+cudaError_t launch_tc_inverse(int nmat, int n, const double* J, const double* hr0, float* out, float* ws,
+                              int sm_count, int* err, cudaStream_t stream);
 cudaError_t launch_rhs_block(const MechLayout& L, const unsigned char* mech_gmem, long ncells, const double* y,
                              double* dy, long ld, double p, int energy, double* qr, double* ws, long nblocks,
                              cudaStream_t stream);

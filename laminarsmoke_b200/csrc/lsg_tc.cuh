@@ -383,5 +383,233 @@ __device__ __noinline__ bool gj_inverse(const double* __restrict__ J, int n, dou
   return ok;
 }
 
+// ---------------------------------------------------------------------------
+// Multi-tile inverse for 128 < n <= 512 components (MT = 2 or 4 row tiles of
+// 128, MT x 128 threads, thread i owns row i).  The matrix no longer fits on
+// the SM, so it is inverted in place in global memory (L2), FP32, column-major
+// with leading dimension Np = 128 MT: R[c * Np + i].
+//
+// In-place Gauss-Jordan with implicit row pivoting: when panel column c is
+// eliminated with pivot row p_c, its storage slot takes over the augmented
+// column of p_c, which before the panel is the unit vector e_{p_c} and after
+// it e_{p_c} + W[:, k] (k: c's place in the panel).  Every other slot
+// (columns still to eliminate, and the slots already taken over) gets the
+// panel's rank-32 update R + W R[P].  After the last panel, slot s holds
+// column p_s of E G^-1 (E: the pivot permutation, row p_a of E G^-1 is row a
+// of G^-1), so
+//     G^-1[a][b] = R[c(b) * Np + p_a]      (c(b): the column row b was pivot of)
+// and a solve is x_a = y_{p_a} with y = R r~, r~_s = r_{p_s}.
+//
+// Schedule per panel: the 32 panel columns are read into registers and
+// eliminated on the CUDA cores as in gj_inverse (pivot search over all rows
+// through shared memory); the coefficients W (Np x 32) go to shared memory as
+// split-TF32 A operands, one per row tile.  Then the columns are updated in
+// chunks of 128: each thread stores its row of the chunk into its warpgroup's
+// 128 TMEM columns (warpgroup g = row tile g), the pivot rows write R[P] for
+// the chunk as the B operand, one thread issues the MT x 4 x 3 MMAs
+// (M = 128, N = 128, K = 8 each), and the rows are read back and stored, the
+// panel's own slots replaced by e_{p_c} + W[:, k].  TMEM: MT x 128 columns.
+// ---------------------------------------------------------------------------
+struct SmemL {
+  float* A;       // MT x {hi, lo} operands of 128 x 32 (16 KB each), 1024-byte aligned
+  float* B;       // {hi, lo} operands of 128 (N) x 32 (K)
+  float* red;     // [2][16] warp maxima
+  int* redi;      // [2][16]
+  float* prow;    // [2][2 * kPanel]
+  int* piv;       // [Np] pivot row of column c (persistent: the solves use it)
+  int* colof;     // [Np] column row i was pivot of, -1 none (persistent)
+  unsigned long long* mbar;
+};
+
+template <int MT>
+__device__ __noinline__ bool gj_inverse_large(const double* __restrict__ J, int jld, int n, double hr0,
+                                              float* __restrict__ R, const SmemL& S, uint32_t tmem,
+                                              uint32_t* phase) {
+  constexpr int BT = MT * 128, NP = BT, NW = BT / 32;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int wg = tid >> 7, r128 = tid & 127;
+  const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+  const uint32_t col_base = (uint32_t)(wg * 128);
+  // G = I - hr0 J, padded with the identity, row tid of every column
+#pragma unroll 4
+  for (int c = 0; c < NP; ++c) {
+    float g;
+    if (tid < n && c < n) {
+      double x = -hr0 * J[(long)c * jld + tid];
+      if (c == tid) x += 1.;
+      g = (float)x;
+    } else {
+      g = c == tid ? 1.f : 0.f;
+    }
+    R[(long)c * NP + tid] = g;
+  }
+  S.colof[tid] = -1;
+  S.piv[tid] = tid;
+  bool pivoted = false;
+  bool ok = true;
+  const int npanels = (n + kPanel - 1) / kPanel;
+  const int nchunks = (n + 127) / 128;
+#pragma unroll 1
+  for (int pn = 0; pn < npanels; ++pn) {
+    const int k0 = pn * kPanel;
+    __syncthreads();   // the previous panel's stores of R are visible to the block
+    float v[32], u[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = R[(long)(k0 + k) * NP + tid];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) u[k] = 0.f;
+    int mine = -1;
+#pragma unroll
+    for (int c = 0; c < kPanel; ++c) {
+      const int buf = c & 1;
+      float best = pivoted ? -1.f : fabsf(v[c]);
+      if (best != best) best = 0.f;
+      int brow = tid;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+        const int orow = __shfl_xor_sync(0xffffffffu, brow, off);
+        if (ob > best || (ob == best && orow < brow)) { best = ob; brow = orow; }
+      }
+      if (lane == 0) { S.red[buf * 16 + warp] = best; S.redi[buf * 16 + warp] = brow; }
+      __syncthreads();
+      float pb = S.red[buf * 16];
+      int prow_i = S.redi[buf * 16];
+#pragma unroll
+      for (int w = 1; w < NW; ++w) {
+        const float ob = S.red[buf * 16 + w];
+        const int orow = S.redi[buf * 16 + w];
+        if (ob > pb || (ob == pb && orow < prow_i)) { pb = ob; prow_i = orow; }
+      }
+      float* pr = S.prow + buf * 2 * kPanel;
+      if (tid == prow_i) {
+        const float a = v[c];
+        const float inv = a != 0.f ? 1.f / a : 0.f;
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+          if (k > c) v[k] *= inv;
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+          if (k < c) u[k] *= inv;
+        u[c] = inv - 1.f;
+        v[c] = 1.f;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          if (k > c) pr[k] = v[k];
+          if (k <= c) pr[kPanel + k] = u[k] + (k == c ? 1.f : 0.f);
+        }
+        pivoted = true;
+        mine = c;
+      }
+      __syncthreads();
+      if (tid != prow_i) {
+        const float m = v[c];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          if (k > c) v[k] = fmaf(-m, pr[k], v[k]);
+          if (k <= c) u[k] = fmaf(-m, pr[kPanel + k], u[k]);
+        }
+        v[c] = 0.f;
+      }
+    }
+    if (mine >= 0) {
+      S.colof[tid] = k0 + mine;
+      S.piv[k0 + mine] = tid;
+    }
+    // A operand of row tile wg: this row's coefficients, split into TF32 hi and lo
+    {
+      char* ah = (char*)(S.A + (size_t)(2 * wg) * kOperandFloats);
+      char* al = (char*)(S.A + (size_t)(2 * wg + 1) * kOperandFloats);
+#pragma unroll
+      for (int kg = 0; kg < 8; ++kg) {
+        float4 hi, lo;
+        float* h4 = &hi.x;
+        float* l4 = &lo.x;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float x = u[kg * 4 + e];
+          const float xh = __uint_as_float(to_tf32(x));
+          h4[e] = xh;
+          l4[e] = __uint_as_float(to_tf32(x - xh));
+        }
+        *(float4*)(ah + op_offset(r128, kg * 4)) = hi;
+        *(float4*)(al + op_offset(r128, kg * 4)) = lo;
+      }
+    }
+    float* const B_hi = S.B;
+    float* const B_lo = S.B + kOperandFloats;
+#pragma unroll 1
+    for (int ch = 0; ch < nchunks; ++ch) {
+      const int c0 = ch * 128;
+      // the chunk of this row into TMEM; the pivot rows also write it as the B operand
+#pragma unroll 1
+      for (int q = 0; q < 4; ++q) {
+        float r[32];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) r[k] = R[(long)(c0 + q * 32 + k) * NP + tid];
+        if (mine >= 0) {
+#pragma unroll
+          for (int k = 0; k < 32; ++k) {
+            const float x = r[k];
+            const float xh = __uint_as_float(to_tf32(x));
+            const uint32_t off = op_offset(q * 32 + k, mine);
+            *(float*)((char*)B_hi + off) = xh;
+            *(float*)((char*)B_lo + off) = __uint_as_float(to_tf32(x - xh));
+          }
+        }
+        tmem_st32(tmem + lane_base + col_base + (uint32_t)(q * 32), r);
+      }
+      tmem_wait_st();
+      fence_async_smem();
+      fence_before_sync();
+      __syncthreads();
+      if (tid == 0) {
+        fence_after_sync();
+        const uint32_t idesc = idesc_tf32(128);
+        const uint32_t bh = smem_addr(B_hi), bl = smem_addr(B_lo);
+#pragma unroll 1
+        for (int g = 0; g < MT; ++g) {
+          const uint32_t d = tmem + (uint32_t)(g * 128);
+          const uint32_t ah = smem_addr(S.A + (size_t)(2 * g) * kOperandFloats);
+          const uint32_t al = smem_addr(S.A + (size_t)(2 * g + 1) * kOperandFloats);
+#pragma unroll
+          for (int s = 0; s < kPanel / 8; ++s) {
+            const uint32_t ko = (uint32_t)s * 256;
+            mma_tf32(d, smem_desc(ah + ko, 128, 1024), smem_desc(bh + ko, 128, 1024), idesc, 1);
+            mma_tf32(d, smem_desc(ah + ko, 128, 1024), smem_desc(bl + ko, 128, 1024), idesc, 1);
+            mma_tf32(d, smem_desc(al + ko, 128, 1024), smem_desc(bh + ko, 128, 1024), idesc, 1);
+          }
+        }
+        mma_commit(S.mbar);
+      }
+      const bool done = mbar_wait(S.mbar, *phase);
+      *phase ^= 1u;
+      if (__syncthreads_or(!done)) ok = false;
+      fence_after_sync();
+      if (!ok) break;
+      // back to R; the panel's slots take over the augmented columns of their pivot rows
+#pragma unroll 1
+      for (int q = 0; q < 4; ++q) {
+        float r[32];
+        tmem_ld32(tmem + lane_base + col_base + (uint32_t)(q * 32), r);
+        const bool panel = c0 + q * 32 == k0;   // these 32 columns are the panel's (k0 is a multiple of 32)
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          const int col = c0 + q * 32 + k;
+          const float x = panel ? u[k] + (S.piv[col] == tid ? 1.f : 0.f) : r[k];
+          R[(long)col * NP + tid] = x;
+        }
+      }
+      fence_before_sync();
+      __syncthreads();   // every warp has read its TMEM columns before the next chunk overwrites them
+      fence_after_sync();
+    }
+    if (!ok) break;
+  }
+  __syncthreads();
+  return ok;
+}
+
 }  // namespace tc
 }  // namespace lsg

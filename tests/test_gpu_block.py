@@ -48,15 +48,19 @@ def _run(data, Y, T, dt, precision=0, **kw):
         (Yo, To, Qo, sto, cnt)
 
 
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
 @pytest.mark.parametrize("k,ncells", [(30, 512), (150, 64), (300, 16)], ids=["n45", "n165", "n315"])
-def test_block_padded_parity(cuda, k, ncells):
+def test_block_padded_parity(cuda, k, ncells, precision):
+    """FP64 block form, and the mixed-precision form: the tensor-core inverse of one 128-row tile (45
+    components) or the in-place multi-tile inverse (165: two row tiles, 315: four), refined on the FP64
+    residual."""
     data, Y, T = _padded_states(k, ncells, seed=11)
-    (Yg, Tg, Qg, stg, nsg), (Yo, To, Qo, sto, cnt) = _run(data, Y, T, 1e-5)
+    (Yg, Tg, Qg, stg, nsg), (Yo, To, Qo, sto, cnt) = _run(data, Y, T, 1e-5, precision=precision)
     np.testing.assert_array_equal(stg, sto)
     rel_T = np.abs(Tg - To) / To
     abs_Y = np.abs(Yg - Yo).max(axis=1)
     same = nsg == cnt[:, 0]
-    print(f"n={k + 15}: max rel T err {rel_T.max():.3e}, max abs Y err {abs_Y.max():.3e}, "
+    print(f"n={k + 15} precision={precision}: max rel T err {rel_T.max():.3e}, max abs Y err {abs_Y.max():.3e}, "
           f"cells within Y bound {np.mean(abs_Y <= ATOL_Y):.4f}, identical step counts {same.mean():.4f}")
     assert rel_T.max() <= RTOL_T
     # Rounding-level differences (tree-ordered sums over up to 315 components) send a few cells down a
@@ -121,7 +125,8 @@ def test_block_synthetic_120_step(cuda):
 
 
 
-def test_block_synthetic_120p_step(cuda):
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_block_synthetic_120p_step(cuda, precision):
     """One step of the physically bounded 120-species / 800-reaction synthetic chemistry (barriers no lower
     than the endothermicity, rate constants at the collision limit; T ~ U[800, 2400] K, dt = 5e-6 s,
     thousands of BDF steps per cell) against the oracle.  At the default tolerances rounding-level
@@ -133,10 +138,11 @@ def test_block_synthetic_120p_step(cuda):
     A, _ = blob.unpack(data)
     Y, T = cells.synthetic_mixing(species, A["mw"], 32, seed=3, t_range=(800.0, 2400.0))
     for rtol, atol in ((1e-7, 1e-12), (1e-10, 1e-16)):
-        (Yg, Tg, Qg, stg, nsg), (Yo, To, Qo, sto, cnt) = _run(data, Y, T, 5e-6, rtol=rtol, atol=atol)
+        (Yg, Tg, Qg, stg, nsg), (Yo, To, Qo, sto, cnt) = _run(data, Y, T, 5e-6, precision=precision, rtol=rtol,
+                                                              atol=atol)
         rel_T = np.abs(Tg - To) / To
         abs_Y = np.abs(Yg - Yo).max(axis=1)
-        print(f"syn120p rtol {rtol:g}: statuses equal {np.mean(stg == sto):.3f}, max rel T err {rel_T.max():.3e}, "
+        print(f"syn120p precision={precision} rtol {rtol:g}: steps/cell {nsg.mean():.0f}, statuses equal {np.mean(stg == sto):.3f}, max rel T err {rel_T.max():.3e}, "
               f"max abs Y err {abs_Y.max():.3e}, cells within 1e-9 {np.mean(abs_Y <= ATOL_Y):.3f}, "
               f"steps {cnt[:, 0].mean():.0f}", flush=True)
     np.testing.assert_array_equal(stg, sto)

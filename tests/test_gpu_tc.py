@@ -27,27 +27,36 @@ def _tc_inverse(ctx, Js, hs, cuda):
     return [x.T.astype(np.float64) for x in inv.cpu().numpy()]
 
 
-@pytest.mark.parametrize("n", [32, 45, 64, 100, 121, 128])
+@pytest.mark.parametrize("n", [32, 45, 64, 100, 121, 128, 129, 200, 256, 301, 501, 512])
 def test_tc_inverse_random(cuda, h2co, n):
+    """Up to 128 one 128-row tile in TMEM; above, the in-place multi-tile inverse in global memory.  G is
+    kept well conditioned (|h J| <= 0.5 in norm) so that the bound is the FP32 rounding of the
+    elimination, which grows with n."""
     from laminarsmoke_b200 import lsg
     ctx = lsg.ReactionStep(lsg.Mechanism(h2co[0]))
     rng = np.random.default_rng(n)
-    Js = [rng.normal(size=(n, n)) for _ in range(40)]
-    hs = rng.uniform(0.01, 0.05, 40)
+    nm = 40 if n <= 128 else 12
+    Js = [rng.normal(size=(n, n)) for _ in range(nm)]
+    hs = rng.uniform(0.2, 1.0, nm) * 0.5 / (2.0 * np.sqrt(n))
+    tol = 1e-5 if n <= 128 else 4e-5
+    worst = 0.0
     for X, J, h in zip(_tc_inverse(ctx, Js, hs, cuda), Js, hs):
         G = np.eye(n) - h * J
         Xe = np.linalg.inv(G)
-        assert np.abs(X - Xe).max() <= 1e-5 * np.abs(Xe).max()
-        assert np.abs(X @ G - np.eye(n)).max() <= 1e-5
+        worst = max(worst, float(np.abs(X @ G - np.eye(n)).max()))
+        assert np.abs(X - Xe).max() <= tol * np.abs(Xe).max()
+        assert np.abs(X @ G - np.eye(n)).max() <= tol
+    print(f"n={n}: worst |X G - I| {worst:.2e}")
 
 
-def test_tc_inverse_chemistry_jacobians(cuda):
-    """Finite-difference Jacobians of H2/CO states padded to 121 components (condition numbers 1e4 to
-    1e8): entrywise error of the FP32 inverse against the FP64 one, relative to its largest entry."""
+@pytest.mark.parametrize("pad", [106, 286], ids=["n121", "n301"])
+def test_tc_inverse_chemistry_jacobians(cuda, pad):
+    """Finite-difference Jacobians of H2/CO states padded to 121 or 301 components (condition numbers 1e4
+    to 1e8): entrywise error of the FP32 inverse against the FP64 one, relative to its largest entry."""
     from laminarsmoke_b200 import lsg, mech
     from laminarsmoke_b200.mech import blob
     from oracle.oracle import OracleMechanism
-    data, species = mech.load("h2co+106")
+    data, species = mech.load(f"h2co+{pad}")
     A, _ = blob.unpack(data)
     om = OracleMechanism(data)
     Y, T = cells.h2co_mixing(species[:14], A["mw"][:14], 8, seed=1)
@@ -68,7 +77,8 @@ def test_tc_inverse_chemistry_jacobians(cuda):
         err = np.abs(X - Xe).max() / np.abs(Xe).max()
         res = np.abs(X @ G - np.eye(J.shape[0])).max()
         worst, worst_res = max(worst, err), max(worst_res, res)
-    print(f"worst entrywise relative error of the split-TF32 inverse {worst:.2e}, worst |X G - I| {worst_res:.2e}")
+    print(f"n={J.shape[0]}: worst entrywise relative error of the split-TF32 inverse {worst:.2e}, "
+          f"worst |X G - I| {worst_res:.2e}")
     assert worst <= 1e-4
     # the simplified Newton iteration with X in place of G^-1 contracts while |I - X G| < 1
     assert worst_res <= 0.5

@@ -440,6 +440,7 @@ struct GearBlock {
   bool tc_failed;
   double tc_hr0;    // hr0 of the matrix the current inverse belongs to
   bool tc_fp64;     // the refinement stalled on this matrix: it was refactorised by the FP64 LU
+  bool tc_sticky;   // ... and the cell's later matrices go to the FP64 LU directly
   // more than 128 components (TCL): the inverse in global memory (lsg_tc.cuh gj_inverse_large), its
   // pivots in shared memory; part/ysm: the solves' partial sums (shared)
   static constexpr bool TCL = TC && BT > 128;
@@ -528,6 +529,12 @@ struct GearBlock {
   // Column storage: G(i, j) at G[j * n + i].
   __device__ void build_and_factorize(double hr0) {
     if constexpr (TC) {
+      if (tc_sticky) {   // this cell's matrices defeated the FP32 inverse before
+        build_and_factorize_fp64(hr0);
+        tc_hr0 = hr0;
+        tc_fp64 = true;
+        return;
+      }
       // G^-1 in FP32 by the tensor-core Gauss-Jordan inverse (lsg_tc.cuh)
       if constexpr (TCL) {
         if (!tc::gj_inverse_large<BT / 128>(J, jld, ne, hr0, RL, TL, tmem, &tc_phase)) tc_failed = true;
@@ -670,22 +677,24 @@ struct GearBlock {
 
   // Mixed-precision solve: x = X r, then refinement sweeps x += X (r - G x) on the FP64 residual until
   // the weighted RMS of a correction is below kBlkRefineTol (the Newton test compares such norms with 1), at
-  // most kBlkRefineMax sweeps.  A sweep that does not halve the correction means |I - X G| is too close to
-  // 1 for this matrix (FP32 cannot hold its conditioning): G is then refactorised by the FP64 LU, which
-  // serves every solve until the next factorisation.
+  // most kBlkRefineMax sweeps.  Each sweep must at least halve the weighted norm of the residual (the
+  // first against r): otherwise X is no usable inverse of G (FP32 cannot hold this matrix's conditioning,
+  // and a correction X res can be small while the residual is not), G is refactorised by the FP64 LU, and
+  // the cell's remaining factorisations stay FP64 (tc_sticky).
   __device__ double solve(double xl) {
     if constexpr (TC) {
       if (!tc_fp64) {
         double x = apply_inverse(xl);
-        double prev = 0.;
+        double prev = error_control(xl);
         bool converged = false;
         for (int s = 0; s < kBlkRefineMax; ++s) {
-          const double d = apply_inverse(xl - apply_g(x, tc_hr0));
+          const double res = xl - apply_g(x, tc_hr0);
+          const double rr = error_control(res);
+          if (!(rr <= 0.5 * prev || rr == 0.)) break;   // (a NaN residual breaks too)
+          prev = rr;
+          const double d = apply_inverse(res);
           x += d;
-          const double nd = error_control(d);
-          if (nd <= kBlkRefineTol) { converged = true; break; }
-          if (s > 0 && !(nd <= 0.5 * prev)) break;
-          prev = nd;
+          if (error_control(d) <= kBlkRefineTol) { converged = true; break; }
         }
         if (converged) {
           ++cnt[CNT_SOLVE];
@@ -694,6 +703,7 @@ struct GearBlock {
         build_and_factorize_fp64(tc_hr0);   // the same matrix: not a factorisation of the method
         --cnt[CNT_FACT];
         tc_fp64 = true;
+        tc_sticky = true;
       }
       return solve_fp64(xl);
     } else {
@@ -1231,6 +1241,7 @@ __global__ void __launch_bounds__(BT, TC ? (BT == 128 ? 2 : 1) : (BT == 128 ? 4 
       g.tc_failed = false;
       g.tc_hr0 = 0.;
       g.tc_fp64 = false;
+      g.tc_sticky = false;
       g.L = &L;
       g.M = M;
       g.W = W;

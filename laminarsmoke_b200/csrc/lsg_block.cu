@@ -99,7 +99,7 @@ __host__ __device__ inline int block_bt(int n) { return n <= 128 ? 128 : (n <= 2
 // dimension Np = the block's threads, the FP64 fallback factors G (n x n), the FP32 inverse (Np x Np),
 // the Nordsieck arrays Z and V (8 Np each: they leave shared memory to the inverse's operands), caches.
 __host__ __device__ inline size_t round32(size_t x) { return (x + 31) & ~(size_t)31; }
-__host__ __device__ inline size_t block_ws_head_doubles(const MechLayout& L) {
+__host__ __device__ inline size_t block_ws_doubles(const MechLayout& L) {
   const size_t n = L.nc + 1;
   const size_t caches = 2 * (size_t)L.nr + 2 * (size_t)(L.n_fo > 0 ? L.n_fo : 1) + 8;
   const size_t fp64 = round32(2 * n * n + caches);
@@ -108,13 +108,6 @@ __host__ __device__ inline size_t block_ws_head_doubles(const MechLayout& L) {
   const size_t tcl = round32(np * np + round32(n * n) + np * np / 2 + 16 * np + caches);
   return fp64 > tcl ? fp64 : tcl;
 }
-// ... followed (mixed-precision form) by the FP64 inverse of the fallback, Np x Np
-__host__ __device__ inline size_t block_ws_doubles(const MechLayout& L) {
-  const size_t np = (size_t)block_bt(L.nc + 1);
-  return block_ws_head_doubles(L) + np * np;
-}
-
-constexpr int GearFallbackRows = 16;   // panel width of the FP64 fallback inverse (gj_inverse_fp64)
 
 // Shared memory of the mixed-precision form above 128 components: a persistent head (solve vector,
 // reductions, LU pivots, the inverse's pivots, TMEM slot, MMA barrier), then, 1024-byte aligned, one
@@ -129,10 +122,8 @@ __host__ __device__ inline size_t tcl_union_bytes(const MechLayout& L) {
   const size_t rhs = sizeof(double) * (3 * (size_t)L.nc + L.nr);
   const size_t inv = sizeof(float) * ((2 * (BT / 128) + 2) * (size_t)tc::kOperandFloats + 64 + 4 * tc::kPanel);
   const size_t sol = sizeof(double) * 5 * (size_t)BT;
-  const size_t fb = sizeof(double) * GearFallbackRows * (size_t)BT;   // gj_inverse_fp64's staged pivot rows
   size_t m = rhs > inv ? rhs : inv;
-  m = m > sol ? m : sol;
-  return m > fb ? m : fb;
+  return m > sol ? m : sol;
 }
 template <int BT>
 __host__ __device__ inline size_t tcl_smem_bytes(const MechLayout& L) {
@@ -457,12 +448,6 @@ struct GearBlock {
   tc::SmemL TL;
   double* part;
   double* ysm;
-  // the FP64 inverse of the fallback (gj_inverse_fp64): global, column-major, leading dimension BT; its
-  // pivots (shared) and the staged pivot rows of a panel (shared, 16 x n)
-  double* R64;
-  int* gpiv;
-  int* gcolof;
-  double* gP;
   double* karr;
   double* ukeq;
   double* kinf;
@@ -545,8 +530,7 @@ struct GearBlock {
   __device__ void build_and_factorize(double hr0) {
     if constexpr (TC) {
       if (tc_sticky) {   // this cell's matrices defeated the FP32 inverse before
-        gj_inverse_fp64(hr0);
-        ++cnt[CNT_FACT];
+        build_and_factorize_fp64(hr0);
         tc_hr0 = hr0;
         tc_fp64 = true;
         return;
@@ -691,132 +675,6 @@ struct GearBlock {
     return s0;
   }
 
-  // FP64 in-place Gauss-Jordan inverse of G = I - hr0 J (the fallback of the mixed-precision form), the
-  // scheme of tc::gj_inverse_large on CUDA cores: panels of 16 columns eliminated in registers (pivot:
-  // largest magnitude among the rows not yet pivoted, lowest row on ties), the panel's pivot rows staged
-  // in shared memory, then every other column c < n of every row i < n updated once per panel,
-  // R[i][c] += sum_k W[i][k] R[p_k][c], and the panel's slots replaced by e_{p_k} + W[:, k].  Columns and
-  // rows beyond n are the identity and stay so.  G^-1[a][b] = R64[c(b) BT + p_a].
-  __device__ void gj_inverse_fp64(double hr0) {
-    const int n = ne;
-    for (int c = 0; c < BT; ++c) {
-      double x = c == tid ? 1. : 0.;
-      if (tid < n && c < n) x -= hr0 * J[(long)c * jld + tid];
-      R64[(long)c * BT + tid] = x;
-    }
-    gcolof[tid] = -1;
-    gpiv[tid] = tid;
-    bool pivoted = false;
-    const int npanels = (n + GearFallbackRows - 1) / GearFallbackRows;
-    for (int pn = 0; pn < npanels; ++pn) {
-      const int k0 = pn * GearFallbackRows;
-      __syncthreads();
-      double v[GearFallbackRows], u[GearFallbackRows];
-#pragma unroll
-      for (int k = 0; k < GearFallbackRows; ++k) {
-        v[k] = R64[(long)(k0 + k) * BT + tid];
-        u[k] = 0.;
-      }
-      int mine = -1;
-#pragma unroll
-      for (int c = 0; c < GearFallbackRows; ++c) {
-        double best = pivoted ? -1. : fabs(v[c]);
-        if (best != best) best = 0.;
-        int brow = tid;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          const double ob = __shfl_xor_sync(kFull, best, off);
-          const int orow = __shfl_xor_sync(kFull, brow, off);
-          if (ob > best || (ob == best && orow < brow)) { best = ob; brow = orow; }
-        }
-        if ((tid & 31) == 0) { W.red[tid >> 5] = best; W.ival[tid >> 5] = brow; }
-        __syncthreads();
-        double pb = W.red[0];
-        int pr = W.ival[0];
-#pragma unroll 4
-        for (int w = 1; w < BT / 32; ++w) {
-          const double ob = W.red[w];
-          const int orow = W.ival[w];
-          if (ob > pb || (ob == pb && orow < pr)) { pb = ob; pr = orow; }
-        }
-        double* prow = W.X + (c & 1) * 2 * GearFallbackRows;   // the pivot row's panel values and coefficients
-        __syncthreads();   // every thread has read W.red before the next column rewrites it
-        if (tid == pr) {
-          const double a = v[c];
-          const double inv = a != 0. ? 1. / a : 0.;
-#pragma unroll
-          for (int k = 0; k < GearFallbackRows; ++k)
-            if (k > c) v[k] *= inv;
-#pragma unroll
-          for (int k = 0; k < GearFallbackRows; ++k)
-            if (k < c) u[k] *= inv;
-          u[c] = inv - 1.;
-          v[c] = 1.;
-#pragma unroll
-          for (int k = 0; k < GearFallbackRows; ++k) {
-            if (k > c) prow[k] = v[k];
-            if (k <= c) prow[GearFallbackRows + k] = u[k] + (k == c ? 1. : 0.);
-          }
-          pivoted = true;
-          mine = c;
-        }
-        __syncthreads();
-        if (tid != pr) {
-          const double m = v[c];
-#pragma unroll
-          for (int k = 0; k < GearFallbackRows; ++k) {
-            if (k > c) v[k] = fma(-m, prow[k], v[k]);
-            if (k <= c) u[k] = fma(-m, prow[GearFallbackRows + k], u[k]);
-          }
-          v[c] = 0.;
-        }
-      }
-      if (mine >= 0) {
-        gcolof[tid] = k0 + mine;
-        gpiv[k0 + mine] = tid;
-      }
-      __syncthreads();
-      // the panel's pivot rows, restricted to the columns below n, into shared memory
-      for (int e = tid; e < GearFallbackRows * n; e += BT) {
-        const int k = e / n, c = e - k * n;
-        gP[e] = R64[(long)c * BT + gpiv[k0 + k]];
-      }
-      __syncthreads();
-      if (tid < n) {
-#pragma unroll 2
-        for (int c = 0; c < n; ++c) {
-          if (c >= k0 && c < k0 + GearFallbackRows) continue;
-          double acc = R64[(long)c * BT + tid];
-#pragma unroll
-          for (int k = 0; k < GearFallbackRows; ++k) acc = fma(u[k], gP[k * n + c], acc);
-          R64[(long)c * BT + tid] = acc;
-        }
-#pragma unroll
-        for (int k = 0; k < GearFallbackRows; ++k) {
-          const int c = k0 + k;
-          if (c < n) R64[(long)c * BT + tid] = u[k] + (gpiv[c] == tid ? 1. : 0.);
-        }
-      }
-    }
-    __syncthreads();
-  }
-
-  // x = G^-1 r with the FP64 inverse: x_a = y_{p_a}, y = R64 r~, r~_s = r_{p_s}
-  __device__ double apply_inverse_fp64(double rl) {
-    const int n = ne;
-    W.X[tid] = 0.;
-    __syncthreads();
-    const int sl = gcolof[tid];
-    if (tid < n && sl >= 0 && sl < n) W.X[sl] = rl;
-    __syncthreads();
-    const double y = gemv_block<BT, double>(R64, n, W.X, part);
-    ysm[tid] = y;
-    __syncthreads();
-    const double x = tid < n ? ysm[gpiv[tid]] : 0.;
-    __syncthreads();
-    return x;
-  }
-
   // Mixed-precision solve: x = X r, then refinement sweeps x += X (r - G x) on the FP64 residual until
   // the weighted RMS of a correction is below kBlkRefineTol (the Newton test compares such norms with 1), at
   // most kBlkRefineMax sweeps.  Each sweep must at least halve the weighted norm of the residual (the
@@ -842,12 +700,12 @@ struct GearBlock {
           ++cnt[CNT_SOLVE];
           return x;
         }
-        gj_inverse_fp64(tc_hr0);   // the same matrix: not a factorisation of the method
+        build_and_factorize_fp64(tc_hr0);   // the same matrix: not a factorisation of the method
+        --cnt[CNT_FACT];
         tc_fp64 = true;
         tc_sticky = true;
       }
-      ++cnt[CNT_SOLVE];
-      return apply_inverse_fp64(xl);
+      return solve_fp64(xl);
     } else {
       return solve_fp64(xl);
     }
@@ -1272,10 +1130,6 @@ __global__ void __launch_bounds__(BT, TC ? (BT == 128 ? 2 : 1) : (BT == 128 ? 4 
   double* part = nullptr;
   double* ysm = nullptr;
   uint32_t* tslot = nullptr;
-  double* R64 = TC ? ws + block_ws_head_doubles(L) : nullptr;
-  int* gpiv = nullptr;
-  int* gcolof = nullptr;
-  double* gP = nullptr;
   if constexpr (TCL) {
     jld = BT;
     Gp = ws + (size_t)BT * BT;
@@ -1312,9 +1166,6 @@ __global__ void __launch_bounds__(BT, TC ? (BT == 128 ? 2 : 1) : (BT == 128 ? 4 
     TL.prow = f;
     part = (double*)un;
     ysm = part + 4 * BT;
-    gP = (double*)un;
-    gpiv = TL.piv;
-    gcolof = TL.colof;
   } else {
     double* p = (double*)bsm;
     W.Z = p; p += 8 * BT;
@@ -1352,11 +1203,6 @@ __global__ void __launch_bounds__(BT, TC ? (BT == 128 ? 2 : 1) : (BT == 128 ? 4 
     TS.redi = (int*)q; q += 8 * sizeof(int);
     TS.prow = (float*)q; q += 4 * tc::kPanel * sizeof(float);
     TS.pivot_of_row = (int*)q;
-    gpiv = TS.pivot_of_row + tc::kRows;
-    gcolof = gpiv + tc::kRows;
-    gP = (double*)TS.op;   // the FP32 inverse's space, dead once the fallback runs
-    part = (double*)TS.op;
-    ysm = part + 4 * BT;
     if (tid < 32) tc::tmem_alloc(TS.tmem_slot, tc::kCols);
     if (tid == 0) tc::mbar_init(TS.mbar, 1);
     tc::fence_before_sync();
@@ -1406,10 +1252,6 @@ __global__ void __launch_bounds__(BT, TC ? (BT == 128 ? 2 : 1) : (BT == 128 ? 4 
       g.TL = TL;
       g.part = part;
       g.ysm = ysm;
-      g.R64 = R64;
-      g.gpiv = gpiv;
-      g.gcolof = gcolof;
-      g.gP = gP;
       g.karr = karr;
       g.ukeq = g.karr + L.nr;
       g.kinf = g.ukeq + L.nr;
@@ -1621,7 +1463,7 @@ namespace {
 size_t tc_block_smem(const MechLayout& L) {
   const size_t base = block_shared_bytes<128>(L) + 1024;   // + the alignment of the operands
   const size_t s = base + 4 * tc::kOperandFloats * sizeof(float) + 32 + 16 * sizeof(float) +
-                   4 * tc::kPanel * sizeof(float) + 3 * tc::kRows * sizeof(int);
+                   4 * tc::kPanel * sizeof(float) + tc::kRows * sizeof(int);
   return s < 80 * 1024 ? 80 * 1024 : s;
 }
 

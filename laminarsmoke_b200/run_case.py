@@ -15,6 +15,11 @@ species, the block-per-cell form above).  --mech h2co+K pads the H2/CO chemistry
 with K inert species (h2co+106: 121 species).
 
   python -m laminarsmoke_b200.run_case --workload coflow --mech h2co+106 --steps 50 --form auto
+
+tc_inverse inverts --cells seeded well-conditioned matrices G = I - h J of order --n (32 to 512) with the
+mixed-precision form's tensor-core inverse (lsg_build_and_invert_g_device), --steps times:
+
+  python -m laminarsmoke_b200.run_case --workload tc_inverse --n 121 --cells 4096
 """
 from __future__ import annotations
 
@@ -26,7 +31,9 @@ import numpy as np
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=("h2co_mixing", "h2co_uneven", "coflow"), default="h2co_mixing")
+    ap.add_argument("--workload", choices=("h2co_mixing", "h2co_uneven", "coflow", "tc_inverse"),
+                    default="h2co_mixing")
+    ap.add_argument("--n", type=int, default=121, help="matrix order of the tc_inverse workload")
     ap.add_argument("--cells", type=int, default=65536)
     ap.add_argument("--form", choices=("plain", "mixed", "batched64", "persistent", "auto"), default="mixed")
     ap.add_argument("--mech", default="h2co", help="h2co or h2co+K (K inert species)")
@@ -47,6 +54,8 @@ def main(argv=None) -> int:
              "auto": (lsg.LSG_TILE_AUTO, lsg.LSG_PRECISION_MIXED)}
     tile, prec = forms[args.form]
     ctx = lsg.ReactionStep(m, tile=tile, precision=prec)
+    if args.workload == "tc_inverse":
+        return tc_inverse(ctx, args)
     if args.workload == "h2co_mixing":
         Y, T = cells.h2co_mixing(species, arrays["mw"], args.cells, seed=args.seed)
     elif args.workload == "coflow":
@@ -80,6 +89,32 @@ def main(argv=None) -> int:
     print(f"{args.form} {args.workload} {args.mech} {args.cells} cells x {args.steps} steps: {ms:.1f} ms, "
           f"{args.cells * args.steps / (ms * 1e-3):.4e} cells*steps/s, cells failing in any step {fails}, "
           f"last statuses {dict(zip(*np.unique(st, return_counts=True)))}")
+    return 0
+
+
+def tc_inverse(ctx, args) -> int:
+    import torch
+    n, nm = args.n, args.cells
+    g = torch.Generator(device="cuda").manual_seed(args.seed)
+    J = torch.randn((nm, n, n), dtype=torch.float64, device="cuda", generator=g)
+    h = (0.2 + 0.8 * torch.rand(nm, dtype=torch.float64, device="cuda", generator=g)) * 0.5 / (2.0 * n ** 0.5)
+    inv = torch.empty((nm, n, n), dtype=torch.float32, device="cuda")
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.build_and_invert_g_device(J, h, inv)   # first call: work matrices, kernel attributes
+    torch.cuda.synchronize()
+    t0.record()
+    for _ in range(args.steps):
+        ctx.build_and_invert_g_device(J, h, inv)
+    t1.record()
+    torch.cuda.synchronize()
+    ctx.check()
+    ms = t0.elapsed_time(t1) / args.steps
+    G = torch.eye(n, dtype=torch.float64, device="cuda") - h[:4, None, None] * J[:4].transpose(1, 2)
+    X = inv[:4].transpose(1, 2).double()
+    res = (X @ G - torch.eye(n, dtype=torch.float64, device="cuda")).abs().max().item()
+    flops = 2.0 * n ** 3 * nm   # Gauss-Jordan inverse: 2 n^3
+    print(f"tc_inverse n={n} x {nm}: {ms:.3f} ms per call, {nm / (ms * 1e-3):.4e} inverses/s, "
+          f"{flops / (ms * 1e-3) / 1e12:.2f} TFLOP/s (2 n^3 per inverse), max |X G - I| {res:.2e}")
     return 0
 
 

@@ -10,8 +10,9 @@ near-equilibrium thirds; the pool is prepared with the plain step), coflow (the
 --steps successive device-resident steps; --cells below 80,000 takes an evenly
 strided subset).  Forms: plain (warp-per-cell FP64), mixed (round scheme, FP32
 factors), batched64 (round scheme, FP64 factors), persistent (persistent lane
-kernel, FP32 factors), auto (the library's choice: the autotuner for up to 31
-species, the block-per-cell form above).  --mech h2co+K pads the H2/CO chemistry
+kernel, FP32 factors), group / group64 (fused lane-group kernel, FP32 / FP64
+factors), auto (the library's choice: the autotuner for up to 31 species, the
+block-per-cell form above).  --mech h2co+K pads the H2/CO chemistry
 with K inert species (h2co+106: 121 species).
 
   python -m laminarsmoke_b200.run_case --workload coflow --mech h2co+106 --steps 50 --form auto
@@ -35,7 +36,8 @@ def main(argv=None) -> int:
                     default="h2co_mixing")
     ap.add_argument("--n", type=int, default=121, help="matrix order of the tc_inverse workload")
     ap.add_argument("--cells", type=int, default=65536)
-    ap.add_argument("--form", choices=("plain", "mixed", "batched64", "persistent", "auto"), default="mixed")
+    ap.add_argument("--form", choices=("plain", "mixed", "batched64", "persistent", "group", "group64", "auto"),
+                    default="mixed")
     ap.add_argument("--mech", default="h2co", help="h2co or h2co+K (K inert species)")
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--dt", type=float, default=1e-5)
@@ -51,6 +53,8 @@ def main(argv=None) -> int:
              "mixed": (lsg.LSG_TILE_LANE, lsg.LSG_PRECISION_MIXED),
              "batched64": (lsg.LSG_TILE_LANE, lsg.LSG_PRECISION_FP64),
              "persistent": (lsg.LSG_TILE_PERSISTENT, lsg.LSG_PRECISION_MIXED),
+             "group": (lsg.LSG_TILE_GROUP, lsg.LSG_PRECISION_MIXED),
+             "group64": (lsg.LSG_TILE_GROUP, lsg.LSG_PRECISION_FP64),
              "auto": (lsg.LSG_TILE_AUTO, lsg.LSG_PRECISION_MIXED)}
     tile, prec = forms[args.form]
     ctx = lsg.ReactionStep(m, tile=tile, precision=prec)

@@ -45,7 +45,18 @@ def _states(data, species, n, seed):
 
 
 def _central(orc, y, j, p):
-    h = 1e-5 * max(abs(y[j]), 1e-6) if j < len(y) - 1 else 1e-5 * y[j]
+    # The temperature row sums species enthalpy terms that cancel to a small net rate, so its rounding is
+    # eps times the sum of their magnitudes, far above eps |f|.  A species step of 1e-5 |y_j| alone makes
+    # that rounding ~1e-6 of the column for a radical at 1e-8 (1e-11 steps).  The right-hand side is a low-order
+    # rational function of the mass fractions (products of concentrations of order <= 2, the mixture
+    # molecular weight), so a step floored at 1e-9 and kept within half of y_j adds no measurable truncation
+    # (checked against steps 4x and 16x larger: within 0.6 of the bound below on H2/CO).
+    if j < len(y) - 1:
+        h = 1e-5 * max(abs(y[j]), 1e-4)
+        if y[j] > 0:
+            h = min(h, 0.5 * y[j])
+    else:
+        h = 1e-5 * y[j]
     yp, ym = y.copy(), y.copy()
     yp[j] += h
     ym[j] -= h

@@ -216,7 +216,12 @@ int lsg_ctx_kernel_times(lsg_ctx* ctx, double* ms, long long* launches, int nkin
  * otherwise) and the measured cells/s of the candidates, in the order round
  * scheme 16 lanes, round scheme 32 lanes, plain warp kernel, persistent lane
  * kernel, fused lane-group kernel at 4 and at 2 blocks per SM (0 for a
- * candidate not tried).  Returns LSG_ERR_ARG when no tuning has run yet. */
+ * candidate not tried).  For mechanisms above 31 species with
+ * LSG_PRECISION_MIXED the candidates are the block form with FP64 LU factors
+ * (rates[0]) and with the tensor-core inverse (rates[1]), timed on one wave of
+ * the FP64 form's blocks (at least 256 cells); tile is then LSG_TILE_BLOCK and
+ * the variant 1 for the tensor-core inverse, 0 for the FP64 factors.  Returns
+ * LSG_ERR_ARG when no tuning has run yet. */
 #define LSG_NTUNE_CANDIDATES 6
 int lsg_ctx_tuning(const lsg_ctx* ctx, int* tile, int* width, double* rates);
 

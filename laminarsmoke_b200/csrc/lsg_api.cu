@@ -317,9 +317,10 @@ int launch_large(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
     cudaStreamSynchronize(s);
     c->timer.collect();
   }
-  // mixed precision at 32 to 128 components: the tensor-core inverse (fewer blocks per SM; the FP64 form's
-  // work space covers them)
-  const bool tc = c->opt.precision == LSG_PRECISION_MIXED && block_tc_eligible(L);
+  // mixed precision: the tensor-core inverse (the FP64 form's work space covers its blocks), unless the
+  // autotuner measured the FP64 LU factors faster on this context's cells
+  const bool tuned_fp64 = c->tuned && c->tuned_tile == LSG_TILE_BLOCK && c->tuned_w == 0;
+  const bool tc = c->opt.precision == LSG_PRECISION_MIXED && block_tc_eligible(L) && !tuned_fp64;
   const long nb = tc ? c->tc_blocks : c->bws_blocks;
   c->timer.begin(KT_BLOCK, s);
   if (launch_block(L, c->mech->d_buf, to_step_options(c->opt), a, c->bws, nb, c->bqueue, tc, c->d_err, s) !=
@@ -332,16 +333,11 @@ int launch_large(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
 
 int launch_tile(lsg_ctx* c, const StepArgs& a, cudaStream_t s, int tile);
 
-// Autotuner: times the candidate forms on (a copy of) the first cells of the
-// call (up to 262,144) and keeps the fastest for tile LSG_TILE_AUTO.  Candidates: round scheme
-// with 16-lane groups (two cells per warp, up to 16 equations) and with 32-lane
-// groups, the plain warp kernel (FP64 only) and the persistent lane kernel.
-int autotune(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
-  const MechLayout& L = c->mech->host.layout;
-  const int nc = L.nc, n = nc + 1;
-  // The round scheme needs many cells to hide its latency: a small sample would
-  // under-rate it, so the sample is up to 262,144 cells (a one-time cost).
-  const long m = a.ncells < 262144 ? a.ncells : 262144;
+// The autotuner's sample: a pristine copy of the first m cells of the call (Y rows, T, dt) and a work copy
+// the trials integrate; t receives the trial arguments over the work copy.
+int tune_sample(lsg_ctx* c, const StepArgs& a, cudaStream_t s, long m, StepArgs* t, double** pristine_out,
+                double** work_out, size_t* per_out) {
+  const int nc = c->mech->host.layout.nc;
   const size_t per = (size_t)nc * m + 2 * (size_t)m;   // Y rows, T, dt
   if (c->tune_cap < m) {
     cudaFree(c->tune_buf);
@@ -361,16 +357,38 @@ int autotune(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
   if (a.dt && cudaMemcpyAsync(pristine + (size_t)nc * m + m, a.dt, m * sizeof(double), cudaMemcpyDeviceToDevice,
                               s) != cudaSuccess)
     return LSG_ERR_CUDA;
-  StepArgs t = a;
-  t.ncells = m;
-  t.ld = m;
-  t.Y = work;
-  t.T = work + (size_t)nc * m;
-  t.dt = a.dt ? work + (size_t)nc * m + m : nullptr;
-  t.Q = nullptr;
-  t.status = nullptr;
-  t.nsteps = nullptr;
-  t.counters = nullptr;
+  *t = a;
+  t->ncells = m;
+  t->ld = m;
+  t->Y = work;
+  t->T = work + (size_t)nc * m;
+  t->dt = a.dt ? work + (size_t)nc * m + m : nullptr;
+  t->Q = nullptr;
+  t->status = nullptr;
+  t->nsteps = nullptr;
+  t->counters = nullptr;
+  *pristine_out = pristine;
+  *work_out = work;
+  *per_out = per;
+  return LSG_OK;
+}
+
+// Autotuner: times the candidate forms on (a copy of) the first cells of the
+// call (up to 262,144) and keeps the fastest for tile LSG_TILE_AUTO.  Candidates: round scheme
+// with 16-lane groups (two cells per warp, up to 16 equations) and with 32-lane
+// groups, the plain warp kernel (FP64 only) and the persistent lane kernel.
+int autotune(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
+  const MechLayout& L = c->mech->host.layout;
+  const int nc = L.nc, n = nc + 1;
+  (void)nc;
+  // The round scheme needs many cells to hide its latency: a small sample would
+  // under-rate it, so the sample is up to 262,144 cells (a one-time cost).
+  const long m = a.ncells < 262144 ? a.ncells : 262144;
+  StepArgs t;
+  double *pristine = nullptr, *work = nullptr;
+  size_t per = 0;
+  const int rs = tune_sample(c, a, s, m, &t, &pristine, &work, &per);
+  if (rs != LSG_OK) return rs;
   struct Cand { int tile, w; };
   const Cand cands[LSG_NTUNE_CANDIDATES] = {
       {LSG_TILE_LANE, 16}, {LSG_TILE_LANE, 32}, {LSG_TILE_WARP, 0}, {LSG_TILE_PERSISTENT, 0},
@@ -421,12 +439,64 @@ int autotune(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
   return LSG_OK;
 }
 
-int launch_step(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
+// Autotuner for mechanisms above 31 species with mixed precision: the block form with the FP64 LU factors
+// (rates[0]) against the block form with the tensor-core inverse (rates[1]), each timed on (a copy of) the
+// first min(ncells, slots of the FP64 form) cells, one wave of the FP64 form.  The tensor-core form holds
+// more shared memory and TMEM per block, so it runs fewer blocks per SM where the FP64 form fits more;
+// which is faster depends on how much of the step the factorisations are.  Keeps tile LSG_TILE_BLOCK with
+// width 1 (tensor-core inverse) or 0 (FP64 factors).
+int autotune_large(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
   const MechLayout& L = c->mech->host.layout;
-  if (L.nc + 1 <= 32 && c->opt.tile == LSG_TILE_AUTO && c->opt.autotune && !c->tuned && a.ncells >= 1024) {
-    const int r = autotune(c, a, s);
-    if (r != LSG_OK) return r;
+  int r = prepare_large(c);
+  if (r != LSG_OK) return r;
+  const long m = a.ncells < c->bws_blocks ? a.ncells : c->bws_blocks;
+  StepArgs t;
+  double *pristine = nullptr, *work = nullptr;
+  size_t per = 0;
+  r = tune_sample(c, a, s, m, &t, &pristine, &work, &per);
+  if (r != LSG_OK) return r;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return LSG_ERR_CUDA;
+  const StepOptions so = to_step_options(c->opt);
+  for (int k = 0; k < LSG_NTUNE_CANDIDATES; ++k) c->tune_rate[k] = 0.;
+  r = LSG_OK;
+  for (int k = 0; k < 2 && r == LSG_OK; ++k) {
+    const bool tc = k == 1;
+    float ms = 0.f;
+    if (cudaMemcpyAsync(work, pristine, per * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+        cudaEventRecord(e0, s) != cudaSuccess ||
+        launch_block(L, c->mech->d_buf, so, t, c->bws, tc ? c->tc_blocks : c->bws_blocks, c->bqueue, tc, c->d_err,
+                     s) != cudaSuccess ||
+        cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+      cudaGetLastError();
+      r = LSG_ERR_CUDA;
+      break;
+    }
+    cudaEventElapsedTime(&ms, e0, e1);
+    c->tune_rate[k] = ms > 0.f ? m / (ms * 1e-3) : 0.;
   }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r != LSG_OK) return r;
+  c->tuned = true;
+  c->tuned_tile = LSG_TILE_BLOCK;
+  c->tuned_w = c->tune_rate[1] > c->tune_rate[0] ? 1 : 0;
+  return LSG_OK;
+}
+
+// The autotuner, once per context, when tile is LSG_TILE_AUTO and autotune is on.
+int maybe_autotune(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
+  const MechLayout& L = c->mech->host.layout;
+  if (c->opt.tile != LSG_TILE_AUTO || !c->opt.autotune || c->tuned) return LSG_OK;
+  if (L.nc + 1 <= 32) return a.ncells >= 1024 ? autotune(c, a, s) : LSG_OK;
+  if (c->opt.precision == LSG_PRECISION_MIXED && block_tc_eligible(L) && a.ncells >= 256)
+    return autotune_large(c, a, s);
+  return LSG_OK;
+}
+
+int launch_step(lsg_ctx* c, const StepArgs& a, cudaStream_t s) {
+  const int r = maybe_autotune(c, a, s);
+  if (r != LSG_OK) return r;
   const int tile = (c->tuned && c->opt.tile == LSG_TILE_AUTO) ? c->tuned_tile : resolve_tile(c->opt);
   return launch_tile(c, a, s, tile);
 }
@@ -818,8 +888,8 @@ int lsg_reaction_step_sequence_device(lsg_ctx* c, int nsteps, int ncells, int ns
   a.Q = Q; a.status = status;
   const MechLayout& L = c->mech->host.layout;
   // the form: tuned once (on copies of the cells) when autotuning is on
-  if (L.nc + 1 <= 32 && c->opt.tile == LSG_TILE_AUTO && c->opt.autotune && !c->tuned && ncells >= 1024) {
-    const int r = autotune(c, a, s);
+  {
+    const int r = maybe_autotune(c, a, s);
     if (r != LSG_OK) return r;
   }
   int tile = (c->tuned && c->opt.tile == LSG_TILE_AUTO) ? c->tuned_tile : resolve_tile(c->opt);

@@ -43,6 +43,9 @@ constexpr int kAT = 128;       // threads per block of the init kernel
 constexpr int kCT = 256;       // threads per block of the compaction kernel
 constexpr int kRefineR = 1;    // refinement sweeps of a solve with FP32 factors
 constexpr int kBins = 6;       // solver-path bins of the compaction
+// Row stride (elements) of the per-group matrices in shared memory (G^-1, J): odd, so the lanes of a group
+// reading one column (lane = row) hit distinct banks; at most n + 1, the stride the buffers are sized for.
+__host__ __device__ constexpr int row_ld(int n) { return n | 1; }
 
 enum Phase : int {
   PH_DONE = 0,
@@ -649,7 +652,7 @@ __device__ __noinline__ double pow_ol(double x, double y) { return pow(x, y); }
 template <typename LUT, int W>
 __device__ __noinline__ void gj_inverse(const double* Js, LUT* As, LUT* Ks, LUT* Xs, LUT* Ig, double hr0, int n,
                                         int lane, unsigned gm) {
-  const int ld = n + 1, la = 2 * n + 1, m2 = 2 * n;
+  const int ld = row_ld(n), la = 2 * n + 1, m2 = 2 * n;
   const bool al = lane < n;
   if (al) {
     for (int j = 0; j < n; ++j) {
@@ -763,7 +766,7 @@ __device__ __forceinline__ void set8(double (&a)[8], unsigned i, double x) {
 template <typename LUT, int W>
 __device__ __noinline__ double solve_ol(const LUT* Xs, const double* Js, double rhs, double hr0, int n, int lane,
                                         unsigned gm, int refine) {
-  const int ld = n + 1;
+  const int ld = row_ld(n);
   const bool al = lane < n;
   double xv = rowdot_ol<LUT, W>(Xs, rhs, n, ld, lane, gm);
   for (int it = 0; it < refine; ++it) {
@@ -1374,7 +1377,7 @@ __global__ void __launch_bounds__(kWA * 32, 4) rounds_advance_kernel(int NC, Ste
   const int lane = wl & (W - 1);                     // component owned by this thread
   const int w = (threadIdx.x >> 5) * CPW + wl / W;   // lane group within the block
   const unsigned gm = W == 32 ? kFull : (0xffffu << (wl & 16));
-  const int n = NC + 1, ld = n + 1;
+  const int n = NC + 1, ld = row_ld(n);
   const RecLayout RL = B.L;
   // per-warp shared memory: G^-1 X[n][ld] (LUT), the Gauss-Jordan work array A[n][2n+1] (LUT), its pivot
   // row K[2n] (LUT) and the Jacobian J[n][ld] (double)
@@ -2189,7 +2192,7 @@ __global__ void __launch_bounds__(kGW * 32, MB) group_kernel(MechLayout Lp, cons
   constexpr int CPW = 32 / W;
   constexpr int GB = kGW * CPW;   // lane groups per block
   const int NC = Lp.nc, NR = Lp.nr;
-  const int n = NC + 1, ld = n + 1, la = 2 * n + 1;
+  const int n = NC + 1, ld = row_ld(n), la = 2 * n + 1;
   const int wl = threadIdx.x & 31;
   const int lane = wl & (W - 1);
   const int w = (threadIdx.x >> 5) * CPW + wl / W;
@@ -2772,7 +2775,7 @@ __global__ void __launch_bounds__(kGW * 32, MB) group_kernel(MechLayout Lp, cons
 }
 
 size_t group_smem_bytes(const MechLayout& L, bool lu64, int width) {
-  const size_t n = L.nc + 1, ld = n + 1, la = 2 * n + 1;
+  const size_t n = L.nc + 1, ld = (size_t)row_ld((int)n), la = 2 * n + 1;
   const size_t groups = (size_t)kGW * (width == 16 ? 2 : 1);
   const size_t gd = 2 * (size_t)L.nc + L.nr + n * ld;
   const size_t gl = n * ld + n * la + 2 * n;

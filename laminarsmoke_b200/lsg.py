@@ -458,6 +458,8 @@ class ReactionStep:
         return {k: (ms[i], nl[i]) for i, k in enumerate(self.KERNEL_KINDS)}
 
     TUNE_CANDIDATES = ("rounds16", "rounds32", "plain_warp", "persistent", "group_4", "group_2")
+    # mechanisms above 31 species, mixed precision: the block form's factorisation
+    TUNE_CANDIDATES_LARGE = ("block_fp64_lu", "block_tc_inverse")
 
     def tuning(self):
         """(tile, width, {candidate: cells/s}) chosen by the autotuner, or None before it ran."""
@@ -466,7 +468,8 @@ class ReactionStep:
         rc = lib().lsg_ctx_tuning(self.h, C.byref(tile), C.byref(width), C.cast(rates, C.c_void_p))
         if rc != 0:
             return None
-        return tile.value, width.value, {k: rates[i] for i, k in enumerate(self.TUNE_CANDIDATES)}
+        names = self.TUNE_CANDIDATES_LARGE if tile.value == LSG_TILE_BLOCK else self.TUNE_CANDIDATES
+        return tile.value, width.value, {k: rates[i] for i, k in enumerate(names)}
 
     def check(self):
         f = C.c_int()

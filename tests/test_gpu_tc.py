@@ -126,3 +126,33 @@ def test_tc_block_step_against_oracle(cuda, rtol, atol, frac):
     assert c[:, 3].sum() > 0
     assert dT.max() <= 1e-6
     assert np.mean(dY <= 1e-9) >= frac and dY.max() <= 1e-7
+
+
+def test_large_autotuner_times_both_factorisations(cuda):
+    """With autotune on, the mixed-precision block form's first call times the FP64 LU factors against the
+    tensor-core inverse on one wave of the FP64 form's blocks and keeps the faster; the step it then takes
+    matches the oracle with the criteria above."""
+    import torch
+    from laminarsmoke_b200 import lsg
+    from oracle.oracle import OracleMechanism
+    n = 512
+    data, Y, T = _padded_states(n, 7)
+    ctx = lsg.ReactionStep(lsg.Mechanism(data), precision=lsg.LSG_PRECISION_MIXED, autotune=1)
+    Yd = torch.tensor(np.ascontiguousarray(Y.T), device=cuda)
+    Td = torch.tensor(T, device=cuda)
+    st = torch.zeros(n, dtype=torch.int32, device=cuda)
+    ctx.step_device(Yd, Td, 1e-5, status=st)
+    torch.cuda.synchronize()
+    ctx.check()
+    tile, width, rates = ctx.tuning()
+    print(f"large autotuner: {rates}, chosen {'tensor-core inverse' if width else 'FP64 LU factors'}")
+    assert tile == lsg.LSG_TILE_BLOCK
+    assert rates["block_fp64_lu"] > 0 and rates["block_tc_inverse"] > 0
+    assert width == int(rates["block_tc_inverse"] > rates["block_fp64_lu"])
+    pick = np.arange(0, n, 8)
+    Yo, To, _, sto, _ = OracleMechanism(data).reaction_step(Y[pick], T[pick], 1e-5, nthreads=8)
+    np.testing.assert_array_equal(st.cpu().numpy()[pick], sto)
+    dT = np.abs(Td.cpu().numpy()[pick] - To) / To
+    dY = np.abs(Yd.cpu().numpy().T[pick] - Yo).max(axis=1)
+    assert dT.max() <= 1e-6
+    assert np.mean(dY <= 1e-9) >= 0.7 and dY.max() <= 1e-7

@@ -5,8 +5,8 @@ allocator, or one that keeps cudaMalloc/cudaFree (which synchronise the device)
 out of its time loop, use this entry point.  It runs the persistent lane kernel
 with its work space in a fixed 16 MiB device array, so it must give the same
 cells the same answers as the context-based call of that kernel, call after
-call (the array keeps the previous call's contents), and it must refuse a
-mechanism whose work space does not fit.
+call (the array keeps the previous call's contents), agree with the CPU oracle,
+and it must refuse a mechanism whose work space does not fit.
 
 This file is collected last on purpose: it runs after every other test.
 """
@@ -22,7 +22,7 @@ ATOL_Y = 1e-9
 
 
 @pytest.mark.parametrize("precision", [0, 1], ids=["fp64-lu", "fp32-lu"])
-def test_noalloc_matches_context_call_twice(h2co, cuda, precision):
+def test_noalloc_matches_context_call_twice(h2co, oracle_h2co, cuda, precision):
     import torch
     from laminarsmoke_b200 import lsg
     _, species, A = h2co
@@ -55,6 +55,15 @@ def test_noalloc_matches_context_call_twice(h2co, cuda, precision):
         np.testing.assert_allclose(Tn.cpu().numpy(), Tr.cpu().numpy(), rtol=RTOL_T, err_msg=f"call {call}")
         np.testing.assert_allclose(Yn.cpu().numpy(), Yr.cpu().numpy(), rtol=0, atol=ATOL_Y, err_msg=f"call {call}")
         np.testing.assert_allclose(Qn.cpu().numpy(), Qr.cpu().numpy(), rtol=1e-9, atol=1e-6, err_msg=f"call {call}")
+    # and against the oracle on 512 of the cells, with the criteria of the other step tests: identical
+    # statuses, T within 1e-6 relative, Y within 1e-9 absolute in 99 % of the cells and 1e-7 in all
+    pick = np.arange(0, n, n // 512)[:512]
+    Yo, To, _, sto, _ = oracle_h2co.reaction_step(Y[pick], T[pick], 1e-5, nthreads=8)
+    Yg, Tg = Yn.cpu().numpy().T[pick], Tn.cpu().numpy()[pick]
+    np.testing.assert_array_equal(stn.cpu().numpy()[pick], sto)
+    assert float(np.max(np.abs(Tg - To) / To)) <= RTOL_T
+    dY = np.abs(Yg - Yo).max(axis=1)
+    assert (dY <= ATOL_Y).mean() >= 0.99 and dY.max() <= 1e-7, (float((dY <= ATOL_Y).mean()), float(dY.max()))
     mech.close()
 
 

@@ -602,8 +602,22 @@ struct GearBlock {
         double l = G[(long)k * n + tid];
         if (d != 0.) l /= d;
         G[(long)k * n + tid] = l;
-#pragma unroll 4
-        for (int j = k + 1; j < n; ++j) G[(long)j * n + tid] -= l * W.X[j];
+        // G lives in global memory: the row's elements are loaded eight at a time before any of them is
+        // written back, so their L2 latencies overlap (a store may alias a later load, so the compiler
+        // cannot reorder them itself)
+        double* Gr = G + tid;
+        int j = k + 1;
+        for (; j + 8 <= n; j += 8) {
+          double g[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) g[q] = Gr[(long)(j + q) * n];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            g[q] -= l * W.X[j + q];
+            Gr[(long)(j + q) * n] = g[q];
+          }
+        }
+        for (; j < n; ++j) Gr[(long)j * n] -= l * W.X[j];
       }
       __syncthreads();
     }
@@ -733,18 +747,40 @@ struct GearBlock {
       if (tid < 32) {
         const int r = j0 + tid;
         double xr = r < j1 ? W.X[r] : 0.;
-        for (int j = j0; j < j1; ++j) {
-          const double g = r < j1 ? G[(long)j * n + r] : 0.;
-          const double xj = __shfl_sync(kFull, xr, j - j0);
-          if (r > j && r < j1) xr -= g * xj;
+        // the diagonal block's row r, loaded 16 columns ahead so the global-memory latencies overlap
+#pragma unroll
+        for (int c = 0; c < 32; c += 16) {
+          double g[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int j = j0 + c + q;
+            g[q] = (r < j1 && j < j1) ? G[(long)j * n + r] : 0.;
+          }
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int j = j0 + c + q;
+            if (j < j1) {   // the same in every lane
+              const double xj = __shfl_sync(kFull, xr, c + q);
+              if (r > j && r < j1) xr -= g[q] * xj;
+            }
+          }
         }
         if (r < j1) W.X[r] = xr;
       }
       __syncthreads();
-      if (tid >= j1 && tid < n)
-        for (int j = j0; j < j1; ++j) x -= G[(long)j * n + tid] * W.X[j];
-      else if (tid >= j0 && tid < j1)
+      if (tid >= j1 && tid < n) {
+        int j = j0;
+        for (; j + 8 <= j1; j += 8) {
+          double g[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) g[q] = G[(long)(j + q) * n + tid];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) x -= g[q] * W.X[j + q];
+        }
+        for (; j < j1; ++j) x -= G[(long)j * n + tid] * W.X[j];
+      } else if (tid >= j0 && tid < j1) {
         x = W.X[tid];
+      }
     }
     for (int j1 = n; j1 > 0; j1 -= 32) {
       const int j0 = max(j1 - 32, 0);
@@ -753,19 +789,40 @@ struct GearBlock {
       if (tid < 32) {
         const int r = j0 + tid;
         double xr = r < j1 ? W.X[r] : 0.;
-        for (int j = j1 - 1; j >= j0; --j) {
-          const double g = r < j1 ? G[(long)j * n + r] : 0.;
-          if (r == j) xr /= g;
-          const double xj = __shfl_sync(kFull, xr, j - j0);
-          if (r < j) xr -= g * xj;
+#pragma unroll
+        for (int c = 0; c < 32; c += 16) {
+          double g[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int j = j1 - 1 - c - q;
+            g[q] = (r < j1 && j >= j0) ? G[(long)j * n + r] : 0.;
+          }
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int j = j1 - 1 - c - q;
+            if (j >= j0) {   // the same in every lane
+              if (r == j) xr /= g[q];
+              const double xj = __shfl_sync(kFull, xr, j - j0);
+              if (r < j) xr -= g[q] * xj;
+            }
+          }
         }
         if (r < j1) W.X[r] = xr;
       }
       __syncthreads();
-      if (tid < j0)
-        for (int j = j1 - 1; j >= j0; --j) x -= G[(long)j * n + tid] * W.X[j];
-      else if (tid < j1)
+      if (tid < j0) {
+        int j = j1 - 1;
+        for (; j - 8 >= j0 - 1; j -= 8) {
+          double g[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) g[q] = G[(long)(j - q) * n + tid];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) x -= g[q] * W.X[j - q];
+        }
+        for (; j >= j0; --j) x -= G[(long)j * n + tid] * W.X[j];
+      } else if (tid < j1) {
         x = W.X[tid];
+      }
     }
     __syncthreads();
     ++cnt[CNT_SOLVE];

@@ -175,6 +175,44 @@ int lsg_reaction_step_sequence_device(lsg_ctx* ctx, int nsteps, int ncells, int 
                                       double* T_dev, double p, double t0, double dt, double* Q_dev, int* status_dev,
                                       int* graph_used, void* stream);
 
+/* ---- DRG-reduced reaction step ----------------------------------------------
+ * Replaces the per-cell loop of solvers/laminarSMOKE/unsteady/chemistry_DRG.H:
+ * 86-200 (with unsteady/DRG.hpp: Analysis, PairWiseErrorMatrix,
+ * ParsePairWiseErrorMatrix, and the reduced system of
+ * BatchReactorHomogeneousConstantPressure.H:253-320).  Per cell above min_T:
+ * the directed-relation-graph analysis at the cell's state with the epsilon of
+ * the first band whose temperature is above the cell's (a cell above every band
+ * keeps the previous analysed cell's epsilon, as the reference's loop does),
+ * the reduced system -- the important species and T; the other species keep
+ * their mass fractions, the dropped reactions have zero rate -- integrated by a
+ * fresh solver from t0 to t0 + dt, the mass fractions normalised after it.  The
+ * reference applies the solver options (tolerances; bounds [0, 1] and
+ * [200, 6000] K) only when celli == 0, the other cells integrating with the
+ * solver's defaults (1e-10 absolute, 100 FLT_EPSILON relative, no bounds):
+ * first_cell_options_only = 1 keeps that, 0 gives every cell the options.
+ * Cells at or below min_T are left as they are (status 0).  Constant-pressure
+ * reactor, FP64, one warp per cell: up to 31 species (LSG_ERR_UNSUPPORTED
+ * above).  Options used from the context: rtol, atol, energy.  n_species /
+ * n_reactions (optional, device): important species and reactions kept per
+ * cell (the reference's drg_important_species / drg_important_reactions
+ * fields), 0 for skipped cells. */
+#define LSG_DRG_MAX_BANDS 16
+typedef struct lsg_drg_options {
+  const int* key;           /* host array: key species indices (the DRG "species" list), 1 to nspecies of them */
+  int nkey;
+  const double* band_T;     /* host arrays of nbands (1..LSG_DRG_MAX_BANDS): temperatures [K] and epsilons */
+  const double* band_eps;
+  int nbands;
+  double epsilon0;          /* epsilon until an analysed cell falls in a band */
+  double min_T;             /* minTemperature: cells at or below are not integrated */
+  int first_cell_options_only;
+} lsg_drg_options;
+
+int lsg_reaction_step_drg_device(lsg_ctx* ctx, int ncells, int nspecies, double* Y_dev, long ld, double* T_dev,
+                                 double p, double t0, const double* dt_dev, double dt_scalar,
+                                 const lsg_drg_options* drg, double* Q_dev, int* status_dev, int* n_species_dev,
+                                 int* n_reactions_dev, long long* counters_dev, void* stream);
+
 /* ---- reaction step, constant-volume reactor ------------------------------
  * The branch of chemistry_DI.H taken with constPressureBatchReactor false
  * (:168-203): BatchReactorHomogeneousConstantVolume::SetReactor(V, P, rho)

@@ -965,6 +965,66 @@ int lsg_reaction_step_sequence_device(lsg_ctx* c, int nsteps, int ncells, int ns
   return LSG_OK;
 }
 
+// DRG-reduced step (chemistry_DRG.H:86-200): the plain warp form on the reduced system of each cell.
+int lsg_reaction_step_drg_device(lsg_ctx* c, int ncells, int nspecies, double* Y, long ld, double* T, double p,
+                                 double t0, const double* dt, double dt_scalar, const lsg_drg_options* drg,
+                                 double* Q, int* status, int* n_species, int* n_reactions, long long* counters,
+                                 void* stream) {
+  if (!c || !drg || ncells < 0 || !Y || !T || ld < ncells || !(p > 0.)) return LSG_ERR_ARG;
+  const MechLayout& L = c->mech->host.layout;
+  if (nspecies != L.nc) return LSG_ERR_ARG;
+  if (!drg->key || drg->nkey < 1 || drg->nkey > L.nc) return LSG_ERR_ARG;
+  if (!drg->band_T || !drg->band_eps || drg->nbands < 1 || drg->nbands > LSG_DRG_MAX_BANDS) return LSG_ERR_ARG;
+  if (L.nc + 1 > 32 || plain_smem_bytes(L) > 227 * 1024) return LSG_ERR_UNSUPPORTED;
+  DrgArgs d{};
+  for (int t = 0; t < drg->nkey; ++t) {
+    if (drg->key[t] < 0 || drg->key[t] >= L.nc) return LSG_ERR_ARG;
+    d.key[t] = drg->key[t];
+  }
+  d.nkey = drg->nkey;
+  for (int b = 0; b < drg->nbands; ++b) {
+    d.band_T[b] = drg->band_T[b];
+    d.band_eps[b] = drg->band_eps[b];
+  }
+  d.nbands = drg->nbands;
+  d.epsilon0 = drg->epsilon0;
+  d.min_T = drg->min_T;
+  d.first_cell_options_only = drg->first_cell_options_only != 0;
+  d.n_species = n_species;
+  d.n_reactions = n_reactions;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  if (ncells > c->frs_cap) {   // each cell's epsilon
+    const cudaStream_t s0 = (cudaStream_t)stream;
+    if (cudaStreamSynchronize(s0) != cudaSuccess) return LSG_ERR_CUDA;
+    cudaFree(c->frs);
+    c->frs = nullptr;
+    c->frs_cap = 0;
+    if (cudaMalloc(&c->frs, sizeof(double) * (size_t)ncells) != cudaSuccess) { cudaGetLastError(); return LSG_ERR_NOMEM; }
+    c->frs_cap = ncells;
+  }
+  d.eps = c->frs;
+  StepArgs a{};
+  a.ncells = ncells;
+  a.ld = ld;
+  a.Y = Y;
+  a.T = T;
+  a.dt = dt;
+  a.dt_scalar = dt_scalar;
+  a.t0 = t0;
+  a.p = p;
+  a.Q = Q;
+  a.status = status;
+  a.counters = counters;
+  if (launch_drg_plain(L, c->mech->d_buf, to_step_options(c->opt), a, d, c->d_err, (cudaStream_t)stream) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return LSG_ERR_CUDA;
+  }
+  c->launches += 2;
+  return LSG_OK;
+}
+
 int lsg_reaction_step(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, double* T, double p, double t0,
                       const double* dt, double dt_scalar, double* Q, int* status, int* nsteps) {
   return host_step(c, ncells, nspecies, Ys, T, p, nullptr, t0, dt, dt_scalar, Q, status, nsteps);

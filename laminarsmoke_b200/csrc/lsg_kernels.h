@@ -44,6 +44,25 @@ struct StepArgs {
   const double* rho;  // constant-volume reactor: per-cell density [kg/m3]; nullptr: constant pressure
 };
 
+// DRG-reduced step (chemistry_DRG.H, DRG.hpp): key species, (temperature, epsilon) bands, the temperature
+// below which cells are skipped, and whether the solver options reach the first cell of the call only.
+constexpr int kDrgMaxBands = 16;
+struct DrgArgs {
+  int key[32];
+  int nkey;
+  double band_T[kDrgMaxBands];
+  double band_eps[kDrgMaxBands];
+  int nbands;
+  double epsilon0;
+  double min_T;
+  int first_cell_options_only;
+  double* eps;        // [ncells] work: each cell's epsilon (the band scan carries it over between cells)
+  int* n_species;     // optional [ncells]: important species (0 for skipped cells)
+  int* n_reactions;   // optional [ncells]: reactions kept
+};
+cudaError_t launch_drg_plain(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                             const StepArgs& a, const DrgArgs& d, int* err, cudaStream_t stream);
+
 size_t plain_smem_bytes(const MechLayout& L);
 cudaError_t upload_gear_plain(const GearConsts& gc);
 cudaError_t launch_plain(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,

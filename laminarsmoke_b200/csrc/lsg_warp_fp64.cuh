@@ -41,13 +41,16 @@ struct WarpWS {
   double* KINF;   // [NFO] k_inf (cache)
   double* LOGF;   // [NFO] log10 Fcent (Troe) / SRI factor (cache)
   int* PIV;       // [32]
-  double* SC;     // [6] scalars: cached kinetic T, QR of the last call, P0, energy flag, rho0 (> 0: constant volume)
+  double* SC;     // [6] scalars: cached kinetic T, QR of the last call, P0, energy flag, rho0 (> 0: constant volume),
+                  // DRG flag (non-zero: the reactions marked in DROP have zero rate)
+  unsigned char* DROP;   // [NR] DRG-reduced step: 1 for a reaction the analysis dropped
 };
 
 __host__ __device__ inline int warp_ws_doubles(const MechLayout& L) {
   const int n = L.nc + 1;
   auto even = [](int x) { return (x + 1) & ~1; };
-  return 8 * 32 * 2 + even(n * (n + 1)) * 2 + 32 * 3 + even(L.nr) * 3 + even(L.n_fo > 0 ? L.n_fo : 1) * 2 + 16 + 6;
+  return 8 * 32 * 2 + even(n * (n + 1)) * 2 + 32 * 3 + even(L.nr) * 3 + even(L.n_fo > 0 ? L.n_fo : 1) * 2 + 16 + 6 +
+         (L.nr + 7) / 8 + 1;
 }
 
 __device__ __forceinline__ WarpWS carve_ws(double* base, const MechLayout& L) {
@@ -68,7 +71,8 @@ __device__ __forceinline__ WarpWS carve_ws(double* base, const MechLayout& L) {
   w.KINF = p; p += even(L.n_fo > 0 ? L.n_fo : 1);
   w.LOGF = p; p += even(L.n_fo > 0 ? L.n_fo : 1);
   w.PIV = (int*)p; p += 16;
-  w.SC = p;
+  w.SC = p; p += 6;
+  w.DROP = (unsigned char*)p;
   return w;
 }
 
@@ -304,6 +308,7 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
         net -= rv;
       }
       net *= kMod;
+      if (W.SC[5] != 0. && W.DROP[j]) net = 0.;   // DRG-reduced system: dropped reactions (chemistry_DRG.H)
       W.NET[j] = net;
     }
   }
@@ -386,13 +391,31 @@ struct GearWarp {
   unsigned numberOfSteps, iterConvergence, iterConvergenceRate, iterConvergenceFailure, iterErrorFailure;
   unsigned numberOfConvergenceFailuresForOrderMax, stepOfLastJacobian;
   long long cnt[NCNT];
+  // DRG-reduced system (BatchReactorHomogeneousConstantPressure.H:253-320): lane l < drg_ni owns species
+  // drg_sp (the l-th important one), lane drg_ni owns T; as a lane of the full layout (species `lane`),
+  // drg_pos is that species' reduced index or -1, drg_omega its fixed mass fraction.
+  bool drg = false;
+  bool unconstrained = false;   // no minimum/maximum constraints: KernelDense's unconstrained increments
+  int drg_ni = 0, drg_sp = 0, drg_pos = -1, drg_nc = 0;
+  double drg_omega = 0.;
 
   __device__ __forceinline__ double& Z(int i) { return W.Z[i * 32 + lane]; }
   __device__ __forceinline__ double& V(int i) { return W.V[i * 32 + lane]; }
 
+  // f(y) of the system being integrated: the full reactor, or the DRG-reduced one evaluated through the
+  // full layout (kept species fixed, dropped reactions at zero rate) and gathered back to the reduced lanes
+  __device__ __forceinline__ double eval(double yl) {
+    if (!drg) return rhs_warp(L, Md, Mi, ws, yl, __shfl_sync(kFull, yl, ne - 1));
+    const double T = __shfl_sync(kFull, yl, drg_ni);
+    const double v = __shfl_sync(kFull, yl, drg_pos >= 0 ? drg_pos : 0);
+    const double yf = lane < drg_nc ? (drg_pos >= 0 ? v : drg_omega) : T;
+    const double df = rhs_warp(L, Md, Mi, ws, yf, T);
+    return __shfl_sync(kFull, df, drg_sp);
+  }
+
   __device__ __forceinline__ double rhs(double yl) {
     ++cnt[CNT_RHS];
-    return rhs_warp(L, Md, Mi, ws, yl, __shfl_sync(kFull, yl, ne - 1));
+    return eval(yl);
   }
 
   __device__ __forceinline__ double error_control(double w, double e) {   // OpenSMOKEUtilities.hpp:689-701
@@ -427,15 +450,24 @@ struct GearWarp {
       const double yh = __shfl_sync(kFull, yl, j);
       const double ej = __shfl_sync(kFull, eps, j);
       const double mxj = __shfl_sync(kFull, maxv, j);
-      const double a = fabs(yh), bb = fabs(1. / ej);
-      double hJ = ETA2 * (a > bb ? a : bb);
-      const double hJf = hf / ej;
-      hJ = fmax(hJ, hJf);
-      hJ = fmax(hJ, ZERO_DER);
-      if (yh + hJ > mxj) hJ = -hJ;
+      double hJ;
+      if (unconstrained) {   // KernelDense.hpp:111-193 without maximum constraints
+        hJ = ETA2 * fabs(fmax(yh, 1. / ej));
+        const double hJf = hf / ej;
+        hJ = fmax(hJ, hJf);
+        hJ = fmax(hJ, ZERO_DER);
+        hJ = fmin(hJ, 0.001 + 0.001 * fabs(yh));
+      } else {
+        const double a = fabs(yh), bb = fabs(1. / ej);
+        hJ = ETA2 * (a > bb ? a : bb);
+        const double hJf = hf / ej;
+        hJ = fmax(hJ, hJf);
+        hJ = fmax(hJ, ZERO_DER);
+        if (yh + hJ > mxj) hJ = -hJ;
+      }
       const double saved = yl;
       if (lane == j) yl += hJ;
-      const double aux = rhs_warp(L, Md, Mi, ws, yl, __shfl_sync(kFull, yl, n - 1));
+      const double aux = eval(yl);
       ++cnt[CNT_JAC_RHS];
       yl = saved;
       const double hInv = 1. / hJ;

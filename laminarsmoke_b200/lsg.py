@@ -53,7 +53,15 @@ EXPORTS = (
     "lsg_reaction_step_cv", "lsg_reaction_step_cv_device", "lsg_steady_sources_device",
     "lsg_mech_transport_info", "lsg_properties_device", "lsg_properties", "lsg_build_and_invert_g_device",
     "lsg_reaction_step_sequence_device", "lsg_jacobian_device", "lsg_steady_sources_sparse_device",
+    "lsg_reaction_step_drg_device",
 )
+
+class DrgOptions(C.Structure):
+    """lsg_drg_options."""
+    _fields_ = [("key", C.c_void_p), ("nkey", C.c_int), ("band_T", C.c_void_p), ("band_eps", C.c_void_p),
+                ("nbands", C.c_int), ("epsilon0", C.c_double), ("min_T", C.c_double),
+                ("first_cell_options_only", C.c_int)]
+
 
 # lsg_property_fields, in declaration order: species rows (nc), scalars, light-species rows
 PROPERTY_FIELDS = ("X", "cTot", "psi", "mu", "lambda", "cp", "cv", "h", "MWmix", "cp_species", "Dmix", "Dsoret")
@@ -94,6 +102,8 @@ def lib():
     L.lsg_reaction_step_sequence_device.argtypes = [vp, i, i, i, vp, l, vp, d, d, d, vp, vp, C.POINTER(i), vp]
     L.lsg_jacobian_device.argtypes = [vp, i, vp, l, d, vp, vp]
     L.lsg_steady_sources_sparse_device.argtypes = [vp, i, i, vp, vp, l, vp, d, i, i, vp, vp, l, vp]
+    L.lsg_reaction_step_drg_device.argtypes = [vp, i, i, vp, l, vp, d, d, vp, d, C.POINTER(DrgOptions), vp, vp, vp,
+                                               vp, vp, vp]
     L.lsg_strerror.argtypes = [i]
     L.lsg_strerror.restype = C.c_char_p
     L.lsg_abi_version.restype = i
@@ -301,6 +311,26 @@ class ReactionStep:
             self.step_device(Y, T, dt, p=p, t0=t0 + k * float(dt), Q=Q, status=st, stream=stream)
             bad |= st < 0
         return int(bad.sum().item())
+
+    def step_drg_device(self, Y, T, dt, key, bands=((1.e6, 1.e-2),), epsilon0: float = 1.e-2, min_T: float = 300.0,
+                        first_cell_options_only: bool = True, p: float = 101325.0, t0: float = 0.0, Q=None,
+                        status=None, n_species=None, n_reactions=None, counters=None, stream=None):
+        """lsg_reaction_step_drg_device: the DRG-reduced step (chemistry_DRG.H) of device arrays Y [NC, ld]
+        and T [ncells], in place.  key: key species indices; bands: (temperature, epsilon) pairs."""
+        _require_layout(Y, T, Q, status, n_species, n_reactions, counters,
+                        dt if hasattr(dt, "data_ptr") else None)
+        nc, ld = Y.shape
+        n = T.shape[0]
+        k = (C.c_int * len(key))(*[int(x) for x in key])
+        bt = (C.c_double * len(bands))(*[float(b[0]) for b in bands])
+        be = (C.c_double * len(bands))(*[float(b[1]) for b in bands])
+        o = DrgOptions(C.cast(k, C.c_void_p), len(key), C.cast(bt, C.c_void_p), C.cast(be, C.c_void_p), len(bands),
+                       float(epsilon0), float(min_T), int(bool(first_cell_options_only)))
+        dtp, dts = (None, float(dt)) if not hasattr(dt, "data_ptr") else (dt.data_ptr(), 0.0)
+        ptr = (lambda x: None if x is None else x.data_ptr())
+        _check(lib().lsg_reaction_step_drg_device(
+            self.h, n, nc, Y.data_ptr(), ld, T.data_ptr(), p, t0, dtp, dts, C.byref(o), ptr(Q), ptr(status),
+            ptr(n_species), ptr(n_reactions), ptr(counters), _stream_handle(stream)), "lsg_reaction_step_drg_device")
 
     def step_sequence_graph(self, Y, T, dt: float, nsteps: int, p: float = 101325.0, t0: float = 0.0, Q=None,
                             status=None, stream=None) -> bool:

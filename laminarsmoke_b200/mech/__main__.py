@@ -47,8 +47,8 @@ def main(argv=None) -> int:
     dims = arrays["dims"]
     print(f"{args.blob}: {int(dims[0])} species, {int(dims[1])} reactions")
     extras = [f"{len(arrays[k])} {what}" for k, what in (
-        ("plog_rxn", "PLOG"), ("cheb_rxn", "CHEB"), ("xplog_rxn", "PLOGMX/PLOGSP (oracle only)"),
-        ("xfo_rxn", "LOWMX/LOWSP (oracle only)")) if k in arrays]
+        ("plog_rxn", "PLOG"), ("cheb_rxn", "CHEB"), ("xplog_rxn", "PLOGMX/PLOGSP"),
+        ("xfo_rxn", "LOWMX/LOWSP")) if k in arrays]
     if extras:
         print("  reactions with " + ", ".join(extras))
     if "tr_eta" in arrays:

@@ -1,6 +1,6 @@
 """DRG-reduced integration in the oracle (solvers/laminarSMOKE/unsteady/DRG.hpp, chemistry_DRG.H).
 
-The CUDA form is not built yet; these tests pin the oracle's restatement: the analysis' limits
+These tests pin the oracle's restatement (tests/test_gpu_drg.py checks the CUDA form against it): the analysis' limits
 (epsilon 0 and 1, monotonicity, inert species), the reduced system with every species kept
 reproducing the full step, the solver options that reach only cell 0, the epsilon carried over
 between cells, and the temperature cut.

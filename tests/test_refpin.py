@@ -8,7 +8,7 @@ against small stand-ins for Eigen and two OpenSMOKE helpers, and drives it with 
 oracle's right-hand side and the per-cell calls of chemistry_DI.H:92-169.  On the same
 cells the oracle's restated integrator (oracle.cpp, class Gear) must give the same
 results bit for bit: Y, T, Q, statuses and all eight per-cell counters.  This pins
-SURVEY rows a8-a12 (finite-difference Jacobian, G = I - h r0 J and its LU, Newton
+the integrator (finite-difference Jacobian, G = I - h r0 J and its LU, Newton
 correction, step/order control, Gear constants) and the driver's pre- and
 post-processing to the reference's code; the oracle's RHS (thermodynamics and
 kinetics maps) remains a restatement.

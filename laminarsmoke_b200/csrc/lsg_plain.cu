@@ -31,7 +31,6 @@ plain_warp_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, Ste
     if (lane == 0) {
       W0.SC[0] = 0.; W0.SC[1] = 0.; W0.SC[2] = a.p; W0.SC[3] = o.energy ? 1. : 0.;
       W0.SC[4] = a.rho ? a.rho[cell] : 0.;
-      W0.SC[5] = 0.;
     }
     __syncwarp();
   }
@@ -159,7 +158,7 @@ drg_warp_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, StepO
   double* wsbase = (double*)(smem + ((L.bytes + 15u) & ~15u)) + (size_t)warp * warp_ws_doubles(L);
   WarpWS W = carve_ws(wsbase, L);
   if (lane == 0) {
-    W.SC[0] = 0.; W.SC[1] = 0.; W.SC[2] = a.p; W.SC[3] = o.energy ? 1. : 0.; W.SC[4] = 0.; W.SC[5] = 0.;
+    W.SC[0] = 0.; W.SC[1] = 0.; W.SC[2] = a.p; W.SC[3] = o.energy ? 1. : 0.; W.SC[4] = 0.;
   }
   __syncwarp();
   const int NC = L.nc, NR = L.nr;
@@ -168,7 +167,7 @@ drg_warp_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, StepO
   int st = 0, nsp = 0, nrx = 0;
   if (Tc > d.min_T) {
     // ---- analysis (DRG.hpp:150-273): rates at the cell's state, then the search from the key species ----
-    rhs_warp(&sL, Md, Mi, wsbase, lane < NC ? om : Tc, Tc);   // W.NET: net rates of progress
+    rhs_warp<false>(&sL, Md, Mi, wsbase, lane < NC ? om : Tc, Tc);   // W.NET: net rates of progress
     __syncwarp();
     const double eps = d.eps[cell];
     double den = 0.;   // sum_k |nu_ki r_k|, reactions in ascending order
@@ -222,8 +221,7 @@ drg_warp_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, StepO
       ndrop += keep ? 0 : 1;
     }
     for (int off = 16; off > 0; off >>= 1) ndrop += __shfl_xor_sync(kFull, ndrop, off);
-    if (lane == 0) W.SC[5] = 1.;   // the dropped reactions have zero rate from here on
-    __syncwarp();
+    __syncwarp();   // the mask is complete before the reduced system reads it
     // ---- the reduced system: lane l < ni owns the l-th important species, lane ni owns T ----
     const int ni = __popc(imp);
     int sp = NC;
@@ -235,7 +233,7 @@ drg_warp_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, StepO
     const int pos = (lane < NC && ((imp >> lane) & 1u)) ? __popc(imp & ((1u << lane) - 1u)) : -1;
     const double ys = __shfl_sync(kFull, om, sp < NC ? sp : 0);
     const double y0 = lane < ni ? ys : (lane == ni ? Tc : 0.);
-    GearWarp g;
+    GearWarpT<true> g;
     g.L = &sL;
     g.Md = Md;
     g.Mi = Mi;
@@ -244,7 +242,6 @@ drg_warp_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, StepO
     g.lane = lane;
     g.ne = ni + 1;
     g.active = lane < ni + 1;
-    g.drg = true;
     g.drg_ni = ni;
     g.drg_nc = NC;
     g.drg_sp = sp;
@@ -320,12 +317,12 @@ rhs_warp_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, long 
   if (cell >= ncells) return;
   double* wsbase = (double*)(smem + ((L.bytes + 15u) & ~15u)) + (size_t)warp * warp_ws_doubles(L);
   WarpWS W = carve_ws(wsbase, L);
-  if (lane == 0) { W.SC[0] = 0.; W.SC[1] = 0.; W.SC[2] = p; W.SC[3] = energy ? 1. : 0.; W.SC[4] = 0.; W.SC[5] = 0.; }
+  if (lane == 0) { W.SC[0] = 0.; W.SC[1] = 0.; W.SC[2] = p; W.SC[3] = energy ? 1. : 0.; W.SC[4] = 0.; }
   __syncwarp();
   const int NC = L.nc;
   const double yl = lane <= NC ? y[(size_t)lane * ld + cell] : 0.;
   const double T = __shfl_sync(kFull, yl, NC);
-  const double d = rhs_warp(&sL, Md, Mi, wsbase, yl, T);
+  const double d = rhs_warp<false>(&sL, Md, Mi, wsbase, yl, T);
   if (lane <= NC) dy[(size_t)lane * ld + cell] = d;
   if (lane == 0 && qr) qr[cell] = W.SC[1];
 }

@@ -41,9 +41,8 @@ struct WarpWS {
   double* KINF;   // [NFO] k_inf (cache)
   double* LOGF;   // [NFO] log10 Fcent (Troe) / SRI factor (cache)
   int* PIV;       // [32]
-  double* SC;     // [6] scalars: cached kinetic T, QR of the last call, P0, energy flag, rho0 (> 0: constant volume),
-                  // DRG flag (non-zero: the reactions marked in DROP have zero rate)
-  unsigned char* DROP;   // [NR] DRG-reduced step: 1 for a reaction the analysis dropped
+  double* SC;     // [6] scalars: cached kinetic T, QR of the last call, P0, energy flag, rho0 (> 0: constant volume)
+  unsigned char* DROP;   // [NR] DRG-reduced step: 1 for a reaction the analysis dropped (zero rate)
 };
 
 __host__ __device__ inline int warp_ws_doubles(const MechLayout& L) {
@@ -100,6 +99,7 @@ __device__ __forceinline__ double conc_factor(double nu, double c1) {
 // instruction footprint small).  L points to the layout in shared memory,
 // ws to this warp's workspace; the cached kinetic temperature, the last QR,
 // P0 and the energy flag live in ws's scalar slots.
+template <bool kDrg = false>
 __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const double* __restrict__ Md,
                                         const int* __restrict__ Mi, double* __restrict__ ws, double yl, double T) {
   const MechLayout& L = *Lp;
@@ -308,7 +308,9 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
         net -= rv;
       }
       net *= kMod;
-      if (W.SC[5] != 0. && W.DROP[j]) net = 0.;   // DRG-reduced system: dropped reactions (chemistry_DRG.H)
+      if constexpr (kDrg) {
+        if (W.DROP[j]) net = 0.;   // DRG-reduced system: dropped reactions (chemistry_DRG.H)
+      }
       W.NET[j] = net;
     }
   }
@@ -360,7 +362,9 @@ __device__ __noinline__ double rhs_warp(const MechLayout* __restrict__ Lp, const
 // Gear / multivalue BDF integrator state for one warp (one cell).  Vectors are
 // held one component per lane (registers) or in the per-warp shared arrays.
 // ---------------------------------------------------------------------------
-struct GearWarp {
+// kDrg: the DRG-reduced system (chemistry_DRG.H) instead of the full reactor.
+template <bool kDrg = false>
+struct GearWarpT {
   static constexpr int MAX_ORDER = 5, MIN_ORDER = 1;
   enum { H_DEC, H_CONST, H_INC };
   enum { O_DEC, O_CONST, O_INC };
@@ -394,7 +398,6 @@ struct GearWarp {
   // DRG-reduced system (BatchReactorHomogeneousConstantPressure.H:253-320): lane l < drg_ni owns species
   // drg_sp (the l-th important one), lane drg_ni owns T; as a lane of the full layout (species `lane`),
   // drg_pos is that species' reduced index or -1, drg_omega its fixed mass fraction.
-  bool drg = false;
   bool unconstrained = false;   // no minimum/maximum constraints: KernelDense's unconstrained increments
   int drg_ni = 0, drg_sp = 0, drg_pos = -1, drg_nc = 0;
   double drg_omega = 0.;
@@ -405,12 +408,15 @@ struct GearWarp {
   // f(y) of the system being integrated: the full reactor, or the DRG-reduced one evaluated through the
   // full layout (kept species fixed, dropped reactions at zero rate) and gathered back to the reduced lanes
   __device__ __forceinline__ double eval(double yl) {
-    if (!drg) return rhs_warp(L, Md, Mi, ws, yl, __shfl_sync(kFull, yl, ne - 1));
-    const double T = __shfl_sync(kFull, yl, drg_ni);
-    const double v = __shfl_sync(kFull, yl, drg_pos >= 0 ? drg_pos : 0);
-    const double yf = lane < drg_nc ? (drg_pos >= 0 ? v : drg_omega) : T;
-    const double df = rhs_warp(L, Md, Mi, ws, yf, T);
-    return __shfl_sync(kFull, df, drg_sp);
+    if constexpr (!kDrg) {
+      return rhs_warp<false>(L, Md, Mi, ws, yl, __shfl_sync(kFull, yl, ne - 1));
+    } else {
+      const double T = __shfl_sync(kFull, yl, drg_ni);
+      const double v = __shfl_sync(kFull, yl, drg_pos >= 0 ? drg_pos : 0);
+      const double yf = lane < drg_nc ? (drg_pos >= 0 ? v : drg_omega) : T;
+      const double df = rhs_warp<true>(L, Md, Mi, ws, yf, T);
+      return __shfl_sync(kFull, df, drg_sp);
+    }
   }
 
   __device__ __forceinline__ double rhs(double yl) {
@@ -451,7 +457,7 @@ struct GearWarp {
       const double ej = __shfl_sync(kFull, eps, j);
       const double mxj = __shfl_sync(kFull, maxv, j);
       double hJ;
-      if (unconstrained) {   // KernelDense.hpp:111-193 without maximum constraints
+      if (kDrg && unconstrained) {   // KernelDense.hpp:111-193 without maximum constraints
         hJ = ETA2 * fabs(fmax(yh, 1. / ej));
         const double hJf = hf / ej;
         hJ = fmax(hJ, hJf);
@@ -903,5 +909,6 @@ struct GearWarp {
     return status;
   }
 };
+using GearWarp = GearWarpT<false>;
 
 }  // namespace lsg

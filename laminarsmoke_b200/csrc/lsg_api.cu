@@ -975,7 +975,7 @@ int lsg_reaction_step_drg_device(lsg_ctx* c, int ncells, int nspecies, double* Y
   if (nspecies != L.nc) return LSG_ERR_ARG;
   if (!drg->key || drg->nkey < 1 || drg->nkey > L.nc) return LSG_ERR_ARG;
   if (!drg->band_T || !drg->band_eps || drg->nbands < 1 || drg->nbands > LSG_DRG_MAX_BANDS) return LSG_ERR_ARG;
-  if (L.nc + 1 > 32 || plain_smem_bytes(L) > 227 * 1024) return LSG_ERR_UNSUPPORTED;
+  if (L.nc + 1 > 32 || drg_smem_bytes(L) > 227 * 1024) return LSG_ERR_UNSUPPORTED;
   DrgArgs d{};
   for (int t = 0; t < drg->nkey; ++t) {
     if (drg->key[t] < 0 || drg->key[t] >= L.nc) return LSG_ERR_ARG;

@@ -60,6 +60,7 @@ struct DrgArgs {
   int* n_species;     // optional [ncells]: important species (0 for skipped cells)
   int* n_reactions;   // optional [ncells]: reactions kept
 };
+size_t drg_smem_bytes(const MechLayout& L);
 cudaError_t launch_drg_plain(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
                              const StepArgs& a, const DrgArgs& d, int* err, cudaStream_t stream);
 

@@ -155,7 +155,7 @@ drg_warp_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, StepO
   const int lane = threadIdx.x & 31;
   const long cell = (long)blockIdx.x * kPlainWarpsPerBlock + warp;
   if (cell >= a.ncells) return;
-  double* wsbase = (double*)(smem + ((L.bytes + 15u) & ~15u)) + (size_t)warp * warp_ws_doubles(L);
+  double* wsbase = (double*)(smem + ((L.bytes + 15u) & ~15u)) + (size_t)warp * drg_ws_doubles(L);
   WarpWS W = carve_ws(wsbase, L);
   if (lane == 0) {
     W.SC[0] = 0.; W.SC[1] = 0.; W.SC[2] = a.p; W.SC[3] = o.energy ? 1. : 0.; W.SC[4] = 0.;
@@ -357,10 +357,14 @@ cudaError_t launch_plain(const MechLayout& L, const unsigned char* mech_gmem, co
   return cudaGetLastError();
 }
 
+size_t drg_smem_bytes(const MechLayout& L) {
+  return ((L.bytes + 15u) & ~15u) + (size_t)kPlainWarpsPerBlock * drg_ws_doubles(L) * sizeof(double);
+}
+
 cudaError_t launch_drg_plain(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
                              const StepArgs& a, const DrgArgs& d, int* err, cudaStream_t stream) {
   if (a.ncells <= 0) return cudaSuccess;
-  const size_t smem = plain_smem_bytes(L);
+  const size_t smem = drg_smem_bytes(L);
   cudaError_t e = cudaFuncSetAttribute(drg_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   drg_eps_kernel<<<1, 32, 0, stream>>>(a.ncells, a.T, d);

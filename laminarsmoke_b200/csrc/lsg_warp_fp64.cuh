@@ -42,15 +42,17 @@ struct WarpWS {
   double* LOGF;   // [NFO] log10 Fcent (Troe) / SRI factor (cache)
   int* PIV;       // [32]
   double* SC;     // [6] scalars: cached kinetic T, QR of the last call, P0, energy flag, rho0 (> 0: constant volume)
-  unsigned char* DROP;   // [NR] DRG-reduced step: 1 for a reaction the analysis dropped (zero rate)
+  unsigned char* DROP;   // [NR] DRG-reduced step only (drg_ws_doubles): 1 for a reaction the analysis dropped
 };
 
 __host__ __device__ inline int warp_ws_doubles(const MechLayout& L) {
   const int n = L.nc + 1;
   auto even = [](int x) { return (x + 1) & ~1; };
-  return 8 * 32 * 2 + even(n * (n + 1)) * 2 + 32 * 3 + even(L.nr) * 3 + even(L.n_fo > 0 ? L.n_fo : 1) * 2 + 16 + 6 +
-         (L.nr + 7) / 8 + 1;
+  return 8 * 32 * 2 + even(n * (n + 1)) * 2 + 32 * 3 + even(L.nr) * 3 + even(L.n_fo > 0 ? L.n_fo : 1) * 2 + 16 + 6;
 }
+
+// The DRG kernel's per-warp workspace: the above and the dropped-reaction mask after it.
+__host__ __device__ inline int drg_ws_doubles(const MechLayout& L) { return warp_ws_doubles(L) + (L.nr + 7) / 8 + 1; }
 
 __device__ __forceinline__ WarpWS carve_ws(double* base, const MechLayout& L) {
   const int n = L.nc + 1;

@@ -61,7 +61,10 @@ extern "C" {
  * 127 species, an in-place multi-tile inverse in global memory above) and
  * solves with the inverse, refined on the FP64 residual of G until a
  * correction's weighted norm is below 1e-6; a matrix on which the refinement
- * stalls (FP32 cannot hold its conditioning) is refactorised by the FP64 LU. */
+ * stalls (FP32 cannot hold its conditioning) is refactorised by the FP64 LU.
+ * With LSG_TILE_AUTO and autotune = 1 the first step times both
+ * factorisations on a sample of the cells and keeps the faster
+ * (lsg_ctx_tuning). */
 
 /* counters per cell (lsg_reaction_step_device counters_out layout) */
 #define LSG_NCOUNTERS 8        /* steps, rhs, jacobians, factorisations, solves, error-test fails, convergence fails, jacobian rhs */

@@ -194,8 +194,8 @@ int lsg_reaction_step_sequence_device(lsg_ctx* ctx, int nsteps, int ncells, int 
  * solver's defaults (1e-10 absolute, 100 FLT_EPSILON relative, no bounds):
  * first_cell_options_only = 1 keeps that, 0 gives every cell the options.
  * Cells at or below min_T are left as they are (status 0).  Constant-pressure
- * reactor, FP64, one warp per cell: up to 31 species (LSG_ERR_UNSUPPORTED
- * above).  Options used from the context: rtol, atol, energy.  n_species /
+ * reactor, FP64: one warp per cell up to 31 species, one thread block per cell
+ * above (up to 511).  Options used from the context: rtol, atol, energy.  n_species /
  * n_reactions (optional, device): important species and reactions kept per
  * cell (the reference's drg_important_species / drg_important_reactions
  * fields), 0 for skipped cells. */

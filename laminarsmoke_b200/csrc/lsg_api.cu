@@ -975,7 +975,8 @@ int lsg_reaction_step_drg_device(lsg_ctx* c, int ncells, int nspecies, double* Y
   if (nspecies != L.nc) return LSG_ERR_ARG;
   if (!drg->key || drg->nkey < 1 || drg->nkey > L.nc) return LSG_ERR_ARG;
   if (!drg->band_T || !drg->band_eps || drg->nbands < 1 || drg->nbands > LSG_DRG_MAX_BANDS) return LSG_ERR_ARG;
-  if (L.nc + 1 > 32 || drg_smem_bytes(L) > 227 * 1024) return LSG_ERR_UNSUPPORTED;
+  const bool warp_form = L.nc + 1 <= 32;
+  if (warp_form && drg_smem_bytes(L) > 227 * 1024) return LSG_ERR_UNSUPPORTED;
   DrgArgs d{};
   for (int t = 0; t < drg->nkey; ++t) {
     if (drg->key[t] < 0 || drg->key[t] >= L.nc) return LSG_ERR_ARG;
@@ -1016,10 +1017,23 @@ int lsg_reaction_step_drg_device(lsg_ctx* c, int ncells, int nspecies, double* Y
   a.Q = Q;
   a.status = status;
   a.counters = counters;
-  if (launch_drg_plain(L, c->mech->d_buf, to_step_options(c->opt), a, d, c->d_err, (cudaStream_t)stream) !=
-      cudaSuccess) {
-    cudaGetLastError();
-    return LSG_ERR_CUDA;
+  if (warp_form) {
+    if (launch_drg_plain(L, c->mech->d_buf, to_step_options(c->opt), a, d, c->d_err, (cudaStream_t)stream) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return LSG_ERR_CUDA;
+    }
+  } else {   // one block per cell over the block form's work space
+    const int r = prepare_large(c);
+    if (r != LSG_OK) return r;
+    if (launch_drg_eps(ncells, T, d, (cudaStream_t)stream) != cudaSuccess) {
+      cudaGetLastError();
+      return LSG_ERR_CUDA;
+    }
+    const cudaError_t e = launch_drg_block(L, c->mech->d_buf, to_step_options(c->opt), a, d, c->bws,
+                                           c->bws_blocks, (cudaStream_t)stream);
+    if (e == cudaErrorInvalidValue) { cudaGetLastError(); return LSG_ERR_UNSUPPORTED; }
+    if (e != cudaSuccess) { cudaGetLastError(); return LSG_ERR_CUDA; }
   }
   c->launches += 2;
   return LSG_OK;

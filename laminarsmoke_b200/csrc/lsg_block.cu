@@ -17,6 +17,8 @@
 #include "lsg_kernels.h"
 #include "lsg_tc.cuh"
 
+#include <math_constants.h>
+
 namespace lsg {
 
 static __constant__ GearConsts c_gear_k;
@@ -83,6 +85,9 @@ struct BlockShared {
   int* PIV;      // [BT]
   int* ival;     // [BT/32 + 1] pivot search scratch
   int* PERM;     // [BT] the factorisation's row interchanges composed: row i of P b is b[PERM[i]]
+  // DRG-reduced step only (drg_block_kernel): the reduced <-> full layout exchange and the dropped reactions
+  double* DX;           // [BT]
+  unsigned char* DROP;  // [NR]
 };
 
 template <int BT>
@@ -133,7 +138,7 @@ __host__ __device__ inline size_t tcl_smem_bytes(const MechLayout& L) {
 // ---------------------------------------------------------------------------
 // RHS, block cooperative (thread i < NC owns species i, thread NC owns T).
 // ---------------------------------------------------------------------------
-template <int BT>
+template <int BT, bool kDrg = false>
 __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, const BlockShared& W,
                                          double* __restrict__ karr, double* __restrict__ ukeq,
                                          double* __restrict__ kinf, double* __restrict__ logf, double yl, double T,
@@ -328,7 +333,11 @@ __device__ __noinline__ double rhs_block(const MechLayout& L, const MechView M, 
         else rv *= ukeq[j] / kArr;
         net -= rv;
       }
-      W.NET[j] = net * kMod;
+      double r = net * kMod;
+      if constexpr (kDrg) {
+        if (W.DROP[j]) r = 0.;   // DRG-reduced system: dropped reactions (chemistry_DRG.H)
+      }
+      W.NET[j] = r;
     }
   }
   __syncthreads();
@@ -419,7 +428,8 @@ __device__ __forceinline__ double gemv_block(const T* __restrict__ A, int n, con
 // ---------------------------------------------------------------------------
 // Gear / multivalue BDF integrator for one block (one cell).
 // ---------------------------------------------------------------------------
-template <int BT, bool TC = false>
+// DRG: the DRG-reduced system (chemistry_DRG.H) instead of the full reactor (FP64 factors only).
+template <int BT, bool TC = false, bool DRG = false>
 struct GearBlock {
   enum { H_DEC, H_CONST, H_INC };
   enum { O_DEC, O_CONST, O_INC };
@@ -471,14 +481,39 @@ struct GearBlock {
   unsigned numberOfSteps, iterConvergence, iterConvergenceRate, iterConvergenceFailure, iterErrorFailure;
   unsigned numberOfConvergenceFailuresForOrderMax, stepOfLastJacobian;
   long long cnt[NCNT];
+  // DRG-reduced system (BatchReactorHomogeneousConstantPressure.H:253-320): thread l < drg_ni owns species
+  // drg_sp (the l-th important one), thread drg_ni owns T; as a thread of the full layout (species tid),
+  // drg_pos is that species' reduced index or -1, drg_omega its fixed mass fraction.
+  bool unconstrained = false;   // no minimum/maximum constraints: KernelDense's unconstrained increments
+  int drg_ni = 0, drg_sp = 0, drg_pos = -1, drg_nc = 0;
+  double drg_omega = 0.;
 
   __device__ __forceinline__ double& Z(int i) { return W.Z[i * BT + tid]; }
   __device__ __forceinline__ double& V(int i) { return W.V[i * BT + tid]; }
 
+  // f(y) of the system being integrated: the full reactor, or the DRG-reduced one evaluated through the
+  // full layout (kept species fixed, dropped reactions at zero rate) and gathered back
+  __device__ double eval(double yl) {
+    if constexpr (!DRG) {
+      const double T = bcast(yl, ne - 1, W.slot);
+      return rhs_block<BT>(*L, M, W, karr, ukeq, kinf, logf, yl, T, P0, energy, rho0);
+    } else {
+      __syncthreads();
+      W.DX[tid] = yl;   // reduced layout
+      __syncthreads();
+      const double T = W.DX[drg_ni];
+      const double yf = tid < drg_nc ? (drg_pos >= 0 ? W.DX[drg_pos] : drg_omega) : T;
+      const double df = rhs_block<BT, true>(*L, M, W, karr, ukeq, kinf, logf, yf, T, P0, energy, rho0);
+      __syncthreads();
+      W.DX[tid] = df;   // full layout
+      __syncthreads();
+      return W.DX[drg_sp];
+    }
+  }
+
   __device__ double rhs(double yl) {
     ++cnt[CNT_RHS];
-    const double T = bcast(yl, ne - 1, W.slot);
-    return rhs_block<BT>(*L, M, W, karr, ukeq, kinf, logf, yl, T, P0, energy, rho0);
+    return eval(yl);
   }
 
   __device__ double error_control(double w) {   // OpenSMOKEUtilities.hpp:689-701
@@ -509,15 +544,22 @@ struct GearBlock {
       const double yh = bcast(yl, j, W.slot);
       const double ej = bcast(eps, j, W.slot);
       const double mxj = bcast(maxv, j, W.slot);
-      const double a = fabs(yh), bb = fabs(1. / ej);
-      double hJ = ETA2 * (a > bb ? a : bb);
-      hJ = fmax(hJ, hf / ej);
-      hJ = fmax(hJ, ZERO_DER);
-      if (yh + hJ > mxj) hJ = -hJ;
+      double hJ;
+      if (DRG && unconstrained) {   // KernelDense.hpp:111-193 without maximum constraints
+        hJ = ETA2 * fabs(fmax(yh, 1. / ej));
+        hJ = fmax(hJ, hf / ej);
+        hJ = fmax(hJ, ZERO_DER);
+        hJ = fmin(hJ, 0.001 + 0.001 * fabs(yh));
+      } else {
+        const double a = fabs(yh), bb = fabs(1. / ej);
+        hJ = ETA2 * (a > bb ? a : bb);
+        hJ = fmax(hJ, hf / ej);
+        hJ = fmax(hJ, ZERO_DER);
+        if (yh + hJ > mxj) hJ = -hJ;
+      }
       double yp = yl;
       if (tid == j) yp += hJ;
-      const double T = bcast(yp, n - 1, W.slot);
-      const double aux = rhs_block<BT>(*L, M, W, karr, ukeq, kinf, logf, yp, T, P0, energy, rho0);
+      const double aux = eval(yp);
       ++cnt[CNT_JAC_RHS];
       const double hInv = 1. / hJ;
       if (active) J[(long)j * jld + tid] = hInv * (aux - fl);
@@ -1364,6 +1406,229 @@ __global__ void __launch_bounds__(BT, TC ? (BT == 128 ? 2 : 1) : (BT == 128 ? 4 
 }
 
 // ---------------------------------------------------------------------------
+// DRG-reduced step for mechanisms above 31 species (chemistry_DRG.H:86-200 with
+// DRG.hpp), one block per cell, FP64 factors: the block form of drg_warp_kernel.
+// Per cell above min_T: the analysis at the cell's (unclipped) state, the
+// reduced system (important species and T) by a fresh solver, the kept species
+// at their start values, the mass fractions normalised after the step.
+// Shared memory: the block form's, then DX [BT] doubles, warp counts, the
+// search queue [2 BT], the reached flags [BT] and the dropped mask [NR].
+// ---------------------------------------------------------------------------
+template <int BT>
+__host__ __device__ inline size_t drg_block_smem(const MechLayout& L) {
+  return ((block_shared_bytes<BT>(L) + 15) & ~(size_t)15) + sizeof(double) * BT + sizeof(int) * (BT / 32 + 4) +
+         sizeof(int) * 3 * BT + (size_t)L.nr + 16;
+}
+
+template <int BT>
+__global__ void __launch_bounds__(BT, BT == 128 ? 4 : (BT == 256 ? 2 : 1))
+    drg_block_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, StepOptions o, StepArgs a, DrgArgs d,
+                     double* __restrict__ ws_all) {
+  extern __shared__ __align__(16) unsigned char bsm[];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int NC = L.nc, NR = L.nr;
+  double* ws = ws_all + (size_t)blockIdx.x * block_ws_doubles(L);
+  double* Jp = ws;
+  double* Gp = ws + (size_t)(NC + 1) * (NC + 1);
+  double* karr = ws + 2 * (size_t)(NC + 1) * (NC + 1);
+  BlockShared W;
+  {
+    double* p = (double*)bsm;
+    W.Z = p; p += 8 * BT;
+    W.V = p; p += 8 * BT;
+    W.C = p; p += NC;
+    W.H = p; p += NC;
+    W.S = p; p += NC;
+    W.NET = p; p += L.nr;
+    W.X = p; p += BT;
+    W.red = p; p += BT / 32 + 1;
+    W.slot = p; p += 4;
+    W.PIV = (int*)p;
+    W.ival = W.PIV + BT;
+    W.PERM = W.ival + BT / 32 + 1;
+  }
+  unsigned char* ex = bsm + ((block_shared_bytes<BT>(L) + 15) & ~(size_t)15);
+  W.DX = (double*)ex;
+  int* WC = (int*)(W.DX + BT);          // per-warp counts
+  int* QU = WC + (BT / 32 + 4);         // the search queue (at most nkey + NC <= 2 NC entries)
+  int* IMPF = QU + 2 * BT;              // reached flags, then the reduced index -> species table
+  W.DROP = (unsigned char*)(IMPF + BT);
+  const MechView M{(const double*)mech_gmem, (const int*)(mech_gmem + (size_t)L.n_double * sizeof(double))};
+  for (long cell = blockIdx.x; cell < a.ncells; cell += gridDim.x) {
+    __syncthreads();
+    const double Tc = a.T[cell];
+    const double om = tid < NC ? a.Y[(size_t)tid * a.ld + cell] : 0.;
+    int st = 0, nsp = 0, nrx = 0;
+    if (Tc > d.min_T) {   // the same in every thread
+      // ---- analysis (DRG.hpp:150-273) ----
+      if (tid == 0) { W.slot[1] = 0.; W.slot[2] = 0.; }
+      __syncthreads();
+      rhs_block<BT>(L, M, W, karr, karr + L.nr, karr + 2 * L.nr, karr + 2 * L.nr + (L.n_fo > 0 ? L.n_fo : 1),
+                    tid < NC ? om : Tc, Tc, a.p, o.energy, 0.);   // W.NET: net rates of progress
+      __syncthreads();
+      const double eps = d.eps[cell];
+      double den = 0.;
+      if (tid < NC)
+        for (int k = 0; k < NR; ++k) {
+          const double nki = drg_net_nu(M, L, k, tid);
+          if (nki != 0.) den += fabs(nki * W.NET[k]);
+        }
+      W.DX[tid] = den;
+      IMPF[tid] = 0;
+      __syncthreads();
+      if (tid == 0)
+        for (int t = 0; t < d.nkey; ++t) {
+          QU[t] = d.key[t];
+          IMPF[d.key[t]] = 1;
+        }
+      __syncthreads();
+      int qlen = d.nkey;
+      for (int head = 0; head < qlen; ++head) {
+        const int q = QU[head];
+        const double denq = W.DX[q];
+        double num = 0.;
+        if (tid < NC)
+          for (int k = 0; k < NR; ++k) {
+            const double nq = drg_net_nu(M, L, k, q);
+            if (nq == 0.) continue;
+            if (drg_net_nu(M, L, k, tid) != 0.) num += fabs(nq * W.NET[k]);
+          }
+        const bool add = tid < NC && IMPF[tid] == 0 && num / (1.e-64 + denq) > eps;
+        const unsigned m = __ballot_sync(kFull, add);
+        if (lane == 0) WC[warp] = __popc(m);
+        __syncthreads();   // every thread has read IMPF and QU for this head
+        int before = 0, total = 0;
+        for (int w = 0; w < BT / 32; ++w) {
+          if (w < warp) before += WC[w];
+          total += WC[w];
+        }
+        if (add) {   // appended in ascending species order
+          QU[qlen + before + __popc(m & ((1u << lane) - 1u))] = tid;
+          IMPF[tid] = 1;
+        }
+        qlen += total;
+        __syncthreads();
+      }
+      // a reaction is dropped when one of its species (non-zero net coefficient) was not reached
+      int nd = 0;
+      {
+        const int* pp = M.I(L.prod_ptr);
+        const int* psp = M.I(L.prod_sp);
+        const int* rpp = M.I(L.reac_ptr);
+        const int* rsp = M.I(L.reac_sp);
+        for (int k = tid; k < NR; k += BT) {
+          bool keep = true;
+          for (int q = pp[k]; q < pp[k + 1]; ++q) {
+            const int sp = psp[q];
+            if (IMPF[sp] == 0 && drg_net_nu(M, L, k, sp) != 0.) keep = false;
+          }
+          for (int q = rpp[k]; q < rpp[k + 1]; ++q) {
+            const int sp = rsp[q];
+            if (IMPF[sp] == 0 && drg_net_nu(M, L, k, sp) != 0.) keep = false;
+          }
+          W.DROP[k] = keep ? 0 : 1;
+          nd += keep ? 0 : 1;
+        }
+      }
+      const double ndrop = bsum<BT>((double)nd, W.red);
+      // ---- the reduced system: thread l < ni owns the l-th important species, thread ni owns T ----
+      const bool imp = tid < NC && IMPF[tid] != 0;
+      const unsigned mi = __ballot_sync(kFull, imp);
+      __syncthreads();
+      if (lane == 0) WC[warp] = __popc(mi);
+      __syncthreads();
+      int before = 0, ni = 0;
+      for (int w = 0; w < BT / 32; ++w) {
+        if (w < warp) before += WC[w];
+        ni += WC[w];
+      }
+      const int pos = imp ? before + __popc(mi & ((1u << lane) - 1u)) : -1;
+      W.DX[tid] = om;   // full layout: the start mass fractions
+      __syncthreads();
+      if (imp) QU[pos] = tid;   // reduced index -> species
+      __syncthreads();
+      const int sp = tid < ni ? QU[tid] : NC;
+      const double y0 = tid < ni ? W.DX[sp] : (tid == ni ? Tc : 0.);
+      __syncthreads();
+      GearBlock<BT, false, true> g;
+      g.L = &L;
+      g.M = M;
+      g.W = W;
+      g.J = Jp;
+      g.jld = NC + 1;
+      g.G = Gp;
+      g.karr = karr;
+      g.ukeq = g.karr + L.nr;
+      g.kinf = g.ukeq + L.nr;
+      g.logf = g.kinf + (L.n_fo > 0 ? L.n_fo : 1);
+      g.P0 = a.p;
+      g.rho0 = 0.;
+      g.energy = o.energy;
+      g.tid = tid;
+      g.ne = ni + 1;
+      g.active = tid < ni + 1;
+      g.drg_ni = ni;
+      g.drg_nc = NC;
+      g.drg_sp = sp;
+      g.drg_pos = pos;
+      g.drg_omega = om;
+      // a fresh solver object per cell (chemistry_DRG.H): its own order-selection state and step limit
+      g.alfa2_4 = 0.8;
+      g.alfa2_5 = 0.8;
+      g.maximum_order = 5u;
+      g.max_number_steps = 500000u;
+      if (cell == 0 || !d.first_cell_options_only) {
+        g.abs_tol = o.atol;
+        g.rel_tol = o.rtol;
+        g.minv = tid < ni ? 0. : 200.;
+        g.maxv = tid < ni ? 1. : 6000.;
+        g.unconstrained = false;
+      } else {   // the solver's own defaults (MultiValueSolver.hpp:41-43), no constraints
+        g.abs_tol = 1.e-10;
+        g.rel_tol = 100. * kMachEpsFloat;
+        g.minv = -CUDART_INF;
+        g.maxv = CUDART_INF;
+        g.unconstrained = true;
+      }
+      g.b = g.deltab = g.f = g.va = g.vb = g.y = 0.;
+      g.eps = 0.;
+      if (tid == 0) { W.slot[1] = 0.; }
+      __syncthreads();
+      g.set_initial_conditions(a.t0, y0);
+      const double dtc = a.dt ? a.dt[cell] : a.dt_scalar;
+      st = g.solve_to(a.t0 + dtc);
+      // ---- scatter: the kept species' start values, the integrated ones, T; normalised ----
+      __syncthreads();
+      W.DX[tid] = g.y;   // reduced layout
+      __syncthreads();
+      const double Tf = W.DX[ni];
+      const double yf = pos >= 0 ? W.DX[pos] : om;
+      const double sum = bsum<BT>(tid < NC ? yf : 0., W.red);
+      if (tid < NC) a.Y[(size_t)tid * a.ld + cell] = yf / sum;
+      if (tid == 0) {
+        if (o.energy) a.T[cell] = Tf;
+        if (a.Q) a.Q[cell] = W.slot[2];
+        if (a.counters)
+          for (int k = 0; k < NCNT; ++k) a.counters[(size_t)cell * NCNT + k] = g.cnt[k];
+        if (a.nsteps) a.nsteps[cell] = (int)g.cnt[CNT_STEPS];
+      }
+      nsp = ni;
+      nrx = NR - (int)ndrop;
+    } else if (tid == 0) {
+      if (a.counters)
+        for (int k = 0; k < NCNT; ++k) a.counters[(size_t)cell * NCNT + k] = 0;
+      if (a.nsteps) a.nsteps[cell] = 0;
+    }
+    if (tid == 0) {
+      if (a.status) a.status[cell] = st;
+      if (d.n_species) d.n_species[cell] = nsp;
+      if (d.n_reactions) d.n_reactions[cell] = nrx;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Stand-alone tensor-core inverse (lsg_build_and_invert_g_device): persistent
 // blocks of 128 threads, one matrix at a time; G^-1 written column-major FP32.
 // ---------------------------------------------------------------------------
@@ -1673,6 +1938,28 @@ cudaError_t launch_rhs_block(const MechLayout& L, const unsigned char* mech_gmem
                                                                                      p, energy, qr, ws);
   }
   return cudaGetLastError();
+}
+
+template <int BT>
+cudaError_t drg_block_launch(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                             const StepArgs& a, const DrgArgs& d, double* ws, long nblocks, cudaStream_t stream) {
+  const size_t smem = drg_block_smem<BT>(L);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(drg_block_kernel<BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const long g = nblocks < a.ncells ? nblocks : a.ncells;
+  drg_block_kernel<BT><<<(unsigned)g, BT, smem, stream>>>(L, mech_gmem, o, a, d, ws);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_drg_block(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                             const StepArgs& a, const DrgArgs& d, double* ws, long nblocks, cudaStream_t stream) {
+  if (a.ncells <= 0) return cudaSuccess;
+  if (L.nc + 1 > kBlkMaxN || nblocks <= 0) return cudaErrorInvalidValue;
+  const int bt = block_threads(L);
+  if (bt == 128) return drg_block_launch<128>(L, mech_gmem, o, a, d, ws, nblocks, stream);
+  if (bt == 256) return drg_block_launch<256>(L, mech_gmem, o, a, d, ws, nblocks, stream);
+  return drg_block_launch<512>(L, mech_gmem, o, a, d, ws, nblocks, stream);
 }
 
 }  // namespace lsg

@@ -214,4 +214,22 @@ __device__ inline bool stage_bulk(void* smem_dst, const void* gsrc, uint32_t byt
   return ok != 0;
 }
 
+// Net stoichiometric coefficient of species s in reaction k, formed as the
+// reference's DRG constructor forms it: products added first, then reactants
+// subtracted (DRG.hpp:45-110).  Zero when s does not take part.
+__device__ __forceinline__ double drg_net_nu(const MechView& M, const MechLayout& L, int k, int s) {
+  const int* rp = M.I(L.reac_ptr);
+  const int* rsp = M.I(L.reac_sp);
+  const double* rnu = M.D(L.reac_nu);
+  const int* pp = M.I(L.prod_ptr);
+  const int* psp = M.I(L.prod_sp);
+  const double* pnu = M.D(L.prod_nu);
+  double v = 0.;
+  for (int q = pp[k]; q < pp[k + 1]; ++q)
+    if (psp[q] == s) v += pnu[q];
+  for (int q = rp[k]; q < rp[k + 1]; ++q)
+    if (rsp[q] == s) v -= rnu[q];
+  return v;
+}
+
 }  // namespace lsg

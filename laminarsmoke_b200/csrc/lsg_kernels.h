@@ -61,6 +61,10 @@ struct DrgArgs {
   int* n_reactions;   // optional [ncells]: reactions kept
 };
 size_t drg_smem_bytes(const MechLayout& L);
+cudaError_t launch_drg_eps(long ncells, const double* T, const DrgArgs& d, cudaStream_t stream);
+// more than 31 species: one block per cell over the block form's work space (ws, nblocks of it)
+cudaError_t launch_drg_block(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
+                             const StepArgs& a, const DrgArgs& d, double* ws, long nblocks, cudaStream_t stream);
 cudaError_t launch_drg_plain(const MechLayout& L, const unsigned char* mech_gmem, const StepOptions& o,
                              const StepArgs& a, const DrgArgs& d, int* err, cudaStream_t stream);
 

@@ -103,24 +103,6 @@ plain_warp_kernel(MechLayout L, const unsigned char* __restrict__ mech_gmem, Ste
 // normalised after the step.
 // ---------------------------------------------------------------------------
 
-// Net stoichiometric coefficient of species s in reaction k, formed as the
-// reference's DRG constructor forms it: products added first, then reactants
-// subtracted (DRG.hpp:45-110).  Zero when s does not take part.
-__device__ __forceinline__ double drg_net_nu(const MechView& M, const MechLayout& L, int k, int s) {
-  const int* rp = M.I(L.reac_ptr);
-  const int* rsp = M.I(L.reac_sp);
-  const double* rnu = M.D(L.reac_nu);
-  const int* pp = M.I(L.prod_ptr);
-  const int* psp = M.I(L.prod_sp);
-  const double* pnu = M.D(L.prod_nu);
-  double v = 0.;
-  for (int q = pp[k]; q < pp[k + 1]; ++q)
-    if (psp[q] == s) v += pnu[q];
-  for (int q = rp[k]; q < rp[k + 1]; ++q)
-    if (rsp[q] == s) v -= rnu[q];
-  return v;
-}
-
 // Each cell's epsilon: the first band whose temperature is above the cell's; a
 // cell above every band keeps the previous analysed cell's epsilon, and cells at
 // or below min_T are not analysed (chemistry_DRG.H).  The carry-over runs in cell
@@ -357,6 +339,12 @@ cudaError_t launch_plain(const MechLayout& L, const unsigned char* mech_gmem, co
   return cudaGetLastError();
 }
 
+cudaError_t launch_drg_eps(long ncells, const double* T, const DrgArgs& d, cudaStream_t stream) {
+  if (ncells <= 0) return cudaSuccess;
+  drg_eps_kernel<<<1, 32, 0, stream>>>(ncells, T, d);
+  return cudaGetLastError();
+}
+
 size_t drg_smem_bytes(const MechLayout& L) {
   return ((L.bytes + 15u) & ~15u) + (size_t)kPlainWarpsPerBlock * drg_ws_doubles(L) * sizeof(double);
 }
@@ -367,8 +355,7 @@ cudaError_t launch_drg_plain(const MechLayout& L, const unsigned char* mech_gmem
   const size_t smem = drg_smem_bytes(L);
   cudaError_t e = cudaFuncSetAttribute(drg_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  drg_eps_kernel<<<1, 32, 0, stream>>>(a.ncells, a.T, d);
-  e = cudaGetLastError();
+  e = launch_drg_eps(a.ncells, a.T, d, stream);
   if (e != cudaSuccess) return e;
   const long blocks = (a.ncells + kPlainWarpsPerBlock - 1) / kPlainWarpsPerBlock;
   drg_warp_kernel<<<(unsigned)blocks, kPlainWarpsPerBlock * 32, smem, stream>>>(L, mech_gmem, o, a, d, err);

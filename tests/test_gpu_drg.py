@@ -4,7 +4,8 @@ The oracle restates solvers/laminarSMOKE/unsteady/chemistry_DRG.H with DRG.hpp (
 per cell above min_T, the analysis at the cell's state, the reduced system integrated by a fresh solver,
 the solver options reaching cell 0 only (the reference's behaviour) or every cell, the epsilon of the
 previous analysed cell kept for a cell above every temperature band.  The GPU form is the plain warp
-kernel (FP64, the reference's operation order) on the reduced system.  Criteria: identical statuses,
+kernel (FP64, the reference's operation order) on the reduced system up to 31 species, one block per
+cell above.  Criteria: identical statuses,
 important-species and kept-reaction counts; T within 1e-6 relative and Y within 1e-9 absolute in every
 cell integrated with the configured tolerances; the cells integrated with the solver's defaults
 (relative 1e-5) within 1e-6 / 1e-7, most within 1e-9.
@@ -129,3 +130,37 @@ def test_drg_rejects_bad_arguments(cuda, h2co):
             ctx.step_drg_device(Y, T, 1e-5, key)
     with pytest.raises(lsg.LsgError):
         ctx.step_drg_device(Y, T, 1e-5, [0], bands=tuple((1e3 + k, 1e-2) for k in range(17)))
+
+
+@pytest.mark.parametrize("pad", [106, 150], ids=["n121-bt128", "n165-bt256"])
+def test_drg_block_form_against_oracle(cuda, pad):
+    """Above 31 species the DRG step runs one block per cell (drg_block_kernel): H2/CO chemistry padded with
+    inert species, which the search never reaches, against the oracle on the same mechanism.  The block form
+    sums over threads in tree order, so a few cells may take another step sequence: statuses and counts
+    identical, T within 1e-6, Y within 1e-9 in 90 % of the cells and 1e-7 in all."""
+    from laminarsmoke_b200 import lsg, mech
+    from laminarsmoke_b200.mech import blob
+    from oracle.oracle import OracleMechanism
+    data, species = mech.load(f"h2co+{pad}")
+    A, _ = blob.unpack(data)
+    n = 96
+    Y, T = cells.h2co_mixing(species[:14], A["mw"][:14], n, seed=25)
+    Yp = np.zeros((n, len(species)))
+    Yp[:, :14] = 0.5 * Y
+    Yp[:, 14:] = 0.5 / (len(species) - 14)
+    T[::9] = 280.0
+    key = [species.index(s) for s in ("H2", "O2", "CO")]
+    kw = dict(bands=((1200.0, 1e-3), (1e6, 1e-2)), epsilon0=1e-2, min_T=300.0, first_cell_options_only=False)
+    ctx = lsg.ReactionStep(lsg.Mechanism(data))
+    Yg, Tg, Qg, sg, cg, ng, rg = _run(ctx, Yp, T, key, cuda, **kw)
+    Yo, To, Qo, so, co, no, ro = OracleMechanism(data).reaction_step_drg(Yp, T, 1e-5, key, **kw)
+    np.testing.assert_array_equal(sg, so)
+    np.testing.assert_array_equal(ng, no)
+    np.testing.assert_array_equal(rg, ro)
+    assert ng.max() <= 14
+    dT = np.abs(Tg - To) / To
+    dY = np.abs(Yg - Yo).max(axis=1)
+    print(f"DRG block form, {len(species)} species: max rel T {dT.max():.2e}, max abs Y {dY.max():.2e}, "
+          f"within 1e-9 {np.mean(dY <= 1e-9):.3f}")
+    assert dT.max() <= 1e-6
+    assert np.mean(dY <= 1e-9) >= 0.9 and dY.max() <= 1e-7

@@ -132,8 +132,9 @@ def test_drg_rejects_bad_arguments(cuda, h2co):
         ctx.step_drg_device(Y, T, 1e-5, [0], bands=tuple((1e3 + k, 1e-2) for k in range(17)))
 
 
-@pytest.mark.parametrize("pad", [106, 150], ids=["n121-bt128", "n165-bt256"])
-def test_drg_block_form_against_oracle(cuda, pad):
+@pytest.mark.parametrize("pad,first_only", [(106, False), (150, False), (106, True)],
+                         ids=["n121-bt128", "n165-bt256", "n121-cell0-options"])
+def test_drg_block_form_against_oracle(cuda, pad, first_only):
     """Above 31 species the DRG step runs one block per cell (drg_block_kernel): H2/CO chemistry padded with
     inert species, which the search never reaches, against the oracle on the same mechanism.  The block form
     sums over threads in tree order, so a few cells may take another step sequence: statuses and counts
@@ -150,7 +151,7 @@ def test_drg_block_form_against_oracle(cuda, pad):
     Yp[:, 14:] = 0.5 / (len(species) - 14)
     T[::9] = 280.0
     key = [species.index(s) for s in ("H2", "O2", "CO")]
-    kw = dict(bands=((1200.0, 1e-3), (1e6, 1e-2)), epsilon0=1e-2, min_T=300.0, first_cell_options_only=False)
+    kw = dict(bands=((1200.0, 1e-3), (1e6, 1e-2)), epsilon0=1e-2, min_T=300.0, first_cell_options_only=first_only)
     ctx = lsg.ReactionStep(lsg.Mechanism(data))
     Yg, Tg, Qg, sg, cg, ng, rg = _run(ctx, Yp, T, key, cuda, **kw)
     Yo, To, Qo, so, co, no, ro = OracleMechanism(data).reaction_step_drg(Yp, T, 1e-5, key, **kw)

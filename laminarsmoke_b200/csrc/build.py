@@ -51,7 +51,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
             continue
         cmd = [nvcc()] + ARCH + COMMON + extra + ["-c", s, "-o", o]
         if src.endswith(".cpp"):
-            cmd = [nvcc()] + COMMON + ["-x", "c++", "-c", s, "-o", o]
+            cmd = [nvcc()] + COMMON + ["-Wno-deprecated-gpu-targets", "-x", "c++", "-c", s, "-o", o]
         if verbose:
             cmd += ["-Xptxas", "-v"] if src.endswith(".cu") else []
             print(" ".join(cmd), flush=True)

@@ -216,6 +216,14 @@ int lsg_reaction_step_drg_device(lsg_ctx* ctx, int ncells, int nspecies, double*
                                  const lsg_drg_options* drg, double* Q_dev, int* status_dev, int* n_species_dev,
                                  int* n_reactions_dev, long long* counters_dev, void* stream);
 
+/* The same from host fields, as lsg_reaction_step takes them (Y_species: NC
+ * pointers to ncells mass fractions; T, dt, Q, status, n_species, n_reactions
+ * host arrays of ncells, the outputs optional); synchronous.  Q keeps the
+ * caller's values for the cells at or below min_T. */
+int lsg_reaction_step_drg(lsg_ctx* ctx, int ncells, int nspecies, double* const* Y_species, double* T, double p,
+                          double t0, const double* dt, double dt_scalar, const lsg_drg_options* drg, double* Q,
+                          int* status, int* n_species, int* n_reactions);
+
 /* ---- reaction step, constant-volume reactor ------------------------------
  * The branch of chemistry_DI.H taken with constPressureBatchReactor false
  * (:168-203): BatchReactorHomogeneousConstantVolume::SetReactor(V, P, rho)

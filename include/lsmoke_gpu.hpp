@@ -26,6 +26,7 @@
 
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "lsmoke_gpu.h"
@@ -95,8 +96,58 @@ class Mechanism {
 };
 
 /* The reactor settings every cell of a call shares. */
+/* The DRG settings of the reference's DRG dictionary (solvers/laminarSMOKE/unsteady/chemistry_DRG.H with
+ * DRG.hpp): key species indices, (temperature, epsilon) bands, the minimum temperature.  Set on the reactor
+ * with SetDRG, as the reference does; the solver then runs the DRG-reduced step over the field and the
+ * important species / reactions of each cell are read back here. */
+class DRG {
+ public:
+  explicit DRG(std::vector<int> key_species) : key_(std::move(key_species)) {
+    if (key_.empty()) throw Error("DRG: no key species", LSG_ERR_ARG);
+  }
+  /* A cell takes the epsilon of the first band whose temperature is above its own. */
+  void SetTemperatureBands(const std::vector<double>& T, const std::vector<double>& epsilon) {
+    if (T.empty() || T.size() != epsilon.size() || T.size() > LSG_DRG_MAX_BANDS)
+      throw Error("DRG::SetTemperatureBands", LSG_ERR_ARG);
+    band_T_ = T;
+    band_eps_ = epsilon;
+  }
+  void SetEpsilon(double epsilon0) { eps0_ = epsilon0; }
+  void SetMinimumTemperature(double T) { min_T_ = T; }
+  /* true (the reference's behaviour): the solver options reach the first cell only. */
+  void SetOptionsOnFirstCellOnly(bool flag) { first_only_ = flag; }
+  const std::vector<int>& NumberOfImportantSpecies() const { return n_species_; }
+  const std::vector<int>& NumberOfImportantReactions() const { return n_reactions_; }
+
+  lsg_drg_options options() const {
+    lsg_drg_options o{};
+    o.key = key_.data();
+    o.nkey = (int)key_.size();
+    o.band_T = band_T_.data();
+    o.band_eps = band_eps_.data();
+    o.nbands = (int)band_T_.size();
+    o.epsilon0 = eps0_;
+    o.min_T = min_T_;
+    o.first_cell_options_only = first_only_ ? 1 : 0;
+    return o;
+  }
+  std::vector<int>& n_species() { return n_species_; }
+  std::vector<int>& n_reactions() { return n_reactions_; }
+
+ private:
+  std::vector<int> key_;
+  std::vector<double> band_T_{1.e6}, band_eps_{1.e-2};
+  double eps0_ = 1.e-2;
+  double min_T_ = 300.;
+  bool first_only_ = true;
+  std::vector<int> n_species_, n_reactions_;
+};
+
 class BatchReactorHomogeneousConstantPressure {
  public:
+  /* The reduced system of chemistry_DRG.H (nullptr: the full reactor). */
+  void SetDRG(DRG* drg) { drg_ = drg; }
+  DRG* drg() const { return drg_; }
   void SetReactor(double P0) {
     if (!(P0 > 0.)) throw Error("SetReactor", LSG_ERR_ARG);
     P0_ = P0;
@@ -108,6 +159,7 @@ class BatchReactorHomogeneousConstantPressure {
  private:
   double P0_ = 101325.;
   bool energy_ = true;
+  DRG* drg_ = nullptr;
 };
 
 /* One context: the batched counterpart of the reference's solver object. */
@@ -187,6 +239,15 @@ class MultiValueSolver {
     status_.assign(n_, 0);
     nsteps_.assign(n_, 0);
     Q_.assign(n_, 0.);
+    if (DRG* drg = reactor_.drg()) {   // chemistry_DRG.H: the reduced step of every cell
+      const lsg_drg_options o = drg->options();
+      drg->n_species().assign(n_, 0);
+      drg->n_reactions().assign(n_, 0);
+      check(lsg_reaction_step_drg(ctx_, n_, mech_.NumberOfSpecies(), Y_, T_, reactor_.P0(), t0_, dt, dt_scalar, &o,
+                                  Q_.data(), status_.data(), drg->n_species().data(), drg->n_reactions().data()),
+            "lsg_reaction_step_drg");
+      return status_;
+    }
     check(lsg_reaction_step(ctx_, n_, mech_.NumberOfSpecies(), Y_, T_, reactor_.P0(), t0_, dt, dt_scalar,
                             Q_.data(), status_.data(), nsteps_.data()),
           "lsg_reaction_step");

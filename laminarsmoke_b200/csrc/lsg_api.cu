@@ -1039,6 +1039,46 @@ int lsg_reaction_step_drg_device(lsg_ctx* c, int ncells, int nspecies, double* Y
   return LSG_OK;
 }
 
+// The DRG-reduced step from host fields: staged through the context's device buffers (the caller's Q is copied
+// in first, so that skipped cells keep it, as the device entry leaves it).
+int lsg_reaction_step_drg(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, double* T, double p, double t0,
+                          const double* dt, double dt_scalar, const lsg_drg_options* drg, double* Q, int* status,
+                          int* n_species, int* n_reactions) {
+  if (!c || ncells < 0 || !Ys || !T || !drg) return LSG_ERR_ARG;
+  if (nspecies != c->mech->host.layout.nc) return LSG_ERR_ARG;
+  for (int i = 0; i < nspecies; ++i) if (!Ys[i]) return LSG_ERR_ARG;
+  if (!(p > 0.)) return LSG_ERR_ARG;
+  if (ncells == 0) return LSG_OK;
+  if (cudaSetDevice(c->device) != cudaSuccess) return LSG_ERR_CUDA;
+  int r = ensure_capacity(c, ncells);
+  if (r != LSG_OK) return r;
+  cudaStream_t s = c->stream;
+  const size_t nb = sizeof(double) * (size_t)ncells;
+  for (int i = 0; i < nspecies; ++i)
+    if (cudaMemcpyAsync(c->dY + (size_t)i * c->cap, Ys[i], nb, cudaMemcpyHostToDevice, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (cudaMemcpyAsync(c->dT, T, nb, cudaMemcpyHostToDevice, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (dt && cudaMemcpyAsync(c->ddt, dt, nb, cudaMemcpyHostToDevice, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (Q && cudaMemcpyAsync(c->dQ, Q, nb, cudaMemcpyHostToDevice, s) != cudaSuccess) return LSG_ERR_CUDA;
+  int* d_nrx = (int*)c->drho;   // the density buffer is free here (constant pressure)
+  r = lsg_reaction_step_drg_device(c, ncells, nspecies, c->dY, c->cap, c->dT, p, t0, dt ? c->ddt : nullptr, dt_scalar,
+                                   drg, Q ? c->dQ : nullptr, status ? c->dstatus : nullptr,
+                                   n_species ? c->dnsteps : nullptr, n_reactions ? d_nrx : nullptr, nullptr, s);
+  if (r != LSG_OK) return r;
+  for (int i = 0; i < nspecies; ++i)
+    if (cudaMemcpyAsync(Ys[i], c->dY + (size_t)i * c->cap, nb, cudaMemcpyDeviceToHost, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (cudaMemcpyAsync(T, c->dT, nb, cudaMemcpyDeviceToHost, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (Q && cudaMemcpyAsync(Q, c->dQ, nb, cudaMemcpyDeviceToHost, s) != cudaSuccess) return LSG_ERR_CUDA;
+  const size_t ni = sizeof(int) * (size_t)ncells;
+  if (status && cudaMemcpyAsync(status, c->dstatus, ni, cudaMemcpyDeviceToHost, s) != cudaSuccess) return LSG_ERR_CUDA;
+  if (n_species && cudaMemcpyAsync(n_species, c->dnsteps, ni, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return LSG_ERR_CUDA;
+  if (n_reactions && cudaMemcpyAsync(n_reactions, d_nrx, ni, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return LSG_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return LSG_ERR_CUDA;
+  int flags = 0;
+  return lsg_ctx_check(c, &flags);
+}
+
 int lsg_reaction_step(lsg_ctx* c, int ncells, int nspecies, double* const* Ys, double* T, double p, double t0,
                       const double* dt, double dt_scalar, double* Q, int* status, int* nsteps) {
   return host_step(c, ncells, nspecies, Ys, T, p, nullptr, t0, dt, dt_scalar, Q, status, nsteps);

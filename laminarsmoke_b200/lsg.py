@@ -53,7 +53,7 @@ EXPORTS = (
     "lsg_reaction_step_cv", "lsg_reaction_step_cv_device", "lsg_steady_sources_device",
     "lsg_mech_transport_info", "lsg_properties_device", "lsg_properties", "lsg_build_and_invert_g_device",
     "lsg_reaction_step_sequence_device", "lsg_jacobian_device", "lsg_steady_sources_sparse_device",
-    "lsg_reaction_step_drg_device",
+    "lsg_reaction_step_drg_device", "lsg_reaction_step_drg",
 )
 
 class DrgOptions(C.Structure):
@@ -104,6 +104,8 @@ def lib():
     L.lsg_steady_sources_sparse_device.argtypes = [vp, i, i, vp, vp, l, vp, d, i, i, vp, vp, l, vp]
     L.lsg_reaction_step_drg_device.argtypes = [vp, i, i, vp, l, vp, d, d, vp, d, C.POINTER(DrgOptions), vp, vp, vp,
                                                vp, vp, vp]
+    L.lsg_reaction_step_drg.argtypes = [vp, i, i, C.POINTER(vp), vp, d, d, vp, d, C.POINTER(DrgOptions), vp, vp, vp,
+                                        vp]
     L.lsg_strerror.argtypes = [i]
     L.lsg_strerror.restype = C.c_char_p
     L.lsg_abi_version.restype = i
@@ -331,6 +333,30 @@ class ReactionStep:
         _check(lib().lsg_reaction_step_drg_device(
             self.h, n, nc, Y.data_ptr(), ld, T.data_ptr(), p, t0, dtp, dts, C.byref(o), ptr(Q), ptr(status),
             ptr(n_species), ptr(n_reactions), ptr(counters), _stream_handle(stream)), "lsg_reaction_step_drg_device")
+
+    def step_drg(self, Y_species: np.ndarray, T: np.ndarray, dt, key, bands=((1.e6, 1.e-2),), epsilon0: float = 1.e-2,
+                 min_T: float = 300.0, first_cell_options_only: bool = True, p: float = 101325.0, t0: float = 0.0):
+        """lsg_reaction_step_drg from host arrays: Y_species [NC, ncells] (C-contiguous float64) and T
+        [ncells], updated in place.  Returns (Q, status, n_species, n_reactions)."""
+        nc, n = Y_species.shape
+        if Y_species.dtype != np.float64 or not Y_species.flags.c_contiguous or T.dtype != np.float64:
+            raise TypeError("Y_species [NC, ncells] and T must be C-contiguous float64")
+        rows = (C.c_void_p * nc)(*[Y_species[i].ctypes.data for i in range(nc)])
+        k = (C.c_int * len(key))(*[int(x) for x in key])
+        bt = (C.c_double * len(bands))(*[float(b[0]) for b in bands])
+        be = (C.c_double * len(bands))(*[float(b[1]) for b in bands])
+        o = DrgOptions(C.cast(k, C.c_void_p), len(key), C.cast(bt, C.c_void_p), C.cast(be, C.c_void_p), len(bands),
+                       float(epsilon0), float(min_T), int(bool(first_cell_options_only)))
+        dt_arr = None if np.ndim(dt) == 0 else np.ascontiguousarray(dt, dtype=np.float64)
+        Q = np.zeros(n)
+        st = np.zeros(n, dtype=np.int32)
+        nsp = np.zeros(n, dtype=np.int32)
+        nrx = np.zeros(n, dtype=np.int32)
+        _check(lib().lsg_reaction_step_drg(
+            self.h, n, nc, C.cast(rows, C.POINTER(C.c_void_p)), T.ctypes.data, p, t0,
+            None if dt_arr is None else dt_arr.ctypes.data, 0.0 if dt_arr is not None else float(dt), C.byref(o),
+            Q.ctypes.data, st.ctypes.data, nsp.ctypes.data, nrx.ctypes.data), "lsg_reaction_step_drg")
+        return Q, st, nsp, nrx
 
     def step_sequence_graph(self, Y, T, dt: float, nsteps: int, p: float = 101325.0, t0: float = 0.0, Q=None,
                             status=None, stream=None) -> bool:

@@ -25,6 +25,15 @@ int main(int argc, char** argv) {
   try { reactor.SetReactor(-1.); return 11; } catch (const lsmoke::Error& e) { if (e.code() != LSG_ERR_ARG) return 12; }
   const char bad[16] = "NOTAMECHANISM00";
   try { lsmoke::Mechanism m(lsmoke::Blob{bad, 16}); return 13; } catch (const lsmoke::Error& e) { if (e.code() != LSG_ERR_MECH) return 14; }
+  // the DRG settings (chemistry_DRG.H), set on the reactor as the reference does
+  try { lsmoke::DRG none(std::vector<int>{}); return 17; } catch (const lsmoke::Error& e) { if (e.code() != LSG_ERR_ARG) return 18; }
+  lsmoke::DRG drg({0, 1});
+  try { drg.SetTemperatureBands({1000.}, {1e-2, 1e-3}); return 19; } catch (const lsmoke::Error& e) { if (e.code() != LSG_ERR_ARG) return 20; }
+  drg.SetTemperatureBands({1200., 1e6}, {1e-3, 1e-2});
+  if (drg.options().nbands != 2 || drg.options().nkey != 2 || drg.options().first_cell_options_only != 1) return 21;
+  reactor.SetDRG(&drg);
+  if (reactor.drg() != &drg) return 22;
+  reactor.SetDRG(nullptr);
   if (argc < 5) {
     // the property map's interface compiles against the same header (its C entry point is tested on the GPU)
     void (lsmoke::TransportPropertiesMap::*ev)(int, const double*, const double*, const double*,

@@ -165,3 +165,27 @@ def test_drg_block_form_against_oracle(cuda, pad, first_only):
           f"within 1e-9 {np.mean(dY <= 1e-9):.3f}")
     assert dT.max() <= 1e-6
     assert np.mean(dY <= 1e-9) >= 0.9 and dY.max() <= 1e-7
+
+
+def test_drg_host_entry_equals_device_entry(cuda, h2co):
+    """lsg_reaction_step_drg (host fields, staged through the context) gives the device entry's results bit for
+    bit, and leaves Q of the skipped cells as the caller had it."""
+    from laminarsmoke_b200 import lsg
+    data, species, A = h2co
+    n = 200
+    Y, T = cells.h2co_mixing(species, A["mw"], n, seed=26)
+    T[::10] = 280.0
+    key = [species.index(s) for s in ("H2", "O2", "CO")]
+    kw = dict(bands=((1200.0, 1e-3), (1e6, 1e-2)), epsilon0=1e-2, min_T=300.0, first_cell_options_only=True)
+    ctx = lsg.ReactionStep(lsg.Mechanism(data))
+    Yd, Td, Qd, sd, _, nd, rd = _run(ctx, Y, T, key, cuda, **kw)
+    Yh = np.ascontiguousarray(Y.T).copy()
+    Th = T.copy()
+    Qh, sh, nh, rh = ctx.step_drg(Yh, Th, 1e-5, key, **kw)
+    np.testing.assert_array_equal(sh, sd)
+    np.testing.assert_array_equal(nh, nd)
+    np.testing.assert_array_equal(rh, rd)
+    np.testing.assert_array_equal(Th, Td)
+    np.testing.assert_array_equal(Yh.T, Yd)
+    np.testing.assert_array_equal(Qh, Qd)
+    assert (Qh[T <= 300.0] == 0.0).all()

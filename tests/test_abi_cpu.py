@@ -103,3 +103,48 @@ def test_loader_rejects_corrupt_headers_and_tables_without_gpu():
     ptr[3], ptr[4] = ptr[4], ptr[3]                          # same length and end, decreasing inside
     bad["reac_ptr"] = ptr
     assert load(blob.pack(bad, species)) == -2
+
+
+_LAYOUT = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "lsmoke_gpu.h"
+#define F(T, m) printf(#T " " #m " %zu\n", offsetof(T, m))
+int main(void) {
+  printf("lsg_options size %zu\n", sizeof(lsg_options));
+  F(lsg_options, rtol); F(lsg_options, max_steps); F(lsg_options, precision); F(lsg_options, alfa2_4);
+  F(lsg_options, maximum_order); F(lsg_options, tile); F(lsg_options, autotune); F(lsg_options, jacobian);
+  printf("lsg_drg_options size %zu\n", sizeof(lsg_drg_options));
+  F(lsg_drg_options, key); F(lsg_drg_options, nkey); F(lsg_drg_options, band_T); F(lsg_drg_options, band_eps);
+  F(lsg_drg_options, nbands); F(lsg_drg_options, epsilon0); F(lsg_drg_options, min_T);
+  F(lsg_drg_options, first_cell_options_only);
+  return 0;
+}
+"""
+
+
+def test_ctypes_structs_match_the_header_layout(tmp_path):
+    """The ctypes mirrors of lsg_options and lsg_drg_options have the C compiler's sizes and offsets."""
+    import shutil
+    import subprocess
+    from laminarsmoke_b200 import lsg
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "layout.c"
+    src.write_text(_LAYOUT)
+    exe = tmp_path / "layout"
+    subprocess.check_call([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    out = subprocess.check_output([str(exe)], text=True).split("\n")
+    got = {}
+    for line in out:
+        parts = line.split()
+        if len(parts) == 3:
+            got[(parts[0], parts[1])] = int(parts[2])
+    assert got[("lsg_options", "size")] == C.sizeof(lsg.Options)
+    assert got[("lsg_drg_options", "size")] == C.sizeof(lsg.DrgOptions)
+    for (struct, field), off in got.items():
+        if field == "size":
+            continue
+        cls = lsg.Options if struct == "lsg_options" else lsg.DrgOptions
+        assert getattr(cls, field).offset == off, (struct, field)

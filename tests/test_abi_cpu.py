@@ -118,13 +118,17 @@ int main(void) {
   F(lsg_drg_options, key); F(lsg_drg_options, nkey); F(lsg_drg_options, band_T); F(lsg_drg_options, band_eps);
   F(lsg_drg_options, nbands); F(lsg_drg_options, epsilon0); F(lsg_drg_options, min_T);
   F(lsg_drg_options, first_cell_options_only);
+  printf("lsg_property_options size %zu\n", sizeof(lsg_property_options));
+  F(lsg_property_options, energy); F(lsg_property_options, simplified_transport); F(lsg_property_options, lewis);
+  printf("lsg_property_fields size %zu\n", sizeof(lsg_property_fields));
+  F(lsg_property_fields, X); F(lsg_property_fields, cp_species); F(lsg_property_fields, Dsoret);
   return 0;
 }
 """
 
 
 def test_ctypes_structs_match_the_header_layout(tmp_path):
-    """The ctypes mirrors of lsg_options and lsg_drg_options have the C compiler's sizes and offsets."""
+    """The ctypes mirrors of the ABI's structs have the C compiler's sizes and offsets."""
     import shutil
     import subprocess
     from laminarsmoke_b200 import lsg
@@ -141,10 +145,11 @@ def test_ctypes_structs_match_the_header_layout(tmp_path):
         parts = line.split()
         if len(parts) == 3:
             got[(parts[0], parts[1])] = int(parts[2])
-    assert got[("lsg_options", "size")] == C.sizeof(lsg.Options)
-    assert got[("lsg_drg_options", "size")] == C.sizeof(lsg.DrgOptions)
+    classes = {"lsg_options": lsg.Options, "lsg_drg_options": lsg.DrgOptions,
+               "lsg_property_options": lsg.PropertyOptions, "lsg_property_fields": lsg.PropertyFields}
     for (struct, field), off in got.items():
+        cls = classes[struct]
         if field == "size":
-            continue
-        cls = lsg.Options if struct == "lsg_options" else lsg.DrgOptions
-        assert getattr(cls, field).offset == off, (struct, field)
+            assert off == C.sizeof(cls), struct
+        else:
+            assert getattr(cls, field).offset == off, (struct, field)
